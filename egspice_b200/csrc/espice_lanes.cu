@@ -1,0 +1,777 @@
+// The C ABI of include/espice_lanes.h: the host lane driver (the role of
+// ESPice's GpuLanes, src/analysis/gpu/lanes.zig) over the sm_100a lane
+// kernels. One handle owns every device buffer of its templates; calls on a
+// handle are serialized on its stream.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/espice_lanes.h"
+#include "lane_kernels.cuh"
+#include "tape.h"
+
+using namespace espl;
+
+namespace {
+
+constexpr uint32_t kBlock = 128;
+constexpr uint32_t kGround = ESPL_GROUND;
+
+uint32_t terms_of(uint32_t kind) {
+    switch (kind) {
+    case ESPL_RES: return ESPL_RES_TERMS;
+    case ESPL_CAP: return ESPL_CAP_TERMS;
+    case ESPL_VSRC: return ESPL_VSRC_TERMS;
+    case ESPL_ISRC: return ESPL_ISRC_TERMS;
+    case ESPL_DIODE: return ESPL_DIODE_TERMS;
+    case ESPL_MOS1: return ESPL_MOS1_TERMS;
+    }
+    return 0;
+}
+
+uint32_t params_of(uint32_t kind) {
+    switch (kind) {
+    case ESPL_RES: return ESPL_RES_PARAMS;
+    case ESPL_CAP: return ESPL_CAP_PARAMS;
+    case ESPL_VSRC: case ESPL_ISRC: return ESPL_SRC_PARAMS;
+    case ESPL_DIODE: return ESPL_DIODE_PARAMS;
+    case ESPL_MOS1: return ESPL_MOS1_PARAMS;
+    }
+    return 0;
+}
+
+bool stamps(uint32_t kind, uint32_t r, uint32_t c) {
+    switch (kind) {
+    case ESPL_RES: case ESPL_CAP: case ESPL_DIODE: return true;
+    case ESPL_VSRC: return (r < 2 && c == 2) || (r == 2 && c < 2);
+    case ESPL_MOS1: return r != 1;
+    }
+    return false;
+}
+
+struct KindHost {
+    uint32_t count = 0;
+    std::vector<uint32_t> term;   // rows, ground -> n
+    std::vector<uint32_t> slot;   // [count][nt][nt], ground/unused -> nnz
+    std::vector<double> param;    // [count][np][P] lane-major, padded lanes copy lane 0
+};
+
+struct Group {
+    uint32_t n = 0, nnz = 0, lanes = 0, P = 0, lane0 = 0, warp0 = 0;
+    std::vector<uint32_t> col_ptr, row_idx, diag;
+    std::vector<uint8_t> cur_row;
+    KindHost kinds[7];
+    std::vector<uint32_t> q;
+    Tape tape;
+    GroupDev dev{};
+    std::vector<void*> owned;       // buffers freed at destroy
+    std::vector<void*> lu_owned;    // LU buffers, reallocated at each retape
+    double* mos_raw = nullptr;
+    double* dio_raw = nullptr;
+    uint32_t meas_row = 0xFFFFFFFFu;
+    double meas_level = 0, meas_t0 = 0;
+};
+
+}  // namespace
+
+struct espl_lanes {
+    int device = 0;
+    uint32_t precision = ESPL_FP64;
+    std::vector<Group> groups;
+    uint32_t n_warps = 0, total_lanes = 0;
+    GroupDev* d_groups = nullptr;
+    uint32_t* d_warp_group = nullptr;
+    LaneState* d_state = nullptr;
+    const double** d_mos_raw = nullptr;
+    const double** d_dio_raw = nullptr;
+    PeelPool pool{};
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    espl_stats stats{};
+    std::string err;
+    TranParams tran{};
+    bool tran_ready = false;
+    std::vector<LaneState> h_state;
+};
+
+namespace {
+
+espl_status fail(espl_lanes* h, espl_status code, const std::string& msg) {
+    if (h) h->err = msg;
+    return code;
+}
+
+#define CK(call)                                                                                  \
+    do {                                                                                          \
+        cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess) {                                                                  \
+            if (h) h->err = std::string(#call) + ": " + cudaGetErrorString(e_);                   \
+            return e_ == cudaErrorMemoryAllocation ? (espl_status)ESPL_OUT_OF_MEMORY              \
+                                                   : (espl_status)ESPL_DRIVER;                    \
+        }                                                                                         \
+    } while (0)
+
+template <typename T>
+espl_status dalloc(espl_lanes* h, std::vector<void*>& own, T** out, size_t count) {
+    void* p = nullptr;
+    CK(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)));
+    CK(cudaMemsetAsync(p, 0, std::max<size_t>(count, 1) * sizeof(T), h->stream));
+    own.push_back(p);
+    *out = static_cast<T*>(p);
+    return ESPL_OK;
+}
+
+template <typename T>
+espl_status dupload(espl_lanes* h, std::vector<void*>& own, const T** out, const std::vector<T>& v) {
+    T* p = nullptr;
+    espl_status s = dalloc(h, own, &p, v.size());
+    if (s) return s;
+    if (!v.empty()) CK(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, h->stream));
+    *out = p;
+    return ESPL_OK;
+}
+
+uint32_t find_slot(const Group& g, uint32_t r, uint32_t c) {
+    if (r == kGround || c == kGround) return g.nnz;
+    for (uint32_t p = g.col_ptr[c]; p < g.col_ptr[c + 1]; p++)
+        if (g.row_idx[p] == r) return p;
+    return kNone;
+}
+
+// Validates one template and lays out its host tables.
+espl_status build_group(espl_lanes* h, const espl_netlist& net, Group& g) {
+    if (net.n == 0 || net.lanes == 0 || !net.col_ptr || !net.row_idx)
+        return fail(h, ESPL_INVALID_ARGUMENT, "empty template");
+    g.n = net.n;
+    g.nnz = net.nnz;
+    g.lanes = net.lanes;
+    g.P = (net.lanes + 31) / 32 * 32;
+    g.col_ptr.assign(net.col_ptr, net.col_ptr + net.n + 1);
+    if (g.col_ptr[0] != 0 || g.col_ptr[net.n] != net.nnz) return fail(h, ESPL_INVALID_ARGUMENT, "bad col_ptr");
+    for (uint32_t c = 0; c < net.n; c++)
+        if (g.col_ptr[c + 1] < g.col_ptr[c]) return fail(h, ESPL_INVALID_ARGUMENT, "col_ptr not monotone");
+    g.row_idx.assign(net.row_idx, net.row_idx + net.nnz);
+    for (uint32_t r : g.row_idx)
+        if (r >= net.n) return fail(h, ESPL_INVALID_ARGUMENT, "row index out of range");
+    g.diag.assign(net.n, 0);
+    for (uint32_t i = 0; i < net.n; i++) {
+        g.diag[i] = find_slot(g, i, i);
+        if (g.diag[i] == kNone) return fail(h, ESPL_INVALID_ARGUMENT, "pattern lacks a diagonal");
+    }
+    g.cur_row.assign(net.n, 0);
+    for (uint32_t b = 0; b < net.n_batches; b++) {
+        const espl_batch& sb = net.batches[b];
+        uint32_t nt = terms_of(sb.kind), np = params_of(sb.kind);
+        if (nt == 0) return fail(h, ESPL_INVALID_ARGUMENT, "unknown device kind");
+        if (sb.count == 0) continue;
+        if (!sb.term || !sb.param) return fail(h, ESPL_INVALID_ARGUMENT, "null device arrays");
+        KindHost& kh = g.kinds[sb.kind];
+        uint32_t base = kh.count;
+        kh.count += sb.count;
+        for (uint32_t i = 0; i < sb.count; i++) {
+            const uint32_t* tm = sb.term + (size_t)i * nt;
+            for (uint32_t t = 0; t < nt; t++) {
+                if (tm[t] != kGround && tm[t] >= net.n) return fail(h, ESPL_INVALID_ARGUMENT, "terminal out of range");
+                kh.term.push_back(tm[t] == kGround ? net.n : tm[t]);
+            }
+            for (uint32_t r = 0; r < nt; r++)
+                for (uint32_t c = 0; c < nt; c++) {
+                    uint32_t s = find_slot(g, tm[r], tm[c]);
+                    if (s == kNone) {
+                        if (stamps(sb.kind, r, c)) return fail(h, ESPL_INVALID_ARGUMENT, "pattern lacks a device stamp");
+                        s = net.nnz;
+                    }
+                    kh.slot.push_back(s);
+                }
+            if (sb.kind == ESPL_VSRC) {
+                if (tm[2] == kGround) return fail(h, ESPL_INVALID_ARGUMENT, "branch unknown on ground");
+                g.cur_row[tm[2]] = 1;
+            }
+        }
+        kh.param.resize((size_t)kh.count * np * g.P);
+        for (uint32_t i = 0; i < sb.count; i++)
+            for (uint32_t k = 0; k < np; k++) {
+                const double* src = sb.param + ((size_t)i * np + k) * net.lanes;
+                double* dst = kh.param.data() + ((size_t)(base + i) * np + k) * g.P;
+                std::memcpy(dst, src, sizeof(double) * net.lanes);
+                for (uint32_t l = net.lanes; l < g.P; l++) dst[l] = src[0];
+            }
+    }
+    if (!order_columns(g.n, g.col_ptr.data(), g.row_idx.data(), g.q))
+        return fail(h, ESPL_NO_TAPE, "column ordering ran out of workspace");
+    return ESPL_OK;
+}
+
+// Allocates the lane-major state of a group; the LU buffers come later.
+espl_status alloc_group(espl_lanes* h, Group& g) {
+    GroupDev& d = g.dev;
+    size_t P = g.P;
+    size_t n1 = g.n + 1, z1 = g.nnz + 1;
+    d.n = g.n;
+    d.nnz = g.nnz;
+    d.lanes = g.lanes;
+    d.P = g.P;
+    d.lane0 = g.lane0;
+    d.warp0 = g.warp0;
+    d.n_res = g.kinds[ESPL_RES].count;
+    d.n_cap = g.kinds[ESPL_CAP].count;
+    d.n_vsrc = g.kinds[ESPL_VSRC].count;
+    d.n_isrc = g.kinds[ESPL_ISRC].count;
+    d.n_dio = g.kinds[ESPL_DIODE].count;
+    d.n_mos = g.kinds[ESPL_MOS1].count;
+    d.n_sites = d.n_cap + d.n_dio;
+    d.has_charge = d.n_cap > 0;
+    for (uint32_t i = 0; i < d.n_dio; i++) {
+        double cjo = g.kinds[ESPL_DIODE].param[((size_t)i * 7 + 2) * P];
+        double tt = g.kinds[ESPL_DIODE].param[((size_t)i * 7 + 6) * P];
+        if (cjo > 0 || tt > 0) d.has_charge = 1;
+    }
+    d.meas_row = 0xFFFFFFFFu;
+    auto& own = g.owned;
+    espl_status s;
+#define UP(field, vec) if ((s = dupload(h, own, &d.field, vec))) return s
+    UP(col_ptr, g.col_ptr);
+    UP(row_idx, g.row_idx);
+    UP(diag, g.diag);
+    UP(cur_row, g.cur_row);
+    UP(res_t, g.kinds[ESPL_RES].term);
+    UP(res_s, g.kinds[ESPL_RES].slot);
+    UP(cap_t, g.kinds[ESPL_CAP].term);
+    UP(cap_s, g.kinds[ESPL_CAP].slot);
+    UP(vsrc_t, g.kinds[ESPL_VSRC].term);
+    UP(vsrc_s, g.kinds[ESPL_VSRC].slot);
+    UP(isrc_t, g.kinds[ESPL_ISRC].term);
+    UP(dio_t, g.kinds[ESPL_DIODE].term);
+    UP(dio_s, g.kinds[ESPL_DIODE].slot);
+    UP(mos_t, g.kinds[ESPL_MOS1].term);
+    UP(mos_s, g.kinds[ESPL_MOS1].slot);
+    UP(res_r, g.kinds[ESPL_RES].param);
+    UP(cap_c, g.kinds[ESPL_CAP].param);
+    UP(vsrc_p, g.kinds[ESPL_VSRC].param);
+    UP(isrc_p, g.kinds[ESPL_ISRC].param);
+#undef UP
+    const double* raw = nullptr;
+    if ((s = dupload(h, own, &raw, g.kinds[ESPL_MOS1].param))) return s;
+    g.mos_raw = const_cast<double*>(raw);
+    if ((s = dupload(h, own, &raw, g.kinds[ESPL_DIODE].param))) return s;
+    g.dio_raw = const_cast<double*>(raw);
+    double* p = nullptr;
+    if ((s = dalloc(h, own, &p, (size_t)d.n_mos * Mos1Prep::count * P))) return s;
+    d.mos_d = p;
+    if ((s = dalloc(h, own, &p, (size_t)d.n_dio * DiodePrep::count * P))) return s;
+    d.dio_d = p;
+#define AL(field, count) if ((s = dalloc(h, own, &d.field, (count)))) return s
+    AL(x, n1 * P);
+    AL(x_old, n1 * P);
+    AL(dx, n1 * P);
+    AL(rhs, n1 * P);
+    AL(qrow, n1 * P);
+    AL(g, z1 * P);
+    AL(c, z1 * P);
+    AL(a, z1 * P);
+    AL(w, n1 * P);
+    AL(y, n1 * P);
+    AL(w32, n1 * P);
+    AL(y32, n1 * P);
+    AL(lim_mos, 3 * (size_t)d.n_mos * P);
+    AL(lim_dio, (size_t)d.n_dio * P);
+    AL(qs, (size_t)d.n_sites * P);
+    AL(q1, n1 * P);
+    AL(ip, n1 * P);
+    AL(cur, n1 * P);
+    AL(prev, n1 * P);
+    AL(sring, 4 * (size_t)d.n_sites * P);
+    AL(sip, (size_t)d.n_sites * P);
+    AL(rr, n1 * P);
+    AL(corr, n1 * P);
+    AL(udiag, n1 * P);
+    AL(udiag32, n1 * P);
+#undef AL
+    return ESPL_OK;
+}
+
+LaunchMap launch_map(espl_lanes* h) { return LaunchMap{h->d_groups, h->d_warp_group, h->n_warps}; }
+uint32_t grid_of(espl_lanes* h) { return (h->n_warps * 32 + kBlock - 1) / kBlock; }
+
+espl_status push_descs(espl_lanes* h) {
+    std::vector<GroupDev> descs;
+    for (auto& g : h->groups) descs.push_back(g.dev);
+    CK(cudaMemcpyAsync(h->d_groups, descs.data(), descs.size() * sizeof(GroupDev), cudaMemcpyHostToDevice, h->stream));
+    return ESPL_OK;
+}
+
+// ownTape (lanes.zig:590-603): every lane is stamped at its x, the lead
+// lane's A = G (+ C / dt) is read back and factored on the host, and the
+// frozen tape goes to the device.
+espl_status retape(espl_lanes* h, int tran, double dt) {
+    auto launch = [&]() {
+        k_assemble<<<grid_of(h), kBlock, 0, h->stream>>>(launch_map(h), tran, 0.0, dt > 0 ? 1.0 / dt : 0.0);
+    };
+    launch();
+    CK(cudaGetLastError());
+    for (auto& g : h->groups) {
+        std::vector<double> a0(g.nnz);
+        if (g.nnz)
+            CK(cudaMemcpy2DAsync(a0.data(), sizeof(double), g.dev.a, sizeof(double) * g.P, sizeof(double), g.nnz,
+                                 cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        if (!factor_tape(g.n, g.col_ptr.data(), g.row_idx.data(), a0.data(), g.q, g.tape))
+            return fail(h, ESPL_NO_TAPE, "the lead lane's factor is singular");
+        for (void* p : g.lu_owned) cudaFree(p);
+        g.lu_owned.clear();
+        GroupDev& d = g.dev;
+        d.nnz_l = (uint32_t)g.tape.li.size();
+        d.nnz_u = (uint32_t)g.tape.ui.size();
+        d.n_void = (uint32_t)g.tape.void_slots.size();
+        espl_status s;
+        auto& own = g.lu_owned;
+#define UP(field, vec) if ((s = dupload(h, own, &d.field, vec))) return s
+        UP(prow, g.tape.prow);
+        UP(q, g.tape.q);
+        UP(pinv, g.tape.pinv);
+        UP(lp, g.tape.lp);
+        UP(li, g.tape.li);
+        UP(up, g.tape.up);
+        UP(ui, g.tape.ui);
+        UP(flags, g.tape.flags);
+        UP(void_slots, g.tape.void_slots);
+#undef UP
+        size_t P = g.P;
+        if ((s = dalloc(h, own, &d.lx, (size_t)d.nnz_l * P))) return s;
+        if ((s = dalloc(h, own, &d.ux, (size_t)d.nnz_u * P))) return s;
+        if (h->precision == ESPL_MIXED) {
+            if ((s = dalloc(h, own, &d.lx32, (size_t)d.nnz_l * P))) return s;
+            if ((s = dalloc(h, own, &d.ux32, (size_t)d.nnz_u * P))) return s;
+        }
+    }
+    return push_descs(h);
+}
+
+NewtonParams newton_params(const espl_newton_opts& o, uint32_t precision) {
+    NewtonParams p{};
+    p.reltol = o.reltol;
+    p.abstol = o.abstol;
+    p.vntol = o.vntol;
+    p.gmin = o.gmin;
+    p.residual_tol = o.residual_tol;
+    p.max_iter = o.max_iter;
+    p.init_fix = o.init_fix;
+    p.mixed = precision == ESPL_MIXED;
+    p.stall_ticks = 12;
+    p.refine = 1;
+    return p;
+}
+
+espl_status run_static(espl_lanes* h, const NewtonParams& np, int tran) {
+    if (h->pool.next) CK(cudaMemsetAsync(h->pool.next, 0, 2 * sizeof(uint32_t), h->stream));
+    CK(cudaEventRecord(h->ev0, h->stream));
+    if (np.mixed) k_static<true><<<grid_of(h), kBlock, 0, h->stream>>>(launch_map(h), np, h->d_state, tran, h->pool);
+    else k_static<false><<<grid_of(h), kBlock, 0, h->stream>>>(launch_map(h), np, h->d_state, tran, h->pool);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(h->ev1, h->stream));
+    CK(cudaEventSynchronize(h->ev1));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    h->stats.newton_ms = ms;
+    h->stats.total_ms += ms;
+    h->stats.launches += 1;
+    return ESPL_OK;
+}
+
+espl_status seed(espl_lanes* h, int cold) {
+    k_seed<<<grid_of(h), kBlock, 0, h->stream>>>(launch_map(h), cold, h->d_state);
+    CK(cudaGetLastError());
+    return ESPL_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+uint32_t espl_abi_version(void) { return ESPL_ABI_VERSION; }
+
+espl_status espl_create(const espl_netlist* nets, uint32_t n_nets, const espl_create_opts* opts, double dt0,
+                        espl_lanes** out) {
+    if (!out) return ESPL_INVALID_ARGUMENT;
+    *out = nullptr;
+    if (!nets || n_nets == 0) return ESPL_INVALID_ARGUMENT;
+    if (opts && opts->abi_version != ESPL_ABI_VERSION) return ESPL_INVALID_ARGUMENT;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return ESPL_NO_IMAGE;
+    espl_lanes* h = new espl_lanes();
+    h->device = opts ? (int)opts->device : 0;
+    h->precision = opts ? opts->precision : ESPL_FP64;
+    auto bail = [&](espl_status s) {
+        std::string e = h->err;
+        espl_destroy(h);
+        (void)e;
+        return s;
+    };
+    if (h->device >= ndev) return bail(ESPL_INVALID_ARGUMENT);
+    if (cudaSetDevice(h->device) != cudaSuccess) return bail(ESPL_DRIVER);
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, k_static<false>) != cudaSuccess) return bail(ESPL_NO_IMAGE);
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(ESPL_DRIVER);
+    cudaEventCreate(&h->ev0);
+    cudaEventCreate(&h->ev1);
+    h->groups.resize(n_nets);
+    uint32_t lane0 = 0, warp0 = 0;
+    for (uint32_t i = 0; i < n_nets; i++) {
+        Group& g = h->groups[i];
+        espl_status s = build_group(h, nets[i], g);
+        if (s) return bail(s);
+        g.lane0 = lane0;
+        g.warp0 = warp0;
+        lane0 += g.P;
+        warp0 += g.P / 32;
+    }
+    h->total_lanes = lane0;
+    h->n_warps = warp0;
+    for (auto& g : h->groups) {
+        espl_status s = alloc_group(h, g);
+        if (s) return bail(s);
+    }
+    std::vector<uint32_t> wg(h->n_warps);
+    std::vector<const double*> mr, dr;
+    for (uint32_t i = 0; i < n_nets; i++) {
+        for (uint32_t w = 0; w < h->groups[i].P / 32; w++) wg[h->groups[i].warp0 + w] = i;
+        mr.push_back(h->groups[i].mos_raw);
+        dr.push_back(h->groups[i].dio_raw);
+    }
+    std::vector<void*> own;
+    if (cudaMalloc(&h->d_groups, sizeof(GroupDev) * n_nets) != cudaSuccess) return bail(ESPL_OUT_OF_MEMORY);
+    if (cudaMalloc(&h->d_warp_group, sizeof(uint32_t) * wg.size()) != cudaSuccess) return bail(ESPL_OUT_OF_MEMORY);
+    if (cudaMalloc(&h->d_state, sizeof(LaneState) * h->total_lanes) != cudaSuccess) return bail(ESPL_OUT_OF_MEMORY);
+    if (cudaMalloc(&h->d_mos_raw, sizeof(double*) * n_nets) != cudaSuccess) return bail(ESPL_OUT_OF_MEMORY);
+    if (cudaMalloc(&h->d_dio_raw, sizeof(double*) * n_nets) != cudaSuccess) return bail(ESPL_OUT_OF_MEMORY);
+    cudaMemsetAsync(h->d_state, 0, sizeof(LaneState) * h->total_lanes, h->stream);
+    cudaMemcpyAsync(h->d_warp_group, wg.data(), sizeof(uint32_t) * wg.size(), cudaMemcpyHostToDevice, h->stream);
+    cudaMemcpyAsync(h->d_mos_raw, mr.data(), sizeof(double*) * n_nets, cudaMemcpyHostToDevice, h->stream);
+    cudaMemcpyAsync(h->d_dio_raw, dr.data(), sizeof(double*) * n_nets, cudaMemcpyHostToDevice, h->stream);
+    // Dense-peel pool for templates of n <= 64 (lanes.zig:908 sizes its
+    // pool by memory; here 256 slots of 64 x 64 + 64 doubles, 8.5 MB).
+    uint32_t nmax_small = 0;
+    for (auto& g : h->groups)
+        if (g.n <= kDensePeelMax) nmax_small = std::max(nmax_small, g.n);
+    if (nmax_small) {
+        h->pool.n_slots = 256;
+        h->pool.slot_words = nmax_small * nmax_small + nmax_small;
+        if (cudaMalloc(&h->pool.scratch, sizeof(double) * h->pool.n_slots * h->pool.slot_words) != cudaSuccess)
+            return bail(ESPL_OUT_OF_MEMORY);
+        uint32_t* ctr = nullptr;
+        if (cudaMalloc(&ctr, 2 * sizeof(uint32_t)) != cudaSuccess) return bail(ESPL_OUT_OF_MEMORY);
+        h->pool.next = ctr;
+        h->pool.over = ctr + 1;
+        cudaMemsetAsync(ctr, 0, 2 * sizeof(uint32_t), h->stream);
+    }
+    if (push_descs(h)) return bail(ESPL_DRIVER);
+    k_prep<<<grid_of(h), kBlock, 0, h->stream>>>(launch_map(h), h->d_mos_raw, h->d_dio_raw);
+    if (cudaGetLastError() != cudaSuccess) return bail(ESPL_DRIVER);
+    if (seed(h, 1)) return bail(ESPL_DRIVER);
+    espl_status s = retape(h, dt0 > 0 ? 1 : 0, dt0);
+    if (s) return bail(s);
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) return bail(ESPL_DRIVER);
+    h->h_state.resize(h->total_lanes);
+    *out = h;
+    return ESPL_OK;
+}
+
+espl_status espl_destroy(espl_lanes* h) {
+    if (!h) return ESPL_OK;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (auto& g : h->groups) {
+        for (void* p : g.owned) cudaFree(p);
+        for (void* p : g.lu_owned) cudaFree(p);
+    }
+    cudaFree(h->d_groups);
+    cudaFree(h->d_warp_group);
+    cudaFree(h->d_state);
+    cudaFree(h->d_mos_raw);
+    cudaFree(h->d_dio_raw);
+    cudaFree(h->pool.scratch);
+    cudaFree(h->pool.next);
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return ESPL_OK;
+}
+
+espl_status espl_tape_info(espl_lanes* h, uint32_t net, uint32_t* n, uint32_t* nnz_l, uint32_t* nnz_u) {
+    if (!h || net >= h->groups.size()) return ESPL_INVALID_ARGUMENT;
+    const Group& g = h->groups[net];
+    if (n) *n = g.n;
+    if (nnz_l) *nnz_l = (uint32_t)g.tape.li.size();
+    if (nnz_u) *nnz_u = (uint32_t)g.tape.ui.size();
+    return ESPL_OK;
+}
+
+espl_status espl_copy_tape(espl_lanes* h, uint32_t net, uint32_t* q, uint32_t* pinv, uint32_t* lp, uint32_t* li,
+                           uint32_t* up, uint32_t* ui, uint32_t* flags) {
+    if (!h || net >= h->groups.size()) return ESPL_INVALID_ARGUMENT;
+    const Tape& t = h->groups[net].tape;
+    auto cp = [](uint32_t* dst, const std::vector<uint32_t>& v) {
+        if (dst && !v.empty()) std::memcpy(dst, v.data(), v.size() * sizeof(uint32_t));
+    };
+    cp(q, t.q);
+    cp(pinv, t.pinv);
+    cp(lp, t.lp);
+    cp(li, t.li);
+    cp(up, t.up);
+    cp(ui, t.ui);
+    cp(flags, t.flags);
+    return ESPL_OK;
+}
+
+espl_status espl_put_x(espl_lanes* h, uint32_t net, const double* x, uint32_t cold) {
+    if (!h || net >= h->groups.size() || !x) return ESPL_INVALID_ARGUMENT;
+    Group& g = h->groups[net];
+    std::vector<double> lm((size_t)(g.n + 1) * g.P, 0.0);
+    for (uint32_t l = 0; l < g.P; l++) {
+        const double* src = x + (size_t)std::min(l, g.lanes - 1) * g.n;
+        for (uint32_t i = 0; i < g.n; i++) lm[(size_t)i * g.P + l] = src[i];
+    }
+    CK(cudaMemcpyAsync(g.dev.x, lm.data(), lm.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    if (seed(h, cold ? 1 : 0)) return ESPL_DRIVER;
+    CK(cudaStreamSynchronize(h->stream));
+    h->tran_ready = false;
+    return ESPL_OK;
+}
+
+espl_status espl_get_x(espl_lanes* h, uint32_t net, double* x) {
+    if (!h || net >= h->groups.size() || !x) return ESPL_INVALID_ARGUMENT;
+    Group& g = h->groups[net];
+    std::vector<double> lm((size_t)g.n * g.P);
+    CK(cudaMemcpyAsync(lm.data(), g.dev.x, lm.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    for (uint32_t l = 0; l < g.lanes; l++)
+        for (uint32_t i = 0; i < g.n; i++) x[(size_t)l * g.n + i] = lm[(size_t)i * g.P + l];
+    return ESPL_OK;
+}
+
+espl_status espl_solve_static(espl_lanes* h, const espl_newton_opts* opts, espl_lane_newton* out) {
+    if (!h || !opts) return ESPL_INVALID_ARGUMENT;
+    if (opts->max_iter == 0 || opts->max_iter > 100000) return fail(h, ESPL_INVALID_ARGUMENT, "max_iter out of range");
+    NewtonParams np = newton_params(*opts, h->precision);
+    espl_status s = run_static(h, np, 0);
+    if (s) return s;
+    if (out) {
+        CK(cudaMemcpyAsync(h->h_state.data(), h->d_state, sizeof(LaneState) * h->total_lanes, cudaMemcpyDeviceToHost,
+                           h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        size_t k = 0;
+        uint64_t iters = 0;
+        for (auto& g : h->groups)
+            for (uint32_t l = 0; l < g.lanes; l++) {
+                const LaneState& st = h->h_state[g.lane0 + l];
+                out[k].bits = st.bits & (kConverged | kSingular | kParked);
+                out[k].iterations = st.iterations;
+                out[k].refactor_fallbacks = st.fallbacks;
+                out[k].reserved = 0;
+                iters += st.iterations;
+                k++;
+            }
+        h->stats.lane_iterations = iters;
+    }
+    return ESPL_OK;
+}
+
+espl_status espl_init_steps(espl_lanes* h, const espl_tran_opts* o) {
+    if (!h || !o) return ESPL_INVALID_ARGUMENT;
+    if (!(o->t_stop > 0) || !(o->dt > 0) || o->max_iter == 0 || o->method > 1)
+        return fail(h, ESPL_INVALID_ARGUMENT, "bad transient options");
+    TranParams& t = h->tran;
+    t.t_stop = o->t_stop;
+    t.dt = o->dt;
+    t.dt_max = o->dt_max > 0 ? o->dt_max : o->t_stop / 50.0;
+    t.dt_min = o->dt_min > 0 ? o->dt_min : 1e-9 * t.dt_max;
+    t.reltol = o->reltol;
+    t.abstol = o->abstol;
+    t.chgtol = o->chgtol;
+    t.trtol = o->trtol;
+    t.vntol = o->vntol;
+    t.residual_tol = o->residual_tol;
+    t.delmin = 1e-11 * t.dt_max;
+    t.min_break = 5e-5 * t.dt_max;
+    t.method = o->method;
+    t.fixed_step = o->fixed_step;
+    t.max_iter = o->max_iter;
+    t.max_steps = o->max_steps ? o->max_steps : 0xFFFFFFFFu;
+    t.predictor = o->predictor;
+    // Operating point at t = 0 with the sources at their t = 0 value, from
+    // a cold start (tran.zig Run.init), on the static tape.
+    for (auto& g : h->groups) {
+        CK(cudaMemsetAsync(g.dev.x, 0, sizeof(double) * (g.n + 1) * g.P, h->stream));
+    }
+    if (seed(h, 1)) return ESPL_DRIVER;
+    espl_status s = retape(h, 1, 0.0);
+    if (s) return s;
+    if (seed(h, 1)) return ESPL_DRIVER;
+    espl_newton_opts op{o->reltol, o->abstol, o->vntol, 0.0, o->residual_tol, 100, 1};
+    NewtonParams np = newton_params(op, h->precision);
+    s = run_static(h, np, 1);
+    if (s) return s;
+    // The step tape: the lead lane's G + C / dt at the operating point.
+    if (seed(h, 0)) return ESPL_DRIVER;
+    double dt_first = o->fixed_step ? o->dt : std::min(std::min(o->dt, o->t_stop / 100.0) / 10.0, t.dt_max) / 10.0;
+    s = retape(h, 1, dt_first);
+    if (s) return s;
+    k_tran_init<<<grid_of(h), kBlock, 0, h->stream>>>(launch_map(h), t, h->d_state);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(h->stream));
+    h->tran_ready = true;
+    h->stats.lane_steps = 0;
+    return ESPL_OK;
+}
+
+espl_status espl_device_launch(espl_lanes* h, uint32_t max_steps, espl_step_report* reports) {
+    if (!h || !h->tran_ready) return ESPL_INVALID_ARGUMENT;
+    TranParams t = h->tran;
+    t.launch_steps = max_steps ? max_steps : 1;
+    espl_newton_opts op{t.reltol, t.abstol, t.vntol, 0.0, t.residual_tol, t.max_iter, 0};
+    NewtonParams np = newton_params(op, h->precision);
+    if (h->pool.next) CK(cudaMemsetAsync(h->pool.next, 0, 2 * sizeof(uint32_t), h->stream));
+    CK(cudaEventRecord(h->ev0, h->stream));
+    if (np.mixed) k_tran<true><<<grid_of(h), kBlock, 0, h->stream>>>(launch_map(h), t, np, h->d_state, h->pool);
+    else k_tran<false><<<grid_of(h), kBlock, 0, h->stream>>>(launch_map(h), t, np, h->d_state, h->pool);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(h->ev1, h->stream));
+    CK(cudaEventSynchronize(h->ev1));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    h->stats.newton_ms = ms;
+    h->stats.total_ms += ms;
+    h->stats.launches += 1;
+    CK(cudaMemcpyAsync(h->h_state.data(), h->d_state, sizeof(LaneState) * h->total_lanes, cudaMemcpyDeviceToHost,
+                       h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    size_t k = 0;
+    uint64_t steps = 0;
+    for (auto& g : h->groups)
+        for (uint32_t l = 0; l < g.lanes; l++) {
+            const LaneState& st = h->h_state[g.lane0 + l];
+            steps += st.steps;
+            if (reports) {
+                espl_step_report& r = reports[k];
+                r.t = st.t;
+                r.dt = st.dt;
+                r.attempts = st.attempts;
+                r.nr_iters = st.nr_iters;
+                r.steps = st.steps;
+                r.rejects = st.rejects;
+                r.status = st.status;
+                r.reserved = 0;
+            }
+            k++;
+        }
+    h->stats.lane_steps = steps;
+    return ESPL_OK;
+}
+
+espl_status espl_set_period_meas(espl_lanes* h, uint32_t net, uint32_t row, double level, double t_start) {
+    if (!h || net >= h->groups.size() || row >= h->groups[net].n) return ESPL_INVALID_ARGUMENT;
+    Group& g = h->groups[net];
+    g.dev.meas_row = row;
+    g.dev.meas_level = level;
+    g.dev.meas_t0 = t_start;
+    return push_descs(h);
+}
+
+espl_status espl_get_period_meas(espl_lanes* h, uint32_t net, double* period, uint32_t* crossings) {
+    if (!h || net >= h->groups.size()) return ESPL_INVALID_ARGUMENT;
+    Group& g = h->groups[net];
+    CK(cudaMemcpyAsync(h->h_state.data(), h->d_state, sizeof(LaneState) * h->total_lanes, cudaMemcpyDeviceToHost,
+                       h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    for (uint32_t l = 0; l < g.lanes; l++) {
+        const LaneState& st = h->h_state[g.lane0 + l];
+        if (period) period[l] = st.m_cross >= 2 ? (st.m_last - st.m_first) / (double)(st.m_cross - 1) : NAN;
+        if (crossings) crossings[l] = st.m_cross;
+    }
+    return ESPL_OK;
+}
+
+espl_status espl_get_stats(espl_lanes* h, espl_stats* out) {
+    if (!h || !out) return ESPL_INVALID_ARGUMENT;
+    *out = h->stats;
+    return ESPL_OK;
+}
+
+espl_status espl_error_message(espl_lanes* h, char* buf, size_t cap) {
+    if (!h || !buf || cap == 0) return ESPL_INVALID_ARGUMENT;
+    size_t n = std::min(cap - 1, h->err.size());
+    std::memcpy(buf, h->err.data(), n);
+    buf[n] = 0;
+    return ESPL_OK;
+}
+
+}  // extern "C"
+
+struct espl_tape {
+    Tape t;
+};
+
+extern "C" {
+
+espl_status espl_order(uint32_t n, const uint32_t* col_ptr, const uint32_t* row_idx, uint32_t* q) {
+    if (!col_ptr || (!row_idx && n && col_ptr[n]) || (!q && n)) return ESPL_INVALID_ARGUMENT;
+    std::vector<uint32_t> qq;
+    if (!order_columns(n, col_ptr, row_idx, qq)) return ESPL_NO_TAPE;
+    if (n) std::memcpy(q, qq.data(), sizeof(uint32_t) * n);
+    return ESPL_OK;
+}
+
+espl_status espl_tape_build(uint32_t n, const uint32_t* col_ptr, const uint32_t* row_idx, const double* vals,
+                            const uint32_t* q, espl_tape** out) {
+    if (!out || !col_ptr || !q || n == 0) return ESPL_INVALID_ARGUMENT;
+    *out = nullptr;
+    for (uint32_t i = 0; i < col_ptr[n]; i++)
+        if (row_idx[i] >= n) return ESPL_INVALID_ARGUMENT;
+    std::vector<uint32_t> qq(q, q + n);
+    espl_tape* t = new espl_tape();
+    if (!factor_tape(n, col_ptr, row_idx, vals, qq, t->t)) {
+        delete t;
+        return ESPL_NO_TAPE;
+    }
+    *out = t;
+    return ESPL_OK;
+}
+
+espl_status espl_tape_sizes(const espl_tape* t, uint32_t* nnz_l, uint32_t* nnz_u, uint32_t* n_void_slots) {
+    if (!t) return ESPL_INVALID_ARGUMENT;
+    if (nnz_l) *nnz_l = (uint32_t)t->t.li.size();
+    if (nnz_u) *nnz_u = (uint32_t)t->t.ui.size();
+    if (n_void_slots) *n_void_slots = (uint32_t)t->t.void_slots.size();
+    return ESPL_OK;
+}
+
+espl_status espl_tape_copy(const espl_tape* t, uint32_t* q, uint32_t* pinv, uint32_t* lp, uint32_t* li, uint32_t* up,
+                           uint32_t* ui, uint32_t* flags, uint32_t* prow, uint32_t* void_slots, double* lx,
+                           double* ux, double* udiag) {
+    if (!t) return ESPL_INVALID_ARGUMENT;
+    auto cp = [](auto* dst, const auto& v) {
+        if (dst && !v.empty()) std::memcpy(dst, v.data(), v.size() * sizeof(v[0]));
+    };
+    cp(q, t->t.q);
+    cp(pinv, t->t.pinv);
+    cp(lp, t->t.lp);
+    cp(li, t->t.li);
+    cp(up, t->t.up);
+    cp(ui, t->t.ui);
+    cp(flags, t->t.flags);
+    cp(prow, t->t.prow);
+    cp(void_slots, t->t.void_slots);
+    cp(lx, t->t.lx);
+    cp(ux, t->t.ux);
+    cp(udiag, t->t.udiag);
+    return ESPL_OK;
+}
+
+void espl_tape_free(espl_tape* t) { delete t; }
+
+}  // extern "C"

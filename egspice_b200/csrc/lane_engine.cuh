@@ -1,0 +1,536 @@
+// The per-lane engine of the lane sweep: stamping, tape refactor, triangular
+// solves, the Newton update and gates, and the transient step machine, each
+// run by the thread that owns the lane. Lanes of one template sit
+// interleaved (element i of lane l at i * P + l, P = lanes padded to a warp
+// multiple), so a warp's 32 lanes read every nonzero of the shared pattern as
+// one coalesced 256-byte load, while the tape's index words are warp-uniform.
+//
+// Semantics restated from ESPice:
+//   eval + ground pin        src/device/eval.zig:780-920, src/analysis/Circuit.zig:861-864
+//   refactor replay          src/solver/kernels/lane.zig:56-125 (Bodies.refactor)
+//   luSolve (negated)        src/solver/kernels/lane.zig:137-157
+//   updateNorm / plausible   src/solver/kernels/lane.zig:161-185
+//   residual gate            src/solver/kernels/lane.zig:189-198
+//   plausibleLimit           src/solver/kernels/lane.zig:202-214
+//   gates / finalize         src/solver/lane_device.zig:326-384
+//   companion rows / combine src/solver/kernels/lane.zig:221-242
+//   stepBound                src/solver/kernels/lane.zig:257-297
+//   step machine             src/solver/kernels/lane.zig:505-700
+//   dense peel               src/solver/kernels/lane.zig:310-350
+#pragma once
+
+#include <cstdint>
+
+#include "lane_models.cuh"
+
+namespace espl {
+
+constexpr uint32_t kTrashNone = 0xFFFFFFFFu;
+constexpr double kXPlausible = 1e9;    // converger.x_plausible
+constexpr double kWide = 1.0 / 1e-3;   // LaneTab.wide = 1 / pivot_tol
+constexpr uint32_t kDensePeelMax = 64; // kernels/lane.zig:301
+
+// Gate bits (kernels/lane.zig:708-711).
+constexpr uint32_t kActive = 1, kInitFix = 2, kConverged = 4, kSingular = 8, kPassed = 16, kParked = 32;
+
+struct GroupDev {
+    uint32_t n, nnz, nnz_l, nnz_u, lanes, P, warp0, lane0;
+    uint32_t n_void, n_res, n_cap, n_vsrc, n_isrc, n_dio, n_mos, n_sites;
+    uint32_t has_charge, meas_row;
+    double meas_level, meas_t0;
+    const uint32_t *col_ptr, *row_idx, *prow, *q, *pinv, *lp, *li, *up, *ui, *flags, *void_slots, *diag;
+    const uint8_t* cur_row;
+    const uint32_t *res_t, *res_s, *cap_t, *cap_s, *vsrc_t, *vsrc_s, *isrc_t, *dio_t, *dio_s, *mos_t, *mos_s;
+    const double *res_r, *cap_c, *vsrc_p, *isrc_p, *dio_d, *mos_d;
+    double *x, *x_old, *dx, *rhs, *qrow, *g, *c, *a, *lx, *ux, *udiag, *w, *y, *lim_mos, *lim_dio, *qs;
+    float *lx32, *ux32, *udiag32, *w32, *y32;
+    double *q1, *ip, *cur, *prev, *sring, *sip;
+    double *rr, *corr;
+};
+
+struct LaneState {
+    double limit;
+    double t, dt, dt_old0, dt_old1, bp_next, bp_save_dt;
+    double m_prev_v, m_prev_t, m_first, m_last;
+    unsigned long long attempts, nr_iters;
+    uint32_t bits, tick, iterations, fallbacks;
+    uint32_t order, steps, status, rejects;
+    uint32_t bp_clamped, m_cross, m_have, peel_slot;
+    uint32_t s_rot, fp64, pad0, pad1;
+};
+
+struct NewtonParams {
+    double reltol, abstol, vntol, gmin, residual_tol;
+    uint32_t max_iter, init_fix;
+    uint32_t mixed, stall_ticks;   // mixed: FP32 LU; a lane past stall_ticks refactors in FP64
+    uint32_t refine;               // mixed: FP64-residual refinement sweeps per solve
+    uint32_t pad;
+};
+
+struct TranParams {
+    double t_stop, dt, dt_min, dt_max, reltol, abstol, chgtol, trtol, vntol, residual_tol;
+    double delmin, min_break;
+    uint32_t method, fixed_step, max_iter, max_steps, predictor, launch_steps;
+};
+
+struct PeelPool {
+    double* scratch;       // n_slots * slot_words doubles
+    uint32_t* next;        // slot counter (zeroed per solve by the host)
+    uint32_t* over;        // lanes turned away by a full pool
+    uint32_t n_slots, slot_words;
+};
+
+struct Companion {
+    int on;
+    uint32_t method;  // 0 BE, 1 trap
+    double ag0, ag1;
+};
+
+#define LM(arr, i) (arr)[(size_t)(i) * P + l]
+
+__device__ __forceinline__ uint64_t dbits(double v) { return (uint64_t)__double_as_longlong(v); }
+__device__ __forceinline__ double bitsd(uint64_t b) { return __longlong_as_double((long long)b); }
+__device__ __forceinline__ uint32_t fbits(float v) { return (uint32_t)__float_as_int(v); }
+
+// ---------------------------------------------------------------------------
+// Stamping
+
+// G, C, the residual F (rhs) and the row charges at the lane's x, each device
+// at its limited branch voltages with the first-order correction to x
+// (eval.zig:826-874), then the ground pin. Terminal rows point at the trash
+// row n for ground, slots at the trash slot nnz.
+__device__ void eval_lane(const GroupDev& d, uint32_t l, int tran, double t) {
+    const uint32_t P = d.P;
+    const uint32_t n = d.n, nnz = d.nnz;
+    double* __restrict__ g = d.g;
+    double* __restrict__ rhs = d.rhs;
+    const double* __restrict__ x = d.x;
+    for (uint32_t p = 0; p <= nnz; p++) LM(g, p) = 0.0;
+    for (uint32_t i = 0; i <= n; i++) LM(rhs, i) = 0.0;
+    if (d.has_charge) {
+        for (uint32_t p = 0; p <= nnz; p++) LM(d.c, p) = 0.0;
+        for (uint32_t i = 0; i <= n; i++) LM(d.qrow, i) = 0.0;
+    }
+    // Resistors: I(p,n) = V(p,n) / r.
+    for (uint32_t i = 0; i < d.n_res; i++) {
+        uint32_t tp = d.res_t[2 * i], tn = d.res_t[2 * i + 1];
+        const uint32_t* s = d.res_s + 4 * i;
+        double v = LM(x, tp) - LM(x, tn);
+        double r = LM(d.res_r, i);
+        double cur = v / r, gg = 1.0 / r;
+        LM(rhs, tp) += cur;
+        LM(g, s[0]) += gg;
+        LM(g, s[1]) += -gg;
+        LM(rhs, tn) += -cur;
+        LM(g, s[2]) += -gg;
+        LM(g, s[3]) += gg;
+    }
+    // Capacitors: q = c V(p,n).
+    for (uint32_t i = 0; i < d.n_cap; i++) {
+        uint32_t tp = d.cap_t[2 * i], tn = d.cap_t[2 * i + 1];
+        const uint32_t* s = d.cap_s + 4 * i;
+        double v = LM(x, tp) - LM(x, tn);
+        double cc = LM(d.cap_c, i);
+        double qq = cc * v;
+        LM(d.qrow, tp) += qq;
+        LM(d.c, s[0]) += cc;
+        LM(d.c, s[1]) += -cc;
+        LM(d.qrow, tn) += -qq;
+        LM(d.c, s[2]) += -cc;
+        LM(d.c, s[3]) += cc;
+        LM(d.qs, i) = qq;
+    }
+    // Voltage sources: branch current ib; row br: V(p,n) - out.
+    for (uint32_t i = 0; i < d.n_vsrc; i++) {
+        uint32_t tp = d.vsrc_t[3 * i], tn = d.vsrc_t[3 * i + 1], tb = d.vsrc_t[3 * i + 2];
+        const uint32_t* s = d.vsrc_s + 9 * i;
+        const double* pp = d.vsrc_p;
+        uint32_t b9 = 9 * i;
+        double val = source_value(LM(pp, b9 + 0), LM(pp, b9 + 1), LM(pp, b9 + 2), LM(pp, b9 + 3), LM(pp, b9 + 4),
+                                  LM(pp, b9 + 5), LM(pp, b9 + 6), LM(pp, b9 + 7), LM(pp, b9 + 8), tran, t);
+        double ib = LM(x, tb);
+        LM(rhs, tp) += ib;
+        LM(g, s[2]) += 1.0;
+        LM(rhs, tn) += -ib;
+        LM(g, s[5]) += -1.0;
+        LM(rhs, tb) += (LM(x, tp) - LM(x, tn)) - val;
+        LM(g, s[6]) += 1.0;
+        LM(g, s[7]) += -1.0;
+    }
+    // Current sources: I(p,n) = out.
+    for (uint32_t i = 0; i < d.n_isrc; i++) {
+        uint32_t tp = d.isrc_t[2 * i], tn = d.isrc_t[2 * i + 1];
+        const double* pp = d.isrc_p;
+        uint32_t b9 = 9 * i;
+        double val = source_value(LM(pp, b9 + 0), LM(pp, b9 + 1), LM(pp, b9 + 2), LM(pp, b9 + 3), LM(pp, b9 + 4),
+                                  LM(pp, b9 + 5), LM(pp, b9 + 6), LM(pp, b9 + 7), LM(pp, b9 + 8), tran, t);
+        LM(rhs, tp) += val;
+        LM(rhs, tn) += -val;
+    }
+    // Diodes at the limited vd, corrected to x.
+    for (uint32_t i = 0; i < d.n_dio; i++) {
+        uint32_t ta = d.dio_t[2 * i], tc = d.dio_t[2 * i + 1];
+        const uint32_t* s = d.dio_s + 4 * i;
+        const double* dd = d.dio_d;
+        uint32_t b = DiodePrep::count * i;
+        double vd = LM(x, ta) - LM(x, tc);
+        double vl = LM(d.lim_dio, i);
+        double id, gd, qd, cd;
+        diode_core(LM(dd, b + DiodePrep::is), LM(dd, b + DiodePrep::vte), LM(dd, b + DiodePrep::gmin),
+                   LM(dd, b + DiodePrep::cjo), LM(dd, b + DiodePrep::cjo_t), LM(dd, b + DiodePrep::vj_t),
+                   LM(dd, b + DiodePrep::mt), LM(dd, b + DiodePrep::fc), LM(dd, b + DiodePrep::tt), vl, id, gd, qd, cd);
+        double f = id + gd * (vd - vl);
+        LM(rhs, ta) += f;
+        LM(g, s[0]) += gd;
+        LM(g, s[1]) += -gd;
+        LM(rhs, tc) += -f;
+        LM(g, s[2]) += -gd;
+        LM(g, s[3]) += gd;
+        if (LM(dd, b + DiodePrep::cjo) > 0.0 || LM(dd, b + DiodePrep::tt) > 0.0) {
+            double qq = qd + cd * (vd - vl);
+            LM(d.qrow, ta) += qq;
+            LM(d.c, s[0]) += cd;
+            LM(d.c, s[1]) += -cd;
+            LM(d.qrow, tc) += -qq;
+            LM(d.c, s[2]) += -cd;
+            LM(d.c, s[3]) += cd;
+            LM(d.qs, d.n_cap + i) = qq;
+        }
+    }
+    // MOS1 at the limited (vgs, vds, vbs), corrected to x.
+    for (uint32_t i = 0; i < d.n_mos; i++) {
+        const uint32_t* tm = d.mos_t + 4 * i;
+        const uint32_t* s = d.mos_s + 16 * i;
+        const double* md = d.mos_d;
+        uint32_t b = Mos1Prep::count * i;
+        double ty = LM(md, b + Mos1Prep::type);
+        double xd = LM(x, tm[0]), xg = LM(x, tm[1]), xs = LM(x, tm[2]), xb = LM(x, tm[3]);
+        double vgs = ty * (xg - xs), vds = ty * (xd - xs), vbs = ty * (xb - xs);
+        double lgs = LM(d.lim_mos, 3 * i), lds = LM(d.lim_mos, 3 * i + 1), lbs = LM(d.lim_mos, 3 * i + 2);
+        Mos1Out o;
+        mos1_core(ty, LM(md, b + Mos1Prep::vt), LM(md, b + Mos1Prep::beta), LM(md, b + Mos1Prep::lambda),
+                  LM(md, b + Mos1Prep::gamma), LM(md, b + Mos1Prep::phit), LM(md, b + Mos1Prep::von0),
+                  LM(md, b + Mos1Prep::isat), LM(md, b + Mos1Prep::gmin), lgs, lds, lbs, o);
+        double dgs = vgs - lgs, dds = vds - lds, dbs = vbs - lbs;
+        double gm = o.mode * o.gm, gds = o.mode * o.gds, gmbs = o.mode * o.gmbs;
+        double ich = o.mode * o.id + gm * dgs + gds * dds + gmbs * dbs;
+        double ibd = o.ibd + o.gbd * (dbs - dds);
+        double ibs = o.ibs + o.gbs * dbs;
+        double gsum = gm + gds + gmbs;
+        LM(rhs, tm[0]) += ty * ich - ty * ibd;
+        LM(g, s[0]) += gds + o.gbd;
+        LM(g, s[1]) += gm;
+        LM(g, s[2]) += -gsum;
+        LM(g, s[3]) += gmbs - o.gbd;
+        LM(rhs, tm[2]) += -ty * ich - ty * ibs;
+        LM(g, s[8]) += -gds;
+        LM(g, s[9]) += -gm;
+        LM(g, s[10]) += gsum + o.gbs;
+        LM(g, s[11]) += -gmbs - o.gbs;
+        LM(rhs, tm[3]) += ty * ibd + ty * ibs;
+        LM(g, s[12]) += -o.gbd;
+        LM(g, s[13]) += 0.0;
+        LM(g, s[14]) += -o.gbs;
+        LM(g, s[15]) += o.gbd + o.gbs;
+    }
+    LM(g, d.diag[0]) += 1.0;
+    LM(rhs, 0) += LM(x, 0);
+}
+
+// Limiter states at the junction seeds (op.zig coldStart: MOS1 vgs = type
+// vbit + gamma sqrt(phit), vds = 0, vbs = -1; the diode, which has no seed,
+// from x), or at x's image for a warm start.
+__device__ void seed_limits(const GroupDev& d, uint32_t l, int cold, const double* x) {
+    const uint32_t P = d.P;
+    for (uint32_t i = 0; i < d.n_mos; i++) {
+        const uint32_t* tm = d.mos_t + 4 * i;
+        uint32_t b = Mos1Prep::count * i;
+        const double* md = d.mos_d;
+        if (cold) {
+            LM(d.lim_mos, 3 * i) = LM(md, b + Mos1Prep::vgs_seed);
+            LM(d.lim_mos, 3 * i + 1) = 0.0;
+            LM(d.lim_mos, 3 * i + 2) = -1.0;
+        } else {
+            double ty = LM(md, b + Mos1Prep::type);
+            double xs = LM(x, tm[2]);
+            LM(d.lim_mos, 3 * i) = ty * (LM(x, tm[1]) - xs);
+            LM(d.lim_mos, 3 * i + 1) = ty * (LM(x, tm[0]) - xs);
+            LM(d.lim_mos, 3 * i + 2) = ty * (LM(x, tm[3]) - xs);
+        }
+    }
+    for (uint32_t i = 0; i < d.n_dio; i++) LM(d.lim_dio, i) = LM(x, d.dio_t[2 * i]) - LM(x, d.dio_t[2 * i + 1]);
+}
+
+// The limiter pass with snapLimited (eval.zig:1115-1171): true when any
+// device clamped its branch voltages.
+__device__ bool limit_lane(const GroupDev& d, uint32_t l) {
+    const uint32_t P = d.P;
+    const double* x = d.x;
+    bool flag = false;
+    const double eps16 = 16 * 2.220446049250313e-16;
+    for (uint32_t i = 0; i < d.n_mos; i++) {
+        const uint32_t* tm = d.mos_t + 4 * i;
+        uint32_t b = Mos1Prep::count * i;
+        const double* md = d.mos_d;
+        double ty = LM(md, b + Mos1Prep::type);
+        double xd = LM(x, tm[0]), xg = LM(x, tm[1]), xs = LM(x, tm[2]), xb = LM(x, tm[3]);
+        double cgs = ty * (xg - xs), cds = ty * (xd - xs), cbs = ty * (xb - xs);
+        double vgs = cgs, vds = cds, vbs = cbs;
+        mos1_limit(LM(md, b + Mos1Prep::vt), LM(md, b + Mos1Prep::gamma), LM(md, b + Mos1Prep::phit),
+                   LM(md, b + Mos1Prep::von0), LM(md, b + Mos1Prep::vcrit), LM(d.lim_mos, 3 * i),
+                   LM(d.lim_mos, 3 * i + 1), LM(d.lim_mos, 3 * i + 2), vgs, vds, vbs);
+        double scale = fmax(fmax(fabs(xd), fabs(xg)), fmax(fabs(xs), fabs(xb)));
+        double tol = eps16 * scale;
+        if (fabs(vgs - cgs) <= tol) vgs = cgs;
+        if (fabs(vds - cds) <= tol) vds = cds;
+        if (fabs(vbs - cbs) <= tol) vbs = cbs;
+        flag |= (vgs != cgs) | (vds != cds) | (vbs != cbs);
+        LM(d.lim_mos, 3 * i) = vgs;
+        LM(d.lim_mos, 3 * i + 1) = vds;
+        LM(d.lim_mos, 3 * i + 2) = vbs;
+    }
+    for (uint32_t i = 0; i < d.n_dio; i++) {
+        double xa = LM(x, d.dio_t[2 * i]), xc = LM(x, d.dio_t[2 * i + 1]);
+        double vd = xa - xc;
+        uint32_t b = DiodePrep::count * i;
+        double v = pnjlim(vd, LM(d.lim_dio, i), LM(d.dio_d, b + DiodePrep::vte), LM(d.dio_d, b + DiodePrep::vcrit));
+        if (fabs(v - vd) <= eps16 * fmax(fabs(xa), fabs(xc))) v = vd;
+        flag |= v != vd;
+        LM(d.lim_dio, i) = v;
+    }
+    return flag;
+}
+
+// ---------------------------------------------------------------------------
+// LU replay of the frozen tape, FP64 (Bodies.refactor + wideMultipliers).
+// True when the lane must peel.
+__device__ bool refactor64(const GroupDev& d, uint32_t l) {
+    const uint32_t P = d.P;
+    const double* __restrict__ a = d.a;
+    double* __restrict__ w = d.w;
+    double* __restrict__ lx = d.lx;
+    double* __restrict__ ux = d.ux;
+    double* __restrict__ ud = d.udiag;
+    for (uint32_t v = 0; v < d.n_void; v++)
+        if (LM(a, d.void_slots[v]) != 0.0) return true;
+    bool bad = false;
+    uint64_t nonfinite = 0;
+    const double growth = 1e-12;
+    for (uint32_t k = 0; k < d.n; k++) {
+        uint32_t c = d.q[k];
+        for (uint32_t p = d.col_ptr[c]; p < d.col_ptr[c + 1]; p++) LM(w, d.prow[p]) = LM(a, p);
+        for (uint32_t p = d.up[k]; p < d.up[k + 1]; p++) {
+            uint32_t i = d.ui[p];
+            double uki = LM(w, i);
+            LM(w, i) = 0.0;
+            LM(ux, p) = uki;
+            nonfinite |= dbits(uki - uki);
+            for (uint32_t pl = d.lp[i]; pl < d.lp[i + 1]; pl++) LM(w, d.li[pl]) -= LM(lx, pl) * uki;
+        }
+        uint32_t fl = d.flags[k];
+        if (fl & 1u) {
+            LM(ud, k) = 1.0;
+            for (uint32_t p = d.lp[k]; p < d.lp[k + 1]; p++) { LM(lx, p) = 0.0; LM(w, d.li[p]) = 0.0; }
+            LM(w, k) = 0.0;
+            for (uint32_t p = d.up[k]; p < d.up[k + 1]; p++) {
+                uint32_t i = d.ui[p];
+                for (uint32_t pl = d.lp[i]; pl < d.lp[i + 1]; pl++) LM(w, d.li[pl]) = 0.0;
+            }
+            continue;
+        }
+        double dk = LM(w, k);
+        LM(w, k) = 0.0;
+        bool dead = dk == 0.0 || !(fabs(dk) < INFINITY);
+        bad |= dead;
+        if (dead) dk = 1.0;
+        LM(ud, k) = dk;
+        if (!(fl & 2u)) {
+            uint64_t cb = dbits(fabs(dk));
+            for (uint32_t p = d.lp[k]; p < d.lp[k + 1]; p++) {
+                uint32_t r = d.li[p];
+                double v = LM(w, r);
+                LM(w, r) = 0.0;
+                uint64_t vb = dbits(fabs(v));
+                cb = cb > vb ? cb : vb;
+                LM(lx, p) = v / dk;
+            }
+            bad |= !(fabs(dk) >= growth * bitsd(cb));
+        } else {
+            for (uint32_t p = d.lp[k]; p < d.lp[k + 1]; p++) {
+                uint32_t r = d.li[p];
+                double lv = LM(w, r) / dk;
+                nonfinite |= dbits(lv - lv);
+                LM(lx, p) = lv;
+                LM(w, r) = 0.0;
+            }
+        }
+    }
+    if (nonfinite) return true;
+    uint64_t worst = 0;
+    for (uint32_t k = 0; k < d.n; k++) {
+        if (d.flags[k] & 2u) continue;
+        for (uint32_t p = d.lp[k]; p < d.lp[k + 1]; p++) {
+            uint64_t b = dbits(fabs(LM(lx, p)));
+            worst = worst > b ? worst : b;
+        }
+    }
+    return bad || !(bitsd(worst) <= kWide);
+}
+
+// The same replay in FP32 with FP32 accumulation over the FP64 matrix.
+__device__ bool refactor32(const GroupDev& d, uint32_t l) {
+    const uint32_t P = d.P;
+    const double* __restrict__ a = d.a;
+    float* __restrict__ w = d.w32;
+    float* __restrict__ lx = d.lx32;
+    float* __restrict__ ux = d.ux32;
+    float* __restrict__ ud = d.udiag32;
+    for (uint32_t v = 0; v < d.n_void; v++)
+        if (LM(a, d.void_slots[v]) != 0.0) return true;
+    bool bad = false;
+    uint32_t nonfinite = 0;
+    const float growth = 1e-12f;
+    for (uint32_t k = 0; k < d.n; k++) {
+        uint32_t c = d.q[k];
+        for (uint32_t p = d.col_ptr[c]; p < d.col_ptr[c + 1]; p++) LM(w, d.prow[p]) = (float)LM(a, p);
+        for (uint32_t p = d.up[k]; p < d.up[k + 1]; p++) {
+            uint32_t i = d.ui[p];
+            float uki = LM(w, i);
+            LM(w, i) = 0.0f;
+            LM(ux, p) = uki;
+            nonfinite |= fbits(uki - uki);
+            for (uint32_t pl = d.lp[i]; pl < d.lp[i + 1]; pl++) LM(w, d.li[pl]) -= LM(lx, pl) * uki;
+        }
+        uint32_t fl = d.flags[k];
+        if (fl & 1u) {
+            LM(ud, k) = 1.0f;
+            for (uint32_t p = d.lp[k]; p < d.lp[k + 1]; p++) { LM(lx, p) = 0.0f; LM(w, d.li[p]) = 0.0f; }
+            LM(w, k) = 0.0f;
+            for (uint32_t p = d.up[k]; p < d.up[k + 1]; p++) {
+                uint32_t i = d.ui[p];
+                for (uint32_t pl = d.lp[i]; pl < d.lp[i + 1]; pl++) LM(w, d.li[pl]) = 0.0f;
+            }
+            continue;
+        }
+        float dk = LM(w, k);
+        LM(w, k) = 0.0f;
+        bool dead = dk == 0.0f || !(fabsf(dk) < INFINITY);
+        bad |= dead;
+        if (dead) dk = 1.0f;
+        LM(ud, k) = dk;
+        float cmax = fabsf(dk);
+        for (uint32_t p = d.lp[k]; p < d.lp[k + 1]; p++) {
+            uint32_t r = d.li[p];
+            float v = LM(w, r);
+            LM(w, r) = 0.0f;
+            cmax = fmaxf(cmax, fabsf(v));
+            float lv = v / dk;
+            nonfinite |= fbits(lv - lv);
+            LM(lx, p) = lv;
+        }
+        if (!(fl & 2u)) bad |= !(fabsf(dk) >= growth * cmax) || !(cmax / fabsf(dk) <= (float)kWide);
+    }
+    return bad || nonfinite;
+}
+
+// dx = -A^-1 rhs through the FP64 factors (luSolve with neg).
+__device__ void solve64(const GroupDev& d, uint32_t l, const double* __restrict__ rhs, double* __restrict__ out) {
+    const uint32_t P = d.P;
+    double* __restrict__ y = d.y;
+    const double* __restrict__ lx = d.lx;
+    const double* __restrict__ ux = d.ux;
+    for (uint32_t r = 0; r < d.n; r++) LM(y, d.pinv[r]) = -LM(rhs, r);
+    for (uint32_t k = 0; k < d.n; k++) {
+        double yk = LM(y, k);
+        if (yk != 0.0)
+            for (uint32_t p = d.lp[k]; p < d.lp[k + 1]; p++) LM(y, d.li[p]) -= LM(lx, p) * yk;
+    }
+    for (uint32_t k = d.n; k-- > 0;) {
+        double zk = LM(y, k) / LM(d.udiag, k);
+        LM(y, k) = zk;
+        if (zk != 0.0)
+            for (uint32_t p = d.up[k]; p < d.up[k + 1]; p++) LM(y, d.ui[p]) -= LM(ux, p) * zk;
+    }
+    for (uint32_t j = 0; j < d.n; j++) LM(out, d.q[j]) = LM(y, j);
+}
+
+// The same through the FP32 factors; the right-hand side is rounded to
+// FP32 and the result widened back.
+__device__ void solve32(const GroupDev& d, uint32_t l, const double* __restrict__ rhs, double* __restrict__ out) {
+    const uint32_t P = d.P;
+    float* __restrict__ y = d.y32;
+    const float* __restrict__ lx = d.lx32;
+    const float* __restrict__ ux = d.ux32;
+    for (uint32_t r = 0; r < d.n; r++) LM(y, d.pinv[r]) = (float)(-LM(rhs, r));
+    for (uint32_t k = 0; k < d.n; k++) {
+        float yk = LM(y, k);
+        if (yk != 0.0f)
+            for (uint32_t p = d.lp[k]; p < d.lp[k + 1]; p++) LM(y, d.li[p]) -= LM(lx, p) * yk;
+    }
+    for (uint32_t k = d.n; k-- > 0;) {
+        float zk = LM(y, k) / LM(d.udiag32, k);
+        LM(y, k) = zk;
+        if (zk != 0.0f)
+            for (uint32_t p = d.up[k]; p < d.up[k + 1]; p++) LM(y, d.ui[p]) -= LM(ux, p) * zk;
+    }
+    for (uint32_t j = 0; j < d.n; j++) LM(out, d.q[j]) = (double)LM(y, j);
+}
+
+// One refinement sweep of a mixed solve. The linear system is A dx = -rhs;
+// r = rhs + A dx is its FP64 residual (negated), and the FP32 factors turn it
+// into the correction -A^-1 r that dx takes.
+__device__ void refine_mixed(const GroupDev& d, uint32_t l) {
+    const uint32_t P = d.P;
+    double* __restrict__ r = d.rr;
+    double* __restrict__ corr = d.corr;
+    for (uint32_t i = 0; i < d.n; i++) LM(r, i) = LM(d.rhs, i);
+    for (uint32_t c = 0; c < d.n; c++) {
+        double xc = LM(d.dx, c);
+        if (xc == 0.0) continue;
+        for (uint32_t p = d.col_ptr[c]; p < d.col_ptr[c + 1]; p++) LM(r, d.row_idx[p]) += LM(d.a, p) * xc;
+    }
+    solve32(d, l, r, corr);
+    for (uint32_t i = 0; i < d.n; i++) LM(d.dx, i) += LM(corr, i);
+}
+
+// x = -A^-1 b by dense LU with partial pivoting for a failed lane of n <= 64
+// (denseSolveNeg, kernels/lane.zig:310-350). m: n x n row-major scratch,
+// xv: n scratch holding b. False when a pivot is tiny or not finite.
+__device__ bool dense_solve_neg(uint32_t n, double* m, double* xv) {
+    const double tiny = 2.220446049250313e-16 * 2.220446049250313e-16;
+    for (uint32_t i = 0; i < n; i++) xv[i] = -xv[i];
+    for (uint32_t k = 0; k < n; k++) {
+        uint32_t mr = k;
+        double mv = fabs(m[k * n + k]);
+        for (uint32_t i = k + 1; i < n; i++) {
+            double v = fabs(m[i * n + k]);
+            if (v > mv) { mv = v; mr = i; }
+        }
+        double p = m[mr * n + k];
+        if (!(fabs(p) >= tiny && fabs(p) <= 1.7976931348623157e308)) return false;
+        if (mr != k) {
+            for (uint32_t j = 0; j < n; j++) {
+                double t = m[k * n + j];
+                m[k * n + j] = m[mr * n + j];
+                m[mr * n + j] = t;
+            }
+            double t = xv[k];
+            xv[k] = xv[mr];
+            xv[mr] = t;
+        }
+        double inv = 1.0 / m[k * n + k];
+        for (uint32_t i = k + 1; i < n; i++) {
+            double f = m[i * n + k] * inv;
+            for (uint32_t j = k + 1; j < n; j++) m[i * n + j] -= f * m[k * n + j];
+            xv[i] -= f * xv[k];
+        }
+    }
+    for (uint32_t ki = n; ki-- > 0;) {
+        double s = 0.0;
+        for (uint32_t j = ki + 1; j < n; j++) s += m[ki * n + j] * xv[j];
+        xv[ki] = (xv[ki] - s) / m[ki * n + ki];
+    }
+    return true;
+}
+
+}  // namespace espl

@@ -1,0 +1,43 @@
+// Host-side symbolic analysis for the lane tapes: the BTF + AMD column order
+// (ESPice src/solver/order.zig) and the lead lane's threshold-pivoted
+// Gilbert-Peierls factor (src/solver/sparse_lu.zig factor/factorPass), frozen
+// into the pivot tape every lane replays (src/solver/kernels/lane.zig
+// LaneTab/buildTab). This is the reference's `ownTape` step
+// (src/analysis/gpu/lanes.zig:590-603), which also runs on the host there.
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+namespace espl {
+
+constexpr uint32_t kNone = 0xFFFFFFFFu;
+constexpr double kPivotTol = 1e-3;          // direct.zig:33
+constexpr double kRepivotFillCap = 3.0;     // direct.zig:36
+constexpr double kGrowthLimit = 1e-12;      // direct.zig:54
+constexpr uint32_t kVoidBit = 1, kScaledBit = 2;  // kernels/lane.zig:41,44
+
+// Column order q (q[k] = column factored at step k). False on
+// OutOfWorkspace, with the reference's slab size 48 n + 8 nnz + 64 words.
+bool order_columns(uint32_t n, const uint32_t* col_ptr, const uint32_t* row_idx, std::vector<uint32_t>& q);
+
+// Strictly-lower plus strictly-upper entries of an LU of the pattern under
+// diagonal pivots in order q: twice the off-diagonal Cholesky count of A+A^T.
+uint64_t diag_fill(uint32_t n, const uint32_t* col_ptr, const uint32_t* row_idx, const std::vector<uint32_t>& q);
+
+// A frozen pivot tape: the factor's pattern and pivot sequence.
+struct Tape {
+    uint32_t n = 0, nnz = 0;
+    std::vector<uint32_t> q, pinv, lp, li, up, ui, prow, flags, void_slots;
+    std::vector<double> lx, ux, udiag;  // the lead lane's factor values
+    bool sn_dfs = false;
+    uint32_t panels = 0;
+};
+
+// The lead lane's full factor of `vals` on order q with the reference's
+// fill caps (a first pass capped at 3 x diag_fill, then the diagonal
+// pivots). False when the matrix is singular.
+bool factor_tape(uint32_t n, const uint32_t* col_ptr, const uint32_t* row_idx, const double* vals,
+                 const std::vector<uint32_t>& q, Tape& out);
+
+}  // namespace espl

@@ -1,0 +1,171 @@
+"""Python host mirror of the lane driver seam (include/espice_lanes.h).
+
+`Lanes` owns one espl_lanes handle: the role of ESPice's `GpuLanes`
+(src/analysis/gpu/lanes.zig) for a batch of sweep points, possibly drawn from
+several templates of different sizes. The compute runs in the sm_100a
+library egspice_b200/_lib/libespice_lanes.so; there is no CPU fallback, and
+a missing library or GPU raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import abi
+from .abi import (CreateOpts, LaneNewton, NetlistC, NewtonOpts, StepReport, Stats, TranOpts, f64p, u32p)
+from .decks import Netlist
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libespice_lanes.so")
+_lib = None
+
+
+class LaneError(RuntimeError):
+    pass
+
+
+def lib():
+    """Loads the CUDA lane library; raises when it is not built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise LaneError(f"{LIB_PATH} is missing: run egspice_b200/build.py (nvcc, sm_100a)")
+        L = C.CDLL(LIB_PATH)
+        L.espl_abi_version.restype = C.c_uint32
+        L.espl_create.argtypes = [C.POINTER(NetlistC), C.c_uint32, C.POINTER(CreateOpts), C.c_double,
+                                  C.POINTER(C.c_void_p)]
+        L.espl_create.restype = C.c_uint32
+        L.espl_destroy.argtypes = [C.c_void_p]
+        L.espl_destroy.restype = C.c_uint32
+        L.espl_tape_info.argtypes = [C.c_void_p, C.c_uint32, u32p, u32p, u32p]
+        L.espl_tape_info.restype = C.c_uint32
+        L.espl_copy_tape.argtypes = [C.c_void_p, C.c_uint32] + [u32p] * 7
+        L.espl_copy_tape.restype = C.c_uint32
+        L.espl_put_x.argtypes = [C.c_void_p, C.c_uint32, f64p, C.c_uint32]
+        L.espl_put_x.restype = C.c_uint32
+        L.espl_get_x.argtypes = [C.c_void_p, C.c_uint32, f64p]
+        L.espl_get_x.restype = C.c_uint32
+        L.espl_solve_static.argtypes = [C.c_void_p, C.POINTER(NewtonOpts), C.POINTER(LaneNewton)]
+        L.espl_solve_static.restype = C.c_uint32
+        L.espl_init_steps.argtypes = [C.c_void_p, C.POINTER(TranOpts)]
+        L.espl_init_steps.restype = C.c_uint32
+        L.espl_device_launch.argtypes = [C.c_void_p, C.c_uint32, C.POINTER(StepReport)]
+        L.espl_device_launch.restype = C.c_uint32
+        L.espl_set_period_meas.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_double, C.c_double]
+        L.espl_set_period_meas.restype = C.c_uint32
+        L.espl_get_period_meas.argtypes = [C.c_void_p, C.c_uint32, f64p, u32p]
+        L.espl_get_period_meas.restype = C.c_uint32
+        L.espl_get_stats.argtypes = [C.c_void_p, C.POINTER(Stats)]
+        L.espl_get_stats.restype = C.c_uint32
+        L.espl_error_message.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t]
+        L.espl_error_message.restype = C.c_uint32
+        _lib = L
+    return _lib
+
+
+PRECISION = {"fp64": abi.ESPL_FP64, "mixed": abi.ESPL_MIXED}
+
+
+class Lanes:
+    """Lanes of one or more templates on one GPU."""
+
+    def __init__(self, nets: Sequence[Netlist], precision: str = "fp64", dt0: float = 0.0, device: int = 0):
+        self.nets = list(nets)
+        self._keep, arr = abi.cnets(self.nets)
+        self._arr = arr
+        opts = CreateOpts(1, PRECISION[precision], device, 0)
+        h = C.c_void_p()
+        st = lib().espl_create(arr, len(self.nets), C.byref(opts), dt0, C.byref(h))
+        if st != 0:
+            raise LaneError(f"espl_create failed with status {st}")
+        self.h = h
+        self.total = sum(n.lanes for n in self.nets)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().espl_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, st: int, what: str):
+        if st != 0:
+            buf = C.create_string_buffer(512)
+            lib().espl_error_message(self.h, buf, 512)
+            raise LaneError(f"{what} failed with status {st}: {buf.value.decode()}")
+
+    def put_x(self, net: int, x: np.ndarray, cold: bool):
+        nl = self.nets[net]
+        x = np.ascontiguousarray(x, dtype=np.float64).reshape(nl.lanes, nl.n)
+        self._check(lib().espl_put_x(self.h, net, x.ctypes.data_as(f64p), int(cold)), "espl_put_x")
+
+    def cold_start(self):
+        for i, nl in enumerate(self.nets):
+            self.put_x(i, np.zeros((nl.lanes, nl.n)), True)
+
+    def get_x(self, net: int) -> np.ndarray:
+        nl = self.nets[net]
+        x = np.zeros((nl.lanes, nl.n))
+        self._check(lib().espl_get_x(self.h, net, x.ctypes.data_as(f64p)), "espl_get_x")
+        return x
+
+    def solve_static(self, opts: NewtonOpts) -> np.ndarray:
+        """Newton per lane; returns [total, 3] of (bits, iterations, fp64 fallbacks)."""
+        out = (LaneNewton * self.total)()
+        self._check(lib().espl_solve_static(self.h, C.byref(opts), out), "espl_solve_static")
+        return np.array([[o.bits, o.iterations, o.refactor_fallbacks] for o in out], dtype=np.int64)
+
+    def init_steps(self, topts: TranOpts):
+        self._check(lib().espl_init_steps(self.h, C.byref(topts)), "espl_init_steps")
+
+    def device_launch(self, max_steps: int) -> List[StepReport]:
+        reps = (StepReport * self.total)()
+        self._check(lib().espl_device_launch(self.h, max_steps, reps), "espl_device_launch")
+        return list(reps)
+
+    def run_tran(self, topts: TranOpts, steps_per_launch: int = 256, max_launches: int = 100000):
+        """Runs every lane to t_stop; returns the final reports."""
+        self.init_steps(topts)
+        reps = None
+        for _ in range(max_launches):
+            reps = self.device_launch(steps_per_launch)
+            if all(r.status != 0 for r in reps):
+                break
+        return reps
+
+    def set_period_meas(self, net: int, row: int, level: float, t_start: float):
+        self._check(lib().espl_set_period_meas(self.h, net, row, level, t_start), "espl_set_period_meas")
+
+    def period_meas(self, net: int):
+        nl = self.nets[net]
+        per = np.zeros(nl.lanes)
+        cr = np.zeros(nl.lanes, dtype=np.uint32)
+        self._check(lib().espl_get_period_meas(self.h, net, per.ctypes.data_as(f64p), cr.ctypes.data_as(u32p)),
+                    "espl_get_period_meas")
+        return per, cr
+
+    def tape(self, net: int) -> dict:
+        n, nl, nu = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        self._check(lib().espl_tape_info(self.h, net, C.byref(n), C.byref(nl), C.byref(nu)), "espl_tape_info")
+        n, nl, nu = n.value, nl.value, nu.value
+        arrs = {"q": n, "pinv": n, "lp": n + 1, "li": nl, "up": n + 1, "ui": nu, "flags": n}
+        out = {k: np.zeros(max(v, 1), dtype=np.uint32) for k, v in arrs.items()}
+        self._check(lib().espl_copy_tape(self.h, net, *[out[k].ctypes.data_as(u32p) for k in
+                                                        ("q", "pinv", "lp", "li", "up", "ui", "flags")]),
+                    "espl_copy_tape")
+        return {k: out[k][:arrs[k]] for k in arrs}
+
+    def stats(self) -> Stats:
+        s = Stats()
+        self._check(lib().espl_get_stats(self.h, C.byref(s)), "espl_get_stats")
+        return s

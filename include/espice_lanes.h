@@ -1,0 +1,250 @@
+/* espice_lanes: the GPU lane-sweep seam of ESPice, as a C ABI for B200
+ * (sm_100a). Many sweep points ("lanes") of one or more circuit templates
+ * run together on the GPU: per-lane device evaluation and MNA stamping,
+ * numeric refactorization of a frozen Gilbert-Peierls pivot tape on the
+ * BTF/AMD column order, and forward/back substitution, inside the
+ * operating-point Newton loop and the transient step loop.
+ *
+ * Each entry point replaces one call of the reference's GPU lane driver
+ * `GpuLanes` (src/analysis/gpu/lanes.zig), which the Zig host code
+ * (src/analysis/dc/op.zig solveGpuLanes, src/analysis/tran/tran.zig
+ * runGpuLanes, src/c_api.zig) reaches through Gompute kernel handles. Only C
+ * types cross this boundary, so a Zig `extern fn` declaration binds it as is.
+ *
+ * Ownership: the handle owns all device memory; arrays passed in are
+ * borrowed for the duration of the call only. Calls on one handle must be
+ * serialized; different handles are independent.
+ */
+#ifndef ESPICE_LANES_H
+#define ESPICE_LANES_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ESPL_ABI_VERSION 1u
+
+/* A device terminal on the datum node. Its residual row and Jacobian
+ * entries are dropped, as the reference's GROUND gather does
+ * (src/device/eval.zig evalRange, `gi != GROUND`). */
+#define ESPL_GROUND 0xFFFFFFFFu
+
+typedef uint32_t espl_status;
+/* Mirrors the reference's lane errors (lanes.zig:165-172: NoLaneImage,
+ * NoLaneTape, IncompatibleLanes) plus driver, memory and timeout codes. */
+enum {
+    ESPL_OK = 0,
+    ESPL_INVALID_ARGUMENT = 1,
+    ESPL_NO_IMAGE = 2,        /* no CUDA device or kernel image for it */
+    ESPL_NO_TAPE = 3,         /* the lead lane's host factor failed */
+    ESPL_INCOMPATIBLE = 4,    /* lanes the device path refuses */
+    ESPL_DRIVER = 5,          /* a CUDA runtime error */
+    ESPL_OUT_OF_MEMORY = 6,
+    ESPL_TIMEOUT = 7,         /* a bounded device loop ran out */
+    ESPL_TOO_LARGE = 8        /* a size beyond a stated maximum */
+};
+
+/* Device kinds. Terminal and parameter rows per kind:
+ *   RES   term p n           param r                                   (models/resistor.va)
+ *   CAP   term p n           param c                                   (models/capacitor.va)
+ *   VSRC  term p n br        param dc wave v1 v2 td tr tf pw per        (models/vsource.va; br = branch-current unknown)
+ *   ISRC  term p n           param dc wave v1 v2 td tr tf pw per        (models/isource.va)
+ *   DIODE term a c           param is n cjo vj m fc tt                  (models/diode.va, rs = 0)
+ *   MOS1  term d g s b       param type vto kp gamma phi lambda is w l  (models/mos1.va, rd = rs = 0, no TOX, no CJ)
+ * wave: 0 DC, 1 PULSE. */
+enum { ESPL_RES = 1, ESPL_CAP = 2, ESPL_VSRC = 3, ESPL_ISRC = 4, ESPL_DIODE = 5, ESPL_MOS1 = 6 };
+#define ESPL_RES_TERMS 2u
+#define ESPL_RES_PARAMS 1u
+#define ESPL_CAP_TERMS 2u
+#define ESPL_CAP_PARAMS 1u
+#define ESPL_SRC_PARAMS 9u
+#define ESPL_VSRC_TERMS 3u
+#define ESPL_ISRC_TERMS 2u
+#define ESPL_DIODE_TERMS 2u
+#define ESPL_DIODE_PARAMS 7u
+#define ESPL_MOS1_TERMS 4u
+#define ESPL_MOS1_PARAMS 9u
+
+/* One device batch of a template: `count` instances of `kind`.
+ * term[i * terms + t] is the unknown of terminal t of instance i, or
+ * ESPL_GROUND. param[(i * params + k) * lanes + l] is parameter k of
+ * instance i in lane l (lane-major, the layout the device reads). */
+typedef struct {
+    uint32_t kind;
+    uint32_t count;
+    const uint32_t *term;
+    const double *param;
+} espl_batch;
+
+/* One circuit template and its lanes. Unknown 0 is the ground row, pinned
+ * by G[0,0] += 1 and F[0] += x[0] after every stamp (src/analysis/Circuit.zig
+ * groundStamp). The CSC pattern must hold every diagonal and every entry the
+ * devices stamp. */
+typedef struct {
+    uint32_t n;
+    uint32_t nnz;
+    const uint32_t *col_ptr; /* n + 1 */
+    const uint32_t *row_idx; /* nnz */
+    uint32_t n_batches;
+    const espl_batch *batches;
+    uint32_t lanes;
+} espl_netlist;
+
+/* Newton controls: `converger.Options` (src/solver/converger.zig) as the
+ * device gates read them (`NewtonOpts`, src/solver/kernels/lane.zig:719). */
+typedef struct {
+    double reltol;       /* 1e-3 */
+    double abstol;       /* 1e-12 A, current rows */
+    double vntol;        /* 1e-6 V */
+    double gmin;         /* diagonal gmin; 0 in the plain operating-point rung */
+    double residual_tol; /* 1e-9 */
+    uint32_t max_iter;   /* 100 */
+    uint32_t init_fix;   /* 1: cold operating point (MODEINITJCT/INITFIX) */
+} espl_newton_opts;
+
+/* Per-lane outcome: `LaneNewton` of lanes.zig. bits: 4 converged,
+ * 8 singular (the lane's replay failed), 32 handed back to the host. */
+typedef struct {
+    uint32_t bits;
+    uint32_t iterations;
+    uint32_t refactor_fallbacks; /* mixed precision: FP64 refactors taken */
+    uint32_t reserved;
+} espl_lane_newton;
+
+#define ESPL_CONVERGED 4u
+#define ESPL_SINGULAR 8u
+#define ESPL_PARKED 32u
+
+/* Precision of the LU refactor and triangular solves. Device evaluation,
+ * residuals, the Newton update and step control are FP64 in both. */
+enum { ESPL_FP64 = 0, ESPL_MIXED = 1 };
+
+typedef struct {
+    uint32_t abi_version;
+    uint32_t precision;      /* ESPL_FP64 or ESPL_MIXED */
+    uint32_t device;         /* CUDA device ordinal */
+    uint32_t lanes_per_cta;  /* 0: the autotuned default */
+} espl_create_opts;
+
+typedef struct espl_lanes espl_lanes;
+
+uint32_t espl_abi_version(void);
+
+/* `GpuLanes.init` / `initStatic` (lanes.zig:610, 1080) over `n_nets`
+ * templates at once: each template gets its pivot tape from its lane 0
+ * (`ownTape`, lanes.zig:590-603: the lead lane's matrix at x = 0, factored
+ * on the host with threshold pivoting on the BTF/AMD order), and all lanes of
+ * all templates run in the same launches (a lane -> tape table). For a
+ * transient, `dt0` > 0 builds the tape from G + C / dt0 as `ownTape` does. */
+espl_status espl_create(const espl_netlist *nets, uint32_t n_nets, const espl_create_opts *opts,
+                        double dt0, espl_lanes **out);
+
+/* `GpuLanes.deinit` (lanes.zig:1004). NULL is a no-op. */
+espl_status espl_destroy(espl_lanes *h);
+
+/* The pivot tape of template `net` (`LaneTab` + index buffer,
+ * src/solver/kernels/lane.zig:17-44, buildTab :778-802), copied out:
+ * q, pinv (n each), lp, up (n + 1 each), li (nnz_l), ui (nnz_u), flags (n;
+ * bit 0 void, bit 1 scaled pivot). A NULL array is skipped. */
+espl_status espl_tape_info(espl_lanes *h, uint32_t net, uint32_t *n, uint32_t *nnz_l, uint32_t *nnz_u);
+espl_status espl_copy_tape(espl_lanes *h, uint32_t net, uint32_t *q, uint32_t *pinv, uint32_t *lp,
+                           uint32_t *li, uint32_t *up, uint32_t *ui, uint32_t *flags);
+
+/* Lane start states, point-major: x[l * n + i] for the lanes of template
+ * `net` (`GpuLanes.reload` / put_x, lanes.zig:1127). cold = 1 also seeds the
+ * junction limiters as `op.coldStart` does (src/analysis/dc/op.zig:28-33;
+ * MOS1 vgs = vto, vds = 0, vbs = -1). */
+espl_status espl_put_x(espl_lanes *h, uint32_t net, const double *x, uint32_t cold);
+espl_status espl_get_x(espl_lanes *h, uint32_t net, double *x);
+
+/* `GpuLanes.solveStatic` (lanes.zig:1171): one device Newton per lane from
+ * its current x, the operating point's plain rung. out[] holds every lane
+ * of every template, template-major. */
+espl_status espl_solve_static(espl_lanes *h, const espl_newton_opts *opts, espl_lane_newton *out);
+
+/* Transient lanes with device step control (`initSteps` lanes.zig:1827,
+ * `deviceLaunch` :1917; the step machine `stepBegin/stepEndA/stepEndB`,
+ * src/solver/kernels/lane.zig:505-700). */
+typedef struct {
+    double t_stop;
+    double dt;        /* first (and, when fixed_step, every) step */
+    double dt_min;
+    double dt_max;
+    double reltol, abstol, chgtol, trtol, vntol, residual_tol;
+    uint32_t method;     /* 0 BE, 1 trapezoidal (order 1 first, then 2) */
+    uint32_t fixed_step; /* 1: no LTE control, every step dt */
+    uint32_t max_iter;   /* Newton iterations per step (ITL4-like) */
+    uint32_t max_steps;
+    uint32_t predictor;  /* 0 none (x_prev), 1 linear (SPICE xfact), 2 learned */
+    uint32_t reserved;
+} espl_tran_opts;
+
+/* `StepReport` (src/solver/kernels/lane.zig:441) per lane. status: 0
+ * stepping, 1 done, 2 dt underflow, 3 parked, 4 stopped. */
+typedef struct {
+    double t;
+    double dt;
+    uint64_t attempts;
+    uint64_t nr_iters;
+    uint32_t steps;
+    uint32_t rejects;
+    uint32_t status;
+    uint32_t reserved;
+} espl_step_report;
+
+espl_status espl_init_steps(espl_lanes *h, const espl_tran_opts *opts);
+
+/* Runs up to `max_steps` accepted steps per lane (or to t_stop), all on the
+ * device, then fills reports[] for every lane, template-major. */
+espl_status espl_device_launch(espl_lanes *h, uint32_t max_steps, espl_step_report *reports);
+
+/* Device-side oscillation-period measure (`arp_lane_meas`,
+ * src/solver/lane_device.zig:45-72, restricted to a period pass): the mean
+ * spacing of rising crossings of `level` by unknown `row` after `t_start`,
+ * over crossings 1..k. Set before espl_init_steps; read after the run. */
+espl_status espl_set_period_meas(espl_lanes *h, uint32_t net, uint32_t row, double level, double t_start);
+espl_status espl_get_period_meas(espl_lanes *h, uint32_t net, double *period, uint32_t *crossings);
+
+/* Timing of the last solve/launch, milliseconds of device time per kernel
+ * family (CUDA events on the launching stream), for roofline reporting. */
+typedef struct {
+    double total_ms;
+    double newton_ms;
+    uint64_t launches;
+    uint64_t lane_iterations;
+    uint64_t lane_steps;
+} espl_stats;
+espl_status espl_get_stats(espl_lanes *h, espl_stats *out);
+
+/* Host-only symbolic seam, no GPU needed. `espl_order` is order.zig's
+ * `order` (src/solver/order.zig:78): q[k] = the column factored at step k,
+ * BTF sink block first, AMD or natural per block. ESPL_NO_TAPE on
+ * OutOfWorkspace. */
+espl_status espl_order(uint32_t n, const uint32_t *col_ptr, const uint32_t *row_idx, uint32_t *q);
+
+/* The lead lane's factor as `ownTape` runs it (lanes.zig:590-603):
+ * SparseLu.factor with threshold pivoting on order q and the fill caps of
+ * direct.Solver (src/solver/sparse_lu.zig:274-311, direct.zig:310-388),
+ * frozen as a tape (kernels/lane.zig buildTab :778-802). ESPL_NO_TAPE when
+ * the matrix is singular. Free with espl_tape_free. */
+typedef struct espl_tape espl_tape;
+espl_status espl_tape_build(uint32_t n, const uint32_t *col_ptr, const uint32_t *row_idx, const double *vals,
+                            const uint32_t *q, espl_tape **out);
+espl_status espl_tape_sizes(const espl_tape *t, uint32_t *nnz_l, uint32_t *nnz_u, uint32_t *n_void_slots);
+/* Copies q, pinv (n), lp, up (n + 1), li (nnz_l), ui (nnz_u), flags (n),
+ * prow (nnz), void_slots, and the lead lane's lx, ux, udiag. NULL skips. */
+espl_status espl_tape_copy(const espl_tape *t, uint32_t *q, uint32_t *pinv, uint32_t *lp, uint32_t *li, uint32_t *up,
+                           uint32_t *ui, uint32_t *flags, uint32_t *prow, uint32_t *void_slots, double *lx,
+                           double *ux, double *udiag);
+void espl_tape_free(espl_tape *t);
+
+/* The last error's text, NUL-terminated (empty when none). */
+espl_status espl_error_message(espl_lanes *h, char *buf, size_t cap);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

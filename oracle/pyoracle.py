@@ -1,0 +1,250 @@
+"""ctypes binding of the oracle library (test infrastructure only).
+
+Imported by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg;
+the product package never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from typing import Optional, Sequence, Tuple
+
+import numpy as np
+
+from egspice_b200.abi import (CNet, NetlistC, NewtonOpts, OrcNewtonResult, StepReport, TranOpts, f64p, u32p)
+from egspice_b200.decks import Netlist
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_build", "liborc.so")
+_lib = None
+
+
+def build() -> str:
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        L = C.CDLL(LIB)
+        L.orc_order.argtypes = [C.c_uint32, u32p, u32p, u32p]
+        L.orc_order.restype = C.c_int
+        L.orc_order_ws.argtypes = [C.c_uint32, u32p, u32p, u32p, u32p, C.c_size_t]
+        L.orc_order_ws.restype = C.c_int
+        L.orc_amd_ws.argtypes = [C.c_uint32, u32p, u32p, u32p, u32p, C.c_size_t]
+        L.orc_amd_ws.restype = C.c_int
+        L.orc_ws_size.argtypes = [C.c_size_t, C.c_size_t]
+        L.orc_ws_size.restype = C.c_size_t
+        L.orc_chol_count.argtypes = [C.c_uint32, u32p, u32p, u32p, C.c_uint64]
+        L.orc_chol_count.restype = C.c_uint64
+        L.orc_lu_new.argtypes = [C.c_uint32, u32p, u32p]
+        L.orc_lu_new.restype = C.c_void_p
+        L.orc_lu_free.argtypes = [C.c_void_p]
+        L.orc_lu_set_caps.argtypes = [C.c_void_p, C.c_uint64, C.c_double, C.c_double]
+        L.orc_lu_factor.argtypes = [C.c_void_p, u32p, u32p, f64p, C.c_double]
+        L.orc_lu_factor.restype = C.c_int
+        L.orc_lu_refactor.argtypes = [C.c_void_p, u32p, f64p, C.c_double]
+        L.orc_lu_refactor.restype = C.c_int
+        L.orc_lu_solve.argtypes = [C.c_void_p, f64p, f64p]
+        L.orc_lu_solve_t.argtypes = [C.c_void_p, f64p, f64p]
+        L.orc_lu_tape.argtypes = [C.c_void_p, C.c_void_p]
+        L.orc_op_lanes.argtypes = [C.POINTER(NetlistC), C.c_uint32, C.c_uint32, C.POINTER(NewtonOpts), f64p, f64p,
+                                   C.POINTER(OrcNewtonResult), C.c_uint32]
+        L.orc_op_lanes.restype = C.c_int
+        L.orc_tran_lanes.argtypes = [C.POINTER(NetlistC), C.c_uint32, C.c_uint32, C.POINTER(TranOpts), u32p,
+                                     C.c_uint32, C.c_uint32, f64p, f64p, C.POINTER(StepReport), C.c_uint32,
+                                     C.c_double, C.c_double, f64p, C.c_uint32]
+        L.orc_tran_lanes.restype = C.c_int
+        L.orc_device_probe.argtypes = [C.POINTER(NetlistC), C.c_uint32, C.c_uint32, C.c_uint32, f64p, f64p, f64p,
+                                       f64p, f64p]
+        L.orc_device_probe.restype = C.c_int
+        L.orc_pnjlim.argtypes = [C.c_double, C.c_double, C.c_double, C.c_double, C.POINTER(C.c_int)]
+        L.orc_pnjlim.restype = C.c_double
+        L.orc_fetlim.argtypes = [C.c_double, C.c_double, C.c_double]
+        L.orc_fetlim.restype = C.c_double
+        L.orc_limvds.argtypes = [C.c_double, C.c_double]
+        L.orc_limvds.restype = C.c_double
+        L.orc_normal_quantile.argtypes = [C.c_double]
+        L.orc_normal_quantile.restype = C.c_double
+        L.orc_site_key.argtypes = [C.c_uint64, C.c_uint64]
+        L.orc_site_key.restype = C.c_uint64
+        L.orc_step_bound.argtypes = [C.c_uint32, C.c_uint32, f64p, f64p, f64p, f64p, f64p, C.c_uint32, f64p]
+        L.orc_step_bound.restype = C.c_double
+        _lib = L
+    return _lib
+
+
+def _u32(a):
+    a = np.ascontiguousarray(a, dtype=np.uint32)
+    return a, a.ctypes.data_as(u32p)
+
+
+def _f64(a):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    return a, a.ctypes.data_as(f64p)
+
+
+def order(col_ptr, row_idx, slab_len: Optional[int] = None) -> Optional[np.ndarray]:
+    """BTF + AMD column order (order.zig `order`); None on OutOfWorkspace."""
+    n = len(col_ptr) - 1
+    cp, cpp = _u32(col_ptr)
+    ri, rip = _u32(row_idx)
+    q = np.zeros(max(n, 1), dtype=np.uint32)
+    if slab_len is None:
+        r = lib().orc_order(n, cpp, rip, q.ctypes.data_as(u32p))
+    else:
+        slab = np.zeros(max(slab_len, 1), dtype=np.uint32)
+        r = lib().orc_order_ws(n, cpp, rip, q.ctypes.data_as(u32p), slab.ctypes.data_as(u32p), slab_len)
+    return None if r != 0 else q[:n]
+
+
+def amd(col_ptr, row_idx, slab_len: Optional[int] = None) -> Optional[np.ndarray]:
+    n = len(col_ptr) - 1
+    cp, cpp = _u32(col_ptr)
+    ri, rip = _u32(row_idx)
+    if slab_len is None:
+        slab_len = ws_size(n, int(cp[-1]))
+    slab = np.zeros(max(slab_len, 1), dtype=np.uint32)
+    q = np.zeros(max(n, 1), dtype=np.uint32)
+    r = lib().orc_amd_ws(n, cpp, rip, q.ctypes.data_as(u32p), slab.ctypes.data_as(u32p), slab_len)
+    return None if r != 0 else q[:n]
+
+
+def ws_size(n: int, nnz: int) -> int:
+    return int(lib().orc_ws_size(n, nnz))
+
+
+def chol_count(col_ptr, row_idx, perm, cap=(1 << 64) - 1) -> int:
+    n = len(col_ptr) - 1
+    cp, cpp = _u32(col_ptr)
+    ri, rip = _u32(row_idx)
+    pm, pmp = _u32(perm)
+    return int(lib().orc_chol_count(n, cpp, rip, pmp, cap))
+
+
+class OrcTape(C.Structure):
+    _fields_ = [("n", C.c_uint32), ("nnz", C.c_uint32), ("nnz_l", C.c_uint32), ("nnz_u", C.c_uint32),
+                ("q", u32p), ("pinv", u32p), ("lp", u32p), ("li", u32p), ("up", u32p), ("ui", u32p),
+                ("prow", u32p), ("void_col", C.POINTER(C.c_uint8)), ("scaled_pivot", C.POINTER(C.c_uint8)),
+                ("void_slots", u32p), ("n_void_slots", C.c_uint32), ("lx", f64p), ("ux", f64p),
+                ("udiag", f64p), ("sn_dfs", C.c_uint32), ("n_panels", C.c_uint32)]
+
+
+class SparseLu:
+    """SparseLu over a caller-given column order."""
+
+    def __init__(self, col_ptr, row_idx, q, diag_fill=0, fill_cap=0.0, keep_min=0.0):
+        self.cp, self.cpp = _u32(col_ptr)
+        self.ri, self.rip = _u32(row_idx)
+        self.q, qp = _u32(q)
+        self.n = len(self.cp) - 1
+        self.h = lib().orc_lu_new(self.n, self.cpp, qp)
+        lib().orc_lu_set_caps(self.h, diag_fill, fill_cap, keep_min)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_lu_free(self.h)
+            self.h = None
+
+    def factor(self, vals, pivot_tol=1e-3) -> int:
+        v, vp = _f64(vals)
+        return lib().orc_lu_factor(self.h, self.cpp, self.rip, vp, pivot_tol)
+
+    def refactor(self, vals, growth=1e-12) -> int:
+        v, vp = _f64(vals)
+        return lib().orc_lu_refactor(self.h, self.cpp, vp, growth)
+
+    def solve(self, b) -> np.ndarray:
+        bb, bp = _f64(b)
+        x = np.zeros(self.n)
+        lib().orc_lu_solve(self.h, bp, x.ctypes.data_as(f64p))
+        return x
+
+    def solve_t(self, b) -> np.ndarray:
+        bb, bp = _f64(b)
+        x = np.zeros(self.n)
+        lib().orc_lu_solve_t(self.h, bp, x.ctypes.data_as(f64p))
+        return x
+
+    def tape(self) -> dict:
+        t = OrcTape()
+        lib().orc_lu_tape(self.h, C.byref(t))
+        n = t.n
+
+        def cp(ptr, m, dt=np.uint32):
+            return np.ctypeslib.as_array(ptr, shape=(m,)).astype(dt).copy() if m else np.zeros(0, dt)
+
+        return {
+            "q": cp(t.q, n), "pinv": cp(t.pinv, n), "lp": cp(t.lp, n + 1), "li": cp(t.li, t.nnz_l),
+            "up": cp(t.up, n + 1), "ui": cp(t.ui, t.nnz_u), "prow": cp(t.prow, t.nnz),
+            "void_col": cp(t.void_col, n, np.uint8), "scaled_pivot": cp(t.scaled_pivot, n, np.uint8),
+            "void_slots": cp(t.void_slots, t.n_void_slots),
+            "lx": cp(t.lx, t.nnz_l, np.float64), "ux": cp(t.ux, t.nnz_u, np.float64),
+            "udiag": cp(t.udiag, n, np.float64), "sn_dfs": t.sn_dfs, "n_panels": t.n_panels,
+        }
+
+
+def op_lanes(net: Netlist, opts: NewtonOpts, lane0: int = 0, count: Optional[int] = None, x_in=None,
+             threads: int = 1) -> Tuple[np.ndarray, np.ndarray]:
+    """Operating points of lanes [lane0, lane0 + count); returns x [count, n]
+    and results [count, 3] (converged, singular, iterations)."""
+    if count is None:
+        count = net.lanes - lane0
+    cn = CNet(net)
+    x = np.zeros((count, net.n))
+    res = (OrcNewtonResult * count)()
+    xin = None
+    if x_in is not None:
+        xi, xin = _f64(x_in)
+    r = lib().orc_op_lanes(C.byref(cn.c), lane0, count, C.byref(opts), xin, x.ctypes.data_as(f64p), res, threads)
+    assert r == 0
+    out = np.array([[e.converged, e.singular, e.iterations] for e in res], dtype=np.int64)
+    return x, out
+
+
+def tran_lanes(net: Netlist, opts: TranOpts, lane0: int = 0, count: Optional[int] = None,
+               probes: Sequence[int] = (), max_rows: int = 0, meas: Optional[Tuple[int, float, float]] = None,
+               threads: int = 1):
+    """Transients of lanes [lane0, lane0 + count). Returns (x_final [count, n],
+    reports list, probe rows [count, max_rows, n_probes] or None, period
+    [count] or None)."""
+    if count is None:
+        count = net.lanes - lane0
+    cn = CNet(net)
+    x = np.zeros((count, net.n))
+    reps = (StepReport * count)()
+    pr, prp = _u32(np.asarray(probes, dtype=np.uint32) if len(probes) else np.zeros(1, np.uint32))
+    rows = None
+    rowp = None
+    if len(probes) and max_rows:
+        rows = np.full((count, max_rows, len(probes)), np.nan)
+        rowp = rows.ctypes.data_as(f64p)
+    per = None
+    perp = None
+    mrow, mlev, mt0 = (0xFFFFFFFF, 0.0, 0.0)
+    if meas is not None:
+        mrow, mlev, mt0 = meas
+        per = np.full(count, np.nan)
+        perp = per.ctypes.data_as(f64p)
+    r = lib().orc_tran_lanes(C.byref(cn.c), lane0, count, C.byref(opts), prp, len(probes), max_rows, rowp,
+                             x.ctypes.data_as(f64p), reps, mrow, mlev, mt0, perp, threads)
+    assert r == 0
+    return x, list(reps), rows, per
+
+
+def device_probe(net: Netlist, batch: int, inst: int, lane: int, v):
+    nt = {1: 2, 2: 2, 3: 3, 4: 2, 5: 2, 6: 4}[net.batches[batch].kind]
+    cn = CNet(net)
+    vv, vp = _f64(v)
+    f = np.zeros(nt)
+    j = np.zeros(nt * nt)
+    q = np.zeros(nt)
+    cj = np.zeros(nt * nt)
+    r = lib().orc_device_probe(C.byref(cn.c), batch, inst, lane, vp, f.ctypes.data_as(f64p),
+                               j.ctypes.data_as(f64p), q.ctypes.data_as(f64p), cj.ctypes.data_as(f64p))
+    assert r == 0
+    return f, j.reshape(nt, nt), q, cj.reshape(nt, nt)
