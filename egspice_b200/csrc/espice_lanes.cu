@@ -454,13 +454,13 @@ espl_status espl_create(const espl_netlist* nets, uint32_t n_nets, const espl_cr
     cudaMemcpyAsync(h->d_mos_raw, mr.data(), sizeof(double*) * n_nets, cudaMemcpyHostToDevice, h->stream);
     cudaMemcpyAsync(h->d_dio_raw, dr.data(), sizeof(double*) * n_nets, cudaMemcpyHostToDevice, h->stream);
     // Dense-peel pool for templates of n <= 64 (lanes.zig:908 sizes its
-    // pool by memory; here 256 slots of 64 x 64 + 64 doubles, 8.5 MB).
+    // pool by memory; here 256 slots of n x n + 5 n doubles, at most 8.8 MB).
     uint32_t nmax_small = 0;
     for (auto& g : h->groups)
         if (g.n <= kDensePeelMax) nmax_small = std::max(nmax_small, g.n);
     if (nmax_small) {
         h->pool.n_slots = 256;
-        h->pool.slot_words = nmax_small * nmax_small + nmax_small;
+        h->pool.slot_words = dense_slot_words(nmax_small);
         if (cudaMalloc(&h->pool.scratch, sizeof(double) * h->pool.n_slots * h->pool.slot_words) != cudaSuccess)
             return bail(ESPL_OUT_OF_MEMORY);
         uint32_t* ctr = nullptr;
@@ -698,6 +698,13 @@ espl_status espl_get_period_meas(espl_lanes* h, uint32_t net, double* period, ui
 
 espl_status espl_get_stats(espl_lanes* h, espl_stats* out) {
     if (!h || !out) return ESPL_INVALID_ARGUMENT;
+    if (h->pool.next) {
+        uint32_t ctr[2] = {0, 0};
+        CK(cudaMemcpyAsync(ctr, h->pool.next, sizeof(ctr), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        h->stats.dense_peels = ctr[0];
+        h->stats.peel_overflow = ctr[1];
+    }
     *out = h->stats;
     return ESPL_OK;
 }

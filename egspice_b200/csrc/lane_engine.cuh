@@ -303,8 +303,10 @@ __device__ bool limit_lane(const GroupDev& d, uint32_t l) {
 
 // ---------------------------------------------------------------------------
 // LU replay of the frozen tape, FP64 (Bodies.refactor + wideMultipliers).
-// True when the lane must peel.
-__device__ bool refactor64(const GroupDev& d, uint32_t l) {
+// 0: the replay holds; 1: a pivot failed (dead, non-finite, growth), an L/U
+// entry is non-finite or a void slot filled; 2: only a multiplier past
+// 1 / pivot_tol, which `replay_holds64` may still accept.
+__device__ int refactor64(const GroupDev& d, uint32_t l) {
     const uint32_t P = d.P;
     const double* __restrict__ a = d.a;
     double* __restrict__ w = d.w;
@@ -312,7 +314,7 @@ __device__ bool refactor64(const GroupDev& d, uint32_t l) {
     double* __restrict__ ux = d.ux;
     double* __restrict__ ud = d.udiag;
     for (uint32_t v = 0; v < d.n_void; v++)
-        if (LM(a, d.void_slots[v]) != 0.0) return true;
+        if (LM(a, d.void_slots[v]) != 0.0) return 1;
     bool bad = false;
     uint64_t nonfinite = 0;
     const double growth = 1e-12;
@@ -365,7 +367,7 @@ __device__ bool refactor64(const GroupDev& d, uint32_t l) {
             }
         }
     }
-    if (nonfinite) return true;
+    if (nonfinite || bad) return 1;
     uint64_t worst = 0;
     for (uint32_t k = 0; k < d.n; k++) {
         if (d.flags[k] & 2u) continue;
@@ -374,7 +376,7 @@ __device__ bool refactor64(const GroupDev& d, uint32_t l) {
             worst = worst > b ? worst : b;
         }
     }
-    return bad || !(bitsd(worst) <= kWide);
+    return bitsd(worst) <= kWide ? 0 : 2;
 }
 
 // The same replay in FP32 with FP32 accumulation over the FP64 matrix.
@@ -454,6 +456,86 @@ __device__ void solve64(const GroupDev& d, uint32_t l, const double* __restrict_
     for (uint32_t j = 0; j < d.n; j++) LM(out, d.q[j]) = LM(y, j);
 }
 
+// x = A^-T b through the FP64 factors (SparseLu.solveT,
+// src/solver/sparse_lu.zig:1326-1361). `y` is the work vector.
+__device__ void solve_t64(const GroupDev& d, uint32_t l, const double* __restrict__ b, double* __restrict__ out) {
+    const uint32_t P = d.P;
+    double* __restrict__ y = d.y;
+    for (uint32_t k = 0; k < d.n; k++) LM(y, k) = LM(b, d.q[k]);
+    for (uint32_t k = 0; k < d.n; k++) {
+        double yk = LM(y, k);
+        for (uint32_t p = d.up[k]; p < d.up[k + 1]; p++) yk -= LM(d.ux, p) * LM(y, d.ui[p]);
+        LM(y, k) = yk / LM(d.udiag, k);
+    }
+    for (uint32_t k = d.n; k-- > 0;) {
+        double yk = LM(y, k);
+        for (uint32_t p = d.lp[k]; p < d.lp[k + 1]; p++) yk -= LM(d.lx, p) * LM(y, d.li[p]);
+        LM(y, k) = yk;
+    }
+    for (uint32_t r = 0; r < d.n; r++) LM(out, r) = LM(y, d.pinv[r]);
+}
+
+// direct.zig replayHolds (:402-447) for a replay whose only failure is a
+// multiplier past 1 / pivot_tol: a probe right-hand side solved both ways
+// must leave a scaled residual within replay_ratio_max / pivot_tol = 3e4.
+// Scratch: rr (residual), corr (solution), x_old (row sums; free until the
+// update that follows the solve).
+__device__ bool replay_holds64(const GroupDev& d, uint32_t l) {
+    const uint32_t P = d.P;
+    const uint32_t n = d.n;
+    double* __restrict__ r = d.rr;
+    double* __restrict__ xs = d.corr;
+    double* __restrict__ rows = d.x_old;
+    for (uint32_t i = 0; i < n; i++) LM(rows, i) = 0.0;
+    double norm_1 = 0.0;
+    for (uint32_t j = 0; j < n; j++) {
+        double col = 0.0;
+        for (uint32_t p = d.col_ptr[j]; p < d.col_ptr[j + 1]; p++) {
+            double av = fabs(LM(d.a, p));
+            LM(rows, d.row_idx[p]) += av;
+            col += av;
+        }
+        norm_1 = fmax(norm_1, col);
+    }
+    uint64_t nb = 0;
+    for (uint32_t i = 0; i < n; i++) {
+        uint64_t b = dbits(fabs(LM(rows, i)));
+        nb = nb > b ? nb : b;
+    }
+    double norm_inf = bitsd(nb);
+    double den = (double)((n > 2 ? n : 2) - 1);
+    for (int transpose = 0; transpose <= 1; transpose++) {
+        // solve64 returns -A^-1 b, so it gets the negated probe.
+        for (uint32_t i = 0; i < n; i++) {
+            double mag = 1.0 + (double)i / den;
+            LM(r, i) = (i % 2 == 0) ? mag : -mag;
+        }
+        if (transpose) {
+            solve_t64(d, l, r, xs);
+        } else {
+            for (uint32_t i = 0; i < n; i++) LM(r, i) = -LM(r, i);
+            solve64(d, l, r, xs);
+            for (uint32_t i = 0; i < n; i++) LM(r, i) = -LM(r, i);
+        }
+        for (uint32_t j = 0; j < n; j++)
+            for (uint32_t p = d.col_ptr[j]; p < d.col_ptr[j + 1]; p++) {
+                uint32_t i = d.row_idx[p];
+                if (transpose) LM(r, j) -= LM(d.a, p) * LM(xs, i);
+                else LM(r, i) -= LM(d.a, p) * LM(xs, j);
+            }
+        uint64_t rm = 0, xm = 0;
+        for (uint32_t i = 0; i < n; i++) {
+            uint64_t b1 = dbits(fabs(LM(r, i))), b2 = dbits(fabs(LM(xs, i)));
+            rm = rm > b1 ? rm : b1;
+            xm = xm > b2 ? xm : b2;
+        }
+        double a_norm = transpose ? norm_1 : norm_inf;
+        double ratio = bitsd(rm) / (a_norm * bitsd(xm) * (double)n * 2.220446049250313e-16);
+        if (!(ratio <= 30.0 / 1e-3)) return false;
+    }
+    return true;
+}
+
 // The same through the FP32 factors; the right-hand side is rounded to
 // FP32 and the result widened back.
 __device__ void solve32(const GroupDev& d, uint32_t l, const double* __restrict__ rhs, double* __restrict__ out) {
@@ -493,43 +575,86 @@ __device__ void refine_mixed(const GroupDev& d, uint32_t l) {
     for (uint32_t i = 0; i < d.n; i++) LM(d.dx, i) += LM(corr, i);
 }
 
-// x = -A^-1 b by dense LU with partial pivoting for a failed lane of n <= 64
-// (denseSolveNeg, kernels/lane.zig:310-350). m: n x n row-major scratch,
-// xv: n scratch holding b. False when a pivot is tiny or not finite.
-__device__ bool dense_solve_neg(uint32_t n, double* m, double* xv) {
-    const double tiny = 2.220446049250313e-16 * 2.220446049250313e-16;
-    for (uint32_t i = 0; i < n; i++) xv[i] = -xv[i];
+// x = -A^-1 b for a lane whose replayed pivots failed, by a dense
+// re-pivoting factor that takes the decisions of the host's full factor
+// (SparseLu.factorPass, src/solver/sparse_lu.zig:505-581) in the tape's
+// column order: per step the diagonal (or the row a hand-off gave the
+// column) while |d| >= pivot_tol * column max, else the same test under row
+// scaling, else the column max; the row a column loses goes to the column
+// that wanted the taken row. No absolute pivot floor: only a zero or
+// non-finite column fails, as there. The reference's device peel is a
+// plain partial-pivoting LU with an eps^2 floor (kernels/lane.zig:310-350)
+// that refuses the ill-conditioned iterates a cold operating point passes
+// through; the host factor accepts them.
+// Slot layout (doubles): m[n*n] row-major, xv[n] (the right-hand side,
+// then the solution by unknown), rscale[n], sol[n], then four u32 arrays of
+// n (want, want_of, pinv, row_of) in the last 2n doubles.
+constexpr uint32_t dense_slot_words(uint32_t n) { return n * n + 5 * n; }
+
+__device__ bool dense_repivot_neg(uint32_t n, const uint32_t* q, double* m, double* xv) {
+    double* rscale = xv + n;
+    double* sol = rscale + n;
+    uint32_t* want = reinterpret_cast<uint32_t*>(sol + n);
+    uint32_t* want_of = want + n;
+    uint32_t* pinv = want_of + n;
+    uint32_t* row_of = pinv + n;
+    const double tol = 1e-3;
+    const double big = 1.7976931348623157e308;
+    const uint32_t none = 0xFFFFFFFFu;
+    for (uint32_t r = 0; r < n; r++) {
+        double mx = 0.0;
+        for (uint32_t c = 0; c < n; c++) mx = fmax(mx, fabs(m[r * n + c]));
+        rscale[r] = (mx > 0.0 && mx <= big) ? 1.0 / mx : 1.0;
+        want[r] = r;
+        want_of[r] = r;
+        pinv[r] = none;
+        xv[r] = -xv[r];
+    }
     for (uint32_t k = 0; k < n; k++) {
-        uint32_t mr = k;
-        double mv = fabs(m[k * n + k]);
-        for (uint32_t i = k + 1; i < n; i++) {
-            double v = fabs(m[i * n + k]);
-            if (v > mv) { mv = v; mr = i; }
+        uint32_t c = q[k];
+        double amax = 0.0, smax = 0.0;
+        uint32_t piv = none;
+        for (uint32_t r = 0; r < n; r++) {
+            if (pinv[r] != none) continue;
+            double av = fabs(m[r * n + c]);
+            if (av > amax) { amax = av; piv = r; }
+            smax = fmax(smax, av * rscale[r]);
         }
-        double p = m[mr * n + k];
-        if (!(fabs(p) >= tiny && fabs(p) <= 1.7976931348623157e308)) return false;
-        if (mr != k) {
-            for (uint32_t j = 0; j < n; j++) {
-                double t = m[k * n + j];
-                m[k * n + j] = m[mr * n + j];
-                m[mr * n + j] = t;
+        if (piv == none || amax == 0.0 || !(amax <= big)) return false;
+        uint32_t pr = want[c];
+        if (pinv[pr] == none) {
+            double dmag = fabs(m[pr * n + c]);
+            if (dmag > 0.0 && (dmag >= tol * amax || dmag * rscale[pr] >= tol * smax)) piv = pr;
+        }
+        if (piv != pr) {
+            uint32_t c2 = want_of[piv];
+            want[c2] = pr;
+            want_of[pr] = c2;
+        }
+        pinv[piv] = k;
+        row_of[k] = piv;
+        double d = m[piv * n + c];
+        for (uint32_t r = 0; r < n; r++) {
+            if (pinv[r] != none) continue;
+            double f = m[r * n + c] / d;
+            if (f == 0.0) continue;
+            for (uint32_t kk = k + 1; kk < n; kk++) {
+                uint32_t cc = q[kk];
+                m[r * n + cc] -= f * m[piv * n + cc];
             }
-            double t = xv[k];
-            xv[k] = xv[mr];
-            xv[mr] = t;
-        }
-        double inv = 1.0 / m[k * n + k];
-        for (uint32_t i = k + 1; i < n; i++) {
-            double f = m[i * n + k] * inv;
-            for (uint32_t j = k + 1; j < n; j++) m[i * n + j] -= f * m[k * n + j];
-            xv[i] -= f * xv[k];
+            xv[r] -= f * xv[piv];
         }
     }
-    for (uint32_t ki = n; ki-- > 0;) {
-        double s = 0.0;
-        for (uint32_t j = ki + 1; j < n; j++) s += m[ki * n + j] * xv[j];
-        xv[ki] = (xv[ki] - s) / m[ki * n + ki];
+    // Back substitution: unknown q[k] from the row pivoted at step k.
+    for (uint32_t k = n; k-- > 0;) {
+        uint32_t r = row_of[k];
+        double acc = xv[r];
+        for (uint32_t kk = k + 1; kk < n; kk++) acc -= m[r * n + q[kk]] * sol[q[kk]];
+        double v = acc / m[r * n + q[k]];
+        if (!(fabs(v) <= big)) return false;
+        sol[q[k]] = v;
     }
+    for (uint32_t i = 0; i < n; i++) xv[i] = sol[i];
     return true;
 }
 

@@ -56,8 +56,9 @@ __device__ bool residual_ok(const GroupDev& d, uint32_t l, const NewtonParams& o
 }
 
 // A failed replay of a lane with n <= 64 solves densely in a pool slot
-// (arp_lane_peel_dense, lane_device.zig:120-147). False when the pool is
-// spent or the dense LU fails.
+// (the place of arp_lane_peel_dense, lane_device.zig:120-147), re-pivoting
+// as the host factor would. False when the pool is spent or the factor
+// fails.
 __device__ bool peel_dense(const GroupDev& d, uint32_t l, LaneState& s, const PeelPool& pool) {
     const uint32_t P = d.P;
     if (d.n > kDensePeelMax || pool.scratch == nullptr) return false;
@@ -76,7 +77,7 @@ __device__ bool peel_dense(const GroupDev& d, uint32_t l, LaneState& s, const Pe
     for (uint32_t c = 0; c < n; c++)
         for (uint32_t p = d.col_ptr[c]; p < d.col_ptr[c + 1]; p++) m[d.row_idx[p] * n + c] += LM(d.a, p);
     for (uint32_t i = 0; i < n; i++) xv[i] = LM(d.rhs, i);
-    if (!dense_solve_neg(n, m, xv)) return false;
+    if (!dense_repivot_neg(n, d.q, m, xv)) return false;
     for (uint32_t i = 0; i < n; i++) LM(d.dx, i) = xv[i];
     return true;
 }
@@ -109,16 +110,16 @@ __device__ void newton_lane(const GroupDev& d, uint32_t l, LaneState& s, const N
         if (it == 0) limit = plausible_limit(d, l);
         bool fail;
         bool use32 = MIXED && !s.fp64;
+        if (use32 && refactor32(d, l)) {
+            s.fp64 = 1;
+            s.fallbacks++;
+            use32 = false;
+        }
         if (use32) {
-            fail = refactor32(d, l);
-            if (fail) {
-                s.fp64 = 1;
-                s.fallbacks++;
-                use32 = false;
-                fail = refactor64(d, l);
-            }
+            fail = false;
         } else {
-            fail = refactor64(d, l);
+            int rc = refactor64(d, l);
+            fail = rc == 1 || (rc == 2 && !replay_holds64(d, l));
         }
         if (fail) {
             if (!peel_dense(d, l, s, pool)) {
@@ -175,6 +176,7 @@ __global__ void __launch_bounds__(128) k_static(LaunchMap m, NewtonParams o, Lan
     uint32_t l;
     if (!lane_of(m, d, l)) return;
     LaneState& s = st[d->lane0 + l];
+    s.peel_slot = 0xFFFFFFFFu;  // the pool's counter restarts every solve
     Companion cp{0, 0, 0.0, 0.0};
     newton_lane<MIXED>(*d, l, s, o, tran, 0.0, cp, pool);
 }
@@ -363,6 +365,7 @@ __global__ void __launch_bounds__(128) k_tran(LaunchMap m, TranParams o, NewtonP
     const GroupDev& d = *dp;
     const uint32_t P = d.P;
     LaneState& s = st[d.lane0 + l];
+    s.peel_slot = 0xFFFFFFFFu;  // the pool's counter restarts every launch
     const uint32_t ns = d.n_sites;
     for (uint32_t attempt = 0; attempt < o.launch_steps; attempt++) {
         if (s.status != 0) break;

@@ -27,6 +27,7 @@
 #include <stdatomic.h>
 #include <stdlib.h>
 #include <string.h>
+#include <stdio.h>
 
 #define X_PLAUSIBLE 1e9
 
@@ -479,7 +480,10 @@ static orc_newton_result newton(ockt *k, double *x, const espl_newton_opts *o, i
             for (uint32_t i = 0; i < k->n; i++) k->rhs[i] += o->gmin * x[i];
         }
         if (iter == 0) limit = plausible_limit(k, x, k->rhs, v);
-        if (orc_direct_factor(k->slv, v, NULL) != 0) {
+        int path = -1;
+        int frc = orc_direct_factor(k->slv, v, &path);
+        if (getenv("ORC_DEBUG")) fprintf(stderr, "iter %u factor rc %d path %d\n", iter, frc, path);
+        if (frc != 0) {
             r.singular = 1;
             r.iterations = iter;
             if (fail_factor) (*fail_factor)++;

@@ -1,0 +1,102 @@
+"""GPU lanes through the C ABI against the CPU FP64 oracle on the same
+seeded decks. Tolerance: |x - x_ref| <= 1e-6 |x_ref| + 1e-9 (V or A), the
+bar of the reference's GPU-vs-CPU lane test (src/tests/espice.zig:3387)."""
+import numpy as np
+import pytest
+
+from egspice_b200 import abi, decks
+from egspice_b200.lanes import Lanes
+
+pytestmark = pytest.mark.gpu
+
+RTOL, ATOL = 1e-6, 1e-9
+
+
+def worst(x, xr):
+    return float((np.abs(x - xr) / (RTOL * np.abs(xr) + ATOL)).max())
+
+
+def opamp_start(net):
+    x0 = np.zeros((net.lanes, net.n))
+    for k, v in dict(vdd=1.8, inp=0.9, vb=0.58, n1=1.2, out=0.9, tail=0.25, n2=1.2).items():
+        x0[:, net.node(k)] = v
+    return x0
+
+
+def test_tape_bit_exact_with_oracle(oracle):
+    net = decks.inverter_chain(32)
+    with Lanes([net]) as L:
+        t = L.tape(0)
+    q = oracle.order(net.col_ptr, net.row_idx)
+    assert np.array_equal(t["q"], q)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_inverter_chain_cold_operating_points(oracle, precision):
+    net = decks.inverter_chain(256)
+    opts = abi.newton_opts()
+    xo, ro = oracle.op_lanes(net, opts, threads=8)
+    with Lanes([net], precision=precision) as L:
+        r = L.solve_static(opts)
+        x = L.get_x(0)
+    ok = (r[:, 0] & abi.CONVERGED) != 0
+    assert ok.mean() >= 0.95, f"converged {ok.sum()} of {len(ok)}"
+    both = ok & (ro[:, 0] == 1)
+    assert worst(x[both], xo[both]) <= 1.0
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_opamp_warm_operating_points(oracle, precision):
+    net = decks.miller_opamp(512)
+    x0 = opamp_start(net)
+    opts = abi.newton_opts(init_fix=0)
+    xo, ro = oracle.op_lanes(net, opts, x_in=x0, threads=8)
+    with Lanes([net], precision=precision) as L:
+        L.put_x(0, x0, False)
+        r = L.solve_static(opts)
+        x = L.get_x(0)
+    assert ((r[:, 0] & abi.CONVERGED) != 0).all()
+    assert worst(x, xo) <= 1.0
+    if precision == "fp64":
+        assert np.array_equal(r[:, 1], ro[:, 2])
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_uneven_ladders_one_launch(oracle, precision):
+    nets = [decks.rc_diode_ladder(n, 40, seed=s) for n, s in ((200, 1), (517, 2), (1203, 3))]
+    topts = abi.tran_opts(t_stop=2e-9, dt=10e-12, fixed_step=1, method=1, max_iter=50)
+    with Lanes(nets, precision=precision, dt0=10e-12) as L:
+        reps = L.run_tran(topts, steps_per_launch=64)
+        xs = [L.get_x(i) for i in range(len(nets))]
+    assert all(r.status == 1 and r.steps == 200 for r in reps)
+    for nl, x in zip(nets, xs):
+        xo, ro, _, _ = oracle.tran_lanes(nl, topts, threads=8)
+        assert worst(x, xo) <= 1.0, nl.name
+
+
+def test_rc_points_lte_control(oracle):
+    r = np.array([1e3, 2e3, 5e3, 1e4])
+    c = np.array([1e-12, 0.5e-12, 2e-13, 2e-13])
+    net = decks.rc_points(4, r, c, tr=0.2e-9)
+    opts = abi.tran_opts(t_stop=8e-9, dt=1e-12, dt_max=20e-12, method=1, max_iter=20, reltol=1e-4)
+    with Lanes([net]) as L:
+        reps = L.run_tran(opts, steps_per_launch=4096)
+        x = L.get_x(0)
+    xo, ro, _, _ = oracle.tran_lanes(net, opts)
+    for a, b in zip(reps, ro):
+        assert a.status == 1 and a.steps == b.steps and a.rejects == b.rejects
+    assert worst(x, xo) <= 1.0
+
+
+def test_ring_oscillator_period(oracle):
+    net = decks.ring_oscillator(16, stages=15)
+    out = net.node("s3")
+    opts = abi.tran_opts(t_stop=3e-9, dt=1e-12, dt_max=5e-12, method=1, max_iter=20)
+    with Lanes([net]) as L:
+        L.set_period_meas(0, out, 0.9, 0.5e-9)
+        reps = L.run_tran(opts, steps_per_launch=2048)
+        per, cr = L.period_meas(0)
+    _, ro, _, po = oracle.tran_lanes(net, opts, meas=(out, 0.9, 0.5e-9), threads=8)
+    assert all(r.status == 1 for r in reps)
+    assert np.all(cr >= 3)
+    assert np.all(np.abs(per - po) <= 1e-3 * np.abs(po)), (per, po)

@@ -1,0 +1,88 @@
+"""The oracle's analyses against analytic answers: the RC points of the C
+API tests (src/tests/c_api.zig:795-821: tpd = RC ln(2RC/T (e^{T/RC} - 1)) -
+T/2 for a ramp of rise T), and the operating points of the configuration
+decks (physical sanity, per-point independence)."""
+import math
+
+import numpy as np
+
+from egspice_b200 import abi, decks
+
+
+def crossing(rows, times, level):
+    for k in range(1, len(rows)):
+        if rows[k - 1] < level <= rows[k]:
+            return times[k - 1] + (level - rows[k - 1]) * (times[k] - times[k - 1]) / (rows[k] - rows[k - 1])
+    return float("nan")
+
+
+def rc_tpd(r, c, tr):
+    rc = r * c
+    return rc * math.log(2 * rc / tr * (math.exp(tr / rc) - 1)) - tr / 2
+
+
+def test_rc_points_analytic_delay(oracle):
+    r = np.array([1e3, 2e3, 5e3, 1e4])
+    c = np.array([1e-12, 0.5e-12, 2e-13, 2e-13])
+    tr = 0.2e-9
+    net = decks.rc_points(len(r), r, c, tr=tr)
+    out = net.node("out")
+    inp = net.node("in")
+    opts = abi.tran_opts(t_stop=8e-9, dt=1e-12, dt_max=20e-12, method=1, max_iter=20, reltol=1e-4)
+    x, reps, rows, _ = oracle.tran_lanes(net, opts, probes=[inp, out], max_rows=20000)
+    for l in range(len(r)):
+        assert reps[l].status == 1
+        n = reps[l].steps
+        # rebuild times: the probe rows carry no time, so run a time probe
+        assert n > 10
+    # delays from rows need times: use the input ramp itself as a clock
+    for l in range(len(r)):
+        rin = rows[l, :, 0]
+        rout = rows[l, :, 1]
+        m = ~np.isnan(rin)
+        rin, rout = rin[m], rout[m]
+        # input ramp: v_in = t / tr during the ramp, so t = v_in * tr there;
+        # after it the step sequence is recovered by the output's exact
+        # response: compare at the output's 50 % crossing via interpolation
+        # against the analytic waveform instead.
+        rc = r[l] * c[l]
+        # analytic output after the ramp: v(t) = 1 - (rc/tr)(e^{tr/rc} - 1) e^{-t/rc}
+        k = np.argmax(rout >= 0.5)
+        assert k > 0
+        v_hi, v_lo = rout[k], rout[k - 1]
+        t_hi = -rc * math.log((1 - v_hi) / ((rc / tr) * (math.exp(tr / rc) - 1)))
+        t_lo = -rc * math.log((1 - v_lo) / ((rc / tr) * (math.exp(tr / rc) - 1)))
+        t50 = t_lo + (0.5 - v_lo) * (t_hi - t_lo) / (v_hi - v_lo)
+        assert abs((t50 - tr / 2) - rc_tpd(r[l], c[l], tr)) <= 0.002 * rc_tpd(r[l], c[l], tr)
+
+
+def test_inverter_chain_operating_point(oracle):
+    net = decks.inverter_chain(16)
+    x, res = oracle.op_lanes(net, abi.newton_opts(), threads=4)
+    assert res[:, 0].all() and not res[:, 1].any()
+    s = [net.node(f"s{k}") for k in range(1, 17)]
+    out = x[:, s]
+    # after the first stages the chain sits at the rails, alternating
+    for k in range(4, 16):
+        hi = out[:, k] > 1.7
+        lo = out[:, k] < 0.1
+        assert np.all(hi | lo)
+        assert np.all(hi != (out[:, k - 1] > 1.7))
+
+
+def test_opamp_operating_point_warm(oracle):
+    net = decks.miller_opamp(32)
+    x0 = np.zeros((32, net.n))
+    for k, v in dict(vdd=1.8, inp=0.9, vb=0.58, n1=1.2, out=0.9, tail=0.25, n2=1.2).items():
+        x0[:, net.node(k)] = v
+    x, res = oracle.op_lanes(net, abi.newton_opts(init_fix=0), x_in=x0)
+    assert res[:, 0].all()
+    assert np.all(np.abs(x[:, net.node("out")] - 0.9) < 0.15)
+
+
+def test_ladder_fixed_step_transient(oracle):
+    net = decks.rc_diode_ladder(60, 3, seed=3)
+    opts = abi.tran_opts(t_stop=1e-9, dt=10e-12, fixed_step=1, method=1, max_iter=50)
+    x, reps, _, _ = oracle.tran_lanes(net, opts)
+    assert all(r.status == 1 and r.steps == 100 for r in reps)
+    assert np.all(x[:, net.node("n1")] > 0.05)
