@@ -1,0 +1,409 @@
+"""Benchmark of the lane-sweep hot path: sweep points per second on B200.
+
+Workload: 16,384 Monte-Carlo lanes of a 31-stage MOS1 ring oscillator plus
+32 seeded variants of 15-63 stages (32 lanes each, different patterns in the
+same launches), trapezoidal transient with LTE step control, 5,000 accepted
+steps per lane, and the oscillation period measured on the device. A "step"
+of the benchmark is one complete sweep of all 17,408 points. The metric is
+points/s of the mixed-precision lanes (FP32 LU and solves; FP64 device
+evaluation, residual, refinement and step control) next to the plain FP64
+lanes of the same build; a sample of lanes is checked against the FP64
+oracle (period and final state).
+
+Launch: `python bench.py --gpus N --steps K --warmup W`; for N > 1 one rank
+per GPU under torch.distributed.run (each rank runs its own seeded sweep:
+weak scaling, no data-path collective). `--impl reference` times the CPU
+FP64 restatement of the reference's CPU path on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "sweep points/s on 1 B200: learned+mixed vs plain FP64 lanes at 1e-6 rel err"
+RTOL, ATOL = 1e-6, 1e-9
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled during the timed region."""
+
+    def __init__(self, device: int):
+        self.device = device
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.samples.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+# ----------------------------------------------------------------------------
+# workloads
+
+def ladder_workload(seed: int):
+    from egspice_b200 import abi, decks
+    nets = decks.rc_diode_batch(n_nets=64, lanes_per_net=64, seed=seed)
+    topts = abi.tran_opts(t_stop=2000 * 10e-12, dt=10e-12, fixed_step=1, method=1, max_iter=50, predictor=1)
+    return nets, topts
+
+
+def ring_workload(seed: int, lanes: int = 16384, variants: int = 32, lanes_per_variant: int = 32):
+    """16,384 Monte-Carlo lanes of a 31-stage MOS1 ring oscillator (20 fF per
+    stage, chain-like variation) plus 32 seeded variants of 15-63 stages
+    (odd), 32 lanes each; trapezoidal transient with LTE step control, 5,000
+    accepted steps per lane; the oscillation period measured on stage 1."""
+    from egspice_b200 import abi, decks
+    rng = np.random.default_rng(seed)
+    nets = [decks.ring_oscillator(lanes, stages=31, base_seed=11 + 1000 * seed)]
+    for v in range(variants):
+        st = int(rng.integers(7, 32)) * 2 + 1
+        nets.append(decks.ring_oscillator(lanes_per_variant, stages=st, base_seed=5000 + 97 * v + 1000 * seed))
+    topts = abi.tran_opts(t_stop=1e-6, dt=2e-12, dt_max=10e-12, method=1, max_iter=20, max_steps=5000,
+                          predictor=1)
+    return nets, topts
+
+
+def algorithmic_bytes(nets, lane_iterations_per_net, s_lu: int):
+    """SURVEY 8(d) bytes per lane-iteration, summed: refactor 8 nnz +
+    s (nnzL + nnzU + n); solve s (nnzL + nnzU + n) + 16 n; update/gates 40 n;
+    assembly 8 (nnz + n) + 16 nnz. Index words are shared by a template's
+    lanes and excluded."""
+    total = 0.0
+    for (net, nl, nu), it in zip(nets, lane_iterations_per_net):
+        n, nnz = net.n, net.nnz
+        per = (8 * nnz + s_lu * (nl + nu + n)) + (s_lu * (nl + nu + n) + 16 * n) + 40 * n + \
+              (8 * (nnz + n) + 16 * nnz)
+        total += per * it
+    return total
+
+
+def run_sweep(nets, topts, precision, steps_per_launch=2000):
+    """One full sweep through the C ABI from host buffers: create (uploads
+    every lane's parameters), operating point, all transient steps, final
+    states back. Returns (device_ms, wall_s, x_final list, reports, tapes,
+    stats)."""
+    from egspice_b200.lanes import Lanes
+    t0 = time.perf_counter()
+    L = Lanes(nets, precision=precision, dt0=topts.dt)
+    L.init_steps(topts)
+    dev_ms = L.stats().newton_ms
+    reps = None
+    launches = 0
+    while True:
+        reps = L.device_launch(steps_per_launch)
+        launches += 1
+        dev_ms += L.stats().newton_ms
+        if all(r.status != 0 for r in reps) or launches > 1000:
+            break
+    xs = [L.get_x(i) for i in range(len(nets))]
+    wall = time.perf_counter() - t0
+    tapes = []
+    for i, net in enumerate(nets):
+        t = L.tape(i)
+        tapes.append((net, len(t["li"]), len(t["ui"])))
+    st = L.stats()
+    L.close()
+    return dev_ms, wall, xs, reps, tapes, st, launches
+
+
+def oracle_check(nets, topts, xs, lanes_per_net=1, threads=None):
+    from oracle import pyoracle as po
+    threads = threads or os.cpu_count()
+    worst = 0.0
+    t0 = time.perf_counter()
+    points = 0
+    for net, x in zip(nets, xs):
+        xo, _, _, _ = po.tran_lanes(net, topts, lane0=0, count=lanes_per_net, threads=threads)
+        worst = max(worst, float((np.abs(x[:lanes_per_net] - xo) / (RTOL * np.abs(xo) + ATOL)).max()))
+        points += lanes_per_net
+    return worst, points, time.perf_counter() - t0
+
+
+def cpu_reference(nets, topts, budget_s: float, threads: int):
+    """The oracle (CPU FP64 restatement of the reference's CPU path) on a
+    bounded sample: the first lane of as many templates as fit the budget,
+    smallest templates excluded so the sample keeps the size mix."""
+    from oracle import pyoracle as po
+    order = list(range(len(nets)))
+    t0 = time.perf_counter()
+    points = 0
+    nodes = 0
+    k = 0
+    # templates in a fixed interleaved order so the sample spans the sizes
+    order = order[::2] + order[1::2]
+    batch = max(1, threads)
+    while k < len(order) and time.perf_counter() - t0 < budget_s:
+        sel = order[k:k + batch]
+        jobs = []
+        for i in sel:
+            th = threading.Thread(target=lambda i=i: po.tran_lanes(nets[i], topts, lane0=0, count=1, threads=1))
+            th.start()
+            jobs.append(th)
+        for th in jobs:
+            th.join()
+        points += len(sel)
+        nodes += sum(nets[i].n for i in sel)
+        k += batch
+    wall = time.perf_counter() - t0
+    return points / wall, points, wall, nodes
+
+
+def ring_check(nets, topts, xs, per_gpu, lanes_per_net=2, threads=None):
+    """Worst error of the GPU lanes against the FP64 oracle on a sample:
+    the oscillation period (.meas) and the final state."""
+    from oracle import pyoracle as po
+    threads = threads or os.cpu_count()
+    worst_p, worst_x = 0.0, 0.0
+    for k, (net, x) in enumerate(zip(nets, xs)):
+        row = net.node("s1")
+        xo, _, _, po_per = po.tran_lanes(net, topts, lane0=0, count=lanes_per_net, meas=(row, 0.9, 1e-9),
+                                         threads=threads)
+        pg = per_gpu[k][:lanes_per_net]
+        ok = np.isfinite(po_per) & np.isfinite(pg)
+        if ok.any():
+            worst_p = max(worst_p, float((np.abs(pg[ok] - po_per[ok]) / (RTOL * np.abs(po_per[ok]))).max()))
+        worst_x = max(worst_x, float((np.abs(x[:lanes_per_net] - xo) / (RTOL * np.abs(xo) + ATOL)).max()))
+    return worst_p, worst_x
+
+
+def run_ring_sweep(nets, topts, precision, steps_per_launch=5000):
+    from egspice_b200.lanes import Lanes
+    t0 = time.perf_counter()
+    L = Lanes(nets, precision=precision, dt0=topts.dt)
+    for i, net in enumerate(nets):
+        L.set_period_meas(i, net.node("s1"), 0.9, 1e-9)
+    L.init_steps(topts)
+    dev_ms = L.stats().newton_ms
+    launches = 0
+    while True:
+        reps = L.device_launch(steps_per_launch)
+        launches += 1
+        dev_ms += L.stats().newton_ms
+        if all(r.status != 0 for r in reps) or launches > 1000:
+            break
+    periods = [L.period_meas(i)[0] for i in range(len(nets))]
+    xs = [L.get_x(i) for i in range(len(nets))]
+    wall = time.perf_counter() - t0
+    tapes = []
+    for i, net in enumerate(nets):
+        t = L.tape(i)
+        tapes.append((net, len(t["li"]), len(t["ui"])))
+    L.close()
+    return dev_ms, wall, xs, reps, tapes, launches, periods
+
+
+def cpu_ring_reference(nets, topts, budget_s: float, threads: int):
+    """The oracle on a bounded sample of the ring workload: lanes of the
+    31-stage template (the workload's bulk), `threads` at a time, until the
+    budget is spent."""
+    from oracle import pyoracle as po
+    t0 = time.perf_counter()
+    points = 0
+    lane = 0
+    while time.perf_counter() - t0 < budget_s and lane < nets[0].lanes:
+        po.tran_lanes(nets[0], topts, lane0=lane, count=threads, threads=threads)
+        lane += threads
+        points += threads
+    wall = time.perf_counter() - t0
+    return points / wall, points, wall
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist_mod
+        dist = dist_mod
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    nets, topts = ring_workload(seed=rank)
+    n_points = sum(n.lanes for n in nets)
+    config = {"workload": "ring_oscillator_mc_uneven", "templates": len(nets), "lanes": n_points,
+              "stages": "31 (16,384 lanes) + 32 variants of 15-63 (32 lanes each)", "steps_per_lane": 5000,
+              "method": "trap, LTE step control", "predictor": "linear (SPICE xfact)",
+              "meas": "oscillation period of stage 1 (rising 0.9 V)",
+              "l2": "inputs larger than L2 (per-sweep working set > 126 MB)", "parallelism": f"lanes x{world} GPUs"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        threads = os.cpu_count() or 1
+        vals = []
+        pts_total = 0
+        for _ in range(max(1, args.steps)):
+            v, pts, wall = cpu_ring_reference(nets, topts, args.cpu_budget / max(1, args.steps), threads)
+            vals.append(v)
+            pts_total += pts
+        v = statistics.median(vals)
+        line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "points/s", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * n_points / v,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded MC ring oscillators)", "config": config,
+                "cpu_baseline": {"value": v, "unit": "points/s", "cores": threads, "kind": "port",
+                                 "sample": f"{pts_total} lanes of the 31-stage template, 5,000 steps each, "
+                                           f"{threads} threads"},
+                "e2e": {"value": v, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    import torch
+    dev = local if world > 1 else 0
+    torch.cuda.set_device(dev)
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    results = {}
+    for prec in ("fp64", "mixed"):
+        for _ in range(args.warmup):
+            run_ring_sweep(nets, topts, prec)
+        dev_ms, walls = [], []
+        barrier()
+        with ClockSampler(dev) as clk:
+            for _ in range(args.steps):
+                barrier()
+                d, w, xs, reps, tapes, launches, periods = run_ring_sweep(nets, topts, prec)
+                barrier()
+                dev_ms.append(d)
+                walls.append(w)
+        dmax = max(dev_ms) / 1000.0
+        wmax = max(walls)
+        if dist:
+            t = torch.tensor([dmax, wmax], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            dmax, wmax = float(t[0]), float(t[1])
+        results[prec] = dict(dev_s=dmax, wall_s=wmax, xs=xs, reps=reps, tapes=tapes, clocks=clk.summary(),
+                             iters=sum(r.nr_iters for r in reps), rejects=sum(r.rejects for r in reps),
+                             launches=launches, periods=periods)
+
+    best, plain = results["mixed"], results["fp64"]
+    points_all = n_points * world
+    value = points_all / best["dev_s"]
+    e2e = points_all / best["wall_s"]
+    err = {}
+    if rank == 0:
+        sample = [0] + list(range(1, len(nets), 8))
+        for prec in ("mixed", "fp64"):
+            r = results[prec]
+            err[prec] = ring_check([nets[i] for i in sample], topts, [r["xs"][i] for i in sample],
+                                   [r["periods"][i] for i in sample])
+    per_net_iters = []
+    off = 0
+    for net in nets:
+        per_net_iters.append(sum(r.nr_iters for r in best["reps"][off:off + net.lanes]))
+        off += net.lanes
+    bytes_alg = algorithmic_bytes(best["tapes"], per_net_iters, 4)
+    hbm, kind = peaks()
+    achieved = bytes_alg / best["dev_s"] / 1e9
+    h2d = sum(sum(b.param.nbytes + b.term.nbytes for b in n.batches) + n.col_ptr.nbytes + n.row_idx.nbytes
+              for n in nets)
+    d2h = sum(n.lanes * n.n * 8 + n.lanes * 8 for n in nets)
+    line = {
+        "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": best["dev_s"] * 1000.0, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64 (eval, residual, step control); f32 LU in mixed",
+        "data": "synthetic (seeded Monte-Carlo MOS1 ring oscillators)", "config": config,
+        "modes": {
+            "mixed": {"points_per_s": value, "ms_per_sweep": best["dev_s"] * 1e3, "newton_iters": best["iters"],
+                      "rejects": best["rejects"], "period_err_over_tol": err.get("mixed", (None,))[0],
+                      "final_x_err_over_tol": err.get("mixed", (None, None))[1]},
+            "fp64": {"points_per_s": points_all / plain["dev_s"], "ms_per_sweep": plain["dev_s"] * 1e3,
+                     "newton_iters": plain["iters"], "rejects": plain["rejects"],
+                     "period_err_over_tol": err.get("fp64", (None,))[0],
+                     "final_x_err_over_tol": err.get("fp64", (None, None))[1]},
+            "mixed_over_fp64": plain["dev_s"] / best["dev_s"],
+            "learned": False,
+        },
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "peak_kind": kind, "traffic": None,
+                     "kernel": "k_tran<true>: per-tile eval + gather + shared-memory FP32 LU + gates, fused"},
+        "e2e": {"value": e2e, "unit": "points/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": int(best["launches"]) + 11,
+        "clocks": best["clocks"],
+    }
+    if rank == 0 and not args.no_cpu_baseline and world == 1:
+        threads = os.cpu_count() or 1
+        v, pts, wall = cpu_ring_reference(nets, topts, args.cpu_budget, threads)
+        line["cpu_baseline"] = {"value": v, "unit": "points/s", "cores": threads, "kind": "port",
+                                "sample": f"{pts} lanes of the 31-stage template (5,000 steps each) in "
+                                          f"{wall:.1f} s on {threads} threads"}
+    if rank == 0:
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -19,7 +19,10 @@ using namespace espl;
 
 namespace {
 
-constexpr uint32_t kBlock = 128;
+constexpr uint32_t kBlock = kTileThreads;
+// Shared-memory budget per tile for the shared LU chain (two tiles per SM
+// of 228 KB with the static tile state).
+constexpr uint32_t kSmemBudget = 100 * 1024;
 constexpr uint32_t kGround = ESPL_GROUND;
 
 uint32_t terms_of(uint32_t kind) {
@@ -75,12 +78,18 @@ struct Group {
     double* dio_raw = nullptr;
     uint32_t meas_row = 0xFFFFFFFFu;
     double meas_level = 0, meas_t0 = 0;
+    struct BatchRec {
+        uint32_t kind, base, count;
+    };
+    std::vector<BatchRec> batch_order;
+    uint32_t tile0 = 0;
 };
 
 }  // namespace
 
 struct espl_lanes {
     int device = 0;
+    uint32_t smem_bytes = 0;   // dynamic shared memory of the Newton launches
     uint32_t precision = ESPL_FP64;
     std::vector<Group> groups;
     uint32_t n_warps = 0, total_lanes = 0;
@@ -89,7 +98,6 @@ struct espl_lanes {
     LaneState* d_state = nullptr;
     const double** d_mos_raw = nullptr;
     const double** d_dio_raw = nullptr;
-    PeelPool pool{};
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     espl_stats stats{};
@@ -116,11 +124,14 @@ espl_status fail(espl_lanes* h, espl_status code, const std::string& msg) {
         }                                                                                         \
     } while (0)
 
+// Every buffer is padded to a 16-byte multiple (the bulk copies that stage
+// the tape read whole 16-byte units).
 template <typename T>
 espl_status dalloc(espl_lanes* h, std::vector<void*>& own, T** out, size_t count) {
     void* p = nullptr;
-    CK(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)));
-    CK(cudaMemsetAsync(p, 0, std::max<size_t>(count, 1) * sizeof(T), h->stream));
+    size_t bytes = (std::max<size_t>(count, 1) * sizeof(T) + 15) & ~size_t(15);
+    CK(cudaMalloc(&p, bytes));
+    CK(cudaMemsetAsync(p, 0, bytes, h->stream));
     own.push_back(p);
     *out = static_cast<T*>(p);
     return ESPL_OK;
@@ -173,6 +184,7 @@ espl_status build_group(espl_lanes* h, const espl_netlist& net, Group& g) {
         KindHost& kh = g.kinds[sb.kind];
         uint32_t base = kh.count;
         kh.count += sb.count;
+        g.batch_order.push_back({sb.kind, base, sb.count});
         for (uint32_t i = 0; i < sb.count; i++) {
             const uint32_t* tm = sb.term + (size_t)i * nt;
             for (uint32_t t = 0; t < nt; t++) {
@@ -207,6 +219,111 @@ espl_status build_group(espl_lanes* h, const espl_netlist& net, Group& g) {
     return ESPL_OK;
 }
 
+
+// The stamp plan: per-instance cells and, per Jacobian slot and residual /
+// charge row, the list of cells that sum into it, in the order the host
+// stamping of the reference adds them (batches in template order, each
+// device's stamps in its own order, the ground pin last), so every sum is
+// bit-for-bit the host's.
+struct Plan {
+    uint32_t c_res, c_cap, c_vsrc, c_isrc, c_dio, c_mos, c_pin, c_const, n_cells;
+    std::vector<std::vector<uint32_t>> g, c, r, q;
+    std::vector<uint32_t> sites;
+    std::vector<uint8_t> slot_diag;
+};
+
+void csr(const std::vector<std::vector<uint32_t>>& lists, std::vector<uint32_t>& ptr, std::vector<uint32_t>& flat) {
+    ptr.assign(lists.size() + 1, 0);
+    flat.clear();
+    for (size_t k = 0; k < lists.size(); k++) {
+        flat.insert(flat.end(), lists[k].begin(), lists[k].end());
+        ptr[k + 1] = (uint32_t)flat.size();
+    }
+}
+
+Plan build_plan(const Group& g) {
+    Plan pl;
+    uint32_t nr = g.kinds[ESPL_RES].count, nc = g.kinds[ESPL_CAP].count, nv = g.kinds[ESPL_VSRC].count;
+    uint32_t ni = g.kinds[ESPL_ISRC].count, nd = g.kinds[ESPL_DIODE].count, nm = g.kinds[ESPL_MOS1].count;
+    pl.c_res = 0;
+    pl.c_cap = pl.c_res + kResCells * nr;
+    pl.c_vsrc = pl.c_cap + kCapCells * nc;
+    pl.c_isrc = pl.c_vsrc + kVsrcCells * nv;
+    pl.c_dio = pl.c_isrc + kIsrcCells * ni;
+    pl.c_mos = pl.c_dio + kDioCells * nd;
+    pl.c_pin = pl.c_mos + kMosCells * nm;
+    pl.c_const = pl.c_pin + 1;
+    pl.n_cells = pl.c_const + 2;
+    const uint32_t kP = pl.c_const, kM = pl.c_const + 1;
+    pl.g.assign(g.nnz, {});
+    pl.c.assign(g.nnz, {});
+    pl.r.assign(g.n, {});
+    pl.q.assign(g.n, {});
+    auto G = [&](uint32_t slot, uint32_t cell) { if (slot < g.nnz) pl.g[slot].push_back(cell); };
+    auto Cc = [&](uint32_t slot, uint32_t cell) { if (slot < g.nnz) pl.c[slot].push_back(cell); };
+    auto R = [&](uint32_t row, uint32_t cell) { if (row < g.n) pl.r[row].push_back(cell); };
+    auto Q = [&](uint32_t row, uint32_t cell) { if (row < g.n) pl.q[row].push_back(cell); };
+    for (const auto& b : g.batch_order) {
+        const KindHost& kh = g.kinds[b.kind];
+        uint32_t nt = terms_of(b.kind);
+        for (uint32_t k = b.base; k < b.base + b.count; k++) {
+            const uint32_t* tm = kh.term.data() + (size_t)k * nt;
+            const uint32_t* sl = kh.slot.data() + (size_t)k * nt * nt;
+            switch (b.kind) {
+            case ESPL_RES: {
+                uint32_t c = pl.c_res + kResCells * k;
+                R(tm[0], c + 1); G(sl[0], c); G(sl[1], c | kNeg);
+                R(tm[1], (c + 1) | kNeg); G(sl[2], c | kNeg); G(sl[3], c);
+                break;
+            }
+            case ESPL_CAP: {
+                uint32_t c = pl.c_cap + kCapCells * k;
+                Q(tm[0], c + 1); Cc(sl[0], c); Cc(sl[1], c | kNeg);
+                Q(tm[1], (c + 1) | kNeg); Cc(sl[2], c | kNeg); Cc(sl[3], c);
+                pl.sites.push_back(c + 1);
+                break;
+            }
+            case ESPL_VSRC: {
+                uint32_t c = pl.c_vsrc + kVsrcCells * k;
+                R(tm[0], c); G(sl[2], kP);
+                R(tm[1], c | kNeg); G(sl[5], kM);
+                R(tm[2], c + 1); G(sl[6], kP); G(sl[7], kM);
+                break;
+            }
+            case ESPL_ISRC: {
+                uint32_t c = pl.c_isrc + kIsrcCells * k;
+                R(tm[0], c); R(tm[1], c | kNeg);
+                break;
+            }
+            case ESPL_DIODE: {
+                uint32_t c = pl.c_dio + kDioCells * k;
+                R(tm[0], c + 1); G(sl[0], c); G(sl[1], c | kNeg);
+                R(tm[1], (c + 1) | kNeg); G(sl[2], c | kNeg); G(sl[3], c);
+                Q(tm[0], c + 3); Cc(sl[0], c + 2); Cc(sl[1], (c + 2) | kNeg);
+                Q(tm[1], (c + 3) | kNeg); Cc(sl[2], (c + 2) | kNeg); Cc(sl[3], c + 2);
+                pl.sites.push_back(c + 3);
+                break;
+            }
+            case ESPL_MOS1: {
+                uint32_t c = pl.c_mos + kMosCells * k;
+                const uint32_t rows[3] = {0, 2, 3};
+                for (int ri = 0; ri < 3; ri++) {
+                    uint32_t r = rows[ri];
+                    R(tm[r], c + ri);
+                    for (uint32_t cc = 0; cc < 4; cc++) G(sl[r * 4 + cc], c + 3 + 4 * ri + cc);
+                }
+                break;
+            }
+            }
+        }
+    }
+    G(g.diag[0], kP);
+    R(0, pl.c_pin);
+    pl.slot_diag.assign(g.nnz, 0);
+    for (uint32_t i = 0; i < g.n; i++) pl.slot_diag[g.diag[i]] = 1;
+    return pl;
+}
+
 // Allocates the lane-major state of a group; the LU buffers come later.
 espl_status alloc_group(espl_lanes* h, Group& g) {
     GroupDev& d = g.dev;
@@ -232,8 +349,34 @@ espl_status alloc_group(espl_lanes* h, Group& g) {
         if (cjo > 0 || tt > 0) d.has_charge = 1;
     }
     d.meas_row = 0xFFFFFFFFu;
+    d.tile0 = g.tile0;
     auto& own = g.owned;
     espl_status s;
+    {
+        Plan pl = build_plan(g);
+        d.n_cells = pl.n_cells;
+        d.c_res = pl.c_res;
+        d.c_cap = pl.c_cap;
+        d.c_vsrc = pl.c_vsrc;
+        d.c_isrc = pl.c_isrc;
+        d.c_dio = pl.c_dio;
+        d.c_mos = pl.c_mos;
+        d.c_pin = pl.c_pin;
+        d.c_const = pl.c_const;
+        if (pl.sites.size() != d.n_sites) return fail(h, ESPL_INVALID_ARGUMENT, "site count mismatch");
+        std::vector<uint32_t> ptr, flat;
+        csr(pl.g, ptr, flat);
+        if ((s = dupload(h, own, &d.g_ptr, ptr)) || (s = dupload(h, own, &d.g_cell, flat))) return s;
+        csr(pl.c, ptr, flat);
+        if ((s = dupload(h, own, &d.c_ptr, ptr)) || (s = dupload(h, own, &d.c_cell, flat))) return s;
+        csr(pl.r, ptr, flat);
+        if ((s = dupload(h, own, &d.r_ptr, ptr)) || (s = dupload(h, own, &d.r_cell, flat))) return s;
+        csr(pl.q, ptr, flat);
+        if ((s = dupload(h, own, &d.q_ptr, ptr)) || (s = dupload(h, own, &d.q_cell, flat))) return s;
+        if ((s = dupload(h, own, &d.site_cell, pl.sites))) return s;
+        if ((s = dupload(h, own, &d.slot_diag, pl.slot_diag))) return s;
+        if ((s = dalloc(h, own, &d.cells, (size_t)pl.n_cells * P))) return s;
+    }
 #define UP(field, vec) if ((s = dupload(h, own, &d.field, vec))) return s
     UP(col_ptr, g.col_ptr);
     UP(row_idx, g.row_idx);
@@ -280,7 +423,6 @@ espl_status alloc_group(espl_lanes* h, Group& g) {
     AL(y32, n1 * P);
     AL(lim_mos, 3 * (size_t)d.n_mos * P);
     AL(lim_dio, (size_t)d.n_dio * P);
-    AL(qs, (size_t)d.n_sites * P);
     AL(q1, n1 * P);
     AL(ip, n1 * P);
     AL(cur, n1 * P);
@@ -291,12 +433,16 @@ espl_status alloc_group(espl_lanes* h, Group& g) {
     AL(corr, n1 * P);
     AL(udiag, n1 * P);
     AL(udiag32, n1 * P);
+    if (g.n <= kDensePeelMax) {
+        AL(peel_m, (size_t)peel_doubles(g.n) * P);
+        AL(peel_i, (size_t)peel_words(g.n) * P);
+    }
 #undef AL
     return ESPL_OK;
 }
 
-LaunchMap launch_map(espl_lanes* h) { return LaunchMap{h->d_groups, h->d_warp_group, h->n_warps}; }
-uint32_t grid_of(espl_lanes* h) { return (h->n_warps * 32 + kBlock - 1) / kBlock; }
+TileMap launch_map(espl_lanes* h) { return TileMap{h->d_groups, h->d_warp_group, h->n_warps}; }
+uint32_t grid_of(espl_lanes* h) { return h->n_warps; }
 
 espl_status push_descs(espl_lanes* h) {
     std::vector<GroupDev> descs;
@@ -310,7 +456,7 @@ espl_status push_descs(espl_lanes* h) {
 // frozen tape goes to the device.
 espl_status retape(espl_lanes* h, int tran, double dt) {
     auto launch = [&]() {
-        k_assemble<<<grid_of(h), kBlock, 0, h->stream>>>(launch_map(h), tran, 0.0, dt > 0 ? 1.0 / dt : 0.0);
+        k_assemble<<<grid_of(h), kBlock, 0, h->stream>>>(launch_map(h), tran, dt > 0 ? 1.0 / dt : 0.0);
     };
     launch();
     CK(cudaGetLastError());
@@ -349,6 +495,21 @@ espl_status retape(espl_lanes* h, int tran, double dt) {
             if ((s = dalloc(h, own, &d.ux32, (size_t)d.nnz_u * P))) return s;
         }
     }
+    // Templates whose LU chain fits a tile's shared memory run it there; the
+    // launch carries the largest such footprint.
+    uint32_t need = 0;
+    for (auto& g : h->groups) {
+        SmemPlan sp = smem_plan(g.n, g.nnz, g.dev.nnz_l, g.dev.nnz_u, h->precision == ESPL_MIXED);
+        g.dev.smem_ok = sp.bytes <= kSmemBudget ? 1u : 0u;
+        if (g.dev.smem_ok) need = std::max(need, sp.bytes);
+    }
+    h->smem_bytes = need;
+    if (need) {
+        CK(cudaFuncSetAttribute(k_static<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
+        CK(cudaFuncSetAttribute(k_static<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
+        CK(cudaFuncSetAttribute(k_tran<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
+        CK(cudaFuncSetAttribute(k_tran<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
+    }
     return push_descs(h);
 }
 
@@ -368,10 +529,11 @@ NewtonParams newton_params(const espl_newton_opts& o, uint32_t precision) {
 }
 
 espl_status run_static(espl_lanes* h, const NewtonParams& np, int tran) {
-    if (h->pool.next) CK(cudaMemsetAsync(h->pool.next, 0, 2 * sizeof(uint32_t), h->stream));
     CK(cudaEventRecord(h->ev0, h->stream));
-    if (np.mixed) k_static<true><<<grid_of(h), kBlock, 0, h->stream>>>(launch_map(h), np, h->d_state, tran, h->pool);
-    else k_static<false><<<grid_of(h), kBlock, 0, h->stream>>>(launch_map(h), np, h->d_state, tran, h->pool);
+    if (np.mixed)
+        k_static<true><<<grid_of(h), kBlock, h->smem_bytes, h->stream>>>(launch_map(h), np, h->d_state, tran);
+    else
+        k_static<false><<<grid_of(h), kBlock, h->smem_bytes, h->stream>>>(launch_map(h), np, h->d_state, tran);
     CK(cudaGetLastError());
     CK(cudaEventRecord(h->ev1, h->stream));
     CK(cudaEventSynchronize(h->ev1));
@@ -427,6 +589,7 @@ espl_status espl_create(const espl_netlist* nets, uint32_t n_nets, const espl_cr
         if (s) return bail(s);
         g.lane0 = lane0;
         g.warp0 = warp0;
+        g.tile0 = warp0;
         lane0 += g.P;
         warp0 += g.P / 32;
     }
@@ -453,22 +616,6 @@ espl_status espl_create(const espl_netlist* nets, uint32_t n_nets, const espl_cr
     cudaMemcpyAsync(h->d_warp_group, wg.data(), sizeof(uint32_t) * wg.size(), cudaMemcpyHostToDevice, h->stream);
     cudaMemcpyAsync(h->d_mos_raw, mr.data(), sizeof(double*) * n_nets, cudaMemcpyHostToDevice, h->stream);
     cudaMemcpyAsync(h->d_dio_raw, dr.data(), sizeof(double*) * n_nets, cudaMemcpyHostToDevice, h->stream);
-    // Dense-peel pool for templates of n <= 64 (lanes.zig:908 sizes its
-    // pool by memory; here 256 slots of n x n + 5 n doubles, at most 8.8 MB).
-    uint32_t nmax_small = 0;
-    for (auto& g : h->groups)
-        if (g.n <= kDensePeelMax) nmax_small = std::max(nmax_small, g.n);
-    if (nmax_small) {
-        h->pool.n_slots = 256;
-        h->pool.slot_words = dense_slot_words(nmax_small);
-        if (cudaMalloc(&h->pool.scratch, sizeof(double) * h->pool.n_slots * h->pool.slot_words) != cudaSuccess)
-            return bail(ESPL_OUT_OF_MEMORY);
-        uint32_t* ctr = nullptr;
-        if (cudaMalloc(&ctr, 2 * sizeof(uint32_t)) != cudaSuccess) return bail(ESPL_OUT_OF_MEMORY);
-        h->pool.next = ctr;
-        h->pool.over = ctr + 1;
-        cudaMemsetAsync(ctr, 0, 2 * sizeof(uint32_t), h->stream);
-    }
     if (push_descs(h)) return bail(ESPL_DRIVER);
     k_prep<<<grid_of(h), kBlock, 0, h->stream>>>(launch_map(h), h->d_mos_raw, h->d_dio_raw);
     if (cudaGetLastError() != cudaSuccess) return bail(ESPL_DRIVER);
@@ -493,8 +640,6 @@ espl_status espl_destroy(espl_lanes* h) {
     cudaFree(h->d_state);
     cudaFree(h->d_mos_raw);
     cudaFree(h->d_dio_raw);
-    cudaFree(h->pool.scratch);
-    cudaFree(h->pool.next);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -635,10 +780,11 @@ espl_status espl_device_launch(espl_lanes* h, uint32_t max_steps, espl_step_repo
     t.launch_steps = max_steps ? max_steps : 1;
     espl_newton_opts op{t.reltol, t.abstol, t.vntol, 0.0, t.residual_tol, t.max_iter, 0};
     NewtonParams np = newton_params(op, h->precision);
-    if (h->pool.next) CK(cudaMemsetAsync(h->pool.next, 0, 2 * sizeof(uint32_t), h->stream));
     CK(cudaEventRecord(h->ev0, h->stream));
-    if (np.mixed) k_tran<true><<<grid_of(h), kBlock, 0, h->stream>>>(launch_map(h), t, np, h->d_state, h->pool);
-    else k_tran<false><<<grid_of(h), kBlock, 0, h->stream>>>(launch_map(h), t, np, h->d_state, h->pool);
+    if (np.mixed)
+        k_tran<true><<<grid_of(h), kBlock, h->smem_bytes, h->stream>>>(launch_map(h), t, np, h->d_state);
+    else
+        k_tran<false><<<grid_of(h), kBlock, h->smem_bytes, h->stream>>>(launch_map(h), t, np, h->d_state);
     CK(cudaGetLastError());
     CK(cudaEventRecord(h->ev1, h->stream));
     CK(cudaEventSynchronize(h->ev1));
@@ -698,13 +844,14 @@ espl_status espl_get_period_meas(espl_lanes* h, uint32_t net, double* period, ui
 
 espl_status espl_get_stats(espl_lanes* h, espl_stats* out) {
     if (!h || !out) return ESPL_INVALID_ARGUMENT;
-    if (h->pool.next) {
-        uint32_t ctr[2] = {0, 0};
-        CK(cudaMemcpyAsync(ctr, h->pool.next, sizeof(ctr), cudaMemcpyDeviceToHost, h->stream));
-        CK(cudaStreamSynchronize(h->stream));
-        h->stats.dense_peels = ctr[0];
-        h->stats.peel_overflow = ctr[1];
-    }
+    CK(cudaMemcpyAsync(h->h_state.data(), h->d_state, sizeof(LaneState) * h->total_lanes, cudaMemcpyDeviceToHost,
+                       h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    uint64_t peels = 0;
+    for (auto& g : h->groups)
+        for (uint32_t l = 0; l < g.lanes; l++) peels += h->h_state[g.lane0 + l].peels;
+    h->stats.dense_peels = (uint32_t)std::min<uint64_t>(peels, 0xFFFFFFFFu);
+    h->stats.peel_overflow = 0;
     *out = h->stats;
     return ESPL_OK;
 }

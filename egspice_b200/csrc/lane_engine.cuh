@@ -1,6 +1,6 @@
-// The per-lane engine of the lane sweep: stamping, tape refactor, triangular
-// solves, the Newton update and gates, and the transient step machine, each
-// run by the thread that owns the lane. Lanes of one template sit
+// The per-lane sequential engine of the lane sweep: the tape refactor, the
+// triangular solves, the replay probe and the re-pivoting peel, each run by
+// the thread that owns the lane. Lanes of one template sit
 // interleaved (element i of lane l at i * P + l, P = lanes padded to a warp
 // multiple), so a warp's 32 lanes read every nonzero of the shared pattern as
 // one coalesced 256-byte load, while the tape's index words are warp-uniform.
@@ -42,10 +42,21 @@ struct GroupDev {
     const uint8_t* cur_row;
     const uint32_t *res_t, *res_s, *cap_t, *cap_s, *vsrc_t, *vsrc_s, *isrc_t, *dio_t, *dio_s, *mos_t, *mos_s;
     const double *res_r, *cap_c, *vsrc_p, *isrc_p, *dio_d, *mos_d;
-    double *x, *x_old, *dx, *rhs, *qrow, *g, *c, *a, *lx, *ux, *udiag, *w, *y, *lim_mos, *lim_dio, *qs;
+    double *x, *x_old, *dx, *rhs, *qrow, *g, *c, *a, *lx, *ux, *udiag, *w, *y, *lim_mos, *lim_dio;
     float *lx32, *ux32, *udiag32, *w32, *y32;
     double *q1, *ip, *cur, *prev, *sring, *sip;
     double *rr, *corr;
+    double* peel_m;      // n <= 64: the lanes' dense peel scratch (peel_doubles(n) per lane)
+    uint32_t* peel_i;    // n <= 64: its index words (peel_words(n) per lane)
+    // Stamp plan: per-instance output cells (lane-major) and, per Jacobian
+    // slot and residual/charge row, the cells that sum into it in the
+    // reference's stamping order (bit 31: the cell enters negated).
+    uint32_t tile0, n_cells, c_res, c_cap, c_vsrc, c_isrc, c_dio, c_mos, c_pin, c_const;
+    const uint32_t *g_ptr, *g_cell, *c_ptr, *c_cell, *r_ptr, *r_cell, *q_ptr, *q_cell, *site_cell;
+    const uint8_t* slot_diag;
+    double* cells;
+    uint32_t smem_ok;     // the LU chain runs in shared memory (lane_smem.cuh)
+    uint32_t smem_pad;
 };
 
 struct LaneState {
@@ -56,7 +67,7 @@ struct LaneState {
     uint32_t bits, tick, iterations, fallbacks;
     uint32_t order, steps, status, rejects;
     uint32_t bp_clamped, m_cross, m_have, peel_slot;
-    uint32_t s_rot, fp64, pad0, pad1;
+    uint32_t s_rot, fp64, peels, pad1;
 };
 
 struct NewtonParams {
@@ -73,13 +84,6 @@ struct TranParams {
     uint32_t method, fixed_step, max_iter, max_steps, predictor, launch_steps;
 };
 
-struct PeelPool {
-    double* scratch;       // n_slots * slot_words doubles
-    uint32_t* next;        // slot counter (zeroed per solve by the host)
-    uint32_t* over;        // lanes turned away by a full pool
-    uint32_t n_slots, slot_words;
-};
-
 struct Companion {
     int on;
     uint32_t method;  // 0 BE, 1 trap
@@ -91,215 +95,6 @@ struct Companion {
 __device__ __forceinline__ uint64_t dbits(double v) { return (uint64_t)__double_as_longlong(v); }
 __device__ __forceinline__ double bitsd(uint64_t b) { return __longlong_as_double((long long)b); }
 __device__ __forceinline__ uint32_t fbits(float v) { return (uint32_t)__float_as_int(v); }
-
-// ---------------------------------------------------------------------------
-// Stamping
-
-// G, C, the residual F (rhs) and the row charges at the lane's x, each device
-// at its limited branch voltages with the first-order correction to x
-// (eval.zig:826-874), then the ground pin. Terminal rows point at the trash
-// row n for ground, slots at the trash slot nnz.
-__device__ void eval_lane(const GroupDev& d, uint32_t l, int tran, double t) {
-    const uint32_t P = d.P;
-    const uint32_t n = d.n, nnz = d.nnz;
-    double* __restrict__ g = d.g;
-    double* __restrict__ rhs = d.rhs;
-    const double* __restrict__ x = d.x;
-    for (uint32_t p = 0; p <= nnz; p++) LM(g, p) = 0.0;
-    for (uint32_t i = 0; i <= n; i++) LM(rhs, i) = 0.0;
-    if (d.has_charge) {
-        for (uint32_t p = 0; p <= nnz; p++) LM(d.c, p) = 0.0;
-        for (uint32_t i = 0; i <= n; i++) LM(d.qrow, i) = 0.0;
-    }
-    // Resistors: I(p,n) = V(p,n) / r.
-    for (uint32_t i = 0; i < d.n_res; i++) {
-        uint32_t tp = d.res_t[2 * i], tn = d.res_t[2 * i + 1];
-        const uint32_t* s = d.res_s + 4 * i;
-        double v = LM(x, tp) - LM(x, tn);
-        double r = LM(d.res_r, i);
-        double cur = v / r, gg = 1.0 / r;
-        LM(rhs, tp) += cur;
-        LM(g, s[0]) += gg;
-        LM(g, s[1]) += -gg;
-        LM(rhs, tn) += -cur;
-        LM(g, s[2]) += -gg;
-        LM(g, s[3]) += gg;
-    }
-    // Capacitors: q = c V(p,n).
-    for (uint32_t i = 0; i < d.n_cap; i++) {
-        uint32_t tp = d.cap_t[2 * i], tn = d.cap_t[2 * i + 1];
-        const uint32_t* s = d.cap_s + 4 * i;
-        double v = LM(x, tp) - LM(x, tn);
-        double cc = LM(d.cap_c, i);
-        double qq = cc * v;
-        LM(d.qrow, tp) += qq;
-        LM(d.c, s[0]) += cc;
-        LM(d.c, s[1]) += -cc;
-        LM(d.qrow, tn) += -qq;
-        LM(d.c, s[2]) += -cc;
-        LM(d.c, s[3]) += cc;
-        LM(d.qs, i) = qq;
-    }
-    // Voltage sources: branch current ib; row br: V(p,n) - out.
-    for (uint32_t i = 0; i < d.n_vsrc; i++) {
-        uint32_t tp = d.vsrc_t[3 * i], tn = d.vsrc_t[3 * i + 1], tb = d.vsrc_t[3 * i + 2];
-        const uint32_t* s = d.vsrc_s + 9 * i;
-        const double* pp = d.vsrc_p;
-        uint32_t b9 = 9 * i;
-        double val = source_value(LM(pp, b9 + 0), LM(pp, b9 + 1), LM(pp, b9 + 2), LM(pp, b9 + 3), LM(pp, b9 + 4),
-                                  LM(pp, b9 + 5), LM(pp, b9 + 6), LM(pp, b9 + 7), LM(pp, b9 + 8), tran, t);
-        double ib = LM(x, tb);
-        LM(rhs, tp) += ib;
-        LM(g, s[2]) += 1.0;
-        LM(rhs, tn) += -ib;
-        LM(g, s[5]) += -1.0;
-        LM(rhs, tb) += (LM(x, tp) - LM(x, tn)) - val;
-        LM(g, s[6]) += 1.0;
-        LM(g, s[7]) += -1.0;
-    }
-    // Current sources: I(p,n) = out.
-    for (uint32_t i = 0; i < d.n_isrc; i++) {
-        uint32_t tp = d.isrc_t[2 * i], tn = d.isrc_t[2 * i + 1];
-        const double* pp = d.isrc_p;
-        uint32_t b9 = 9 * i;
-        double val = source_value(LM(pp, b9 + 0), LM(pp, b9 + 1), LM(pp, b9 + 2), LM(pp, b9 + 3), LM(pp, b9 + 4),
-                                  LM(pp, b9 + 5), LM(pp, b9 + 6), LM(pp, b9 + 7), LM(pp, b9 + 8), tran, t);
-        LM(rhs, tp) += val;
-        LM(rhs, tn) += -val;
-    }
-    // Diodes at the limited vd, corrected to x.
-    for (uint32_t i = 0; i < d.n_dio; i++) {
-        uint32_t ta = d.dio_t[2 * i], tc = d.dio_t[2 * i + 1];
-        const uint32_t* s = d.dio_s + 4 * i;
-        const double* dd = d.dio_d;
-        uint32_t b = DiodePrep::count * i;
-        double vd = LM(x, ta) - LM(x, tc);
-        double vl = LM(d.lim_dio, i);
-        double id, gd, qd, cd;
-        diode_core(LM(dd, b + DiodePrep::is), LM(dd, b + DiodePrep::vte), LM(dd, b + DiodePrep::gmin),
-                   LM(dd, b + DiodePrep::cjo), LM(dd, b + DiodePrep::cjo_t), LM(dd, b + DiodePrep::vj_t),
-                   LM(dd, b + DiodePrep::mt), LM(dd, b + DiodePrep::fc), LM(dd, b + DiodePrep::tt), vl, id, gd, qd, cd);
-        double f = id + gd * (vd - vl);
-        LM(rhs, ta) += f;
-        LM(g, s[0]) += gd;
-        LM(g, s[1]) += -gd;
-        LM(rhs, tc) += -f;
-        LM(g, s[2]) += -gd;
-        LM(g, s[3]) += gd;
-        if (LM(dd, b + DiodePrep::cjo) > 0.0 || LM(dd, b + DiodePrep::tt) > 0.0) {
-            double qq = qd + cd * (vd - vl);
-            LM(d.qrow, ta) += qq;
-            LM(d.c, s[0]) += cd;
-            LM(d.c, s[1]) += -cd;
-            LM(d.qrow, tc) += -qq;
-            LM(d.c, s[2]) += -cd;
-            LM(d.c, s[3]) += cd;
-            LM(d.qs, d.n_cap + i) = qq;
-        }
-    }
-    // MOS1 at the limited (vgs, vds, vbs), corrected to x.
-    for (uint32_t i = 0; i < d.n_mos; i++) {
-        const uint32_t* tm = d.mos_t + 4 * i;
-        const uint32_t* s = d.mos_s + 16 * i;
-        const double* md = d.mos_d;
-        uint32_t b = Mos1Prep::count * i;
-        double ty = LM(md, b + Mos1Prep::type);
-        double xd = LM(x, tm[0]), xg = LM(x, tm[1]), xs = LM(x, tm[2]), xb = LM(x, tm[3]);
-        double vgs = ty * (xg - xs), vds = ty * (xd - xs), vbs = ty * (xb - xs);
-        double lgs = LM(d.lim_mos, 3 * i), lds = LM(d.lim_mos, 3 * i + 1), lbs = LM(d.lim_mos, 3 * i + 2);
-        Mos1Out o;
-        mos1_core(ty, LM(md, b + Mos1Prep::vt), LM(md, b + Mos1Prep::beta), LM(md, b + Mos1Prep::lambda),
-                  LM(md, b + Mos1Prep::gamma), LM(md, b + Mos1Prep::phit), LM(md, b + Mos1Prep::von0),
-                  LM(md, b + Mos1Prep::isat), LM(md, b + Mos1Prep::gmin), lgs, lds, lbs, o);
-        double dgs = vgs - lgs, dds = vds - lds, dbs = vbs - lbs;
-        double gm = o.mode * o.gm, gds = o.mode * o.gds, gmbs = o.mode * o.gmbs;
-        double ich = o.mode * o.id + gm * dgs + gds * dds + gmbs * dbs;
-        double ibd = o.ibd + o.gbd * (dbs - dds);
-        double ibs = o.ibs + o.gbs * dbs;
-        double gsum = gm + gds + gmbs;
-        LM(rhs, tm[0]) += ty * ich - ty * ibd;
-        LM(g, s[0]) += gds + o.gbd;
-        LM(g, s[1]) += gm;
-        LM(g, s[2]) += -gsum;
-        LM(g, s[3]) += gmbs - o.gbd;
-        LM(rhs, tm[2]) += -ty * ich - ty * ibs;
-        LM(g, s[8]) += -gds;
-        LM(g, s[9]) += -gm;
-        LM(g, s[10]) += gsum + o.gbs;
-        LM(g, s[11]) += -gmbs - o.gbs;
-        LM(rhs, tm[3]) += ty * ibd + ty * ibs;
-        LM(g, s[12]) += -o.gbd;
-        LM(g, s[13]) += 0.0;
-        LM(g, s[14]) += -o.gbs;
-        LM(g, s[15]) += o.gbd + o.gbs;
-    }
-    LM(g, d.diag[0]) += 1.0;
-    LM(rhs, 0) += LM(x, 0);
-}
-
-// Limiter states at the junction seeds (op.zig coldStart: MOS1 vgs = type
-// vbit + gamma sqrt(phit), vds = 0, vbs = -1; the diode, which has no seed,
-// from x), or at x's image for a warm start.
-__device__ void seed_limits(const GroupDev& d, uint32_t l, int cold, const double* x) {
-    const uint32_t P = d.P;
-    for (uint32_t i = 0; i < d.n_mos; i++) {
-        const uint32_t* tm = d.mos_t + 4 * i;
-        uint32_t b = Mos1Prep::count * i;
-        const double* md = d.mos_d;
-        if (cold) {
-            LM(d.lim_mos, 3 * i) = LM(md, b + Mos1Prep::vgs_seed);
-            LM(d.lim_mos, 3 * i + 1) = 0.0;
-            LM(d.lim_mos, 3 * i + 2) = -1.0;
-        } else {
-            double ty = LM(md, b + Mos1Prep::type);
-            double xs = LM(x, tm[2]);
-            LM(d.lim_mos, 3 * i) = ty * (LM(x, tm[1]) - xs);
-            LM(d.lim_mos, 3 * i + 1) = ty * (LM(x, tm[0]) - xs);
-            LM(d.lim_mos, 3 * i + 2) = ty * (LM(x, tm[3]) - xs);
-        }
-    }
-    for (uint32_t i = 0; i < d.n_dio; i++) LM(d.lim_dio, i) = LM(x, d.dio_t[2 * i]) - LM(x, d.dio_t[2 * i + 1]);
-}
-
-// The limiter pass with snapLimited (eval.zig:1115-1171): true when any
-// device clamped its branch voltages.
-__device__ bool limit_lane(const GroupDev& d, uint32_t l) {
-    const uint32_t P = d.P;
-    const double* x = d.x;
-    bool flag = false;
-    const double eps16 = 16 * 2.220446049250313e-16;
-    for (uint32_t i = 0; i < d.n_mos; i++) {
-        const uint32_t* tm = d.mos_t + 4 * i;
-        uint32_t b = Mos1Prep::count * i;
-        const double* md = d.mos_d;
-        double ty = LM(md, b + Mos1Prep::type);
-        double xd = LM(x, tm[0]), xg = LM(x, tm[1]), xs = LM(x, tm[2]), xb = LM(x, tm[3]);
-        double cgs = ty * (xg - xs), cds = ty * (xd - xs), cbs = ty * (xb - xs);
-        double vgs = cgs, vds = cds, vbs = cbs;
-        mos1_limit(LM(md, b + Mos1Prep::vt), LM(md, b + Mos1Prep::gamma), LM(md, b + Mos1Prep::phit),
-                   LM(md, b + Mos1Prep::von0), LM(md, b + Mos1Prep::vcrit), LM(d.lim_mos, 3 * i),
-                   LM(d.lim_mos, 3 * i + 1), LM(d.lim_mos, 3 * i + 2), vgs, vds, vbs);
-        double scale = fmax(fmax(fabs(xd), fabs(xg)), fmax(fabs(xs), fabs(xb)));
-        double tol = eps16 * scale;
-        if (fabs(vgs - cgs) <= tol) vgs = cgs;
-        if (fabs(vds - cds) <= tol) vds = cds;
-        if (fabs(vbs - cbs) <= tol) vbs = cbs;
-        flag |= (vgs != cgs) | (vds != cds) | (vbs != cbs);
-        LM(d.lim_mos, 3 * i) = vgs;
-        LM(d.lim_mos, 3 * i + 1) = vds;
-        LM(d.lim_mos, 3 * i + 2) = vbs;
-    }
-    for (uint32_t i = 0; i < d.n_dio; i++) {
-        double xa = LM(x, d.dio_t[2 * i]), xc = LM(x, d.dio_t[2 * i + 1]);
-        double vd = xa - xc;
-        uint32_t b = DiodePrep::count * i;
-        double v = pnjlim(vd, LM(d.lim_dio, i), LM(d.dio_d, b + DiodePrep::vte), LM(d.dio_d, b + DiodePrep::vcrit));
-        if (fabs(v - vd) <= eps16 * fmax(fabs(xa), fabs(xc))) v = vd;
-        flag |= v != vd;
-        LM(d.lim_dio, i) = v;
-    }
-    return flag;
-}
 
 // ---------------------------------------------------------------------------
 // LU replay of the frozen tape, FP64 (Bodies.refactor + wideMultipliers).
@@ -586,76 +381,99 @@ __device__ void refine_mixed(const GroupDev& d, uint32_t l) {
 // plain partial-pivoting LU with an eps^2 floor (kernels/lane.zig:310-350)
 // that refuses the ill-conditioned iterates a cold operating point passes
 // through; the host factor accepts them.
-// Slot layout (doubles): m[n*n] row-major, xv[n] (the right-hand side,
-// then the solution by unknown), rscale[n], sol[n], then four u32 arrays of
-// n (want, want_of, pinv, row_of) in the last 2n doubles.
-constexpr uint32_t dense_slot_words(uint32_t n) { return n * n + 5 * n; }
+// The peel scratch of a template of n <= 64, per lane, lane-interleaved
+// like every other per-lane array (element i of lane l at i * P + l):
+// m[n * n] row-major, xv[n] (right-hand side, then the solution by unknown),
+// rscale[n], sol[n] as doubles; want, want_of, pinv, row_of[n] as u32.
+__host__ __device__ constexpr uint32_t peel_doubles(uint32_t n) { return n * n + 3 * n; }
+__host__ __device__ constexpr uint32_t peel_words(uint32_t n) { return 4 * n; }
 
-__device__ bool dense_repivot_neg(uint32_t n, const uint32_t* q, double* m, double* xv) {
-    double* rscale = xv + n;
-    double* sol = rscale + n;
-    uint32_t* want = reinterpret_cast<uint32_t*>(sol + n);
-    uint32_t* want_of = want + n;
-    uint32_t* pinv = want_of + n;
-    uint32_t* row_of = pinv + n;
+#define PM(i) pm[(size_t)(i) * P + l]
+#define PI(i) pi[(size_t)(i) * P + l]
+
+__device__ bool dense_repivot_neg(uint32_t n, const uint32_t* q, double* pm, uint32_t* pi, uint32_t P, uint32_t l) {
+    const uint32_t X = n * n, RS = X + n, SOL = RS + n;
+    const uint32_t WANT = 0, WOF = n, PINV = 2 * n, ROW = 3 * n;
     const double tol = 1e-3;
     const double big = 1.7976931348623157e308;
     const uint32_t none = 0xFFFFFFFFu;
     for (uint32_t r = 0; r < n; r++) {
         double mx = 0.0;
-        for (uint32_t c = 0; c < n; c++) mx = fmax(mx, fabs(m[r * n + c]));
-        rscale[r] = (mx > 0.0 && mx <= big) ? 1.0 / mx : 1.0;
-        want[r] = r;
-        want_of[r] = r;
-        pinv[r] = none;
-        xv[r] = -xv[r];
+        for (uint32_t c = 0; c < n; c++) mx = fmax(mx, fabs(PM(r * n + c)));
+        PM(RS + r) = (mx > 0.0 && mx <= big) ? 1.0 / mx : 1.0;
+        PI(WANT + r) = r;
+        PI(WOF + r) = r;
+        PI(PINV + r) = none;
+        PM(X + r) = -PM(X + r);
     }
     for (uint32_t k = 0; k < n; k++) {
         uint32_t c = q[k];
         double amax = 0.0, smax = 0.0;
         uint32_t piv = none;
         for (uint32_t r = 0; r < n; r++) {
-            if (pinv[r] != none) continue;
-            double av = fabs(m[r * n + c]);
+            if (PI(PINV + r) != none) continue;
+            double av = fabs(PM(r * n + c));
             if (av > amax) { amax = av; piv = r; }
-            smax = fmax(smax, av * rscale[r]);
+            smax = fmax(smax, av * PM(RS + r));
         }
         if (piv == none || amax == 0.0 || !(amax <= big)) return false;
-        uint32_t pr = want[c];
-        if (pinv[pr] == none) {
-            double dmag = fabs(m[pr * n + c]);
-            if (dmag > 0.0 && (dmag >= tol * amax || dmag * rscale[pr] >= tol * smax)) piv = pr;
+        uint32_t pr = PI(WANT + c);
+        if (PI(PINV + pr) == none) {
+            double dmag = fabs(PM(pr * n + c));
+            if (dmag > 0.0 && (dmag >= tol * amax || dmag * PM(RS + pr) >= tol * smax)) piv = pr;
         }
         if (piv != pr) {
-            uint32_t c2 = want_of[piv];
-            want[c2] = pr;
-            want_of[pr] = c2;
+            uint32_t c2 = PI(WOF + piv);
+            PI(WANT + c2) = pr;
+            PI(WOF + pr) = c2;
         }
-        pinv[piv] = k;
-        row_of[k] = piv;
-        double d = m[piv * n + c];
+        PI(PINV + piv) = k;
+        PI(ROW + k) = piv;
+        double dv = PM(piv * n + c);
+        double xp = PM(X + piv);
         for (uint32_t r = 0; r < n; r++) {
-            if (pinv[r] != none) continue;
-            double f = m[r * n + c] / d;
+            if (PI(PINV + r) != none) continue;
+            double f = PM(r * n + c) / dv;
             if (f == 0.0) continue;
             for (uint32_t kk = k + 1; kk < n; kk++) {
                 uint32_t cc = q[kk];
-                m[r * n + cc] -= f * m[piv * n + cc];
+                PM(r * n + cc) -= f * PM(piv * n + cc);
             }
-            xv[r] -= f * xv[piv];
+            PM(X + r) -= f * xp;
         }
     }
-    // Back substitution: unknown q[k] from the row pivoted at step k.
     for (uint32_t k = n; k-- > 0;) {
-        uint32_t r = row_of[k];
-        double acc = xv[r];
-        for (uint32_t kk = k + 1; kk < n; kk++) acc -= m[r * n + q[kk]] * sol[q[kk]];
-        double v = acc / m[r * n + q[k]];
+        uint32_t r = PI(ROW + k);
+        double acc = PM(X + r);
+        for (uint32_t kk = k + 1; kk < n; kk++) acc -= PM(r * n + q[kk]) * PM(SOL + q[kk]);
+        double v = acc / PM(r * n + q[k]);
         if (!(fabs(v) <= big)) return false;
-        sol[q[k]] = v;
+        PM(SOL + q[k]) = v;
     }
-    for (uint32_t i = 0; i < n; i++) xv[i] = sol[i];
     return true;
 }
+
+// A failed replay of a lane with n <= 64 solves densely in the lane's own
+// peel scratch (the place of arp_lane_peel_dense, lane_device.zig:120-147),
+// re-pivoting as the host factor would; dx gets the step.
+__device__ bool peel_dense(const GroupDev& d, uint32_t l, LaneState& s) {
+    const uint32_t P = d.P;
+    const uint32_t n = d.n;
+    if (n > kDensePeelMax || d.peel_m == nullptr) return false;
+    double* pm = d.peel_m;
+    uint32_t* pi = d.peel_i;
+    for (uint32_t i = 0; i < n * n; i++) PM(i) = 0.0;
+    for (uint32_t c = 0; c < n; c++)
+        for (uint32_t p = d.col_ptr[c]; p < d.col_ptr[c + 1]; p++) PM(d.row_idx[p] * n + c) += LM(d.a, p);
+    for (uint32_t i = 0; i < n; i++) PM(n * n + i) = LM(d.rhs, i);
+    s.peels++;
+    if (!dense_repivot_neg(n, d.q, pm, pi, P, l)) return false;
+    const uint32_t SOL = n * n + 2 * n;
+    for (uint32_t i = 0; i < n; i++) LM(d.dx, i) = PM(SOL + i);
+    return true;
+}
+
+#undef PM
+#undef PI
 
 }  // namespace espl

@@ -1,233 +1,323 @@
-// Kernels of the lane sweep: one thread per lane, the whole Newton solve of
-// an operating point, or up to `launch_steps` transient steps with device
-// step control, in one launch. A warp holds 32 lanes of one template; the
-// warp -> template table lets one launch carry templates of different sizes.
+// Kernels of the lane sweep. One CTA per 32-lane tile of one template
+// (kWarps warps): the whole Newton solve of an operating point, or up to
+// `launch_steps` transient attempts with device step control, in one launch.
+// The tile -> template table lets one launch carry templates of different
+// sizes. Every loop is bounded by max_iter / launch_steps; no kernel waits on
+// another block.
 #pragma once
 
-#include "lane_engine.cuh"
+#include <climits>
+
+#include "lane_smem.cuh"
 
 namespace espl {
 
-// plausibleLimit (kernels/lane.zig:202-214): the runaway bound of a solve,
-// read off its first assembly.
-__device__ double plausible_limit(const GroupDev& d, uint32_t l) {
-    const uint32_t P = d.P;
-    double g = 1.0;
-    for (uint32_t i = 0; i < d.n; i++) g = fmax(g, fabs(LM(d.a, d.diag[i])));
-    uint64_t xm = 0, fm = 0;
-    for (uint32_t i = 0; i < d.n; i++) {
-        uint64_t xb = dbits(fabs(LM(d.x, i))), fb = dbits(fabs(LM(d.rhs, i)));
-        xm = xm > xb ? xm : xb;
-        fm = fm > fb ? fm : fb;
-    }
-    double scale = fmin(fmax(bitsd(xm), bitsd(fm) * g), 1e18);
-    if (isnan(bitsd(xm)) || isnan(bitsd(fm))) scale = NAN;
-    return !(1e3 * scale > kXPlausible) ? kXPlausible : 1e3 * scale;
-}
-
-// updateNorm (kernels/lane.zig:161-179): x_old = x, x += dx, the delta score.
-__device__ double update_norm(const GroupDev& d, uint32_t l, double reltol, double abstol, double vntol) {
-    const uint32_t P = d.P;
-    uint64_t worst = 0;
-    for (uint32_t i = 0; i < d.n; i++) {
-        double xo = LM(d.x, i), dd = LM(d.dx, i);
-        double xn = xo + dd;
-        LM(d.x_old, i) = xo;
-        LM(d.x, i) = xn;
-        double tol = reltol * fmax(fabs(xn), fabs(xo)) + (d.cur_row[i] ? abstol : vntol);
-        bool finite = fabs(xn) < INFINITY && fabs(dd) < INFINITY;
-        double q = fabs(dd) / tol;
-        double score = !finite ? INFINITY : (q == q ? q : 0.0);
-        uint64_t b = dbits(score);
-        worst = worst > b ? worst : b;
-    }
-    return bitsd(worst);
-}
-
-__device__ bool residual_ok(const GroupDev& d, uint32_t l, const NewtonParams& o) {
-    const uint32_t P = d.P;
-    for (uint32_t i = 0; i < d.n; i++) {
-        double scale = fabs(LM(d.a, d.diag[i]));
-        double s = scale == 0.0 ? 1.0 : scale;
-        double tol = fmax(o.residual_tol, 10.0 * s * (o.reltol * fabs(LM(d.x, i)) + o.vntol));
-        if (!(fabs(LM(d.rhs, i)) <= tol)) return false;
-    }
-    return true;
-}
-
-// A failed replay of a lane with n <= 64 solves densely in a pool slot
-// (the place of arp_lane_peel_dense, lane_device.zig:120-147), re-pivoting
-// as the host factor would. False when the pool is spent or the factor
-// fails.
-__device__ bool peel_dense(const GroupDev& d, uint32_t l, LaneState& s, const PeelPool& pool) {
-    const uint32_t P = d.P;
-    if (d.n > kDensePeelMax || pool.scratch == nullptr) return false;
-    if (s.peel_slot == 0xFFFFFFFFu) {
-        uint32_t slot = atomicAdd(pool.next, 1u);
-        if (slot >= pool.n_slots) {
-            atomicAdd(pool.over, 1u);
-            return false;
-        }
-        s.peel_slot = slot;
-    }
-    double* m = pool.scratch + (size_t)s.peel_slot * pool.slot_words;
-    double* xv = m + (size_t)d.n * d.n;
-    uint32_t n = d.n;
-    for (uint32_t i = 0; i < n * n; i++) m[i] = 0.0;
-    for (uint32_t c = 0; c < n; c++)
-        for (uint32_t p = d.col_ptr[c]; p < d.col_ptr[c + 1]; p++) m[d.row_idx[p] * n + c] += LM(d.a, p);
-    for (uint32_t i = 0; i < n; i++) xv[i] = LM(d.rhs, i);
-    if (!dense_repivot_neg(n, d.q, m, xv)) return false;
-    for (uint32_t i = 0; i < n; i++) LM(d.dx, i) = xv[i];
-    return true;
-}
-
-// One lane's Newton (converger.newtonLanes at W = 1 as the lane kernels
-// split it: assemble, gmin, refactor, solve, update, limit, gates, finalize).
-template <bool MIXED>
-__device__ void newton_lane(const GroupDev& d, uint32_t l, LaneState& s, const NewtonParams& o, int tran, double t,
-                            const Companion& cp, const PeelPool& pool) {
-    const uint32_t P = d.P;
-    uint32_t bits = kActive | (o.init_fix ? kInitFix : 0u);
-    double limit = kXPlausible;
-    s.iterations = o.max_iter;
-    for (uint32_t it = 0; it < o.max_iter; it++) {
-        eval_lane(d, l, tran, t);
-        if (cp.on) {
-            for (uint32_t i = 0; i < d.n; i++) {
-                double dq = cp.ag0 * (LM(d.qrow, i) - LM(d.q1, i));
-                double base = LM(d.rhs, i) + dq;
-                LM(d.rhs, i) = cp.method == 1 ? base - cp.ag1 * LM(d.ip, i) : base;
-            }
-            for (uint32_t p = 0; p < d.nnz; p++) LM(d.a, p) = LM(d.g, p) + cp.ag0 * LM(d.c, p);
-        } else {
-            for (uint32_t p = 0; p < d.nnz; p++) LM(d.a, p) = LM(d.g, p);
-        }
-        if (o.gmin > 0.0) {
-            for (uint32_t i = 0; i < d.n; i++) LM(d.a, d.diag[i]) += o.gmin;
-            for (uint32_t i = 0; i < d.n; i++) LM(d.rhs, i) += o.gmin * LM(d.x, i);
-        }
-        if (it == 0) limit = plausible_limit(d, l);
-        bool fail;
-        bool use32 = MIXED && !s.fp64;
-        if (use32 && refactor32(d, l)) {
-            s.fp64 = 1;
-            s.fallbacks++;
-            use32 = false;
-        }
-        if (use32) {
-            fail = false;
-        } else {
-            int rc = refactor64(d, l);
-            fail = rc == 1 || (rc == 2 && !replay_holds64(d, l));
-        }
-        if (fail) {
-            if (!peel_dense(d, l, s, pool)) {
-                bits = (bits | kSingular) & ~kActive;
-                s.iterations = it;
-                break;
-            }
-        } else if (use32) {
-            solve32(d, l, d.rhs, d.dx);
-            for (uint32_t r = 0; r < o.refine; r++) refine_mixed(d, l);
-        } else {
-            solve64(d, l, d.rhs, d.dx);
-        }
-        double scaled = update_norm(d, l, o.reltol, o.abstol, o.vntol);
-        bool limited = limit_lane(d, l);
-        bool ok = !limited && it != 0 && !(scaled >= 1.0);
-        if (ok)
-            for (uint32_t i = 0; i < d.n; i++)
-                if (!(fabs(LM(d.x, i)) <= limit)) { ok = false; break; }
-        if (ok) ok = residual_ok(d, l, o);
-        if (ok && (bits & kInitFix)) {
-            bits &= ~kInitFix;
-        } else if (ok) {
-            for (uint32_t i = 0; i < d.n; i++) LM(d.x, i) = LM(d.x_old, i);
-            bits = (bits | kConverged) & ~kActive;
-            s.iterations = it + 1;
-            break;
-        }
-        if (MIXED && !s.fp64 && it + 1 >= o.stall_ticks) {
-            s.fp64 = 1;
-            s.fallbacks++;
-        }
-    }
-    s.bits = bits & ~kActive;
-}
-
-struct LaunchMap {
+struct TileMap {
     const GroupDev* groups;
-    const uint32_t* warp_group;
-    uint32_t n_warps;
+    const uint32_t* tile_group;
+    uint32_t n_tiles;
 };
 
-__device__ __forceinline__ bool lane_of(const LaunchMap& m, const GroupDev*& d, uint32_t& l) {
-    uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (gw >= m.n_warps) return false;
-    d = &m.groups[m.warp_group[gw]];
-    l = ((gw - d->warp0) << 5) | (threadIdx.x & 31);
-    return l < d->lanes;
+__device__ __forceinline__ TileCtx tile_ctx(const TileMap& m) {
+    TileCtx c;
+    c.d = &m.groups[m.tile_group[blockIdx.x]];
+    c.lane = threadIdx.x & 31;
+    c.warp = threadIdx.x >> 5;
+    c.l = (blockIdx.x - c.d->tile0) * 32 + c.lane;
+    c.valid = c.l < c.d->lanes;
+    return c;
+}
+
+// Per-tile shared state of a Newton solve and a transient attempt.
+struct TileShared {
+    uint32_t active[32];
+    uint32_t bits[32];
+    uint32_t restore[32];
+    uint32_t pflag[kWarps][32];
+    unsigned long long pmax[kWarps][32];
+    unsigned long long pmax2[kWarps][32];
+    double pg[kWarps][32];
+    double limit[32];
+    double ag0[32], ag1[32], t[32], xfact[32], dt_next[32];
+    uint32_t method[32], on[32], accept[32], rot[32];
+};
+
+// Gate flags reduced over warps.
+constexpr uint32_t kLimited = 1, kImplausible = 2, kResidualMiss = 4;
+
+// One Newton solve per lane of the tile (converger.newtonLanes at W = 1 as
+// the lane kernels split it: assemble, gmin, refactor, solve, update,
+// limit, gates, finalize). `on` lanes take part; with `tran_companion` a
+// lane's companion scalars and time come from the shared arrays.
+template <bool MIXED>
+__device__ void newton_tile(const TileCtx& c, LaneState* s, const NewtonParams& o, int tran, bool tran_companion,
+                            bool on, TileShared& sh, unsigned char* dsm) {
+    const GroupDev& d = *c.d;
+    const uint32_t l = c.l, P = d.P, lane = c.lane, warp = c.warp;
+    const uint32_t ninst = n_instances(d);
+    const bool sm = dsm != nullptr;
+    SmemTile st{};
+    if (sm) st = smem_tile(dsm, smem_plan(d.n, d.nnz, d.nnz_l, d.nnz_u, MIXED));
+    if (warp == 0) {
+        sh.active[lane] = (c.valid && on) ? 1u : 0u;
+        sh.bits[lane] = (o.init_fix ? kInitFix : 0u);
+        sh.limit[lane] = kXPlausible;
+        if (s) s->iterations = o.max_iter;
+    }
+    __syncthreads();
+    for (uint32_t it = 0; it < o.max_iter; it++) {
+        bool act = c.valid && sh.active[lane];
+        if (!__syncthreads_or(act)) break;
+        Companion cp{0, 0, 0.0, 0.0};
+        double tm = 0.0;
+        if (tran_companion) {
+            cp.on = 1;
+            cp.method = sh.method[lane];
+            cp.ag0 = sh.ag0[lane];
+            cp.ag1 = sh.ag1[lane];
+            tm = sh.t[lane];
+        }
+        if (act)
+            for (uint32_t t = warp; t < ninst; t += kWarps) inst_eval(d, l, t, tran, tm);
+        __syncthreads();
+        if (act) {
+            if (sm) {
+                for (uint32_t p = warp; p < d.nnz; p += kWarps) st.a[p * 32 + lane] = gather_slot(d, l, p, cp, o.gmin);
+                for (uint32_t i = warp; i < d.n; i += kWarps) st.rhs[i * 32 + lane] = gather_row(d, l, i, cp, o.gmin);
+            } else {
+                for (uint32_t p = warp; p < d.nnz; p += kWarps) gather_slot(d, l, p, cp, o.gmin);
+                for (uint32_t i = warp; i < d.n; i += kWarps) gather_row(d, l, i, cp, o.gmin);
+            }
+        }
+        __syncthreads();
+        if (it == 0) {
+            // plausibleLimit (kernels/lane.zig:202-214).
+            double g = 1.0;
+            unsigned long long xm = 0, fm = 0;
+            if (act)
+                for (uint32_t i = warp; i < d.n; i += kWarps) {
+                    g = fmax(g, fabs(LM(d.a, d.diag[i])));
+                    unsigned long long xb = dbits(fabs(LM(d.x, i))), fb = dbits(fabs(LM(d.rhs, i)));
+                    xm = xm > xb ? xm : xb;
+                    fm = fm > fb ? fm : fb;
+                }
+            sh.pg[warp][lane] = g;
+            sh.pmax[warp][lane] = xm;
+            sh.pmax2[warp][lane] = fm;
+            __syncthreads();
+            if (warp == 0 && act) {
+                for (int w = 1; w < kWarps; w++) {
+                    g = fmax(g, sh.pg[w][lane]);
+                    xm = xm > sh.pmax[w][lane] ? xm : sh.pmax[w][lane];
+                    fm = fm > sh.pmax2[w][lane] ? fm : sh.pmax2[w][lane];
+                }
+                double scale = fmin(fmax(bitsd(xm), bitsd(fm) * g), 1e18);
+                if (isnan(bitsd(xm)) || isnan(bitsd(fm))) scale = NAN;
+                sh.limit[lane] = !(1e3 * scale > kXPlausible) ? kXPlausible : 1e3 * scale;
+            }
+        }
+        // The LU chain: warp 0, one thread per lane; in shared memory when the
+        // template fits there.
+        if (warp == 0 && act && sm) {
+            bool use32 = MIXED && !s->fp64;
+            int rc = use32 ? refactor_smem<float>(d, st, lane) : 1;
+            if (use32 && rc != 0) {
+                s->fp64 = 1;
+                s->fallbacks++;
+                use32 = false;
+            }
+            if (!use32) {
+                rc = refactor_smem<double>(d, st, lane);
+                if (rc == 2) {
+                    spill_factor<double>(d, st, lane, l);
+                    rc = replay_holds64(d, l) ? 0 : 1;
+                }
+            }
+            if (rc == 0) {
+                if (use32) {
+                    solve_smem<float>(d, st, lane, st.rhs, st.dx);
+                    for (uint32_t r = 0; r < o.refine; r++) refine_smem(d, st, lane);
+                } else {
+                    solve_smem<double>(d, st, lane, st.rhs, st.dx);
+                }
+                for (uint32_t i = 0; i < d.n; i++) LM(d.dx, i) = st.dx[i * 32 + lane];
+            } else if (!peel_dense(d, l, *s)) {
+                sh.bits[lane] |= kSingular;
+                sh.active[lane] = 0;
+                s->iterations = it;
+            }
+        } else if (warp == 0 && act) {
+            bool use32 = MIXED && !s->fp64;
+            if (use32 && refactor32(d, l)) {
+                s->fp64 = 1;
+                s->fallbacks++;
+                use32 = false;
+            }
+            bool fail = false;
+            if (!use32) {
+                int rc = refactor64(d, l);
+                fail = rc == 1 || (rc == 2 && !replay_holds64(d, l));
+            }
+            if (fail) {
+                if (!peel_dense(d, l, *s)) {
+                    sh.bits[lane] |= kSingular;
+                    sh.active[lane] = 0;
+                    s->iterations = it;
+                }
+            } else if (use32) {
+                solve32(d, l, d.rhs, d.dx);
+                for (uint32_t r = 0; r < o.refine; r++) refine_mixed(d, l);
+            } else {
+                solve64(d, l, d.rhs, d.dx);
+            }
+        }
+        __syncthreads();
+        act = c.valid && sh.active[lane];
+        // updateNorm (kernels/lane.zig:161-179), rows split over warps.
+        unsigned long long worst = 0;
+        if (act)
+            for (uint32_t i = warp; i < d.n; i += kWarps) {
+                double xo = LM(d.x, i), dd = LM(d.dx, i);
+                double xn = xo + dd;
+                LM(d.x_old, i) = xo;
+                LM(d.x, i) = xn;
+                double tol = o.reltol * fmax(fabs(xn), fabs(xo)) + (d.cur_row[i] ? o.abstol : o.vntol);
+                bool finite = fabs(xn) < INFINITY && fabs(dd) < INFINITY;
+                double q = fabs(dd) / tol;
+                double score = !finite ? INFINITY : (q == q ? q : 0.0);
+                unsigned long long b = dbits(score);
+                worst = worst > b ? worst : b;
+            }
+        sh.pmax[warp][lane] = worst;
+        __syncthreads();
+        // The limiter pass over instances; plausible and residual gates over rows.
+        uint32_t flags = 0;
+        if (act) {
+            for (uint32_t t = warp; t < ninst; t += kWarps)
+                if (inst_limit(d, l, t)) flags |= kLimited;
+            double lim = sh.limit[lane];
+            for (uint32_t i = warp; i < d.n; i += kWarps) {
+                double xi = LM(d.x, i);
+                if (!(fabs(xi) <= lim)) flags |= kImplausible;
+                double scale = fabs(LM(d.a, d.diag[i]));
+                double sc = scale == 0.0 ? 1.0 : scale;
+                double tol = fmax(o.residual_tol, 10.0 * sc * (o.reltol * fabs(xi) + o.vntol));
+                if (!(fabs(LM(d.rhs, i)) <= tol)) flags |= kResidualMiss;
+            }
+        }
+        sh.pflag[warp][lane] = flags;
+        __syncthreads();
+        if (warp == 0) {
+            sh.restore[lane] = 0;
+            if (act) {
+                unsigned long long wb = 0;
+                uint32_t f = 0;
+                for (int w = 0; w < kWarps; w++) {
+                    wb = wb > sh.pmax[w][lane] ? wb : sh.pmax[w][lane];
+                    f |= sh.pflag[w][lane];
+                }
+                double scaled = bitsd(wb);
+                bool ok = !(f & kLimited) && it != 0 && !(scaled >= 1.0) && !(f & (kImplausible | kResidualMiss));
+                if (ok && (sh.bits[lane] & kInitFix)) {
+                    sh.bits[lane] &= ~kInitFix;
+                } else if (ok) {
+                    sh.bits[lane] |= kConverged;
+                    sh.active[lane] = 0;
+                    sh.restore[lane] = 1;
+                    s->iterations = it + 1;
+                }
+                if (MIXED && sh.active[lane] && !s->fp64 && it + 1 >= o.stall_ticks) {
+                    s->fp64 = 1;
+                    s->fallbacks++;
+                }
+            }
+        }
+        __syncthreads();
+        if (c.valid && sh.restore[lane])
+            for (uint32_t i = warp; i < d.n; i += kWarps) LM(d.x, i) = LM(d.x_old, i);
+    }
+    __syncthreads();
+    if (warp == 0 && s) s->bits = sh.bits[lane];
+}
+
+extern __shared__ __align__(16) unsigned char g_dsm[];
+
+// Stages the tile's tape into shared memory when its template runs the LU
+// chain there; null otherwise (or when the bounded wait ran out).
+template <bool MIXED>
+__device__ unsigned char* tile_smem(const GroupDev& d) {
+    if (!d.smem_ok) return nullptr;
+    bool ok = stage_tape(d, g_dsm, smem_plan(d.n, d.nnz, d.nnz_l, d.nnz_u, MIXED));
+    return ok ? g_dsm : nullptr;
 }
 
 template <bool MIXED>
-__global__ void __launch_bounds__(128) k_static(LaunchMap m, NewtonParams o, LaneState* st, int tran, PeelPool pool) {
-    const GroupDev* d;
-    uint32_t l;
-    if (!lane_of(m, d, l)) return;
-    LaneState& s = st[d->lane0 + l];
-    s.peel_slot = 0xFFFFFFFFu;  // the pool's counter restarts every solve
-    Companion cp{0, 0, 0.0, 0.0};
-    newton_lane<MIXED>(*d, l, s, o, tran, 0.0, cp, pool);
+__global__ void __launch_bounds__(kTileThreads) k_static(TileMap m, NewtonParams o, LaneState* st, int tran) {
+    __shared__ TileShared sh;
+    TileCtx c = tile_ctx(m);
+    LaneState* s = (c.warp == 0 && c.valid) ? &st[c.d->lane0 + c.l] : nullptr;
+    unsigned char* dsm = tile_smem<MIXED>(*c.d);
+    newton_tile<MIXED>(c, s, o, tran, false, true, sh, dsm);
 }
 
-// Bias-independent prep per (instance, lane), from the raw lane-major rows.
-__global__ void __launch_bounds__(128) k_prep(LaunchMap m, const double* const* mos_raw, const double* const* dio_raw) {
-    const GroupDev* d;
-    uint32_t l;
-    if (!lane_of(m, d, l)) return;
-    const uint32_t P = d->P;
-    uint32_t g = m.warp_group[(blockIdx.x * blockDim.x + threadIdx.x) >> 5];
+// Bias-independent prep per (instance, lane) from the raw lane-major rows,
+// and the constant cells (+1, -1).
+__global__ void __launch_bounds__(kTileThreads) k_prep(TileMap m, const double* const* mos_raw,
+                                                       const double* const* dio_raw) {
+    TileCtx c = tile_ctx(m);
+    if (!c.valid) return;
+    const GroupDev& d = *c.d;
+    const uint32_t P = d.P, l = c.l;
+    uint32_t g = m.tile_group[blockIdx.x];
     const double* mr = mos_raw[g];
     const double* dr = dio_raw[g];
-    double* md = const_cast<double*>(d->mos_d);
-    double* dd = const_cast<double*>(d->dio_d);
-    for (uint32_t i = 0; i < d->n_mos; i++) {
+    double* md = const_cast<double*>(d.mos_d);
+    double* dd = const_cast<double*>(d.dio_d);
+    for (uint32_t i = c.warp; i < d.n_mos; i += kWarps) {
         double p[9], o[Mos1Prep::count];
         for (int k = 0; k < 9; k++) p[k] = LM(mr, 9 * i + k);
         mos1_setup(p, o);
         for (int k = 0; k < Mos1Prep::count; k++) LM(md, Mos1Prep::count * i + k) = o[k];
     }
-    for (uint32_t i = 0; i < d->n_dio; i++) {
+    for (uint32_t i = c.warp; i < d.n_dio; i += kWarps) {
         double p[7], o[DiodePrep::count];
         for (int k = 0; k < 7; k++) p[k] = LM(dr, 7 * i + k);
         diode_setup(p, o);
         for (int k = 0; k < DiodePrep::count; k++) LM(dd, DiodePrep::count * i + k) = o[k];
     }
+    if (c.warp == 0) {
+        LM(d.cells, d.c_const) = 1.0;
+        LM(d.cells, d.c_const + 1) = -1.0;
+    }
 }
 
-// Seeds the limiter states for a cold (MODEINITJCT) or warm start.
-__global__ void __launch_bounds__(128) k_seed(LaunchMap m, int cold, LaneState* st) {
-    const GroupDev* d;
-    uint32_t l;
-    if (!lane_of(m, d, l)) return;
-    seed_limits(*d, l, cold, d->x);
-    LaneState& s = st[d->lane0 + l];
-    s.fp64 = 0;
-    s.fallbacks = 0;
-    s.peel_slot = 0xFFFFFFFFu;
+// Limiter states for a cold (MODEINITJCT) or warm start; resets the lane's
+// per-solve bookkeeping.
+__global__ void __launch_bounds__(kTileThreads) k_seed(TileMap m, int cold, LaneState* st) {
+    TileCtx c = tile_ctx(m);
+    if (!c.valid) return;
+    const GroupDev& d = *c.d;
+    const uint32_t ninst = n_instances(d);
+    for (uint32_t t = c.warp; t < ninst; t += kWarps) inst_seed(d, c.l, t, cold, d.x);
+    if (c.warp == 0) {
+        LaneState& s = st[d.lane0 + c.l];
+        s.fp64 = 0;
+        s.fallbacks = 0;
+        s.peels = 0;
+    }
 }
 
-// Stamps every lane at its x and writes A = G (+ C / dt) for the lead
-// lane's tape (ownTape's matrix).
-__global__ void __launch_bounds__(128) k_assemble(LaunchMap m, int tran, double t, double inv_dt) {
-    const GroupDev* d;
-    uint32_t l;
-    if (!lane_of(m, d, l)) return;
-    const uint32_t P = d->P;
-    eval_lane(*d, l, tran, t);
-    for (uint32_t p = 0; p < d->nnz; p++)
-        LM(d->a, p) = inv_dt > 0.0 ? LM(d->g, p) + inv_dt * LM(d->c, p) : LM(d->g, p);
+// Every lane stamped at its x: A = G (+ C / dt) for the lead lane's tape
+// (ownTape's matrix).
+__global__ void __launch_bounds__(kTileThreads) k_assemble(TileMap m, int tran, double inv_dt) {
+    TileCtx c = tile_ctx(m);
+    const GroupDev& d = *c.d;
+    if (c.valid)
+        for (uint32_t t = c.warp; t < n_instances(d); t += kWarps) inst_eval(d, c.l, t, tran, 0.0);
+    __syncthreads();
+    Companion cp{inv_dt > 0.0 ? 1 : 0, 0, inv_dt, 1.0};
+    if (c.valid)
+        for (uint32_t p = c.warp; p < d.nnz; p += kWarps) gather_slot(d, c.l, p, cp, 0.0);
 }
 
 // ---------------------------------------------------------------------------
@@ -244,7 +334,6 @@ __device__ __forceinline__ bool at_stop(double t, double t_stop) {
 __device__ __forceinline__ bool almost_equal_ulps(double a, double b, long long max_ulps) {
     if (a == b) return true;
     long long ia = __double_as_longlong(a), ib = __double_as_longlong(b);
-    // lex order of IEEE bits as tran.almostEqualUlps defines it, in 128 bits.
     __int128 la = ia < 0 ? (__int128)LLONG_MIN - ia : ia;
     __int128 lb = ib < 0 ? (__int128)LLONG_MIN - ib : ib;
     __int128 dd = la - lb;
@@ -270,8 +359,11 @@ __device__ double next_bp(const GroupDev& d, uint32_t l, double t) {
     return best;
 }
 
-// stepBound (kernels/lane.zig:257-297) over the lane's sites; ring slots
-// are the logical 0..3 of the site ring.
+__device__ __forceinline__ double* ring_slot(const GroupDev& d, uint32_t rot, uint32_t logical) {
+    return d.sring + (size_t)((rot + logical) & 3) * d.n_sites * d.P;
+}
+
+// stepBound (kernels/lane.zig:257-297) over the lane's sites.
 __device__ double step_bound(const GroupDev& d, uint32_t l, uint32_t rot, uint32_t method, uint32_t cur_method,
                              double dt, double dt1, double dt2, double reltol, double abstol, double chgtol,
                              double trtol, double ag0, double ag1) {
@@ -280,10 +372,8 @@ __device__ double step_bound(const GroupDev& d, uint32_t l, uint32_t rot, uint32
     double coeff = method == 0 ? 0.5 : method == 1 ? 0.08333333333 : 0.2222222222;
     double sum01 = dt + dt1, sum12 = dt1 + dt2, sum012 = dt + (dt1 + dt2);
     double vmin = INFINITY, poison = 0.0;
-    const double* r0 = d.sring + (size_t)((rot + 0) & 3) * ns * P;
-    const double* r1 = d.sring + (size_t)((rot + 1) & 3) * ns * P;
-    const double* r2 = d.sring + (size_t)((rot + 2) & 3) * ns * P;
-    const double* r3 = d.sring + (size_t)((rot + 3) & 3) * ns * P;
+    const double *r0 = ring_slot(d, rot, 0), *r1 = ring_slot(d, rot, 1);
+    const double *r2 = ring_slot(d, rot, 2), *r3 = ring_slot(d, rot, 3);
     for (uint32_t j = 0; j < ns; j++) {
         double qc = LM(r0, j), qp = LM(r1, j), qp2 = LM(r2, j), qp3 = LM(r3, j), i_p = LM(d.sip, j);
         double i_new = cur_method == 1 ? ag0 * (qc - qp) - ag1 * i_p : ag0 * (qc - qp);
@@ -307,25 +397,33 @@ __device__ double step_bound(const GroupDev& d, uint32_t l, uint32_t rot, uint32
 }
 
 // Transient start from the operating point in x: histories, the site ring,
-// the first step (tran.zig:688-699 for LTE control), breakpoints.
-__global__ void __launch_bounds__(128) k_tran_init(LaunchMap m, TranParams o, LaneState* st) {
-    const GroupDev* d;
-    uint32_t l;
-    if (!lane_of(m, d, l)) return;
-    const uint32_t P = d->P;
-    LaneState& s = st[d->lane0 + l];
-    seed_limits(*d, l, 0, d->x);
-    eval_lane(*d, l, 1, 0.0);
-    for (uint32_t i = 0; i < d->n; i++) {
-        LM(d->cur, i) = LM(d->x, i);
-        LM(d->prev, i) = LM(d->x, i);
-        LM(d->q1, i) = LM(d->qrow, i);
-        LM(d->ip, i) = 0.0;
+// the first step (tran.zig:688-699 under LTE control), breakpoints.
+__global__ void __launch_bounds__(kTileThreads) k_tran_init(TileMap m, TranParams o, LaneState* st) {
+    TileCtx c = tile_ctx(m);
+    const GroupDev& d = *c.d;
+    const uint32_t P = d.P, l = c.l;
+    const uint32_t ninst = n_instances(d);
+    if (c.valid)
+        for (uint32_t t = c.warp; t < ninst; t += kWarps) {
+            inst_seed(d, l, t, 0, d.x);
+            inst_eval(d, l, t, 1, 0.0);
+        }
+    __syncthreads();
+    if (!c.valid) return;
+    for (uint32_t i = c.warp; i < d.n; i += kWarps) {
+        gather_charge_row(d, l, i);
+        LM(d.cur, i) = LM(d.x, i);
+        LM(d.prev, i) = LM(d.x, i);
+        LM(d.q1, i) = LM(d.qrow, i);
+        LM(d.ip, i) = 0.0;
     }
-    uint32_t ns = d->n_sites;
-    for (uint32_t k = 0; k < 4; k++)
-        for (uint32_t j = 0; j < ns; j++) LM(d->sring + (size_t)k * ns * P, j) = LM(d->qs, j);
-    for (uint32_t j = 0; j < ns; j++) LM(d->sip, j) = 0.0;
+    for (uint32_t j = c.warp; j < d.n_sites; j += kWarps) {
+        double q = LM(d.cells, d.site_cell[j]);
+        for (uint32_t k = 0; k < 4; k++) LM(d.sring + (size_t)k * d.n_sites * P, j) = q;
+        LM(d.sip, j) = 0.0;
+    }
+    if (c.warp != 0) return;
+    LaneState& s = st[d.lane0 + l];
     s.s_rot = 0;
     s.t = 0.0;
     double dt;
@@ -334,7 +432,7 @@ __global__ void __launch_bounds__(128) k_tran_init(LaunchMap m, TranParams o, La
         s.dt_old0 = s.dt_old1 = o.dt;
     } else {
         dt = fmin(fmin(o.dt, o.t_stop / 100.0) / 10.0, o.dt_max);
-        double bp0 = next_bp(*d, l, 0.0);
+        double bp0 = next_bp(d, l, 0.0);
         if (bp0 < INFINITY) dt = fmin(dt, 0.1 * bp0);
         dt /= 10.0;
         s.dt_old0 = s.dt_old1 = o.dt_max;
@@ -346,162 +444,214 @@ __global__ void __launch_bounds__(128) k_tran_init(LaunchMap m, TranParams o, La
     s.rejects = 0;
     s.attempts = 0;
     s.nr_iters = 0;
-    s.bp_next = o.fixed_step ? INFINITY : next_bp(*d, l, 0.0);
+    s.bp_next = o.fixed_step ? INFINITY : next_bp(d, l, 0.0);
     s.bp_save_dt = 0.0;
     s.bp_clamped = 0;
     s.m_cross = 0;
     s.m_have = 0;
     s.m_first = s.m_last = NAN;
     s.fp64 = 0;
-    s.peel_slot = 0xFFFFFFFFu;
+    s.peels = 0;
 }
 
-// Up to o.launch_steps accepted-or-rejected attempts per lane.
+// Up to o.launch_steps attempts per lane, each: stepBegin, the linear
+// predictor, the limiter pass, Newton with the companion rows, stepEndA
+// (Newton and LTE rejections, order promotion), the accepted-step history
+// advance, stepEndB (breakpoints, next dt) and the period measure.
 template <bool MIXED>
-__global__ void __launch_bounds__(128) k_tran(LaunchMap m, TranParams o, NewtonParams no, LaneState* st, PeelPool pool) {
-    const GroupDev* dp;
-    uint32_t l;
-    if (!lane_of(m, dp, l)) return;
-    const GroupDev& d = *dp;
-    const uint32_t P = d.P;
-    LaneState& s = st[d.lane0 + l];
-    s.peel_slot = 0xFFFFFFFFu;  // the pool's counter restarts every launch
-    const uint32_t ns = d.n_sites;
+__global__ void __launch_bounds__(kTileThreads) k_tran(TileMap m, TranParams o, NewtonParams no, LaneState* st) {
+    __shared__ TileShared sh;
+    TileCtx c = tile_ctx(m);
+    const GroupDev& d = *c.d;
+    const uint32_t P = d.P, l = c.l, lane = c.lane, warp = c.warp;
+    const uint32_t ns = d.n_sites, ninst = n_instances(d);
+    LaneState* s = (warp == 0 && c.valid) ? &st[d.lane0 + l] : nullptr;
+    unsigned char* dsm = tile_smem<MIXED>(d);
+    NewtonParams np = no;
+    np.init_fix = 0;
+    np.max_iter = o.max_iter;
     for (uint32_t attempt = 0; attempt < o.launch_steps; attempt++) {
-        if (s.status != 0) break;
-        if (!(s.t < o.t_stop && !at_stop(s.t, o.t_stop) && s.steps < o.max_steps)) {
-            s.status = 1;
-            break;
-        }
-        double dt = s.dt;
-        uint32_t method = s.order == 1 ? 0 : o.method;
-        Companion cp;
-        cp.on = 1;
-        cp.method = method;
-        if (method == 0) { cp.ag0 = 1.0 / dt; cp.ag1 = 1.0; }
-        else { cp.ag0 = 1.0 / dt / (1.0 - 0.5); cp.ag1 = 0.5 / (1.0 - 0.5); }
-        double t_dev = s.t + dt;
-        double xfact = dt / s.dt_old0;
-        for (uint32_t i = 0; i < d.n; i++) {
-            double c = LM(d.cur, i);
-            LM(d.x, i) = o.predictor == 1 ? c + xfact * (c - LM(d.prev, i)) : c;
-        }
-        // The limiter state restarts from the accepted point, then limits
-        // the predicted iterate.
-        seed_limits(d, l, 0, d.cur);
-        limit_lane(d, l);
-        NewtonParams np = no;
-        np.init_fix = 0;
-        np.max_iter = o.max_iter;
-        s.fp64 = 0;
-        newton_lane<MIXED>(d, l, s, np, 1, t_dev, cp, pool);
-        s.attempts++;
-        bool conv = (s.bits & kConverged) != 0;
-        if (!(s.bits & kSingular)) s.nr_iters += s.iterations < o.max_iter ? s.iterations : o.max_iter;
-        if (!conv) {
-            s.rejects++;
-            s.order = 1;
-            if (o.fixed_step) { s.status = 2; break; }
-            double ndt = dt / 8.0;
-            if (ndt < o.dt_min && dt > o.dt_min && s.t + o.dt_min > s.t) ndt = o.dt_min;
-            s.dt = ndt;
-            if (ndt < o.dt_min) { s.status = 2; break; }
-            continue;
-        }
-        // The last eval ran at the published x: its charges are the point's.
-        double* r0 = d.sring + (size_t)(s.s_rot & 3) * ns * P;
-        for (uint32_t j = 0; j < ns; j++) LM(r0, j) = LM(d.qs, j);
-        double dt_next = s.steps == 0 ? dt : fmin(dt * 2.0, o.dt_max);
-        if (o.fixed_step) {
-            dt_next = dt;
-            if (s.order == 1 && o.method != 0) s.order = 2;
-        } else if (ns > 0 && s.steps > 0) {
-            double del = step_bound(d, l, s.s_rot, method, method, dt, s.dt_old0, s.dt_old1, o.reltol, o.abstol,
-                                    o.chgtol, o.trtol, cp.ag0, cp.ag1);
-            double del2 = method == 0 ? step_bound(d, l, s.s_rot, o.method, method, dt, s.dt_old0, s.dt_old1,
-                                                   o.reltol, o.abstol, o.chgtol, o.trtol, cp.ag0, cp.ag1)
-                                      : del;
-            if (!(del >= 0.9 * dt)) {
-                s.rejects++;
-                double ndt;
-                if (isnan(del)) { s.order = 1; ndt = dt / 8.0; }
-                else ndt = del;
-                if (ndt < o.dt_min && dt > o.dt_min && s.t + o.dt_min > s.t) ndt = o.dt_min;
-                s.dt = ndt;
-                if (ndt < o.dt_min) { s.status = 2; break; }
-                continue;
-            }
-            dt_next = fmin(fmin(fmax(del, o.dt_min), 2 * dt), o.dt_max);
-            if (s.order == 1) {
-                double trial = o.method == method ? del : del2;
-                if (!isnan(trial)) {
-                    double nd2 = fmin(2.0 * dt, trial);
-                    if (nd2 > 1.05 * dt) s.order = 2;
-                    dt_next = fmin(fmax(nd2, o.dt_min), o.dt_max);
+        // stepBegin (kernels/lane.zig:508-545).
+        if (warp == 0) {
+            uint32_t on = 0;
+            if (s && s->status == 0) {
+                if (!(s->t < o.t_stop && !at_stop(s->t, o.t_stop) && s->steps < o.max_steps)) {
+                    s->status = 1;
+                } else {
+                    on = 1;
+                    double dt = s->dt;
+                    uint32_t method = s->order == 1 ? 0 : o.method;
+                    sh.method[lane] = method;
+                    if (method == 0) { sh.ag0[lane] = 1.0 / dt; sh.ag1[lane] = 1.0; }
+                    else { sh.ag0[lane] = 1.0 / dt / (1.0 - 0.5); sh.ag1[lane] = 0.5 / (1.0 - 0.5); }
+                    sh.t[lane] = s->t + dt;
+                    sh.xfact[lane] = dt / s->dt_old0;
+                    sh.rot[lane] = s->s_rot;
+                    s->fp64 = 0;
                 }
             }
+            sh.on[lane] = on;
         }
-        // Accept (lane_device.zig accept): row histories, companion currents.
-        for (uint32_t i = 0; i < d.n; i++) {
-            double dq = cp.ag0 * (LM(d.qrow, i) - LM(d.q1, i));
-            LM(d.ip, i) = method == 1 ? dq - cp.ag1 * LM(d.ip, i) : dq;
-            LM(d.q1, i) = LM(d.qrow, i);
-            LM(d.prev, i) = LM(d.cur, i);
-            LM(d.cur, i) = LM(d.x, i);
-        }
-        {
-            const double* q0 = d.sring + (size_t)((s.s_rot + 0) & 3) * ns * P;
-            const double* q1 = d.sring + (size_t)((s.s_rot + 1) & 3) * ns * P;
-            for (uint32_t j = 0; j < ns; j++) {
-                double dq = cp.ag0 * (LM(q0, j) - LM(q1, j));
-                LM(d.sip, j) = method == 1 ? dq - cp.ag1 * LM(d.sip, j) : dq;
+        __syncthreads();
+        bool on = c.valid && sh.on[lane];
+        if (!__syncthreads_or(on)) break;
+        if (on) {
+            double xf = sh.xfact[lane];
+            for (uint32_t i = warp; i < d.n; i += kWarps) {
+                double cu = LM(d.cur, i);
+                LM(d.x, i) = o.predictor == 1 ? cu + xf * (cu - LM(d.prev, i)) : cu;
             }
         }
-        s.s_rot = (s.s_rot + 3) & 3;  // rotate right: new logical k = old k - 1
-        s.dt_old1 = s.dt_old0;
-        s.dt_old0 = dt;
-        double t_new = s.t + dt;
-        s.steps++;
-        if (d.meas_row != 0xFFFFFFFFu && t_new >= d.meas_t0) {
-            double v = LM(d.x, d.meas_row);
-            if (s.m_have && s.m_prev_v < d.meas_level && v >= d.meas_level) {
-                double tc = s.m_prev_t + (d.meas_level - s.m_prev_v) * (t_new - s.m_prev_t) / (v - s.m_prev_v);
-                if (s.m_cross == 0) s.m_first = tc;
-                s.m_last = tc;
-                s.m_cross++;
+        __syncthreads();
+        // The limiter state restarts from the accepted point, then limits the
+        // predicted iterate.
+        if (on)
+            for (uint32_t t = warp; t < ninst; t += kWarps) {
+                inst_seed(d, l, t, 0, d.cur);
+                inst_limit(d, l, t);
             }
-            s.m_prev_v = v;
-            s.m_prev_t = t_new;
-            s.m_have = 1;
+        __syncthreads();
+        newton_tile<MIXED>(c, s, np, 1, true, on, sh, dsm);
+        // The last eval ran at the published x: its site charges are the
+        // point's, logical slot 0 of the ring.
+        bool conv = on && (sh.bits[lane] & kConverged);
+        if (conv) {
+            double* r0 = ring_slot(d, sh.rot[lane], 0);
+            for (uint32_t j = warp; j < ns; j += kWarps) LM(r0, j) = LM(d.cells, d.site_cell[j]);
         }
-        // stepEndB (kernels/lane.zig:667-700).
-        s.t = t_new;
-        if (!o.fixed_step) {
-            double nb = next_bp(d, l, t_new + o.min_break);
-            if (s.bp_next != INFINITY) {
-                double bp = s.bp_next;
-                bool landed = s.bp_clamped ? fabs(t_new - bp) <= o.min_break
-                                           : (bp - t_new <= o.delmin || almost_equal_ulps(t_new, bp, 100));
-                if (landed) {
-                    s.order = 1;
-                    double shrink = s.bp_save_dt;
-                    if (nb != INFINITY) shrink = fmin(shrink, nb - t_new);
-                    dt_next = fmin(dt_next, 0.1 * shrink);
+        __syncthreads();
+        // stepEndA (kernels/lane.zig:563-654).
+        if (warp == 0) {
+            uint32_t acc = 0;
+            if (s && on) {
+                double dt = s->dt;
+                uint32_t method = sh.method[lane];
+                s->attempts++;
+                if (!(sh.bits[lane] & kSingular)) s->nr_iters += s->iterations < o.max_iter ? s->iterations : o.max_iter;
+                if (!conv) {
+                    s->rejects++;
+                    s->order = 1;
+                    if (o.fixed_step) {
+                        s->status = 2;
+                    } else {
+                        double ndt = dt / 8.0;
+                        if (ndt < o.dt_min && dt > o.dt_min && s->t + o.dt_min > s->t) ndt = o.dt_min;
+                        s->dt = ndt;
+                        if (ndt < o.dt_min) s->status = 2;
+                    }
+                } else {
+                    double dt_next = s->steps == 0 ? dt : fmin(dt * 2.0, o.dt_max);
+                    bool reject = false;
+                    if (o.fixed_step) {
+                        dt_next = dt;
+                        if (s->order == 1 && o.method != 0) s->order = 2;
+                    } else if (ns > 0 && s->steps > 0) {
+                        double del = step_bound(d, l, s->s_rot, method, method, dt, s->dt_old0, s->dt_old1, o.reltol,
+                                                o.abstol, o.chgtol, o.trtol, sh.ag0[lane], sh.ag1[lane]);
+                        double del2 = method == 0 ? step_bound(d, l, s->s_rot, o.method, method, dt, s->dt_old0,
+                                                               s->dt_old1, o.reltol, o.abstol, o.chgtol, o.trtol,
+                                                               sh.ag0[lane], sh.ag1[lane])
+                                                  : del;
+                        if (!(del >= 0.9 * dt)) {
+                            reject = true;
+                            s->rejects++;
+                            double ndt;
+                            if (isnan(del)) { s->order = 1; ndt = dt / 8.0; }
+                            else ndt = del;
+                            if (ndt < o.dt_min && dt > o.dt_min && s->t + o.dt_min > s->t) ndt = o.dt_min;
+                            s->dt = ndt;
+                            if (ndt < o.dt_min) s->status = 2;
+                        } else {
+                            dt_next = fmin(fmin(fmax(del, o.dt_min), 2 * dt), o.dt_max);
+                            if (s->order == 1) {
+                                double trial = o.method == method ? del : del2;
+                                if (!isnan(trial)) {
+                                    double nd2 = fmin(2.0 * dt, trial);
+                                    if (nd2 > 1.05 * dt) s->order = 2;
+                                    dt_next = fmin(fmax(nd2, o.dt_min), o.dt_max);
+                                }
+                            }
+                        }
+                    }
+                    if (!reject) {
+                        acc = 1;
+                        sh.dt_next[lane] = dt_next;
+                    }
                 }
             }
-            s.bp_next = nb;
-            s.bp_clamped = 0;
-            if (nb != INFINITY) {
-                double to_bp = nb - t_new;
-                if (to_bp < dt_next) {
-                    s.bp_save_dt = dt_next;
-                    dt_next = to_bp;
-                    s.bp_clamped = 1;
-                }
+            sh.accept[lane] = acc;
+        }
+        __syncthreads();
+        // Accept (lane_device.zig accept): row histories and companion currents.
+        bool acc = c.valid && sh.accept[lane];
+        if (acc) {
+            double ag0 = sh.ag0[lane], ag1 = sh.ag1[lane];
+            uint32_t method = sh.method[lane];
+            for (uint32_t i = warp; i < d.n; i += kWarps) {
+                double dq = ag0 * (LM(d.qrow, i) - LM(d.q1, i));
+                LM(d.ip, i) = method == 1 ? dq - ag1 * LM(d.ip, i) : dq;
+                LM(d.q1, i) = LM(d.qrow, i);
+                LM(d.prev, i) = LM(d.cur, i);
+                LM(d.cur, i) = LM(d.x, i);
+            }
+            const double* q0 = ring_slot(d, sh.rot[lane], 0);
+            const double* q1 = ring_slot(d, sh.rot[lane], 1);
+            for (uint32_t j = warp; j < ns; j += kWarps) {
+                double dq = ag0 * (LM(q0, j) - LM(q1, j));
+                LM(d.sip, j) = method == 1 ? dq - ag1 * LM(d.sip, j) : dq;
             }
         }
-        s.dt = dt_next;
-        if (t_new + s.dt > o.t_stop) s.dt = o.t_stop - t_new;
+        __syncthreads();
+        if (warp == 0 && s && acc) {
+            double dt = s->dt;
+            double dt_next = sh.dt_next[lane];
+            s->s_rot = (s->s_rot + 3) & 3;  // rotate right: new logical k = old k - 1
+            s->dt_old1 = s->dt_old0;
+            s->dt_old0 = dt;
+            double t_new = s->t + dt;
+            s->steps++;
+            if (d.meas_row != 0xFFFFFFFFu && t_new >= d.meas_t0) {
+                double v = LM(d.x, d.meas_row);
+                if (s->m_have && s->m_prev_v < d.meas_level && v >= d.meas_level) {
+                    double tc = s->m_prev_t + (d.meas_level - s->m_prev_v) * (t_new - s->m_prev_t) / (v - s->m_prev_v);
+                    if (s->m_cross == 0) s->m_first = tc;
+                    s->m_last = tc;
+                    s->m_cross++;
+                }
+                s->m_prev_v = v;
+                s->m_prev_t = t_new;
+                s->m_have = 1;
+            }
+            // stepEndB (kernels/lane.zig:667-700).
+            s->t = t_new;
+            if (!o.fixed_step) {
+                double nb = next_bp(d, l, t_new + o.min_break);
+                if (s->bp_next != INFINITY) {
+                    double bp = s->bp_next;
+                    bool landed = s->bp_clamped ? fabs(t_new - bp) <= o.min_break
+                                                : (bp - t_new <= o.delmin || almost_equal_ulps(t_new, bp, 100));
+                    if (landed) {
+                        s->order = 1;
+                        double shrink = s->bp_save_dt;
+                        if (nb != INFINITY) shrink = fmin(shrink, nb - t_new);
+                        dt_next = fmin(dt_next, 0.1 * shrink);
+                    }
+                }
+                s->bp_next = nb;
+                s->bp_clamped = 0;
+                if (nb != INFINITY) {
+                    double to_bp = nb - t_new;
+                    if (to_bp < dt_next) {
+                        s->bp_save_dt = dt_next;
+                        dt_next = to_bp;
+                        s->bp_clamped = 1;
+                    }
+                }
+            }
+            s->dt = dt_next;
+            if (t_new + s->dt > o.t_stop) s->dt = o.t_stop - t_new;
+        }
+        __syncthreads();
     }
 }
 

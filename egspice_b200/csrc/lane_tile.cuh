@@ -1,0 +1,273 @@
+// The 32-lane tile: a CTA of kWarps warps owns 32 lanes of one template.
+// The element-parallel work of a Newton iteration (device evaluation, the
+// stamp gather, the update, limiter and gates) is spread over all warps;
+// the sequential LU chain runs on warp 0, one thread per lane.
+//
+// Device evaluation is split in two, the way the reference's GPU sink
+// writes per-contribution staging cells and reduces them into the planes
+// (src/device/eval.zig LaneSink :3732, hub reduce, lane_device.zig:77-98):
+// the instance phase writes each instance's contributions into its own
+// cells, then the gather phase sums, per Jacobian slot and per residual or
+// charge row, the cells that stamp there, in the order the host stamping
+// adds them (Circuit.zig stamp -> eval.zig evalRange), so a slot's sum is
+// the reference's sum bit for bit. No atomics, no races between warps.
+#pragma once
+
+#include "lane_engine.cuh"
+
+namespace espl {
+
+constexpr int kWarps = 4;
+constexpr int kTileThreads = kWarps * 32;
+constexpr uint32_t kNeg = 0x80000000u;
+
+// Cells per instance.
+constexpr uint32_t kResCells = 2;   // g, current
+constexpr uint32_t kCapCells = 2;   // c, q
+constexpr uint32_t kVsrcCells = 2;  // ib, branch residual
+constexpr uint32_t kIsrcCells = 1;  // value
+constexpr uint32_t kDioCells = 4;   // g, f, c, q
+constexpr uint32_t kMosCells = 15;  // fd, fs, fb, jd[4], js[4], jb[4]
+
+struct TileCtx {
+    const GroupDev* d;
+    uint32_t l;      // lane in the template
+    uint32_t lane;   // 0..31
+    uint32_t warp;   // 0..kWarps-1
+    bool valid;      // l < lanes
+};
+
+// ---------------------------------------------------------------------------
+// Instance phase: one instance of one kind at the lane's x, its limiter
+// state giving the linearization point (eval.zig:826-874).
+
+__device__ __forceinline__ void inst_eval(const GroupDev& d, uint32_t l, uint32_t t, int tran, double tm) {
+    const uint32_t P = d.P;
+    const double* __restrict__ x = d.x;
+    double* __restrict__ cells = d.cells;
+    uint32_t i = t;
+    if (i < d.n_res) {
+        uint32_t tp = d.res_t[2 * i], tn = d.res_t[2 * i + 1];
+        double v = LM(x, tp) - LM(x, tn);
+        double r = LM(d.res_r, i);
+        uint32_t c = d.c_res + kResCells * i;
+        LM(cells, c) = 1.0 / r;
+        LM(cells, c + 1) = v / r;
+        return;
+    }
+    i -= d.n_res;
+    if (i < d.n_cap) {
+        uint32_t tp = d.cap_t[2 * i], tn = d.cap_t[2 * i + 1];
+        double v = LM(x, tp) - LM(x, tn);
+        double cc = LM(d.cap_c, i);
+        uint32_t c = d.c_cap + kCapCells * i;
+        LM(cells, c) = cc;
+        LM(cells, c + 1) = cc * v;
+        return;
+    }
+    i -= d.n_cap;
+    if (i < d.n_vsrc) {
+        uint32_t tp = d.vsrc_t[3 * i], tn = d.vsrc_t[3 * i + 1], tb = d.vsrc_t[3 * i + 2];
+        const double* pp = d.vsrc_p;
+        uint32_t b9 = 9 * i;
+        double val = source_value(LM(pp, b9 + 0), LM(pp, b9 + 1), LM(pp, b9 + 2), LM(pp, b9 + 3), LM(pp, b9 + 4),
+                                  LM(pp, b9 + 5), LM(pp, b9 + 6), LM(pp, b9 + 7), LM(pp, b9 + 8), tran, tm);
+        uint32_t c = d.c_vsrc + kVsrcCells * i;
+        LM(cells, c) = LM(x, tb);
+        LM(cells, c + 1) = (LM(x, tp) - LM(x, tn)) - val;
+        return;
+    }
+    i -= d.n_vsrc;
+    if (i < d.n_isrc) {
+        const double* pp = d.isrc_p;
+        uint32_t b9 = 9 * i;
+        LM(cells, d.c_isrc + i) = source_value(LM(pp, b9 + 0), LM(pp, b9 + 1), LM(pp, b9 + 2), LM(pp, b9 + 3),
+                                               LM(pp, b9 + 4), LM(pp, b9 + 5), LM(pp, b9 + 6), LM(pp, b9 + 7),
+                                               LM(pp, b9 + 8), tran, tm);
+        return;
+    }
+    i -= d.n_isrc;
+    if (i < d.n_dio) {
+        uint32_t ta = d.dio_t[2 * i], tc = d.dio_t[2 * i + 1];
+        const double* dd = d.dio_d;
+        uint32_t b = DiodePrep::count * i;
+        double vd = LM(x, ta) - LM(x, tc);
+        double vl = LM(d.lim_dio, i);
+        double id, gd, qd, cd;
+        diode_core(LM(dd, b + DiodePrep::is), LM(dd, b + DiodePrep::vte), LM(dd, b + DiodePrep::gmin),
+                   LM(dd, b + DiodePrep::cjo), LM(dd, b + DiodePrep::cjo_t), LM(dd, b + DiodePrep::vj_t),
+                   LM(dd, b + DiodePrep::mt), LM(dd, b + DiodePrep::fc), LM(dd, b + DiodePrep::tt), vl, id, gd, qd, cd);
+        uint32_t c = d.c_dio + kDioCells * i;
+        LM(cells, c) = gd;
+        LM(cells, c + 1) = id + gd * (vd - vl);
+        bool charge = LM(dd, b + DiodePrep::cjo) > 0.0 || LM(dd, b + DiodePrep::tt) > 0.0;
+        LM(cells, c + 2) = charge ? cd : 0.0;
+        LM(cells, c + 3) = charge ? qd + cd * (vd - vl) : 0.0;
+        return;
+    }
+    i -= d.n_dio;
+    if (i < d.n_mos) {
+        const uint32_t* tmv = d.mos_t + 4 * i;
+        const double* md = d.mos_d;
+        uint32_t b = Mos1Prep::count * i;
+        double ty = LM(md, b + Mos1Prep::type);
+        double xd = LM(x, tmv[0]), xg = LM(x, tmv[1]), xs = LM(x, tmv[2]), xb = LM(x, tmv[3]);
+        double vgs = ty * (xg - xs), vds = ty * (xd - xs), vbs = ty * (xb - xs);
+        double lgs = LM(d.lim_mos, 3 * i), lds = LM(d.lim_mos, 3 * i + 1), lbs = LM(d.lim_mos, 3 * i + 2);
+        Mos1Out o;
+        mos1_core(ty, LM(md, b + Mos1Prep::vt), LM(md, b + Mos1Prep::beta), LM(md, b + Mos1Prep::lambda),
+                  LM(md, b + Mos1Prep::gamma), LM(md, b + Mos1Prep::phit), LM(md, b + Mos1Prep::von0),
+                  LM(md, b + Mos1Prep::isat), LM(md, b + Mos1Prep::gmin), lgs, lds, lbs, o);
+        double dgs = vgs - lgs, dds = vds - lds, dbs = vbs - lbs;
+        double gm = o.mode * o.gm, gds = o.mode * o.gds, gmbs = o.mode * o.gmbs;
+        double ich = o.mode * o.id + gm * dgs + gds * dds + gmbs * dbs;
+        double ibd = o.ibd + o.gbd * (dbs - dds);
+        double ibs = o.ibs + o.gbs * dbs;
+        double gsum = gm + gds + gmbs;
+        uint32_t c = d.c_mos + kMosCells * i;
+        LM(cells, c + 0) = ty * ich - ty * ibd;
+        LM(cells, c + 1) = -ty * ich - ty * ibs;
+        LM(cells, c + 2) = ty * ibd + ty * ibs;
+        LM(cells, c + 3) = gds + o.gbd;
+        LM(cells, c + 4) = gm;
+        LM(cells, c + 5) = -gsum;
+        LM(cells, c + 6) = gmbs - o.gbd;
+        LM(cells, c + 7) = -gds;
+        LM(cells, c + 8) = -gm;
+        LM(cells, c + 9) = gsum + o.gbs;
+        LM(cells, c + 10) = -gmbs - o.gbs;
+        LM(cells, c + 11) = -o.gbd;
+        LM(cells, c + 12) = 0.0;
+        LM(cells, c + 13) = -o.gbs;
+        LM(cells, c + 14) = o.gbd + o.gbs;
+        return;
+    }
+    i -= d.n_mos;
+    if (i == 0) LM(cells, d.c_pin) = LM(x, 0);  // the ground pin's residual term
+}
+
+__device__ __forceinline__ uint32_t n_instances(const GroupDev& d) {
+    return d.n_res + d.n_cap + d.n_vsrc + d.n_isrc + d.n_dio + d.n_mos + 1;
+}
+
+// Limiter state of instance t (MOS1 or diode) at the seeds (cold) or at
+// the image of `xs` (warm). Other kinds have none.
+__device__ __forceinline__ void inst_seed(const GroupDev& d, uint32_t l, uint32_t t, int cold, const double* xs) {
+    const uint32_t P = d.P;
+    uint32_t base = d.n_res + d.n_cap + d.n_vsrc + d.n_isrc;
+    if (t < base) return;
+    uint32_t i = t - base;
+    if (i < d.n_dio) {
+        LM(d.lim_dio, i) = LM(xs, d.dio_t[2 * i]) - LM(xs, d.dio_t[2 * i + 1]);
+        return;
+    }
+    i -= d.n_dio;
+    if (i >= d.n_mos) return;
+    const uint32_t* tmv = d.mos_t + 4 * i;
+    uint32_t b = Mos1Prep::count * i;
+    const double* md = d.mos_d;
+    if (cold) {
+        LM(d.lim_mos, 3 * i) = LM(md, b + Mos1Prep::vgs_seed);
+        LM(d.lim_mos, 3 * i + 1) = 0.0;
+        LM(d.lim_mos, 3 * i + 2) = -1.0;
+    } else {
+        double ty = LM(md, b + Mos1Prep::type);
+        double xsrc = LM(xs, tmv[2]);
+        LM(d.lim_mos, 3 * i) = ty * (LM(xs, tmv[1]) - xsrc);
+        LM(d.lim_mos, 3 * i + 1) = ty * (LM(xs, tmv[0]) - xsrc);
+        LM(d.lim_mos, 3 * i + 2) = ty * (LM(xs, tmv[3]) - xsrc);
+    }
+}
+
+// The limiter pass of instance t with snapLimited (eval.zig:1115-1171):
+// true when it clamped.
+__device__ __forceinline__ bool inst_limit(const GroupDev& d, uint32_t l, uint32_t t) {
+    const uint32_t P = d.P;
+    const double* x = d.x;
+    const double eps16 = 16 * 2.220446049250313e-16;
+    uint32_t base = d.n_res + d.n_cap + d.n_vsrc + d.n_isrc;
+    if (t < base) return false;
+    uint32_t i = t - base;
+    if (i < d.n_dio) {
+        double xa = LM(x, d.dio_t[2 * i]), xc = LM(x, d.dio_t[2 * i + 1]);
+        double vd = xa - xc;
+        uint32_t b = DiodePrep::count * i;
+        double v = pnjlim(vd, LM(d.lim_dio, i), LM(d.dio_d, b + DiodePrep::vte), LM(d.dio_d, b + DiodePrep::vcrit));
+        if (fabs(v - vd) <= eps16 * fmax(fabs(xa), fabs(xc))) v = vd;
+        LM(d.lim_dio, i) = v;
+        return v != vd;
+    }
+    i -= d.n_dio;
+    if (i >= d.n_mos) return false;
+    const uint32_t* tmv = d.mos_t + 4 * i;
+    uint32_t b = Mos1Prep::count * i;
+    const double* md = d.mos_d;
+    double ty = LM(md, b + Mos1Prep::type);
+    double xd = LM(x, tmv[0]), xg = LM(x, tmv[1]), xs = LM(x, tmv[2]), xb = LM(x, tmv[3]);
+    double cgs = ty * (xg - xs), cds = ty * (xd - xs), cbs = ty * (xb - xs);
+    double vgs = cgs, vds = cds, vbs = cbs;
+    mos1_limit(LM(md, b + Mos1Prep::vt), LM(md, b + Mos1Prep::gamma), LM(md, b + Mos1Prep::phit),
+               LM(md, b + Mos1Prep::von0), LM(md, b + Mos1Prep::vcrit), LM(d.lim_mos, 3 * i),
+               LM(d.lim_mos, 3 * i + 1), LM(d.lim_mos, 3 * i + 2), vgs, vds, vbs);
+    double tol = eps16 * fmax(fmax(fabs(xd), fabs(xg)), fmax(fabs(xs), fabs(xb)));
+    if (fabs(vgs - cgs) <= tol) vgs = cgs;
+    if (fabs(vds - cds) <= tol) vds = cds;
+    if (fabs(vbs - cbs) <= tol) vbs = cbs;
+    LM(d.lim_mos, 3 * i) = vgs;
+    LM(d.lim_mos, 3 * i + 1) = vds;
+    LM(d.lim_mos, 3 * i + 2) = vbs;
+    return (vgs != cgs) | (vds != cds) | (vbs != cbs);
+}
+
+__device__ __forceinline__ double gather_sum(const double* __restrict__ cells, uint32_t P, uint32_t l,
+                                             const uint32_t* __restrict__ ptr, const uint32_t* __restrict__ list,
+                                             uint32_t k) {
+    double s = 0.0;
+    for (uint32_t e = ptr[k]; e < ptr[k + 1]; e++) {
+        uint32_t c = list[e];
+        double v = cells[(size_t)(c & ~kNeg) * P + l];
+        s += (c & kNeg) ? -v : v;
+    }
+    return s;
+}
+
+// Gather phase: A (G + ag0 C, with gmin on the diagonals), the residual
+// with the companion rows and gmin load, and the row charges.
+__device__ __forceinline__ double gather_slot(const GroupDev& d, uint32_t l, uint32_t p, const Companion& cp,
+                                              double gmin) {
+    const uint32_t P = d.P;
+    double g = gather_sum(d.cells, P, l, d.g_ptr, d.g_cell, p);
+    double a = g;
+    if (cp.on) {
+        double c = gather_sum(d.cells, P, l, d.c_ptr, d.c_cell, p);
+        a = g + cp.ag0 * c;
+    }
+    if (gmin > 0.0 && d.slot_diag[p]) a += gmin;
+    LM(d.a, p) = a;
+    return a;
+}
+
+__device__ __forceinline__ double gather_row(const GroupDev& d, uint32_t l, uint32_t i, const Companion& cp,
+                                             double gmin) {
+    const uint32_t P = d.P;
+    double r = gather_sum(d.cells, P, l, d.r_ptr, d.r_cell, i);
+    if (cp.on) {
+        double q = gather_sum(d.cells, P, l, d.q_ptr, d.q_cell, i);
+        LM(d.qrow, i) = q;
+        double dq = cp.ag0 * (q - LM(d.q1, i));
+        double base = r + dq;
+        r = cp.method == 1 ? base - cp.ag1 * LM(d.ip, i) : base;
+    }
+    if (gmin > 0.0) r += gmin * LM(d.x, i);
+    LM(d.rhs, i) = r;
+    return r;
+}
+
+// Row charges without a Newton (the transient start and the tape's charge
+// planes are read from them).
+__device__ __forceinline__ void gather_charge_row(const GroupDev& d, uint32_t l, uint32_t i) {
+    const uint32_t P = d.P;
+    LM(d.qrow, i) = gather_sum(d.cells, P, l, d.q_ptr, d.q_cell, i);
+}
+
+}  // namespace espl

@@ -216,8 +216,8 @@ typedef struct {
     uint64_t launches;
     uint64_t lane_iterations;
     uint64_t lane_steps;
-    uint32_t dense_peels;     /* lanes that took a dense-peel slot in the last launch */
-    uint32_t peel_overflow;   /* lanes the full slot pool turned away */
+    uint32_t dense_peels;     /* dense re-pivoting solves of failed replays, since the last reset */
+    uint32_t peel_overflow;   /* reserved (0) */
 } espl_stats;
 espl_status espl_get_stats(espl_lanes *h, espl_stats *out);
 
