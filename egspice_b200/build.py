@@ -10,7 +10,8 @@ SRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libespice_lanes.so")
 SOURCES = ["espice_lanes.cu", "tape.cpp"]
-HEADERS = ["lane_engine.cuh", "lane_kernels.cuh", "lane_models.cuh", "tape.h", "../../include/espice_lanes.h"]
+HEADERS = ["lane_engine.cuh", "lane_kernels.cuh", "lane_models.cuh", "lane_smem.cuh", "lane_tile.cuh", "tape.h",
+           "../../include/espice_lanes.h"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
          "--expt-relaxed-constexpr", "-Xptxas", "-v"]

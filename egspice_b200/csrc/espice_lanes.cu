@@ -20,9 +20,18 @@ using namespace espl;
 namespace {
 
 constexpr uint32_t kBlock = kTileThreads;
-// Shared-memory budget per tile for the shared LU chain (two tiles per SM
-// of 228 KB with the static tile state).
-constexpr uint32_t kSmemBudget = 100 * 1024;
+
+// The tiles of the Newton launches whose templates keep the same number of
+// tiles resident per SM: one launch per class, each on its own stream, with
+// the shared memory its largest template needs.
+struct LaunchClass {
+    uint32_t smem = 0;        // dynamic shared memory per tile
+    uint32_t per_sm = 0;      // resident tiles per SM at that size
+    std::vector<uint32_t> tiles;
+    uint32_t* d_tiles = nullptr;
+    cudaStream_t stream = nullptr;  // null: the handle's stream
+    cudaEvent_t done = nullptr;
+};
 constexpr uint32_t kGround = ESPL_GROUND;
 
 uint32_t terms_of(uint32_t kind) {
@@ -89,7 +98,6 @@ struct Group {
 
 struct espl_lanes {
     int device = 0;
-    uint32_t smem_bytes = 0;   // dynamic shared memory of the Newton launches
     uint32_t precision = ESPL_FP64;
     std::vector<Group> groups;
     uint32_t n_warps = 0, total_lanes = 0;
@@ -105,6 +113,8 @@ struct espl_lanes {
     TranParams tran{};
     bool tran_ready = false;
     std::vector<LaneState> h_state;
+    std::vector<LaunchClass> classes;
+    cudaEvent_t fork = nullptr;
 };
 
 namespace {
@@ -380,6 +390,22 @@ espl_status alloc_group(espl_lanes* h, Group& g) {
 #define UP(field, vec) if ((s = dupload(h, own, &d.field, vec))) return s
     UP(col_ptr, g.col_ptr);
     UP(row_idx, g.row_idx);
+    {
+        // The row view: per row, its entries' columns and slots by column.
+        std::vector<uint32_t> rptr(g.n + 1, 0), rcol(g.nnz), rpos(g.nnz);
+        for (uint32_t p = 0; p < g.nnz; p++) rptr[g.row_idx[p] + 1]++;
+        for (uint32_t i = 0; i < g.n; i++) rptr[i + 1] += rptr[i];
+        std::vector<uint32_t> fill(rptr.begin(), rptr.end() - 1);
+        for (uint32_t c = 0; c < g.n; c++)
+            for (uint32_t p = g.col_ptr[c]; p < g.col_ptr[c + 1]; p++) {
+                uint32_t e = fill[g.row_idx[p]]++;
+                rcol[e] = c;
+                rpos[e] = p;
+            }
+        UP(rt_ptr, rptr);
+        UP(rt_col, rcol);
+        UP(rt_pos, rpos);
+    }
     UP(diag, g.diag);
     UP(cur_row, g.cur_row);
     UP(res_t, g.kinds[ESPL_RES].term);
@@ -441,8 +467,90 @@ espl_status alloc_group(espl_lanes* h, Group& g) {
     return ESPL_OK;
 }
 
-TileMap launch_map(espl_lanes* h) { return TileMap{h->d_groups, h->d_warp_group, h->n_warps}; }
+TileMap launch_map(espl_lanes* h) { return TileMap{h->d_groups, h->d_warp_group, nullptr, h->n_warps}; }
 uint32_t grid_of(espl_lanes* h) { return h->n_warps; }
+
+// Launches `fn(map, grid, smem, stream)` once per class, the classes after
+// the first on their own streams, forked from and joined back into the
+// handle's stream.
+template <typename F>
+espl_status launch_classes(espl_lanes* h, F fn) {
+    CK(cudaEventRecord(h->fork, h->stream));
+    for (size_t k = 0; k < h->classes.size(); k++) {
+        LaunchClass& c = h->classes[k];
+        cudaStream_t st = k == 0 ? h->stream : c.stream;
+        if (k) CK(cudaStreamWaitEvent(st, h->fork, 0));
+        TileMap m{h->d_groups, h->d_warp_group, c.d_tiles, (uint32_t)c.tiles.size()};
+        fn(m, (uint32_t)c.tiles.size(), c.smem, st);
+        CK(cudaGetLastError());
+        if (k) CK(cudaEventRecord(c.done, st));
+    }
+    for (size_t k = 1; k < h->classes.size(); k++) CK(cudaStreamWaitEvent(h->stream, h->classes[k].done, 0));
+    return ESPL_OK;
+}
+
+void free_classes(espl_lanes* h) {
+    for (auto& c : h->classes) {
+        cudaFree(c.d_tiles);
+        if (c.stream) cudaStreamDestroy(c.stream);
+        if (c.done) cudaEventDestroy(c.done);
+    }
+    h->classes.clear();
+}
+
+// Shared-memory plan of every template and the launch classes: templates
+// whose LU chain fits the per-block opt-in limit run it in shared memory;
+// templates are grouped by how many of their tiles fit an SM together.
+template <bool MIXED>
+espl_status plan_classes(espl_lanes* h) {
+    int dev = h->device, optin = 0;
+    CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    cudaFuncAttributes fs, ft;
+    CK(cudaFuncGetAttributes(&fs, k_static<MIXED>));
+    CK(cudaFuncGetAttributes(&ft, k_tran<MIXED>));
+    int max_dyn = optin - (int)std::max(fs.sharedSizeBytes, ft.sharedSizeBytes);
+    CK(cudaFuncSetAttribute(k_static<MIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn));
+    CK(cudaFuncSetAttribute(k_tran<MIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn));
+    free_classes(h);
+    std::vector<uint32_t> bytes(h->groups.size(), 0), per(h->groups.size(), 0);
+    for (size_t i = 0; i < h->groups.size(); i++) {
+        Group& g = h->groups[i];
+        SmemPlan sp = smem_plan(g.n, g.nnz, g.dev.nnz_l, g.dev.nnz_u, MIXED);
+        g.dev.smem_ok = sp.bytes <= (uint32_t)max_dyn ? 1u : 0u;
+        bytes[i] = g.dev.smem_ok ? sp.bytes : 0u;
+        int a = 0, b = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_tran<MIXED>, kBlock, bytes[i]));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_static<MIXED>, kBlock, bytes[i]));
+        per[i] = (uint32_t)std::max(1, std::min(a, b));
+    }
+    // classes by resident tiles per SM, the one with the most tiles first
+    std::vector<uint32_t> keys(per.begin(), per.end());
+    std::sort(keys.begin(), keys.end());
+    keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
+    for (uint32_t key : keys) {
+        LaunchClass c;
+        c.per_sm = key;
+        for (size_t i = 0; i < h->groups.size(); i++) {
+            if (per[i] != key) continue;
+            c.smem = std::max(c.smem, bytes[i]);
+            for (uint32_t t = 0; t < h->groups[i].P / 32; t++) c.tiles.push_back(h->groups[i].tile0 + t);
+        }
+        h->classes.push_back(std::move(c));
+    }
+    std::stable_sort(h->classes.begin(), h->classes.end(),
+                     [](const LaunchClass& a, const LaunchClass& b) { return a.tiles.size() > b.tiles.size(); });
+    for (size_t k = 0; k < h->classes.size(); k++) {
+        LaunchClass& c = h->classes[k];
+        CK(cudaMalloc(&c.d_tiles, sizeof(uint32_t) * c.tiles.size()));
+        CK(cudaMemcpyAsync(c.d_tiles, c.tiles.data(), sizeof(uint32_t) * c.tiles.size(), cudaMemcpyHostToDevice,
+                           h->stream));
+        if (k) {
+            CK(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+            CK(cudaEventCreateWithFlags(&c.done, cudaEventDisableTiming));
+        }
+    }
+    return ESPL_OK;
+}
 
 espl_status push_descs(espl_lanes* h) {
     std::vector<GroupDev> descs;
@@ -495,21 +603,8 @@ espl_status retape(espl_lanes* h, int tran, double dt) {
             if ((s = dalloc(h, own, &d.ux32, (size_t)d.nnz_u * P))) return s;
         }
     }
-    // Templates whose LU chain fits a tile's shared memory run it there; the
-    // launch carries the largest such footprint.
-    uint32_t need = 0;
-    for (auto& g : h->groups) {
-        SmemPlan sp = smem_plan(g.n, g.nnz, g.dev.nnz_l, g.dev.nnz_u, h->precision == ESPL_MIXED);
-        g.dev.smem_ok = sp.bytes <= kSmemBudget ? 1u : 0u;
-        if (g.dev.smem_ok) need = std::max(need, sp.bytes);
-    }
-    h->smem_bytes = need;
-    if (need) {
-        CK(cudaFuncSetAttribute(k_static<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
-        CK(cudaFuncSetAttribute(k_static<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
-        CK(cudaFuncSetAttribute(k_tran<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
-        CK(cudaFuncSetAttribute(k_tran<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
-    }
+    espl_status s = h->precision == ESPL_MIXED ? plan_classes<true>(h) : plan_classes<false>(h);
+    if (s) return s;
     return push_descs(h);
 }
 
@@ -530,11 +625,13 @@ NewtonParams newton_params(const espl_newton_opts& o, uint32_t precision) {
 
 espl_status run_static(espl_lanes* h, const NewtonParams& np, int tran) {
     CK(cudaEventRecord(h->ev0, h->stream));
-    if (np.mixed)
-        k_static<true><<<grid_of(h), kBlock, h->smem_bytes, h->stream>>>(launch_map(h), np, h->d_state, tran);
-    else
-        k_static<false><<<grid_of(h), kBlock, h->smem_bytes, h->stream>>>(launch_map(h), np, h->d_state, tran);
-    CK(cudaGetLastError());
+    espl_status s = launch_classes(h, [&](const TileMap& m, uint32_t grid, uint32_t smem, cudaStream_t st) {
+        if (np.mixed)
+            k_static<true><<<grid, kBlock, smem, st>>>(m, np, h->d_state, tran);
+        else
+            k_static<false><<<grid, kBlock, smem, st>>>(m, np, h->d_state, tran);
+    });
+    if (s) return s;
     CK(cudaEventRecord(h->ev1, h->stream));
     CK(cudaEventSynchronize(h->ev1));
     float ms = 0;
@@ -581,6 +678,7 @@ espl_status espl_create(const espl_netlist* nets, uint32_t n_nets, const espl_cr
     if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(ESPL_DRIVER);
     cudaEventCreate(&h->ev0);
     cudaEventCreate(&h->ev1);
+    cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming);
     h->groups.resize(n_nets);
     uint32_t lane0 = 0, warp0 = 0;
     for (uint32_t i = 0; i < n_nets; i++) {
@@ -640,8 +738,10 @@ espl_status espl_destroy(espl_lanes* h) {
     cudaFree(h->d_state);
     cudaFree(h->d_mos_raw);
     cudaFree(h->d_dio_raw);
+    free_classes(h);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->fork) cudaEventDestroy(h->fork);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return ESPL_OK;
@@ -781,11 +881,13 @@ espl_status espl_device_launch(espl_lanes* h, uint32_t max_steps, espl_step_repo
     espl_newton_opts op{t.reltol, t.abstol, t.vntol, 0.0, t.residual_tol, t.max_iter, 0};
     NewtonParams np = newton_params(op, h->precision);
     CK(cudaEventRecord(h->ev0, h->stream));
-    if (np.mixed)
-        k_tran<true><<<grid_of(h), kBlock, h->smem_bytes, h->stream>>>(launch_map(h), t, np, h->d_state);
-    else
-        k_tran<false><<<grid_of(h), kBlock, h->smem_bytes, h->stream>>>(launch_map(h), t, np, h->d_state);
-    CK(cudaGetLastError());
+    espl_status s = launch_classes(h, [&](const TileMap& m, uint32_t grid, uint32_t smem, cudaStream_t st) {
+        if (np.mixed)
+            k_tran<true><<<grid, kBlock, smem, st>>>(m, t, np, h->d_state);
+        else
+            k_tran<false><<<grid, kBlock, smem, st>>>(m, t, np, h->d_state);
+    });
+    if (s) return s;
     CK(cudaEventRecord(h->ev1, h->stream));
     CK(cudaEventSynchronize(h->ev1));
     float ms = 0;

@@ -39,6 +39,7 @@ struct GroupDev {
     uint32_t has_charge, meas_row;
     double meas_level, meas_t0;
     const uint32_t *col_ptr, *row_idx, *prow, *q, *pinv, *lp, *li, *up, *ui, *flags, *void_slots, *diag;
+    const uint32_t *rt_ptr, *rt_col, *rt_pos;  // row view of the pattern: per row, (column, slot) by column
     const uint8_t* cur_row;
     const uint32_t *res_t, *res_s, *cap_t, *cap_s, *vsrc_t, *vsrc_s, *isrc_t, *dio_t, *dio_s, *mos_t, *mos_s;
     const double *res_r, *cap_c, *vsrc_p, *isrc_p, *dio_d, *mos_d;

@@ -7,23 +7,28 @@
 #pragma once
 
 #include <climits>
+#include <type_traits>
 
 #include "lane_smem.cuh"
 
 namespace espl {
 
+// The tiles of one launch: block b runs tile tiles[b] (all tiles in order
+// when tiles is null); tile_group maps a tile to its template.
 struct TileMap {
     const GroupDev* groups;
     const uint32_t* tile_group;
+    const uint32_t* tiles;
     uint32_t n_tiles;
 };
 
 __device__ __forceinline__ TileCtx tile_ctx(const TileMap& m) {
     TileCtx c;
-    c.d = &m.groups[m.tile_group[blockIdx.x]];
+    c.tile = m.tiles ? m.tiles[blockIdx.x] : blockIdx.x;
+    c.d = &m.groups[m.tile_group[c.tile]];
     c.lane = threadIdx.x & 31;
     c.warp = threadIdx.x >> 5;
-    c.l = (blockIdx.x - c.d->tile0) * 32 + c.lane;
+    c.l = (c.tile - c.d->tile0) * 32 + c.lane;
     c.valid = c.l < c.d->lanes;
     return c;
 }
@@ -55,6 +60,7 @@ __device__ void newton_tile(const TileCtx& c, LaneState* s, const NewtonParams& 
     const GroupDev& d = *c.d;
     const uint32_t l = c.l, P = d.P, lane = c.lane, warp = c.warp;
     const uint32_t ninst = n_instances(d);
+    using T = typename std::conditional<MIXED, float, double>::type;
     const bool sm = dsm != nullptr;
     SmemTile st{};
     if (sm) st = smem_tile(dsm, smem_plan(d.n, d.nnz, d.nnz_l, d.nnz_u, MIXED));
@@ -82,12 +88,12 @@ __device__ void newton_tile(const TileCtx& c, LaneState* s, const NewtonParams& 
         __syncthreads();
         if (act) {
             if (sm) {
-                for (uint32_t p = warp; p < d.nnz; p += kWarps) st.a[p * 32 + lane] = gather_slot(d, l, p, cp, o.gmin);
-                for (uint32_t i = warp; i < d.n; i += kWarps) st.rhs[i * 32 + lane] = gather_row(d, l, i, cp, o.gmin);
+                T* sa = static_cast<T*>(st.a);
+                for (uint32_t p = warp; p < d.nnz; p += kWarps) sa[p * 32 + lane] = (T)gather_slot(d, l, p, cp, o.gmin);
             } else {
                 for (uint32_t p = warp; p < d.nnz; p += kWarps) gather_slot(d, l, p, cp, o.gmin);
-                for (uint32_t i = warp; i < d.n; i += kWarps) gather_row(d, l, i, cp, o.gmin);
             }
+            for (uint32_t i = warp; i < d.n; i += kWarps) gather_row(d, l, i, cp, o.gmin);
         }
         __syncthreads();
         if (it == 0) {
@@ -117,58 +123,56 @@ __device__ void newton_tile(const TileCtx& c, LaneState* s, const NewtonParams& 
             }
         }
         // The LU chain: warp 0, one thread per lane; in shared memory when the
-        // template fits there.
-        if (warp == 0 && act && sm) {
+        // template fits there (FP32 tiles: only the lanes still in FP32).
+        if (warp == 0 && act) {
             bool use32 = MIXED && !s->fp64;
-            int rc = use32 ? refactor_smem<float>(d, st, lane) : 1;
-            if (use32 && rc != 0) {
-                s->fp64 = 1;
-                s->fallbacks++;
-                use32 = false;
-            }
-            if (!use32) {
-                rc = refactor_smem<double>(d, st, lane);
-                if (rc == 2) {
-                    spill_factor<double>(d, st, lane, l);
-                    rc = replay_holds64(d, l) ? 0 : 1;
-                }
-            }
-            if (rc == 0) {
-                if (use32) {
-                    solve_smem<float>(d, st, lane, st.rhs, st.dx);
-                    for (uint32_t r = 0; r < o.refine; r++) refine_smem(d, st, lane);
+            bool done = false;
+            if (sm && (use32 || !MIXED)) {
+                int rc = refactor_smem<T>(d, st, lane, l);
+                if (MIXED && rc != 0) {
+                    s->fp64 = 1;
+                    s->fallbacks++;
+                    use32 = false;
                 } else {
-                    solve_smem<double>(d, st, lane, st.rhs, st.dx);
+                    if (!MIXED && rc == 2) {
+                        spill_factor<T>(d, st, lane, l);
+                        rc = replay_holds64(d, l) ? 0 : 1;
+                    }
+                    if (rc == 0) {
+                        solve_smem<T>(d, st, lane, l);
+                        if (MIXED)
+                            for (uint32_t r = 0; r < o.refine; r++) refine_smem(d, st, lane, l);
+                    } else if (!peel_dense(d, l, *s)) {
+                        sh.bits[lane] |= kSingular;
+                        sh.active[lane] = 0;
+                        s->iterations = it;
+                    }
+                    done = true;
                 }
-                for (uint32_t i = 0; i < d.n; i++) LM(d.dx, i) = st.dx[i * 32 + lane];
-            } else if (!peel_dense(d, l, *s)) {
-                sh.bits[lane] |= kSingular;
-                sh.active[lane] = 0;
-                s->iterations = it;
             }
-        } else if (warp == 0 && act) {
-            bool use32 = MIXED && !s->fp64;
-            if (use32 && refactor32(d, l)) {
-                s->fp64 = 1;
-                s->fallbacks++;
-                use32 = false;
-            }
-            bool fail = false;
-            if (!use32) {
-                int rc = refactor64(d, l);
-                fail = rc == 1 || (rc == 2 && !replay_holds64(d, l));
-            }
-            if (fail) {
-                if (!peel_dense(d, l, *s)) {
-                    sh.bits[lane] |= kSingular;
-                    sh.active[lane] = 0;
-                    s->iterations = it;
+            if (!done) {
+                if (use32 && refactor32(d, l)) {
+                    s->fp64 = 1;
+                    s->fallbacks++;
+                    use32 = false;
                 }
-            } else if (use32) {
-                solve32(d, l, d.rhs, d.dx);
-                for (uint32_t r = 0; r < o.refine; r++) refine_mixed(d, l);
-            } else {
-                solve64(d, l, d.rhs, d.dx);
+                bool fail = false;
+                if (!use32) {
+                    int rc = refactor64(d, l);
+                    fail = rc == 1 || (rc == 2 && !replay_holds64(d, l));
+                }
+                if (fail) {
+                    if (!peel_dense(d, l, *s)) {
+                        sh.bits[lane] |= kSingular;
+                        sh.active[lane] = 0;
+                        s->iterations = it;
+                    }
+                } else if (use32) {
+                    solve32(d, l, d.rhs, d.dx);
+                    for (uint32_t r = 0; r < o.refine; r++) refine_mixed(d, l);
+                } else {
+                    solve64(d, l, d.rhs, d.dx);
+                }
             }
         }
         __syncthreads();
@@ -252,7 +256,7 @@ __device__ unsigned char* tile_smem(const GroupDev& d) {
 }
 
 template <bool MIXED>
-__global__ void __launch_bounds__(kTileThreads) k_static(TileMap m, NewtonParams o, LaneState* st, int tran) {
+__global__ void __launch_bounds__(kTileThreads, 4) k_static(TileMap m, NewtonParams o, LaneState* st, int tran) {
     __shared__ TileShared sh;
     TileCtx c = tile_ctx(m);
     LaneState* s = (c.warp == 0 && c.valid) ? &st[c.d->lane0 + c.l] : nullptr;
@@ -268,7 +272,7 @@ __global__ void __launch_bounds__(kTileThreads) k_prep(TileMap m, const double* 
     if (!c.valid) return;
     const GroupDev& d = *c.d;
     const uint32_t P = d.P, l = c.l;
-    uint32_t g = m.tile_group[blockIdx.x];
+    uint32_t g = m.tile_group[c.tile];
     const double* mr = mos_raw[g];
     const double* dr = dio_raw[g];
     double* md = const_cast<double*>(d.mos_d);
@@ -363,37 +367,46 @@ __device__ __forceinline__ double* ring_slot(const GroupDev& d, uint32_t rot, ui
     return d.sring + (size_t)((rot + logical) & 3) * d.n_sites * d.P;
 }
 
-// stepBound (kernels/lane.zig:257-297) over the lane's sites.
-__device__ double step_bound(const GroupDev& d, uint32_t l, uint32_t rot, uint32_t method, uint32_t cur_method,
-                             double dt, double dt1, double dt2, double reltol, double abstol, double chgtol,
-                             double trtol, double ag0, double ag1) {
+// stepBound (kernels/lane.zig:257-297) over the sites j = j0, j0 + stride,
+// ... of a lane, for the integration method m0 and, with `two`, also m1 (the
+// trial order of a backward-Euler step), sharing the loads. The minimum
+// over the sites is order-free, so warps can split them and take the
+// minimum of their parts; a NaN in a site's inputs or bound poisons the
+// method's result (bad0, bad1).
+__device__ void step_bound_part(const GroupDev& d, uint32_t l, uint32_t rot, uint32_t m0, uint32_t m1, bool two,
+                                uint32_t cur_method, double dt, double dt1, double dt2, double reltol, double abstol,
+                                double chgtol, double trtol, double ag0, double ag1, uint32_t j0, uint32_t stride,
+                                double& v0, double& v1, bool& bad0, bool& bad1) {
     const uint32_t P = d.P;
     const uint32_t ns = d.n_sites;
-    double coeff = method == 0 ? 0.5 : method == 1 ? 0.08333333333 : 0.2222222222;
+    double c0 = m0 == 0 ? 0.5 : m0 == 1 ? 0.08333333333 : 0.2222222222;
+    double c1 = m1 == 0 ? 0.5 : m1 == 1 ? 0.08333333333 : 0.2222222222;
     double sum01 = dt + dt1, sum12 = dt1 + dt2, sum012 = dt + (dt1 + dt2);
-    double vmin = INFINITY, poison = 0.0;
     const double *r0 = ring_slot(d, rot, 0), *r1 = ring_slot(d, rot, 1);
     const double *r2 = ring_slot(d, rot, 2), *r3 = ring_slot(d, rot, 3);
-    for (uint32_t j = 0; j < ns; j++) {
+    for (uint32_t j = j0; j < ns; j += stride) {
         double qc = LM(r0, j), qp = LM(r1, j), qp2 = LM(r2, j), qp3 = LM(r3, j), i_p = LM(d.sip, j);
         double i_new = cur_method == 1 ? ag0 * (qc - qp) - ag1 * i_p : ag0 * (qc - qp);
         double volttol = abstol + reltol * fmax(fabs(i_new), fabs(i_p));
         double chargetol = reltol * fmax(fmax(fabs(qc), fabs(qp)), chgtol) / dt;
         double tol = fmax(volttol, chargetol);
-        poison += (qc - qc) + (qp - qp) + (qp2 - qp2) + (i_p - i_p);
+        bool in_bad = isnan((qc - qc) + (qp - qp) + (qp2 - qp2) + (i_p - i_p));
+        bool bad3 = isnan(qp3 - qp3);
         double f12 = (qp - qp2) / dt1;
-        double dd = ((qc - qp) / dt - f12) / sum01;
-        if (method != 0) {
-            poison += qp3 - qp3;
-            double f123 = (f12 - (qp2 - qp3) / dt2) / sum12;
-            dd = (dd - f123) / sum012;
+        double dd0 = ((qc - qp) / dt - f12) / sum01;
+        double f123 = 0.0;
+        if (m0 != 0 || (two && m1 != 0)) f123 = (f12 - (qp2 - qp3) / dt2) / sum12;
+        double dd = m0 != 0 ? (dd0 - f123) / sum012 : dd0;
+        double del = trtol * tol / fmax(abstol, c0 * fabs(dd));
+        bad0 |= in_bad || (m0 != 0 && bad3) || del != del;
+        v0 = fmin(v0, del);
+        if (two) {
+            double dd1 = m1 != 0 ? (dd0 - f123) / sum012 : dd0;
+            double del1 = trtol * tol / fmax(abstol, c1 * fabs(dd1));
+            bad1 |= in_bad || (m1 != 0 && bad3) || del1 != del1;
+            v1 = fmin(v1, del1);
         }
-        double del = trtol * tol / fmax(abstol, coeff * fabs(dd));
-        poison += del == del ? 0.0 : del;
-        vmin = fmin(vmin, del);
     }
-    if (isnan(poison)) return NAN;
-    return method == 0 ? vmin : sqrt(vmin);
 }
 
 // Transient start from the operating point in x: histories, the site ring,
@@ -459,7 +472,7 @@ __global__ void __launch_bounds__(kTileThreads) k_tran_init(TileMap m, TranParam
 // (Newton and LTE rejections, order promotion), the accepted-step history
 // advance, stepEndB (breakpoints, next dt) and the period measure.
 template <bool MIXED>
-__global__ void __launch_bounds__(kTileThreads) k_tran(TileMap m, TranParams o, NewtonParams no, LaneState* st) {
+__global__ void __launch_bounds__(kTileThreads, 4) k_tran(TileMap m, TranParams o, NewtonParams no, LaneState* st) {
     __shared__ TileShared sh;
     TileCtx c = tile_ctx(m);
     const GroupDev& d = *c.d;
@@ -520,6 +533,25 @@ __global__ void __launch_bounds__(kTileThreads) k_tran(TileMap m, TranParams o, 
             for (uint32_t j = warp; j < ns; j += kWarps) LM(r0, j) = LM(d.cells, d.site_cell[j]);
         }
         __syncthreads();
+        // The LTE bound of a converged LTE-controlled step, its sites split
+        // over the warps (partial minima in pg / pmax, poison bits in pflag).
+        {
+            double v0 = INFINITY, v1 = INFINITY;
+            bool b0 = false, b1 = false;
+            if (conv && !o.fixed_step && ns > 0) {
+                const LaneState& ls = st[d.lane0 + l];
+                if (ls.steps > 0) {
+                    uint32_t method = sh.method[lane];
+                    step_bound_part(d, l, ls.s_rot, method, o.method, method == 0, method, ls.dt, ls.dt_old0,
+                                    ls.dt_old1, o.reltol, o.abstol, o.chgtol, o.trtol, sh.ag0[lane], sh.ag1[lane],
+                                    warp, kWarps, v0, v1, b0, b1);
+                }
+            }
+            sh.pg[warp][lane] = v0;
+            sh.pmax[warp][lane] = dbits(v1);
+            sh.pflag[warp][lane] = (b0 ? 1u : 0u) | (b1 ? 2u : 0u);
+        }
+        __syncthreads();
         // stepEndA (kernels/lane.zig:563-654).
         if (warp == 0) {
             uint32_t acc = 0;
@@ -546,12 +578,15 @@ __global__ void __launch_bounds__(kTileThreads) k_tran(TileMap m, TranParams o, 
                         dt_next = dt;
                         if (s->order == 1 && o.method != 0) s->order = 2;
                     } else if (ns > 0 && s->steps > 0) {
-                        double del = step_bound(d, l, s->s_rot, method, method, dt, s->dt_old0, s->dt_old1, o.reltol,
-                                                o.abstol, o.chgtol, o.trtol, sh.ag0[lane], sh.ag1[lane]);
-                        double del2 = method == 0 ? step_bound(d, l, s->s_rot, o.method, method, dt, s->dt_old0,
-                                                               s->dt_old1, o.reltol, o.abstol, o.chgtol, o.trtol,
-                                                               sh.ag0[lane], sh.ag1[lane])
-                                                  : del;
+                        double v0 = INFINITY, v1 = INFINITY;
+                        uint32_t bad = 0;
+                        for (int w = 0; w < kWarps; w++) {
+                            v0 = fmin(v0, sh.pg[w][lane]);
+                            v1 = fmin(v1, bitsd(sh.pmax[w][lane]));
+                            bad |= sh.pflag[w][lane];
+                        }
+                        double del = (bad & 1u) ? NAN : method == 0 ? v0 : sqrt(v0);
+                        double del2 = method == 0 ? ((bad & 2u) ? NAN : o.method == 0 ? v1 : sqrt(v1)) : del;
                         if (!(del >= 0.9 * dt)) {
                             reject = true;
                             s->rejects++;

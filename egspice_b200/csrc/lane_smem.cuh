@@ -1,15 +1,18 @@
-// The LU chain of a small template entirely in shared memory. The tape's
-// index words are staged once per launch by bulk copies (cp.async.bulk, the
-// TMA's 1-D form) completing on an mbarrier; the gather phase writes the
-// assembled matrix and right-hand side into the tile's shared copies as well
-// as to global memory; the replay, the triangular solves and the FP32
-// refinement then touch only shared memory, one thread per lane, with the
-// 32 lanes interleaved (element i of lane j at i * 32 + j: a warp reads one
-// element of all lanes as 32 consecutive words, conflict-free).
+// The LU chain of a template in shared memory. The tape's index words are
+// staged once per launch by bulk copies (cp.async.bulk, the TMA's 1-D form)
+// completing on an mbarrier; the gather phase writes the assembled matrix
+// into the tile's shared copy (in the factor's precision) as well as to
+// global memory (FP64); the replay and the triangular solves then touch
+// only shared memory, one thread per lane, with the 32 lanes interleaved
+// (element i of lane j at i * 32 + j: a warp reads one element of all lanes
+// as 32 consecutive words, conflict-free). Right-hand sides, the Newton step
+// and the FP64 refinement residual stay in global memory, read once per
+// row.
 //
-// Same operations in the same order as refactor64/refactor32 and
-// solve64/solve32 (src/solver/kernels/lane.zig:56-157), so a lane's factor
-// and step are bitwise the global path's.
+// FP64 tiles run the same operations in the same order as refactor64 and
+// solve64 (src/solver/kernels/lane.zig:56-157), so a lane's factor and step
+// are bitwise the global path's; FP32 tiles those of refactor32/solve32 and
+// refine_mixed. A mixed lane that falls back to FP64 takes the global path.
 #pragma once
 
 #include "lane_tile.cuh"
@@ -48,8 +51,10 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 
 // Tape arrays staged per tile, in this order; each starts on a 16-byte
 // boundary and is copied padded to a 16-byte multiple (the global buffers
-// carry that padding).
-enum TapeArr { T_Q, T_COLPTR, T_ROWIDX, T_PROW, T_UP, T_UI, T_LP, T_LI, T_FLAGS, T_PINV, T_COUNT };
+// carry that padding). The row view (RTPTR/RTCOL/RTPOS: per row, the
+// columns and slots of its entries by ascending column) feeds the FP32
+// tiles' refinement residual.
+enum TapeArr { T_Q, T_COLPTR, T_PROW, T_UP, T_UI, T_LP, T_LI, T_FLAGS, T_PINV, T_RTPTR, T_RTCOL, T_RTPOS, T_COUNT };
 
 __host__ __device__ inline uint32_t pad4(uint32_t words) { return (words + 3u) & ~3u; }
 
@@ -57,18 +62,18 @@ struct SmemPlan {
     uint32_t off[T_COUNT];   // u32-word offsets of the tape arrays
     uint32_t len[T_COUNT];   // padded word counts
     uint32_t tape_words;     // total (multiple of 4)
-    uint32_t a_off, rhs_off, w_off, y_off, lx_off, ux_off, ud_off, r_off, c_off, dx_off;  // byte offsets
+    uint32_t a_off, w_off, y_off, lx_off, ux_off, ud_off;  // byte offsets
     uint32_t bytes;          // total dynamic shared memory of the tile
 };
 
 // Layout of the tile's dynamic shared memory for template sizes (n, nnz,
-// nnz_l, nnz_u). The LU arrays hold doubles, so a mixed lane can fall back to
-// FP64 in place; an FP32 view uses the first half of each. `mixed` adds the
-// refinement vectors.
-__host__ __device__ inline SmemPlan smem_plan(uint32_t n, uint32_t nnz, uint32_t nl, uint32_t nu, bool mixed) {
-    const uint32_t es = 8;
+// nnz_l, nnz_u): the staged tape, then A, the work vectors w and y, and
+// the factor, all in FP32 for `f32` tiles and FP64 otherwise.
+__host__ __device__ inline SmemPlan smem_plan(uint32_t n, uint32_t nnz, uint32_t nl, uint32_t nu, bool f32) {
+    const uint32_t es = f32 ? 4u : 8u;
     SmemPlan p;
-    uint32_t words[T_COUNT] = {n, n + 1, nnz, nnz, n + 1, nu, n + 1, nl, n, n};
+    uint32_t words[T_COUNT] = {n, n + 1, nnz, n + 1, nu, n + 1, nl, n, n,
+                               f32 ? n + 1 : 0u, f32 ? nnz : 0u, f32 ? nnz : 0u};
     uint32_t o = 4;  // the first 16 bytes hold the mbarrier
     for (int k = 0; k < T_COUNT; k++) {
         p.off[k] = o;
@@ -79,15 +84,7 @@ __host__ __device__ inline SmemPlan smem_plan(uint32_t n, uint32_t nnz, uint32_t
     uint32_t b = o * 4;
     b = (b + 15u) & ~15u;
     p.a_off = b;
-    b += nnz * 32u * 8u;
-    p.rhs_off = b;
-    b += n * 32u * 8u;
-    p.dx_off = b;
-    b += n * 32u * 8u;
-    p.r_off = b;           // FP64 refinement residual
-    if (mixed) b += n * 32u * 8u;
-    p.c_off = b;           // FP64 refinement correction
-    if (mixed) b += n * 32u * 8u;
+    b += nnz * 32u * es;
     p.w_off = b;
     b += n * 32u * es;
     p.y_off = b;
@@ -103,9 +100,8 @@ __host__ __device__ inline SmemPlan smem_plan(uint32_t n, uint32_t nnz, uint32_t
 }
 
 struct SmemTile {
-    const uint32_t *q, *col_ptr, *row_idx, *prow, *up, *ui, *lp, *li, *flags, *pinv;
-    double *a, *rhs, *dx, *r, *corr;
-    void *w, *y, *lx, *ux, *ud;
+    const uint32_t *q, *col_ptr, *prow, *up, *ui, *lp, *li, *flags, *pinv, *rt_ptr, *rt_col, *rt_pos;
+    void *a, *w, *y, *lx, *ux, *ud;
 };
 
 __device__ __forceinline__ SmemTile smem_tile(unsigned char* base, const SmemPlan& p) {
@@ -113,7 +109,6 @@ __device__ __forceinline__ SmemTile smem_tile(unsigned char* base, const SmemPla
     SmemTile t;
     t.q = u + p.off[T_Q];
     t.col_ptr = u + p.off[T_COLPTR];
-    t.row_idx = u + p.off[T_ROWIDX];
     t.prow = u + p.off[T_PROW];
     t.up = u + p.off[T_UP];
     t.ui = u + p.off[T_UI];
@@ -121,11 +116,10 @@ __device__ __forceinline__ SmemTile smem_tile(unsigned char* base, const SmemPla
     t.li = u + p.off[T_LI];
     t.flags = u + p.off[T_FLAGS];
     t.pinv = u + p.off[T_PINV];
-    t.a = reinterpret_cast<double*>(base + p.a_off);
-    t.rhs = reinterpret_cast<double*>(base + p.rhs_off);
-    t.dx = reinterpret_cast<double*>(base + p.dx_off);
-    t.r = reinterpret_cast<double*>(base + p.r_off);
-    t.corr = reinterpret_cast<double*>(base + p.c_off);
+    t.rt_ptr = u + p.off[T_RTPTR];
+    t.rt_col = u + p.off[T_RTCOL];
+    t.rt_pos = u + p.off[T_RTPOS];
+    t.a = base + p.a_off;
     t.w = base + p.w_off;
     t.y = base + p.y_off;
     t.lx = base + p.lx_off;
@@ -140,7 +134,8 @@ __device__ __forceinline__ SmemTile smem_tile(unsigned char* base, const SmemPla
 // vectors start at zero.
 __device__ bool stage_tape(const GroupDev& d, unsigned char* base, const SmemPlan& p) {
     uint64_t* bar = reinterpret_cast<uint64_t*>(base);
-    const uint32_t* src[T_COUNT] = {d.q, d.col_ptr, d.row_idx, d.prow, d.up, d.ui, d.lp, d.li, d.flags, d.pinv};
+    const uint32_t* src[T_COUNT] = {d.q, d.col_ptr, d.prow, d.up, d.ui, d.lp, d.li, d.flags, d.pinv,
+                                    d.rt_ptr, d.rt_col, d.rt_pos};
     if (threadIdx.x == 0) {
         mbar_init(bar, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -152,7 +147,7 @@ __device__ bool stage_tape(const GroupDev& d, unsigned char* base, const SmemPla
     }
     // zero w and y (both precisions share the invariant: all-zero bits)
     uint32_t* wz = reinterpret_cast<uint32_t*>(base + p.w_off);
-    uint32_t nz = (p.lx_off - p.w_off) / 4u;
+    uint32_t nz = (p.lx_off - p.w_off) / 4u;  // w and y
     for (uint32_t i = threadIdx.x; i < nz; i += blockDim.x) wz[i] = 0u;
     __syncthreads();
     bool ok = true;
@@ -173,21 +168,22 @@ __device__ bool stage_tape(const GroupDev& d, unsigned char* base, const SmemPla
 // The replay in shared memory; T = double or float. 0 holds, 1 pivot or
 // store failure, 2 only a multiplier past 1 / pivot_tol.
 template <typename T>
-__device__ int refactor_smem(const GroupDev& d, const SmemTile& s, uint32_t lane) {
+__device__ int refactor_smem(const GroupDev& d, const SmemTile& s, uint32_t lane, uint32_t l) {
     T* __restrict__ w = static_cast<T*>(s.w);
     T* __restrict__ lx = static_cast<T*>(s.lx);
     T* __restrict__ ux = static_cast<T*>(s.ux);
     T* __restrict__ ud = static_cast<T*>(s.ud);
-    const double* __restrict__ a = s.a;
+    const T* __restrict__ a = static_cast<const T*>(s.a);
+    const uint32_t P = d.P;
     for (uint32_t v = 0; v < d.n_void; v++)
-        if (SL(a, d.void_slots[v]) != 0.0) return 1;
+        if (LM(d.a, d.void_slots[v]) != 0.0) return 1;
     constexpr bool f64 = sizeof(T) == 8;
     bool bad = false, nonfinite = false;
     const T growth = (T)1e-12;
     const T inf = (T)INFINITY;
     for (uint32_t k = 0; k < d.n; k++) {
         uint32_t c = s.q[k];
-        for (uint32_t p = s.col_ptr[c]; p < s.col_ptr[c + 1]; p++) SL(w, s.prow[p]) = (T)SL(a, p);
+        for (uint32_t p = s.col_ptr[c]; p < s.col_ptr[c + 1]; p++) SL(w, s.prow[p]) = SL(a, p);
         for (uint32_t p = s.up[k]; p < s.up[k + 1]; p++) {
             uint32_t i = s.ui[p];
             T uki = SL(w, i);
@@ -263,15 +259,14 @@ __device__ int refactor_smem(const GroupDev& d, const SmemTile& s, uint32_t lane
     return 0;
 }
 
-// out = -A^-1 b through the shared factors (luSolve with neg), b and out by
-// original row/column in shared memory.
+// Forward and back substitution of y in place through the shared factors
+// (luSolve's two sweeps).
 template <typename T>
-__device__ void solve_smem(const GroupDev& d, const SmemTile& s, uint32_t lane, const double* b, double* out) {
+__device__ __forceinline__ void subst_smem(const GroupDev& d, const SmemTile& s, uint32_t lane) {
     T* __restrict__ y = static_cast<T*>(s.y);
     const T* __restrict__ lx = static_cast<const T*>(s.lx);
     const T* __restrict__ ux = static_cast<const T*>(s.ux);
     const T* __restrict__ ud = static_cast<const T*>(s.ud);
-    for (uint32_t r = 0; r < d.n; r++) SL(y, s.pinv[r]) = (T)(-SL(b, r));
     for (uint32_t k = 0; k < d.n; k++) {
         T yk = SL(y, k);
         if (yk != (T)0)
@@ -283,20 +278,36 @@ __device__ void solve_smem(const GroupDev& d, const SmemTile& s, uint32_t lane, 
         if (zk != (T)0)
             for (uint32_t p = s.up[k]; p < s.up[k + 1]; p++) SL(y, s.ui[p]) -= SL(ux, p) * zk;
     }
-    for (uint32_t j = 0; j < d.n; j++) SL(out, s.q[j]) = (double)SL(y, j);
 }
 
-// One FP64-residual refinement sweep of an FP32 solve in shared memory:
-// r = rhs + A dx, dx += -A^-1 r.
-__device__ void refine_smem(const GroupDev& d, const SmemTile& s, uint32_t lane) {
-    for (uint32_t i = 0; i < d.n; i++) SL(s.r, i) = SL(s.rhs, i);
-    for (uint32_t c = 0; c < d.n; c++) {
-        double xc = SL(s.dx, c);
-        if (xc == 0.0) continue;
-        for (uint32_t p = s.col_ptr[c]; p < s.col_ptr[c + 1]; p++) SL(s.r, s.row_idx[p]) += SL(s.a, p) * xc;
+// dx = -A^-1 rhs through the shared factors (luSolve with neg); rhs and dx
+// are the lane's global rows.
+template <typename T>
+__device__ void solve_smem(const GroupDev& d, const SmemTile& s, uint32_t lane, uint32_t l) {
+    const uint32_t P = d.P;
+    T* __restrict__ y = static_cast<T*>(s.y);
+    for (uint32_t r = 0; r < d.n; r++) SL(y, s.pinv[r]) = (T)(-LM(d.rhs, r));
+    subst_smem<T>(d, s, lane);
+    for (uint32_t j = 0; j < d.n; j++) LM(d.dx, s.q[j]) = (double)SL(y, j);
+}
+
+// One FP64-residual refinement sweep of an FP32 solve (refine_mixed):
+// r = rhs + A dx row by row, the products added by ascending column as the
+// column sweep adds them (columns with dx = 0 skipped), then
+// dx += -A^-1 r through the FP32 factors.
+__device__ void refine_smem(const GroupDev& d, const SmemTile& s, uint32_t lane, uint32_t l) {
+    const uint32_t P = d.P;
+    float* __restrict__ y = static_cast<float*>(s.y);
+    for (uint32_t i = 0; i < d.n; i++) {
+        double r = LM(d.rhs, i);
+        for (uint32_t e = s.rt_ptr[i]; e < s.rt_ptr[i + 1]; e++) {
+            double xc = LM(d.dx, s.rt_col[e]);
+            if (xc != 0.0) r += LM(d.a, s.rt_pos[e]) * xc;
+        }
+        SL(y, s.pinv[i]) = (float)(-r);
     }
-    solve_smem<float>(d, s, lane, s.r, s.corr);
-    for (uint32_t i = 0; i < d.n; i++) SL(s.dx, i) += SL(s.corr, i);
+    subst_smem<float>(d, s, lane);
+    for (uint32_t j = 0; j < d.n; j++) LM(d.dx, s.q[j]) += (double)SL(y, j);
 }
 
 // Copies a shared factor out to the lane's global factor arrays, for the

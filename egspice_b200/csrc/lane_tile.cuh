@@ -31,6 +31,7 @@ constexpr uint32_t kMosCells = 15;  // fd, fs, fb, jd[4], js[4], jb[4]
 
 struct TileCtx {
     const GroupDev* d;
+    uint32_t tile;   // tile index over all templates
     uint32_t l;      // lane in the template
     uint32_t lane;   // 0..31
     uint32_t warp;   // 0..kWarps-1
