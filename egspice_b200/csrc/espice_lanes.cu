@@ -99,6 +99,7 @@ struct Group {
 struct espl_lanes {
     int device = 0;
     uint32_t precision = ESPL_FP64;
+    uint32_t refine_sweeps = 0;
     std::vector<Group> groups;
     uint32_t n_warps = 0, total_lanes = 0;
     GroupDev* d_groups = nullptr;
@@ -376,12 +377,16 @@ espl_status alloc_group(espl_lanes* h, Group& g) {
         if (pl.sites.size() != d.n_sites) return fail(h, ESPL_INVALID_ARGUMENT, "site count mismatch");
         std::vector<uint32_t> ptr, flat;
         csr(pl.g, ptr, flat);
+        d.n_gc = (uint32_t)flat.size();
         if ((s = dupload(h, own, &d.g_ptr, ptr)) || (s = dupload(h, own, &d.g_cell, flat))) return s;
         csr(pl.c, ptr, flat);
+        d.n_cc = (uint32_t)flat.size();
         if ((s = dupload(h, own, &d.c_ptr, ptr)) || (s = dupload(h, own, &d.c_cell, flat))) return s;
         csr(pl.r, ptr, flat);
+        d.n_rc = (uint32_t)flat.size();
         if ((s = dupload(h, own, &d.r_ptr, ptr)) || (s = dupload(h, own, &d.r_cell, flat))) return s;
         csr(pl.q, ptr, flat);
+        d.n_qc = (uint32_t)flat.size();
         if ((s = dupload(h, own, &d.q_ptr, ptr)) || (s = dupload(h, own, &d.q_cell, flat))) return s;
         if ((s = dupload(h, own, &d.site_cell, pl.sites))) return s;
         if ((s = dupload(h, own, &d.slot_diag, pl.slot_diag))) return s;
@@ -515,9 +520,16 @@ espl_status plan_classes(espl_lanes* h) {
     std::vector<uint32_t> bytes(h->groups.size(), 0), per(h->groups.size(), 0);
     for (size_t i = 0; i < h->groups.size(); i++) {
         Group& g = h->groups[i];
-        SmemPlan sp = smem_plan(g.n, g.nnz, g.dev.nnz_l, g.dev.nnz_u, MIXED);
-        g.dev.smem_ok = sp.bytes <= (uint32_t)max_dyn ? 1u : 0u;
-        bytes[i] = g.dev.smem_ok ? sp.bytes : 0u;
+        g.dev.refine_rows = MIXED && h->refine_sweeps > 0 ? 1u : 0u;
+        g.dev.stage_mode = kStageNone;
+        for (uint32_t mode : {kStageLu, kStageIndex}) {
+            SmemPlan sp = smem_plan(g.dev, mode, MIXED);
+            if (sp.bytes <= (uint32_t)max_dyn) {
+                g.dev.stage_mode = mode;
+                bytes[i] = sp.bytes;
+                break;
+            }
+        }
         int a = 0, b = 0;
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_tran<MIXED>, kBlock, bytes[i]));
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_static<MIXED>, kBlock, bytes[i]));
@@ -608,7 +620,7 @@ espl_status retape(espl_lanes* h, int tran, double dt) {
     return push_descs(h);
 }
 
-NewtonParams newton_params(const espl_newton_opts& o, uint32_t precision) {
+NewtonParams newton_params(const espl_newton_opts& o, uint32_t precision, uint32_t refine) {
     NewtonParams p{};
     p.reltol = o.reltol;
     p.abstol = o.abstol;
@@ -619,7 +631,7 @@ NewtonParams newton_params(const espl_newton_opts& o, uint32_t precision) {
     p.init_fix = o.init_fix;
     p.mixed = precision == ESPL_MIXED;
     p.stall_ticks = 12;
-    p.refine = 1;
+    p.refine = p.mixed ? refine : 0;
     return p;
 }
 
@@ -665,6 +677,12 @@ espl_status espl_create(const espl_netlist* nets, uint32_t n_nets, const espl_cr
     espl_lanes* h = new espl_lanes();
     h->device = opts ? (int)opts->device : 0;
     h->precision = opts ? opts->precision : ESPL_FP64;
+    h->refine_sweeps = opts ? opts->refine_sweeps : 0;
+    if (opts && (opts->refine_sweeps > 4 || (opts->lanes_per_cta != 0 && opts->lanes_per_cta != 32) ||
+                 opts->precision > ESPL_MIXED)) {
+        delete h;
+        return ESPL_INVALID_ARGUMENT;
+    }
     auto bail = [&](espl_status s) {
         std::string e = h->err;
         espl_destroy(h);
@@ -802,7 +820,7 @@ espl_status espl_get_x(espl_lanes* h, uint32_t net, double* x) {
 espl_status espl_solve_static(espl_lanes* h, const espl_newton_opts* opts, espl_lane_newton* out) {
     if (!h || !opts) return ESPL_INVALID_ARGUMENT;
     if (opts->max_iter == 0 || opts->max_iter > 100000) return fail(h, ESPL_INVALID_ARGUMENT, "max_iter out of range");
-    NewtonParams np = newton_params(*opts, h->precision);
+    NewtonParams np = newton_params(*opts, h->precision, h->refine_sweeps);
     espl_status s = run_static(h, np, 0);
     if (s) return s;
     if (out) {
@@ -858,7 +876,7 @@ espl_status espl_init_steps(espl_lanes* h, const espl_tran_opts* o) {
     if (s) return s;
     if (seed(h, 1)) return ESPL_DRIVER;
     espl_newton_opts op{o->reltol, o->abstol, o->vntol, 0.0, o->residual_tol, 100, 1};
-    NewtonParams np = newton_params(op, h->precision);
+    NewtonParams np = newton_params(op, h->precision, h->refine_sweeps);
     s = run_static(h, np, 1);
     if (s) return s;
     // The step tape: the lead lane's G + C / dt at the operating point.
@@ -879,7 +897,7 @@ espl_status espl_device_launch(espl_lanes* h, uint32_t max_steps, espl_step_repo
     TranParams t = h->tran;
     t.launch_steps = max_steps ? max_steps : 1;
     espl_newton_opts op{t.reltol, t.abstol, t.vntol, 0.0, t.residual_tol, t.max_iter, 0};
-    NewtonParams np = newton_params(op, h->precision);
+    NewtonParams np = newton_params(op, h->precision, h->refine_sweeps);
     CK(cudaEventRecord(h->ev0, h->stream));
     espl_status s = launch_classes(h, [&](const TileMap& m, uint32_t grid, uint32_t smem, cudaStream_t st) {
         if (np.mixed)

@@ -56,8 +56,9 @@ struct GroupDev {
     const uint32_t *g_ptr, *g_cell, *c_ptr, *c_cell, *r_ptr, *r_cell, *q_ptr, *q_cell, *site_cell;
     const uint8_t* slot_diag;
     double* cells;
-    uint32_t smem_ok;     // the LU chain runs in shared memory (lane_smem.cuh)
-    uint32_t smem_pad;
+    uint32_t n_gc, n_cc, n_rc, n_qc;  // lengths of g_cell, c_cell, r_cell, q_cell
+    uint32_t stage_mode;  // what a tile stages in shared memory (lane_smem.cuh)
+    uint32_t refine_rows; // the row view is staged (FP32 refinement sweeps on)
 };
 
 struct LaneState {

@@ -34,14 +34,16 @@ __device__ __forceinline__ TileCtx tile_ctx(const TileMap& m) {
 }
 
 // Per-tile shared state of a Newton solve and a transient attempt.
+// Per-lane reductions over the warps go through shared atomics on
+// order-free quantities: maxima of non-negative doubles by their bit
+// patterns, minima likewise, and OR of flags.
 struct TileShared {
+    GroupDev gd;  // the tile's template descriptor, index arrays staged
     uint32_t active[32];
     uint32_t bits[32];
     uint32_t restore[32];
-    uint32_t pflag[kWarps][32];
-    unsigned long long pmax[kWarps][32];
-    unsigned long long pmax2[kWarps][32];
-    double pg[kWarps][32];
+    uint32_t accf[32];
+    unsigned long long acc0[32], acc1[32], acc2[32];
     double limit[32];
     double ag0[32], ag1[32], t[32], xfact[32], dt_next[32];
     uint32_t method[32], on[32], accept[32], rot[32];
@@ -61,13 +63,16 @@ __device__ void newton_tile(const TileCtx& c, LaneState* s, const NewtonParams& 
     const uint32_t l = c.l, P = d.P, lane = c.lane, warp = c.warp;
     const uint32_t ninst = n_instances(d);
     using T = typename std::conditional<MIXED, float, double>::type;
-    const bool sm = dsm != nullptr;
+    const bool sm = d.stage_mode == kStageLu;
     SmemTile st{};
-    if (sm) st = smem_tile(dsm, smem_plan(d.n, d.nnz, d.nnz_l, d.nnz_u, MIXED));
+    if (sm) st = smem_tile(dsm, smem_plan(d, kStageLu, MIXED));
     if (warp == 0) {
         sh.active[lane] = (c.valid && on) ? 1u : 0u;
         sh.bits[lane] = (o.init_fix ? kInitFix : 0u);
         sh.limit[lane] = kXPlausible;
+        sh.acc0[lane] = dbits(1.0);
+        sh.acc1[lane] = 0;
+        sh.acc2[lane] = 0;
         if (s) s->iterations = o.max_iter;
     }
     __syncthreads();
@@ -100,23 +105,23 @@ __device__ void newton_tile(const TileCtx& c, LaneState* s, const NewtonParams& 
             // plausibleLimit (kernels/lane.zig:202-214).
             double g = 1.0;
             unsigned long long xm = 0, fm = 0;
-            if (act)
+            if (act) {
                 for (uint32_t i = warp; i < d.n; i += kWarps) {
                     g = fmax(g, fabs(LM(d.a, d.diag[i])));
                     unsigned long long xb = dbits(fabs(LM(d.x, i))), fb = dbits(fabs(LM(d.rhs, i)));
                     xm = xm > xb ? xm : xb;
                     fm = fm > fb ? fm : fb;
                 }
-            sh.pg[warp][lane] = g;
-            sh.pmax[warp][lane] = xm;
-            sh.pmax2[warp][lane] = fm;
+                // g >= 1 and never NaN (fmax drops NaN): its bits order as it does
+                atomicMax(&sh.acc0[lane], dbits(g));
+                atomicMax(&sh.acc1[lane], xm);
+                atomicMax(&sh.acc2[lane], fm);
+            }
             __syncthreads();
             if (warp == 0 && act) {
-                for (int w = 1; w < kWarps; w++) {
-                    g = fmax(g, sh.pg[w][lane]);
-                    xm = xm > sh.pmax[w][lane] ? xm : sh.pmax[w][lane];
-                    fm = fm > sh.pmax2[w][lane] ? fm : sh.pmax2[w][lane];
-                }
+                g = bitsd(sh.acc0[lane]);
+                xm = sh.acc1[lane];
+                fm = sh.acc2[lane];
                 double scale = fmin(fmax(bitsd(xm), bitsd(fm) * g), 1e18);
                 if (isnan(bitsd(xm)) || isnan(bitsd(fm))) scale = NAN;
                 sh.limit[lane] = !(1e3 * scale > kXPlausible) ? kXPlausible : 1e3 * scale;
@@ -124,6 +129,10 @@ __device__ void newton_tile(const TileCtx& c, LaneState* s, const NewtonParams& 
         }
         // The LU chain: warp 0, one thread per lane; in shared memory when the
         // template fits there (FP32 tiles: only the lanes still in FP32).
+        if (warp == 0) {
+            sh.acc0[lane] = 0;
+            sh.accf[lane] = 0;
+        }
         if (warp == 0 && act) {
             bool use32 = MIXED && !s->fp64;
             bool done = false;
@@ -192,7 +201,7 @@ __device__ void newton_tile(const TileCtx& c, LaneState* s, const NewtonParams& 
                 unsigned long long b = dbits(score);
                 worst = worst > b ? worst : b;
             }
-        sh.pmax[warp][lane] = worst;
+        if (act) atomicMax(&sh.acc0[lane], worst);
         __syncthreads();
         // The limiter pass over instances; plausible and residual gates over rows.
         uint32_t flags = 0;
@@ -209,17 +218,13 @@ __device__ void newton_tile(const TileCtx& c, LaneState* s, const NewtonParams& 
                 if (!(fabs(LM(d.rhs, i)) <= tol)) flags |= kResidualMiss;
             }
         }
-        sh.pflag[warp][lane] = flags;
+        if (flags) atomicOr(&sh.accf[lane], flags);
         __syncthreads();
         if (warp == 0) {
             sh.restore[lane] = 0;
             if (act) {
-                unsigned long long wb = 0;
-                uint32_t f = 0;
-                for (int w = 0; w < kWarps; w++) {
-                    wb = wb > sh.pmax[w][lane] ? wb : sh.pmax[w][lane];
-                    f |= sh.pflag[w][lane];
-                }
+                unsigned long long wb = sh.acc0[lane];
+                uint32_t f = sh.accf[lane];
                 double scaled = bitsd(wb);
                 bool ok = !(f & kLimited) && it != 0 && !(scaled >= 1.0) && !(f & (kImplausible | kResidualMiss));
                 if (ok && (sh.bits[lane] & kInitFix)) {
@@ -246,22 +251,13 @@ __device__ void newton_tile(const TileCtx& c, LaneState* s, const NewtonParams& 
 
 extern __shared__ __align__(16) unsigned char g_dsm[];
 
-// Stages the tile's tape into shared memory when its template runs the LU
-// chain there; null otherwise (or when the bounded wait ran out).
-template <bool MIXED>
-__device__ unsigned char* tile_smem(const GroupDev& d) {
-    if (!d.smem_ok) return nullptr;
-    bool ok = stage_tape(d, g_dsm, smem_plan(d.n, d.nnz, d.nnz_l, d.nnz_u, MIXED));
-    return ok ? g_dsm : nullptr;
-}
-
 template <bool MIXED>
 __global__ void __launch_bounds__(kTileThreads, 4) k_static(TileMap m, NewtonParams o, LaneState* st, int tran) {
     __shared__ TileShared sh;
     TileCtx c = tile_ctx(m);
+    c.d = stage_template(*c.d, sh.gd, g_dsm, MIXED);
     LaneState* s = (c.warp == 0 && c.valid) ? &st[c.d->lane0 + c.l] : nullptr;
-    unsigned char* dsm = tile_smem<MIXED>(*c.d);
-    newton_tile<MIXED>(c, s, o, tran, false, true, sh, dsm);
+    newton_tile<MIXED>(c, s, o, tran, false, true, sh, g_dsm);
 }
 
 // Bias-independent prep per (instance, lane) from the raw lane-major rows,
@@ -475,11 +471,12 @@ template <bool MIXED>
 __global__ void __launch_bounds__(kTileThreads, 4) k_tran(TileMap m, TranParams o, NewtonParams no, LaneState* st) {
     __shared__ TileShared sh;
     TileCtx c = tile_ctx(m);
+    c.d = stage_template(*c.d, sh.gd, g_dsm, MIXED);
     const GroupDev& d = *c.d;
     const uint32_t P = d.P, l = c.l, lane = c.lane, warp = c.warp;
     const uint32_t ns = d.n_sites, ninst = n_instances(d);
     LaneState* s = (warp == 0 && c.valid) ? &st[d.lane0 + l] : nullptr;
-    unsigned char* dsm = tile_smem<MIXED>(d);
+    unsigned char* dsm = g_dsm;
     NewtonParams np = no;
     np.init_fix = 0;
     np.max_iter = o.max_iter;
@@ -528,13 +525,18 @@ __global__ void __launch_bounds__(kTileThreads, 4) k_tran(TileMap m, TranParams 
         // The last eval ran at the published x: its site charges are the
         // point's, logical slot 0 of the ring.
         bool conv = on && (sh.bits[lane] & kConverged);
+        if (warp == 0) {
+            sh.acc1[lane] = dbits(INFINITY);
+            sh.acc2[lane] = dbits(INFINITY);
+            sh.accf[lane] = 0;
+        }
         if (conv) {
             double* r0 = ring_slot(d, sh.rot[lane], 0);
             for (uint32_t j = warp; j < ns; j += kWarps) LM(r0, j) = LM(d.cells, d.site_cell[j]);
         }
         __syncthreads();
         // The LTE bound of a converged LTE-controlled step, its sites split
-        // over the warps (partial minima in pg / pmax, poison bits in pflag).
+        // over the warps (minima in acc1 / acc2, poison bits in accf).
         {
             double v0 = INFINITY, v1 = INFINITY;
             bool b0 = false, b1 = false;
@@ -547,9 +549,10 @@ __global__ void __launch_bounds__(kTileThreads, 4) k_tran(TileMap m, TranParams 
                                     warp, kWarps, v0, v1, b0, b1);
                 }
             }
-            sh.pg[warp][lane] = v0;
-            sh.pmax[warp][lane] = dbits(v1);
-            sh.pflag[warp][lane] = (b0 ? 1u : 0u) | (b1 ? 2u : 0u);
+            // the bounds are >= 0 (NaN ones only poison): their bits order as they do
+            if (v0 < INFINITY) atomicMin(&sh.acc1[lane], dbits(v0));
+            if (v1 < INFINITY) atomicMin(&sh.acc2[lane], dbits(v1));
+            if (b0 || b1) atomicOr(&sh.accf[lane], (b0 ? 1u : 0u) | (b1 ? 2u : 0u));
         }
         __syncthreads();
         // stepEndA (kernels/lane.zig:563-654).
@@ -578,13 +581,8 @@ __global__ void __launch_bounds__(kTileThreads, 4) k_tran(TileMap m, TranParams 
                         dt_next = dt;
                         if (s->order == 1 && o.method != 0) s->order = 2;
                     } else if (ns > 0 && s->steps > 0) {
-                        double v0 = INFINITY, v1 = INFINITY;
-                        uint32_t bad = 0;
-                        for (int w = 0; w < kWarps; w++) {
-                            v0 = fmin(v0, sh.pg[w][lane]);
-                            v1 = fmin(v1, bitsd(sh.pmax[w][lane]));
-                            bad |= sh.pflag[w][lane];
-                        }
+                        double v0 = bitsd(sh.acc1[lane]), v1 = bitsd(sh.acc2[lane]);
+                        uint32_t bad = sh.accf[lane];
                         double del = (bad & 1u) ? NAN : method == 0 ? v0 : sqrt(v0);
                         double del2 = method == 0 ? ((bad & 2u) ? NAN : o.method == 0 ? v1 : sqrt(v1)) : del;
                         if (!(del >= 0.9 * dt)) {

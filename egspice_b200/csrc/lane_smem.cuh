@@ -1,13 +1,18 @@
-// The LU chain of a template in shared memory. The tape's index words are
-// staged once per launch by bulk copies (cp.async.bulk, the TMA's 1-D form)
-// completing on an mbarrier; the gather phase writes the assembled matrix
-// into the tile's shared copy (in the factor's precision) as well as to
-// global memory (FP64); the replay and the triangular solves then touch
+// Shared-memory staging of a tile's template and the LU chain in shared
+// memory.
+//
+// Every lane of a template reads the same index words each Newton iteration
+// (instance terminals, the stamp gather lists, the pivot tape), so a tile
+// stages them once per launch by bulk copies (cp.async.bulk, the TMA's 1-D
+// form) completing on an mbarrier, and runs on a copy of its template
+// descriptor in shared memory whose index pointers are redirected to the
+// staged copies. When the factor fits as well, the gather phase writes the
+// assembled matrix into the tile's shared copy (in the factor's precision)
+// besides global memory (FP64), and the replay and triangular solves touch
 // only shared memory, one thread per lane, with the 32 lanes interleaved
 // (element i of lane j at i * 32 + j: a warp reads one element of all lanes
 // as 32 consecutive words, conflict-free). Right-hand sides, the Newton step
-// and the FP64 refinement residual stay in global memory, read once per
-// row.
+// and the FP64 refinement residual stay in global memory, read once per row.
 //
 // FP64 tiles run the same operations in the same order as refactor64 and
 // solve64 (src/solver/kernels/lane.zig:56-157), so a lane's factor and step
@@ -49,106 +54,223 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     return ok != 0;
 }
 
-// Tape arrays staged per tile, in this order; each starts on a 16-byte
-// boundary and is copied padded to a 16-byte multiple (the global buffers
-// carry that padding). The row view (RTPTR/RTCOL/RTPOS: per row, the
-// columns and slots of its entries by ascending column) feeds the FP32
-// tiles' refinement residual.
-enum TapeArr { T_Q, T_COLPTR, T_PROW, T_UP, T_UI, T_LP, T_LI, T_FLAGS, T_PINV, T_RTPTR, T_RTCOL, T_RTPOS, T_COUNT };
+// Index arrays a tile stages: the template's, then the tape, then the row
+// view (RTPTR/RTCOL/RTPOS: per row, the columns and slots of its entries by
+// ascending column) that the FP32 refinement residual reads. Each starts on
+// a 16-byte boundary and is copied padded to a 16-byte multiple (the global
+// buffers carry that padding); u8 arrays are copied as words.
+enum StageArr {
+    S_DIAG, S_VOID, S_CURROW, S_SLOTDIAG, S_RES_T, S_CAP_T, S_VSRC_T, S_DIO_T, S_MOS_T,
+    S_GPTR, S_GCELL, S_CPTR, S_CCELL, S_RPTR, S_RCELL, S_QPTR, S_QCELL, S_SITE,
+    S_Q, S_PINV, S_COLPTR, S_PROW, S_UP, S_UI, S_LP, S_LI, S_FLAGS,
+    S_RTPTR, S_RTCOL, S_RTPOS, S_COUNT
+};
+
+// Staging modes of a template: nothing, the index arrays, or the index
+// arrays and the LU chain.
+enum : uint32_t { kStageNone = 0, kStageIndex = 1, kStageLu = 2 };
 
 __host__ __device__ inline uint32_t pad4(uint32_t words) { return (words + 3u) & ~3u; }
 
+__host__ __device__ inline uint32_t stage_words(const GroupDev& d, int k) {
+    const bool rows = d.refine_rows != 0;
+    switch (k) {
+    case S_DIAG: return d.n;
+    case S_VOID: return d.n_void;
+    case S_CURROW: return (d.n + 3u) / 4u;
+    case S_SLOTDIAG: return (d.nnz + 3u) / 4u;
+    case S_RES_T: return 2 * d.n_res;
+    case S_CAP_T: return 2 * d.n_cap;
+    case S_VSRC_T: return 3 * d.n_vsrc;
+    case S_DIO_T: return 2 * d.n_dio;
+    case S_MOS_T: return 4 * d.n_mos;
+    case S_GPTR: return d.nnz + 1;
+    case S_GCELL: return d.n_gc;
+    case S_CPTR: return d.nnz + 1;
+    case S_CCELL: return d.n_cc;
+    case S_RPTR: return d.n + 1;
+    case S_RCELL: return d.n_rc;
+    case S_QPTR: return d.n + 1;
+    case S_QCELL: return d.n_qc;
+    case S_SITE: return d.n_sites;
+    case S_Q: return d.n;
+    case S_PINV: return d.n;
+    case S_COLPTR: return d.n + 1;
+    case S_PROW: return d.nnz;
+    case S_UP: return d.n + 1;
+    case S_UI: return d.nnz_u;
+    case S_LP: return d.n + 1;
+    case S_LI: return d.nnz_l;
+    case S_FLAGS: return d.n;
+    case S_RTPTR: return rows ? d.n + 1 : 0u;
+    case S_RTCOL: return rows ? d.nnz : 0u;
+    case S_RTPOS: return rows ? d.nnz : 0u;
+    default: return 0u;
+    }
+}
+
+__host__ __device__ inline const void* stage_src(const GroupDev& d, int k) {
+    switch (k) {
+    case S_DIAG: return d.diag;
+    case S_VOID: return d.void_slots;
+    case S_CURROW: return d.cur_row;
+    case S_SLOTDIAG: return d.slot_diag;
+    case S_RES_T: return d.res_t;
+    case S_CAP_T: return d.cap_t;
+    case S_VSRC_T: return d.vsrc_t;
+    case S_DIO_T: return d.dio_t;
+    case S_MOS_T: return d.mos_t;
+    case S_GPTR: return d.g_ptr;
+    case S_GCELL: return d.g_cell;
+    case S_CPTR: return d.c_ptr;
+    case S_CCELL: return d.c_cell;
+    case S_RPTR: return d.r_ptr;
+    case S_RCELL: return d.r_cell;
+    case S_QPTR: return d.q_ptr;
+    case S_QCELL: return d.q_cell;
+    case S_SITE: return d.site_cell;
+    case S_Q: return d.q;
+    case S_PINV: return d.pinv;
+    case S_COLPTR: return d.col_ptr;
+    case S_PROW: return d.prow;
+    case S_UP: return d.up;
+    case S_UI: return d.ui;
+    case S_LP: return d.lp;
+    case S_LI: return d.li;
+    case S_FLAGS: return d.flags;
+    case S_RTPTR: return d.rt_ptr;
+    case S_RTCOL: return d.rt_col;
+    case S_RTPOS: return d.rt_pos;
+    default: return nullptr;
+    }
+}
+
+__device__ inline void stage_redirect(GroupDev& d, int k, const void* p) {
+    const uint32_t* u = static_cast<const uint32_t*>(p);
+    switch (k) {
+    case S_DIAG: d.diag = u; break;
+    case S_VOID: d.void_slots = u; break;
+    case S_CURROW: d.cur_row = static_cast<const uint8_t*>(p); break;
+    case S_SLOTDIAG: d.slot_diag = static_cast<const uint8_t*>(p); break;
+    case S_RES_T: d.res_t = u; break;
+    case S_CAP_T: d.cap_t = u; break;
+    case S_VSRC_T: d.vsrc_t = u; break;
+    case S_DIO_T: d.dio_t = u; break;
+    case S_MOS_T: d.mos_t = u; break;
+    case S_GPTR: d.g_ptr = u; break;
+    case S_GCELL: d.g_cell = u; break;
+    case S_CPTR: d.c_ptr = u; break;
+    case S_CCELL: d.c_cell = u; break;
+    case S_RPTR: d.r_ptr = u; break;
+    case S_RCELL: d.r_cell = u; break;
+    case S_QPTR: d.q_ptr = u; break;
+    case S_QCELL: d.q_cell = u; break;
+    case S_SITE: d.site_cell = u; break;
+    case S_Q: d.q = u; break;
+    case S_PINV: d.pinv = u; break;
+    case S_COLPTR: d.col_ptr = u; break;
+    case S_PROW: d.prow = u; break;
+    case S_UP: d.up = u; break;
+    case S_UI: d.ui = u; break;
+    case S_LP: d.lp = u; break;
+    case S_LI: d.li = u; break;
+    case S_FLAGS: d.flags = u; break;
+    case S_RTPTR: d.rt_ptr = u; break;
+    case S_RTCOL: d.rt_col = u; break;
+    case S_RTPOS: d.rt_pos = u; break;
+    default: break;
+    }
+}
+
 struct SmemPlan {
-    uint32_t off[T_COUNT];   // u32-word offsets of the tape arrays
-    uint32_t len[T_COUNT];   // padded word counts
-    uint32_t tape_words;     // total (multiple of 4)
-    uint32_t a_off, w_off, y_off, lx_off, ux_off, ud_off;  // byte offsets
+    uint32_t off[S_COUNT];   // u32-word offsets of the staged arrays
+    uint32_t len[S_COUNT];   // padded word counts
+    uint32_t idx_words;      // total staged words (multiple of 4)
+    uint32_t a_off, w_off, lx_off, ux_off, ud_off;  // byte offsets of the LU chain (kStageLu)
     uint32_t bytes;          // total dynamic shared memory of the tile
 };
 
-// Layout of the tile's dynamic shared memory for template sizes (n, nnz,
-// nnz_l, nnz_u): the staged tape, then A, the work vectors w and y, and
-// the factor, all in FP32 for `f32` tiles and FP64 otherwise.
-__host__ __device__ inline SmemPlan smem_plan(uint32_t n, uint32_t nnz, uint32_t nl, uint32_t nu, bool f32) {
+// Layout of the tile's dynamic shared memory in staging mode `mode`: the
+// mbarrier, the index arrays, then (kStageLu) A, the work vector w (the
+// solves' y aliases it: w is all-zero between replays, and each solve
+// zeroes y after use), and the factor, in FP32 for `f32` tiles and FP64
+// otherwise.
+__host__ __device__ inline SmemPlan smem_plan(const GroupDev& d, uint32_t mode, bool f32) {
+    SmemPlan p{};
+    if (mode == kStageNone) return p;
     const uint32_t es = f32 ? 4u : 8u;
-    SmemPlan p;
-    uint32_t words[T_COUNT] = {n, n + 1, nnz, n + 1, nu, n + 1, nl, n, n,
-                               f32 ? n + 1 : 0u, f32 ? nnz : 0u, f32 ? nnz : 0u};
     uint32_t o = 4;  // the first 16 bytes hold the mbarrier
-    for (int k = 0; k < T_COUNT; k++) {
+    for (int k = 0; k < S_COUNT; k++) {
         p.off[k] = o;
-        p.len[k] = pad4(words[k]);
+        p.len[k] = pad4(stage_words(d, k));
         o += p.len[k];
     }
-    p.tape_words = o - 4;
+    p.idx_words = o - 4;
     uint32_t b = o * 4;
-    b = (b + 15u) & ~15u;
-    p.a_off = b;
-    b += nnz * 32u * es;
-    p.w_off = b;
-    b += n * 32u * es;
-    p.y_off = b;
-    b += n * 32u * es;
-    p.lx_off = b;
-    b += nl * 32u * es;
-    p.ux_off = b;
-    b += nu * 32u * es;
-    p.ud_off = b;
-    b += n * 32u * es;
+    if (mode == kStageLu) {
+        b = (b + 15u) & ~15u;
+        p.a_off = b;
+        b += d.nnz * 32u * es;
+        p.w_off = b;
+        b += d.n * 32u * es;
+        p.lx_off = b;
+        b += d.nnz_l * 32u * es;
+        p.ux_off = b;
+        b += d.nnz_u * 32u * es;
+        p.ud_off = b;
+        b += d.n * 32u * es;
+    }
     p.bytes = (b + 15u) & ~15u;
     return p;
 }
 
 struct SmemTile {
-    const uint32_t *q, *col_ptr, *prow, *up, *ui, *lp, *li, *flags, *pinv, *rt_ptr, *rt_col, *rt_pos;
-    void *a, *w, *y, *lx, *ux, *ud;
+    void *a, *w, *lx, *ux, *ud;
 };
 
 __device__ __forceinline__ SmemTile smem_tile(unsigned char* base, const SmemPlan& p) {
-    const uint32_t* u = reinterpret_cast<const uint32_t*>(base);
     SmemTile t;
-    t.q = u + p.off[T_Q];
-    t.col_ptr = u + p.off[T_COLPTR];
-    t.prow = u + p.off[T_PROW];
-    t.up = u + p.off[T_UP];
-    t.ui = u + p.off[T_UI];
-    t.lp = u + p.off[T_LP];
-    t.li = u + p.off[T_LI];
-    t.flags = u + p.off[T_FLAGS];
-    t.pinv = u + p.off[T_PINV];
-    t.rt_ptr = u + p.off[T_RTPTR];
-    t.rt_col = u + p.off[T_RTCOL];
-    t.rt_pos = u + p.off[T_RTPOS];
     t.a = base + p.a_off;
     t.w = base + p.w_off;
-    t.y = base + p.y_off;
     t.lx = base + p.lx_off;
     t.ux = base + p.ux_off;
     t.ud = base + p.ud_off;
     return t;
 }
 
-// Stages the tape by bulk copies; thread 0 issues them, every thread of
-// warp 0 waits (bounded: a copy of in-bounds memory completes, and past the
-// bound the flag tells the caller to stay on the global path). The work
-// vectors start at zero.
-__device__ bool stage_tape(const GroupDev& d, unsigned char* base, const SmemPlan& p) {
+// Copies the tile's template descriptor to shared memory and stages its
+// index arrays by bulk copies: thread 0 issues them, every thread of warp 0
+// waits (bounded: a copy of in-bounds memory completes; past the bound the
+// descriptor keeps its global pointers and the tile runs unstaged). In
+// kStageLu the work vector starts at zero. Returns the descriptor the tile
+// runs on.
+__device__ const GroupDev* stage_template(const GroupDev& g, GroupDev& sd, unsigned char* base, bool f32) {
+    {
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(&g);
+        uint32_t* dst = reinterpret_cast<uint32_t*>(&sd);
+        for (uint32_t i = threadIdx.x; i < sizeof(GroupDev) / 4; i += blockDim.x) dst[i] = src[i];
+    }
+    const uint32_t mode = g.stage_mode;
+    if (mode == kStageNone) {
+        __syncthreads();
+        return &sd;
+    }
+    const SmemPlan p = smem_plan(g, mode, f32);
     uint64_t* bar = reinterpret_cast<uint64_t*>(base);
-    const uint32_t* src[T_COUNT] = {d.q, d.col_ptr, d.prow, d.up, d.ui, d.lp, d.li, d.flags, d.pinv,
-                                    d.rt_ptr, d.rt_col, d.rt_pos};
+    uint32_t* u = reinterpret_cast<uint32_t*>(base);
     if (threadIdx.x == 0) {
         mbar_init(bar, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        mbar_arrive_expect_tx(bar, p.tape_words * 4u);
-        uint32_t* u = reinterpret_cast<uint32_t*>(base);
-        for (int k = 0; k < T_COUNT; k++)
-            if (p.len[k]) bulk_g2s(u + p.off[k], src[k], p.len[k] * 4u, bar);
+        mbar_arrive_expect_tx(bar, p.idx_words * 4u);
+        for (int k = 0; k < S_COUNT; k++)
+            if (p.len[k]) bulk_g2s(u + p.off[k], stage_src(g, k), p.len[k] * 4u, bar);
     }
-    // zero w and y (both precisions share the invariant: all-zero bits)
-    uint32_t* wz = reinterpret_cast<uint32_t*>(base + p.w_off);
-    uint32_t nz = (p.lx_off - p.w_off) / 4u;  // w and y
-    for (uint32_t i = threadIdx.x; i < nz; i += blockDim.x) wz[i] = 0u;
+    if (mode == kStageLu) {
+        uint32_t* wz = reinterpret_cast<uint32_t*>(base + p.w_off);
+        uint32_t nz = (p.lx_off - p.w_off) / 4u;
+        for (uint32_t i = threadIdx.x; i < nz; i += blockDim.x) wz[i] = 0u;
+    }
     __syncthreads();
     bool ok = true;
     if (threadIdx.x < 32) {
@@ -160,10 +282,30 @@ __device__ bool stage_tape(const GroupDev& d, unsigned char* base, const SmemPla
             }
         }
     }
-    return __syncthreads_and(ok || threadIdx.x >= 32) != 0;
+    ok = __syncthreads_and(ok || threadIdx.x >= 32) != 0;
+    if (threadIdx.x == 0) {
+        if (ok)
+            for (int k = 0; k < S_COUNT; k++)
+                if (p.len[k]) stage_redirect(sd, k, u + p.off[k]);
+        if (!ok) sd.stage_mode = kStageNone;
+    }
+    __syncthreads();
+    return &sd;
 }
 
 #define SL(arr, i) (arr)[(size_t)(i) * 32 + lane]
+
+// The template's tape words, read into registers once per call (the
+// descriptor may sit in shared memory next to the stores of the chain).
+struct TapeView {
+    const uint32_t *__restrict__ q, *__restrict__ col_ptr, *__restrict__ prow, *__restrict__ up,
+        *__restrict__ ui, *__restrict__ lp, *__restrict__ li, *__restrict__ flags, *__restrict__ pinv;
+    uint32_t n;
+};
+
+__device__ __forceinline__ TapeView tape_view(const GroupDev& d) {
+    return TapeView{d.q, d.col_ptr, d.prow, d.up, d.ui, d.lp, d.li, d.flags, d.pinv, d.n};
+}
 
 // The replay in shared memory; T = double or float. 0 holds, 1 pivot or
 // store failure, 2 only a multiplier past 1 / pivot_tol.
@@ -175,31 +317,32 @@ __device__ int refactor_smem(const GroupDev& d, const SmemTile& s, uint32_t lane
     T* __restrict__ ud = static_cast<T*>(s.ud);
     const T* __restrict__ a = static_cast<const T*>(s.a);
     const uint32_t P = d.P;
+    const TapeView t = tape_view(d);
     for (uint32_t v = 0; v < d.n_void; v++)
         if (LM(d.a, d.void_slots[v]) != 0.0) return 1;
     constexpr bool f64 = sizeof(T) == 8;
     bool bad = false, nonfinite = false;
     const T growth = (T)1e-12;
     const T inf = (T)INFINITY;
-    for (uint32_t k = 0; k < d.n; k++) {
-        uint32_t c = s.q[k];
-        for (uint32_t p = s.col_ptr[c]; p < s.col_ptr[c + 1]; p++) SL(w, s.prow[p]) = SL(a, p);
-        for (uint32_t p = s.up[k]; p < s.up[k + 1]; p++) {
-            uint32_t i = s.ui[p];
+    for (uint32_t k = 0; k < t.n; k++) {
+        uint32_t c = t.q[k];
+        for (uint32_t p = t.col_ptr[c]; p < t.col_ptr[c + 1]; p++) SL(w, t.prow[p]) = SL(a, p);
+        for (uint32_t p = t.up[k]; p < t.up[k + 1]; p++) {
+            uint32_t i = t.ui[p];
             T uki = SL(w, i);
             SL(w, i) = (T)0;
             SL(ux, p) = uki;
             nonfinite |= !(uki - uki == (T)0);
-            for (uint32_t pl = s.lp[i]; pl < s.lp[i + 1]; pl++) SL(w, s.li[pl]) -= SL(lx, pl) * uki;
+            for (uint32_t pl = t.lp[i]; pl < t.lp[i + 1]; pl++) SL(w, t.li[pl]) -= SL(lx, pl) * uki;
         }
-        uint32_t fl = s.flags[k];
+        uint32_t fl = t.flags[k];
         if (fl & 1u) {
             SL(ud, k) = (T)1;
-            for (uint32_t p = s.lp[k]; p < s.lp[k + 1]; p++) { SL(lx, p) = (T)0; SL(w, s.li[p]) = (T)0; }
+            for (uint32_t p = t.lp[k]; p < t.lp[k + 1]; p++) { SL(lx, p) = (T)0; SL(w, t.li[p]) = (T)0; }
             SL(w, k) = (T)0;
-            for (uint32_t p = s.up[k]; p < s.up[k + 1]; p++) {
-                uint32_t i = s.ui[p];
-                for (uint32_t pl = s.lp[i]; pl < s.lp[i + 1]; pl++) SL(w, s.li[pl]) = (T)0;
+            for (uint32_t p = t.up[k]; p < t.up[k + 1]; p++) {
+                uint32_t i = t.ui[p];
+                for (uint32_t pl = t.lp[i]; pl < t.lp[i + 1]; pl++) SL(w, t.li[pl]) = (T)0;
             }
             continue;
         }
@@ -212,8 +355,8 @@ __device__ int refactor_smem(const GroupDev& d, const SmemTile& s, uint32_t lane
         if constexpr (f64) {
             if (!(fl & 2u)) {
                 uint64_t cb = dbits(fabs((double)dk));
-                for (uint32_t p = s.lp[k]; p < s.lp[k + 1]; p++) {
-                    uint32_t r = s.li[p];
+                for (uint32_t p = t.lp[k]; p < t.lp[k + 1]; p++) {
+                    uint32_t r = t.li[p];
                     T v = SL(w, r);
                     SL(w, r) = (T)0;
                     uint64_t vb = dbits(fabs((double)v));
@@ -222,8 +365,8 @@ __device__ int refactor_smem(const GroupDev& d, const SmemTile& s, uint32_t lane
                 }
                 bad |= !(fabs((double)dk) >= 1e-12 * bitsd(cb));
             } else {
-                for (uint32_t p = s.lp[k]; p < s.lp[k + 1]; p++) {
-                    uint32_t r = s.li[p];
+                for (uint32_t p = t.lp[k]; p < t.lp[k + 1]; p++) {
+                    uint32_t r = t.li[p];
                     T lv = SL(w, r) / dk;
                     nonfinite |= !(lv - lv == (T)0);
                     SL(lx, p) = lv;
@@ -232,8 +375,8 @@ __device__ int refactor_smem(const GroupDev& d, const SmemTile& s, uint32_t lane
             }
         } else {
             T cmax = fabs(dk);
-            for (uint32_t p = s.lp[k]; p < s.lp[k + 1]; p++) {
-                uint32_t r = s.li[p];
+            for (uint32_t p = t.lp[k]; p < t.lp[k + 1]; p++) {
+                uint32_t r = t.li[p];
                 T v = SL(w, r);
                 SL(w, r) = (T)0;
                 cmax = fmaxf(cmax, fabsf(v));
@@ -247,9 +390,9 @@ __device__ int refactor_smem(const GroupDev& d, const SmemTile& s, uint32_t lane
     if (nonfinite || bad) return 1;
     if constexpr (f64) {
         uint64_t worst = 0;
-        for (uint32_t k = 0; k < d.n; k++) {
-            if (s.flags[k] & 2u) continue;
-            for (uint32_t p = s.lp[k]; p < s.lp[k + 1]; p++) {
+        for (uint32_t k = 0; k < t.n; k++) {
+            if (t.flags[k] & 2u) continue;
+            for (uint32_t p = t.lp[k]; p < t.lp[k + 1]; p++) {
                 uint64_t b = dbits(fabs((double)SL(lx, p)));
                 worst = worst > b ? worst : b;
             }
@@ -262,33 +405,38 @@ __device__ int refactor_smem(const GroupDev& d, const SmemTile& s, uint32_t lane
 // Forward and back substitution of y in place through the shared factors
 // (luSolve's two sweeps).
 template <typename T>
-__device__ __forceinline__ void subst_smem(const GroupDev& d, const SmemTile& s, uint32_t lane) {
-    T* __restrict__ y = static_cast<T*>(s.y);
+__device__ __forceinline__ void subst_smem(const TapeView& t, const SmemTile& s, T* __restrict__ y, uint32_t lane) {
     const T* __restrict__ lx = static_cast<const T*>(s.lx);
     const T* __restrict__ ux = static_cast<const T*>(s.ux);
     const T* __restrict__ ud = static_cast<const T*>(s.ud);
-    for (uint32_t k = 0; k < d.n; k++) {
+    for (uint32_t k = 0; k < t.n; k++) {
         T yk = SL(y, k);
         if (yk != (T)0)
-            for (uint32_t p = s.lp[k]; p < s.lp[k + 1]; p++) SL(y, s.li[p]) -= SL(lx, p) * yk;
+            for (uint32_t p = t.lp[k]; p < t.lp[k + 1]; p++) SL(y, t.li[p]) -= SL(lx, p) * yk;
     }
-    for (uint32_t k = d.n; k-- > 0;) {
+    for (uint32_t k = t.n; k-- > 0;) {
         T zk = SL(y, k) / SL(ud, k);
         SL(y, k) = zk;
         if (zk != (T)0)
-            for (uint32_t p = s.up[k]; p < s.up[k + 1]; p++) SL(y, s.ui[p]) -= SL(ux, p) * zk;
+            for (uint32_t p = t.up[k]; p < t.up[k + 1]; p++) SL(y, t.ui[p]) -= SL(ux, p) * zk;
     }
 }
 
 // dx = -A^-1 rhs through the shared factors (luSolve with neg); rhs and dx
-// are the lane's global rows.
+// are the lane's global rows. y is the work vector w, zero again on return.
 template <typename T>
 __device__ void solve_smem(const GroupDev& d, const SmemTile& s, uint32_t lane, uint32_t l) {
     const uint32_t P = d.P;
-    T* __restrict__ y = static_cast<T*>(s.y);
-    for (uint32_t r = 0; r < d.n; r++) SL(y, s.pinv[r]) = (T)(-LM(d.rhs, r));
-    subst_smem<T>(d, s, lane);
-    for (uint32_t j = 0; j < d.n; j++) LM(d.dx, s.q[j]) = (double)SL(y, j);
+    const TapeView t = tape_view(d);
+    const double* __restrict__ rhs = d.rhs;
+    double* __restrict__ dx = d.dx;
+    T* __restrict__ y = static_cast<T*>(s.w);
+    for (uint32_t r = 0; r < t.n; r++) SL(y, t.pinv[r]) = (T)(-LM(rhs, r));
+    subst_smem<T>(t, s, y, lane);
+    for (uint32_t j = 0; j < t.n; j++) {
+        LM(dx, t.q[j]) = (double)SL(y, j);
+        SL(y, j) = (T)0;
+    }
 }
 
 // One FP64-residual refinement sweep of an FP32 solve (refine_mixed):
@@ -297,17 +445,25 @@ __device__ void solve_smem(const GroupDev& d, const SmemTile& s, uint32_t lane, 
 // dx += -A^-1 r through the FP32 factors.
 __device__ void refine_smem(const GroupDev& d, const SmemTile& s, uint32_t lane, uint32_t l) {
     const uint32_t P = d.P;
-    float* __restrict__ y = static_cast<float*>(s.y);
-    for (uint32_t i = 0; i < d.n; i++) {
-        double r = LM(d.rhs, i);
-        for (uint32_t e = s.rt_ptr[i]; e < s.rt_ptr[i + 1]; e++) {
-            double xc = LM(d.dx, s.rt_col[e]);
-            if (xc != 0.0) r += LM(d.a, s.rt_pos[e]) * xc;
+    const TapeView t = tape_view(d);
+    const uint32_t *__restrict__ rt_ptr = d.rt_ptr, *__restrict__ rt_col = d.rt_col, *__restrict__ rt_pos = d.rt_pos;
+    const double* __restrict__ rhs = d.rhs;
+    const double* __restrict__ a = d.a;
+    double* __restrict__ dx = d.dx;
+    float* __restrict__ y = static_cast<float*>(s.w);
+    for (uint32_t i = 0; i < t.n; i++) {
+        double r = LM(rhs, i);
+        for (uint32_t e = rt_ptr[i]; e < rt_ptr[i + 1]; e++) {
+            double xc = LM(dx, rt_col[e]);
+            if (xc != 0.0) r += LM(a, rt_pos[e]) * xc;
         }
-        SL(y, s.pinv[i]) = (float)(-r);
+        SL(y, t.pinv[i]) = (float)(-r);
     }
-    subst_smem<float>(d, s, lane);
-    for (uint32_t j = 0; j < d.n; j++) LM(d.dx, s.q[j]) += (double)SL(y, j);
+    subst_smem<float>(t, s, y, lane);
+    for (uint32_t j = 0; j < t.n; j++) {
+        LM(dx, t.q[j]) += (double)SL(y, j);
+        SL(y, j) = 0.0f;
+    }
 }
 
 // Copies a shared factor out to the lane's global factor arrays, for the

@@ -72,11 +72,12 @@ PRECISION = {"fp64": abi.ESPL_FP64, "mixed": abi.ESPL_MIXED}
 class Lanes:
     """Lanes of one or more templates on one GPU."""
 
-    def __init__(self, nets: Sequence[Netlist], precision: str = "fp64", dt0: float = 0.0, device: int = 0):
+    def __init__(self, nets: Sequence[Netlist], precision: str = "fp64", dt0: float = 0.0, device: int = 0,
+                 refine_sweeps: int = 0):
         self.nets = list(nets)
         self._keep, arr = abi.cnets(self.nets)
         self._arr = arr
-        opts = CreateOpts(1, PRECISION[precision], device, 0)
+        opts = CreateOpts(abi.ABI_VERSION, PRECISION[precision], device, 0, refine_sweeps, 0)
         h = C.c_void_p()
         st = lib().espl_create(arr, len(self.nets), C.byref(opts), dt0, C.byref(h))
         if st != 0:

@@ -25,7 +25,7 @@
 extern "C" {
 #endif
 
-#define ESPL_ABI_VERSION 1u
+#define ESPL_ABI_VERSION 2u
 
 /* A device terminal on the datum node. Its residual row and Jacobian
  * entries are dropped, as the reference's GROUND gather does
@@ -126,7 +126,12 @@ typedef struct {
     uint32_t abi_version;
     uint32_t precision;      /* ESPL_FP64 or ESPL_MIXED */
     uint32_t device;         /* CUDA device ordinal */
-    uint32_t lanes_per_cta;  /* 0: the autotuned default */
+    uint32_t lanes_per_cta;  /* 0 or 32: one 32-lane tile per CTA (the only width) */
+    uint32_t refine_sweeps;  /* ESPL_MIXED: FP64-residual refinement sweeps after
+                              * each FP32 solve inside Newton (0: none; each Newton
+                              * iteration then refines the step against the FP64
+                              * KCL residual). At most 4. */
+    uint32_t reserved;       /* 0 */
 } espl_create_opts;
 
 typedef struct espl_lanes espl_lanes;

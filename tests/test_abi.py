@@ -16,13 +16,14 @@ def declared_symbols():
 
 
 def test_library_exports_every_declared_symbol():
+    from egspice_b200 import abi
     from egspice_b200.lanes import lib
     L = lib()
     syms = declared_symbols()
     assert len(syms) >= 15
     for s in syms:
         assert hasattr(L, s), f"{s} missing from the library"
-    assert L.espl_abi_version() == 1
+    assert L.espl_abi_version() == abi.ABI_VERSION
 
 
 def test_create_without_a_gpu_reports_no_image_or_runs():
