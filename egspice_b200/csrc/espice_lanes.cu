@@ -650,7 +650,7 @@ espl_status run_static(espl_lanes* h, const NewtonParams& np, int tran) {
     CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
     h->stats.newton_ms = ms;
     h->stats.total_ms += ms;
-    h->stats.launches += 1;
+    h->stats.launches += (uint32_t)h->classes.size();
     return ESPL_OK;
 }
 
@@ -912,7 +912,7 @@ espl_status espl_device_launch(espl_lanes* h, uint32_t max_steps, espl_step_repo
     CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
     h->stats.newton_ms = ms;
     h->stats.total_ms += ms;
-    h->stats.launches += 1;
+    h->stats.launches += (uint32_t)h->classes.size();
     CK(cudaMemcpyAsync(h->h_state.data(), h->d_state, sizeof(LaneState) * h->total_lanes, cudaMemcpyDeviceToHost,
                        h->stream));
     CK(cudaStreamSynchronize(h->stream));

@@ -100,3 +100,50 @@ def test_ring_oscillator_period(oracle):
     assert all(r.status == 1 for r in reps)
     assert np.all(cr >= 3)
     assert np.all(np.abs(per - po) <= 1e-3 * np.abs(po)), (per, po)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_golden_fixtures_on_the_gpu(precision):
+    """The committed oracle fixtures (tests/golden), without the oracle: FP64
+    lanes reproduce them to 1e-12 with the same iteration and step counts;
+    mixed lanes meet the 1e-6 bar."""
+    import json
+    import os
+    import sys
+    here = os.path.dirname(os.path.abspath(__file__))
+    sys.path.insert(0, os.path.join(here, "golden"))
+    import make_golden as mg
+    with open(os.path.join(here, "golden", "golden.json")) as f:
+        g = json.load(f)
+    tight = precision == "fp64"
+    for name, net, opts, x0 in mg.op_cases():
+        with Lanes([net], precision=precision) as L:
+            if x0 is not None:
+                L.put_x(0, x0, False)
+            r = L.solve_static(opts)
+            x = L.get_x(0)
+        xr = np.array(g["op"][name]["x"])
+        if tight:
+            assert r[:, 1].tolist() == g["op"][name]["iterations"], name
+            np.testing.assert_allclose(x, xr, rtol=1e-12, atol=1e-15)
+        else:
+            assert worst(x, xr) <= 1.0, name
+    for name, net, topts, meas in mg.tran_cases():
+        with Lanes([net], precision=precision, dt0=topts.dt) as L:
+            if meas:
+                L.set_period_meas(0, net.node(meas[0]), meas[1], meas[2])
+            reps = L.run_tran(topts, steps_per_launch=10000)
+            x = L.get_x(0)
+            per = L.period_meas(0)[0] if meas else None
+        gt = g["tran"][name]
+        xr = np.array(gt["x"])
+        if tight:
+            assert [rp.steps for rp in reps] == gt["steps"], name
+            assert [rp.rejects for rp in reps] == gt["rejects"], name
+            np.testing.assert_allclose(x, xr, rtol=1e-12, atol=1e-15)
+            if per is not None:
+                np.testing.assert_allclose(per, np.array(gt["period"]), rtol=1e-12)
+        else:
+            assert worst(x, xr) <= 1.0, name
+            if per is not None:
+                assert float(np.abs(per - np.array(gt["period"])).max()) <= 1e-6 * float(np.abs(gt["period"]).max())
