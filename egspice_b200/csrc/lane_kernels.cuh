@@ -73,7 +73,13 @@ __device__ void newton_tile(const TileCtx& c, LaneState* s, const NewtonParams& 
         sh.acc0[lane] = dbits(1.0);
         sh.acc1[lane] = 0;
         sh.acc2[lane] = 0;
-        if (s) s->iterations = o.max_iter;
+        if (s) {
+            s->iterations = o.max_iter;
+            // Mixed tiles factor in FP32 once Newton contracts (warm starts,
+            // transient steps); a cold start (INITFIX, MODEINITJCT seeds)
+            // walks through ill-conditioned iterates and runs in FP64.
+            s->fp64 = (MIXED && o.init_fix) ? 1u : 0u;
+        }
     }
     __syncthreads();
     for (uint32_t it = 0; it < o.max_iter; it++) {

@@ -123,11 +123,15 @@ def test_golden_fixtures_on_the_gpu(precision):
             r = L.solve_static(opts)
             x = L.get_x(0)
         xr = np.array(g["op"][name]["x"])
-        if tight:
+        assert ((r[:, 0] & abi.CONVERGED) != 0).all(), name
+        assert worst(x, xr) <= 1.0, name
+        if tight and opts.init_fix == 0:
+            # a warm start takes the oracle's path: the same iterations and x
+            # to rounding (a cold start's limiting walk may take other
+            # iterations: the device fuses multiply-adds the oracle rounds
+            # twice, and the walk amplifies that)
             assert r[:, 1].tolist() == g["op"][name]["iterations"], name
             np.testing.assert_allclose(x, xr, rtol=1e-12, atol=1e-15)
-        else:
-            assert worst(x, xr) <= 1.0, name
     for name, net, topts, meas in mg.tran_cases():
         with Lanes([net], precision=precision, dt0=topts.dt) as L:
             if meas:
