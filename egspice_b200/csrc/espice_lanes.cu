@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1049,3 +1050,122 @@ espl_status espl_tape_copy(const espl_tape* t, uint32_t* q, uint32_t* pinv, uint
 void espl_tape_free(espl_tape* t) { delete t; }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// espl_tape_replay_noalloc: the lane replay (refactor64) with its work vector
+// and tape words in a file-scope device array instead of handle memory.
+
+namespace {
+
+constexpr int kReplayMaxDevices = 64;
+static __device__ __align__(256) unsigned char g_replay_scratch[ESPL_REPLAY_SCRATCH_BYTES];
+std::mutex g_replay_mu;
+void* g_replay_addr[kReplayMaxDevices] = {};
+
+__global__ void __launch_bounds__(128) k_replay_noalloc(GroupDev d, uint32_t* status) {
+    uint32_t l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l < d.lanes) status[l] = (uint32_t)refactor64(d, l);
+}
+
+void put_err(char* err, size_t cap, const std::string& m) {
+    if (!err || cap == 0) return;
+    size_t k = std::min(cap - 1, m.size());
+    std::memcpy(err, m.data(), k);
+    err[k] = 0;
+}
+
+}  // namespace
+
+extern "C" espl_status espl_tape_replay_noalloc(const espl_tape* t, const uint32_t* col_ptr, const double* vals,
+                                                uint32_t lanes, double* lx, double* ux, double* udiag,
+                                                uint32_t* lane_status, void* stream, char* err, size_t err_cap) {
+    put_err(err, err_cap, "");
+    if (!t || !col_ptr || !vals || !udiag || !lane_status || lanes == 0) {
+        put_err(err, err_cap, "null argument or zero lanes");
+        return ESPL_INVALID_ARGUMENT;
+    }
+    const Tape& tp = t->t;
+    const uint64_t n = tp.q.size(), nnz = tp.prow.size(), nl = tp.li.size(), nu = tp.ui.size();
+    if ((nl && !lx) || (nu && !ux) || col_ptr[n] != nnz) {
+        put_err(err, err_cap, "factor arrays missing or col_ptr does not match the tape");
+        return ESPL_INVALID_ARGUMENT;
+    }
+    // Layout: the tape words (q, col_ptr, prow, up, ui, lp, li, flags,
+    // void_slots), then the work vector at a 256-byte boundary.
+    const std::vector<uint32_t>* vecs[] = {&tp.q, nullptr, &tp.prow, &tp.up, &tp.ui, &tp.lp, &tp.li, &tp.flags,
+                                           &tp.void_slots};
+    uint64_t words = 0, off[9];
+    for (int k = 0; k < 9; k++) {
+        off[k] = words;
+        words += k == 1 ? n + 1 : vecs[k]->size();
+    }
+    const uint64_t w_off = (words * 4 + 255) & ~uint64_t(255);
+    const uint64_t need = w_off + 8 * n * (uint64_t)lanes;
+    if (need > ESPL_REPLAY_SCRATCH_BYTES) {
+        put_err(err, err_cap, "replay scratch needs " + std::to_string(need) + " bytes (n = " + std::to_string(n) +
+                                  ", lanes = " + std::to_string(lanes) + "); the limit is " +
+                                  std::to_string(ESPL_REPLAY_SCRATCH_BYTES) + " bytes per device");
+        return ESPL_TOO_LARGE;
+    }
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess || dev < 0 || dev >= kReplayMaxDevices) {
+        put_err(err, err_cap, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+        return e == cudaSuccess ? ESPL_INVALID_ARGUMENT : ESPL_NO_IMAGE;
+    }
+    unsigned char* base = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_replay_mu);
+        if (!g_replay_addr[dev]) {
+            void* p = nullptr;
+            e = cudaGetSymbolAddress(&p, g_replay_scratch);
+            if (e != cudaSuccess) {
+                put_err(err, err_cap, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+                return ESPL_NO_IMAGE;
+            }
+            g_replay_addr[dev] = p;
+        }
+        base = static_cast<unsigned char*>(g_replay_addr[dev]);
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    uint32_t* u = reinterpret_cast<uint32_t*>(base);
+    for (int k = 0; k < 9; k++) {
+        const uint32_t* src = k == 1 ? col_ptr : vecs[k]->data();
+        uint64_t cnt = k == 1 ? n + 1 : vecs[k]->size();
+        if (!cnt) continue;
+        e = cudaMemcpyAsync(u + off[k], src, cnt * 4, cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) {
+            put_err(err, err_cap, std::string("cudaMemcpyAsync: ") + cudaGetErrorString(e));
+            return ESPL_DRIVER;
+        }
+    }
+    GroupDev d{};
+    d.n = (uint32_t)n;
+    d.nnz = (uint32_t)nnz;
+    d.nnz_l = (uint32_t)nl;
+    d.nnz_u = (uint32_t)nu;
+    d.lanes = lanes;
+    d.P = lanes;
+    d.n_void = (uint32_t)tp.void_slots.size();
+    d.q = u + off[0];
+    d.col_ptr = u + off[1];
+    d.prow = u + off[2];
+    d.up = u + off[3];
+    d.ui = u + off[4];
+    d.lp = u + off[5];
+    d.li = u + off[6];
+    d.flags = u + off[7];
+    d.void_slots = u + off[8];
+    d.w = reinterpret_cast<double*>(base + w_off);
+    d.a = const_cast<double*>(vals);
+    d.lx = lx;
+    d.ux = ux;
+    d.udiag = udiag;
+    k_replay_noalloc<<<(lanes + 127) / 128, 128, 0, st>>>(d, lane_status);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        put_err(err, err_cap, std::string("launch: ") + cudaGetErrorString(e));
+        return ESPL_DRIVER;
+    }
+    return ESPL_OK;
+}

@@ -251,6 +251,41 @@ void espl_tape_free(espl_tape *t);
 /* The last error's text, NUL-terminated (empty when none). */
 espl_status espl_error_message(espl_lanes *h, char *buf, size_t cap);
 
+/* No counterpart in the reference. Replays a host-built tape
+ * (espl_tape_build) on `lanes` lanes of matrix values already on the
+ * device, WITHOUT ALLOCATING: for callers that cannot allocate device memory
+ * at the point of the call -- a host that sized all device memory up front,
+ * or a framework whose caching allocator must not be bypassed -- and so
+ * cannot create a handle. The work vector and the staged tape words live in
+ * one file-scope device array of ESPL_REPLAY_SCRATCH_BYTES per device.
+ *
+ *   col_ptr     host, n + 1: the pattern the tape was built from
+ *   vals        device, nnz x lanes, lane-interleaved (slot p of lane l at
+ *               p * lanes + l)
+ *   lx, ux      device, nnz_l x lanes and nnz_u x lanes, same interleaving
+ *   udiag       device, n x lanes
+ *   lane_status device, lanes words: 0 the replay holds, 1 a pivot failed
+ *               (dead, non-finite, growth 1e-12) or a void slot filled, 2 only
+ *               a multiplier past 1 / pivot_tol (kernels/lane.zig:56-125 and
+ *               wideMultipliers)
+ *   stream      a cudaStream_t, or NULL for the legacy default stream
+ *   err         optional, err_cap bytes: the reason of a non-OK status
+ *
+ * ESPL_TOO_LARGE, with the sizes in `err`, when the tape words plus
+ * 8 * n * lanes bytes of work vector exceed ESPL_REPLAY_SCRATCH_BYTES.
+ * The results are ready when `stream` reaches the call (the launch is
+ * asynchronous; the tape words are copied from host memory first).
+ * The work vector must be all-zero on entry: the array starts at zero and
+ * every replay leaves it at zero, so it stays so unless a launch of this
+ * entry point is aborted. Calls on one device share the array: overlapping
+ * calls (other streams, other host threads) race; serialize them. The first
+ * call on a device resolves the array's address (cudaGetSymbolAddress, with
+ * that device current); make it before any stream capture begins. */
+#define ESPL_REPLAY_SCRATCH_BYTES (8u << 20)
+espl_status espl_tape_replay_noalloc(const espl_tape *t, const uint32_t *col_ptr, const double *vals,
+                                     uint32_t lanes, double *lx, double *ux, double *udiag, uint32_t *lane_status,
+                                     void *stream, char *err, size_t err_cap);
+
 #ifdef __cplusplus
 }
 #endif
