@@ -272,7 +272,16 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    # smaller cases of the same workload (profiling); the defaults are the benchmark
+    ap.add_argument("--lanes", type=int, default=16384, help="lanes of the 31-stage template")
+    ap.add_argument("--variants", type=int, default=32, help="seeded 15-63-stage variants, 32 lanes each")
+    ap.add_argument("--max-steps", type=int, default=5000, help="accepted steps per lane")
+    ap.add_argument("--modes", default="fp64,mixed", help="precisions to run, comma-separated")
+    ap.add_argument("--no-check", action="store_true", help="skip the oracle check of sampled lanes")
     args = ap.parse_args()
+    modes = [m for m in args.modes.split(",") if m]
+    if not modes or any(m not in ("fp64", "mixed") for m in modes):
+        ap.error("--modes takes fp64 and/or mixed")
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -286,10 +295,14 @@ def main():
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
-    nets, topts = ring_workload(seed=rank)
+    nets, topts = ring_workload(seed=rank, lanes=args.lanes, variants=args.variants)
+    topts.max_steps = args.max_steps
     n_points = sum(n.lanes for n in nets)
-    config = {"workload": "ring_oscillator_mc_uneven", "templates": len(nets), "lanes": n_points,
-              "stages": "31 (16,384 lanes) + 32 variants of 15-63 (32 lanes each)", "steps_per_lane": 5000,
+    full = (args.lanes, args.variants, args.max_steps) == (16384, 32, 5000)
+    config = {"workload": "ring_oscillator_mc_uneven" + ("" if full else " (reduced)"), "templates": len(nets),
+              "lanes": n_points,
+              "stages": f"31 ({args.lanes:,} lanes) + {args.variants} variants of 15-63 (32 lanes each)",
+              "steps_per_lane": args.max_steps,
               "method": "trap, LTE step control", "predictor": "linear (SPICE xfact)",
               "meas": "oscillation period of stage 1 (rising 0.9 V)",
               "l2": "inputs larger than L2 (per-sweep working set > 126 MB)", "parallelism": f"lanes x{world} GPUs"}
@@ -326,7 +339,7 @@ def main():
         torch.cuda.synchronize()
 
     results = {}
-    for prec in ("fp64", "mixed"):
+    for prec in modes:
         for _ in range(args.warmup):
             run_ring_sweep(nets, topts, prec)
         dev_ms, walls = [], []
@@ -348,14 +361,15 @@ def main():
                              iters=sum(r.nr_iters for r in reps), rejects=sum(r.rejects for r in reps),
                              launches=launches, periods=periods)
 
-    best, plain = results["mixed"], results["fp64"]
+    best = results.get("mixed") or results["fp64"]
+    plain = results.get("fp64")
     points_all = n_points * world
     value = points_all / best["dev_s"]
     e2e = points_all / best["wall_s"]
     err = {}
-    if rank == 0:
+    if rank == 0 and not args.no_check:
         sample = [0] + list(range(1, len(nets), 8))
-        for prec in ("mixed", "fp64"):
+        for prec in modes:
             r = results[prec]
             err[prec] = ring_check([nets[i] for i in sample], topts, [r["xs"][i] for i in sample],
                                    [r["periods"][i] for i in sample])
@@ -375,20 +389,17 @@ def main():
         "warmup": args.warmup, "ms_per_step": best["dev_s"] * 1000.0, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64 (eval, residual, step control); f32 LU in mixed",
         "data": "synthetic (seeded Monte-Carlo MOS1 ring oscillators)", "config": config,
-        "modes": {
-            "mixed": {"points_per_s": value, "ms_per_sweep": best["dev_s"] * 1e3, "newton_iters": best["iters"],
-                      "rejects": best["rejects"], "period_err_over_tol": err.get("mixed", (None,))[0],
-                      "final_x_err_over_tol": err.get("mixed", (None, None))[1]},
-            "fp64": {"points_per_s": points_all / plain["dev_s"], "ms_per_sweep": plain["dev_s"] * 1e3,
-                     "newton_iters": plain["iters"], "rejects": plain["rejects"],
-                     "period_err_over_tol": err.get("fp64", (None,))[0],
-                     "final_x_err_over_tol": err.get("fp64", (None, None))[1]},
-            "mixed_over_fp64": plain["dev_s"] / best["dev_s"],
-            "learned": False,
-        },
+        "modes": dict(
+            {m: {"points_per_s": points_all / results[m]["dev_s"], "ms_per_sweep": results[m]["dev_s"] * 1e3,
+                 "newton_iters": results[m]["iters"], "rejects": results[m]["rejects"],
+                 "period_err_over_tol": err.get(m, (None,))[0],
+                 "final_x_err_over_tol": err.get(m, (None, None))[1]} for m in modes},
+            mixed_over_fp64=(plain["dev_s"] / best["dev_s"]) if (plain and "mixed" in results) else None,
+            learned=False),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "peak_kind": kind, "traffic": None,
-                     "kernel": "k_tran<true>: per-tile eval + gather + shared-memory FP32 LU + gates, fused"},
+                     "kernel": ("k_tran<true>" if "mixed" in results else "k_tran<false>") +
+                               ": per-tile eval + gather + shared-memory LU + gates, fused"},
         "e2e": {"value": e2e, "unit": "points/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(best["launches"]),
         "clocks": best["clocks"],
