@@ -607,6 +607,11 @@ espl_status retape(espl_lanes* h, int tran, double dt) {
         UP(ui, g.tape.ui);
         UP(flags, g.tape.flags);
         UP(void_slots, g.tape.void_slots);
+        {
+            std::vector<uint32_t> prog;
+            d.n_prog = lu_program(g.tape, g.col_ptr.data(), prog) ? (uint32_t)prog.size() : 0u;
+            if (d.n_prog) UP(lu_prog, prog);
+        }
 #undef UP
         size_t P = g.P;
         if ((s = dalloc(h, own, &d.lx, (size_t)d.nnz_l * P))) return s;

@@ -40,6 +40,8 @@ struct GroupDev {
     double meas_level, meas_t0;
     const uint32_t *col_ptr, *row_idx, *prow, *q, *pinv, *lp, *li, *up, *ui, *flags, *void_slots, *diag;
     const uint32_t *rt_ptr, *rt_col, *rt_pos;  // row view of the pattern: per row, (column, slot) by column
+    const uint32_t* lu_prog;                   // the replay as a flat program (tape.h lu_program)
+    uint32_t n_prog, prog_pad;
     const uint8_t* cur_row;
     const uint32_t *res_t, *res_s, *cap_t, *cap_s, *vsrc_t, *vsrc_s, *isrc_t, *dio_t, *dio_s, *mos_t, *mos_s;
     const double *res_r, *cap_c, *vsrc_p, *isrc_p, *dio_d, *mos_d;

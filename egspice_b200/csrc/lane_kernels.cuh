@@ -143,7 +143,7 @@ __device__ void newton_tile(const TileCtx& c, LaneState* s, const NewtonParams& 
             bool use32 = MIXED && !s->fp64;
             bool done = false;
             if (sm && (use32 || !MIXED)) {
-                int rc = refactor_smem<T>(d, st, lane, l);
+                int rc = d.n_prog ? refactor_prog<T>(d, st, lane, l) : refactor_smem<T>(d, st, lane, l);
                 if (MIXED && rc != 0) {
                     s->fp64 = 1;
                     s->fallbacks++;

@@ -21,6 +21,7 @@
 #pragma once
 
 #include "lane_tile.cuh"
+#include "tape.h"
 
 namespace espl {
 
@@ -63,7 +64,7 @@ enum StageArr {
     S_DIAG, S_VOID, S_CURROW, S_SLOTDIAG, S_RES_T, S_CAP_T, S_VSRC_T, S_DIO_T, S_MOS_T,
     S_GPTR, S_GCELL, S_CPTR, S_CCELL, S_RPTR, S_RCELL, S_QPTR, S_QCELL, S_SITE,
     S_Q, S_PINV, S_COLPTR, S_PROW, S_UP, S_UI, S_LP, S_LI, S_FLAGS,
-    S_RTPTR, S_RTCOL, S_RTPOS, S_COUNT
+    S_RTPTR, S_RTCOL, S_RTPOS, S_PROG, S_COUNT
 };
 
 // Staging modes of a template: nothing, the index arrays, or the index
@@ -72,7 +73,7 @@ enum : uint32_t { kStageNone = 0, kStageIndex = 1, kStageLu = 2 };
 
 __host__ __device__ inline uint32_t pad4(uint32_t words) { return (words + 3u) & ~3u; }
 
-__host__ __device__ inline uint32_t stage_words(const GroupDev& d, int k) {
+__host__ __device__ inline uint32_t stage_words(const GroupDev& d, int k, uint32_t mode) {
     const bool rows = d.refine_rows != 0;
     switch (k) {
     case S_DIAG: return d.n;
@@ -105,6 +106,7 @@ __host__ __device__ inline uint32_t stage_words(const GroupDev& d, int k) {
     case S_RTPTR: return rows ? d.n + 1 : 0u;
     case S_RTCOL: return rows ? d.nnz : 0u;
     case S_RTPOS: return rows ? d.nnz : 0u;
+    case S_PROG: return mode == kStageLu ? d.n_prog : 0u;
     default: return 0u;
     }
 }
@@ -141,6 +143,7 @@ __host__ __device__ inline const void* stage_src(const GroupDev& d, int k) {
     case S_RTPTR: return d.rt_ptr;
     case S_RTCOL: return d.rt_col;
     case S_RTPOS: return d.rt_pos;
+    case S_PROG: return d.lu_prog;
     default: return nullptr;
     }
 }
@@ -178,6 +181,7 @@ __device__ inline void stage_redirect(GroupDev& d, int k, const void* p) {
     case S_RTPTR: d.rt_ptr = u; break;
     case S_RTCOL: d.rt_col = u; break;
     case S_RTPOS: d.rt_pos = u; break;
+    case S_PROG: d.lu_prog = u; break;
     default: break;
     }
 }
@@ -202,7 +206,7 @@ __host__ __device__ inline SmemPlan smem_plan(const GroupDev& d, uint32_t mode, 
     uint32_t o = 4;  // the first 16 bytes hold the mbarrier
     for (int k = 0; k < S_COUNT; k++) {
         p.off[k] = o;
-        p.len[k] = pad4(stage_words(d, k));
+        p.len[k] = pad4(stage_words(d, k, mode));
         o += p.len[k];
     }
     p.idx_words = o - 4;
@@ -402,6 +406,134 @@ __device__ int refactor_smem(const GroupDev& d, const SmemTile& s, uint32_t lane
     return 0;
 }
 
+// The replay driven by the template's flat program (tape.h lu_program): the
+// same operations on the same locations in the same order as
+// refactor_smem, without the index chase through the tape's columns, and
+// with the independent entries of a scatter, an axpy or a division issued
+// two at a time. The FP64 wide-multiplier scan is folded into the
+// divisions.
+template <typename T>
+__device__ int refactor_prog(const GroupDev& d, const SmemTile& s, uint32_t lane, uint32_t l) {
+    T* __restrict__ w = static_cast<T*>(s.w);
+    T* __restrict__ lx = static_cast<T*>(s.lx);
+    T* __restrict__ ux = static_cast<T*>(s.ux);
+    T* __restrict__ ud = static_cast<T*>(s.ud);
+    const T* __restrict__ a = static_cast<const T*>(s.a);
+    const uint32_t* __restrict__ prog = d.lu_prog;
+    const uint32_t P = d.P;
+    for (uint32_t v = 0; v < d.n_void; v++)
+        if (LM(d.a, d.void_slots[v]) != 0.0) return 1;
+    constexpr bool f64 = sizeof(T) == 8;
+    bool bad = false, nonfinite = false;
+    uint64_t worst = 0;
+    const T growth = (T)1e-12;
+    const T inf = (T)INFINITY;
+    for (uint32_t pc = 0;;) {
+        const uint32_t h = prog[pc];
+        const uint32_t op = h & 15u;
+        if (op == kOpScat) {
+            const uint32_t cnt = h >> 4;
+            const uint32_t* __restrict__ e = prog + pc + 1;
+            uint32_t j = 0;
+            for (; j + 1 < cnt; j += 2) {
+                const uint32_t e0 = e[j], e1 = e[j + 1];
+                const T v0 = SL(a, e0 & 0xffffu), v1 = SL(a, e1 & 0xffffu);
+                SL(w, e0 >> 16) = v0;
+                SL(w, e1 >> 16) = v1;
+            }
+            if (j < cnt) SL(w, e[j] >> 16) = SL(a, e[j] & 0xffffu);
+            pc += 1 + cnt;
+        } else if (op == kOpTake) {
+            const uint32_t cnt = h >> 4;
+            const uint32_t ip = prog[pc + 1];
+            const uint32_t i = ip >> 16;
+            const T uki = SL(w, i);
+            SL(w, i) = (T)0;
+            SL(ux, ip & 0xffffu) = uki;
+            nonfinite |= !(uki - uki == (T)0);
+            const uint32_t* __restrict__ e = prog + pc + 2;
+            uint32_t j = 0;
+            for (; j + 1 < cnt; j += 2) {
+                const uint32_t e0 = e[j], e1 = e[j + 1];
+                const uint32_t r0 = e0 >> 16, r1 = e1 >> 16;
+                const T w0 = SL(w, r0), w1 = SL(w, r1);
+                const T l0 = SL(lx, e0 & 0xffffu), l1 = SL(lx, e1 & 0xffffu);
+                SL(w, r0) = w0 - l0 * uki;
+                SL(w, r1) = w1 - l1 * uki;
+            }
+            if (j < cnt) {
+                const uint32_t r0 = e[j] >> 16;
+                SL(w, r0) -= SL(lx, e[j] & 0xffffu) * uki;
+            }
+            pc += 2 + cnt;
+        } else if (op == kOpPiv) {
+            const uint32_t fl = (h >> 4) & 15u, cnt = h >> 8;
+            const uint32_t k = prog[pc + 1];
+            const uint32_t* __restrict__ e = prog + pc + 2;
+            T dk = SL(w, k);
+            SL(w, k) = (T)0;
+            bool dead = dk == (T)0 || !(fabs(dk) < inf);
+            bad |= dead;
+            if (dead) dk = (T)1;
+            SL(ud, k) = dk;
+            if constexpr (f64) {
+                if (!(fl & 2u)) {
+                    uint64_t cb = dbits(fabs((double)dk));
+                    for (uint32_t j = 0; j < cnt; j++) {
+                        const uint32_t r = e[j] >> 16;
+                        const T v = SL(w, r);
+                        SL(w, r) = (T)0;
+                        const uint64_t vb = dbits(fabs((double)v));
+                        cb = cb > vb ? cb : vb;
+                        const T lv = v / dk;
+                        SL(lx, e[j] & 0xffffu) = lv;
+                        const uint64_t lb = dbits(fabs((double)lv));
+                        worst = worst > lb ? worst : lb;
+                    }
+                    bad |= !(fabs((double)dk) >= 1e-12 * bitsd(cb));
+                } else {
+                    for (uint32_t j = 0; j < cnt; j++) {
+                        const uint32_t r = e[j] >> 16;
+                        const T lv = SL(w, r) / dk;
+                        nonfinite |= !(lv - lv == (T)0);
+                        SL(lx, e[j] & 0xffffu) = lv;
+                        SL(w, r) = (T)0;
+                    }
+                }
+            } else {
+                T cmax = fabs(dk);
+                for (uint32_t j = 0; j < cnt; j++) {
+                    const uint32_t r = e[j] >> 16;
+                    const T v = SL(w, r);
+                    SL(w, r) = (T)0;
+                    cmax = fmaxf(cmax, fabsf(v));
+                    const T lv = v / dk;
+                    nonfinite |= !(lv - lv == (T)0);
+                    SL(lx, e[j] & 0xffffu) = lv;
+                }
+                if (!(fl & 2u)) bad |= !(fabsf(dk) >= growth * cmax) || !(cmax / fabsf(dk) <= (T)kWide);
+            }
+            pc += 2 + cnt;
+        } else if (op == kOpVoid) {
+            const uint32_t k = prog[pc + 1];
+            const TapeView t = tape_view(d);
+            SL(ud, k) = (T)1;
+            for (uint32_t p = t.lp[k]; p < t.lp[k + 1]; p++) { SL(lx, p) = (T)0; SL(w, t.li[p]) = (T)0; }
+            SL(w, k) = (T)0;
+            for (uint32_t p = t.up[k]; p < t.up[k + 1]; p++) {
+                uint32_t i = t.ui[p];
+                for (uint32_t pl = t.lp[i]; pl < t.lp[i + 1]; pl++) SL(w, t.li[pl]) = (T)0;
+            }
+            pc += 2;
+        } else {
+            break;
+        }
+    }
+    if (nonfinite || bad) return 1;
+    if constexpr (f64) return bitsd(worst) <= kWide ? 0 : 2;
+    return 0;
+}
+
 // Forward and back substitution of y in place through the shared factors
 // (luSolve's two sweeps).
 template <typename T>
@@ -409,16 +541,37 @@ __device__ __forceinline__ void subst_smem(const TapeView& t, const SmemTile& s,
     const T* __restrict__ lx = static_cast<const T*>(s.lx);
     const T* __restrict__ ux = static_cast<const T*>(s.ux);
     const T* __restrict__ ud = static_cast<const T*>(s.ud);
+    // the entries of one column update distinct rows: two at a time
     for (uint32_t k = 0; k < t.n; k++) {
-        T yk = SL(y, k);
-        if (yk != (T)0)
-            for (uint32_t p = t.lp[k]; p < t.lp[k + 1]; p++) SL(y, t.li[p]) -= SL(lx, p) * yk;
+        const T yk = SL(y, k);
+        if (yk != (T)0) {
+            uint32_t p = t.lp[k];
+            const uint32_t pe = t.lp[k + 1];
+            for (; p + 1 < pe; p += 2) {
+                const uint32_t r0 = t.li[p], r1 = t.li[p + 1];
+                const T y0 = SL(y, r0), y1 = SL(y, r1);
+                const T l0 = SL(lx, p), l1 = SL(lx, p + 1);
+                SL(y, r0) = y0 - l0 * yk;
+                SL(y, r1) = y1 - l1 * yk;
+            }
+            if (p < pe) SL(y, t.li[p]) -= SL(lx, p) * yk;
+        }
     }
     for (uint32_t k = t.n; k-- > 0;) {
-        T zk = SL(y, k) / SL(ud, k);
+        const T zk = SL(y, k) / SL(ud, k);
         SL(y, k) = zk;
-        if (zk != (T)0)
-            for (uint32_t p = t.up[k]; p < t.up[k + 1]; p++) SL(y, t.ui[p]) -= SL(ux, p) * zk;
+        if (zk != (T)0) {
+            uint32_t p = t.up[k];
+            const uint32_t pe = t.up[k + 1];
+            for (; p + 1 < pe; p += 2) {
+                const uint32_t r0 = t.ui[p], r1 = t.ui[p + 1];
+                const T y0 = SL(y, r0), y1 = SL(y, r1);
+                const T u0 = SL(ux, p), u1 = SL(ux, p + 1);
+                SL(y, r0) = y0 - u0 * zk;
+                SL(y, r1) = y1 - u1 * zk;
+            }
+            if (p < pe) SL(y, t.ui[p]) -= SL(ux, p) * zk;
+        }
     }
 }
 
@@ -431,7 +584,16 @@ __device__ void solve_smem(const GroupDev& d, const SmemTile& s, uint32_t lane, 
     const double* __restrict__ rhs = d.rhs;
     double* __restrict__ dx = d.dx;
     T* __restrict__ y = static_cast<T*>(s.w);
-    for (uint32_t r = 0; r < t.n; r++) SL(y, t.pinv[r]) = (T)(-LM(rhs, r));
+    // the right-hand side comes from global memory: eight loads in flight
+    uint32_t r = 0;
+    for (; r + 7 < t.n; r += 8) {
+        double b[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++) b[j] = LM(rhs, r + j);
+#pragma unroll
+        for (int j = 0; j < 8; j++) SL(y, t.pinv[r + j]) = (T)(-b[j]);
+    }
+    for (; r < t.n; r++) SL(y, t.pinv[r]) = (T)(-LM(rhs, r));
     subst_smem<T>(t, s, y, lane);
     for (uint32_t j = 0; j < t.n; j++) {
         LM(dx, t.q[j]) = (double)SL(y, j);

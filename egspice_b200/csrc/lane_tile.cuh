@@ -234,8 +234,8 @@ __device__ __forceinline__ double gather_sum(const double* __restrict__ cells, u
 
 // Gather phase: A (G + ag0 C, with gmin on the diagonals), the residual
 // with the companion rows and gmin load, and the row charges.
-__device__ __forceinline__ double gather_slot(const GroupDev& d, uint32_t l, uint32_t p, const Companion& cp,
-                                              double gmin) {
+__device__ __forceinline__ double slot_value(const GroupDev& d, uint32_t l, uint32_t p, const Companion& cp,
+                                             double gmin) {
     const uint32_t P = d.P;
     double g = gather_sum(d.cells, P, l, d.g_ptr, d.g_cell, p);
     double a = g;
@@ -244,6 +244,13 @@ __device__ __forceinline__ double gather_slot(const GroupDev& d, uint32_t l, uin
         a = g + cp.ag0 * c;
     }
     if (gmin > 0.0 && d.slot_diag[p]) a += gmin;
+    return a;
+}
+
+__device__ __forceinline__ double gather_slot(const GroupDev& d, uint32_t l, uint32_t p, const Companion& cp,
+                                              double gmin) {
+    const uint32_t P = d.P;
+    double a = slot_value(d, l, p, cp, gmin);
     LM(d.a, p) = a;
     return a;
 }

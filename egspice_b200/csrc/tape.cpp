@@ -801,4 +801,39 @@ bool factor_tape(uint32_t n, const uint32_t* col_ptr, const uint32_t* row_idx, c
     return true;
 }
 
+bool lu_program(const Tape& t, const uint32_t* col_ptr, std::vector<uint32_t>& prog) {
+    prog.clear();
+    const uint32_t n = t.n;
+    auto fits = [](uint64_t v) { return v < 65536u; };
+    if (!fits(n) || !fits(t.prow.size()) || !fits(t.li.size()) || !fits(t.ui.size())) return false;
+    auto pack = [](uint32_t hi, uint32_t lo) { return (hi << 16) | lo; };
+    for (uint32_t k = 0; k < n; k++) {
+        uint32_t c = t.q[k];
+        uint32_t fl = t.flags[k];
+        uint32_t cnt = col_ptr[c + 1] - col_ptr[c];
+        if (cnt) {
+            prog.push_back(kOpScat | (cnt << 4));
+            for (uint32_t p = col_ptr[c]; p < col_ptr[c + 1]; p++) prog.push_back(pack(t.prow[p], p));
+        }
+        for (uint32_t p = t.up[k]; p < t.up[k + 1]; p++) {
+            uint32_t i = t.ui[p];
+            uint32_t m = t.lp[i + 1] - t.lp[i];
+            prog.push_back(kOpTake | (m << 4));
+            prog.push_back(pack(i, p));
+            for (uint32_t pl = t.lp[i]; pl < t.lp[i + 1]; pl++) prog.push_back(pack(t.li[pl], pl));
+        }
+        if (fl & 1u) {
+            prog.push_back(kOpVoid);
+            prog.push_back(k);
+            continue;
+        }
+        uint32_t m = t.lp[k + 1] - t.lp[k];
+        prog.push_back(kOpPiv | ((fl & 15u) << 4) | (m << 8));
+        prog.push_back(k);
+        for (uint32_t p = t.lp[k]; p < t.lp[k + 1]; p++) prog.push_back(pack(t.li[p], p));
+    }
+    prog.push_back(kOpEnd);
+    return true;
+}
+
 }  // namespace espl

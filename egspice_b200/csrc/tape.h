@@ -40,4 +40,18 @@ struct Tape {
 bool factor_tape(uint32_t n, const uint32_t* col_ptr, const uint32_t* row_idx, const double* vals,
                  const std::vector<uint32_t>& q, Tape& out);
 
+// The replay as a flat program for the shared-memory LU chain: per column,
+// the scatter of A's column, each U entry's take with the axpy of its L
+// column, and the pivot with the division of the column's L entries, in the
+// replay's order (kernels/lane.zig:56-125). Entries are (row << 16 | slot)
+// words, so every index must be below 2^16; false (empty program) when one
+// is not.
+//   SCAT  hdr = 1 | cnt << 4, then cnt x (w row << 16 | A slot)
+//   TAKE  hdr = 2 | cnt << 4, then (i << 16 | U slot), then cnt x (L row << 16 | L slot)
+//   PIV   hdr = 3 | flags << 4 | cnt << 8, then k, then cnt x (L row << 16 | L slot)
+//   VOID  hdr = 4, then k (after column k's scatter and takes: a void column)
+//   END   0
+enum LuOp : uint32_t { kOpEnd = 0, kOpScat = 1, kOpTake = 2, kOpPiv = 3, kOpVoid = 4 };
+bool lu_program(const Tape& t, const uint32_t* col_ptr, std::vector<uint32_t>& prog);
+
 }  // namespace espl
