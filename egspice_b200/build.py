@@ -9,8 +9,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libespice_lanes.so")
-SOURCES = ["espice_lanes.cu", "tape.cpp"]
+SOURCES = ["espice_lanes.cu", "tape.cpp", "mlp.cu"]
 HEADERS = ["lane_engine.cuh", "lane_kernels.cuh", "lane_models.cuh", "lane_smem.cuh", "lane_tile.cuh", "tape.h",
+           "mlp_gemm.cuh", "../../include/espice_learned.h",
            "../../include/espice_lanes.h"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",

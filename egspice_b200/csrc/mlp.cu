@@ -1,0 +1,548 @@
+// The learned warm start: a small MLP (in -> 128 -> 128 -> out, tanh hidden
+// layers) that maps a sweep point's parameters to a Newton start point. Its
+// dense layers run on the tensor cores (k_gemm_tc: tcgen05.mma, BF16 operands,
+// FP32 accumulation in tensor memory); training is this file's own forward,
+// backward (MSE loss) and Adam kernels with FP32 master weights and BF16
+// copies for the GEMMs. Inputs and targets are standardized per feature;
+// predictions are de-standardized to FP64.
+//
+// No counterpart in the reference: ESPice warm-starts lanes from a nominal
+// operating point (--warm-start); this module only changes where Newton
+// starts, never the Newton that judges convergence.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <random>
+#include <string>
+#include <vector>
+
+#include "../../include/espice_learned.h"
+#include "mlp_gemm.cuh"
+
+using namespace espl::mlp;
+
+namespace {
+
+inline int up16(int v) { return (v + 15) & ~15; }
+
+__global__ void k_to_bf16(const float* __restrict__ src, __nv_bfloat16* __restrict__ dst, long long n) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = __float2bfloat16(src[i]);
+}
+
+// Standardized, zero-padded rows: dst[r, j] = (src[r, j] - mean[j]) / std[j]
+// for j < cols, 0 for cols <= j < ld.
+__global__ void k_standardize(const double* __restrict__ src, int rows, int cols, int ld, const float* __restrict__ mean,
+                              const float* __restrict__ stdv, float* __restrict__ dst_f, __nv_bfloat16* __restrict__ dst_b) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= (long long)rows * ld) return;
+    int r = (int)(i / ld), j = (int)(i % ld);
+    float v = 0.0f;
+    if (j < cols) v = (float)((src[(long long)r * cols + j] - (double)mean[j]) / (double)stdv[j]);
+    if (dst_f) dst_f[i] = v;
+    if (dst_b) dst_b[i] = __float2bfloat16(v);
+}
+
+// dY = 2 (Y - T) / (rows * cols) on the real columns (0 on the padding),
+// its BF16 copy, and the loss sum.
+__global__ void k_mse_grad(const float* __restrict__ y, const float* __restrict__ t, int rows, int cols, int ld,
+                           float* __restrict__ dy, __nv_bfloat16* __restrict__ dyb, double* __restrict__ loss) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    float l = 0.0f;
+    if (i < (long long)rows * ld) {
+        int j = (int)(i % ld);
+        float g = 0.0f;
+        if (j < cols) {
+            float e = y[i] - t[i];
+            l = e * e;
+            g = 2.0f * e / ((float)rows * (float)cols);
+        }
+        dy[i] = g;
+        dyb[i] = __float2bfloat16(g);
+    }
+    for (int o = 16; o > 0; o >>= 1) l += __shfl_down_sync(0xffffffffu, l, o);
+    if ((threadIdx.x & 31) == 0 && l != 0.0f) atomicAdd(loss, (double)l);
+}
+
+// dZ = dH * (1 - H^2) (tanh), with its BF16 copy.
+__global__ void k_tanh_back(const float* __restrict__ dh, const float* __restrict__ h, long long n,
+                            float* __restrict__ dz, __nv_bfloat16* __restrict__ dzb) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float v = h[i];
+    float g = dh[i] * (1.0f - v * v);
+    dz[i] = g;
+    dzb[i] = __float2bfloat16(g);
+}
+
+// out[j] += sum over rows of src[r, j] (bias gradients).
+__global__ void k_colsum(const float* __restrict__ src, int rows, int ld, int cols, float* __restrict__ out) {
+    int j = blockIdx.x;
+    if (j >= cols) return;
+    float s = 0.0f;
+    for (int r = threadIdx.x; r < rows; r += blockDim.x) s += src[(long long)r * ld + j];
+    __shared__ float part[256];
+    part[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) part[threadIdx.x] += part[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[j] += part[0];
+}
+
+// Adam with bias correction on the FP32 master parameters.
+__global__ void k_adam(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m, float* __restrict__ v,
+                       long long n, float lr, float b1, float b2, float eps, float c1, float c2) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float gi = g[i];
+    float mi = b1 * m[i] + (1.0f - b1) * gi;
+    float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+}
+
+__global__ void k_destandardize(const float* __restrict__ y, int rows, int cols, int ld, const float* __restrict__ mean,
+                                const float* __restrict__ stdv, double* __restrict__ out) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= (long long)rows * cols) return;
+    int r = (int)(i / cols), j = (int)(i % cols);
+    out[i] = (double)y[(long long)r * ld + j] * (double)stdv[j] + (double)mean[j];
+}
+
+inline unsigned blocks(long long n, int t = 256) { return (unsigned)((n + t - 1) / t); }
+
+}  // namespace
+
+struct espl_mlp {
+    int device = 0;
+    int D = 0, Dp = 0, H = 128, O = 0, Op = 0, cap = 0;
+    // parameters, packed: W1 [H x Dp], b1 [H], W2 [H x H], b2 [H], W3 [Op x H], b3 [Op]
+    long long off_w1 = 0, off_b1 = 0, off_w2 = 0, off_b2 = 0, off_w3 = 0, off_b3 = 0, n_par = 0;
+    float *p = nullptr, *g = nullptr, *m = nullptr, *v = nullptr;
+    __nv_bfloat16 *w1b = nullptr, *w2b = nullptr, *w3b = nullptr;
+    float *in_mean = nullptr, *in_std = nullptr, *out_mean = nullptr, *out_std = nullptr;
+    bool scaled = false;
+    // batch buffers (cap rows)
+    double *x_raw = nullptr, *y_raw = nullptr;
+    __nv_bfloat16 *xb = nullptr, *h1b = nullptr, *h2b = nullptr, *dyb = nullptr, *dzb = nullptr;
+    float *t = nullptr, *h1 = nullptr, *h2 = nullptr, *y = nullptr, *dy = nullptr, *dh = nullptr, *dz = nullptr;
+    double* loss = nullptr;
+    int* err = nullptr;
+    long long adam_t = 0;
+    cudaStream_t stream = nullptr;
+    std::vector<void*> owned;
+    std::string msg;
+};
+
+namespace {
+
+#define MCK(call)                                                                                   \
+    do {                                                                                            \
+        cudaError_t e_ = (call);                                                                    \
+        if (e_ != cudaSuccess) {                                                                    \
+            if (h) h->msg = std::string(#call) + ": " + cudaGetErrorString(e_);                     \
+            return e_ == cudaErrorMemoryAllocation ? (espl_status)ESPL_OUT_OF_MEMORY                \
+                                                   : (espl_status)ESPL_DRIVER;                      \
+        }                                                                                           \
+    } while (0)
+
+template <typename T>
+espl_status alloc(espl_mlp* h, T** out, size_t count) {
+    void* q = nullptr;
+    MCK(cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T)));
+    MCK(cudaMemsetAsync(q, 0, std::max<size_t>(count, 1) * sizeof(T), h->stream));
+    h->owned.push_back(q);
+    *out = static_cast<T*>(q);
+    return ESPL_OK;
+}
+
+// One GEMM C = A B^T through the tensor cores (see mlp_gemm.cuh).
+template <int EPI>
+espl_status gemm(espl_mlp* h, const __nv_bfloat16* a, long long sam, long long sak, const __nv_bfloat16* b,
+                 long long sbn, long long sbk, float* c, int ldc, int M, int N, int K, const float* bias = nullptr,
+                 __nv_bfloat16* cb = nullptr, int splits = 1) {
+    GemmArgs g{a, b, sam, sak, sbn, sbk, c, cb, bias, M, N, K, ldc, 0, h->err};
+    int kps = (K + splits - 1) / splits;
+    kps = (kps + kBK - 1) / kBK * kBK;
+    g.k_per_split = std::max(kps, kBK);
+    int gz = (K + g.k_per_split - 1) / g.k_per_split;
+    if (N <= 16) {
+        dim3 grid((M + kBM - 1) / kBM, (N + 15) / 16, gz);
+        k_gemm_tc<16, EPI><<<grid, kGemmThreads, 0, h->stream>>>(g);
+    } else if (N <= 32) {
+        dim3 grid((M + kBM - 1) / kBM, (N + 31) / 32, gz);
+        k_gemm_tc<32, EPI><<<grid, kGemmThreads, 0, h->stream>>>(g);
+    } else {
+        dim3 grid((M + kBM - 1) / kBM, (N + 127) / 128, gz);
+        k_gemm_tc<128, EPI><<<grid, kGemmThreads, 0, h->stream>>>(g);
+    }
+    MCK(cudaGetLastError());
+    return ESPL_OK;
+}
+
+espl_status refresh_bf16(espl_mlp* h) {
+    k_to_bf16<<<blocks((long long)h->H * h->Dp), 256, 0, h->stream>>>(h->p + h->off_w1, h->w1b, (long long)h->H * h->Dp);
+    k_to_bf16<<<blocks((long long)h->H * h->H), 256, 0, h->stream>>>(h->p + h->off_w2, h->w2b, (long long)h->H * h->H);
+    k_to_bf16<<<blocks((long long)h->Op * h->H), 256, 0, h->stream>>>(h->p + h->off_w3, h->w3b, (long long)h->Op * h->H);
+    MCK(cudaGetLastError());
+    return ESPL_OK;
+}
+
+// Forward of `rows` standardized rows already in xb: h1, h2 (FP32 + BF16), y.
+espl_status forward(espl_mlp* h, int rows) {
+    espl_status s;
+    const int H = h->H;
+    if ((s = gemm<kEpiBiasTanh>(h, h->xb, h->Dp, 1, h->w1b, h->Dp, 1, h->h1, H, rows, H, h->Dp, h->p + h->off_b1,
+                                h->h1b)))
+        return s;
+    if ((s = gemm<kEpiBiasTanh>(h, h->h1b, H, 1, h->w2b, H, 1, h->h2, H, rows, H, H, h->p + h->off_b2, h->h2b)))
+        return s;
+    return gemm<kEpiBias>(h, h->h2b, H, 1, h->w3b, H, 1, h->y, h->Op, rows, h->Op, H, h->p + h->off_b3);
+}
+
+// Loss and gradients (into h->g) of `rows` rows with targets in h->t.
+espl_status backward(espl_mlp* h, int rows) {
+    espl_status s;
+    const int H = h->H, Op = h->Op, Dp = h->Dp;
+    MCK(cudaMemsetAsync(h->g, 0, sizeof(float) * h->n_par, h->stream));
+    MCK(cudaMemsetAsync(h->loss, 0, sizeof(double), h->stream));
+    k_mse_grad<<<blocks((long long)rows * Op), 256, 0, h->stream>>>(h->y, h->t, rows, h->O, Op, h->dy, h->dyb,
+                                                                    h->loss);
+    const int splits = std::max(1, std::min(64, rows / 256));
+    // layer 3: dW3 = dY^T H2, db3 = colsum dY, dH2 = dY W3
+    if ((s = gemm<kEpiAtomic>(h, h->dyb, 1, Op, h->h2b, 1, H, h->g + h->off_w3, H, Op, H, rows, nullptr, nullptr,
+                              splits)))
+        return s;
+    k_colsum<<<Op, 256, 0, h->stream>>>(h->dy, rows, Op, Op, h->g + h->off_b3);
+    if ((s = gemm<kEpiStore>(h, h->dyb, Op, 1, h->w3b, 1, H, h->dh, H, rows, H, Op))) return s;
+    k_tanh_back<<<blocks((long long)rows * H), 256, 0, h->stream>>>(h->dh, h->h2, (long long)rows * H, h->dz, h->dzb);
+    // layer 2
+    if ((s = gemm<kEpiAtomic>(h, h->dzb, 1, H, h->h1b, 1, H, h->g + h->off_w2, H, H, H, rows, nullptr, nullptr,
+                              splits)))
+        return s;
+    k_colsum<<<H, 256, 0, h->stream>>>(h->dz, rows, H, H, h->g + h->off_b2);
+    if ((s = gemm<kEpiStore>(h, h->dzb, H, 1, h->w2b, 1, H, h->dh, H, rows, H, H))) return s;
+    k_tanh_back<<<blocks((long long)rows * H), 256, 0, h->stream>>>(h->dh, h->h1, (long long)rows * H, h->dz, h->dzb);
+    // layer 1
+    if ((s = gemm<kEpiAtomic>(h, h->dzb, 1, H, h->xb, 1, Dp, h->g + h->off_w1, Dp, H, Dp, rows, nullptr, nullptr,
+                              splits)))
+        return s;
+    k_colsum<<<H, 256, 0, h->stream>>>(h->dz, rows, H, H, h->g + h->off_b1);
+    MCK(cudaGetLastError());
+    return ESPL_OK;
+}
+
+espl_status check_err(espl_mlp* h) {
+    int e = 0;
+    MCK(cudaMemcpyAsync(&e, h->err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    MCK(cudaStreamSynchronize(h->stream));
+    if (e) {
+        h->msg = "a tensor-core GEMM wait ran out";
+        return ESPL_TIMEOUT;
+    }
+    return ESPL_OK;
+}
+
+// Uploads rows [r0, r0 + rows) of x (and y) standardized into the batch buffers.
+espl_status upload(espl_mlp* h, const double* x, const double* y, const std::vector<uint32_t>* order, long long r0,
+                   int rows) {
+    std::vector<double> xs, ys;
+    const double* xp = x + r0 * h->D;
+    const double* yp = y ? y + r0 * h->O : nullptr;
+    if (order) {
+        xs.resize((size_t)rows * h->D);
+        if (y) ys.resize((size_t)rows * h->O);
+        for (int r = 0; r < rows; r++) {
+            uint32_t src = (*order)[r0 + r];
+            std::memcpy(&xs[(size_t)r * h->D], x + (size_t)src * h->D, sizeof(double) * h->D);
+            if (y) std::memcpy(&ys[(size_t)r * h->O], y + (size_t)src * h->O, sizeof(double) * h->O);
+        }
+        xp = xs.data();
+        yp = y ? ys.data() : nullptr;
+    }
+    MCK(cudaMemcpyAsync(h->x_raw, xp, sizeof(double) * rows * h->D, cudaMemcpyHostToDevice, h->stream));
+    k_standardize<<<blocks((long long)rows * h->Dp), 256, 0, h->stream>>>(h->x_raw, rows, h->D, h->Dp, h->in_mean,
+                                                                          h->in_std, nullptr, h->xb);
+    if (yp) {
+        MCK(cudaMemcpyAsync(h->y_raw, yp, sizeof(double) * rows * h->O, cudaMemcpyHostToDevice, h->stream));
+        k_standardize<<<blocks((long long)rows * h->Op), 256, 0, h->stream>>>(h->y_raw, rows, h->O, h->Op,
+                                                                              h->out_mean, h->out_std, h->t, nullptr);
+    }
+    MCK(cudaGetLastError());
+    // the raw buffers are reused by the next upload; keep the copies ordered
+    MCK(cudaStreamSynchronize(h->stream));
+    return ESPL_OK;
+}
+
+espl_status set_scaling(espl_mlp* h, const double* x, const double* y, uint32_t n) {
+    auto stats = [&](const double* a, int cols, int ld, std::vector<float>& mean, std::vector<float>& sd) {
+        mean.assign(ld, 0.0f);
+        sd.assign(ld, 1.0f);
+        for (int j = 0; j < cols; j++) {
+            double s = 0, s2 = 0;
+            for (uint32_t r = 0; r < n; r++) s += a[(size_t)r * cols + j];
+            double mu = s / n;
+            for (uint32_t r = 0; r < n; r++) {
+                double e = a[(size_t)r * cols + j] - mu;
+                s2 += e * e;
+            }
+            double sdv = std::sqrt(s2 / std::max<uint32_t>(n, 1));
+            mean[j] = (float)mu;
+            sd[j] = (float)(sdv > 1e-12 ? sdv : 1.0);
+        }
+    };
+    std::vector<float> im, is, om, os;
+    stats(x, h->D, h->Dp, im, is);
+    stats(y, h->O, h->Op, om, os);
+    MCK(cudaMemcpyAsync(h->in_mean, im.data(), sizeof(float) * h->Dp, cudaMemcpyHostToDevice, h->stream));
+    MCK(cudaMemcpyAsync(h->in_std, is.data(), sizeof(float) * h->Dp, cudaMemcpyHostToDevice, h->stream));
+    MCK(cudaMemcpyAsync(h->out_mean, om.data(), sizeof(float) * h->Op, cudaMemcpyHostToDevice, h->stream));
+    MCK(cudaMemcpyAsync(h->out_std, os.data(), sizeof(float) * h->Op, cudaMemcpyHostToDevice, h->stream));
+    MCK(cudaStreamSynchronize(h->stream));
+    h->scaled = true;
+    return ESPL_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+espl_status espl_mlp_create(uint32_t in_dim, uint32_t out_dim, uint32_t capacity, uint64_t seed, uint32_t device,
+                            espl_mlp** out) {
+    if (!out) return ESPL_INVALID_ARGUMENT;
+    *out = nullptr;
+    if (in_dim == 0 || in_dim > 128 || out_dim == 0 || out_dim > 128 || capacity == 0) return ESPL_INVALID_ARGUMENT;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return ESPL_NO_IMAGE;
+    if ((int)device >= ndev) return ESPL_INVALID_ARGUMENT;
+    espl_mlp* h = new espl_mlp();
+    auto bail = [&](espl_status s) {
+        espl_mlp_destroy(h);
+        return s;
+    };
+    h->device = (int)device;
+    if (cudaSetDevice(h->device) != cudaSuccess) return bail(ESPL_DRIVER);
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, k_gemm_tc<128, kEpiStore>) != cudaSuccess) return bail(ESPL_NO_IMAGE);
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(ESPL_DRIVER);
+    h->D = (int)in_dim;
+    h->Dp = up16(h->D);
+    h->O = (int)out_dim;
+    h->Op = up16(h->O);
+    h->cap = (int)((capacity + 127) / 128 * 128);
+    const int H = h->H;
+    h->off_w1 = 0;
+    h->off_b1 = h->off_w1 + (long long)H * h->Dp;
+    h->off_w2 = h->off_b1 + H;
+    h->off_b2 = h->off_w2 + (long long)H * H;
+    h->off_w3 = h->off_b2 + H;
+    h->off_b3 = h->off_w3 + (long long)h->Op * H;
+    h->n_par = h->off_b3 + h->Op;
+    espl_status s;
+#define AL(ptr, count) if ((s = alloc(h, &h->ptr, count))) return bail(s)
+    AL(p, h->n_par);
+    AL(g, h->n_par);
+    AL(m, h->n_par);
+    AL(v, h->n_par);
+    AL(w1b, (size_t)H * h->Dp);
+    AL(w2b, (size_t)H * H);
+    AL(w3b, (size_t)h->Op * H);
+    AL(in_mean, h->Dp);
+    AL(in_std, h->Dp);
+    AL(out_mean, h->Op);
+    AL(out_std, h->Op);
+    const size_t c = (size_t)h->cap;
+    AL(x_raw, c * h->D);
+    AL(y_raw, c * h->O);
+    AL(xb, c * h->Dp);
+    AL(t, c * h->Op);
+    AL(h1, c * H);
+    AL(h1b, c * H);
+    AL(h2, c * H);
+    AL(h2b, c * H);
+    AL(y, c * h->Op);
+    AL(dy, c * h->Op);
+    AL(dyb, c * h->Op);
+    AL(dh, c * H);
+    AL(dz, c * H);
+    AL(dzb, c * H);
+    AL(loss, 1);
+    AL(err, 1);
+#undef AL
+    // Glorot-uniform weights from the seed, zero biases (host draw, FP32).
+    std::vector<float> par((size_t)h->n_par, 0.0f);
+    std::mt19937_64 rng(seed);
+    auto fill = [&](long long off, int rows, int cols, int ld) {
+        float a = std::sqrt(6.0f / (float)(rows + cols));
+        std::uniform_real_distribution<float> u(-a, a);
+        for (int r = 0; r < rows; r++)
+            for (int cc = 0; cc < cols; cc++) par[(size_t)(off + (long long)r * ld + cc)] = u(rng);
+    };
+    fill(h->off_w1, H, h->D, h->Dp);
+    fill(h->off_w2, H, H, H);
+    fill(h->off_w3, h->O, H, H);
+    if (cudaMemcpyAsync(h->p, par.data(), sizeof(float) * par.size(), cudaMemcpyHostToDevice, h->stream) != cudaSuccess)
+        return bail(ESPL_DRIVER);
+    std::vector<float> ones(std::max(h->Dp, h->Op), 1.0f);
+    cudaMemcpyAsync(h->in_std, ones.data(), sizeof(float) * h->Dp, cudaMemcpyHostToDevice, h->stream);
+    cudaMemcpyAsync(h->out_std, ones.data(), sizeof(float) * h->Op, cudaMemcpyHostToDevice, h->stream);
+    if ((s = refresh_bf16(h))) return bail(s);
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) return bail(ESPL_DRIVER);
+    *out = h;
+    return ESPL_OK;
+}
+
+espl_status espl_mlp_destroy(espl_mlp* h) {
+    if (!h) return ESPL_OK;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (void* q : h->owned) cudaFree(q);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return ESPL_OK;
+}
+
+espl_status espl_mlp_param_count(const espl_mlp* h, uint32_t* count) {
+    if (!h || !count) return ESPL_INVALID_ARGUMENT;
+    *count = (uint32_t)((long long)h->H * h->D + h->H + (long long)h->H * h->H + h->H + (long long)h->O * h->H + h->O);
+    return ESPL_OK;
+}
+
+// Parameters in the API order W1 [128 x in], b1, W2 [128 x 128], b2,
+// W3 [out x 128], b3 (row-major), FP32.
+espl_status espl_mlp_get_params(espl_mlp* h, float* out) {
+    if (!h || !out) return ESPL_INVALID_ARGUMENT;
+    std::vector<float> par((size_t)h->n_par);
+    MCK(cudaMemcpyAsync(par.data(), h->p, sizeof(float) * par.size(), cudaMemcpyDeviceToHost, h->stream));
+    MCK(cudaStreamSynchronize(h->stream));
+    size_t k = 0;
+    const int H = h->H;
+    for (int r = 0; r < H; r++)
+        for (int c = 0; c < h->D; c++) out[k++] = par[(size_t)(h->off_w1 + (long long)r * h->Dp + c)];
+    for (int r = 0; r < H; r++) out[k++] = par[(size_t)(h->off_b1 + r)];
+    for (long long i = 0; i < (long long)H * H; i++) out[k++] = par[(size_t)(h->off_w2 + i)];
+    for (int r = 0; r < H; r++) out[k++] = par[(size_t)(h->off_b2 + r)];
+    for (int r = 0; r < h->O; r++)
+        for (int c = 0; c < H; c++) out[k++] = par[(size_t)(h->off_w3 + (long long)r * H + c)];
+    for (int r = 0; r < h->O; r++) out[k++] = par[(size_t)(h->off_b3 + r)];
+    return ESPL_OK;
+}
+
+espl_status espl_mlp_set_params(espl_mlp* h, const float* in) {
+    if (!h || !in) return ESPL_INVALID_ARGUMENT;
+    std::vector<float> par((size_t)h->n_par, 0.0f);
+    size_t k = 0;
+    const int H = h->H;
+    for (int r = 0; r < H; r++)
+        for (int c = 0; c < h->D; c++) par[(size_t)(h->off_w1 + (long long)r * h->Dp + c)] = in[k++];
+    for (int r = 0; r < H; r++) par[(size_t)(h->off_b1 + r)] = in[k++];
+    for (long long i = 0; i < (long long)H * H; i++) par[(size_t)(h->off_w2 + i)] = in[k++];
+    for (int r = 0; r < H; r++) par[(size_t)(h->off_b2 + r)] = in[k++];
+    for (int r = 0; r < h->O; r++)
+        for (int c = 0; c < H; c++) par[(size_t)(h->off_w3 + (long long)r * H + c)] = in[k++];
+    for (int r = 0; r < h->O; r++) par[(size_t)(h->off_b3 + r)] = in[k++];
+    MCK(cudaMemcpyAsync(h->p, par.data(), sizeof(float) * par.size(), cudaMemcpyHostToDevice, h->stream));
+    espl_status s = refresh_bf16(h);
+    if (s) return s;
+    MCK(cudaStreamSynchronize(h->stream));
+    return ESPL_OK;
+}
+
+espl_status espl_mlp_set_scaling(espl_mlp* h, const double* x, const double* y, uint32_t n) {
+    if (!h || !x || !y || n == 0) return ESPL_INVALID_ARGUMENT;
+    return set_scaling(h, x, y, n);
+}
+
+espl_status espl_mlp_loss_grad(espl_mlp* h, const double* x, const double* y, uint32_t n, double* loss, float* grad) {
+    if (!h || !x || !y || n == 0 || (int)n > h->cap) return ESPL_INVALID_ARGUMENT;
+    espl_status s;
+    if ((s = upload(h, x, y, nullptr, 0, (int)n))) return s;
+    if ((s = forward(h, (int)n))) return s;
+    if ((s = backward(h, (int)n))) return s;
+    if ((s = check_err(h))) return s;
+    double l = 0;
+    MCK(cudaMemcpyAsync(&l, h->loss, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    MCK(cudaStreamSynchronize(h->stream));
+    if (loss) *loss = l / ((double)n * h->O);
+    if (grad) {
+        // the same API order as espl_mlp_get_params, read from the gradient buffer
+        float* keep = h->p;
+        h->p = h->g;
+        s = espl_mlp_get_params(h, grad);
+        h->p = keep;
+        if (s) return s;
+    }
+    return ESPL_OK;
+}
+
+espl_status espl_mlp_train(espl_mlp* h, const double* x, const double* y, uint32_t n, const espl_train_opts* o,
+                           double* epoch_loss) {
+    if (!h || !x || !y || n == 0 || !o || o->batch == 0 || (int)o->batch > h->cap || o->epochs == 0)
+        return ESPL_INVALID_ARGUMENT;
+    espl_status s;
+    if (!h->scaled && (s = set_scaling(h, x, y, n))) return s;
+    std::vector<uint32_t> order(n);
+    std::iota(order.begin(), order.end(), 0u);
+    std::mt19937_64 rng(o->seed);
+    const float b1 = o->beta1, b2 = o->beta2;
+    for (uint32_t ep = 0; ep < o->epochs; ep++) {
+        std::shuffle(order.begin(), order.end(), rng);
+        double sum = 0;
+        for (uint32_t r0 = 0; r0 + o->batch <= n; r0 += o->batch) {
+            const int rows = (int)o->batch;
+            if ((s = upload(h, x, y, &order, r0, rows))) return s;
+            if ((s = forward(h, rows))) return s;
+            if ((s = backward(h, rows))) return s;
+            h->adam_t++;
+            float c1 = 1.0f - std::pow(b1, (float)h->adam_t), c2 = 1.0f - std::pow(b2, (float)h->adam_t);
+            float lr = o->lr;
+            if (o->lr_final > 0.0f && o->epochs > 1)
+                lr = o->lr * std::pow(o->lr_final / o->lr, (float)ep / (float)(o->epochs - 1));
+            k_adam<<<blocks(h->n_par), 256, 0, h->stream>>>(h->p, h->g, h->m, h->v, h->n_par, lr, b1, b2, o->eps, c1,
+                                                              c2);
+            if ((s = refresh_bf16(h))) return s;
+            double l = 0;
+            MCK(cudaMemcpyAsync(&l, h->loss, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+            MCK(cudaStreamSynchronize(h->stream));
+            sum += l / ((double)rows * h->O);
+        }
+        if ((s = check_err(h))) return s;
+        if (epoch_loss) epoch_loss[ep] = sum / std::max<uint32_t>(1, n / o->batch);
+    }
+    return ESPL_OK;
+}
+
+espl_status espl_mlp_predict(espl_mlp* h, const double* x, uint32_t n, double* y) {
+    if (!h || !x || !y) return ESPL_INVALID_ARGUMENT;
+    espl_status s;
+    double* out = nullptr;
+    for (uint32_t r0 = 0; r0 < n; r0 += (uint32_t)h->cap) {
+        int rows = (int)std::min<uint32_t>((uint32_t)h->cap, n - r0);
+        if ((s = upload(h, x, nullptr, nullptr, r0, rows))) return s;
+        if ((s = forward(h, rows))) return s;
+        out = h->y_raw;  // reuse: rows x O doubles fit (cap x O)
+        k_destandardize<<<blocks((long long)rows * h->O), 256, 0, h->stream>>>(h->y, rows, h->O, h->Op, h->out_mean,
+                                                                              h->out_std, out);
+        MCK(cudaGetLastError());
+        MCK(cudaMemcpyAsync(y + (size_t)r0 * h->O, out, sizeof(double) * rows * h->O, cudaMemcpyDeviceToHost,
+                            h->stream));
+        MCK(cudaStreamSynchronize(h->stream));
+    }
+    return check_err(h);
+}
+
+espl_status espl_mlp_error_message(espl_mlp* h, char* buf, size_t cap) {
+    if (!h || !buf || cap == 0) return ESPL_INVALID_ARGUMENT;
+    size_t k = std::min(cap - 1, h->msg.size());
+    std::memcpy(buf, h->msg.data(), k);
+    buf[k] = 0;
+    return ESPL_OK;
+}
+
+}  // extern "C"
