@@ -248,6 +248,84 @@ def run_ring_sweep(nets, topts, precision, steps_per_launch=5000):
     return dev_ms, wall, xs, reps, tapes, launches, periods
 
 
+def opamp_nominal(net):
+    x0 = np.zeros((net.lanes, net.n))
+    for k, v in dict(vdd=1.8, inp=0.9, vb=0.58, n1=1.2, out=0.9, tail=0.25, n2=1.2).items():
+        x0[:, net.node(k)] = v
+    return x0
+
+
+def run_learned_dc(points: int = 65536, train_points: int = 8192, epochs: int = 120, seed: int = 0):
+    """Config 4: a Monte-Carlo op-amp operating-point sweep (16 varied
+    parameters). Plain: every point's Newton (FP64 LU) starts from the
+    nominal operating point. Learned + mixed: the first `train_points` points
+    are solved that way (FP32 LU), the MLP is trained on them on the GPU, and
+    the remaining points start from its predictions. Time = Newton device time
+    plus the MLP's training and inference (wall, synchronized)."""
+    from egspice_b200 import abi, decks
+    from egspice_b200.lanes import Lanes
+    from egspice_b200.learned import Mlp, train_opts
+    net = decks.miller_opamp(points, base_seed=7 + 1000 * seed)
+    x0 = opamp_nominal(net)
+    opts = abi.newton_opts(init_fix=0)
+
+    def solve(sub, start, precision):
+        with Lanes([sub], precision=precision) as L:
+            L.put_x(0, start, False)
+            r = L.solve_static(opts)
+            return r, L.get_x(0), L.stats().newton_ms
+
+    r_plain, x_plain, dev_plain = solve(net, x0, "fp64")
+    head = net.subset(list(range(train_points)))
+    tail = net.subset(list(range(train_points, points)))
+    r_head, x_head, dev_head = solve(head, x0[:train_points], "mixed")
+    import torch
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    with Mlp(net.sweep.shape[1], net.n, capacity=8192, seed=7) as m:
+        losses = m.train(net.sweep[:train_points], x_head, train_opts(epochs=epochs, batch=512, lr=3e-3,
+                                                                      lr_final=1e-4))
+        t_train = time.perf_counter() - t0
+        guess = m.predict(net.sweep[train_points:])
+    t_mlp = time.perf_counter() - t0
+    r_tail, x_tail, dev_tail = solve(tail, guess, "mixed")
+    # plain Newton stays the fallback: a lane that does not converge from its
+    # predicted start is solved again from the nominal one
+    bad = np.nonzero((r_tail[:, 0] & abi.CONVERGED) == 0)[0]
+    refallback = len(bad)
+    if refallback:
+        rb, xb, dev_b = solve(tail.subset(list(bad)), x0[train_points + bad], "mixed")
+        r_tail[bad] = rb
+        x_tail[bad] = xb
+        dev_tail += dev_b
+    x_learned = np.concatenate([x_head, x_tail])
+    r_learned = np.concatenate([r_head, r_tail])
+    conv = lambda r: int(((r[:, 0] & abi.CONVERGED) != 0).sum())  # noqa: E731
+    cur = np.asarray(net.current_rows, dtype=bool)
+    newton_tol = opts.reltol * np.maximum(np.abs(x_plain), np.abs(x_learned)) + np.where(cur, opts.abstol, opts.vntol)
+    err_newton = float((np.abs(x_learned - x_plain) / newton_tol).max())
+    err_bar = float((np.abs(x_learned - x_plain) / (RTOL * np.abs(x_plain) + ATOL)).max())
+    t_plain = dev_plain / 1e3
+    t_learned = (dev_head + dev_tail) / 1e3 + t_mlp
+    return {
+        "workload": f"miller_opamp_mc_dc ({points:,} points, 16 varied parameters)",
+        "plain_fp64": {"points_per_s": points / t_plain, "ms": t_plain * 1e3,
+                       "mean_newton_iters": float(r_plain[:, 1].mean()), "converged": conv(r_plain)},
+        "learned_mixed": {"points_per_s": points / t_learned, "ms": t_learned * 1e3,
+                          "newton_ms": dev_head + dev_tail, "mlp_train_ms": t_train * 1e3,
+                          "mlp_predict_ms": (t_mlp - t_train) * 1e3, "train_points": train_points,
+                          "epochs": epochs, "final_loss": float(losses[-1]),
+                          "mean_newton_iters_predicted": float(r_tail[:, 1].mean()),
+                          "mean_newton_iters_all": float(r_learned[:, 1].mean()), "converged": conv(r_learned),
+                          "fallbacks_to_nominal": refallback},
+        "learned_over_plain": t_plain / t_learned,
+        "max_err_over_newton_tol": err_newton,
+        "max_err_over_1e-6_bar": err_bar,
+        "note": "learned and plain runs stop at the same Newton test, so they agree to the Newton tolerance "
+                "(reltol|x| + vntol), not bit for bit",
+    }
+
+
 def cpu_ring_reference(nets, topts, budget_s: float, threads: int):
     """The oracle on a bounded sample of the ring workload: lanes of the
     31-stage template (the workload's bulk), `threads` at a time, until the
@@ -278,6 +356,7 @@ def main():
     ap.add_argument("--max-steps", type=int, default=5000, help="accepted steps per lane")
     ap.add_argument("--modes", default="fp64,mixed", help="precisions to run, comma-separated")
     ap.add_argument("--no-check", action="store_true", help="skip the oracle check of sampled lanes")
+    ap.add_argument("--no-learned-dc", action="store_true", help="skip the learned warm-start DC measurement")
     args = ap.parse_args()
     modes = [m for m in args.modes.split(",") if m]
     if not modes or any(m not in ("fp64", "mixed") for m in modes):
@@ -404,6 +483,8 @@ def main():
         "gpu_launches": int(best["launches"]),
         "clocks": best["clocks"],
     }
+    if not args.no_learned_dc:
+        line["modes"]["learned_dc"] = run_learned_dc(seed=rank)
     if rank == 0 and not args.no_cpu_baseline and world == 1:
         threads = os.cpu_count() or 1
         v, pts, wall = cpu_ring_reference(nets, topts, args.cpu_budget, threads)

@@ -116,6 +116,22 @@ __global__ void k_destandardize(const float* __restrict__ y, int rows, int cols,
     out[i] = (double)y[(long long)r * ld + j] * (double)stdv[j] + (double)mean[j];
 }
 
+// Rows perm[0 .. rows) of the resident data set into the batch buffers.
+__global__ void k_gather_rows(const __nv_bfloat16* __restrict__ xs, const float* __restrict__ ts,
+                              const uint32_t* __restrict__ perm, int rows, int dp, int op,
+                              __nv_bfloat16* __restrict__ xb, float* __restrict__ t) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    long long nx = (long long)rows * dp, nt = (long long)rows * op;
+    if (i < nx) {
+        int r = (int)(i / dp), j = (int)(i % dp);
+        xb[i] = xs[(long long)perm[r] * dp + j];
+    }
+    if (i < nt) {
+        int r = (int)(i / op), j = (int)(i % op);
+        t[i] = ts[(long long)perm[r] * op + j];
+    }
+}
+
 inline unsigned blocks(long long n, int t = 256) { return (unsigned)((n + t - 1) / t); }
 
 }  // namespace
@@ -207,14 +223,14 @@ espl_status forward(espl_mlp* h, int rows) {
     return gemm<kEpiBias>(h, h->h2b, H, 1, h->w3b, H, 1, h->y, h->Op, rows, h->Op, H, h->p + h->off_b3);
 }
 
-// Loss and gradients (into h->g) of `rows` rows with targets in h->t.
-espl_status backward(espl_mlp* h, int rows) {
+// Gradients (into h->g) of `rows` rows with targets in h->t; the summed
+// squared error is added to *loss.
+espl_status backward(espl_mlp* h, int rows, double* loss) {
     espl_status s;
     const int H = h->H, Op = h->Op, Dp = h->Dp;
     MCK(cudaMemsetAsync(h->g, 0, sizeof(float) * h->n_par, h->stream));
-    MCK(cudaMemsetAsync(h->loss, 0, sizeof(double), h->stream));
     k_mse_grad<<<blocks((long long)rows * Op), 256, 0, h->stream>>>(h->y, h->t, rows, h->O, Op, h->dy, h->dyb,
-                                                                    h->loss);
+                                                                    loss);
     const int splits = std::max(1, std::min(64, rows / 256));
     // layer 3: dW3 = dY^T H2, db3 = colsum dY, dH2 = dY W3
     if ((s = gemm<kEpiAtomic>(h, h->dyb, 1, Op, h->h2b, 1, H, h->g + h->off_w3, H, Op, H, rows, nullptr, nullptr,
@@ -464,7 +480,8 @@ espl_status espl_mlp_loss_grad(espl_mlp* h, const double* x, const double* y, ui
     espl_status s;
     if ((s = upload(h, x, y, nullptr, 0, (int)n))) return s;
     if ((s = forward(h, (int)n))) return s;
-    if ((s = backward(h, (int)n))) return s;
+    MCK(cudaMemsetAsync(h->loss, 0, sizeof(double), h->stream));
+    if ((s = backward(h, (int)n, h->loss))) return s;
     if ((s = check_err(h))) return s;
     double l = 0;
     MCK(cudaMemcpyAsync(&l, h->loss, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
@@ -483,39 +500,85 @@ espl_status espl_mlp_loss_grad(espl_mlp* h, const double* x, const double* y, ui
 
 espl_status espl_mlp_train(espl_mlp* h, const double* x, const double* y, uint32_t n, const espl_train_opts* o,
                            double* epoch_loss) {
-    if (!h || !x || !y || n == 0 || !o || o->batch == 0 || (int)o->batch > h->cap || o->epochs == 0)
+    if (!h || !x || !y || n == 0 || !o || o->batch == 0 || (int)o->batch > h->cap || o->epochs == 0 ||
+        o->batch > n)
         return ESPL_INVALID_ARGUMENT;
-    espl_status s;
+    espl_status s = ESPL_OK;
     if (!h->scaled && (s = set_scaling(h, x, y, n))) return s;
+    // The data set stays on the device, standardized; each epoch uploads a
+    // permutation and every Adam step gathers its rows on the device.
+    double *xr = nullptr, *yr = nullptr, *lsum = nullptr;
+    __nv_bfloat16* xs = nullptr;
+    float* ts = nullptr;
+    uint32_t* perm = nullptr;
+    std::vector<void*> tmp;
+    auto dalloc = [&](void** q, size_t bytes) {
+        cudaError_t e = cudaMalloc(q, bytes);
+        if (e == cudaSuccess) tmp.push_back(*q);
+        return e;
+    };
+    auto cleanup = [&]() {
+        cudaStreamSynchronize(h->stream);
+        for (void* q : tmp) cudaFree(q);
+    };
+    if (dalloc((void**)&xr, sizeof(double) * n * h->D) || dalloc((void**)&yr, sizeof(double) * n * h->O) ||
+        dalloc((void**)&xs, sizeof(__nv_bfloat16) * n * h->Dp) || dalloc((void**)&ts, sizeof(float) * n * h->Op) ||
+        dalloc((void**)&perm, sizeof(uint32_t) * n) || dalloc((void**)&lsum, sizeof(double) * o->epochs)) {
+        cleanup();
+        h->msg = "out of device memory for the training set";
+        return ESPL_OUT_OF_MEMORY;
+    }
+    cudaMemcpyAsync(xr, x, sizeof(double) * n * h->D, cudaMemcpyHostToDevice, h->stream);
+    cudaMemcpyAsync(yr, y, sizeof(double) * n * h->O, cudaMemcpyHostToDevice, h->stream);
+    cudaMemsetAsync(lsum, 0, sizeof(double) * o->epochs, h->stream);
+    k_standardize<<<blocks((long long)n * h->Dp), 256, 0, h->stream>>>(xr, (int)n, h->D, h->Dp, h->in_mean, h->in_std,
+                                                                        nullptr, xs);
+    k_standardize<<<blocks((long long)n * h->Op), 256, 0, h->stream>>>(yr, (int)n, h->O, h->Op, h->out_mean,
+                                                                        h->out_std, ts, nullptr);
     std::vector<uint32_t> order(n);
     std::iota(order.begin(), order.end(), 0u);
     std::mt19937_64 rng(o->seed);
     const float b1 = o->beta1, b2 = o->beta2;
-    for (uint32_t ep = 0; ep < o->epochs; ep++) {
+    const uint32_t per_epoch = n / o->batch;
+    const int rows = (int)o->batch;
+    for (uint32_t ep = 0; ep < o->epochs && !s; ep++) {
         std::shuffle(order.begin(), order.end(), rng);
-        double sum = 0;
-        for (uint32_t r0 = 0; r0 + o->batch <= n; r0 += o->batch) {
-            const int rows = (int)o->batch;
-            if ((s = upload(h, x, y, &order, r0, rows))) return s;
-            if ((s = forward(h, rows))) return s;
-            if ((s = backward(h, rows))) return s;
+        // the permutation buffer is rewritten each epoch: order the copy
+        // after the previous epoch's gathers
+        if (cudaStreamSynchronize(h->stream) != cudaSuccess ||
+            cudaMemcpyAsync(perm, order.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, h->stream) !=
+                cudaSuccess) {
+            s = ESPL_DRIVER;
+            break;
+        }
+        float lr = o->lr;
+        if (o->lr_final > 0.0f && o->epochs > 1)
+            lr = o->lr * std::pow(o->lr_final / o->lr, (float)ep / (float)(o->epochs - 1));
+        for (uint32_t b = 0; b < per_epoch && !s; b++) {
+            long long nb = (long long)rows * std::max(h->Dp, h->Op);
+            k_gather_rows<<<blocks(nb), 256, 0, h->stream>>>(xs, ts, perm + (size_t)b * rows, rows, h->Dp, h->Op,
+                                                             h->xb, h->t);
+            if ((s = forward(h, rows))) break;
+            if ((s = backward(h, rows, lsum + ep))) break;
             h->adam_t++;
             float c1 = 1.0f - std::pow(b1, (float)h->adam_t), c2 = 1.0f - std::pow(b2, (float)h->adam_t);
-            float lr = o->lr;
-            if (o->lr_final > 0.0f && o->epochs > 1)
-                lr = o->lr * std::pow(o->lr_final / o->lr, (float)ep / (float)(o->epochs - 1));
             k_adam<<<blocks(h->n_par), 256, 0, h->stream>>>(h->p, h->g, h->m, h->v, h->n_par, lr, b1, b2, o->eps, c1,
                                                               c2);
-            if ((s = refresh_bf16(h))) return s;
-            double l = 0;
-            MCK(cudaMemcpyAsync(&l, h->loss, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-            MCK(cudaStreamSynchronize(h->stream));
-            sum += l / ((double)rows * h->O);
+            s = refresh_bf16(h);
         }
-        if ((s = check_err(h))) return s;
-        if (epoch_loss) epoch_loss[ep] = sum / std::max<uint32_t>(1, n / o->batch);
     }
-    return ESPL_OK;
+    if (!s) s = check_err(h);
+    if (!s && epoch_loss) {
+        std::vector<double> l(o->epochs);
+        if (cudaMemcpyAsync(l.data(), lsum, sizeof(double) * o->epochs, cudaMemcpyDeviceToHost, h->stream) !=
+                cudaSuccess ||
+            cudaStreamSynchronize(h->stream) != cudaSuccess)
+            s = ESPL_DRIVER;
+        for (uint32_t ep = 0; ep < o->epochs && !s; ep++)
+            epoch_loss[ep] = l[ep] / ((double)per_epoch * rows * h->O);
+    }
+    cleanup();
+    return s;
 }
 
 espl_status espl_mlp_predict(espl_mlp* h, const double* x, uint32_t n, double* y) {
