@@ -583,13 +583,52 @@ espl_status espl_mlp_train(espl_mlp* h, const double* x, const double* y, uint32
 
 espl_status espl_mlp_predict(espl_mlp* h, const double* x, uint32_t n, double* y) {
     if (!h || !x || !y) return ESPL_INVALID_ARGUMENT;
+    if (n == 0) return ESPL_OK;
+    // One fused launch (k_mlp_infer): each CTA runs the whole network on 128
+    // rows with the weights and activations in shared memory.
+    double *dx = nullptr, *dy = nullptr;
+    MCK(cudaMalloc(&dx, sizeof(double) * (size_t)n * h->D));
+    if (cudaMalloc(&dy, sizeof(double) * (size_t)n * h->O) != cudaSuccess) {
+        cudaFree(dx);
+        h->msg = "out of device memory for the predictions";
+        return ESPL_OUT_OF_MEMORY;
+    }
+    espl_status s = ESPL_OK;
+    const size_t smem = infer_smem_bytes(h->Dp, h->Op);
+    InferArgs g{dx, dy, h->p + h->off_w1, h->p + h->off_b1, h->p + h->off_w2, h->p + h->off_b2, h->p + h->off_w3,
+                h->p + h->off_b3, h->in_mean, h->in_std, h->out_mean, h->out_std, (int)n, h->D, h->Dp, h->O, h->Op,
+                h->err};
+    if (cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+        cudaMemcpyAsync(dx, x, sizeof(double) * (size_t)n * h->D, cudaMemcpyHostToDevice, h->stream) != cudaSuccess) {
+        s = ESPL_DRIVER;
+    } else {
+        k_mlp_infer<<<(n + 127) / 128, 128, smem, h->stream>>>(g);
+        if (cudaGetLastError() != cudaSuccess ||
+            cudaMemcpyAsync(y, dy, sizeof(double) * (size_t)n * h->O, cudaMemcpyDeviceToHost, h->stream) !=
+                cudaSuccess)
+            s = ESPL_DRIVER;
+    }
+    cudaStreamSynchronize(h->stream);
+    cudaFree(dx);
+    cudaFree(dy);
+    if (s) {
+        h->msg = "predict launch failed";
+        return s;
+    }
+    return check_err(h);
+}
+
+// The layer-by-layer predictions through the training GEMMs (one launch per
+// layer on capacity-sized chunks): the fused kernel's cross-check.
+espl_status espl_mlp_predict_layers(espl_mlp* h, const double* x, uint32_t n, double* y) {
+    if (!h || !x || !y) return ESPL_INVALID_ARGUMENT;
     espl_status s;
     double* out = nullptr;
     for (uint32_t r0 = 0; r0 < n; r0 += (uint32_t)h->cap) {
         int rows = (int)std::min<uint32_t>((uint32_t)h->cap, n - r0);
         if ((s = upload(h, x, nullptr, nullptr, r0, rows))) return s;
         if ((s = forward(h, rows))) return s;
-        out = h->y_raw;  // reuse: rows x O doubles fit (cap x O)
+        out = h->y_raw;  // rows x O doubles fit (cap x O)
         k_destandardize<<<blocks((long long)rows * h->O), 256, 0, h->stream>>>(h->y, rows, h->O, h->Op, h->out_mean,
                                                                               h->out_std, out);
         MCK(cudaGetLastError());

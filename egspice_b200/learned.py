@@ -1,10 +1,11 @@
 """The learned warm start (include/espice_learned.h) from Python.
 
-`Mlp` wraps the tensor-core MLP of egspice_b200/csrc/mlp.cu; `warm_start`
-trains it on operating points the plain method solved and predicts start
-points for the rest of a sweep. Newton from the predicted x is the same
-plain Newton (espl_solve_static), so the answers do not change, only the
-iteration counts.
+`Mlp` wraps the tensor-core MLP of egspice_b200/csrc/mlp.cu: it is trained on
+operating points the plain method solved and predicts start points for the
+rest of a sweep. Newton from a predicted x is the same plain Newton
+(espl_solve_static) with the same tolerances, so only the iteration count
+changes; a lane that does not converge from its prediction is solved again
+from the nominal start (bench.py run_learned_dc).
 """
 from __future__ import annotations
 
@@ -41,9 +42,10 @@ def _setup(L):
     L.espl_mlp_loss_grad.argtypes = [C.c_void_p, f64p, f64p, C.c_uint32, f64p, f32p]
     L.espl_mlp_train.argtypes = [C.c_void_p, f64p, f64p, C.c_uint32, C.POINTER(TrainOpts), f64p]
     L.espl_mlp_predict.argtypes = [C.c_void_p, f64p, C.c_uint32, f64p]
+    L.espl_mlp_predict_layers.argtypes = [C.c_void_p, f64p, C.c_uint32, f64p]
     L.espl_mlp_error_message.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t]
     for f in ("create", "destroy", "param_count", "get_params", "set_params", "set_scaling", "loss_grad", "train",
-              "predict", "error_message"):
+              "predict", "predict_layers", "error_message"):
         getattr(L, "espl_mlp_" + f).restype = C.c_uint32
     L._mlp_ready = True
     return L
@@ -114,11 +116,11 @@ class Mlp:
                                           C.byref(opts), losses.ctypes.data_as(f64p)), "train")
         return losses
 
-    def predict(self, x) -> np.ndarray:
+    def predict(self, x, fused: bool = True) -> np.ndarray:
         x = _f64(x)
         y = np.zeros((len(x), self.out_dim))
-        self._check(self.L.espl_mlp_predict(self.h, x.ctypes.data_as(f64p), len(x), y.ctypes.data_as(f64p)),
-                    "predict")
+        f = self.L.espl_mlp_predict if fused else self.L.espl_mlp_predict_layers
+        self._check(f(self.h, x.ctypes.data_as(f64p), len(x), y.ctypes.data_as(f64p)), "predict")
         return y
 
     def __enter__(self):

@@ -66,8 +66,13 @@ espl_status espl_mlp_loss_grad(espl_mlp *m, const double *x, const double *y, ui
 espl_status espl_mlp_train(espl_mlp *m, const double *x, const double *y, uint32_t n, const espl_train_opts *opts,
                            double *epoch_loss);
 
-/* Predictions for n rows (any n; processed in capacity-sized chunks). */
+/* Predictions for n rows (any n): one fused inference launch, each CTA
+ * running the whole network on 128 rows from shared memory and tensor
+ * memory. */
 espl_status espl_mlp_predict(espl_mlp *m, const double *x, uint32_t n, double *y);
+/* The same predictions layer by layer through the training GEMMs, in
+ * capacity-sized chunks (a cross-check of the fused kernel). */
+espl_status espl_mlp_predict_layers(espl_mlp *m, const double *x, uint32_t n, double *y);
 
 espl_status espl_mlp_error_message(espl_mlp *m, char *buf, size_t cap);
 

@@ -47,10 +47,13 @@ def test_predictions_match_the_oracle():
     with Mlp(16, 11, capacity=256, seed=12) as m:
         m.set_scaling(x, y)
         p = m.get_params()
-        yp = m.predict(x)  # two chunks of the capacity
+        yp = m.predict(x)  # the fused kernel: three 128-row tiles, the last one partial
+        yl = m.predict(x, fused=False)  # layer by layer: two chunks of the capacity
     ref = om.predict(p, x, om.scaling(x), om.scaling(y), 11)
     scale = np.abs(ref).max()
     assert np.abs(yp - ref).max() <= 2e-2 * scale
+    assert np.abs(yl - ref).max() <= 2e-2 * scale
+    assert np.abs(yp - yl).max() <= 1e-5 * scale
 
 
 def test_training_reduces_the_loss():
