@@ -43,6 +43,7 @@ struct TileShared {
     uint32_t bits[32];
     uint32_t restore[32];
     uint32_t accf[32];
+    uint32_t cbuf[32];  // the cells buffer of a converged lane's published iterate
     unsigned long long acc0[32], acc1[32], acc2[32];
     double limit[32];
     double ag0[32], ag1[32], t[32], xfact[32], dt_next[32];
@@ -55,10 +56,13 @@ constexpr uint32_t kLimited = 1, kImplausible = 2, kResidualMiss = 4;
 // One Newton solve per lane of the tile (converger.newtonLanes at W = 1 as
 // the lane kernels split it: assemble, gmin, refactor, solve, update,
 // limit, gates, finalize). `on` lanes take part; with `tran_companion` a
-// lane's companion scalars and time come from the shared arrays.
+// lane's companion scalars and time come from the shared arrays. The
+// instance phase of iteration k + 1 runs inside iteration k's limiter pass
+// (same loads, into the other cells buffer); `eval0` runs iteration 0's
+// instance phase first (else the caller left it in cells buffer 0).
 template <bool MIXED>
 __device__ void newton_tile(const TileCtx& c, LaneState* s, const NewtonParams& o, int tran, bool tran_companion,
-                            bool on, TileShared& sh, unsigned char* dsm) {
+                            bool on, TileShared& sh, unsigned char* dsm, bool eval0) {
     const GroupDev& d = *c.d;
     const uint32_t l = c.l, P = d.P, lane = c.lane, warp = c.warp;
     const uint32_t ninst = n_instances(d);
@@ -81,7 +85,10 @@ __device__ void newton_tile(const TileCtx& c, LaneState* s, const NewtonParams& 
             s->fp64 = (MIXED && o.init_fix) ? 1u : 0u;
         }
     }
+    if (eval0 && c.valid && on)
+        for (uint32_t t = warp; t < ninst; t += kWarps) inst_eval(d, l, t, tran, 0.0, cell_buf(d, 0));
     __syncthreads();
+    uint32_t cur = 0;
     for (uint32_t it = 0; it < o.max_iter; it++) {
         bool act = c.valid && sh.active[lane];
         if (!__syncthreads_or(act)) break;
@@ -94,17 +101,16 @@ __device__ void newton_tile(const TileCtx& c, LaneState* s, const NewtonParams& 
             cp.ag1 = sh.ag1[lane];
             tm = sh.t[lane];
         }
-        if (act)
-            for (uint32_t t = warp; t < ninst; t += kWarps) inst_eval(d, l, t, tran, tm);
-        __syncthreads();
+        const double* cells = cell_buf(d, cur);
         if (act) {
             if (sm) {
                 T* sa = static_cast<T*>(st.a);
-                for (uint32_t p = warp; p < d.nnz; p += kWarps) sa[p * 32 + lane] = (T)gather_slot(d, l, p, cp, o.gmin);
+                for (uint32_t p = warp; p < d.nnz; p += kWarps)
+                    sa[p * 32 + lane] = (T)gather_slot(d, l, p, cp, o.gmin, cells);
             } else {
-                for (uint32_t p = warp; p < d.nnz; p += kWarps) gather_slot(d, l, p, cp, o.gmin);
+                for (uint32_t p = warp; p < d.nnz; p += kWarps) gather_slot(d, l, p, cp, o.gmin, cells);
             }
-            for (uint32_t i = warp; i < d.n; i += kWarps) gather_row(d, l, i, cp, o.gmin);
+            for (uint32_t i = warp; i < d.n; i += kWarps) gather_row(d, l, i, cp, o.gmin, cells);
         }
         __syncthreads();
         if (it == 0) {
@@ -209,11 +215,14 @@ __device__ void newton_tile(const TileCtx& c, LaneState* s, const NewtonParams& 
             }
         if (act) atomicMax(&sh.acc0[lane], worst);
         __syncthreads();
-        // The limiter pass over instances; plausible and residual gates over rows.
+        // The limiter pass over instances (each then evaluated at its new
+        // limited point for the next iteration); plausible and residual gates
+        // over rows.
         uint32_t flags = 0;
         if (act) {
+            double* next = cell_buf(d, cur ^ 1u);
             for (uint32_t t = warp; t < ninst; t += kWarps)
-                if (inst_limit(d, l, t)) flags |= kLimited;
+                if (inst_limit_eval(d, l, t, tran, tm, next)) flags |= kLimited;
             double lim = sh.limit[lane];
             for (uint32_t i = warp; i < d.n; i += kWarps) {
                 double xi = LM(d.x, i);
@@ -239,6 +248,7 @@ __device__ void newton_tile(const TileCtx& c, LaneState* s, const NewtonParams& 
                     sh.bits[lane] |= kConverged;
                     sh.active[lane] = 0;
                     sh.restore[lane] = 1;
+                    sh.cbuf[lane] = cur;
                     s->iterations = it + 1;
                 }
                 if (MIXED && sh.active[lane] && !s->fp64 && it + 1 >= o.stall_ticks) {
@@ -250,6 +260,7 @@ __device__ void newton_tile(const TileCtx& c, LaneState* s, const NewtonParams& 
         __syncthreads();
         if (c.valid && sh.restore[lane])
             for (uint32_t i = warp; i < d.n; i += kWarps) LM(d.x, i) = LM(d.x_old, i);
+        cur ^= 1u;
     }
     __syncthreads();
     if (warp == 0 && s) s->bits = sh.bits[lane];
@@ -263,7 +274,7 @@ __global__ void __launch_bounds__(kTileThreads, 4) k_static(TileMap m, NewtonPar
     TileCtx c = tile_ctx(m);
     c.d = stage_template(*c.d, sh.gd, g_dsm, MIXED);
     LaneState* s = (c.warp == 0 && c.valid) ? &st[c.d->lane0 + c.l] : nullptr;
-    newton_tile<MIXED>(c, s, o, tran, false, true, sh, g_dsm);
+    newton_tile<MIXED>(c, s, o, tran, false, true, sh, g_dsm, true);
 }
 
 // Bias-independent prep per (instance, lane) from the raw lane-major rows,
@@ -292,8 +303,10 @@ __global__ void __launch_bounds__(kTileThreads) k_prep(TileMap m, const double* 
         for (int k = 0; k < DiodePrep::count; k++) LM(dd, DiodePrep::count * i + k) = o[k];
     }
     if (c.warp == 0) {
-        LM(d.cells, d.c_const) = 1.0;
-        LM(d.cells, d.c_const + 1) = -1.0;
+        for (uint32_t b = 0; b < 2; b++) {
+            LM(cell_buf(d, b), d.c_const) = 1.0;
+            LM(cell_buf(d, b), d.c_const + 1) = -1.0;
+        }
     }
 }
 
@@ -319,11 +332,11 @@ __global__ void __launch_bounds__(kTileThreads) k_assemble(TileMap m, int tran, 
     TileCtx c = tile_ctx(m);
     const GroupDev& d = *c.d;
     if (c.valid)
-        for (uint32_t t = c.warp; t < n_instances(d); t += kWarps) inst_eval(d, c.l, t, tran, 0.0);
+        for (uint32_t t = c.warp; t < n_instances(d); t += kWarps) inst_eval(d, c.l, t, tran, 0.0, cell_buf(d, 0));
     __syncthreads();
     Companion cp{inv_dt > 0.0 ? 1 : 0, 0, inv_dt, 1.0};
     if (c.valid)
-        for (uint32_t p = c.warp; p < d.nnz; p += kWarps) gather_slot(d, c.l, p, cp, 0.0);
+        for (uint32_t p = c.warp; p < d.nnz; p += kWarps) gather_slot(d, c.l, p, cp, 0.0, cell_buf(d, 0));
 }
 
 // ---------------------------------------------------------------------------
@@ -421,19 +434,19 @@ __global__ void __launch_bounds__(kTileThreads) k_tran_init(TileMap m, TranParam
     if (c.valid)
         for (uint32_t t = c.warp; t < ninst; t += kWarps) {
             inst_seed(d, l, t, 0, d.x);
-            inst_eval(d, l, t, 1, 0.0);
+            inst_eval(d, l, t, 1, 0.0, cell_buf(d, 0));
         }
     __syncthreads();
     if (!c.valid) return;
     for (uint32_t i = c.warp; i < d.n; i += kWarps) {
-        gather_charge_row(d, l, i);
+        gather_charge_row(d, l, i, cell_buf(d, 0));
         LM(d.cur, i) = LM(d.x, i);
         LM(d.prev, i) = LM(d.x, i);
         LM(d.q1, i) = LM(d.qrow, i);
         LM(d.ip, i) = 0.0;
     }
     for (uint32_t j = c.warp; j < d.n_sites; j += kWarps) {
-        double q = LM(d.cells, d.site_cell[j]);
+        double q = LM(cell_buf(d, 0), d.site_cell[j]);
         for (uint32_t k = 0; k < 4; k++) LM(d.sring + (size_t)k * d.n_sites * P, j) = q;
         LM(d.sip, j) = 0.0;
     }
@@ -520,14 +533,15 @@ __global__ void __launch_bounds__(kTileThreads, 4) k_tran(TileMap m, TranParams 
         }
         __syncthreads();
         // The limiter state restarts from the accepted point, then limits the
-        // predicted iterate.
+        // predicted iterate and evaluates the instances there (the instance
+        // phase of Newton's iteration 0, into cells buffer 0).
         if (on)
             for (uint32_t t = warp; t < ninst; t += kWarps) {
                 inst_seed(d, l, t, 0, d.cur);
-                inst_limit(d, l, t);
+                inst_limit_eval(d, l, t, 1, sh.t[lane], cell_buf(d, 0));
             }
         __syncthreads();
-        newton_tile<MIXED>(c, s, np, 1, true, on, sh, dsm);
+        newton_tile<MIXED>(c, s, np, 1, true, on, sh, dsm, false);
         // The last eval ran at the published x: its site charges are the
         // point's, logical slot 0 of the ring.
         bool conv = on && (sh.bits[lane] & kConverged);
@@ -538,7 +552,8 @@ __global__ void __launch_bounds__(kTileThreads, 4) k_tran(TileMap m, TranParams 
         }
         if (conv) {
             double* r0 = ring_slot(d, sh.rot[lane], 0);
-            for (uint32_t j = warp; j < ns; j += kWarps) LM(r0, j) = LM(d.cells, d.site_cell[j]);
+            const double* cb = cell_buf(d, sh.cbuf[lane]);
+            for (uint32_t j = warp; j < ns; j += kWarps) LM(r0, j) = LM(cb, d.site_cell[j]);
         }
         __syncthreads();
         // The LTE bound of a converged LTE-controlled step, its sites split

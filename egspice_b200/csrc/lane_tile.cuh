@@ -42,10 +42,75 @@ struct TileCtx {
 // Instance phase: one instance of one kind at the lane's x, its limiter
 // state giving the linearization point (eval.zig:826-874).
 
-__device__ __forceinline__ void inst_eval(const GroupDev& d, uint32_t l, uint32_t t, int tran, double tm) {
+// Diode i's cells at its terminal voltage vd, linearized at the limited vl.
+__device__ __forceinline__ void diode_cells(const GroupDev& d, uint32_t l, uint32_t i, double vd, double vl,
+                                            double* __restrict__ cells) {
+    const uint32_t P = d.P;
+    const double* dd = d.dio_d;
+    uint32_t b = DiodePrep::count * i;
+    double id, gd, qd, cd;
+    diode_core(LM(dd, b + DiodePrep::is), LM(dd, b + DiodePrep::vte), LM(dd, b + DiodePrep::gmin),
+               LM(dd, b + DiodePrep::cjo), LM(dd, b + DiodePrep::cjo_t), LM(dd, b + DiodePrep::vj_t),
+               LM(dd, b + DiodePrep::mt), LM(dd, b + DiodePrep::fc), LM(dd, b + DiodePrep::tt), vl, id, gd, qd, cd);
+    uint32_t c = d.c_dio + kDioCells * i;
+    LM(cells, c) = gd;
+    LM(cells, c + 1) = id + gd * (vd - vl);
+    bool charge = LM(dd, b + DiodePrep::cjo) > 0.0 || LM(dd, b + DiodePrep::tt) > 0.0;
+    LM(cells, c + 2) = charge ? cd : 0.0;
+    LM(cells, c + 3) = charge ? qd + cd * (vd - vl) : 0.0;
+}
+
+// MOS i's cells at its terminal voltages (normalized frame vgs, vds, vbs),
+// linearized at the limited (lgs, lds, lbs).
+struct MosPrep {
+    double ty, vt, beta, lambda, gamma, phit, von0, isat, gmin, vcrit;
+};
+
+__device__ __forceinline__ MosPrep mos_prep(const GroupDev& d, uint32_t l, uint32_t i) {
+    const uint32_t P = d.P;
+    const double* md = d.mos_d;
+    uint32_t b = Mos1Prep::count * i;
+    return MosPrep{LM(md, b + Mos1Prep::type),  LM(md, b + Mos1Prep::vt),    LM(md, b + Mos1Prep::beta),
+                   LM(md, b + Mos1Prep::lambda), LM(md, b + Mos1Prep::gamma), LM(md, b + Mos1Prep::phit),
+                   LM(md, b + Mos1Prep::von0),   LM(md, b + Mos1Prep::isat),  LM(md, b + Mos1Prep::gmin),
+                   LM(md, b + Mos1Prep::vcrit)};
+}
+
+__device__ __forceinline__ void mos_cells(const GroupDev& d, uint32_t l, uint32_t i, const MosPrep& m, double vgs,
+                                          double vds, double vbs, double lgs, double lds, double lbs,
+                                          double* __restrict__ cells) {
+    const uint32_t P = d.P;
+    const double ty = m.ty;
+    Mos1Out o;
+    mos1_core(ty, m.vt, m.beta, m.lambda, m.gamma, m.phit, m.von0, m.isat, m.gmin, lgs, lds, lbs, o);
+    double dgs = vgs - lgs, dds = vds - lds, dbs = vbs - lbs;
+    double gm = o.mode * o.gm, gds = o.mode * o.gds, gmbs = o.mode * o.gmbs;
+    double ich = o.mode * o.id + gm * dgs + gds * dds + gmbs * dbs;
+    double ibd = o.ibd + o.gbd * (dbs - dds);
+    double ibs = o.ibs + o.gbs * dbs;
+    double gsum = gm + gds + gmbs;
+    uint32_t c = d.c_mos + kMosCells * i;
+    LM(cells, c + 0) = ty * ich - ty * ibd;
+    LM(cells, c + 1) = -ty * ich - ty * ibs;
+    LM(cells, c + 2) = ty * ibd + ty * ibs;
+    LM(cells, c + 3) = gds + o.gbd;
+    LM(cells, c + 4) = gm;
+    LM(cells, c + 5) = -gsum;
+    LM(cells, c + 6) = gmbs - o.gbd;
+    LM(cells, c + 7) = -gds;
+    LM(cells, c + 8) = -gm;
+    LM(cells, c + 9) = gsum + o.gbs;
+    LM(cells, c + 10) = -gmbs - o.gbs;
+    LM(cells, c + 11) = -o.gbd;
+    LM(cells, c + 12) = 0.0;
+    LM(cells, c + 13) = -o.gbs;
+    LM(cells, c + 14) = o.gbd + o.gbs;
+}
+
+__device__ __forceinline__ void inst_eval(const GroupDev& d, uint32_t l, uint32_t t, int tran, double tm,
+                                          double* __restrict__ cells) {
     const uint32_t P = d.P;
     const double* __restrict__ x = d.x;
-    double* __restrict__ cells = d.cells;
     uint32_t i = t;
     if (i < d.n_res) {
         uint32_t tp = d.res_t[2 * i], tn = d.res_t[2 * i + 1];
@@ -90,57 +155,17 @@ __device__ __forceinline__ void inst_eval(const GroupDev& d, uint32_t l, uint32_
     i -= d.n_isrc;
     if (i < d.n_dio) {
         uint32_t ta = d.dio_t[2 * i], tc = d.dio_t[2 * i + 1];
-        const double* dd = d.dio_d;
-        uint32_t b = DiodePrep::count * i;
-        double vd = LM(x, ta) - LM(x, tc);
-        double vl = LM(d.lim_dio, i);
-        double id, gd, qd, cd;
-        diode_core(LM(dd, b + DiodePrep::is), LM(dd, b + DiodePrep::vte), LM(dd, b + DiodePrep::gmin),
-                   LM(dd, b + DiodePrep::cjo), LM(dd, b + DiodePrep::cjo_t), LM(dd, b + DiodePrep::vj_t),
-                   LM(dd, b + DiodePrep::mt), LM(dd, b + DiodePrep::fc), LM(dd, b + DiodePrep::tt), vl, id, gd, qd, cd);
-        uint32_t c = d.c_dio + kDioCells * i;
-        LM(cells, c) = gd;
-        LM(cells, c + 1) = id + gd * (vd - vl);
-        bool charge = LM(dd, b + DiodePrep::cjo) > 0.0 || LM(dd, b + DiodePrep::tt) > 0.0;
-        LM(cells, c + 2) = charge ? cd : 0.0;
-        LM(cells, c + 3) = charge ? qd + cd * (vd - vl) : 0.0;
+        diode_cells(d, l, i, LM(x, ta) - LM(x, tc), LM(d.lim_dio, i), cells);
         return;
     }
     i -= d.n_dio;
     if (i < d.n_mos) {
         const uint32_t* tmv = d.mos_t + 4 * i;
-        const double* md = d.mos_d;
-        uint32_t b = Mos1Prep::count * i;
-        double ty = LM(md, b + Mos1Prep::type);
+        const MosPrep m = mos_prep(d, l, i);
         double xd = LM(x, tmv[0]), xg = LM(x, tmv[1]), xs = LM(x, tmv[2]), xb = LM(x, tmv[3]);
-        double vgs = ty * (xg - xs), vds = ty * (xd - xs), vbs = ty * (xb - xs);
-        double lgs = LM(d.lim_mos, 3 * i), lds = LM(d.lim_mos, 3 * i + 1), lbs = LM(d.lim_mos, 3 * i + 2);
-        Mos1Out o;
-        mos1_core(ty, LM(md, b + Mos1Prep::vt), LM(md, b + Mos1Prep::beta), LM(md, b + Mos1Prep::lambda),
-                  LM(md, b + Mos1Prep::gamma), LM(md, b + Mos1Prep::phit), LM(md, b + Mos1Prep::von0),
-                  LM(md, b + Mos1Prep::isat), LM(md, b + Mos1Prep::gmin), lgs, lds, lbs, o);
-        double dgs = vgs - lgs, dds = vds - lds, dbs = vbs - lbs;
-        double gm = o.mode * o.gm, gds = o.mode * o.gds, gmbs = o.mode * o.gmbs;
-        double ich = o.mode * o.id + gm * dgs + gds * dds + gmbs * dbs;
-        double ibd = o.ibd + o.gbd * (dbs - dds);
-        double ibs = o.ibs + o.gbs * dbs;
-        double gsum = gm + gds + gmbs;
-        uint32_t c = d.c_mos + kMosCells * i;
-        LM(cells, c + 0) = ty * ich - ty * ibd;
-        LM(cells, c + 1) = -ty * ich - ty * ibs;
-        LM(cells, c + 2) = ty * ibd + ty * ibs;
-        LM(cells, c + 3) = gds + o.gbd;
-        LM(cells, c + 4) = gm;
-        LM(cells, c + 5) = -gsum;
-        LM(cells, c + 6) = gmbs - o.gbd;
-        LM(cells, c + 7) = -gds;
-        LM(cells, c + 8) = -gm;
-        LM(cells, c + 9) = gsum + o.gbs;
-        LM(cells, c + 10) = -gmbs - o.gbs;
-        LM(cells, c + 11) = -o.gbd;
-        LM(cells, c + 12) = 0.0;
-        LM(cells, c + 13) = -o.gbs;
-        LM(cells, c + 14) = o.gbd + o.gbs;
+        double vgs = m.ty * (xg - xs), vds = m.ty * (xd - xs), vbs = m.ty * (xb - xs);
+        mos_cells(d, l, i, m, vgs, vds, vbs, LM(d.lim_mos, 3 * i), LM(d.lim_mos, 3 * i + 1), LM(d.lim_mos, 3 * i + 2),
+                  cells);
         return;
     }
     i -= d.n_mos;
@@ -178,6 +203,54 @@ __device__ __forceinline__ void inst_seed(const GroupDev& d, uint32_t l, uint32_
         LM(d.lim_mos, 3 * i + 1) = ty * (LM(xs, tmv[0]) - xsrc);
         LM(d.lim_mos, 3 * i + 2) = ty * (LM(xs, tmv[3]) - xsrc);
     }
+}
+
+// The limiter pass of instance t with snapLimited (eval.zig:1115-1171),
+// then the instance evaluated at its new limited point into `cells` (what
+// the next Newton iteration's instance phase would compute), on one load of
+// the instance's state: true when the limiter clamped.
+__device__ __forceinline__ bool inst_limit_eval(const GroupDev& d, uint32_t l, uint32_t t, int tran, double tm,
+                                                double* __restrict__ cells) {
+    const uint32_t P = d.P;
+    const double* x = d.x;
+    const double eps16 = 16 * 2.220446049250313e-16;
+    uint32_t base = d.n_res + d.n_cap + d.n_vsrc + d.n_isrc;
+    if (t < base) {
+        inst_eval(d, l, t, tran, tm, cells);
+        return false;
+    }
+    uint32_t i = t - base;
+    if (i < d.n_dio) {
+        double xa = LM(x, d.dio_t[2 * i]), xc = LM(x, d.dio_t[2 * i + 1]);
+        double vd = xa - xc;
+        uint32_t b = DiodePrep::count * i;
+        double v = pnjlim(vd, LM(d.lim_dio, i), LM(d.dio_d, b + DiodePrep::vte), LM(d.dio_d, b + DiodePrep::vcrit));
+        if (fabs(v - vd) <= eps16 * fmax(fabs(xa), fabs(xc))) v = vd;
+        LM(d.lim_dio, i) = v;
+        diode_cells(d, l, i, vd, v, cells);
+        return v != vd;
+    }
+    i -= d.n_dio;
+    if (i >= d.n_mos) {
+        inst_eval(d, l, t, tran, tm, cells);
+        return false;
+    }
+    const uint32_t* tmv = d.mos_t + 4 * i;
+    const MosPrep m = mos_prep(d, l, i);
+    double xd = LM(x, tmv[0]), xg = LM(x, tmv[1]), xs = LM(x, tmv[2]), xb = LM(x, tmv[3]);
+    double cgs = m.ty * (xg - xs), cds = m.ty * (xd - xs), cbs = m.ty * (xb - xs);
+    double vgs = cgs, vds = cds, vbs = cbs;
+    mos1_limit(m.vt, m.gamma, m.phit, m.von0, m.vcrit, LM(d.lim_mos, 3 * i), LM(d.lim_mos, 3 * i + 1),
+               LM(d.lim_mos, 3 * i + 2), vgs, vds, vbs);
+    double tol = eps16 * fmax(fmax(fabs(xd), fabs(xg)), fmax(fabs(xs), fabs(xb)));
+    if (fabs(vgs - cgs) <= tol) vgs = cgs;
+    if (fabs(vds - cds) <= tol) vds = cds;
+    if (fabs(vbs - cbs) <= tol) vbs = cbs;
+    LM(d.lim_mos, 3 * i) = vgs;
+    LM(d.lim_mos, 3 * i + 1) = vds;
+    LM(d.lim_mos, 3 * i + 2) = vbs;
+    mos_cells(d, l, i, m, cgs, cds, cbs, vgs, vds, vbs, cells);
+    return (vgs != cgs) | (vds != cds) | (vbs != cbs);
 }
 
 // The limiter pass of instance t with snapLimited (eval.zig:1115-1171):
@@ -235,12 +308,12 @@ __device__ __forceinline__ double gather_sum(const double* __restrict__ cells, u
 // Gather phase: A (G + ag0 C, with gmin on the diagonals), the residual
 // with the companion rows and gmin load, and the row charges.
 __device__ __forceinline__ double slot_value(const GroupDev& d, uint32_t l, uint32_t p, const Companion& cp,
-                                             double gmin) {
+                                             double gmin, const double* __restrict__ cells) {
     const uint32_t P = d.P;
-    double g = gather_sum(d.cells, P, l, d.g_ptr, d.g_cell, p);
+    double g = gather_sum(cells, P, l, d.g_ptr, d.g_cell, p);
     double a = g;
     if (cp.on) {
-        double c = gather_sum(d.cells, P, l, d.c_ptr, d.c_cell, p);
+        double c = gather_sum(cells, P, l, d.c_ptr, d.c_cell, p);
         a = g + cp.ag0 * c;
     }
     if (gmin > 0.0 && d.slot_diag[p]) a += gmin;
@@ -248,19 +321,19 @@ __device__ __forceinline__ double slot_value(const GroupDev& d, uint32_t l, uint
 }
 
 __device__ __forceinline__ double gather_slot(const GroupDev& d, uint32_t l, uint32_t p, const Companion& cp,
-                                              double gmin) {
+                                              double gmin, const double* __restrict__ cells) {
     const uint32_t P = d.P;
-    double a = slot_value(d, l, p, cp, gmin);
+    double a = slot_value(d, l, p, cp, gmin, cells);
     LM(d.a, p) = a;
     return a;
 }
 
 __device__ __forceinline__ double gather_row(const GroupDev& d, uint32_t l, uint32_t i, const Companion& cp,
-                                             double gmin) {
+                                             double gmin, const double* __restrict__ cells) {
     const uint32_t P = d.P;
-    double r = gather_sum(d.cells, P, l, d.r_ptr, d.r_cell, i);
+    double r = gather_sum(cells, P, l, d.r_ptr, d.r_cell, i);
     if (cp.on) {
-        double q = gather_sum(d.cells, P, l, d.q_ptr, d.q_cell, i);
+        double q = gather_sum(cells, P, l, d.q_ptr, d.q_cell, i);
         LM(d.qrow, i) = q;
         double dq = cp.ag0 * (q - LM(d.q1, i));
         double base = r + dq;
@@ -273,9 +346,17 @@ __device__ __forceinline__ double gather_row(const GroupDev& d, uint32_t l, uint
 
 // Row charges without a Newton (the transient start and the tape's charge
 // planes are read from them).
-__device__ __forceinline__ void gather_charge_row(const GroupDev& d, uint32_t l, uint32_t i) {
+__device__ __forceinline__ void gather_charge_row(const GroupDev& d, uint32_t l, uint32_t i,
+                                                  const double* __restrict__ cells) {
     const uint32_t P = d.P;
-    LM(d.qrow, i) = gather_sum(d.cells, P, l, d.q_ptr, d.q_cell, i);
+    LM(d.qrow, i) = gather_sum(cells, P, l, d.q_ptr, d.q_cell, i);
+}
+
+// Cells buffer b (0 or 1) of a template: the instance phase of one Newton
+// iteration writes one while the gather of the same iteration reads it, and
+// the limiter pass evaluates the next iteration into the other.
+__device__ __forceinline__ double* cell_buf(const GroupDev& d, uint32_t b) {
+    return d.cells + (b ? (size_t)d.n_cells * d.P : 0);
 }
 
 }  // namespace espl
