@@ -61,8 +61,9 @@ constexpr uint32_t kLimited = 1, kImplausible = 2, kResidualMiss = 4;
 // (same loads, into the other cells buffer); `eval0` runs iteration 0's
 // instance phase first (else the caller left it in cells buffer 0).
 template <bool MIXED>
-__device__ void newton_tile(const TileCtx& c, LaneState* s, const NewtonParams& o, int tran, bool tran_companion,
-                            bool on, TileShared& sh, unsigned char* dsm, bool eval0) {
+__device__ __forceinline__ void newton_tile(const TileCtx& c, LaneState* s, const NewtonParams& o, int tran,
+                                            bool tran_companion, bool on, TileShared& sh, unsigned char* dsm,
+                                            bool eval0) {
     const GroupDev& d = *c.d;
     const uint32_t l = c.l, P = d.P, lane = c.lane, warp = c.warp;
     const uint32_t ninst = n_instances(d);
@@ -266,7 +267,6 @@ __device__ void newton_tile(const TileCtx& c, LaneState* s, const NewtonParams& 
     if (warp == 0 && s) s->bits = sh.bits[lane];
 }
 
-extern __shared__ __align__(16) unsigned char g_dsm[];
 
 template <bool MIXED>
 __global__ void __launch_bounds__(kTileThreads, 4) k_static(TileMap m, NewtonParams o, LaneState* st, int tran) {

@@ -25,6 +25,11 @@
 
 namespace espl {
 
+// The tile's dynamic shared memory. The LU chain derives its pointers from
+// this symbol (not from pointers handed around), so the compiler addresses
+// them as shared memory.
+extern __shared__ __align__(16) unsigned char g_dsm[];
+
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
     return (uint32_t)__cvta_generic_to_shared(p);
 }
@@ -230,10 +235,12 @@ __host__ __device__ inline SmemPlan smem_plan(const GroupDev& d, uint32_t mode, 
 
 struct SmemTile {
     void *a, *w, *lx, *ux, *ud;
+    SmemPlan plan;
 };
 
 __device__ __forceinline__ SmemTile smem_tile(unsigned char* base, const SmemPlan& p) {
     SmemTile t;
+    t.plan = p;
     t.a = base + p.a_off;
     t.w = base + p.w_off;
     t.lx = base + p.lx_off;
@@ -311,17 +318,24 @@ __device__ __forceinline__ TapeView tape_view(const GroupDev& d) {
     return TapeView{d.q, d.col_ptr, d.prow, d.up, d.ui, d.lp, d.li, d.flags, d.pinv, d.n};
 }
 
+// The staged tape of a kStageLu tile, addressed from the shared-memory symbol.
+__device__ __forceinline__ TapeView tape_view_smem(const GroupDev& d, const SmemPlan& p) {
+    const uint32_t* u = reinterpret_cast<const uint32_t*>(g_dsm);
+    return TapeView{u + p.off[S_Q],  u + p.off[S_COLPTR], u + p.off[S_PROW],  u + p.off[S_UP],  u + p.off[S_UI],
+                    u + p.off[S_LP], u + p.off[S_LI],     u + p.off[S_FLAGS], u + p.off[S_PINV], d.n};
+}
+
 // The replay in shared memory; T = double or float. 0 holds, 1 pivot or
 // store failure, 2 only a multiplier past 1 / pivot_tol.
 template <typename T>
-__device__ int refactor_smem(const GroupDev& d, const SmemTile& s, uint32_t lane, uint32_t l) {
+__device__ __forceinline__ int refactor_smem(const GroupDev& d, const SmemTile& s, uint32_t lane, uint32_t l) {
     T* __restrict__ w = static_cast<T*>(s.w);
     T* __restrict__ lx = static_cast<T*>(s.lx);
     T* __restrict__ ux = static_cast<T*>(s.ux);
     T* __restrict__ ud = static_cast<T*>(s.ud);
     const T* __restrict__ a = static_cast<const T*>(s.a);
     const uint32_t P = d.P;
-    const TapeView t = tape_view(d);
+    const TapeView t = tape_view_smem(d, s.plan);
     for (uint32_t v = 0; v < d.n_void; v++)
         if (LM(d.a, d.void_slots[v]) != 0.0) return 1;
     constexpr bool f64 = sizeof(T) == 8;
@@ -413,13 +427,13 @@ __device__ int refactor_smem(const GroupDev& d, const SmemTile& s, uint32_t lane
 // two at a time. The FP64 wide-multiplier scan is folded into the
 // divisions.
 template <typename T>
-__device__ int refactor_prog(const GroupDev& d, const SmemTile& s, uint32_t lane, uint32_t l) {
+__device__ __forceinline__ int refactor_prog(const GroupDev& d, const SmemTile& s, uint32_t lane, uint32_t l) {
     T* __restrict__ w = static_cast<T*>(s.w);
     T* __restrict__ lx = static_cast<T*>(s.lx);
     T* __restrict__ ux = static_cast<T*>(s.ux);
     T* __restrict__ ud = static_cast<T*>(s.ud);
     const T* __restrict__ a = static_cast<const T*>(s.a);
-    const uint32_t* __restrict__ prog = d.lu_prog;
+    const uint32_t* __restrict__ prog = reinterpret_cast<const uint32_t*>(g_dsm) + s.plan.off[S_PROG];
     const uint32_t P = d.P;
     for (uint32_t v = 0; v < d.n_void; v++)
         if (LM(d.a, d.void_slots[v]) != 0.0) return 1;
@@ -516,7 +530,7 @@ __device__ int refactor_prog(const GroupDev& d, const SmemTile& s, uint32_t lane
             pc += 2 + cnt;
         } else if (op == kOpVoid) {
             const uint32_t k = prog[pc + 1];
-            const TapeView t = tape_view(d);
+            const TapeView t = tape_view_smem(d, s.plan);
             SL(ud, k) = (T)1;
             for (uint32_t p = t.lp[k]; p < t.lp[k + 1]; p++) { SL(lx, p) = (T)0; SL(w, t.li[p]) = (T)0; }
             SL(w, k) = (T)0;
@@ -578,9 +592,9 @@ __device__ __forceinline__ void subst_smem(const TapeView& t, const SmemTile& s,
 // dx = -A^-1 rhs through the shared factors (luSolve with neg); rhs and dx
 // are the lane's global rows. y is the work vector w, zero again on return.
 template <typename T>
-__device__ void solve_smem(const GroupDev& d, const SmemTile& s, uint32_t lane, uint32_t l) {
+__device__ __forceinline__ void solve_smem(const GroupDev& d, const SmemTile& s, uint32_t lane, uint32_t l) {
     const uint32_t P = d.P;
-    const TapeView t = tape_view(d);
+    const TapeView t = tape_view_smem(d, s.plan);
     const double* __restrict__ rhs = d.rhs;
     double* __restrict__ dx = d.dx;
     T* __restrict__ y = static_cast<T*>(s.w);
@@ -605,10 +619,12 @@ __device__ void solve_smem(const GroupDev& d, const SmemTile& s, uint32_t lane, 
 // r = rhs + A dx row by row, the products added by ascending column as the
 // column sweep adds them (columns with dx = 0 skipped), then
 // dx += -A^-1 r through the FP32 factors.
-__device__ void refine_smem(const GroupDev& d, const SmemTile& s, uint32_t lane, uint32_t l) {
+__device__ __forceinline__ void refine_smem(const GroupDev& d, const SmemTile& s, uint32_t lane, uint32_t l) {
     const uint32_t P = d.P;
-    const TapeView t = tape_view(d);
-    const uint32_t *__restrict__ rt_ptr = d.rt_ptr, *__restrict__ rt_col = d.rt_col, *__restrict__ rt_pos = d.rt_pos;
+    const TapeView t = tape_view_smem(d, s.plan);
+    const uint32_t* u = reinterpret_cast<const uint32_t*>(g_dsm);
+    const uint32_t *__restrict__ rt_ptr = u + s.plan.off[S_RTPTR], *__restrict__ rt_col = u + s.plan.off[S_RTCOL],
+                   *__restrict__ rt_pos = u + s.plan.off[S_RTPOS];
     const double* __restrict__ rhs = d.rhs;
     const double* __restrict__ a = d.a;
     double* __restrict__ dx = d.dx;
