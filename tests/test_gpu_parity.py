@@ -151,3 +151,49 @@ def test_golden_fixtures_on_the_gpu(precision):
             assert worst(x, xr) <= 1.0, name
             if per is not None:
                 assert float(np.abs(per - np.array(gt["period"])).max()) <= 1e-6 * float(np.abs(gt["period"]).max())
+
+
+@pytest.mark.parametrize("precision,refine", [("fp64", 0), ("mixed", 0), ("mixed", 1)])
+def test_power_grid_transient(oracle, precision, refine):
+    """Config-3 shape at a test size: a 16 x 16 resistive mesh with decaps,
+    corner pads and current-pulse loads, trapezoidal fixed steps; in mixed
+    mode with and without the FP64-residual refinement sweep."""
+    net = decks.power_grid(6, side=16, loads=24)
+    topts = abi.tran_opts(t_stop=1e-9, dt=10e-12, fixed_step=1, method=1, max_iter=20)
+    with Lanes([net], precision=precision, dt0=topts.dt, refine_sweeps=refine) as L:
+        reps = L.run_tran(topts, steps_per_launch=4096)
+        x = L.get_x(0)
+    assert all(r.status == 1 and r.steps == 100 for r in reps)
+    xo, _, _, _ = oracle.tran_lanes(net, topts, threads=6)
+    assert worst(x, xo) <= 1.0
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_inverter_pair_width_step(oracle, precision):
+    """The reference's GPU-vs-CPU lane deck shape (src/tests/espice.zig:
+    3353-3389): two inverters with a .step over the NMOS width, cold
+    operating points, every lane within the 1e-6 bar of the CPU run."""
+    net = decks.inverter_pair(64)
+    opts = abi.newton_opts()
+    xo, ro = oracle.op_lanes(net, opts, threads=8)
+    with Lanes([net], precision=precision) as L:
+        r = L.solve_static(opts)
+        x = L.get_x(0)
+    assert ((r[:, 0] & abi.CONVERGED) != 0).all() and (ro[:, 0] == 1).all()
+    assert worst(x, xo) <= 1.0
+
+
+def test_backward_euler_lte_steps(oracle):
+    """Backward Euler under LTE control: the same accepted and rejected
+    steps as the oracle."""
+    r = np.array([1e3, 5e3, 2e4])
+    c = np.array([1e-12, 2e-13, 5e-14])
+    net = decks.rc_points(3, r, c, tr=0.1e-9)
+    opts = abi.tran_opts(t_stop=5e-9, dt=1e-12, dt_max=20e-12, method=0, max_iter=20, reltol=1e-4)
+    with Lanes([net]) as L:
+        reps = L.run_tran(opts, steps_per_launch=4096)
+        x = L.get_x(0)
+    xo, ro, _, _ = oracle.tran_lanes(net, opts)
+    for a, b in zip(reps, ro):
+        assert a.status == 1 and a.steps == b.steps and a.rejects == b.rejects
+    assert worst(x, xo) <= 1.0
