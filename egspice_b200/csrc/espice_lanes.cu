@@ -21,6 +21,8 @@ using namespace espl;
 namespace {
 
 constexpr uint32_t kBlock = kTileThreads;
+// The banded streaming replay: widest band, largest L ring, chunk capacity.
+constexpr uint32_t kBandMax = 15, kBandLRing = 64, kBandWords = 1024, kBandEntries = 64;
 
 // The tiles of the Newton launches whose templates keep the same number of
 // tiles resident per SM: one launch per class, each on its own stream, with
@@ -524,14 +526,27 @@ espl_status plan_classes(espl_lanes* h) {
         Group& g = h->groups[i];
         g.dev.refine_rows = MIXED && h->refine_sweeps > 0 ? 1u : 0u;
         g.dev.stage_mode = kStageNone;
-        for (uint32_t mode : {kStageLu, kStageIndex}) {
+        bytes[i] = 0;
+        const uint32_t band = g.dev.band_ok;
+        bool placed = false;
+        for (uint32_t mode : {kStageLu, kStageIndex, kStageNone}) {
             SmemPlan sp = smem_plan(g.dev, mode, MIXED);
             if (sp.bytes <= (uint32_t)max_dyn) {
                 g.dev.stage_mode = mode;
+                g.dev.band_off = sp.band_off;
                 bytes[i] = sp.bytes;
+                placed = true;
                 break;
             }
         }
+        if (!placed && band) {
+            // not even the band buffers fit: the global replay
+            g.dev.band_ok = 0;
+            g.dev.stage_mode = kStageNone;
+            bytes[i] = 0;
+        }
+        if (g.dev.stage_mode == kStageLu) g.dev.band_ok = 0;
+        (void)band;
         int a = 0, b = 0;
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_tran<MIXED>, kBlock, bytes[i]));
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_static<MIXED>, kBlock, bytes[i]));
@@ -612,6 +627,21 @@ espl_status retape(espl_lanes* h, int tran, double dt) {
             std::vector<uint32_t> prog;
             d.n_prog = lu_program(g.tape, g.col_ptr.data(), prog) ? (uint32_t)prog.size() : 0u;
             if (d.n_prog) UP(lu_prog, prog);
+            // the banded streaming replay, for templates the shared LU chain
+            // cannot hold (plan_classes decides which run it)
+            BandPlan bp;
+            d.band_ok = 0;
+            if (d.n_prog && band_plan(g.tape, prog, kBandMax, kBandLRing, kBandWords, kBandEntries, bp)) {
+                d.band_ok = 1;
+                d.band_w = bp.w_ring;
+                d.band_l = bp.l_ring;
+                d.band_chunks = (uint32_t)bp.chunk_pc.size() - 1;
+                d.band_cw = bp.max_words;
+                d.band_ce = bp.max_entries;
+                UP(band_cpc, bp.chunk_pc);
+                UP(band_cent, bp.chunk_e);
+                UP(band_slot, bp.scat_slot);
+            }
         }
 #undef UP
         size_t P = g.P;

@@ -9,7 +9,7 @@
 #include <climits>
 #include <type_traits>
 
-#include "lane_smem.cuh"
+#include "lane_band.cuh"
 
 namespace espl {
 
@@ -146,6 +146,15 @@ __device__ __forceinline__ void newton_tile(const TileCtx& c, LaneState* s, cons
             sh.acc0[lane] = 0;
             sh.accf[lane] = 0;
         }
+        // The banded streaming replay (lane_band.cuh) of a template the
+        // shared chain cannot hold: every warp takes part; it replays the
+        // lanes in the tile's precision (FP32 lanes of a mixed tile, or FP64).
+        int band_rc = -1;
+        if (!sm && d.band_ok) {
+            const bool comp = warp == 0 && act && (!MIXED || !s->fp64);
+            band_rc = band_refactor<T>(d, warp, lane, l, comp);
+            if (!comp) band_rc = -1;
+        }
         if (warp == 0 && act) {
             bool use32 = MIXED && !s->fp64;
             bool done = false;
@@ -173,14 +182,14 @@ __device__ __forceinline__ void newton_tile(const TileCtx& c, LaneState* s, cons
                 }
             }
             if (!done) {
-                if (use32 && refactor32(d, l)) {
+                if (use32 && (band_rc >= 0 ? band_rc != 0 : refactor32(d, l))) {
                     s->fp64 = 1;
                     s->fallbacks++;
                     use32 = false;
                 }
                 bool fail = false;
                 if (!use32) {
-                    int rc = refactor64(d, l);
+                    int rc = (!MIXED && band_rc >= 0) ? band_rc : refactor64(d, l);
                     fail = rc == 1 || (rc == 2 && !replay_holds64(d, l));
                 }
                 if (fail) {

@@ -196,6 +196,7 @@ struct SmemPlan {
     uint32_t len[S_COUNT];   // padded word counts
     uint32_t idx_words;      // total staged words (multiple of 4)
     uint32_t a_off, w_off, lx_off, ux_off, ud_off;  // byte offsets of the LU chain (kStageLu)
+    uint32_t band_off;       // byte offset of the banded replay's buffers
     uint32_t bytes;          // total dynamic shared memory of the tile
 };
 
@@ -206,16 +207,18 @@ struct SmemPlan {
 // otherwise.
 __host__ __device__ inline SmemPlan smem_plan(const GroupDev& d, uint32_t mode, bool f32) {
     SmemPlan p{};
-    if (mode == kStageNone) return p;
     const uint32_t es = f32 ? 4u : 8u;
-    uint32_t o = 4;  // the first 16 bytes hold the mbarrier
-    for (int k = 0; k < S_COUNT; k++) {
-        p.off[k] = o;
-        p.len[k] = pad4(stage_words(d, k, mode));
-        o += p.len[k];
+    uint32_t b = 0;
+    if (mode != kStageNone) {
+        uint32_t o = 4;  // the first 16 bytes hold the mbarrier
+        for (int k = 0; k < S_COUNT; k++) {
+            p.off[k] = o;
+            p.len[k] = pad4(stage_words(d, k, mode));
+            o += p.len[k];
+        }
+        p.idx_words = o - 4;
+        b = o * 4;
     }
-    p.idx_words = o - 4;
-    uint32_t b = o * 4;
     if (mode == kStageLu) {
         b = (b + 15u) & ~15u;
         p.a_off = b;
@@ -228,6 +231,12 @@ __host__ __device__ inline SmemPlan smem_plan(const GroupDev& d, uint32_t mode, 
         b += d.nnz_u * 32u * es;
         p.ud_off = b;
         b += d.n * 32u * es;
+    }
+    // the banded replay's buffers (lane_band.cuh) after the staged arrays
+    if (mode != kStageLu && d.band_ok) {
+        b = (b + 15u) & ~15u;
+        p.band_off = b;
+        b += 2u * d.band_cw * 4u + 2u * d.band_ce * 32u * 8u + (d.band_w + d.band_l) * 32u * 8u;
     }
     p.bytes = (b + 15u) & ~15u;
     return p;

@@ -836,4 +836,100 @@ bool lu_program(const Tape& t, const uint32_t* col_ptr, std::vector<uint32_t>& p
     return true;
 }
 
+namespace {
+uint32_t pow2_at_least(uint32_t v) {
+    uint32_t p = 1;
+    while (p < v) p <<= 1;
+    return p;
+}
+}  // namespace
+
+bool band_plan(const Tape& t, const std::vector<uint32_t>& prog, uint32_t max_band, uint32_t max_l_ring,
+               uint32_t chunk_words, uint32_t chunk_entries, BandPlan& out) {
+    out = BandPlan{};
+    const uint32_t n = t.n;
+    if (prog.empty() || n == 0) return false;
+    for (uint32_t k = 0; k < n; k++)
+        if (t.flags[k] & 1u) return false;
+    // the band: every row the replay and the solves touch at column k
+    uint32_t band = 0;
+    auto see = [&](uint32_t r, uint32_t k) { band = std::max(band, r > k ? r - k : k - r); };
+    {
+        uint32_t k = 0;
+        for (uint32_t pc = 0; pc < prog.size();) {
+            uint32_t h = prog[pc], op = h & 15u;
+            if (op == kOpEnd) break;
+            if (op == kOpScat) {
+                uint32_t cnt = h >> 4;
+                for (uint32_t j = 0; j < cnt; j++) see(prog[pc + 1 + j] >> 16, k);
+                pc += 1 + cnt;
+            } else if (op == kOpTake) {
+                uint32_t cnt = h >> 4;
+                see(prog[pc + 1] >> 16, k);
+                for (uint32_t j = 0; j < cnt; j++) see(prog[pc + 2 + j] >> 16, k);
+                pc += 2 + cnt;
+            } else if (op == kOpPiv) {
+                uint32_t cnt = h >> 8;
+                k = prog[pc + 1];
+                see(k, k);
+                for (uint32_t j = 0; j < cnt; j++) see(prog[pc + 2 + j] >> 16, k);
+                pc += 2 + cnt;
+                k++;
+            } else {
+                return false;
+            }
+        }
+    }
+    // (a column's scatter and take entries come before its pivot op, which
+    // names k; the running k is already that column)
+    if (band > max_band) return false;
+    uint32_t lwin = 0;
+    for (uint32_t k = 0; k < n; k++) {
+        uint32_t k0 = k > band ? k - band : 0;
+        lwin = std::max(lwin, t.lp[k + 1] - t.lp[k0]);
+    }
+    out.band = band;
+    out.w_ring = pow2_at_least(2 * band + 2);
+    out.l_ring = pow2_at_least(std::max(lwin, 1u));
+    if (out.l_ring > max_l_ring) return false;
+    // chunks on op boundaries
+    uint32_t words = 0, entries = 0, e = 0;
+    out.chunk_pc.push_back(0);
+    out.chunk_e.push_back(0);
+    for (uint32_t pc = 0; pc < prog.size();) {
+        uint32_t h = prog[pc], op = h & 15u;
+        uint32_t size = 1, ents = 0;
+        if (op == kOpEnd) break;
+        if (op == kOpScat) {
+            size = 1 + (h >> 4);
+            ents = h >> 4;
+            for (uint32_t j = 0; j < ents; j++) out.scat_slot.push_back(prog[pc + 1 + j] & 0xffffu);
+        } else if (op == kOpTake) {
+            size = 2 + (h >> 4);
+        } else {
+            size = 2 + (h >> 8);
+        }
+        if (size > chunk_words || ents > chunk_entries) return false;
+        if (words + size > chunk_words || entries + ents > chunk_entries) {
+            out.chunk_pc.push_back(pc);
+            out.chunk_e.push_back(e);
+            words = entries = 0;
+        }
+        words += size;
+        entries += ents;
+        e += ents;
+        pc += size;
+    }
+    uint32_t end = 0;
+    while (end < prog.size() && prog[end] != kOpEnd) {
+        uint32_t h = prog[end], op = h & 15u;
+        end += op == kOpScat ? 1 + (h >> 4) : op == kOpTake ? 2 + (h >> 4) : 2 + (h >> 8);
+    }
+    out.chunk_pc.push_back(end);
+    out.chunk_e.push_back(e);
+    out.max_words = chunk_words;
+    out.max_entries = chunk_entries;
+    return true;
+}
+
 }  // namespace espl

@@ -54,4 +54,21 @@ bool factor_tape(uint32_t n, const uint32_t* col_ptr, const uint32_t* row_idx, c
 enum LuOp : uint32_t { kOpEnd = 0, kOpScat = 1, kOpTake = 2, kOpPiv = 3, kOpVoid = 4 };
 bool lu_program(const Tape& t, const uint32_t* col_ptr, std::vector<uint32_t>& prog);
 
+// The banded streaming replay: when the replay of every column k touches
+// only work-vector rows within k - band .. k + band (a ladder's elimination
+// walks its chain), the work vector fits a ring of w_ring rows and the L
+// entries an axpy can read (those of the previous `band` columns) a ring of
+// l_ring slots, both in shared memory. The program streams through shared
+// memory in chunks that end on op boundaries (chunk_pc, chunk_e: the
+// program word and scatter-entry offsets of each chunk, n_chunks + 1 each),
+// with the A slot of every scatter entry in program order (scat_slot).
+struct BandPlan {
+    uint32_t band = 0, w_ring = 0, l_ring = 0, max_words = 0, max_entries = 0;
+    std::vector<uint32_t> chunk_pc, chunk_e, scat_slot;
+};
+// False when the template does not qualify (a void column, a band past
+// max_band, an L ring past max_l_ring, or no program).
+bool band_plan(const Tape& t, const std::vector<uint32_t>& prog, uint32_t max_band, uint32_t max_l_ring,
+               uint32_t chunk_words, uint32_t chunk_entries, BandPlan& out);
+
 }  // namespace espl
