@@ -638,9 +638,13 @@ espl_status retape(espl_lanes* h, int tran, double dt) {
                 d.band_chunks = (uint32_t)bp.chunk_pc.size() - 1;
                 d.band_cw = bp.max_words;
                 d.band_ce = bp.max_entries;
+                d.band_b = bp.band;
+                d.band_nblk = (uint32_t)bp.solve_col.size() - 1;
                 UP(band_cpc, bp.chunk_pc);
                 UP(band_cent, bp.chunk_e);
                 UP(band_slot, bp.scat_slot);
+                UP(band_scol, bp.solve_col);
+                UP(band_rowof, bp.rowof);
             }
         }
 #undef UP

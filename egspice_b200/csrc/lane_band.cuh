@@ -23,6 +23,26 @@ __host__ __device__ inline uint32_t band_bytes(uint32_t words, uint32_t entries,
     return 2u * words * 4u + 2u * entries * 32u * 8u + (w_ring + l_ring) * 32u * 8u;
 }
 
+// Streams count values into dst with warps 1-3 (thread t of nt), eight per
+// thread in flight: all eight sources are loaded before any is stored, so
+// the loads' latencies overlap instead of adding up.
+template <typename F>
+__device__ __forceinline__ void stream8(uint32_t t, uint32_t nt, uint32_t count, double* __restrict__ dst, F src) {
+    for (uint32_t b0 = t; b0 < count; b0 += 8u * nt) {
+        double v[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            const uint32_t i = b0 + (uint32_t)j * nt;
+            v[j] = i < count ? src(i) : 0.0;
+        }
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            const uint32_t i = b0 + (uint32_t)j * nt;
+            if (i < count) dst[i] = v[j];
+        }
+    }
+}
+
 struct BandAcc {
     bool bad, nonfinite;
     uint64_t worst;
@@ -153,12 +173,10 @@ __device__ int band_refactor(const GroupDev& d, uint32_t warp, uint32_t lane, ui
         const uint32_t e0 = d.band_cent[c], ne = d.band_cent[c + 1] - e0;
         uint32_t* pb = progbuf + b * d.band_cw;
         double* ab = abuf + (size_t)b * d.band_ce * 32u;
-        const uint32_t t = threadIdx.x - 32u;
-        for (uint32_t i = t; i < nw; i += blockDim.x - 32u) pb[i] = d.lu_prog[pc0 + i];
-        for (uint32_t i = t; i < ne * 32u; i += blockDim.x - 32u) {
-            const uint32_t e = i >> 5, ln = i & 31u;
-            ab[i] = d.a[(size_t)d.band_slot[e0 + e] * P + lbase + ln];
-        }
+        const uint32_t t = threadIdx.x - 32u, nt = blockDim.x - 32u;
+        for (uint32_t i = t; i < nw; i += nt) pb[i] = d.lu_prog[pc0 + i];
+        stream8(t, nt, ne * 32u, ab,
+                [&](uint32_t i) { return d.a[(size_t)d.band_slot[e0 + (i >> 5)] * P + lbase + (i & 31u)]; });
     };
     // the work ring starts at zero; every column leaves it at zero
     {
@@ -186,6 +204,128 @@ __device__ int band_refactor(const GroupDev& d, uint32_t warp, uint32_t lane, ui
     if (void_hit || acc.nonfinite || acc.bad) return 1;
     if constexpr (f64) return bitsd(acc.worst) <= kWide ? 0 : 2;
     return 0;
+}
+
+// The forward and back substitutions of the banded lanes (luSolve with neg,
+// the same operations and order as solve64 / solve32), streamed by column
+// blocks: y lives in a ring of band_w rows; pivot position j enters the
+// forward ring (as -rhs of its row) when column j - band starts, and the
+// back ring (as its forward result, kept in the lane's global y) when
+// column j + band starts; dx[q[k]] is written as column k finishes. Warps
+// 1-3 stage the next block's indices and factor values while warp 0 runs
+// the current one.
+template <typename T>
+__device__ void band_solve(const GroupDev& d, uint32_t warp, uint32_t lane, uint32_t l, bool compute) {
+    const uint32_t P = d.P, n = d.n, B = d.band_b, wm = d.band_w - 1;
+    constexpr uint32_t kC = kSolveCols, kE = kSolveEntries;
+    unsigned char* base = g_dsm + d.band_off;
+    T* yr = reinterpret_cast<T*>(base + 2u * kSolveBufBytes);
+    constexpr bool f64 = sizeof(T) == 8;
+    const T* lxg;
+    const T* uxg;
+    const T* udg;
+    T* yg;
+    if constexpr (f64) {
+        lxg = d.lx;
+        uxg = d.ux;
+        udg = d.udiag;
+        yg = d.y;
+    } else {
+        lxg = d.lx32;
+        uxg = d.ux32;
+        udg = d.udiag32;
+        yg = d.y32;
+    }
+    const uint32_t lbase = l - lane;
+    const uint32_t t = threadIdx.x - 32u, nt = blockDim.x - 32u;
+    auto bidx = [&](uint32_t b) { return reinterpret_cast<uint32_t*>(base + b * kSolveBufBytes); };
+    auto bval = [&](uint32_t b) { return reinterpret_cast<double*>(base + b * kSolveBufBytes + kSolveIdxWords * 4u); };
+    auto bcol = [&](uint32_t b) {
+        return reinterpret_cast<double*>(base + b * kSolveBufBytes + kSolveIdxWords * 4u + kE * 32u * 8u);
+    };
+#define YR(r) yr[(size_t)((r) & wm) * 32 + lane]
+    const uint32_t nblk = d.band_nblk;
+    // forward: block c covers columns scol[c] .. scol[c + 1)
+    auto load_fwd = [&](uint32_t c, uint32_t b) {
+        const uint32_t k0 = d.band_scol[c], k1 = d.band_scol[c + 1], cols = k1 - k0;
+        const uint32_t e0 = d.lp[k0], ne = d.lp[k1] - e0;
+        uint32_t* ix = bidx(b);
+        double* vv = bval(b);
+        double* cv = bcol(b);
+        for (uint32_t i = t; i <= cols; i += nt) ix[i] = d.lp[k0 + i] - e0;
+        for (uint32_t i = t; i < ne; i += nt) ix[kC + 1 + i] = d.li[e0 + i];
+        stream8(t, nt, ne * 32u, vv,
+                [&](uint32_t i) { return (double)lxg[(size_t)(e0 + (i >> 5)) * P + lbase + (i & 31u)]; });
+        stream8(t, nt, cols * 32u, cv, [&](uint32_t i) {
+            const uint32_t k = k0 + (i >> 5), j = k + B;
+            return (k >= 1 && j < n) ? d.rhs[(size_t)d.band_rowof[j] * P + lbase + (i & 31u)] : 0.0;
+        });
+    };
+    if (compute)
+        for (uint32_t j = 0; j <= B && j < n; j++) YR(j) = (T)(-LM(d.rhs, d.band_rowof[j]));
+    if (warp != 0) load_fwd(0, 0);
+    __syncthreads();
+    for (uint32_t c = 0; c < nblk; c++) {
+        if (warp != 0 && c + 1 < nblk) load_fwd(c + 1, (c + 1) & 1u);
+        if (compute) {
+            const uint32_t b = c & 1u, k0 = d.band_scol[c], cols = d.band_scol[c + 1] - k0;
+            const uint32_t* ix = bidx(b);
+            const double* vv = bval(b);
+            const double* cv = bcol(b);
+            for (uint32_t kk = 0; kk < cols; kk++) {
+                const uint32_t k = k0 + kk;
+                if (k >= 1 && k + B < n) YR(k + B) = (T)(-cv[kk * 32 + lane]);
+                const T yk = YR(k);
+                LM(yg, k) = yk;
+                if (yk != (T)0)
+                    for (uint32_t j = ix[kk]; j < ix[kk + 1]; j++) YR(ix[kC + 1 + j]) -= (T)vv[j * 32 + lane] * yk;
+            }
+        }
+        __syncthreads();
+    }
+    // back: blocks in reverse, columns descending
+    auto load_bwd = [&](uint32_t c, uint32_t b) {
+        const uint32_t k0 = d.band_scol[c], k1 = d.band_scol[c + 1], cols = k1 - k0;
+        const uint32_t e0 = d.up[k0], ne = d.up[k1] - e0;
+        uint32_t* ix = bidx(b);
+        double* vv = bval(b);
+        double* cv = bcol(b);
+        for (uint32_t i = t; i <= cols; i += nt) ix[i] = d.up[k0 + i] - e0;
+        for (uint32_t i = t; i < ne; i += nt) ix[kC + 1 + i] = d.ui[e0 + i];
+        for (uint32_t i = t; i < cols; i += nt) ix[kC + 1 + kE + i] = d.q[k0 + i];
+        stream8(t, nt, ne * 32u, vv,
+                [&](uint32_t i) { return (double)uxg[(size_t)(e0 + (i >> 5)) * P + lbase + (i & 31u)]; });
+        stream8(t, nt, cols * 32u, cv,
+                [&](uint32_t i) { return (double)udg[(size_t)(k0 + (i >> 5)) * P + lbase + (i & 31u)]; });
+        stream8(t, nt, cols * 32u, cv + kC * 32u, [&](uint32_t i) {
+            const uint32_t k = k0 + (i >> 5);
+            return (k + 2 <= n && k >= B) ? (double)yg[(size_t)(k - B) * P + lbase + (i & 31u)] : 0.0;
+        });
+    };
+    if (compute)
+        for (uint32_t j = (n - 1 >= B ? n - 1 - B : 0); j < n; j++) YR(j) = LM(yg, j);
+    if (warp != 0) load_bwd(nblk - 1, (nblk - 1) & 1u);
+    __syncthreads();
+    for (uint32_t cc = nblk; cc-- > 0;) {
+        if (warp != 0 && cc > 0) load_bwd(cc - 1, (cc - 1) & 1u);
+        if (compute) {
+            const uint32_t b = cc & 1u, k0 = d.band_scol[cc], cols = d.band_scol[cc + 1] - k0;
+            const uint32_t* ix = bidx(b);
+            const double* vv = bval(b);
+            const double* cv = bcol(b);
+            for (uint32_t kk = cols; kk-- > 0;) {
+                const uint32_t k = k0 + kk;
+                if (k + 2 <= n && k >= B) YR(k - B) = (T)cv[kC * 32u + kk * 32 + lane];
+                const T zk = YR(k) / (T)cv[kk * 32 + lane];
+                YR(k) = zk;
+                LM(d.dx, ix[kC + 1 + kE + kk]) = (double)zk;
+                if (zk != (T)0)
+                    for (uint32_t j = ix[kk]; j < ix[kk + 1]; j++) YR(ix[kC + 1 + j]) -= (T)vv[j * 32 + lane] * zk;
+            }
+        }
+        __syncthreads();
+    }
+#undef YR
 }
 
 }  // namespace espl

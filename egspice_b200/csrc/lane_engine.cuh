@@ -45,8 +45,9 @@ struct GroupDev {
     // The banded streaming replay (lane_band.cuh, tape.h BandPlan): ring
     // sizes, chunk capacities and count, the shared-memory offset of its
     // buffers, and the chunk tables and scatter slots in global memory.
-    uint32_t band_ok, band_w, band_l, band_chunks, band_cw, band_ce, band_off, band_pad;
-    const uint32_t *band_cpc, *band_cent, *band_slot;
+    uint32_t band_ok, band_w, band_l, band_chunks, band_cw, band_ce, band_off, band_b;
+    uint32_t band_nblk, band_pad;
+    const uint32_t *band_cpc, *band_cent, *band_slot, *band_scol, *band_rowof;
     const uint8_t* cur_row;
     const uint32_t *res_t, *res_s, *cap_t, *cap_s, *vsrc_t, *vsrc_s, *isrc_t, *dio_t, *dio_s, *mos_t, *mos_s;
     const double *res_r, *cap_c, *vsrc_p, *isrc_p, *dio_d, *mos_d;

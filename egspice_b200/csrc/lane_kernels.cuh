@@ -150,14 +150,20 @@ __device__ __forceinline__ void newton_tile(const TileCtx& c, LaneState* s, cons
         // shared chain cannot hold: every warp takes part; it replays the
         // lanes in the tile's precision (FP32 lanes of a mixed tile, or FP64).
         int band_rc = -1;
+        bool band_solved = false;
         if (!sm && d.band_ok) {
             const bool comp = warp == 0 && act && (!MIXED || !s->fp64);
             band_rc = band_refactor<T>(d, warp, lane, l, comp);
             if (!comp) band_rc = -1;
+            // lanes whose replay held solve through the streamed blocks too
+            band_solved = band_rc == 0;
+            band_solve<T>(d, warp, lane, l, band_solved);
         }
         if (warp == 0 && act) {
             bool use32 = MIXED && !s->fp64;
-            bool done = false;
+            bool done = band_solved;
+            if (band_solved && MIXED)
+                for (uint32_t r = 0; r < o.refine; r++) refine_mixed(d, l);
             if (sm && (use32 || !MIXED)) {
                 int rc = d.n_prog ? refactor_prog<T>(d, st, lane, l) : refactor_smem<T>(d, st, lane, l);
                 if (MIXED && rc != 0) {

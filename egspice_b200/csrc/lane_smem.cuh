@@ -72,6 +72,12 @@ enum StageArr {
     S_RTPTR, S_RTCOL, S_RTPOS, S_PROG, S_COUNT
 };
 
+// One streamed block of the banded solves (lane_band.cuh): index words
+// (column pointers, row indices, output columns), the block's factor entries
+// and its per-column values, for 32 lanes.
+constexpr uint32_t kSolveIdxWords = 160;  // >= kSolveCols + 1 + kSolveEntries + kSolveCols
+constexpr uint32_t kSolveBufBytes = kSolveIdxWords * 4u + 64u * 32u * 8u + 2u * 32u * 32u * 8u;
+
 // Staging modes of a template: nothing, the index arrays, or the index
 // arrays and the LU chain.
 enum : uint32_t { kStageNone = 0, kStageIndex = 1, kStageLu = 2 };
@@ -232,11 +238,14 @@ __host__ __device__ inline SmemPlan smem_plan(const GroupDev& d, uint32_t mode, 
         p.ud_off = b;
         b += d.n * 32u * es;
     }
-    // the banded replay's buffers (lane_band.cuh) after the staged arrays
+    // the banded replay's and solves' buffers (lane_band.cuh, shared in
+    // time) after the staged arrays
     if (mode != kStageLu && d.band_ok) {
         b = (b + 15u) & ~15u;
         p.band_off = b;
-        b += 2u * d.band_cw * 4u + 2u * d.band_ce * 32u * 8u + (d.band_w + d.band_l) * 32u * 8u;
+        uint32_t refac = 2u * d.band_cw * 4u + 2u * d.band_ce * 32u * 8u + (d.band_w + d.band_l) * 32u * 8u;
+        uint32_t solve = 2u * kSolveBufBytes + d.band_w * 32u * 8u;
+        b += refac > solve ? refac : solve;
     }
     p.bytes = (b + 15u) & ~15u;
     return p;

@@ -929,6 +929,20 @@ bool band_plan(const Tape& t, const std::vector<uint32_t>& prog, uint32_t max_ba
     out.chunk_e.push_back(e);
     out.max_words = chunk_words;
     out.max_entries = chunk_entries;
+    // column blocks of the solves
+    out.solve_col.push_back(0);
+    uint32_t k0 = 0;
+    for (uint32_t k = 0; k < n; k++) {
+        uint32_t nl = t.lp[k + 1] - t.lp[k0], nu = t.up[k + 1] - t.up[k0];
+        if (t.lp[k + 1] - t.lp[k] > kSolveEntries || t.up[k + 1] - t.up[k] > kSolveEntries) return false;
+        if (k + 1 - k0 > kSolveCols || nl > kSolveEntries || nu > kSolveEntries) {
+            out.solve_col.push_back(k);
+            k0 = k;
+        }
+    }
+    out.solve_col.push_back(n);
+    out.rowof.assign(n, 0);
+    for (uint32_t r = 0; r < n; r++) out.rowof[t.pinv[r]] = r;
     return true;
 }
 

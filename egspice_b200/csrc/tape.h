@@ -65,7 +65,12 @@ bool lu_program(const Tape& t, const uint32_t* col_ptr, std::vector<uint32_t>& p
 struct BandPlan {
     uint32_t band = 0, w_ring = 0, l_ring = 0, max_words = 0, max_entries = 0;
     std::vector<uint32_t> chunk_pc, chunk_e, scat_slot;
+    // The solves stream the factor by column blocks: solve_col[c] .. solve_col[c + 1]
+    // is block c (at most kSolveCols columns, kSolveEntries L and U entries);
+    // rowof[j] is the row whose right-hand side starts pivot position j.
+    std::vector<uint32_t> solve_col, rowof;
 };
+constexpr uint32_t kSolveCols = 32, kSolveEntries = 64;
 // False when the template does not qualify (a void column, a band past
 // max_band, an L ring past max_l_ring, or no program).
 bool band_plan(const Tape& t, const std::vector<uint32_t>& prog, uint32_t max_band, uint32_t max_l_ring,
