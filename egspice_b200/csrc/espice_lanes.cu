@@ -30,6 +30,7 @@ constexpr uint32_t kBandMax = 15, kBandLRing = 64, kBandWords = 1024, kBandEntri
 struct LaunchClass {
     uint32_t smem = 0;        // dynamic shared memory per tile
     uint32_t per_sm = 0;      // resident tiles per SM at that size
+    bool wide = false;        // kWideWarps per tile (the banded replay's templates)
     std::vector<uint32_t> tiles;
     uint32_t* d_tiles = nullptr;
     cudaStream_t stream = nullptr;  // null: the handle's stream
@@ -490,7 +491,7 @@ espl_status launch_classes(espl_lanes* h, F fn) {
         cudaStream_t st = k == 0 ? h->stream : c.stream;
         if (k) CK(cudaStreamWaitEvent(st, h->fork, 0));
         TileMap m{h->d_groups, h->d_warp_group, c.d_tiles, (uint32_t)c.tiles.size()};
-        fn(m, (uint32_t)c.tiles.size(), c.smem, st);
+        fn(m, (uint32_t)c.tiles.size(), c.smem, st, c.wide);
         CK(cudaGetLastError());
         if (k) CK(cudaEventRecord(c.done, st));
     }
@@ -515,13 +516,16 @@ espl_status plan_classes(espl_lanes* h) {
     int dev = h->device, optin = 0;
     CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     cudaFuncAttributes fs, ft;
-    CK(cudaFuncGetAttributes(&fs, k_static<MIXED>));
-    CK(cudaFuncGetAttributes(&ft, k_tran<MIXED>));
+    CK(cudaFuncGetAttributes(&fs, k_static<MIXED, false>));
+    CK(cudaFuncGetAttributes(&ft, k_tran<MIXED, false>));
     int max_dyn = optin - (int)std::max(fs.sharedSizeBytes, ft.sharedSizeBytes);
-    CK(cudaFuncSetAttribute(k_static<MIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn));
-    CK(cudaFuncSetAttribute(k_tran<MIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn));
+    CK(cudaFuncSetAttribute(k_static<MIXED, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn));
+    CK(cudaFuncSetAttribute(k_tran<MIXED, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn));
+    CK(cudaFuncSetAttribute(k_static<MIXED, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn));
+    CK(cudaFuncSetAttribute(k_tran<MIXED, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn));
     free_classes(h);
     std::vector<uint32_t> bytes(h->groups.size(), 0), per(h->groups.size(), 0);
+    std::vector<bool> wide(h->groups.size(), false);
     for (size_t i = 0; i < h->groups.size(); i++) {
         Group& g = h->groups[i];
         g.dev.refine_rows = MIXED && h->refine_sweeps > 0 ? 1u : 0u;
@@ -547,20 +551,29 @@ espl_status plan_classes(espl_lanes* h) {
         }
         if (g.dev.stage_mode == kStageLu) g.dev.band_ok = 0;
         (void)band;
+        wide[i] = g.dev.band_ok != 0;
         int a = 0, b = 0;
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_tran<MIXED>, kBlock, bytes[i]));
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_static<MIXED>, kBlock, bytes[i]));
+        if (wide[i]) {
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_tran<MIXED, true>, kWideThreads, bytes[i]));
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_static<MIXED, true>, kWideThreads, bytes[i]));
+        } else {
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_tran<MIXED, false>, kBlock, bytes[i]));
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_static<MIXED, false>, kBlock, bytes[i]));
+        }
         per[i] = (uint32_t)std::max(1, std::min(a, b));
     }
-    // classes by resident tiles per SM, the one with the most tiles first
-    std::vector<uint32_t> keys(per.begin(), per.end());
+    // classes by (tile width, resident tiles per SM), the one with the most
+    // tiles first
+    std::vector<uint32_t> keys;
+    for (size_t i = 0; i < per.size(); i++) keys.push_back(per[i] | (wide[i] ? 0x10000u : 0u));
     std::sort(keys.begin(), keys.end());
     keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
     for (uint32_t key : keys) {
         LaunchClass c;
-        c.per_sm = key;
+        c.per_sm = key & 0xffffu;
+        c.wide = (key & 0x10000u) != 0;
         for (size_t i = 0; i < h->groups.size(); i++) {
-            if (per[i] != key) continue;
+            if ((per[i] | (wide[i] ? 0x10000u : 0u)) != key) continue;
             c.smem = std::max(c.smem, bytes[i]);
             for (uint32_t t = 0; t < h->groups[i].P / 32; t++) c.tiles.push_back(h->groups[i].tile0 + t);
         }
@@ -678,12 +691,17 @@ NewtonParams newton_params(const espl_newton_opts& o, uint32_t precision, uint32
 
 espl_status run_static(espl_lanes* h, const NewtonParams& np, int tran) {
     CK(cudaEventRecord(h->ev0, h->stream));
-    espl_status s = launch_classes(h, [&](const TileMap& m, uint32_t grid, uint32_t smem, cudaStream_t st) {
-        if (np.mixed)
-            k_static<true><<<grid, kBlock, smem, st>>>(m, np, h->d_state, tran);
-        else
-            k_static<false><<<grid, kBlock, smem, st>>>(m, np, h->d_state, tran);
-    });
+    espl_status s =
+        launch_classes(h, [&](const TileMap& m, uint32_t grid, uint32_t smem, cudaStream_t st, bool wide) {
+            if (np.mixed && wide)
+                k_static<true, true><<<grid, kWideThreads, smem, st>>>(m, np, h->d_state, tran);
+            else if (np.mixed)
+                k_static<true, false><<<grid, kBlock, smem, st>>>(m, np, h->d_state, tran);
+            else if (wide)
+                k_static<false, true><<<grid, kWideThreads, smem, st>>>(m, np, h->d_state, tran);
+            else
+                k_static<false, false><<<grid, kBlock, smem, st>>>(m, np, h->d_state, tran);
+        });
     if (s) return s;
     CK(cudaEventRecord(h->ev1, h->stream));
     CK(cudaEventSynchronize(h->ev1));
@@ -733,7 +751,7 @@ espl_status espl_create(const espl_netlist* nets, uint32_t n_nets, const espl_cr
     if (h->device >= ndev) return bail(ESPL_INVALID_ARGUMENT);
     if (cudaSetDevice(h->device) != cudaSuccess) return bail(ESPL_DRIVER);
     cudaFuncAttributes fa;
-    if (cudaFuncGetAttributes(&fa, k_static<false>) != cudaSuccess) return bail(ESPL_NO_IMAGE);
+    if (cudaFuncGetAttributes(&fa, k_static<false, false>) != cudaSuccess) return bail(ESPL_NO_IMAGE);
     if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(ESPL_DRIVER);
     cudaEventCreate(&h->ev0);
     cudaEventCreate(&h->ev1);
@@ -940,12 +958,17 @@ espl_status espl_device_launch(espl_lanes* h, uint32_t max_steps, espl_step_repo
     espl_newton_opts op{t.reltol, t.abstol, t.vntol, 0.0, t.residual_tol, t.max_iter, 0};
     NewtonParams np = newton_params(op, h->precision, h->refine_sweeps);
     CK(cudaEventRecord(h->ev0, h->stream));
-    espl_status s = launch_classes(h, [&](const TileMap& m, uint32_t grid, uint32_t smem, cudaStream_t st) {
-        if (np.mixed)
-            k_tran<true><<<grid, kBlock, smem, st>>>(m, t, np, h->d_state);
-        else
-            k_tran<false><<<grid, kBlock, smem, st>>>(m, t, np, h->d_state);
-    });
+    espl_status s =
+        launch_classes(h, [&](const TileMap& m, uint32_t grid, uint32_t smem, cudaStream_t st, bool wide) {
+            if (np.mixed && wide)
+                k_tran<true, true><<<grid, kWideThreads, smem, st>>>(m, t, np, h->d_state);
+            else if (np.mixed)
+                k_tran<true, false><<<grid, kBlock, smem, st>>>(m, t, np, h->d_state);
+            else if (wide)
+                k_tran<false, true><<<grid, kWideThreads, smem, st>>>(m, t, np, h->d_state);
+            else
+                k_tran<false, false><<<grid, kBlock, smem, st>>>(m, t, np, h->d_state);
+        });
     if (s) return s;
     CK(cudaEventRecord(h->ev1, h->stream));
     CK(cudaEventSynchronize(h->ev1));

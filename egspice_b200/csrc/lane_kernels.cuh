@@ -1,5 +1,5 @@
 // Kernels of the lane sweep. One CTA per 32-lane tile of one template
-// (kWarps warps): the whole Newton solve of an operating point, or up to
+// (kWarps warps, kWideWarps for large templates): the whole Newton solve of an operating point, or up to
 // `launch_steps` transient attempts with device step control, in one launch.
 // The tile -> template table lets one launch carry templates of different
 // sizes. Every loop is bounded by max_iter / launch_steps; no kernel waits on
@@ -28,6 +28,7 @@ __device__ __forceinline__ TileCtx tile_ctx(const TileMap& m) {
     c.d = &m.groups[m.tile_group[c.tile]];
     c.lane = threadIdx.x & 31;
     c.warp = threadIdx.x >> 5;
+    c.nw = blockDim.x >> 5;
     c.l = (c.tile - c.d->tile0) * 32 + c.lane;
     c.valid = c.l < c.d->lanes;
     return c;
@@ -65,7 +66,7 @@ __device__ __forceinline__ void newton_tile(const TileCtx& c, LaneState* s, cons
                                             bool tran_companion, bool on, TileShared& sh, unsigned char* dsm,
                                             bool eval0) {
     const GroupDev& d = *c.d;
-    const uint32_t l = c.l, P = d.P, lane = c.lane, warp = c.warp;
+    const uint32_t l = c.l, P = d.P, lane = c.lane, warp = c.warp, nw = c.nw;
     const uint32_t ninst = n_instances(d);
     using T = typename std::conditional<MIXED, float, double>::type;
     const bool sm = d.stage_mode == kStageLu;
@@ -87,7 +88,7 @@ __device__ __forceinline__ void newton_tile(const TileCtx& c, LaneState* s, cons
         }
     }
     if (eval0 && c.valid && on)
-        for (uint32_t t = warp; t < ninst; t += kWarps) inst_eval(d, l, t, tran, 0.0, cell_buf(d, 0));
+        for (uint32_t t = warp; t < ninst; t += nw) inst_eval(d, l, t, tran, 0.0, cell_buf(d, 0));
     __syncthreads();
     uint32_t cur = 0;
     for (uint32_t it = 0; it < o.max_iter; it++) {
@@ -106,12 +107,12 @@ __device__ __forceinline__ void newton_tile(const TileCtx& c, LaneState* s, cons
         if (act) {
             if (sm) {
                 T* sa = static_cast<T*>(st.a);
-                for (uint32_t p = warp; p < d.nnz; p += kWarps)
+                for (uint32_t p = warp; p < d.nnz; p += nw)
                     sa[p * 32 + lane] = (T)gather_slot(d, l, p, cp, o.gmin, cells);
             } else {
-                for (uint32_t p = warp; p < d.nnz; p += kWarps) gather_slot(d, l, p, cp, o.gmin, cells);
+                for (uint32_t p = warp; p < d.nnz; p += nw) gather_slot(d, l, p, cp, o.gmin, cells);
             }
-            for (uint32_t i = warp; i < d.n; i += kWarps) gather_row(d, l, i, cp, o.gmin, cells);
+            for (uint32_t i = warp; i < d.n; i += nw) gather_row(d, l, i, cp, o.gmin, cells);
         }
         __syncthreads();
         if (it == 0) {
@@ -119,7 +120,7 @@ __device__ __forceinline__ void newton_tile(const TileCtx& c, LaneState* s, cons
             double g = 1.0;
             unsigned long long xm = 0, fm = 0;
             if (act) {
-                for (uint32_t i = warp; i < d.n; i += kWarps) {
+                for (uint32_t i = warp; i < d.n; i += nw) {
                     g = fmax(g, fabs(LM(d.a, d.diag[i])));
                     unsigned long long xb = dbits(fabs(LM(d.x, i))), fb = dbits(fabs(LM(d.rhs, i)));
                     xm = xm > xb ? xm : xb;
@@ -217,7 +218,7 @@ __device__ __forceinline__ void newton_tile(const TileCtx& c, LaneState* s, cons
         // updateNorm (kernels/lane.zig:161-179), rows split over warps.
         unsigned long long worst = 0;
         if (act)
-            for (uint32_t i = warp; i < d.n; i += kWarps) {
+            for (uint32_t i = warp; i < d.n; i += nw) {
                 double xo = LM(d.x, i), dd = LM(d.dx, i);
                 double xn = xo + dd;
                 LM(d.x_old, i) = xo;
@@ -237,10 +238,10 @@ __device__ __forceinline__ void newton_tile(const TileCtx& c, LaneState* s, cons
         uint32_t flags = 0;
         if (act) {
             double* next = cell_buf(d, cur ^ 1u);
-            for (uint32_t t = warp; t < ninst; t += kWarps)
+            for (uint32_t t = warp; t < ninst; t += nw)
                 if (inst_limit_eval(d, l, t, tran, tm, next)) flags |= kLimited;
             double lim = sh.limit[lane];
-            for (uint32_t i = warp; i < d.n; i += kWarps) {
+            for (uint32_t i = warp; i < d.n; i += nw) {
                 double xi = LM(d.x, i);
                 if (!(fabs(xi) <= lim)) flags |= kImplausible;
                 double scale = fabs(LM(d.a, d.diag[i]));
@@ -275,7 +276,7 @@ __device__ __forceinline__ void newton_tile(const TileCtx& c, LaneState* s, cons
         }
         __syncthreads();
         if (c.valid && sh.restore[lane])
-            for (uint32_t i = warp; i < d.n; i += kWarps) LM(d.x, i) = LM(d.x_old, i);
+            for (uint32_t i = warp; i < d.n; i += nw) LM(d.x, i) = LM(d.x_old, i);
         cur ^= 1u;
     }
     __syncthreads();
@@ -283,8 +284,9 @@ __device__ __forceinline__ void newton_tile(const TileCtx& c, LaneState* s, cons
 }
 
 
-template <bool MIXED>
-__global__ void __launch_bounds__(kTileThreads, 4) k_static(TileMap m, NewtonParams o, LaneState* st, int tran) {
+template <bool MIXED, bool WIDE>
+__global__ void __launch_bounds__(WIDE ? kWideThreads : kTileThreads, WIDE ? 1 : 4)
+    k_static(TileMap m, NewtonParams o, LaneState* st, int tran) {
     __shared__ TileShared sh;
     TileCtx c = tile_ctx(m);
     c.d = stage_template(*c.d, sh.gd, g_dsm, MIXED);
@@ -297,6 +299,7 @@ __global__ void __launch_bounds__(kTileThreads, 4) k_static(TileMap m, NewtonPar
 __global__ void __launch_bounds__(kTileThreads) k_prep(TileMap m, const double* const* mos_raw,
                                                        const double* const* dio_raw) {
     TileCtx c = tile_ctx(m);
+    const uint32_t nw = c.nw;
     if (!c.valid) return;
     const GroupDev& d = *c.d;
     const uint32_t P = d.P, l = c.l;
@@ -305,13 +308,13 @@ __global__ void __launch_bounds__(kTileThreads) k_prep(TileMap m, const double* 
     const double* dr = dio_raw[g];
     double* md = const_cast<double*>(d.mos_d);
     double* dd = const_cast<double*>(d.dio_d);
-    for (uint32_t i = c.warp; i < d.n_mos; i += kWarps) {
+    for (uint32_t i = c.warp; i < d.n_mos; i += nw) {
         double p[9], o[Mos1Prep::count];
         for (int k = 0; k < 9; k++) p[k] = LM(mr, 9 * i + k);
         mos1_setup(p, o);
         for (int k = 0; k < Mos1Prep::count; k++) LM(md, Mos1Prep::count * i + k) = o[k];
     }
-    for (uint32_t i = c.warp; i < d.n_dio; i += kWarps) {
+    for (uint32_t i = c.warp; i < d.n_dio; i += nw) {
         double p[7], o[DiodePrep::count];
         for (int k = 0; k < 7; k++) p[k] = LM(dr, 7 * i + k);
         diode_setup(p, o);
@@ -329,10 +332,11 @@ __global__ void __launch_bounds__(kTileThreads) k_prep(TileMap m, const double* 
 // per-solve bookkeeping.
 __global__ void __launch_bounds__(kTileThreads) k_seed(TileMap m, int cold, LaneState* st) {
     TileCtx c = tile_ctx(m);
+    const uint32_t nw = c.nw;
     if (!c.valid) return;
     const GroupDev& d = *c.d;
     const uint32_t ninst = n_instances(d);
-    for (uint32_t t = c.warp; t < ninst; t += kWarps) inst_seed(d, c.l, t, cold, d.x);
+    for (uint32_t t = c.warp; t < ninst; t += nw) inst_seed(d, c.l, t, cold, d.x);
     if (c.warp == 0) {
         LaneState& s = st[d.lane0 + c.l];
         s.fp64 = 0;
@@ -345,13 +349,14 @@ __global__ void __launch_bounds__(kTileThreads) k_seed(TileMap m, int cold, Lane
 // (ownTape's matrix).
 __global__ void __launch_bounds__(kTileThreads) k_assemble(TileMap m, int tran, double inv_dt) {
     TileCtx c = tile_ctx(m);
+    const uint32_t nw = c.nw;
     const GroupDev& d = *c.d;
     if (c.valid)
-        for (uint32_t t = c.warp; t < n_instances(d); t += kWarps) inst_eval(d, c.l, t, tran, 0.0, cell_buf(d, 0));
+        for (uint32_t t = c.warp; t < n_instances(d); t += nw) inst_eval(d, c.l, t, tran, 0.0, cell_buf(d, 0));
     __syncthreads();
     Companion cp{inv_dt > 0.0 ? 1 : 0, 0, inv_dt, 1.0};
     if (c.valid)
-        for (uint32_t p = c.warp; p < d.nnz; p += kWarps) gather_slot(d, c.l, p, cp, 0.0, cell_buf(d, 0));
+        for (uint32_t p = c.warp; p < d.nnz; p += nw) gather_slot(d, c.l, p, cp, 0.0, cell_buf(d, 0));
 }
 
 // ---------------------------------------------------------------------------
@@ -443,24 +448,25 @@ __device__ void step_bound_part(const GroupDev& d, uint32_t l, uint32_t rot, uin
 // the first step (tran.zig:688-699 under LTE control), breakpoints.
 __global__ void __launch_bounds__(kTileThreads) k_tran_init(TileMap m, TranParams o, LaneState* st) {
     TileCtx c = tile_ctx(m);
+    const uint32_t nw = c.nw;
     const GroupDev& d = *c.d;
     const uint32_t P = d.P, l = c.l;
     const uint32_t ninst = n_instances(d);
     if (c.valid)
-        for (uint32_t t = c.warp; t < ninst; t += kWarps) {
+        for (uint32_t t = c.warp; t < ninst; t += nw) {
             inst_seed(d, l, t, 0, d.x);
             inst_eval(d, l, t, 1, 0.0, cell_buf(d, 0));
         }
     __syncthreads();
     if (!c.valid) return;
-    for (uint32_t i = c.warp; i < d.n; i += kWarps) {
+    for (uint32_t i = c.warp; i < d.n; i += nw) {
         gather_charge_row(d, l, i, cell_buf(d, 0));
         LM(d.cur, i) = LM(d.x, i);
         LM(d.prev, i) = LM(d.x, i);
         LM(d.q1, i) = LM(d.qrow, i);
         LM(d.ip, i) = 0.0;
     }
-    for (uint32_t j = c.warp; j < d.n_sites; j += kWarps) {
+    for (uint32_t j = c.warp; j < d.n_sites; j += nw) {
         double q = LM(cell_buf(d, 0), d.site_cell[j]);
         for (uint32_t k = 0; k < 4; k++) LM(d.sring + (size_t)k * d.n_sites * P, j) = q;
         LM(d.sip, j) = 0.0;
@@ -501,13 +507,14 @@ __global__ void __launch_bounds__(kTileThreads) k_tran_init(TileMap m, TranParam
 // predictor, the limiter pass, Newton with the companion rows, stepEndA
 // (Newton and LTE rejections, order promotion), the accepted-step history
 // advance, stepEndB (breakpoints, next dt) and the period measure.
-template <bool MIXED>
-__global__ void __launch_bounds__(kTileThreads, 4) k_tran(TileMap m, TranParams o, NewtonParams no, LaneState* st) {
+template <bool MIXED, bool WIDE>
+__global__ void __launch_bounds__(WIDE ? kWideThreads : kTileThreads, WIDE ? 1 : 4)
+    k_tran(TileMap m, TranParams o, NewtonParams no, LaneState* st) {
     __shared__ TileShared sh;
     TileCtx c = tile_ctx(m);
     c.d = stage_template(*c.d, sh.gd, g_dsm, MIXED);
     const GroupDev& d = *c.d;
-    const uint32_t P = d.P, l = c.l, lane = c.lane, warp = c.warp;
+    const uint32_t P = d.P, l = c.l, lane = c.lane, warp = c.warp, nw = c.nw;
     const uint32_t ns = d.n_sites, ninst = n_instances(d);
     LaneState* s = (warp == 0 && c.valid) ? &st[d.lane0 + l] : nullptr;
     unsigned char* dsm = g_dsm;
@@ -541,7 +548,7 @@ __global__ void __launch_bounds__(kTileThreads, 4) k_tran(TileMap m, TranParams 
         if (!__syncthreads_or(on)) break;
         if (on) {
             double xf = sh.xfact[lane];
-            for (uint32_t i = warp; i < d.n; i += kWarps) {
+            for (uint32_t i = warp; i < d.n; i += nw) {
                 double cu = LM(d.cur, i);
                 LM(d.x, i) = o.predictor == 1 ? cu + xf * (cu - LM(d.prev, i)) : cu;
             }
@@ -551,7 +558,7 @@ __global__ void __launch_bounds__(kTileThreads, 4) k_tran(TileMap m, TranParams 
         // predicted iterate and evaluates the instances there (the instance
         // phase of Newton's iteration 0, into cells buffer 0).
         if (on)
-            for (uint32_t t = warp; t < ninst; t += kWarps) {
+            for (uint32_t t = warp; t < ninst; t += nw) {
                 inst_seed(d, l, t, 0, d.cur);
                 inst_limit_eval(d, l, t, 1, sh.t[lane], cell_buf(d, 0));
             }
@@ -568,7 +575,7 @@ __global__ void __launch_bounds__(kTileThreads, 4) k_tran(TileMap m, TranParams 
         if (conv) {
             double* r0 = ring_slot(d, sh.rot[lane], 0);
             const double* cb = cell_buf(d, sh.cbuf[lane]);
-            for (uint32_t j = warp; j < ns; j += kWarps) LM(r0, j) = LM(cb, d.site_cell[j]);
+            for (uint32_t j = warp; j < ns; j += nw) LM(r0, j) = LM(cb, d.site_cell[j]);
         }
         __syncthreads();
         // The LTE bound of a converged LTE-controlled step, its sites split
@@ -582,7 +589,7 @@ __global__ void __launch_bounds__(kTileThreads, 4) k_tran(TileMap m, TranParams 
                     uint32_t method = sh.method[lane];
                     step_bound_part(d, l, ls.s_rot, method, o.method, method == 0, method, ls.dt, ls.dt_old0,
                                     ls.dt_old1, o.reltol, o.abstol, o.chgtol, o.trtol, sh.ag0[lane], sh.ag1[lane],
-                                    warp, kWarps, v0, v1, b0, b1);
+                                    warp, nw, v0, v1, b0, b1);
                 }
             }
             // the bounds are >= 0 (NaN ones only poison): their bits order as they do
@@ -656,7 +663,7 @@ __global__ void __launch_bounds__(kTileThreads, 4) k_tran(TileMap m, TranParams 
         if (acc) {
             double ag0 = sh.ag0[lane], ag1 = sh.ag1[lane];
             uint32_t method = sh.method[lane];
-            for (uint32_t i = warp; i < d.n; i += kWarps) {
+            for (uint32_t i = warp; i < d.n; i += nw) {
                 double dq = ag0 * (LM(d.qrow, i) - LM(d.q1, i));
                 LM(d.ip, i) = method == 1 ? dq - ag1 * LM(d.ip, i) : dq;
                 LM(d.q1, i) = LM(d.qrow, i);
@@ -665,7 +672,7 @@ __global__ void __launch_bounds__(kTileThreads, 4) k_tran(TileMap m, TranParams 
             }
             const double* q0 = ring_slot(d, sh.rot[lane], 0);
             const double* q1 = ring_slot(d, sh.rot[lane], 1);
-            for (uint32_t j = warp; j < ns; j += kWarps) {
+            for (uint32_t j = warp; j < ns; j += nw) {
                 double dq = ag0 * (LM(q0, j) - LM(q1, j));
                 LM(d.sip, j) = method == 1 ? dq - ag1 * LM(d.sip, j) : dq;
             }

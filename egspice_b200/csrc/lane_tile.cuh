@@ -19,6 +19,10 @@ namespace espl {
 
 constexpr int kWarps = 4;
 constexpr int kTileThreads = kWarps * 32;
+// Tiles of large templates (the banded replay's) run 16 warps: their
+// instance, gather and update phases split over four times the threads.
+constexpr int kWideWarps = 16;
+constexpr int kWideThreads = kWideWarps * 32;
 constexpr uint32_t kNeg = 0x80000000u;
 
 // Cells per instance.
@@ -34,7 +38,8 @@ struct TileCtx {
     uint32_t tile;   // tile index over all templates
     uint32_t l;      // lane in the template
     uint32_t lane;   // 0..31
-    uint32_t warp;   // 0..kWarps-1
+    uint32_t warp;   // 0..nw-1
+    uint32_t nw;     // warps of the CTA (kWarps, or kWideWarps for large templates)
     bool valid;      // l < lanes
 };
 
