@@ -531,7 +531,6 @@ espl_status plan_classes(espl_lanes* h) {
         g.dev.refine_rows = MIXED && h->refine_sweeps > 0 ? 1u : 0u;
         g.dev.stage_mode = kStageNone;
         bytes[i] = 0;
-        const uint32_t band = g.dev.band_ok;
         bool placed = false;
         for (uint32_t mode : {kStageLu, kStageIndex, kStageNone}) {
             SmemPlan sp = smem_plan(g.dev, mode, MIXED);
@@ -543,14 +542,13 @@ espl_status plan_classes(espl_lanes* h) {
                 break;
             }
         }
-        if (!placed && band) {
-            // not even the band buffers fit: the global replay
+        if (!placed) {
+            // not even the banded replay's buffers fit: the global replay
             g.dev.band_ok = 0;
             g.dev.stage_mode = kStageNone;
             bytes[i] = 0;
         }
         if (g.dev.stage_mode == kStageLu) g.dev.band_ok = 0;
-        (void)band;
         wide[i] = g.dev.band_ok != 0;
         int a = 0, b = 0;
         if (wide[i]) {

@@ -1,7 +1,7 @@
 // The banded streaming replay for templates too large for the shared-memory
 // LU chain whose elimination stays within a narrow band of the pivot order
-// (an RC ladder's walks its chain: every column k touches only rows
-// k - band .. k + band). The work vector lives in a ring of band_w rows and
+// (an RC ladder's elimination walks its chain: every column k touches only
+// rows k - band .. k + band). The work vector lives in a ring of band_w rows and
 // the recently produced L entries (the only ones a later axpy reads) in a
 // ring of band_l slots, both in shared memory, so the dependent chain of the
 // replay touches only shared memory. The replay program and the scattered A
@@ -17,11 +17,6 @@
 #include "lane_smem.cuh"
 
 namespace espl {
-
-// Shared-memory bytes of the band buffers of a template.
-__host__ __device__ inline uint32_t band_bytes(uint32_t words, uint32_t entries, uint32_t w_ring, uint32_t l_ring) {
-    return 2u * words * 4u + 2u * entries * 32u * 8u + (w_ring + l_ring) * 32u * 8u;
-}
 
 // Streams count values into dst with warps 1-3 (thread t of nt), eight per
 // thread in flight: all eight sources are loaded before any is stored, so

@@ -258,46 +258,6 @@ __device__ __forceinline__ bool inst_limit_eval(const GroupDev& d, uint32_t l, u
     return (vgs != cgs) | (vds != cds) | (vbs != cbs);
 }
 
-// The limiter pass of instance t with snapLimited (eval.zig:1115-1171):
-// true when it clamped.
-__device__ __forceinline__ bool inst_limit(const GroupDev& d, uint32_t l, uint32_t t) {
-    const uint32_t P = d.P;
-    const double* x = d.x;
-    const double eps16 = 16 * 2.220446049250313e-16;
-    uint32_t base = d.n_res + d.n_cap + d.n_vsrc + d.n_isrc;
-    if (t < base) return false;
-    uint32_t i = t - base;
-    if (i < d.n_dio) {
-        double xa = LM(x, d.dio_t[2 * i]), xc = LM(x, d.dio_t[2 * i + 1]);
-        double vd = xa - xc;
-        uint32_t b = DiodePrep::count * i;
-        double v = pnjlim(vd, LM(d.lim_dio, i), LM(d.dio_d, b + DiodePrep::vte), LM(d.dio_d, b + DiodePrep::vcrit));
-        if (fabs(v - vd) <= eps16 * fmax(fabs(xa), fabs(xc))) v = vd;
-        LM(d.lim_dio, i) = v;
-        return v != vd;
-    }
-    i -= d.n_dio;
-    if (i >= d.n_mos) return false;
-    const uint32_t* tmv = d.mos_t + 4 * i;
-    uint32_t b = Mos1Prep::count * i;
-    const double* md = d.mos_d;
-    double ty = LM(md, b + Mos1Prep::type);
-    double xd = LM(x, tmv[0]), xg = LM(x, tmv[1]), xs = LM(x, tmv[2]), xb = LM(x, tmv[3]);
-    double cgs = ty * (xg - xs), cds = ty * (xd - xs), cbs = ty * (xb - xs);
-    double vgs = cgs, vds = cds, vbs = cbs;
-    mos1_limit(LM(md, b + Mos1Prep::vt), LM(md, b + Mos1Prep::gamma), LM(md, b + Mos1Prep::phit),
-               LM(md, b + Mos1Prep::von0), LM(md, b + Mos1Prep::vcrit), LM(d.lim_mos, 3 * i),
-               LM(d.lim_mos, 3 * i + 1), LM(d.lim_mos, 3 * i + 2), vgs, vds, vbs);
-    double tol = eps16 * fmax(fmax(fabs(xd), fabs(xg)), fmax(fabs(xs), fabs(xb)));
-    if (fabs(vgs - cgs) <= tol) vgs = cgs;
-    if (fabs(vds - cds) <= tol) vds = cds;
-    if (fabs(vbs - cbs) <= tol) vbs = cbs;
-    LM(d.lim_mos, 3 * i) = vgs;
-    LM(d.lim_mos, 3 * i + 1) = vds;
-    LM(d.lim_mos, 3 * i + 2) = vbs;
-    return (vgs != cgs) | (vds != cds) | (vbs != cbs);
-}
-
 __device__ __forceinline__ double gather_sum(const double* __restrict__ cells, uint32_t P, uint32_t l,
                                              const uint32_t* __restrict__ ptr, const uint32_t* __restrict__ list,
                                              uint32_t k) {
