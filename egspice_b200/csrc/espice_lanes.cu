@@ -96,6 +96,7 @@ struct Group {
     };
     std::vector<BatchRec> batch_order;
     uint32_t tile0 = 0;
+    uint32_t n_prog = 0;  // words of the uploaded replay program (0: none)
 };
 
 }  // namespace
@@ -469,7 +470,9 @@ espl_status alloc_group(espl_lanes* h, Group& g) {
     AL(corr, n1 * P);
     AL(udiag, n1 * P);
     AL(udiag32, n1 * P);
-    if (g.n <= kDensePeelMax) {
+    // the dense peel's scratch, where the template's lanes need at most 4 GB
+    // of it (past that a failed lane reports singular)
+    if (g.n <= kDensePeelMax && (double)peel_doubles(g.n) * 8.0 * (double)P <= 4.0e9) {
         AL(peel_m, (size_t)peel_doubles(g.n) * P);
         AL(peel_i, (size_t)peel_words(g.n) * P);
     }
@@ -526,9 +529,22 @@ espl_status plan_classes(espl_lanes* h) {
     free_classes(h);
     std::vector<uint32_t> bytes(h->groups.size(), 0), per(h->groups.size(), 0);
     std::vector<bool> wide(h->groups.size(), false);
+    auto tiles_per_sm = [&](bool w, uint32_t smem, int& per_sm) -> espl_status {
+        int a = 0, b = 0;
+        if (w) {
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_tran<MIXED, true>, kWideThreads, smem));
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_static<MIXED, true>, kWideThreads, smem));
+        } else {
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_tran<MIXED, false>, kBlock, smem));
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_static<MIXED, false>, kBlock, smem));
+        }
+        per_sm = std::max(1, std::min(a, b));
+        return ESPL_OK;
+    };
     for (size_t i = 0; i < h->groups.size(); i++) {
         Group& g = h->groups[i];
         g.dev.refine_rows = MIXED && h->refine_sweeps > 0 ? 1u : 0u;
+        g.dev.n_prog = g.n_prog;
         g.dev.stage_mode = kStageNone;
         bytes[i] = 0;
         bool placed = false;
@@ -550,15 +566,25 @@ espl_status plan_classes(espl_lanes* h) {
         }
         if (g.dev.stage_mode == kStageLu) g.dev.band_ok = 0;
         wide[i] = g.dev.band_ok != 0;
-        int a = 0, b = 0;
-        if (wide[i]) {
-            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_tran<MIXED, true>, kWideThreads, bytes[i]));
-            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_static<MIXED, true>, kWideThreads, bytes[i]));
-        } else {
-            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_tran<MIXED, false>, kBlock, bytes[i]));
-            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_static<MIXED, false>, kBlock, bytes[i]));
+        int t = 0;
+        espl_status s;
+        if ((s = tiles_per_sm(wide[i], bytes[i], t))) return s;
+        if (g.dev.stage_mode == kStageLu && g.dev.n_prog) {
+            // The staged program replaces the tape's column pointers, scatter
+            // rows and flags but costs its own words; where that drops a
+            // resident tile per SM the tile replays from the tape instead.
+            GroupDev bare = g.dev;
+            bare.n_prog = 0;
+            SmemPlan sp = smem_plan(bare, kStageLu, MIXED);
+            int tb = 0;
+            if ((s = tiles_per_sm(false, sp.bytes, tb))) return s;
+            if (tb > t) {
+                g.dev.n_prog = 0;
+                bytes[i] = sp.bytes;
+                t = tb;
+            }
         }
-        per[i] = (uint32_t)std::max(1, std::min(a, b));
+        per[i] = (uint32_t)t;
     }
     // classes by (tile width, resident tiles per SM), the one with the most
     // tiles first
@@ -638,6 +664,7 @@ espl_status retape(espl_lanes* h, int tran, double dt) {
             std::vector<uint32_t> prog;
             d.n_prog = lu_program(g.tape, g.col_ptr.data(), prog) ? (uint32_t)prog.size() : 0u;
             if (d.n_prog) UP(lu_prog, prog);
+            g.n_prog = d.n_prog;
             // the banded streaming replay, for templates the shared LU chain
             // cannot hold (plan_classes decides which run it)
             BandPlan bp;

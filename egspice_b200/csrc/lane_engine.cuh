@@ -28,7 +28,11 @@ namespace espl {
 constexpr uint32_t kTrashNone = 0xFFFFFFFFu;
 constexpr double kXPlausible = 1e9;    // converger.x_plausible
 constexpr double kWide = 1.0 / 1e-3;   // LaneTab.wide = 1 / pivot_tol
-constexpr uint32_t kDensePeelMax = 64; // kernels/lane.zig:301
+// Lanes of templates up to this size whose replay fails re-pivot densely on
+// the device. The reference stops at 64 unknowns (kernels/lane.zig:301) and
+// hands larger failed lanes to the host factor; with no host path here the
+// dense peel covers up to 256, within a scratch budget (alloc_group).
+constexpr uint32_t kDensePeelMax = 256;
 
 // Gate bits (kernels/lane.zig:708-711).
 constexpr uint32_t kActive = 1, kInitFix = 2, kConverged = 4, kSingular = 8, kPassed = 16, kParked = 32;
@@ -55,8 +59,8 @@ struct GroupDev {
     float *lx32, *ux32, *udiag32, *w32, *y32;
     double *q1, *ip, *cur, *prev, *sring, *sip;
     double *rr, *corr;
-    double* peel_m;      // n <= 64: the lanes' dense peel scratch (peel_doubles(n) per lane)
-    uint32_t* peel_i;    // n <= 64: its index words (peel_words(n) per lane)
+    double* peel_m;      // n <= kDensePeelMax: the lanes' dense peel scratch (peel_doubles(n) per lane)
+    uint32_t* peel_i;    // n <= kDensePeelMax: its index words (peel_words(n) per lane)
     // Stamp plan: per-instance output cells (lane-major) and, per Jacobian
     // slot and residual/charge row, the cells that sum into it in the
     // reference's stamping order (bit 31: the cell enters negated).
@@ -391,7 +395,7 @@ __device__ void refine_mixed(const GroupDev& d, uint32_t l) {
 // plain partial-pivoting LU with an eps^2 floor (kernels/lane.zig:310-350)
 // that refuses the ill-conditioned iterates a cold operating point passes
 // through; the host factor accepts them.
-// The peel scratch of a template of n <= 64, per lane, lane-interleaved
+// The peel scratch of a template of n <= kDensePeelMax, per lane, lane-interleaved
 // like every other per-lane array (element i of lane l at i * P + l):
 // m[n * n] row-major, xv[n] (right-hand side, then the solution by unknown),
 // rscale[n], sol[n] as doubles; want, want_of, pinv, row_of[n] as u32.
@@ -463,7 +467,7 @@ __device__ bool dense_repivot_neg(uint32_t n, const uint32_t* q, double* pm, uin
     return true;
 }
 
-// A failed replay of a lane with n <= 64 solves densely in the lane's own
+// A failed replay of a lane with n <= kDensePeelMax solves densely in the lane's own
 // peel scratch (the place of arp_lane_peel_dense, lane_device.zig:120-147),
 // re-pivoting as the host factor would; dx gets the step.
 __device__ bool peel_dense(const GroupDev& d, uint32_t l, LaneState& s) {

@@ -86,6 +86,9 @@ __host__ __device__ inline uint32_t pad4(uint32_t words) { return (words + 3u) &
 
 __host__ __device__ inline uint32_t stage_words(const GroupDev& d, int k, uint32_t mode) {
     const bool rows = d.refine_rows != 0;
+    // a tile replaying from the staged program reads neither the tape's
+    // column pointers, scatter rows nor flags
+    const bool by_prog = mode == kStageLu && d.n_prog != 0;
     switch (k) {
     case S_DIAG: return d.n;
     case S_VOID: return d.n_void;
@@ -107,13 +110,13 @@ __host__ __device__ inline uint32_t stage_words(const GroupDev& d, int k, uint32
     case S_SITE: return d.n_sites;
     case S_Q: return d.n;
     case S_PINV: return d.n;
-    case S_COLPTR: return d.n + 1;
-    case S_PROW: return d.nnz;
+    case S_COLPTR: return by_prog ? 0u : d.n + 1;
+    case S_PROW: return by_prog ? 0u : d.nnz;
     case S_UP: return d.n + 1;
     case S_UI: return d.nnz_u;
     case S_LP: return d.n + 1;
     case S_LI: return d.nnz_l;
-    case S_FLAGS: return d.n;
+    case S_FLAGS: return by_prog ? 0u : d.n;
     case S_RTPTR: return rows ? d.n + 1 : 0u;
     case S_RTCOL: return rows ? d.nnz : 0u;
     case S_RTPOS: return rows ? d.nnz : 0u;
