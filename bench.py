@@ -230,10 +230,17 @@ def run_ring_sweep(nets, topts, precision, steps_per_launch=5000):
     L.init_steps(topts)
     dev_ms = L.stats().newton_ms
     calls = 0
+    classes = None
     while True:
         reps = L.device_launch(steps_per_launch)
         calls += 1
         dev_ms += L.stats().newton_ms
+        cl = L.classes()
+        if classes is None:
+            classes = cl
+        else:
+            for a, b in zip(classes, cl):
+                a["ms"] += b["ms"]
         if all(r.status != 0 for r in reps) or calls > 1000:
             break
     launches = L.stats().launches  # Newton kernels: one per launch class per call
@@ -245,7 +252,7 @@ def run_ring_sweep(nets, topts, precision, steps_per_launch=5000):
         t = L.tape(i)
         tapes.append((net, len(t["li"]), len(t["ui"])))
     L.close()
-    return dev_ms, wall, xs, reps, tapes, launches, periods
+    return dev_ms, wall, xs, reps, tapes, launches, periods, classes
 
 
 def opamp_nominal(net):
@@ -426,7 +433,7 @@ def main():
         with ClockSampler(dev) as clk:
             for _ in range(args.steps):
                 barrier()
-                d, w, xs, reps, tapes, launches, periods = run_ring_sweep(nets, topts, prec)
+                d, w, xs, reps, tapes, launches, periods, classes = run_ring_sweep(nets, topts, prec)
                 barrier()
                 dev_ms.append(d)
                 walls.append(w)
@@ -438,7 +445,7 @@ def main():
             dmax, wmax = float(t[0]), float(t[1])
         results[prec] = dict(dev_s=dmax, wall_s=wmax, xs=xs, reps=reps, tapes=tapes, clocks=clk.summary(),
                              iters=sum(r.nr_iters for r in reps), rejects=sum(r.rejects for r in reps),
-                             launches=launches, periods=periods)
+                             launches=launches, periods=periods, classes=classes)
 
     best = results.get("mixed") or results["fp64"]
     plain = results.get("fp64")
@@ -472,7 +479,9 @@ def main():
             {m: {"points_per_s": points_all / results[m]["dev_s"], "ms_per_sweep": results[m]["dev_s"] * 1e3,
                  "newton_iters": results[m]["iters"], "rejects": results[m]["rejects"],
                  "period_err_over_tol": err.get(m, (None,))[0],
-                 "final_x_err_over_tol": err.get(m, (None, None))[1]} for m in modes},
+                 "final_x_err_over_tol": err.get(m, (None, None))[1],
+                 "launch_classes": [[c["tiles"], int(c["wide"]), c["per_sm"], round(c["ms"], 1)]
+                                    for c in results[m]["classes"]]} for m in modes},
             mixed_over_fp64=(plain["dev_s"] / best["dev_s"]) if (plain and "mixed" in results) else None,
             learned=False),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,

@@ -59,6 +59,11 @@ class Stats(C.Structure):
                 ("peel_overflow", C.c_uint32)]
 
 
+class ClassInfo(C.Structure):
+    _fields_ = [("tiles", C.c_uint32), ("wide", C.c_uint32), ("per_sm", C.c_uint32), ("smem_bytes", C.c_uint32),
+                ("last_ms", C.c_double)]
+
+
 class OrcNewtonResult(C.Structure):
     _fields_ = [("converged", C.c_uint32), ("singular", C.c_uint32), ("iterations", C.c_uint32),
                 ("reserved", C.c_uint32)]

@@ -30,10 +30,11 @@ constexpr uint32_t kBandMax = 15, kBandLRing = 64, kBandWords = 1024, kBandEntri
 struct LaunchClass {
     uint32_t smem = 0;        // dynamic shared memory per tile
     uint32_t per_sm = 0;      // resident tiles per SM at that size
-    bool wide = false;        // kWideWarps per tile (the banded replay's templates)
+    bool wide = false;        // kWideWarps per tile (banded templates; the largest others while the rest fit)
     std::vector<uint32_t> tiles;
     uint32_t* d_tiles = nullptr;
-    cudaStream_t stream = nullptr;  // null: the handle's stream
+    cudaStream_t stream = nullptr;  // null: the handle's stream (a single class)
+    cudaEvent_t t0 = nullptr, t1 = nullptr;  // around the class's last launch
     cudaEvent_t done = nullptr;
 };
 constexpr uint32_t kGround = ESPL_GROUND;
@@ -96,7 +97,7 @@ struct Group {
     };
     std::vector<BatchRec> batch_order;
     uint32_t tile0 = 0;
-    uint32_t n_prog = 0;  // words of the uploaded replay program (0: none)
+    uint32_t n_rec = 0;  // words of the uploaded replay records (0: none)
 };
 
 }  // namespace
@@ -380,19 +381,59 @@ espl_status alloc_group(espl_lanes* h, Group& g) {
         d.c_pin = pl.c_pin;
         d.c_const = pl.c_const;
         if (pl.sites.size() != d.n_sites) return fail(h, ESPL_INVALID_ARGUMENT, "site count mismatch");
-        std::vector<uint32_t> ptr, flat;
-        csr(pl.g, ptr, flat);
-        d.n_gc = (uint32_t)flat.size();
-        if ((s = dupload(h, own, &d.g_ptr, ptr)) || (s = dupload(h, own, &d.g_cell, flat))) return s;
-        csr(pl.c, ptr, flat);
-        d.n_cc = (uint32_t)flat.size();
-        if ((s = dupload(h, own, &d.c_ptr, ptr)) || (s = dupload(h, own, &d.c_cell, flat))) return s;
-        csr(pl.r, ptr, flat);
-        d.n_rc = (uint32_t)flat.size();
-        if ((s = dupload(h, own, &d.r_ptr, ptr)) || (s = dupload(h, own, &d.r_cell, flat))) return s;
-        csr(pl.q, ptr, flat);
-        d.n_qc = (uint32_t)flat.size();
-        if ((s = dupload(h, own, &d.q_ptr, ptr)) || (s = dupload(h, own, &d.q_cell, flat))) return s;
+        std::vector<uint32_t> gp, gf, cp, cf, rp, rf, qp, qf;
+        csr(pl.g, gp, gf);
+        d.n_gc = (uint32_t)gf.size();
+        if ((s = dupload(h, own, &d.g_ptr, gp)) || (s = dupload(h, own, &d.g_cell, gf))) return s;
+        csr(pl.c, cp, cf);
+        d.n_cc = (uint32_t)cf.size();
+        if ((s = dupload(h, own, &d.c_ptr, cp)) || (s = dupload(h, own, &d.c_cell, cf))) return s;
+        csr(pl.r, rp, rf);
+        d.n_rc = (uint32_t)rf.size();
+        if ((s = dupload(h, own, &d.r_ptr, rp)) || (s = dupload(h, own, &d.r_cell, rf))) return s;
+        csr(pl.q, qp, qf);
+        d.n_qc = (uint32_t)qf.size();
+        if ((s = dupload(h, own, &d.q_ptr, qp)) || (s = dupload(h, own, &d.q_cell, qf))) return s;
+        if (pl.n_cells > kGiIdx) return fail(h, ESPL_TOO_LARGE, "more stamp cells than the gather list can index");
+        {
+            std::vector<uint32_t> ip, ie;
+            auto put = [&](const std::vector<uint32_t>& ptr, const std::vector<uint32_t>& flat, uint32_t k,
+                           uint32_t kind) {
+                for (uint32_t e = ptr[k]; e < ptr[k + 1]; e++)
+                    ie.push_back((flat[e] & kNeg) | (kind << kGiKindShift) | (flat[e] & ~kNeg));
+            };
+            ip.push_back(0);
+            for (uint32_t p = 0; p < g.nnz; p++) {
+                put(gp, gf, p, kGiCell);
+                put(cp, cf, p, kGiCellC);
+                if (ie.size() == ip.back()) ie.push_back(kGiNop << kGiKindShift);
+                ip.push_back((uint32_t)ie.size());
+            }
+            for (uint32_t i = 0; i < g.n; i++) {
+                put(rp, rf, i, kGiCell);
+                put(qp, qf, i, kGiCellC);
+                ie.push_back((kGiQ1 << kGiKindShift) | i);
+                ie.push_back((kGiIp << kGiKindShift) | i);
+                ie.push_back((kGiX << kGiKindShift) | i);
+                ip.push_back((uint32_t)ie.size());
+            }
+            d.n_items = g.nnz + g.n;
+            d.n_gi = (uint32_t)ie.size();
+            // runs of items with about the same number of entries per warp
+            auto split = [&](uint32_t nw, uint32_t* out) {
+                uint32_t k = 0;
+                out[0] = 0;
+                for (uint32_t w = 1; w < nw; w++) {
+                    const uint64_t target = (uint64_t)d.n_gi * w / nw;
+                    while (k < d.n_items && ip[k] < target) k++;
+                    out[w] = k;
+                }
+                out[nw] = d.n_items;
+            };
+            split(4, d.gsplit4);
+            split(16, d.gsplit16);
+            if ((s = dupload(h, own, &d.gi_ptr, ip)) || (s = dupload(h, own, &d.gi_ent, ie))) return s;
+        }
         if ((s = dupload(h, own, &d.site_cell, pl.sites))) return s;
         if ((s = dupload(h, own, &d.slot_diag, pl.slot_diag))) return s;
         // two cells buffers: an iteration's instance phase and the next one's
@@ -483,22 +524,25 @@ espl_status alloc_group(espl_lanes* h, Group& g) {
 TileMap launch_map(espl_lanes* h) { return TileMap{h->d_groups, h->d_warp_group, nullptr, h->n_warps}; }
 uint32_t grid_of(espl_lanes* h) { return h->n_warps; }
 
-// Launches `fn(map, grid, smem, stream)` once per class, the classes after
-// the first on their own streams, forked from and joined back into the
-// handle's stream.
+// Launches `fn(map, grid, smem, stream)` once per class: a single class on
+// the handle's stream, several each on its own stream, forked from and
+// joined back into the handle's stream.
 template <typename F>
 espl_status launch_classes(espl_lanes* h, F fn) {
     CK(cudaEventRecord(h->fork, h->stream));
     for (size_t k = 0; k < h->classes.size(); k++) {
         LaunchClass& c = h->classes[k];
-        cudaStream_t st = k == 0 ? h->stream : c.stream;
-        if (k) CK(cudaStreamWaitEvent(st, h->fork, 0));
+        cudaStream_t st = c.stream ? c.stream : h->stream;
+        if (c.stream) CK(cudaStreamWaitEvent(st, h->fork, 0));
         TileMap m{h->d_groups, h->d_warp_group, c.d_tiles, (uint32_t)c.tiles.size()};
+        CK(cudaEventRecord(c.t0, st));
         fn(m, (uint32_t)c.tiles.size(), c.smem, st, c.wide);
         CK(cudaGetLastError());
-        if (k) CK(cudaEventRecord(c.done, st));
+        CK(cudaEventRecord(c.t1, st));
+        if (c.stream) CK(cudaEventRecord(c.done, st));
     }
-    for (size_t k = 1; k < h->classes.size(); k++) CK(cudaStreamWaitEvent(h->stream, h->classes[k].done, 0));
+    for (auto& c : h->classes)
+        if (c.stream) CK(cudaStreamWaitEvent(h->stream, c.done, 0));
     return ESPL_OK;
 }
 
@@ -507,6 +551,8 @@ void free_classes(espl_lanes* h) {
         cudaFree(c.d_tiles);
         if (c.stream) cudaStreamDestroy(c.stream);
         if (c.done) cudaEventDestroy(c.done);
+        if (c.t0) cudaEventDestroy(c.t0);
+        if (c.t1) cudaEventDestroy(c.t1);
     }
     h->classes.clear();
 }
@@ -544,7 +590,8 @@ espl_status plan_classes(espl_lanes* h) {
     for (size_t i = 0; i < h->groups.size(); i++) {
         Group& g = h->groups[i];
         g.dev.refine_rows = MIXED && h->refine_sweeps > 0 ? 1u : 0u;
-        g.dev.n_prog = g.n_prog;
+        g.dev.n_rec = g.n_rec;
+        g.dev.rec_stage = g.n_rec ? 1u : 0u;
         g.dev.stage_mode = kStageNone;
         bytes[i] = 0;
         bool placed = false;
@@ -569,22 +616,64 @@ espl_status plan_classes(espl_lanes* h) {
         int t = 0;
         espl_status s;
         if ((s = tiles_per_sm(wide[i], bytes[i], t))) return s;
-        if (g.dev.stage_mode == kStageLu && g.dev.n_prog) {
-            // The staged program replaces the tape's column pointers, scatter
-            // rows and flags but costs its own words; where that drops a
-            // resident tile per SM the tile replays from the tape instead.
+        if (g.dev.stage_mode == kStageLu && g.dev.n_rec) {
+            // Staged records cost their own words of shared memory; where
+            // that drops a resident tile per SM they stay in global memory
+            // (read through L1, one record ahead).
             GroupDev bare = g.dev;
-            bare.n_prog = 0;
+            bare.rec_stage = 0;
             SmemPlan sp = smem_plan(bare, kStageLu, MIXED);
             int tb = 0;
             if ((s = tiles_per_sm(false, sp.bytes, tb))) return s;
             if (tb > t) {
-                g.dev.n_prog = 0;
+                g.dev.rec_stage = 0;
                 bytes[i] = sp.bytes;
                 t = tb;
             }
         }
         per[i] = (uint32_t)t;
+    }
+    // Wide tiles (kWideWarps, one per SM) for the largest templates, as long
+    // as the narrow tiles still fit the remaining SMs in one wave. A wide
+    // tile splits its instance, gather and update phases over four times
+    // the warps and has its SM to itself, so templates whose few tiles would
+    // otherwise set the launch's length (large variants beside a bulk of
+    // small lanes, or lanes that leave SMs idle) finish sooner; the LU chain
+    // stays on warp 0 either way.
+    {
+        int sms = 0;
+        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        double narrow_sms = 0.0;
+        uint32_t wide_tiles = 0;
+        std::vector<size_t> order;
+        for (size_t i = 0; i < h->groups.size(); i++) {
+            const uint32_t tiles = h->groups[i].P / 32;
+            if (wide[i]) {
+                wide_tiles += tiles;
+            } else {
+                narrow_sms += (double)tiles / per[i];
+                order.push_back(i);
+            }
+        }
+        auto work = [&](size_t i) {
+            const GroupDev& d = h->groups[i].dev;
+            return (double)d.nnz + d.nnz_l + d.nnz_u + d.n_res + d.n_cap + d.n_vsrc + d.n_isrc + d.n_dio + d.n_mos;
+        };
+        std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return work(a) > work(b); });
+        for (size_t i : order) {
+            const uint32_t tiles = h->groups[i].P / 32;
+            const double rest = narrow_sms - (double)tiles / per[i];
+            // one SM of slack: tiles of different sizes do not pack an SM
+            // as tightly as the count of SMs by occupancy assumes
+            if (wide_tiles + tiles + (uint32_t)std::ceil(rest - 1e-9) + 1 > (uint32_t)sms) continue;
+            int t = 0;
+            espl_status s;
+            if ((s = tiles_per_sm(true, bytes[i], t))) return s;
+            wide[i] = true;
+            per[i] = (uint32_t)t;
+            wide_tiles += tiles;
+            narrow_sms = rest;
+        }
     }
     // classes by (tile width, resident tiles per SM), the one with the most
     // tiles first
@@ -603,15 +692,29 @@ espl_status plan_classes(espl_lanes* h) {
         }
         h->classes.push_back(std::move(c));
     }
-    std::stable_sort(h->classes.begin(), h->classes.end(),
-                     [](const LaunchClass& a, const LaunchClass& b) { return a.tiles.size() > b.tiles.size(); });
+    // wide classes first, so that their tiles take SMs of their own; then
+    // the narrow classes by resident tiles per SM, the larger tiles first,
+    // so that the most numerous small tiles fill the slots that are left
+    std::stable_sort(h->classes.begin(), h->classes.end(), [](const LaunchClass& a, const LaunchClass& b) {
+        if (a.wide != b.wide) return a.wide;
+        if (a.per_sm != b.per_sm) return a.per_sm < b.per_sm;
+        return a.tiles.size() > b.tiles.size();
+    });
     for (size_t k = 0; k < h->classes.size(); k++) {
         LaunchClass& c = h->classes[k];
         CK(cudaMalloc(&c.d_tiles, sizeof(uint32_t) * c.tiles.size()));
+        CK(cudaEventCreate(&c.t0));
+        CK(cudaEventCreate(&c.t1));
         CK(cudaMemcpyAsync(c.d_tiles, c.tiles.data(), sizeof(uint32_t) * c.tiles.size(), cudaMemcpyHostToDevice,
                            h->stream));
-        if (k) {
-            CK(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+        // With more than one class each runs on a stream of its own; all but
+        // the last (the small tiles that fill in) at the greatest priority,
+        // so that their tiles are dispatched first when both wait.
+        if (h->classes.size() > 1) {
+            int least = 0, greatest = 0;
+            CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+            const bool first = k + 1 < h->classes.size();
+            CK(cudaStreamCreateWithPriority(&c.stream, cudaStreamNonBlocking, first ? greatest : least));
             CK(cudaEventCreateWithFlags(&c.done, cudaEventDisableTiming));
         }
     }
@@ -664,7 +767,10 @@ espl_status retape(espl_lanes* h, int tran, double dt) {
             std::vector<uint32_t> prog;
             d.n_prog = lu_program(g.tape, g.col_ptr.data(), prog) ? (uint32_t)prog.size() : 0u;
             if (d.n_prog) UP(lu_prog, prog);
-            g.n_prog = d.n_prog;
+            std::vector<uint32_t> rec;
+            d.n_rec = lu_records(g.tape, g.col_ptr.data(), rec) ? (uint32_t)rec.size() : 0u;
+            if (d.n_rec) UP(lu_rec, rec);
+            g.n_rec = d.n_rec;
             // the banded streaming replay, for templates the shared LU chain
             // cannot hold (plan_classes decides which run it)
             BandPlan bp;
@@ -1062,6 +1168,26 @@ espl_status espl_get_stats(espl_lanes* h, espl_stats* out) {
     h->stats.dense_peels = (uint32_t)std::min<uint64_t>(peels, 0xFFFFFFFFu);
     h->stats.peel_overflow = 0;
     *out = h->stats;
+    return ESPL_OK;
+}
+
+espl_status espl_get_classes(espl_lanes* h, espl_class_info* out, uint32_t cap, uint32_t* count) {
+    if (!h || (!out && cap)) return ESPL_INVALID_ARGUMENT;
+    if (count) *count = (uint32_t)h->classes.size();
+    for (uint32_t k = 0; k < cap && k < h->classes.size(); k++) {
+        const LaunchClass& c = h->classes[k];
+        espl_class_info& o = out[k];
+        o.tiles = (uint32_t)c.tiles.size();
+        o.wide = c.wide ? 1u : 0u;
+        o.per_sm = c.per_sm;
+        o.smem_bytes = c.smem;
+        o.last_ms = 0.0;
+        float ms = 0.0f;
+        if (c.t1 && cudaEventQuery(c.t1) == cudaSuccess && cudaEventElapsedTime(&ms, c.t0, c.t1) == cudaSuccess)
+            o.last_ms = ms;
+        else
+            (void)cudaGetLastError();  // not launched yet: no time
+    }
     return ESPL_OK;
 }
 

@@ -46,6 +46,9 @@ struct GroupDev {
     const uint32_t *rt_ptr, *rt_col, *rt_pos;  // row view of the pattern: per row, (column, slot) by column
     const uint32_t* lu_prog;                   // the replay as a flat program (tape.h lu_program)
     uint32_t n_prog, prog_pad;
+    const uint32_t* lu_rec;                    // the replay as 16-byte records (tape.h lu_records)
+    uint32_t n_rec, rec_stage;                 // n_rec words (0: the shared chain replays from the tape);
+                                               // rec_stage: the records are staged in shared memory
     // The banded streaming replay (lane_band.cuh, tape.h BandPlan): ring
     // sizes, chunk capacities and count, the shared-memory offset of its
     // buffers, and the chunk tables and scatter slots in global memory.
@@ -69,6 +72,16 @@ struct GroupDev {
     const uint8_t* slot_diag;
     double* cells;
     uint32_t n_gc, n_cc, n_rc, n_qc;  // lengths of g_cell, c_cell, r_cell, q_cell
+    // The same sums as one flat list for the Newton gather (lane_tile.cuh
+    // gather_items): items are the nnz slots, then the n rows; an item's
+    // entries (gi_ptr[k] .. gi_ptr[k + 1]) are its G (R) cells, its C (Q)
+    // cells, and for a row the q1, ip and x values its companion and gmin
+    // terms read. Each warp of a tile takes a run of items with about the
+    // same number of entries: gsplit4 for 4-warp tiles, gsplit16 for 16.
+    const uint32_t *gi_ptr, *gi_ent;
+    uint32_t n_gi, n_items;
+    uint32_t gsplit4[5], gsplit16[17];
+    uint32_t gsplit_pad[2];
     uint32_t stage_mode;  // what a tile stages in shared memory (lane_smem.cuh)
     uint32_t refine_rows; // the row view is staged (FP32 refinement sweeps on)
 };

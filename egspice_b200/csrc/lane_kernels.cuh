@@ -105,14 +105,18 @@ __device__ __forceinline__ void newton_tile(const TileCtx& c, LaneState* s, cons
         }
         const double* cells = cell_buf(d, cur);
         if (act) {
-            if (sm) {
-                T* sa = static_cast<T*>(st.a);
-                for (uint32_t p = warp; p < d.nnz; p += nw)
-                    sa[p * 32 + lane] = (T)gather_slot(d, l, p, cp, o.gmin, cells);
+            uint32_t it0, it1;
+            if (nw == 4) {
+                it0 = d.gsplit4[warp];
+                it1 = d.gsplit4[warp + 1];
+            } else if (nw == 16) {
+                it0 = d.gsplit16[warp];
+                it1 = d.gsplit16[warp + 1];
             } else {
-                for (uint32_t p = warp; p < d.nnz; p += nw) gather_slot(d, l, p, cp, o.gmin, cells);
+                it0 = (uint32_t)((uint64_t)d.n_items * warp / nw);
+                it1 = (uint32_t)((uint64_t)d.n_items * (warp + 1) / nw);
             }
-            for (uint32_t i = warp; i < d.n; i += nw) gather_row(d, l, i, cp, o.gmin, cells);
+            gather_items<T>(d, l, lane, it0, it1, cp, o.gmin, cells, sm ? static_cast<T*>(st.a) : nullptr);
         }
         __syncthreads();
         if (it == 0) {
@@ -166,7 +170,7 @@ __device__ __forceinline__ void newton_tile(const TileCtx& c, LaneState* s, cons
             if (band_solved && MIXED)
                 for (uint32_t r = 0; r < o.refine; r++) refine_mixed(d, l);
             if (sm && (use32 || !MIXED)) {
-                int rc = d.n_prog ? refactor_prog<T>(d, st, lane, l) : refactor_smem<T>(d, st, lane, l);
+                int rc = d.n_rec ? refactor_rec<T>(d, st, lane, l) : refactor_smem<T>(d, st, lane, l);
                 if (MIXED && rc != 0) {
                     s->fp64 = 1;
                     s->fallbacks++;

@@ -67,7 +67,7 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 // buffers carry that padding); u8 arrays are copied as words.
 enum StageArr {
     S_DIAG, S_VOID, S_CURROW, S_SLOTDIAG, S_RES_T, S_CAP_T, S_VSRC_T, S_DIO_T, S_MOS_T,
-    S_GPTR, S_GCELL, S_CPTR, S_CCELL, S_RPTR, S_RCELL, S_QPTR, S_QCELL, S_SITE,
+    S_GIPTR, S_GIENT, S_SITE,
     S_Q, S_PINV, S_COLPTR, S_PROW, S_UP, S_UI, S_LP, S_LI, S_FLAGS,
     S_RTPTR, S_RTCOL, S_RTPOS, S_PROG, S_COUNT
 };
@@ -88,7 +88,7 @@ __host__ __device__ inline uint32_t stage_words(const GroupDev& d, int k, uint32
     const bool rows = d.refine_rows != 0;
     // a tile replaying from the staged program reads neither the tape's
     // column pointers, scatter rows nor flags
-    const bool by_prog = mode == kStageLu && d.n_prog != 0;
+    const bool by_prog = mode == kStageLu && d.n_rec != 0;
     switch (k) {
     case S_DIAG: return d.n;
     case S_VOID: return d.n_void;
@@ -99,14 +99,8 @@ __host__ __device__ inline uint32_t stage_words(const GroupDev& d, int k, uint32
     case S_VSRC_T: return 3 * d.n_vsrc;
     case S_DIO_T: return 2 * d.n_dio;
     case S_MOS_T: return 4 * d.n_mos;
-    case S_GPTR: return d.nnz + 1;
-    case S_GCELL: return d.n_gc;
-    case S_CPTR: return d.nnz + 1;
-    case S_CCELL: return d.n_cc;
-    case S_RPTR: return d.n + 1;
-    case S_RCELL: return d.n_rc;
-    case S_QPTR: return d.n + 1;
-    case S_QCELL: return d.n_qc;
+    case S_GIPTR: return d.n_items + 1;
+    case S_GIENT: return d.n_gi;
     case S_SITE: return d.n_sites;
     case S_Q: return d.n;
     case S_PINV: return d.n;
@@ -120,7 +114,7 @@ __host__ __device__ inline uint32_t stage_words(const GroupDev& d, int k, uint32
     case S_RTPTR: return rows ? d.n + 1 : 0u;
     case S_RTCOL: return rows ? d.nnz : 0u;
     case S_RTPOS: return rows ? d.nnz : 0u;
-    case S_PROG: return mode == kStageLu ? d.n_prog : 0u;
+    case S_PROG: return (mode == kStageLu && d.rec_stage) ? d.n_rec : 0u;
     default: return 0u;
     }
 }
@@ -136,14 +130,8 @@ __host__ __device__ inline const void* stage_src(const GroupDev& d, int k) {
     case S_VSRC_T: return d.vsrc_t;
     case S_DIO_T: return d.dio_t;
     case S_MOS_T: return d.mos_t;
-    case S_GPTR: return d.g_ptr;
-    case S_GCELL: return d.g_cell;
-    case S_CPTR: return d.c_ptr;
-    case S_CCELL: return d.c_cell;
-    case S_RPTR: return d.r_ptr;
-    case S_RCELL: return d.r_cell;
-    case S_QPTR: return d.q_ptr;
-    case S_QCELL: return d.q_cell;
+    case S_GIPTR: return d.gi_ptr;
+    case S_GIENT: return d.gi_ent;
     case S_SITE: return d.site_cell;
     case S_Q: return d.q;
     case S_PINV: return d.pinv;
@@ -157,7 +145,7 @@ __host__ __device__ inline const void* stage_src(const GroupDev& d, int k) {
     case S_RTPTR: return d.rt_ptr;
     case S_RTCOL: return d.rt_col;
     case S_RTPOS: return d.rt_pos;
-    case S_PROG: return d.lu_prog;
+    case S_PROG: return d.lu_rec;
     default: return nullptr;
     }
 }
@@ -174,14 +162,8 @@ __device__ inline void stage_redirect(GroupDev& d, int k, const void* p) {
     case S_VSRC_T: d.vsrc_t = u; break;
     case S_DIO_T: d.dio_t = u; break;
     case S_MOS_T: d.mos_t = u; break;
-    case S_GPTR: d.g_ptr = u; break;
-    case S_GCELL: d.g_cell = u; break;
-    case S_CPTR: d.c_ptr = u; break;
-    case S_CCELL: d.c_cell = u; break;
-    case S_RPTR: d.r_ptr = u; break;
-    case S_RCELL: d.r_cell = u; break;
-    case S_QPTR: d.q_ptr = u; break;
-    case S_QCELL: d.q_cell = u; break;
+    case S_GIPTR: d.gi_ptr = u; break;
+    case S_GIENT: d.gi_ent = u; break;
     case S_SITE: d.site_cell = u; break;
     case S_Q: d.q = u; break;
     case S_PINV: d.pinv = u; break;
@@ -195,7 +177,7 @@ __device__ inline void stage_redirect(GroupDev& d, int k, const void* p) {
     case S_RTPTR: d.rt_ptr = u; break;
     case S_RTCOL: d.rt_col = u; break;
     case S_RTPOS: d.rt_pos = u; break;
-    case S_PROG: d.lu_prog = u; break;
+    case S_PROG: d.lu_rec = u; break;
     default: break;
     }
 }
@@ -441,116 +423,108 @@ __device__ __forceinline__ int refactor_smem(const GroupDev& d, const SmemTile& 
     return 0;
 }
 
-// The replay driven by the template's flat program (tape.h lu_program): the
+// The replay from the template's 16-byte records (tape.h lu_records): the
 // same operations on the same locations in the same order as
-// refactor_smem, without the index chase through the tape's columns, and
-// with the independent entries of a scatter, an axpy or a division issued
-// two at a time. The FP64 wide-multiplier scan is folded into the
-// divisions.
+// refactor_smem, except that an FP32 tile multiplies a pivot column by the
+// pivot's reciprocal instead of dividing each entry (the FP64 residual and
+// Newton take up the rounding). Each record's loads are issued together and
+// the next record is read while the current one runs. `d` is the tile's
+// staged descriptor: lu_rec points into shared memory when the records are
+// staged there.
 template <typename T>
-__device__ __forceinline__ int refactor_prog(const GroupDev& d, const SmemTile& s, uint32_t lane, uint32_t l) {
+__device__ __forceinline__ int refactor_rec(const GroupDev& d, const SmemTile& s, uint32_t lane, uint32_t l) {
     T* __restrict__ w = static_cast<T*>(s.w);
     T* __restrict__ lx = static_cast<T*>(s.lx);
     T* __restrict__ ux = static_cast<T*>(s.ux);
     T* __restrict__ ud = static_cast<T*>(s.ud);
     const T* __restrict__ a = static_cast<const T*>(s.a);
-    const uint32_t* __restrict__ prog = reinterpret_cast<const uint32_t*>(g_dsm) + s.plan.off[S_PROG];
+    // staged in shared memory, or read from global memory through L1
+    const uint4* __restrict__ rec = reinterpret_cast<const uint4*>(d.lu_rec);
     const uint32_t P = d.P;
     for (uint32_t v = 0; v < d.n_void; v++)
         if (LM(d.a, d.void_slots[v]) != 0.0) return 1;
     constexpr bool f64 = sizeof(T) == 8;
     bool bad = false, nonfinite = false;
-    uint64_t worst = 0;
+    uint64_t worst = 0, cb = 0;
     const T growth = (T)1e-12;
     const T inf = (T)INFINITY;
-    for (uint32_t pc = 0;;) {
-        const uint32_t h = prog[pc];
-        const uint32_t op = h & 15u;
-        if (op == kOpScat) {
-            const uint32_t cnt = h >> 4;
-            const uint32_t* __restrict__ e = prog + pc + 1;
-            uint32_t j = 0;
-            for (; j + 1 < cnt; j += 2) {
-                const uint32_t e0 = e[j], e1 = e[j + 1];
-                const T v0 = SL(a, e0 & 0xffffu), v1 = SL(a, e1 & 0xffffu);
-                SL(w, e0 >> 16) = v0;
-                SL(w, e1 >> 16) = v1;
+    T uki = (T)0, dk = (T)1, rk = (T)1, cmax = (T)0;
+    uint32_t pfl = 0;
+    uint4 cur = rec[0];
+    for (uint32_t pc = 1;; pc++) {
+        const uint4 nxt = rec[pc];
+        const uint32_t op = cur.x & 15u, m = (cur.x >> 4) & 15u;
+        if (op == kRecScat) {
+            const T v0 = SL(a, cur.y & 0xffffu);
+            const T v1 = m > 1 ? SL(a, cur.z & 0xffffu) : (T)0;
+            const T v2 = m > 2 ? SL(a, cur.w & 0xffffu) : (T)0;
+            SL(w, cur.y >> 16) = v0;
+            if (m > 1) SL(w, cur.z >> 16) = v1;
+            if (m > 2) SL(w, cur.w >> 16) = v2;
+        } else if (op == kRecTake || op == kRecAxpy) {
+            // TAKE: u_ki leaves the work vector for U; both: w -= L(:, i) u_ki
+            const bool take = op == kRecTake;
+            const uint32_t e0 = take ? cur.z : cur.y, e1 = take ? cur.w : cur.z, e2 = cur.w;
+            const uint32_t i = cur.x >> 16;
+            if (take) uki = SL(w, i);
+            const T w0 = m > 0 ? SL(w, e0 >> 16) : (T)0, l0 = m > 0 ? SL(lx, e0 & 0xffffu) : (T)0;
+            const T w1 = m > 1 ? SL(w, e1 >> 16) : (T)0, l1 = m > 1 ? SL(lx, e1 & 0xffffu) : (T)0;
+            const T w2 = (!take && m > 2) ? SL(w, e2 >> 16) : (T)0, l2 = (!take && m > 2) ? SL(lx, e2 & 0xffffu) : (T)0;
+            if (take) {
+                SL(w, i) = (T)0;
+                SL(ux, cur.y) = uki;
+                nonfinite |= !(uki - uki == (T)0);
             }
-            if (j < cnt) SL(w, e[j] >> 16) = SL(a, e[j] & 0xffffu);
-            pc += 1 + cnt;
-        } else if (op == kOpTake) {
-            const uint32_t cnt = h >> 4;
-            const uint32_t ip = prog[pc + 1];
-            const uint32_t i = ip >> 16;
-            const T uki = SL(w, i);
-            SL(w, i) = (T)0;
-            SL(ux, ip & 0xffffu) = uki;
-            nonfinite |= !(uki - uki == (T)0);
-            const uint32_t* __restrict__ e = prog + pc + 2;
-            uint32_t j = 0;
-            for (; j + 1 < cnt; j += 2) {
-                const uint32_t e0 = e[j], e1 = e[j + 1];
-                const uint32_t r0 = e0 >> 16, r1 = e1 >> 16;
-                const T w0 = SL(w, r0), w1 = SL(w, r1);
-                const T l0 = SL(lx, e0 & 0xffffu), l1 = SL(lx, e1 & 0xffffu);
-                SL(w, r0) = w0 - l0 * uki;
-                SL(w, r1) = w1 - l1 * uki;
+            if (m > 0) SL(w, e0 >> 16) = w0 - l0 * uki;
+            if (m > 1) SL(w, e1 >> 16) = w1 - l1 * uki;
+            if (!take && m > 2) SL(w, e2 >> 16) = w2 - l2 * uki;
+        } else if (op == kRecPiv || op == kRecDiv) {
+            if (op == kRecPiv) {
+                const uint32_t k = cur.x >> 16;
+                pfl = (cur.x >> 8) & 15u;
+                dk = SL(w, k);
+                SL(w, k) = (T)0;
+                const bool dead = dk == (T)0 || !(fabs(dk) < inf);
+                bad |= dead;
+                if (dead) dk = (T)1;
+                SL(ud, k) = dk;
+                if constexpr (f64) cb = dbits(fabs((double)dk));
+                else {
+                    cmax = fabsf(dk);
+                    rk = (T)1 / dk;
+                }
             }
-            if (j < cnt) {
-                const uint32_t r0 = e[j] >> 16;
-                SL(w, r0) -= SL(lx, e[j] & 0xffffu) * uki;
-            }
-            pc += 2 + cnt;
-        } else if (op == kOpPiv) {
-            const uint32_t fl = (h >> 4) & 15u, cnt = h >> 8;
-            const uint32_t k = prog[pc + 1];
-            const uint32_t* __restrict__ e = prog + pc + 2;
-            T dk = SL(w, k);
-            SL(w, k) = (T)0;
-            bool dead = dk == (T)0 || !(fabs(dk) < inf);
-            bad |= dead;
-            if (dead) dk = (T)1;
-            SL(ud, k) = dk;
-            if constexpr (f64) {
-                if (!(fl & 2u)) {
-                    uint64_t cb = dbits(fabs((double)dk));
-                    for (uint32_t j = 0; j < cnt; j++) {
-                        const uint32_t r = e[j] >> 16;
-                        const T v = SL(w, r);
-                        SL(w, r) = (T)0;
-                        const uint64_t vb = dbits(fabs((double)v));
+            const uint32_t e[3] = {cur.y, cur.z, cur.w};
+            T v[3];
+#pragma unroll
+            for (int j = 0; j < 3; j++) v[j] = (uint32_t)j < m ? SL(w, e[j] >> 16) : (T)0;
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                if ((uint32_t)j >= m) break;
+                SL(w, e[j] >> 16) = (T)0;
+                T lv;
+                if constexpr (f64) {
+                    lv = v[j] / dk;
+                    if (!(pfl & 2u)) {
+                        const uint64_t vb = dbits(fabs((double)v[j])), lb = dbits(fabs((double)lv));
                         cb = cb > vb ? cb : vb;
-                        const T lv = v / dk;
-                        SL(lx, e[j] & 0xffffu) = lv;
-                        const uint64_t lb = dbits(fabs((double)lv));
                         worst = worst > lb ? worst : lb;
-                    }
-                    bad |= !(fabs((double)dk) >= 1e-12 * bitsd(cb));
-                } else {
-                    for (uint32_t j = 0; j < cnt; j++) {
-                        const uint32_t r = e[j] >> 16;
-                        const T lv = SL(w, r) / dk;
+                    } else {
                         nonfinite |= !(lv - lv == (T)0);
-                        SL(lx, e[j] & 0xffffu) = lv;
-                        SL(w, r) = (T)0;
                     }
-                }
-            } else {
-                T cmax = fabs(dk);
-                for (uint32_t j = 0; j < cnt; j++) {
-                    const uint32_t r = e[j] >> 16;
-                    const T v = SL(w, r);
-                    SL(w, r) = (T)0;
-                    cmax = fmaxf(cmax, fabsf(v));
-                    const T lv = v / dk;
+                } else {
+                    lv = v[j] * rk;
+                    cmax = fmaxf(cmax, fabsf(v[j]));
                     nonfinite |= !(lv - lv == (T)0);
-                    SL(lx, e[j] & 0xffffu) = lv;
                 }
-                if (!(fl & 2u)) bad |= !(fabsf(dk) >= growth * cmax) || !(cmax / fabsf(dk) <= (T)kWide);
+                SL(lx, e[j] & 0xffffu) = lv;
             }
-            pc += 2 + cnt;
-        } else if (op == kOpVoid) {
-            const uint32_t k = prog[pc + 1];
+            if ((cur.x & (1u << 12)) && !(pfl & 2u)) {
+                if constexpr (f64) bad |= !(fabs((double)dk) >= 1e-12 * bitsd(cb));
+                else bad |= !(fabsf(dk) >= growth * cmax) || !(cmax / fabsf(dk) <= (T)kWide);
+            }
+        } else if (op == kRecVoid) {
+            const uint32_t k = cur.x >> 16;
             const TapeView t = tape_view_smem(d, s.plan);
             SL(ud, k) = (T)1;
             for (uint32_t p = t.lp[k]; p < t.lp[k + 1]; p++) { SL(lx, p) = (T)0; SL(w, t.li[p]) = (T)0; }
@@ -559,10 +533,10 @@ __device__ __forceinline__ int refactor_prog(const GroupDev& d, const SmemTile& 
                 uint32_t i = t.ui[p];
                 for (uint32_t pl = t.lp[i]; pl < t.lp[i + 1]; pl++) SL(w, t.li[pl]) = (T)0;
             }
-            pc += 2;
         } else {
             break;
         }
+        cur = nxt;
     }
     if (nonfinite || bad) return 1;
     if constexpr (f64) return bitsd(worst) <= kWide ? 0 : 2;

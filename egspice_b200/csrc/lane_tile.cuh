@@ -24,6 +24,11 @@ constexpr int kTileThreads = kWarps * 32;
 constexpr int kWideWarps = 16;
 constexpr int kWideThreads = kWideWarps * 32;
 constexpr uint32_t kNeg = 0x80000000u;
+// Entries of the flat gather list (GroupDev gi_ent): bit 31 negates, bits
+// 28-30 the kind, bits 0-27 a cell, or for a row's q1 / ip / x value the row.
+constexpr uint32_t kGiKindShift = 28;
+constexpr uint32_t kGiIdx = 0x0fffffffu;
+enum : uint32_t { kGiCell = 0, kGiCellC = 1, kGiQ1 = 2, kGiIp = 3, kGiX = 4, kGiNop = 5 };
 
 // Cells per instance.
 constexpr uint32_t kResCells = 2;   // g, current
@@ -307,6 +312,73 @@ __device__ __forceinline__ double gather_row(const GroupDev& d, uint32_t l, uint
     if (gmin > 0.0) r += gmin * LM(d.x, i);
     LM(d.rhs, i) = r;
     return r;
+}
+
+// The gather of Newton's items it0 .. it1 (slots, then rows) from the flat
+// list: gather_slot and gather_row's sums, term for term in the same order,
+// with the loads of eight entries in flight at a time instead of one sum's.
+// Slot values also go to `sa` (the shared LU chain's A) when it is given.
+template <typename T>
+__device__ __forceinline__ void gather_items(const GroupDev& d, uint32_t l, uint32_t lane, uint32_t it0, uint32_t it1,
+                                             const Companion& cp, double gmin, const double* __restrict__ cells,
+                                             T* __restrict__ sa) {
+    if (it0 >= it1) return;
+    const uint32_t P = d.P;
+    const uint32_t* __restrict__ ptr = d.gi_ptr;
+    const uint32_t* __restrict__ ent = d.gi_ent;
+    const uint32_t e_end = ptr[it1];
+    uint32_t it = it0, nxt = ptr[it0 + 1];
+    double s0 = 0.0, s1 = 0.0, xq1 = 0.0, xip = 0.0, xx = 0.0;
+    for (uint32_t e = ptr[it0]; e < e_end; e += 8) {
+        uint32_t w[8];
+        double v[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++) w[j] = e + j < e_end ? ent[e + j] : (kGiNop << kGiKindShift);
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            const uint32_t k = (w[j] >> kGiKindShift) & 7u;
+            const double* b = k == kGiQ1 ? d.q1 : k == kGiIp ? d.ip : k == kGiX ? d.x : cells;
+            v[j] = b[(size_t)(w[j] & kGiIdx) * P + l];
+        }
+        // every entry is consumed without a branch (padding is a no-op
+        // kind past the last item, which no item boundary reaches), so the
+        // eight loads stay ahead of their uses
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            const uint32_t k = (w[j] >> kGiKindShift) & 7u;
+            const double vj = (w[j] & kNeg) ? -v[j] : v[j];
+            s0 = k == kGiCell ? s0 + vj : s0;
+            s1 = k == kGiCellC ? s1 + vj : s1;
+            xq1 = k == kGiQ1 ? vj : xq1;
+            xip = k == kGiIp ? vj : xip;
+            xx = k == kGiX ? vj : xx;
+            if (e + j + 1 == nxt) {
+                if (it < d.nnz) {
+                    double a = s0;
+                    if (cp.on) a = s0 + cp.ag0 * s1;
+                    if (gmin > 0.0 && d.slot_diag[it]) a += gmin;
+                    LM(d.a, it) = a;
+                    if (sa) sa[it * 32 + lane] = (T)a;
+                } else {
+                    const uint32_t i = it - d.nnz;
+                    double r = s0;
+                    if (cp.on) {
+                        const double q = s1;
+                        LM(d.qrow, i) = q;
+                        double dq = cp.ag0 * (q - xq1);
+                        double base = r + dq;
+                        r = cp.method == 1 ? base - cp.ag1 * xip : base;
+                    }
+                    if (gmin > 0.0) r += gmin * xx;
+                    LM(d.rhs, i) = r;
+                }
+                s0 = 0.0;
+                s1 = 0.0;
+                it++;
+                nxt = it < it1 ? ptr[it + 1] : 0xFFFFFFFFu;
+            }
+        }
+    }
 }
 
 // Row charges without a Newton (the transient start and the tape's charge

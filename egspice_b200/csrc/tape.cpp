@@ -836,6 +836,60 @@ bool lu_program(const Tape& t, const uint32_t* col_ptr, std::vector<uint32_t>& p
     return true;
 }
 
+bool lu_records(const Tape& t, const uint32_t* col_ptr, std::vector<uint32_t>& rec) {
+    rec.clear();
+    const uint32_t n = t.n;
+    auto fits = [](uint64_t v) { return v < 65536u; };
+    if (!fits(n) || !fits(t.prow.size()) || !fits(t.li.size()) || !fits(t.ui.size())) return false;
+    auto pack = [](uint32_t hi, uint32_t lo) { return (hi << 16) | lo; };
+    auto put = [&](uint32_t x, uint32_t y, uint32_t z, uint32_t w) {
+        rec.push_back(x);
+        rec.push_back(y);
+        rec.push_back(z);
+        rec.push_back(w);
+    };
+    std::vector<uint32_t> e;
+    for (uint32_t k = 0; k < n; k++) {
+        const uint32_t c = t.q[k];
+        const uint32_t fl = t.flags[k];
+        e.clear();
+        for (uint32_t p = col_ptr[c]; p < col_ptr[c + 1]; p++) e.push_back(pack(t.prow[p], p));
+        for (size_t j = 0; j < e.size(); j += 3) {
+            const uint32_t m = (uint32_t)std::min<size_t>(3, e.size() - j);
+            put(kRecScat | (m << 4), e[j], m > 1 ? e[j + 1] : 0u, m > 2 ? e[j + 2] : 0u);
+        }
+        for (uint32_t p = t.up[k]; p < t.up[k + 1]; p++) {
+            const uint32_t i = t.ui[p];
+            e.clear();
+            for (uint32_t pl = t.lp[i]; pl < t.lp[i + 1]; pl++) e.push_back(pack(t.li[pl], pl));
+            const uint32_t m0 = (uint32_t)std::min<size_t>(2, e.size());
+            put(kRecTake | (m0 << 4) | (i << 16), p, m0 > 0 ? e[0] : 0u, m0 > 1 ? e[1] : 0u);
+            for (size_t j = m0; j < e.size(); j += 3) {
+                const uint32_t m = (uint32_t)std::min<size_t>(3, e.size() - j);
+                put(kRecAxpy | (m << 4), e[j], m > 1 ? e[j + 1] : 0u, m > 2 ? e[j + 2] : 0u);
+            }
+        }
+        if (fl & 1u) {
+            put(kRecVoid | (k << 16), 0, 0, 0);
+            continue;
+        }
+        e.clear();
+        for (uint32_t p = t.lp[k]; p < t.lp[k + 1]; p++) e.push_back(pack(t.li[p], p));
+        const uint32_t m0 = (uint32_t)std::min<size_t>(3, e.size());
+        const uint32_t last0 = e.size() <= 3 ? 1u : 0u;
+        put(kRecPiv | (m0 << 4) | ((fl & 15u) << 8) | (last0 << 12) | (k << 16), m0 > 0 ? e[0] : 0u,
+            m0 > 1 ? e[1] : 0u, m0 > 2 ? e[2] : 0u);
+        for (size_t j = m0; j < e.size(); j += 3) {
+            const uint32_t m = (uint32_t)std::min<size_t>(3, e.size() - j);
+            const uint32_t last = j + m == e.size() ? 1u : 0u;
+            put(kRecDiv | (m << 4) | (last << 12), e[j], m > 1 ? e[j + 1] : 0u, m > 2 ? e[j + 2] : 0u);
+        }
+    }
+    put(kRecEnd, 0, 0, 0);
+    put(kRecEnd, 0, 0, 0);
+    return true;
+}
+
 namespace {
 uint32_t pow2_at_least(uint32_t v) {
     uint32_t p = 1;

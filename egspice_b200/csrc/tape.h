@@ -54,6 +54,21 @@ bool factor_tape(uint32_t n, const uint32_t* col_ptr, const uint32_t* row_idx, c
 enum LuOp : uint32_t { kOpEnd = 0, kOpScat = 1, kOpTake = 2, kOpPiv = 3, kOpVoid = 4 };
 bool lu_program(const Tape& t, const uint32_t* col_ptr, std::vector<uint32_t>& prog);
 
+// The same replay as fixed 16-byte records (4 words each) for the shared
+// LU chain: a record's entries update distinct rows, so its loads issue
+// together, and the next record's address is known before the current one
+// is decoded. Entries are (row << 16 | slot) words as in lu_program.
+//   SCAT  x = 1 | n << 4; y, z, w: n x (w row << 16 | A slot), n = 1..3
+//   TAKE  x = 2 | n << 4 | i << 16; y = U slot; z, w: n x (L row << 16 | L slot), n = 0..2
+//   AXPY  x = 3 | n << 4; y, z, w: the TAKE's further entries, n = 1..3
+//   PIV   x = 4 | n << 4 | flags << 8 | last << 12 | k << 16; y, z, w: n x (L row << 16 | L slot)
+//   DIV   x = 5 | n << 4 | last << 12; y, z, w: the pivot's further entries
+//   VOID  x = 6 | k << 16 (a void column, after its scatter and takes)
+//   END   x = 0, twice (the second one is read ahead and never run)
+// `last` marks the final record of a pivot column (its checks run there).
+enum LuRec : uint32_t { kRecEnd = 0, kRecScat = 1, kRecTake = 2, kRecAxpy = 3, kRecPiv = 4, kRecDiv = 5, kRecVoid = 6 };
+bool lu_records(const Tape& t, const uint32_t* col_ptr, std::vector<uint32_t>& rec);
+
 // The banded streaming replay: when the replay of every column k touches
 // only work-vector rows within k - band .. k + band (a ladder's elimination
 // walks its chain), the work vector fits a ring of w_ring rows and the L

@@ -15,7 +15,7 @@ from typing import List, Optional, Sequence
 import numpy as np
 
 from . import abi
-from .abi import (CreateOpts, LaneNewton, NetlistC, NewtonOpts, StepReport, Stats, TranOpts, f64p, u32p)
+from .abi import (ClassInfo, CreateOpts, LaneNewton, NetlistC, NewtonOpts, StepReport, Stats, TranOpts, f64p, u32p)
 from .decks import Netlist
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -60,6 +60,8 @@ def lib():
         L.espl_get_period_meas.restype = C.c_uint32
         L.espl_get_stats.argtypes = [C.c_void_p, C.POINTER(Stats)]
         L.espl_get_stats.restype = C.c_uint32
+        L.espl_get_classes.argtypes = [C.c_void_p, C.POINTER(ClassInfo), C.c_uint32, u32p]
+        L.espl_get_classes.restype = C.c_uint32
         L.espl_error_message.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t]
         L.espl_error_message.restype = C.c_uint32
         _lib = L
@@ -165,6 +167,16 @@ class Lanes:
                                                         ("q", "pinv", "lp", "li", "up", "ui", "flags")]),
                     "espl_copy_tape")
         return {k: out[k][:arrs[k]] for k in arrs}
+
+    def classes(self) -> List[dict]:
+        """The launch classes in launch order, each with its kernel's device
+        time in the last solve or device launch."""
+        n = C.c_uint32()
+        self._check(lib().espl_get_classes(self.h, None, 0, C.byref(n)), "espl_get_classes")
+        out = (ClassInfo * max(n.value, 1))()
+        self._check(lib().espl_get_classes(self.h, out, n.value, C.byref(n)), "espl_get_classes")
+        return [dict(tiles=c.tiles, wide=bool(c.wide), per_sm=c.per_sm, smem_bytes=c.smem_bytes, ms=c.last_ms)
+                for c in out[:n.value]]
 
     def stats(self) -> Stats:
         s = Stats()

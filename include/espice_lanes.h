@@ -226,6 +226,23 @@ typedef struct {
 } espl_stats;
 espl_status espl_get_stats(espl_lanes *h, espl_stats *out);
 
+/* The launch classes of the current plan, in launch order: templates
+ * grouped by tile width and resident tiles per SM, one kernel launch per
+ * class, each class on a stream of its own when there are several. With
+ * each, the device time of its kernel in the last solve or device launch
+ * (CUDA events around the launch on its stream; 0 before the first). At
+ * most `cap` are written; `count` gets how many there are. The per-launch
+ * counterpart of the reference driver's per-round phase split
+ * (ESPICE_GPU_STATS, src/analysis/gpu/lanes.zig:372-413). */
+typedef struct {
+    uint32_t tiles;       /* 32-lane tiles in the class */
+    uint32_t wide;        /* 1: 16-warp tiles, 0: 4-warp tiles */
+    uint32_t per_sm;      /* resident tiles per SM */
+    uint32_t smem_bytes;  /* dynamic shared memory per tile */
+    double last_ms;       /* device time of the class's last kernel */
+} espl_class_info;
+espl_status espl_get_classes(espl_lanes *h, espl_class_info *out, uint32_t cap, uint32_t *count);
+
 /* Host-only symbolic seam, no GPU needed. `espl_order` is order.zig's
  * `order` (src/solver/order.zig:78): q[k] = the column factored at step k,
  * BTF sink block first, AMD or natural per block. ESPL_NO_TAPE on
