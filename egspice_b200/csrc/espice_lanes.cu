@@ -97,7 +97,8 @@ struct Group {
     };
     std::vector<BatchRec> batch_order;
     uint32_t tile0 = 0;
-    uint32_t n_rec = 0;  // words of the uploaded replay records (0: none)
+    uint32_t n_rec = 0;   // words of the uploaded replay records (0: none)
+    uint32_t n_srec = 0;  // words of the uploaded solve records (0: none)
 };
 
 }  // namespace
@@ -592,11 +593,18 @@ espl_status plan_classes(espl_lanes* h) {
         g.dev.refine_rows = MIXED && h->refine_sweeps > 0 ? 1u : 0u;
         g.dev.n_rec = g.n_rec;
         g.dev.rec_stage = g.n_rec ? 1u : 0u;
+        g.dev.n_srec = g.n_srec;
+        g.dev.srec_stage = g.n_srec ? 1u : 0u;
         g.dev.stage_mode = kStageNone;
         bytes[i] = 0;
         bool placed = false;
         for (uint32_t mode : {kStageLu, kStageIndex, kStageNone}) {
             SmemPlan sp = smem_plan(g.dev, mode, MIXED);
+            if (mode == kStageLu && sp.bytes > (uint32_t)max_dyn) {
+                // the chain may still fit with its records left in global memory
+                g.dev.rec_stage = g.dev.srec_stage = 0;
+                sp = smem_plan(g.dev, mode, MIXED);
+            }
             if (sp.bytes <= (uint32_t)max_dyn) {
                 g.dev.stage_mode = mode;
                 g.dev.band_off = sp.band_off;
@@ -616,19 +624,24 @@ espl_status plan_classes(espl_lanes* h) {
         int t = 0;
         espl_status s;
         if ((s = tiles_per_sm(wide[i], bytes[i], t))) return s;
-        if (g.dev.stage_mode == kStageLu && g.dev.n_rec) {
+        if (g.dev.stage_mode == kStageLu && (g.dev.n_rec || g.dev.n_srec)) {
             // Staged records cost their own words of shared memory; where
             // that drops a resident tile per SM they stay in global memory
-            // (read through L1, one record ahead).
-            GroupDev bare = g.dev;
-            bare.rec_stage = 0;
-            SmemPlan sp = smem_plan(bare, kStageLu, MIXED);
-            int tb = 0;
-            if ((s = tiles_per_sm(false, sp.bytes, tb))) return s;
-            if (tb > t) {
-                g.dev.rec_stage = 0;
-                bytes[i] = sp.bytes;
-                t = tb;
+            // (read through L1, one record ahead). The solve records go
+            // first, then the replay's.
+            for (uint32_t keep : {2u, 0u}) {
+                GroupDev bare = g.dev;
+                bare.srec_stage = 0;
+                bare.rec_stage = keep ? g.dev.rec_stage : 0u;
+                SmemPlan sp = smem_plan(bare, kStageLu, MIXED);
+                int tb = 0;
+                if ((s = tiles_per_sm(false, sp.bytes, tb))) return s;
+                if (tb > t) {
+                    g.dev.srec_stage = 0;
+                    g.dev.rec_stage = bare.rec_stage;
+                    bytes[i] = sp.bytes;
+                    t = tb;
+                }
             }
         }
         per[i] = (uint32_t)t;
@@ -771,6 +784,10 @@ espl_status retape(espl_lanes* h, int tran, double dt) {
             d.n_rec = lu_records(g.tape, g.col_ptr.data(), rec) ? (uint32_t)rec.size() : 0u;
             if (d.n_rec) UP(lu_rec, rec);
             g.n_rec = d.n_rec;
+            std::vector<uint32_t> srec;
+            d.n_srec = solve_records(g.tape, srec) ? (uint32_t)srec.size() : 0u;
+            if (d.n_srec) UP(sol_rec, srec);
+            g.n_srec = d.n_srec;
             // the banded streaming replay, for templates the shared LU chain
             // cannot hold (plan_classes decides which run it)
             BandPlan bp;

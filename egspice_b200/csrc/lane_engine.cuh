@@ -49,6 +49,8 @@ struct GroupDev {
     const uint32_t* lu_rec;                    // the replay as 16-byte records (tape.h lu_records)
     uint32_t n_rec, rec_stage;                 // n_rec words (0: the shared chain replays from the tape);
                                                // rec_stage: the records are staged in shared memory
+    const uint32_t* sol_rec;                   // the solves as 16-byte records (tape.h solve_records)
+    uint32_t n_srec, srec_stage;               // likewise for the solves
     // The banded streaming replay (lane_band.cuh, tape.h BandPlan): ring
     // sizes, chunk capacities and count, the shared-memory offset of its
     // buffers, and the chunk tables and scatter slots in global memory.

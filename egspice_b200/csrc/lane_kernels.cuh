@@ -181,7 +181,10 @@ __device__ __forceinline__ void newton_tile(const TileCtx& c, LaneState* s, cons
                         rc = replay_holds64(d, l) ? 0 : 1;
                     }
                     if (rc == 0) {
-                        solve_smem<T>(d, st, lane, l);
+                        if (d.n_srec)
+                            solve_rec<T>(d, st, lane, l);
+                        else
+                            solve_smem<T>(d, st, lane, l);
                         if (MIXED)
                             for (uint32_t r = 0; r < o.refine; r++) refine_smem(d, st, lane, l);
                     } else if (!peel_dense(d, l, *s)) {

@@ -69,7 +69,7 @@ enum StageArr {
     S_DIAG, S_VOID, S_CURROW, S_SLOTDIAG, S_RES_T, S_CAP_T, S_VSRC_T, S_DIO_T, S_MOS_T,
     S_GIPTR, S_GIENT, S_SITE,
     S_Q, S_PINV, S_COLPTR, S_PROW, S_UP, S_UI, S_LP, S_LI, S_FLAGS,
-    S_RTPTR, S_RTCOL, S_RTPOS, S_PROG, S_COUNT
+    S_RTPTR, S_RTCOL, S_RTPOS, S_PROG, S_SREC, S_COUNT
 };
 
 // One streamed block of the banded solves (lane_band.cuh): index words
@@ -115,6 +115,7 @@ __host__ __device__ inline uint32_t stage_words(const GroupDev& d, int k, uint32
     case S_RTCOL: return rows ? d.nnz : 0u;
     case S_RTPOS: return rows ? d.nnz : 0u;
     case S_PROG: return (mode == kStageLu && d.rec_stage) ? d.n_rec : 0u;
+    case S_SREC: return (mode == kStageLu && d.srec_stage) ? d.n_srec : 0u;
     default: return 0u;
     }
 }
@@ -146,6 +147,7 @@ __host__ __device__ inline const void* stage_src(const GroupDev& d, int k) {
     case S_RTCOL: return d.rt_col;
     case S_RTPOS: return d.rt_pos;
     case S_PROG: return d.lu_rec;
+    case S_SREC: return d.sol_rec;
     default: return nullptr;
     }
 }
@@ -178,6 +180,7 @@ __device__ inline void stage_redirect(GroupDev& d, int k, const void* p) {
     case S_RTCOL: d.rt_col = u; break;
     case S_RTPOS: d.rt_pos = u; break;
     case S_PROG: d.lu_rec = u; break;
+    case S_SREC: d.sol_rec = u; break;
     default: break;
     }
 }
@@ -604,6 +607,58 @@ __device__ __forceinline__ void solve_smem(const GroupDev& d, const SmemTile& s,
     }
     for (; r < t.n; r++) SL(y, t.pinv[r]) = (T)(-LM(rhs, r));
     subst_smem<T>(t, s, y, lane);
+    for (uint32_t j = 0; j < t.n; j++) {
+        LM(dx, t.q[j]) = (double)SL(y, j);
+        SL(y, j) = (T)0;
+    }
+}
+
+// solve_smem from the template's solve records (tape.h solve_records): the
+// same sweeps on the same locations in the same order, a record's loads
+// issued together and the next record read while the current one runs,
+// without the skip of zero entries (y - L * 0 is y).
+template <typename T>
+__device__ __forceinline__ void solve_rec(const GroupDev& d, const SmemTile& s, uint32_t lane, uint32_t l) {
+    const uint32_t P = d.P;
+    const TapeView t = tape_view_smem(d, s.plan);
+    const double* __restrict__ rhs = d.rhs;
+    double* __restrict__ dx = d.dx;
+    T* __restrict__ y = static_cast<T*>(s.w);
+    const T* __restrict__ lx = static_cast<const T*>(s.lx);
+    const T* __restrict__ ux = static_cast<const T*>(s.ux);
+    const T* __restrict__ ud = static_cast<const T*>(s.ud);
+    uint32_t r = 0;
+    for (; r + 7 < t.n; r += 8) {
+        double b[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++) b[j] = LM(rhs, r + j);
+#pragma unroll
+        for (int j = 0; j < 8; j++) SL(y, t.pinv[r + j]) = (T)(-b[j]);
+    }
+    for (; r < t.n; r++) SL(y, t.pinv[r]) = (T)(-LM(rhs, r));
+    const uint4* __restrict__ rec = reinterpret_cast<const uint4*>(d.sol_rec);
+    T yk = (T)0;
+    uint4 cur = rec[0];
+    for (uint32_t pc = 1;; pc++) {
+        const uint4 nxt = rec[pc];
+        const uint32_t op = cur.x & 15u, m = (cur.x >> 4) & 15u;
+        if (op == kSolEnd) break;
+        const T* __restrict__ f = (op == kSolFwd || op == kSolFwdC) ? lx : ux;
+        const T y0 = m > 0 ? SL(y, cur.y >> 16) : (T)0, f0 = m > 0 ? SL(f, cur.y & 0xffffu) : (T)0;
+        const T y1 = m > 1 ? SL(y, cur.z >> 16) : (T)0, f1 = m > 1 ? SL(f, cur.z & 0xffffu) : (T)0;
+        const T y2 = m > 2 ? SL(y, cur.w >> 16) : (T)0, f2 = m > 2 ? SL(f, cur.w & 0xffffu) : (T)0;
+        if (op == kSolFwd) {
+            yk = SL(y, cur.x >> 16);
+        } else if (op == kSolBwd) {
+            const uint32_t k = cur.x >> 16;
+            yk = SL(y, k) / SL(ud, k);
+            SL(y, k) = yk;
+        }
+        if (m > 0) SL(y, cur.y >> 16) = y0 - f0 * yk;
+        if (m > 1) SL(y, cur.z >> 16) = y1 - f1 * yk;
+        if (m > 2) SL(y, cur.w >> 16) = y2 - f2 * yk;
+        cur = nxt;
+    }
     for (uint32_t j = 0; j < t.n; j++) {
         LM(dx, t.q[j]) = (double)SL(y, j);
         SL(y, j) = (T)0;

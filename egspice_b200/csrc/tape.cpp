@@ -890,6 +890,42 @@ bool lu_records(const Tape& t, const uint32_t* col_ptr, std::vector<uint32_t>& r
     return true;
 }
 
+bool solve_records(const Tape& t, std::vector<uint32_t>& rec) {
+    rec.clear();
+    const uint32_t n = t.n;
+    auto fits = [](uint64_t v) { return v < 65536u; };
+    if (!fits(n) || !fits(t.li.size()) || !fits(t.ui.size())) return false;
+    auto put = [&](uint32_t x, uint32_t y, uint32_t z, uint32_t w) {
+        rec.push_back(x);
+        rec.push_back(y);
+        rec.push_back(z);
+        rec.push_back(w);
+    };
+    std::vector<uint32_t> e;
+    auto column = [&](uint32_t first, uint32_t cont, uint32_t k, bool always) {
+        if (e.empty() && !always) return;
+        const uint32_t m0 = (uint32_t)std::min<size_t>(3, e.size());
+        put(first | (m0 << 4) | (k << 16), m0 > 0 ? e[0] : 0u, m0 > 1 ? e[1] : 0u, m0 > 2 ? e[2] : 0u);
+        for (size_t j = m0; j < e.size(); j += 3) {
+            const uint32_t m = (uint32_t)std::min<size_t>(3, e.size() - j);
+            put(cont | (m << 4), e[j], m > 1 ? e[j + 1] : 0u, m > 2 ? e[j + 2] : 0u);
+        }
+    };
+    for (uint32_t k = 0; k < n; k++) {
+        e.clear();
+        for (uint32_t p = t.lp[k]; p < t.lp[k + 1]; p++) e.push_back((t.li[p] << 16) | p);
+        column(kSolFwd, kSolFwdC, k, false);
+    }
+    for (uint32_t k = n; k-- > 0;) {
+        e.clear();
+        for (uint32_t p = t.up[k]; p < t.up[k + 1]; p++) e.push_back((t.ui[p] << 16) | p);
+        column(kSolBwd, kSolBwdC, k, true);
+    }
+    put(kSolEnd, 0, 0, 0);
+    put(kSolEnd, 0, 0, 0);
+    return true;
+}
+
 namespace {
 uint32_t pow2_at_least(uint32_t v) {
     uint32_t p = 1;

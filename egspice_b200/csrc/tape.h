@@ -69,6 +69,19 @@ bool lu_program(const Tape& t, const uint32_t* col_ptr, std::vector<uint32_t>& p
 enum LuRec : uint32_t { kRecEnd = 0, kRecScat = 1, kRecTake = 2, kRecAxpy = 3, kRecPiv = 4, kRecDiv = 5, kRecVoid = 6 };
 bool lu_records(const Tape& t, const uint32_t* col_ptr, std::vector<uint32_t>& rec);
 
+// The triangular solves (luSolve's two sweeps, kernels/lane.zig:130-157) as
+// 16-byte records in the same style: the forward sweep by columns k = 0 ..
+// n-1, then the back sweep by columns k = n-1 .. 0.
+//   FWD   x = 1 | n << 4 | k << 16; y, z, w: n x (row << 16 | L slot): y[row] -= L y[k], n = 1..3
+//   FWDC  x = 2 | n << 4: the column's further entries
+//   BWD   x = 3 | n << 4 | k << 16; y[k] /= U_kk, then y, z, w: n x (row << 16 | U slot):
+//         y[row] -= U y[k], n = 0..3
+//   BWDC  x = 4 | n << 4
+//   END   x = 0, twice
+// A column without L entries has no FWD record; every column has a BWD one.
+enum SolveRec : uint32_t { kSolEnd = 0, kSolFwd = 1, kSolFwdC = 2, kSolBwd = 3, kSolBwdC = 4 };
+bool solve_records(const Tape& t, std::vector<uint32_t>& rec);
+
 // The banded streaming replay: when the replay of every column k touches
 // only work-vector rows within k - band .. k + band (a ladder's elimination
 // walks its chain), the work vector fits a ring of w_ring rows and the L
