@@ -118,6 +118,13 @@ def ring_workload(seed: int, lanes: int = 16384, variants: int = 32, lanes_per_v
     return nets, topts
 
 
+# DRAM bytes per lane-step of the bulk k_tran class (31-stage ring lanes, mixed):
+# dram__bytes_read.sum + dram__bytes_write.sum from one ncu capture of the
+# benchmark's full lane count cut to 200 steps (425.9 GB for 16,704 lanes x 200
+# steps), scaled by the run's lane-steps for the roofline's traffic figure.
+DRAM_BYTES_PER_LANE_STEP = 127475.0
+
+
 def algorithmic_bytes(nets, lane_iterations_per_net, s_lu: int):
     """SURVEY 8(d) bytes per lane-iteration, summed: refactor 8 nnz +
     s (nnzL + nnzU + n); solve s (nnzL + nnzU + n) + 16 n; update/gates 40 n;
@@ -485,7 +492,12 @@ def main():
             mixed_over_fp64=(plain["dev_s"] / best["dev_s"]) if (plain and "mixed" in results) else None,
             learned=False),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "peak_kind": kind, "traffic": None,
+                     "peak_kind": kind,
+                     "traffic": (DRAM_BYTES_PER_LANE_STEP * sum(r.steps for r in best["reps"]) / 1e9
+                                 if "mixed" in results else None),
+                     "traffic_unit": "GB per sweep (ncu capture scaled by lane-steps)",
+                     "traffic_per_lane_step": DRAM_BYTES_PER_LANE_STEP if "mixed" in results else None,
+                     "algorithmic_per_sweep_gb": bytes_alg / 1e9,
                      "kernel": ("k_tran<true>" if "mixed" in results else "k_tran<false>") +
                                ": per-tile eval + gather + shared-memory LU + gates, fused"},
         "e2e": {"value": e2e, "unit": "points/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
