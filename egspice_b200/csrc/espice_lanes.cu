@@ -485,6 +485,22 @@ espl_status alloc_group(espl_lanes* h, Group& g) {
     double* p = nullptr;
     if ((s = dalloc(h, own, &p, (size_t)d.n_mos * Mos1Prep::count * P))) return s;
     d.mos_d = p;
+    {
+        // lane-uniform MOS prep: type (0), gamma (3), phi (4), lambda (5)
+        // and IS (6) the same on every lane of every instance
+        const std::vector<double>& mp = g.kinds[ESPL_MOS1].param;
+        bool uni = d.n_mos > 0;
+        for (uint32_t i = 0; uni && i < d.n_mos; i++)
+            for (uint32_t k : {0u, 3u, 4u, 5u, 6u}) {
+                const double* row = mp.data() + ((size_t)i * 9 + k) * P;
+                for (size_t l = 1; l < P && uni; l++) uni = row[l] == row[0];
+            }
+        d.mos_uni = uni ? 1u : 0u;
+        if (uni) {
+            if ((s = dalloc(h, own, &p, (size_t)d.n_mos * kMosUni))) return s;
+            d.mos_u = p;
+        }
+    }
     if ((s = dalloc(h, own, &p, (size_t)d.n_dio * DiodePrep::count * P))) return s;
     d.dio_d = p;
 #define AL(field, count) if ((s = dalloc(h, own, &d.field, (count)))) return s

@@ -60,6 +60,13 @@ struct GroupDev {
     const uint8_t* cur_row;
     const uint32_t *res_t, *res_s, *cap_t, *cap_s, *vsrc_t, *vsrc_s, *isrc_t, *dio_t, *dio_s, *mos_t, *mos_s;
     const double *res_r, *cap_c, *vsrc_p, *isrc_p, *dio_d, *mos_d;
+    // When every MOS has the same type, gamma, phi, lambda and IS on all
+    // lanes (Monte Carlo varies VTO and KP), the prep values that depend only
+    // on those are the same on every lane: mos_u holds them once per
+    // instance (kMosUni values: type, vt, lambda, gamma, phit, isat, vcrit,
+    // gmin), read as broadcast loads instead of one load per lane.
+    const double* mos_u;
+    uint32_t mos_uni, mos_uni_pad;
     double *x, *x_old, *dx, *rhs, *qrow, *g, *c, *a, *lx, *ux, *udiag, *w, *y, *lim_mos, *lim_dio;
     float *lx32, *ux32, *udiag32, *w32, *y32;
     double *q1, *ip, *cur, *prev, *sring, *sip;

@@ -320,6 +320,8 @@ __global__ void __launch_bounds__(kTileThreads) k_prep(TileMap m, const double* 
         for (int k = 0; k < 9; k++) p[k] = LM(mr, 9 * i + k);
         mos1_setup(p, o);
         for (int k = 0; k < Mos1Prep::count; k++) LM(md, Mos1Prep::count * i + k) = o[k];
+        if (d.mos_uni && l == 0)
+            for (uint32_t k = 0; k < kMosUni; k++) const_cast<double*>(d.mos_u)[kMosUni * i + k] = o[mos_uni_field(k)];
     }
     for (uint32_t i = c.warp; i < d.n_dio; i += nw) {
         double p[7], o[DiodePrep::count];

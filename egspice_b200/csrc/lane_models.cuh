@@ -31,6 +31,12 @@ constexpr double kGminDevice = 1e-12;  // $simparam("gmin"), the .options defaul
 struct Mos1Prep {
     enum { type, vt, beta, lambda, gamma, phit, von0, isat, vcrit, gmin, vgs_seed, count };
 };
+// The lane-uniform MOS prep values (GroupDev mos_u), in this order.
+constexpr uint32_t kMosUni = 8;
+__host__ __device__ constexpr int mos_uni_field(uint32_t k) {
+    return k == 0 ? Mos1Prep::type : k == 1 ? Mos1Prep::vt : k == 2 ? Mos1Prep::lambda : k == 3 ? Mos1Prep::gamma
+         : k == 4 ? Mos1Prep::phit : k == 5 ? Mos1Prep::isat : k == 6 ? Mos1Prep::vcrit : Mos1Prep::gmin;
+}
 struct DiodePrep {
     enum { is, vte, vcrit, gmin, cjo, cjo_t, vj_t, mt, fc, tt, count };
 };

@@ -29,6 +29,7 @@ constexpr uint32_t kNeg = 0x80000000u;
 constexpr uint32_t kGiKindShift = 28;
 constexpr uint32_t kGiIdx = 0x0fffffffu;
 enum : uint32_t { kGiCell = 0, kGiCellC = 1, kGiQ1 = 2, kGiIp = 3, kGiX = 4, kGiNop = 5 };
+constexpr uint32_t kGiChunk = 12;  // entries whose loads are in flight together
 
 // Cells per instance.
 constexpr uint32_t kResCells = 2;   // g, current
@@ -80,6 +81,11 @@ __device__ __forceinline__ MosPrep mos_prep(const GroupDev& d, uint32_t l, uint3
     const uint32_t P = d.P;
     const double* md = d.mos_d;
     uint32_t b = Mos1Prep::count * i;
+    if (d.mos_uni) {
+        const double* u = d.mos_u + kMosUni * i;
+        return MosPrep{__ldg(u + 0), __ldg(u + 1), LM(md, b + Mos1Prep::beta), __ldg(u + 2), __ldg(u + 3),
+                       __ldg(u + 4), LM(md, b + Mos1Prep::von0), __ldg(u + 5), __ldg(u + 7), __ldg(u + 6)};
+    }
     return MosPrep{LM(md, b + Mos1Prep::type),  LM(md, b + Mos1Prep::vt),    LM(md, b + Mos1Prep::beta),
                    LM(md, b + Mos1Prep::lambda), LM(md, b + Mos1Prep::gamma), LM(md, b + Mos1Prep::phit),
                    LM(md, b + Mos1Prep::von0),   LM(md, b + Mos1Prep::isat),  LM(md, b + Mos1Prep::gmin),
@@ -316,7 +322,7 @@ __device__ __forceinline__ double gather_row(const GroupDev& d, uint32_t l, uint
 
 // The gather of Newton's items it0 .. it1 (slots, then rows) from the flat
 // list: gather_slot and gather_row's sums, term for term in the same order,
-// with the loads of eight entries in flight at a time instead of one sum's.
+// with the loads of kGiChunk entries in flight at a time instead of one sum's.
 // Slot values also go to `sa` (the shared LU chain's A) when it is given.
 template <typename T>
 __device__ __forceinline__ void gather_items(const GroupDev& d, uint32_t l, uint32_t lane, uint32_t it0, uint32_t it1,
@@ -329,22 +335,22 @@ __device__ __forceinline__ void gather_items(const GroupDev& d, uint32_t l, uint
     const uint32_t e_end = ptr[it1];
     uint32_t it = it0, nxt = ptr[it0 + 1];
     double s0 = 0.0, s1 = 0.0, xq1 = 0.0, xip = 0.0, xx = 0.0;
-    for (uint32_t e = ptr[it0]; e < e_end; e += 8) {
-        uint32_t w[8];
-        double v[8];
+    for (uint32_t e = ptr[it0]; e < e_end; e += kGiChunk) {
+        uint32_t w[kGiChunk];
+        double v[kGiChunk];
 #pragma unroll
-        for (int j = 0; j < 8; j++) w[j] = e + j < e_end ? ent[e + j] : (kGiNop << kGiKindShift);
+        for (int j = 0; j < (int)kGiChunk; j++) w[j] = e + j < e_end ? ent[e + j] : (kGiNop << kGiKindShift);
 #pragma unroll
-        for (int j = 0; j < 8; j++) {
+        for (int j = 0; j < (int)kGiChunk; j++) {
             const uint32_t k = (w[j] >> kGiKindShift) & 7u;
             const double* b = k == kGiQ1 ? d.q1 : k == kGiIp ? d.ip : k == kGiX ? d.x : cells;
             v[j] = b[(size_t)(w[j] & kGiIdx) * P + l];
         }
         // every entry is consumed without a branch (padding is a no-op
         // kind past the last item, which no item boundary reaches), so the
-        // eight loads stay ahead of their uses
+        // chunk's loads stay ahead of their uses
 #pragma unroll
-        for (int j = 0; j < 8; j++) {
+        for (int j = 0; j < (int)kGiChunk; j++) {
             const uint32_t k = (w[j] >> kGiKindShift) & 7u;
             const double vj = (w[j] & kNeg) ? -v[j] : v[j];
             s0 = k == kGiCell ? s0 + vj : s0;
