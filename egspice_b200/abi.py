@@ -56,7 +56,7 @@ class StepReport(C.Structure):
 class Stats(C.Structure):
     _fields_ = [("total_ms", C.c_double), ("newton_ms", C.c_double), ("launches", C.c_uint64),
                 ("lane_iterations", C.c_uint64), ("lane_steps", C.c_uint64), ("dense_peels", C.c_uint32),
-                ("peel_overflow", C.c_uint32)]
+                ("retapes", C.c_uint32)]
 
 
 class ClassInfo(C.Structure):

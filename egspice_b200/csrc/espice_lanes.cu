@@ -112,6 +112,7 @@ struct espl_lanes {
     GroupDev* d_groups = nullptr;
     uint32_t* d_warp_group = nullptr;
     LaneState* d_state = nullptr;
+    uint32_t* d_stale = nullptr;  // two stale-tape words per template (GroupDev stale)
     const double** d_mos_raw = nullptr;
     const double** d_dio_raw = nullptr;
     cudaStream_t stream = nullptr;
@@ -757,6 +758,9 @@ espl_status push_descs(espl_lanes* h) {
     return ESPL_OK;
 }
 
+espl_status lane_matrix(espl_lanes* h, Group& g, uint32_t l, std::vector<double>& a);
+espl_status upload_tape(espl_lanes* h, Group& g);
+
 // ownTape (lanes.zig:590-603): every lane is stamped at its x, the lead
 // lane's A = G (+ C / dt) is read back and factored on the host, and the
 // frozen tape goes to the device.
@@ -767,13 +771,32 @@ espl_status retape(espl_lanes* h, int tran, double dt) {
     launch();
     CK(cudaGetLastError());
     for (auto& g : h->groups) {
-        std::vector<double> a0(g.nnz);
-        if (g.nnz)
-            CK(cudaMemcpy2DAsync(a0.data(), sizeof(double), g.dev.a, sizeof(double) * g.P, sizeof(double), g.nnz,
-                                 cudaMemcpyDeviceToHost, h->stream));
-        CK(cudaStreamSynchronize(h->stream));
+        std::vector<double> a0;
+        espl_status s = lane_matrix(h, g, 0, a0);
+        if (s) return s;
         if (!factor_tape(g.n, g.col_ptr.data(), g.row_idx.data(), a0.data(), g.q, g.tape))
             return fail(h, ESPL_NO_TAPE, "the lead lane's factor is singular");
+        if ((s = upload_tape(h, g))) return s;
+    }
+    espl_status s = h->precision == ESPL_MIXED ? plan_classes<true>(h) : plan_classes<false>(h);
+    if (s) return s;
+    return push_descs(h);
+}
+
+// Lane l's assembled A (the values its last Newton iteration factored).
+espl_status lane_matrix(espl_lanes* h, Group& g, uint32_t l, std::vector<double>& a) {
+    a.assign(g.nnz, 0.0);
+    if (g.nnz)
+        CK(cudaMemcpy2DAsync(a.data(), sizeof(double), g.dev.a + l, sizeof(double) * g.P, sizeof(double), g.nnz,
+                             cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return ESPL_OK;
+}
+
+// The device side of g's tape (g.tape): index arrays, replay program and
+// records, banded plan, and the lanes' factor arrays.
+espl_status upload_tape(espl_lanes* h, Group& g) {
+    {
         for (void* p : g.lu_owned) cudaFree(p);
         g.lu_owned.clear();
         GroupDev& d = g.dev;
@@ -833,9 +856,50 @@ espl_status retape(espl_lanes* h, int tran, double dt) {
             if ((s = dalloc(h, own, &d.ux32, (size_t)d.nnz_u * P))) return s;
         }
     }
-    espl_status s = h->precision == ESPL_MIXED ? plan_classes<true>(h) : plan_classes<false>(h);
-    if (s) return s;
-    return push_descs(h);
+    return ESPL_OK;
+}
+
+// Clears every template's stale-tape words.
+espl_status clear_stale(espl_lanes* h) {
+    std::vector<uint32_t> w(2 * h->groups.size());
+    for (size_t i = 0; i < h->groups.size(); i++) {
+        w[2 * i] = 0;
+        w[2 * i + 1] = 0xFFFFFFFFu;
+    }
+    CK(cudaMemcpyAsync(h->d_stale, w.data(), w.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return ESPL_OK;
+}
+
+// After a solve or a launch (stream idle): every template whose tape went
+// stale is retaped from its flagged lane's matrix, factored on the host
+// (retapeFrom, lanes.zig:1700-1752); a singular factor leaves the tape as
+// it was. The lanes' next refactor fills the new factor arrays.
+espl_status retape_stale(espl_lanes* h) {
+    std::vector<uint32_t> w(2 * h->groups.size());
+    CK(cudaMemcpyAsync(w.data(), h->d_stale, w.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    bool any = false;
+    for (size_t i = 0; i < h->groups.size(); i++) {
+        Group& g = h->groups[i];
+        const uint32_t l = w[2 * i + 1];
+        if (!w[2 * i] || l >= g.lanes) continue;
+        std::vector<double> a;
+        espl_status s = lane_matrix(h, g, l, a);
+        if (s) return s;
+        Tape t;
+        if (!factor_tape(g.n, g.col_ptr.data(), g.row_idx.data(), a.data(), g.q, t)) continue;
+        g.tape = std::move(t);
+        if ((s = upload_tape(h, g))) return s;
+        h->stats.retapes++;
+        any = true;
+    }
+    if (any) {
+        espl_status s = h->precision == ESPL_MIXED ? plan_classes<true>(h) : plan_classes<false>(h);
+        if (s) return s;
+        if ((s = push_descs(h))) return s;
+    }
+    return clear_stale(h);
 }
 
 NewtonParams newton_params(const espl_newton_opts& o, uint32_t precision, uint32_t refine) {
@@ -951,6 +1015,9 @@ espl_status espl_create(const espl_netlist* nets, uint32_t n_nets, const espl_cr
     if (cudaMalloc(&h->d_state, sizeof(LaneState) * h->total_lanes) != cudaSuccess) return bail(ESPL_OUT_OF_MEMORY);
     if (cudaMalloc(&h->d_mos_raw, sizeof(double*) * n_nets) != cudaSuccess) return bail(ESPL_OUT_OF_MEMORY);
     if (cudaMalloc(&h->d_dio_raw, sizeof(double*) * n_nets) != cudaSuccess) return bail(ESPL_OUT_OF_MEMORY);
+    if (cudaMalloc(&h->d_stale, sizeof(uint32_t) * 2 * n_nets) != cudaSuccess) return bail(ESPL_OUT_OF_MEMORY);
+    for (uint32_t i = 0; i < n_nets; i++) h->groups[i].dev.stale = h->d_stale + 2 * i;
+    if (clear_stale(h)) return bail(ESPL_DRIVER);
     cudaMemsetAsync(h->d_state, 0, sizeof(LaneState) * h->total_lanes, h->stream);
     cudaMemcpyAsync(h->d_warp_group, wg.data(), sizeof(uint32_t) * wg.size(), cudaMemcpyHostToDevice, h->stream);
     cudaMemcpyAsync(h->d_mos_raw, mr.data(), sizeof(double*) * n_nets, cudaMemcpyHostToDevice, h->stream);
@@ -979,6 +1046,7 @@ espl_status espl_destroy(espl_lanes* h) {
     cudaFree(h->d_state);
     cudaFree(h->d_mos_raw);
     cudaFree(h->d_dio_raw);
+    cudaFree(h->d_stale);
     free_classes(h);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
@@ -1046,6 +1114,7 @@ espl_status espl_solve_static(espl_lanes* h, const espl_newton_opts* opts, espl_
     NewtonParams np = newton_params(*opts, h->precision, h->refine_sweeps);
     espl_status s = run_static(h, np, 0);
     if (s) return s;
+    if ((s = retape_stale(h))) return s;
     if (out) {
         CK(cudaMemcpyAsync(h->h_state.data(), h->d_state, sizeof(LaneState) * h->total_lanes, cudaMemcpyDeviceToHost,
                            h->stream));
@@ -1107,6 +1176,7 @@ espl_status espl_init_steps(espl_lanes* h, const espl_tran_opts* o) {
     double dt_first = o->fixed_step ? o->dt : std::min(std::min(o->dt, o->t_stop / 100.0) / 10.0, t.dt_max) / 10.0;
     s = retape(h, 1, dt_first);
     if (s) return s;
+    if ((s = clear_stale(h))) return s;
     k_tran_init<<<grid_of(h), kBlock, 0, h->stream>>>(launch_map(h), t, h->d_state);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(h->stream));
@@ -1141,6 +1211,7 @@ espl_status espl_device_launch(espl_lanes* h, uint32_t max_steps, espl_step_repo
     h->stats.newton_ms = ms;
     h->stats.total_ms += ms;
     h->stats.launches += (uint32_t)h->classes.size();
+    if ((s = retape_stale(h))) return s;
     CK(cudaMemcpyAsync(h->h_state.data(), h->d_state, sizeof(LaneState) * h->total_lanes, cudaMemcpyDeviceToHost,
                        h->stream));
     CK(cudaStreamSynchronize(h->stream));
@@ -1199,7 +1270,6 @@ espl_status espl_get_stats(espl_lanes* h, espl_stats* out) {
     for (auto& g : h->groups)
         for (uint32_t l = 0; l < g.lanes; l++) peels += h->h_state[g.lane0 + l].peels;
     h->stats.dense_peels = (uint32_t)std::min<uint64_t>(peels, 0xFFFFFFFFu);
-    h->stats.peel_overflow = 0;
     *out = h->stats;
     return ESPL_OK;
 }

@@ -91,6 +91,10 @@ struct GroupDev {
     uint32_t n_gi, n_items;
     uint32_t gsplit4[5], gsplit16[17];
     uint32_t gsplit_pad[2];
+    // Stale-tape words of the template: [0] set when, in some Newton
+    // iteration, at least half of a tile's active lanes failed the replay;
+    // [1] the smallest such failing lane (the host retapes from its A).
+    uint32_t* stale;
     uint32_t stage_mode;  // what a tile stages in shared memory (lane_smem.cuh)
     uint32_t refine_rows; // the row view is staged (FP32 refinement sweeps on)
 };

@@ -156,6 +156,7 @@ __device__ __forceinline__ void newton_tile(const TileCtx& c, LaneState* s, cons
         // lanes in the tile's precision (FP32 lanes of a mixed tile, or FP64).
         int band_rc = -1;
         bool band_solved = false;
+        bool failed = false;  // the lane's replay failed this iteration (it peels)
         if (!sm && d.band_ok) {
             const bool comp = warp == 0 && act && (!MIXED || !s->fp64);
             band_rc = band_refactor<T>(d, warp, lane, l, comp);
@@ -187,10 +188,13 @@ __device__ __forceinline__ void newton_tile(const TileCtx& c, LaneState* s, cons
                             solve_smem<T>(d, st, lane, l);
                         if (MIXED)
                             for (uint32_t r = 0; r < o.refine; r++) refine_smem(d, st, lane, l);
-                    } else if (!peel_dense(d, l, *s)) {
-                        sh.bits[lane] |= kSingular;
-                        sh.active[lane] = 0;
-                        s->iterations = it;
+                    } else {
+                        failed = true;
+                        if (!peel_dense(d, l, *s)) {
+                            sh.bits[lane] |= kSingular;
+                            sh.active[lane] = 0;
+                            s->iterations = it;
+                        }
                     }
                     done = true;
                 }
@@ -207,6 +211,7 @@ __device__ __forceinline__ void newton_tile(const TileCtx& c, LaneState* s, cons
                     fail = rc == 1 || (rc == 2 && !replay_holds64(d, l));
                 }
                 if (fail) {
+                    failed = true;
                     if (!peel_dense(d, l, *s)) {
                         sh.bits[lane] |= kSingular;
                         sh.active[lane] = 0;
@@ -218,6 +223,17 @@ __device__ __forceinline__ void newton_tile(const TileCtx& c, LaneState* s, cons
                 } else {
                     solve64(d, l, d.rhs, d.dx);
                 }
+            }
+        }
+        // A stale tape (lanes.zig:1573-1591, per tile and iteration here):
+        // when at least half of the tile's active lanes failed the replay,
+        // the host rebuilds the template's tape from a failing lane's matrix
+        // after the launch.
+        if (warp == 0 && d.stale) {
+            const unsigned am = __ballot_sync(0xffffffffu, act), fm = __ballot_sync(0xffffffffu, act && failed);
+            if (lane == 0 && fm && 2u * (unsigned)__popc(fm) >= (unsigned)__popc(am)) {
+                atomicOr(&d.stale[0], 1u);
+                atomicMin(&d.stale[1], (c.tile - d.tile0) * 32u + (uint32_t)(__ffs(fm) - 1));
             }
         }
         __syncthreads();

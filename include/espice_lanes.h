@@ -222,7 +222,10 @@ typedef struct {
     uint64_t lane_iterations;
     uint64_t lane_steps;
     uint32_t dense_peels;     /* dense re-pivoting solves of failed replays, since the last reset */
-    uint32_t peel_overflow;   /* reserved (0) */
+    uint32_t retapes;         /* tapes rebuilt from a failing lane since create: after a solve or a
+                               * launch in which, in some Newton iteration, at least half of a
+                               * tile's active lanes failed the replay (the reference's stale-tape
+                               * retape, lanes.zig:1573-1591,1700-1752, per tile here) */
 } espl_stats;
 espl_status espl_get_stats(espl_lanes *h, espl_stats *out);
 

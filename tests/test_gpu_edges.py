@@ -42,8 +42,11 @@ def test_ragged_lane_counts_cold_operating_points(oracle, precision):
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_dense_peel_past_64_unknowns(oracle, precision):
     """The 63-stage ring (66 unknowns): from the cold start the replay of the
-    lead lane's tape fails on some lanes, which re-pivot densely on the
-    device instead of reporting singular."""
+    lead lane's tape fails on the lanes, which re-pivot densely on the device
+    instead of reporting singular. Most of a tile's lanes failing in one
+    iteration marks the tape stale, so the solve ends with a tape rebuilt
+    from a failing lane's matrix (the reference's retapeFrom); a warm solve
+    from the answer runs on it."""
     net = decks.ring_oscillator(32, stages=63)
     assert net.n > 64
     opts = abi.newton_opts()
@@ -51,12 +54,20 @@ def test_dense_peel_past_64_unknowns(oracle, precision):
     with Lanes([net], precision=precision) as L:
         r = L.solve_static(opts)
         x = L.get_x(0)
-        peels = L.stats().dense_peels
-    print(f"dense peels: {peels}")
+        st = L.stats()
+        peels, retapes = st.dense_peels, st.retapes
+        L.put_x(0, x, False)
+        r2 = L.solve_static(abi.newton_opts(init_fix=0))
+        x2 = L.get_x(0)
+        peels2 = L.stats().dense_peels
+    print(f"dense peels: {peels}, retapes: {retapes}, warm solve's dense peels: {peels2}")
     assert (ro[:, 0] == 1).all()
     assert ((r[:, 0] & abi.CONVERGED) != 0).all(), r[:, 0]
     assert ((r[:, 0] & abi.SINGULAR) == 0).all()
     assert worst(x, xo) <= 1.0
+    assert retapes >= 1
+    assert ((r2[:, 0] & abi.CONVERGED) != 0).all(), r2[:, 0]
+    assert worst(x2, xo) <= 1.0
 
 
 def test_ragged_lane_counts_transient(oracle):
