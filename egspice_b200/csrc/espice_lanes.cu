@@ -416,6 +416,7 @@ espl_status alloc_group(espl_lanes* h, Group& g) {
                 put(qp, qf, i, kGiCellC);
                 ie.push_back((kGiQ1 << kGiKindShift) | i);
                 ie.push_back((kGiIp << kGiKindShift) | i);
+                ie.push_back((kGiQ2 << kGiKindShift) | i);
                 ie.push_back((kGiX << kGiKindShift) | i);
                 ip.push_back((uint32_t)ie.size());
             }
@@ -520,6 +521,7 @@ espl_status alloc_group(espl_lanes* h, Group& g) {
     AL(lim_mos, 3 * (size_t)d.n_mos * P);
     AL(lim_dio, (size_t)d.n_dio * P);
     AL(q1, n1 * P);
+    AL(q2, n1 * P);
     AL(ip, n1 * P);
     AL(cur, n1 * P);
     AL(prev, n1 * P);
@@ -1138,7 +1140,7 @@ espl_status espl_solve_static(espl_lanes* h, const espl_newton_opts* opts, espl_
 
 espl_status espl_init_steps(espl_lanes* h, const espl_tran_opts* o) {
     if (!h || !o) return ESPL_INVALID_ARGUMENT;
-    if (!(o->t_stop > 0) || !(o->dt > 0) || o->max_iter == 0 || o->method > 1)
+    if (!(o->t_stop > 0) || !(o->dt > 0) || o->max_iter == 0 || o->method > 2)
         return fail(h, ESPL_INVALID_ARGUMENT, "bad transient options");
     TranParams& t = h->tran;
     t.t_stop = o->t_stop;

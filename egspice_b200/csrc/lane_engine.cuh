@@ -69,7 +69,7 @@ struct GroupDev {
     uint32_t mos_uni, mos_uni_pad;
     double *x, *x_old, *dx, *rhs, *qrow, *g, *c, *a, *lx, *ux, *udiag, *w, *y, *lim_mos, *lim_dio;
     float *lx32, *ux32, *udiag32, *w32, *y32;
-    double *q1, *ip, *cur, *prev, *sring, *sip;
+    double *q1, *q2, *ip, *cur, *prev, *sring, *sip;  // q2: row charges two accepted steps back (gear-2)
     double *rr, *corr;
     double* peel_m;      // n <= kDensePeelMax: the lanes' dense peel scratch (peel_doubles(n) per lane)
     uint32_t* peel_i;    // n <= kDensePeelMax: its index words (peel_words(n) per lane)
@@ -84,7 +84,7 @@ struct GroupDev {
     // The same sums as one flat list for the Newton gather (lane_tile.cuh
     // gather_items): items are the nnz slots, then the n rows; an item's
     // entries (gi_ptr[k] .. gi_ptr[k + 1]) are its G (R) cells, its C (Q)
-    // cells, and for a row the q1, ip and x values its companion and gmin
+    // cells, and for a row the q1, ip, q2 and x values its companion and gmin
     // terms read. Each warp of a tile takes a run of items with about the
     // same number of entries: gsplit4 for 4-warp tiles, gsplit16 for 16.
     const uint32_t *gi_ptr, *gi_ent;
@@ -126,8 +126,8 @@ struct TranParams {
 
 struct Companion {
     int on;
-    uint32_t method;  // 0 BE, 1 trap
-    double ag0, ag1;
+    uint32_t method;  // 0 BE, 1 trap, 2 gear-2
+    double ag0, ag1, ag2;
 };
 
 #define LM(arr, i) (arr)[(size_t)(i) * P + l]

@@ -47,7 +47,7 @@ struct TileShared {
     uint32_t cbuf[32];  // the cells buffer of a converged lane's published iterate
     unsigned long long acc0[32], acc1[32], acc2[32];
     double limit[32];
-    double ag0[32], ag1[32], t[32], xfact[32], dt_next[32];
+    double ag0[32], ag1[32], ag2[32], t[32], xfact[32], dt_next[32];
     uint32_t method[32], on[32], accept[32], rot[32];
 };
 
@@ -94,13 +94,14 @@ __device__ __forceinline__ void newton_tile(const TileCtx& c, LaneState* s, cons
     for (uint32_t it = 0; it < o.max_iter; it++) {
         bool act = c.valid && sh.active[lane];
         if (!__syncthreads_or(act)) break;
-        Companion cp{0, 0, 0.0, 0.0};
+        Companion cp{0, 0, 0.0, 0.0, 0.0};
         double tm = 0.0;
         if (tran_companion) {
             cp.on = 1;
             cp.method = sh.method[lane];
             cp.ag0 = sh.ag0[lane];
             cp.ag1 = sh.ag1[lane];
+            cp.ag2 = sh.ag2[lane];
             tm = sh.t[lane];
         }
         const double* cells = cell_buf(d, cur);
@@ -379,7 +380,7 @@ __global__ void __launch_bounds__(kTileThreads) k_assemble(TileMap m, int tran, 
     if (c.valid)
         for (uint32_t t = c.warp; t < n_instances(d); t += nw) inst_eval(d, c.l, t, tran, 0.0, cell_buf(d, 0));
     __syncthreads();
-    Companion cp{inv_dt > 0.0 ? 1 : 0, 0, inv_dt, 1.0};
+    Companion cp{inv_dt > 0.0 ? 1 : 0, 0, inv_dt, 1.0, 0.0};
     if (c.valid)
         for (uint32_t p = c.warp; p < d.nnz; p += nw) gather_slot(d, c.l, p, cp, 0.0, cell_buf(d, 0));
 }
@@ -435,7 +436,8 @@ __device__ __forceinline__ double* ring_slot(const GroupDev& d, uint32_t rot, ui
 // method's result (bad0, bad1).
 __device__ void step_bound_part(const GroupDev& d, uint32_t l, uint32_t rot, uint32_t m0, uint32_t m1, bool two,
                                 uint32_t cur_method, double dt, double dt1, double dt2, double reltol, double abstol,
-                                double chgtol, double trtol, double ag0, double ag1, uint32_t j0, uint32_t stride,
+                                double chgtol, double trtol, double ag0, double ag1, double ag2, uint32_t j0,
+                                uint32_t stride,
                                 double& v0, double& v1, bool& bad0, bool& bad1) {
     const uint32_t P = d.P;
     const uint32_t ns = d.n_sites;
@@ -446,7 +448,9 @@ __device__ void step_bound_part(const GroupDev& d, uint32_t l, uint32_t rot, uin
     const double *r2 = ring_slot(d, rot, 2), *r3 = ring_slot(d, rot, 3);
     for (uint32_t j = j0; j < ns; j += stride) {
         double qc = LM(r0, j), qp = LM(r1, j), qp2 = LM(r2, j), qp3 = LM(r3, j), i_p = LM(d.sip, j);
-        double i_new = cur_method == 1 ? ag0 * (qc - qp) - ag1 * i_p : ag0 * (qc - qp);
+        double i_new = cur_method == 1   ? ag0 * (qc - qp) - ag1 * i_p
+                       : cur_method == 2 ? ag0 * (qc - qp) - ag2 * (qp - qp2)
+                                         : ag0 * (qc - qp);
         double volttol = abstol + reltol * fmax(fabs(i_new), fabs(i_p));
         double chargetol = reltol * fmax(fmax(fabs(qc), fabs(qp)), chgtol) / dt;
         double tol = fmax(volttol, chargetol);
@@ -489,6 +493,7 @@ __global__ void __launch_bounds__(kTileThreads) k_tran_init(TileMap m, TranParam
         LM(d.cur, i) = LM(d.x, i);
         LM(d.prev, i) = LM(d.x, i);
         LM(d.q1, i) = LM(d.qrow, i);
+        LM(d.q2, i) = LM(d.qrow, i);
         LM(d.ip, i) = 0.0;
     }
     for (uint32_t j = c.warp; j < d.n_sites; j += nw) {
@@ -558,8 +563,20 @@ __global__ void __launch_bounds__(WIDE ? kWideThreads : kTileThreads, WIDE ? 1 :
                     double dt = s->dt;
                     uint32_t method = s->order == 1 ? 0 : o.method;
                     sh.method[lane] = method;
-                    if (method == 0) { sh.ag0[lane] = 1.0 / dt; sh.ag1[lane] = 1.0; }
-                    else { sh.ag0[lane] = 1.0 / dt / (1.0 - 0.5); sh.ag1[lane] = 0.5 / (1.0 - 0.5); }
+                    // integrator.zig coeffs (src/analysis/tran/integrator.zig:39-52)
+                    sh.ag2[lane] = 0.0;
+                    if (method == 0) {
+                        sh.ag0[lane] = 1.0 / dt;
+                        sh.ag1[lane] = 1.0;
+                    } else if (method == 1) {
+                        sh.ag0[lane] = 1.0 / dt / (1.0 - 0.5);
+                        sh.ag1[lane] = 0.5 / (1.0 - 0.5);
+                    } else {  // gear-2, the variable-step BDF2
+                        const double r = dt / s->dt_old0;
+                        sh.ag0[lane] = (1.0 + 2.0 * r) / ((1.0 + r) * dt);
+                        sh.ag2[lane] = r * r / ((1.0 + r) * dt);
+                        sh.ag1[lane] = 1.0;
+                    }
                     sh.t[lane] = s->t + dt;
                     sh.xfact[lane] = dt / s->dt_old0;
                     sh.rot[lane] = s->s_rot;
@@ -613,7 +630,7 @@ __global__ void __launch_bounds__(WIDE ? kWideThreads : kTileThreads, WIDE ? 1 :
                 if (ls.steps > 0) {
                     uint32_t method = sh.method[lane];
                     step_bound_part(d, l, ls.s_rot, method, o.method, method == 0, method, ls.dt, ls.dt_old0,
-                                    ls.dt_old1, o.reltol, o.abstol, o.chgtol, o.trtol, sh.ag0[lane], sh.ag1[lane],
+                                    ls.dt_old1, o.reltol, o.abstol, o.chgtol, o.trtol, sh.ag0[lane], sh.ag1[lane], sh.ag2[lane],
                                     warp, nw, v0, v1, b0, b1);
                 }
             }
@@ -686,20 +703,25 @@ __global__ void __launch_bounds__(WIDE ? kWideThreads : kTileThreads, WIDE ? 1 :
         // Accept (lane_device.zig accept): row histories and companion currents.
         bool acc = c.valid && sh.accept[lane];
         if (acc) {
-            double ag0 = sh.ag0[lane], ag1 = sh.ag1[lane];
+            double ag0 = sh.ag0[lane], ag1 = sh.ag1[lane], ag2 = sh.ag2[lane];
             uint32_t method = sh.method[lane];
             for (uint32_t i = warp; i < d.n; i += nw) {
-                double dq = ag0 * (LM(d.qrow, i) - LM(d.q1, i));
-                LM(d.ip, i) = method == 1 ? dq - ag1 * LM(d.ip, i) : dq;
+                const double q1 = LM(d.q1, i);
+                double dq = ag0 * (LM(d.qrow, i) - q1);
+                LM(d.ip, i) = method == 1 ? dq - ag1 * LM(d.ip, i) : method == 2 ? dq - ag2 * (q1 - LM(d.q2, i)) : dq;
+                LM(d.q2, i) = q1;
                 LM(d.q1, i) = LM(d.qrow, i);
                 LM(d.prev, i) = LM(d.cur, i);
                 LM(d.cur, i) = LM(d.x, i);
             }
             const double* q0 = ring_slot(d, sh.rot[lane], 0);
             const double* q1 = ring_slot(d, sh.rot[lane], 1);
+            const double* q2 = ring_slot(d, sh.rot[lane], 2);
             for (uint32_t j = warp; j < ns; j += nw) {
                 double dq = ag0 * (LM(q0, j) - LM(q1, j));
-                LM(d.sip, j) = method == 1 ? dq - ag1 * LM(d.sip, j) : dq;
+                LM(d.sip, j) = method == 1   ? dq - ag1 * LM(d.sip, j)
+                               : method == 2 ? dq - ag2 * (LM(q1, j) - LM(q2, j))
+                                             : dq;
             }
         }
         __syncthreads();

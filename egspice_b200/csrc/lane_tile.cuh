@@ -28,7 +28,7 @@ constexpr uint32_t kNeg = 0x80000000u;
 // 28-30 the kind, bits 0-27 a cell, or for a row's q1 / ip / x value the row.
 constexpr uint32_t kGiKindShift = 28;
 constexpr uint32_t kGiIdx = 0x0fffffffu;
-enum : uint32_t { kGiCell = 0, kGiCellC = 1, kGiQ1 = 2, kGiIp = 3, kGiX = 4, kGiNop = 5 };
+enum : uint32_t { kGiCell = 0, kGiCellC = 1, kGiQ1 = 2, kGiIp = 3, kGiX = 4, kGiNop = 5, kGiQ2 = 6 };
 constexpr uint32_t kGiChunk = 12;  // entries whose loads are in flight together
 
 // Cells per instance.
@@ -334,7 +334,7 @@ __device__ __forceinline__ void gather_items(const GroupDev& d, uint32_t l, uint
     const uint32_t* __restrict__ ent = d.gi_ent;
     const uint32_t e_end = ptr[it1];
     uint32_t it = it0, nxt = ptr[it0 + 1];
-    double s0 = 0.0, s1 = 0.0, xq1 = 0.0, xip = 0.0, xx = 0.0;
+    double s0 = 0.0, s1 = 0.0, xq1 = 0.0, xip = 0.0, xx = 0.0, xq2 = 0.0;
     for (uint32_t e = ptr[it0]; e < e_end; e += kGiChunk) {
         uint32_t w[kGiChunk];
         double v[kGiChunk];
@@ -343,7 +343,7 @@ __device__ __forceinline__ void gather_items(const GroupDev& d, uint32_t l, uint
 #pragma unroll
         for (int j = 0; j < (int)kGiChunk; j++) {
             const uint32_t k = (w[j] >> kGiKindShift) & 7u;
-            const double* b = k == kGiQ1 ? d.q1 : k == kGiIp ? d.ip : k == kGiX ? d.x : cells;
+            const double* b = k == kGiQ1 ? d.q1 : k == kGiIp ? d.ip : k == kGiX ? d.x : k == kGiQ2 ? d.q2 : cells;
             v[j] = b[(size_t)(w[j] & kGiIdx) * P + l];
         }
         // every entry is consumed without a branch (padding is a no-op
@@ -358,6 +358,7 @@ __device__ __forceinline__ void gather_items(const GroupDev& d, uint32_t l, uint
             xq1 = k == kGiQ1 ? vj : xq1;
             xip = k == kGiIp ? vj : xip;
             xx = k == kGiX ? vj : xx;
+            xq2 = k == kGiQ2 ? vj : xq2;
             if (e + j + 1 == nxt) {
                 if (it < d.nnz) {
                     double a = s0;
@@ -373,7 +374,7 @@ __device__ __forceinline__ void gather_items(const GroupDev& d, uint32_t l, uint
                         LM(d.qrow, i) = q;
                         double dq = cp.ag0 * (q - xq1);
                         double base = r + dq;
-                        r = cp.method == 1 ? base - cp.ag1 * xip : base;
+                        r = cp.method == 1 ? base - cp.ag1 * xip : cp.method == 2 ? base - cp.ag2 * (xq1 - xq2) : base;
                     }
                     if (gmin > 0.0) r += gmin * xx;
                     LM(d.rhs, i) = r;

@@ -179,7 +179,7 @@ typedef struct {
     double dt_min;
     double dt_max;
     double reltol, abstol, chgtol, trtol, vntol, residual_tol;
-    uint32_t method;     /* 0 BE, 1 trapezoidal (order 1 first, then 2) */
+    uint32_t method;     /* 0 BE, 1 trapezoidal, 2 gear-2 (variable-step BDF2); order 1 (BE) first, then 2 */
     uint32_t fixed_step; /* 1: no LTE control, every step dt */
     uint32_t max_iter;   /* Newton iterations per step (ITL4-like) */
     uint32_t max_steps;

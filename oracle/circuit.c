@@ -449,9 +449,10 @@ static int residual_ok(const ockt *k, const espl_newton_opts *o, const double *r
 /* Companion state of a transient attempt. */
 typedef struct {
     int on;
-    uint32_t method; /* 0 BE, 1 trap */
-    double ag0, ag1;
+    uint32_t method; /* 0 BE, 1 trap, 2 gear-2 */
+    double ag0, ag1, ag2;
     const double *q1;     /* row charges at the last accepted step */
+    const double *q2;     /* and at the one before (gear-2) */
     const double *i_prev; /* row companion currents there */
 } companion;
 
@@ -467,7 +468,9 @@ static orc_newton_result newton(ockt *k, double *x, const espl_newton_opts *o, i
             for (uint32_t i = 0; i < k->n; i++) {
                 double d = cp->ag0 * (k->q[i] - cp->q1[i]);
                 double base = k->rhs[i] + d;
-                k->rhs[i] = cp->method == 1 ? base - cp->ag1 * cp->i_prev[i] : base;
+                k->rhs[i] = cp->method == 1   ? base - cp->ag1 * cp->i_prev[i]
+                            : cp->method == 2 ? base - cp->ag2 * (cp->q1[i] - cp->q2[i])
+                                              : base;
             }
             for (uint32_t p = 0; p < k->nnz; p++) k->a[p] = k->g[p] + cp->ag0 * k->c[p];
             v = k->a;
@@ -594,10 +597,20 @@ int orc_op_lanes(const espl_netlist *net, uint32_t lane0, uint32_t count, const 
 
 /* ---------------- transient ---------------- */
 
-/* kernels/lane.zig coeffs over method codes (BE, trap). */
-static void coeffs(uint32_t method, double dt, double xmu, double *ag0, double *ag1) {
+/* kernels/lane.zig coeffs over method codes (BE, trap, gear-2), after
+ * integrator.zig coeffs (src/analysis/tran/integrator.zig:39-52): gear-2 is
+ * the variable-step BDF2 with r = dt / dt_prev, ag0 = (1 + 2r) / ((1 + r) dt),
+ * ag2 = r^2 / ((1 + r) dt); ag1 defaults to 1. */
+static void coeffs(uint32_t method, double dt, double dt_prev, double xmu, double *ag0, double *ag1, double *ag2) {
+    *ag2 = 0;
     if (method == 0) { *ag0 = 1.0 / dt; *ag1 = 1; }
-    else { *ag0 = 1.0 / dt / (1.0 - xmu); *ag1 = xmu / (1.0 - xmu); }
+    else if (method == 1) { *ag0 = 1.0 / dt / (1.0 - xmu); *ag1 = xmu / (1.0 - xmu); }
+    else {
+        double r = dt / dt_prev;
+        *ag0 = (1.0 + 2.0 * r) / ((1.0 + r) * dt);
+        *ag2 = r * r / ((1.0 + r) * dt);
+        *ag1 = 1;
+    }
 }
 
 double orc_step_bound(uint32_t method, uint32_t cur_method, const double *q0, const double *q1, const double *q2,
@@ -722,7 +735,7 @@ static void tran_one(job_t *j, uint32_t li) {
     }
     double dt_old[6];
     for (int i = 0; i < 6; i++) dt_old[i] = o->fixed_step ? o->dt : dt_max;
-    uint32_t order = 1, top = o->method; /* top: 0 BE, 1 trap */
+    uint32_t order = 1, top = o->method; /* top: 0 BE, 1 trap, 2 gear-2 */
     uint32_t steps = 0;
     double bp_next = o->fixed_step ? INFINITY : next_bp(k, 0.0);
     double bp_save_dt = 0;
@@ -738,8 +751,8 @@ static void tran_one(job_t *j, uint32_t li) {
     while (1) {
         if (!(t < o->t_stop && !at_stop(t, o->t_stop) && steps < o->max_steps)) { rep->status = 1; break; }
         uint32_t method = (order == 1) ? 0 : top;
-        double ag0, ag1;
-        coeffs(method, dt, 0.5, &ag0, &ag1);
+        double ag0, ag1, ag2;
+        coeffs(method, dt, dt_old[0], 0.5, &ag0, &ag1, &ag2);
         double t_dev = t + dt;
         /* Predictor (lane_device.zig predict): trial = cur + xfact (cur - prev). */
         double xfact = dt / dt_old[0];
@@ -756,7 +769,9 @@ static void tran_one(job_t *j, uint32_t li) {
         cp.method = method;
         cp.ag0 = ag0;
         cp.ag1 = ag1;
+        cp.ag2 = ag2;
         cp.q1 = q1;
+        cp.q2 = q2;
         cp.i_prev = ip;
         espl_newton_opts no = {o->reltol, o->abstol, o->vntol, 0.0, o->residual_tol, o->max_iter, 0};
         orc_newton_result nr = newton(k, x, &no, 1, t_dev, &cp, NULL);
@@ -779,7 +794,7 @@ static void tran_one(job_t *j, uint32_t li) {
             dt_next = steps == 0 ? dt : fmin(dt * 2.0, dt_max);
             int lte_reject = 0;
             if (!o->fixed_step && ns > 0 && steps > 0) {
-                double lin[10] = {dt, dt_old[0], dt_old[1], o->reltol, o->abstol, o->chgtol, o->trtol, ag0, ag1, 0};
+                double lin[10] = {dt, dt_old[0], dt_old[1], o->reltol, o->abstol, o->chgtol, o->trtol, ag0, ag1, ag2};
                 double del = orc_step_bound(method, method, s0, s1, s2, s3, sip, ns, lin);
                 double del2 = method == 0 ? orc_step_bound(top, method, s0, s1, s2, s3, sip, ns, lin) : del;
                 if (!(del >= 0.9 * dt)) {
@@ -816,14 +831,14 @@ static void tran_one(job_t *j, uint32_t li) {
         /* Accept: histories (lane_device.zig accept). */
         for (uint32_t i = 0; i < n1; i++) {
             double d = ag0 * (k->q[i] - q1[i]);
-            double nip = method == 1 ? d - ag1 * ip[i] : d;
+            double nip = method == 1 ? d - ag1 * ip[i] : method == 2 ? d - ag2 * (q1[i] - q2[i]) : d;
             ip[i] = nip;
             q2[i] = q1[i];
             q1[i] = k->q[i];
         }
         for (uint32_t s = 0; s < ns; s++) {
             double d = ag0 * (s0[s] - s1[s]);
-            sip[s] = method == 1 ? d - ag1 * sip[s] : d;
+            sip[s] = method == 1 ? d - ag1 * sip[s] : method == 2 ? d - ag2 * (s1[s] - s2[s]) : d;
         }
         {
             double *tmp = s3; s3 = s2; s2 = s1; s1 = s0; s0 = tmp;

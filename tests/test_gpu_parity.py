@@ -74,11 +74,14 @@ def test_uneven_ladders_one_launch(oracle, precision):
         assert worst(x, xo) <= 1.0, nl.name
 
 
-def test_rc_points_lte_control(oracle):
+@pytest.mark.parametrize("method", [1, 2])
+def test_rc_points_lte_control(oracle, method):
+    """Trapezoidal (1) and gear-2 (2) steps under LTE control: the same
+    accepted and rejected steps as the oracle, lane by lane."""
     r = np.array([1e3, 2e3, 5e3, 1e4])
     c = np.array([1e-12, 0.5e-12, 2e-13, 2e-13])
     net = decks.rc_points(4, r, c, tr=0.2e-9)
-    opts = abi.tran_opts(t_stop=8e-9, dt=1e-12, dt_max=20e-12, method=1, max_iter=20, reltol=1e-4)
+    opts = abi.tran_opts(t_stop=8e-9, dt=1e-12, dt_max=20e-12, method=method, max_iter=20, reltol=1e-4)
     with Lanes([net]) as L:
         reps = L.run_tran(opts, steps_per_launch=4096)
         x = L.get_x(0)
@@ -88,10 +91,11 @@ def test_rc_points_lte_control(oracle):
     assert worst(x, xo) <= 1.0
 
 
-def test_ring_oscillator_period(oracle):
+@pytest.mark.parametrize("method", [1, 2])
+def test_ring_oscillator_period(oracle, method):
     net = decks.ring_oscillator(16, stages=15)
     out = net.node("s3")
-    opts = abi.tran_opts(t_stop=3e-9, dt=1e-12, dt_max=5e-12, method=1, max_iter=20)
+    opts = abi.tran_opts(t_stop=3e-9, dt=1e-12, dt_max=5e-12, method=method, max_iter=20)
     with Lanes([net]) as L:
         L.set_period_meas(0, out, 0.9, 0.5e-9)
         reps = L.run_tran(opts, steps_per_launch=2048)

@@ -86,3 +86,27 @@ def test_ladder_fixed_step_transient(oracle):
     x, reps, _, _ = oracle.tran_lanes(net, opts)
     assert all(r.status == 1 and r.steps == 100 for r in reps)
     assert np.all(x[:, net.node("n1")] > 0.05)
+
+
+def test_gear2_fixed_step_order(oracle):
+    """Gear-2 (variable-step BDF2, integrator.zig coeffs) on an RC low pass
+    after a ramp: halving the fixed step cuts the error against the analytic
+    response by about 4 (second order), as for the trapezoid, where backward
+    Euler's error halves."""
+    r, c, tr, t_end = np.array([1e3]), np.array([1e-12]), 0.2e-9, 1e-9
+    net = decks.rc_points(1, r, c, tr=tr)
+    out = net.node("out")
+    rc = r[0] * c[0]
+    exact = 1 - (rc / tr) * (math.exp(tr / rc) - 1) * math.exp(-t_end / rc)
+    ratios = {}
+    for method in (0, 1, 2):
+        err = []
+        for dt in (20e-12, 10e-12, 5e-12):
+            x, reps, _, _ = oracle.tran_lanes(net, abi.tran_opts(t_stop=t_end, dt=dt, fixed_step=1, method=method,
+                                                                 max_iter=50))
+            assert reps[0].status == 1
+            err.append(abs(x[0, out] - exact))
+        ratios[method] = (err[0] / err[1], err[1] / err[2])
+    assert all(1.8 < q < 2.2 for q in ratios[0]), ratios
+    assert all(3.6 < q < 4.4 for q in ratios[1]), ratios
+    assert all(3.6 < q < 4.4 for q in ratios[2]), ratios
