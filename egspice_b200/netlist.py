@@ -1,0 +1,361 @@
+"""A reader for the SPICE decks the lane sweep runs (ngspice syntax).
+
+The front end on the input side of the path: deck text in, the frozen MNA
+pattern and per-kind device batches out (what the reference gets from
+src/frontend/netlist.zig `parse` and `Circuit.freeze`), as an
+`egspice_b200.decks.Netlist` that `Lanes` takes directly. It reads the subset
+the lanes carry:
+
+* R, C            ``Rname n1 n2 value``
+* V, I            ``Vname n+ n- [DC] value [PULSE(v1 v2 td tr tf pw per)]``
+* D               ``Dname anode cathode model``
+* M (level 1)     ``Mname d g s b model [W=value] [L=value]``
+* ``.model name nmos|pmos|d (params)`` — MOS: LEVEL=1, VTO, KP, GAMMA, PHI,
+  LAMBDA, IS (TOX, RD, RS must be absent or zero: the lanes carry no Meyer
+  capacitances and no series resistances); diode: IS, N, CJO, VJ, M, FC, TT
+  (RS absent or zero)
+* ``.param name=value``; values anywhere may be numbers with SPICE scale
+  suffixes (t g meg k m u n p f a mil), parameter names, or ``{expression}``
+  over numbers, parameters, + - * / ** and parentheses
+* ``+`` continuation lines, ``*`` comment lines, ``;`` and ``$ `` inline
+  comments; the first line is the title; ``.end`` ends the deck; analysis
+  cards (.op .tran .dc .option .options .temp .meas .print .save .probe) are
+  accepted and ignored (the caller runs the analysis through the API).
+
+Per-lane values: `params` maps parameter names to a scalar or to an array of
+one value per lane (a Monte Carlo draw or a sweep); they override `.param`
+cards, and any expression that reads one becomes per-lane. The arrays also
+form the netlist's sweep matrix (the learned warm start's inputs), in the
+order given. Numbers read as ngspice's INPevaluate reads them (every digit
+into one mantissa, then times a correctly rounded power of ten), so a value
+is bit for bit the value the reference parses from the same text. Anything
+outside the subset raises `DeckError` naming the line.
+"""
+from __future__ import annotations
+
+import ast
+import math
+import operator
+import re
+from typing import Dict, List, Mapping, Optional, Sequence, Union
+
+import numpy as np
+
+from .decks import Builder, Netlist
+
+Value = Union[float, np.ndarray]
+
+
+class DeckError(ValueError):
+    pass
+
+
+_SCALE = {"t": 12, "g": 9, "k": 3, "m": -3, "u": -6, "n": -9, "p": -12, "f": -15, "a": -18}
+_NUM = re.compile(r"[+-]?(?:\d+\.?\d*|\.\d+)(?:[eEdD][+-]?\d+)?")
+
+
+def _pow10(e: int) -> float:
+    """10**e as the C library's pow(10, e) gives it to ngspice: correctly
+    rounded except at e = 23 and 210, which it rounds up; 0 below 1e-330 and
+    inf past 1e308."""
+    if e < -330:
+        return 0.0
+    if e > 308:
+        return float("inf")
+    v = float(f"1e{e}")
+    return math.nextafter(v, math.inf) if e in (23, 210) else v
+
+
+def parse_number(text: str) -> Optional[float]:
+    """A SPICE number with its scale suffix (``10meg``, ``2.5u``, ``1mil``),
+    or None when `text` does not start with a number. The digits go into one
+    mantissa and the value is sign * mantissa * 10**exponent, as ngspice's
+    INPevaluate computes it (so ``0.1n`` is 1e-10 exactly as ngspice reads
+    it, not 0.1 * 1e-9)."""
+    t = text.strip().lower()
+    m = _NUM.match(t)
+    if not m:
+        return None
+    lit, rest = m.group(0), t[m.end():]
+    if rest.startswith("meg"):
+        scale, mil = 6, False
+    elif rest.startswith("mil"):
+        scale, mil = -6, True
+    else:
+        scale, mil = (_SCALE.get(rest[0], 0) if rest else 0), False
+    sign = -1.0 if lit.startswith("-") else 1.0
+    body = lit.lstrip("+-")
+    mant, exp = body, 0
+    for sep in "ed":
+        if sep in mant:
+            mant, ex = mant.split(sep)
+            exp = int(ex)
+    e = scale + exp
+    digits = mant
+    if "." in mant:
+        a, b = mant.split(".")
+        digits = a + b
+        e -= len(b)
+    mantissa = 0.0
+    for ch in digits:
+        mantissa = 10.0 * mantissa + float(ord(ch) - 48)
+    if mil:
+        mantissa *= 25.4
+    if mantissa == 0.0:
+        return sign * 0.0
+    return sign * mantissa * _pow10(e)
+
+
+_BINOPS = {ast.Add: operator.add, ast.Sub: operator.sub, ast.Mult: operator.mul, ast.Div: operator.truediv,
+           ast.Pow: operator.pow}
+
+
+class _Env:
+    def __init__(self, lanes: int, params: Mapping[str, Value]):
+        self.lanes = lanes
+        self.vals: Dict[str, Value] = {}
+        for k, v in params.items():
+            a = np.asarray(v, dtype=np.float64)
+            if a.ndim == 0:
+                self.vals[k.lower()] = float(a)
+            elif a.shape == (lanes,):
+                self.vals[k.lower()] = a
+            else:
+                raise DeckError(f"parameter {k}: {a.shape[0]} values for {lanes} lanes")
+        self.given = set(self.vals)
+
+    def value(self, text: str, where: str) -> Value:
+        t = text.strip()
+        if t.startswith("{") and t.endswith("}"):
+            return self.expr(t[1:-1], where)
+        if t.startswith("'") and t.endswith("'"):
+            return self.expr(t[1:-1], where)
+        m = _NUM.match(t.lower())
+        if m and re.fullmatch(r"[a-z]*", t.lower()[m.end():]):
+            return parse_number(t)
+        name = t.lower()
+        if name in self.vals:
+            return self.vals[name]
+        raise DeckError(f"{where}: cannot read the value {text!r}")
+
+    def expr(self, text: str, where: str) -> Value:
+        # every number literal (with its scale suffix) reads as parse_number reads it
+        src = re.sub(r"(?<![\w.])(?:\d+\.?\d*|\.\d+)(?:e[+-]?\d+)?(?:meg|mil|[tgkmunpfa](?![a-z_0-9]))?",
+                     lambda m: repr(parse_number(m.group(0))), text.lower())
+        try:
+            tree = ast.parse(src, mode="eval")
+        except SyntaxError:
+            raise DeckError(f"{where}: cannot parse the expression {{{text}}}") from None
+
+        def ev(n):
+            if isinstance(n, ast.Expression):
+                return ev(n.body)
+            if isinstance(n, ast.Constant) and isinstance(n.value, (int, float)):
+                return float(n.value)
+            if isinstance(n, ast.Name):
+                if n.id in self.vals:
+                    return self.vals[n.id]
+                raise DeckError(f"{where}: unknown parameter {n.id!r}")
+            if isinstance(n, ast.BinOp) and type(n.op) in _BINOPS:
+                return _BINOPS[type(n.op)](ev(n.left), ev(n.right))
+            if isinstance(n, ast.UnaryOp) and isinstance(n.op, (ast.USub, ast.UAdd)):
+                v = ev(n.operand)
+                return -v if isinstance(n.op, ast.USub) else v
+            raise DeckError(f"{where}: unsupported expression {{{text}}}")
+
+        return ev(tree)
+
+
+def _logical_lines(text: str) -> List[tuple]:
+    """(line number, text) of each card: continuations joined, comments cut,
+    lower case; the title line dropped."""
+    raw = text.splitlines()
+    out: List[list] = []
+    for k, line in enumerate(raw[1:], start=2):
+        s = line.strip()
+        if not s or s.startswith("*"):
+            continue
+        for cut in (";", "$ "):
+            i = s.find(cut)
+            if i >= 0:
+                s = s[:i].rstrip()
+        if not s:
+            continue
+        if s.startswith("+"):
+            if not out:
+                raise DeckError(f"line {k}: continuation with nothing to continue")
+            out[-1][1] += " " + s[1:].strip().lower()
+        else:
+            out.append([k, s.lower()])
+    return [tuple(x) for x in out]
+
+
+def _split(card: str) -> List[str]:
+    """Tokens of a card: spaces separate, `=` binds, braces and parentheses
+    keep their contents together."""
+    card = re.sub(r"\s*=\s*", "=", card)
+    toks, cur, depth = [], "", 0
+    for ch in card:
+        if ch in "{(":
+            depth += 1
+        elif ch in "})":
+            depth -= 1
+        if (ch.isspace() or ch == ",") and depth == 0:
+            if cur:
+                toks.append(cur)
+            cur = ""
+        else:
+            cur += ch
+    if cur:
+        toks.append(cur)
+    return toks
+
+
+_IGNORED = {".op", ".tran", ".dc", ".option", ".options", ".temp", ".meas", ".measure", ".print", ".save",
+            ".probe", ".plot", ".control", ".endc", ".title"}
+_MOS_DEFAULTS = dict(level=1.0, vto=0.0, kp=2e-5, gamma=0.0, phi=0.6, lambda_=0.0, is_=1e-14, tox=0.0, rd=0.0,
+                     rs=0.0)
+_DIODE_DEFAULTS = dict(is_=1e-14, n=1.0, cjo=0.0, vj=1.0, m=0.5, fc=0.5, tt=0.0, rs=0.0)
+
+
+def _kv(tokens: Sequence[str], where: str) -> Dict[str, str]:
+    out = {}
+    flat: List[str] = []
+    for t in tokens:
+        if t.startswith("(") and t.endswith(")"):
+            flat += _split(t[1:-1])  # a parenthesized parameter list
+        else:
+            flat.append(t)
+    for t in flat:
+        t = t.strip("()")
+        if not t:
+            continue
+        if "=" not in t:
+            raise DeckError(f"{where}: expected name=value, got {t!r}")
+        k, v = t.split("=", 1)
+        out[k] = v
+    return out
+
+
+def read_deck(text: str, lanes: int = 1, params: Optional[Mapping[str, Value]] = None,
+              name: Optional[str] = None) -> Netlist:
+    """The deck `text` as a Netlist of `lanes` lanes; `params` gives
+    parameter values (scalars or one per lane) that override `.param`."""
+    if lanes < 1:
+        raise DeckError("a deck needs at least one lane")
+    params = dict(params or {})
+    env = _Env(lanes, params)
+    cards = _logical_lines(text)
+    title = text.splitlines()[0].strip() if text.strip() else "deck"
+    # .param and .model first (SPICE cards are order-free)
+    models: Dict[str, tuple] = {}
+    for ln, card in cards:
+        toks = _split(card)
+        where = f"line {ln}"
+        if toks[0] == ".param":
+            for k, v in _kv(toks[1:], where).items():
+                if k not in env.given:
+                    env.vals[k] = env.value(v, where)
+        elif toks[0] == ".model":
+            if len(toks) < 3:
+                raise DeckError(f"{where}: .model needs a name and a type")
+            mtype = toks[2].split("(")[0]
+            rest = [toks[2][len(mtype):]] + toks[3:]
+            models[toks[1]] = (mtype, rest, where)
+    b = Builder(name or title, lanes)
+    node = lambda t: "0" if t in ("0", "gnd") else t  # noqa: E731
+
+    def model_vals(mname: str, kinds: Sequence[str], defaults: dict, where: str) -> tuple:
+        if mname not in models:
+            raise DeckError(f"{where}: unknown model {mname!r}")
+        mtype, rest, mwhere = models[mname]
+        if mtype not in kinds:
+            raise DeckError(f"{where}: model {mname!r} is a {mtype}, not a {'/'.join(kinds)}")
+        vals = dict(defaults)
+        for k, v in _kv(rest, mwhere).items():
+            key = {"lambda": "lambda_", "is": "is_"}.get(k, k)
+            if key not in vals:
+                raise DeckError(f"{mwhere}: model parameter {k!r} is outside what the lanes carry")
+            vals[key] = env.value(v, mwhere)
+        return mtype, vals
+
+    def source(toks: List[str], where: str) -> tuple:
+        dc, pulse = 0.0, None
+        i = 0
+        while i < len(toks):
+            t = toks[i]
+            if t == "dc":
+                dc = env.value(toks[i + 1], where)
+                i += 2
+            elif t.startswith("pulse"):
+                body = t[len("pulse"):].strip()
+                if not body.startswith("("):
+                    body = " ".join(toks[i + 1:])
+                    i = len(toks)
+                else:
+                    i += 1
+                vals = [env.value(v, where) for v in _split(body.strip("()"))]
+                if len(vals) != 7:
+                    raise DeckError(f"{where}: PULSE needs all seven values (v1 v2 td tr tf pw per)")
+                pulse = tuple(vals)
+            elif t.startswith(("sin", "exp", "pwl", "sffm", "am", "ac")):
+                raise DeckError(f"{where}: only DC and PULSE sources ride the lanes")
+            else:
+                dc = env.value(t, where)
+                i += 1
+        return dc, pulse
+
+    for ln, card in cards:
+        toks = _split(card)
+        where = f"line {ln}"
+        head = toks[0]
+        if head.startswith("."):
+            if head in (".param", ".model") or head in _IGNORED:
+                continue
+            if head == ".end":
+                break
+            raise DeckError(f"{where}: the card {head} is outside what the lanes carry")
+        kind = head[0]
+        if kind == "r":
+            if len(toks) != 4:
+                raise DeckError(f"{where}: R needs two nodes and a value")
+            b.r(node(toks[1]), node(toks[2]), env.value(toks[3], where))
+        elif kind == "c":
+            if len(toks) != 4:
+                raise DeckError(f"{where}: C needs two nodes and a value")
+            b.c(node(toks[1]), node(toks[2]), env.value(toks[3], where))
+        elif kind in "vi":
+            if len(toks) < 3:
+                raise DeckError(f"{where}: a source needs two nodes")
+            dc, pulse = source(toks[3:], where)
+            (b.v if kind == "v" else b.i)(node(toks[1]), node(toks[2]), dc=dc, pulse=pulse)
+        elif kind == "d":
+            if len(toks) != 4:
+                raise DeckError(f"{where}: D needs two nodes and a model")
+            _, m = model_vals(toks[3], ("d",), _DIODE_DEFAULTS, where)
+            if np.any(np.asarray(m["rs"]) != 0):
+                raise DeckError(f"{where}: diode series resistance is outside what the lanes carry")
+            b.d(node(toks[1]), node(toks[2]), is_=m["is_"], n=m["n"], cjo=m["cjo"], vj=m["vj"], m=m["m"],
+                fc=m["fc"], tt=m["tt"])
+        elif kind == "m":
+            if len(toks) < 6:
+                raise DeckError(f"{where}: M needs four nodes and a model")
+            mtype, m = model_vals(toks[5], ("nmos", "pmos"), _MOS_DEFAULTS, where)
+            if np.any(np.asarray(m["level"]) != 1):
+                raise DeckError(f"{where}: only level-1 MOS models ride the lanes")
+            for k in ("tox", "rd", "rs"):
+                if np.any(np.asarray(m[k]) != 0):
+                    raise DeckError(f"{where}: MOS {k.upper()} is outside what the lanes carry")
+            inst = _kv(toks[6:], where)
+            w = env.value(inst.pop("w"), where) if "w" in inst else 1e-4
+            l_ = env.value(inst.pop("l"), where) if "l" in inst else 1e-4
+            if inst:
+                raise DeckError(f"{where}: instance parameters {sorted(inst)} are outside what the lanes carry")
+            typ = 1.0 if mtype == "nmos" else -1.0
+            b.m(node(toks[1]), node(toks[2]), node(toks[3]), node(toks[4]), typ, m["vto"], m["kp"], w, l_,
+                gamma=m["gamma"], phi=m["phi"], lam=m["lambda_"], is_=m["is_"])
+        else:
+            raise DeckError(f"{where}: the element {head!r} is outside what the lanes carry")
+    arrays = [np.asarray(v, dtype=np.float64) for k, v in params.items() if np.ndim(v) == 1]
+    sweep = np.stack(arrays, axis=1) if arrays else None
+    return b.freeze(sweep)

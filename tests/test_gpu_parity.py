@@ -201,3 +201,31 @@ def test_backward_euler_lte_steps(oracle):
     for a, b in zip(reps, ro):
         assert a.status == 1 and a.steps == b.steps and a.rejects == b.rejects
     assert worst(x, xo) <= 1.0
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_deck_text_dc_sweep(oracle, precision):
+    """A deck read from SPICE text (egspice_b200/netlist.py) drives the
+    lanes: a 4-stage inverter chain whose input sweeps 0 .. 1.8 V across 64
+    lanes, cold operating points against the oracle on the same netlist."""
+    from egspice_b200.netlist import read_deck
+    text = """inverter chain, input swept per lane
+vdd vdd 0 dc 1.8
+vin s0 0 dc {vin}
+.model nch nmos level=1 vto=0.45 kp=200u lambda=0.02
+.model pch pmos level=1 vto=-0.45 kp=80u lambda=0.02
+""" + "".join(f"mn{k} s{k + 1} s{k} 0 0 nch w=2u l=0.18u\nmp{k} s{k + 1} s{k} vdd vdd pch w=4u l=0.18u\n"
+              for k in range(4)) + ".op\n.end\n"
+    net = read_deck(text, lanes=64, params={"vin": np.linspace(0.0, 1.8, 64)})
+    opts = abi.newton_opts()
+    xo, ro = oracle.op_lanes(net, opts, threads=8)
+    with Lanes([net], precision=precision) as L:
+        r = L.solve_static(opts)
+        x = L.get_x(0)
+    ok = (r[:, 0] & abi.CONVERGED) != 0
+    assert (ok | (ro[:, 0] != 1)).all()
+    assert ok.mean() >= 0.95
+    both = ok & (ro[:, 0] == 1)
+    assert worst(x[both], xo[both]) <= 1.0
+    out = x[:, net.node("s4")]
+    assert out[0] < 0.1 and out[-1] > 1.7  # four inversions: the output follows the input to its rail
