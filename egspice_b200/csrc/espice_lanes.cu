@@ -88,6 +88,8 @@ struct Group {
     GroupDev dev{};
     std::vector<void*> owned;       // buffers freed at destroy
     std::vector<void*> lu_owned;    // LU buffers, reallocated at each retape
+    std::vector<void*> meas_owned;  // .meas pass descriptors and states
+    std::vector<espl_meas> passes;
     double* mos_raw = nullptr;
     double* dio_raw = nullptr;
     uint32_t meas_row = 0xFFFFFFFFu;
@@ -1042,6 +1044,7 @@ espl_status espl_destroy(espl_lanes* h) {
     for (auto& g : h->groups) {
         for (void* p : g.owned) cudaFree(p);
         for (void* p : g.lu_owned) cudaFree(p);
+        for (void* p : g.meas_owned) cudaFree(p);
     }
     cudaFree(h->d_groups);
     cudaFree(h->d_warp_group);
@@ -1260,6 +1263,48 @@ espl_status espl_get_period_meas(espl_lanes* h, uint32_t net, double* period, ui
         if (period) period[l] = st.m_cross >= 2 ? (st.m_last - st.m_first) / (double)(st.m_cross - 1) : NAN;
         if (crossings) crossings[l] = st.m_cross;
     }
+    return ESPL_OK;
+}
+
+espl_status espl_set_meas(espl_lanes* h, uint32_t net, const espl_meas* passes, uint32_t n) {
+    if (!h || net >= h->groups.size() || (n && !passes)) return ESPL_INVALID_ARGUMENT;
+    if (n > ESPL_MEAS_MAX_PASSES) return fail(h, ESPL_TOO_LARGE, "more .meas passes than ESPL_MEAS_MAX_PASSES");
+    Group& g = h->groups[net];
+    for (uint32_t p = 0; p < n; p++) {
+        if (passes[p].kind < ESPL_MEAS_WHEN || passes[p].kind > ESPL_MEAS_RMS)
+            return fail(h, ESPL_INVALID_ARGUMENT, "unknown .meas kind");
+        if (passes[p].row >= g.n) return fail(h, ESPL_INVALID_ARGUMENT, ".meas row out of range");
+    }
+    for (void* p : g.meas_owned) cudaFree(p);
+    g.meas_owned.clear();
+    g.passes.assign(passes, passes + n);
+    GroupDev& d = g.dev;
+    d.n_mpass = n;
+    d.mpass = nullptr;
+    d.mstate = nullptr;
+    if (n) {
+        espl_status s;
+        if ((s = dupload(h, g.meas_owned, &d.mpass, g.passes))) return s;
+        if ((s = dalloc(h, g.meas_owned, &d.mstate, (size_t)n * kMeasWords * g.P))) return s;
+    }
+    return push_descs(h);
+}
+
+espl_status espl_get_meas(espl_lanes* h, uint32_t net, double* value, double* at) {
+    if (!h || net >= h->groups.size()) return ESPL_INVALID_ARGUMENT;
+    Group& g = h->groups[net];
+    const uint32_t n = (uint32_t)g.passes.size();
+    if (!n) return ESPL_OK;
+    std::vector<double> st((size_t)n * kMeasWords * g.P);
+    CK(cudaMemcpyAsync(st.data(), g.dev.mstate, st.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    for (uint32_t l = 0; l < g.lanes; l++)
+        for (uint32_t p = 0; p < n; p++) {
+            double v, a;
+            meas_result(g.passes[p], st.data() + (size_t)p * kMeasWords * g.P + l, g.P, v, a);
+            if (value) value[(size_t)l * n + p] = v;
+            if (at) at[(size_t)l * n + p] = a;
+        }
     return ESPL_OK;
 }
 

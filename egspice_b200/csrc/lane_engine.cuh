@@ -21,6 +21,7 @@
 
 #include <cstdint>
 
+#include "lane_meas.cuh"
 #include "lane_models.cuh"
 
 namespace espl {
@@ -42,6 +43,11 @@ struct GroupDev {
     uint32_t n_void, n_res, n_cap, n_vsrc, n_isrc, n_dio, n_mos, n_sites;
     uint32_t has_charge, meas_row;
     double meas_level, meas_t0;
+    // Streaming .meas passes (lane_meas.cuh): n_mpass descriptors and their
+    // lane-major states (n_mpass * kMeasWords * P).
+    const espl_meas* mpass;
+    double* mstate;
+    uint32_t n_mpass, mpass_pad;
     const uint32_t *col_ptr, *row_idx, *prow, *q, *pinv, *lp, *li, *up, *ui, *flags, *void_slots, *diag;
     const uint32_t *rt_ptr, *rt_col, *rt_pos;  // row view of the pattern: per row, (column, slot) by column
     const uint32_t* lu_prog;                   // the replay as a flat program (tape.h lu_program)

@@ -531,6 +531,12 @@ __global__ void __launch_bounds__(kTileThreads) k_tran_init(TileMap m, TranParam
     s.m_first = s.m_last = NAN;
     s.fp64 = 0;
     s.peels = 0;
+    // the .meas passes start, reading the operating point at t = 0
+    for (uint32_t p = 0; p < d.n_mpass; p++) {
+        double* ms = d.mstate + (size_t)p * kMeasWords * P + l;
+        meas_init(d.mpass[p], ms, P);
+        meas_feed(d.mpass[p], ms, P, 0.0, LM(d.x, d.mpass[p].row));
+    }
 }
 
 // Up to o.launch_steps attempts per lane, each: stepBegin, the linear
@@ -745,6 +751,8 @@ __global__ void __launch_bounds__(WIDE ? kWideThreads : kTileThreads, WIDE ? 1 :
                 s->m_prev_t = t_new;
                 s->m_have = 1;
             }
+            for (uint32_t p = 0; p < d.n_mpass; p++)
+                meas_feed(d.mpass[p], d.mstate + (size_t)p * kMeasWords * P + l, P, t_new, LM(d.x, d.mpass[p].row));
             // stepEndB (kernels/lane.zig:667-700).
             s->t = t_new;
             if (!o.fixed_step) {

@@ -15,7 +15,7 @@ from typing import List, Optional, Sequence
 import numpy as np
 
 from . import abi
-from .abi import (ClassInfo, CreateOpts, LaneNewton, NetlistC, NewtonOpts, StepReport, Stats, TranOpts, f64p, u32p)
+from .abi import (ClassInfo, CreateOpts, MeasPass, LaneNewton, NetlistC, NewtonOpts, StepReport, Stats, TranOpts, f64p, u32p)
 from .decks import Netlist
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -60,6 +60,10 @@ def lib():
         L.espl_get_period_meas.restype = C.c_uint32
         L.espl_get_stats.argtypes = [C.c_void_p, C.POINTER(Stats)]
         L.espl_get_stats.restype = C.c_uint32
+        L.espl_set_meas.argtypes = [C.c_void_p, C.c_uint32, C.POINTER(MeasPass), C.c_uint32]
+        L.espl_set_meas.restype = C.c_uint32
+        L.espl_get_meas.argtypes = [C.c_void_p, C.c_uint32, f64p, f64p]
+        L.espl_get_meas.restype = C.c_uint32
         L.espl_get_classes.argtypes = [C.c_void_p, C.POINTER(ClassInfo), C.c_uint32, u32p]
         L.espl_get_classes.restype = C.c_uint32
         L.espl_error_message.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t]
@@ -167,6 +171,23 @@ class Lanes:
                                                         ("q", "pinv", "lp", "li", "up", "ui", "flags")]),
                     "espl_copy_tape")
         return {k: out[k][:arrs[k]] for k in arrs}
+
+    def set_meas(self, net: int, passes: Sequence[MeasPass]):
+        """Streaming .meas passes of template `net` (abi.meas_pass), set
+        before init_steps."""
+        arr = (MeasPass * max(len(passes), 1))(*passes)
+        self._check(lib().espl_set_meas(self.h, net, arr, len(passes)), "espl_set_meas")
+        self._n_meas = getattr(self, "_n_meas", {})
+        self._n_meas[net] = len(passes)
+
+    def get_meas(self, net: int):
+        """(value, at), each [lanes, passes]."""
+        n = getattr(self, "_n_meas", {}).get(net, 0)
+        lanes = self.nets[net].lanes
+        v = np.full((lanes, max(n, 1)), np.nan)
+        a = np.full((lanes, max(n, 1)), np.nan)
+        self._check(lib().espl_get_meas(self.h, net, v.ctypes.data_as(f64p), a.ctypes.data_as(f64p)), "espl_get_meas")
+        return v[:, :n], a[:, :n]
 
     def classes(self) -> List[dict]:
         """The launch classes in launch order, each with its kernel's device

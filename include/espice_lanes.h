@@ -213,6 +213,43 @@ espl_status espl_device_launch(espl_lanes *h, uint32_t max_steps, espl_step_repo
 espl_status espl_set_period_meas(espl_lanes *h, uint32_t net, uint32_t row, double level, double t_start);
 espl_status espl_get_period_meas(espl_lanes *h, uint32_t net, double *period, uint32_t *crossings);
 
+/* Streaming .meas passes over each lane's transient, on the device: every
+ * pass reads unknown `row` at t = 0 (the operating point) and at every
+ * accepted step, with ngspice's measure semantics as the reference streams
+ * them on its lanes (src/output/scan.zig Cross, At, Extremum, Integ; run per
+ * lane from src/solver/lane_device.zig). Kinds:
+ *   WHEN     the time `row` crosses `val` (after `td`, inside [from, to]):
+ *            the `rise`-th rising, `fall`-th falling or `cross`-th crossing
+ *            (ESPL_MEAS_LAST: the last one; all ESPL_MEAS_UNSET: the first)
+ *   FIND_AT  the value at time `at` (linear between steps)
+ *   MIN/MAX  the extremum over [from, to] (to = 0: to the end), `at` where
+ *   AVG      the trapezoidal average over [from, to]
+ *   INTEG    the integral over [from, to] (Simpson 3/8, Simpson, trapezoid
+ *            panels as ngspice chooses them); RMS its root-mean-square
+ * TRIG/TARG is the difference of two WHEN passes, PP that of MAX and MIN.
+ * Set before espl_init_steps (at most ESPL_MEAS_MAX_PASSES per template);
+ * read after the run: value and at are [lanes][n], NaN where a pass saw no
+ * result. */
+enum {
+    ESPL_MEAS_WHEN = 1, ESPL_MEAS_FIND_AT = 2, ESPL_MEAS_MIN = 3, ESPL_MEAS_MAX = 4, ESPL_MEAS_AVG = 5,
+    ESPL_MEAS_INTEG = 6, ESPL_MEAS_RMS = 7
+};
+#define ESPL_MEAS_UNSET (-1)
+#define ESPL_MEAS_LAST (-2)
+#define ESPL_MEAS_MAX_PASSES 16u
+typedef struct {
+    uint32_t kind;
+    uint32_t row;
+    double val;                  /* WHEN: the level */
+    double td;                   /* WHEN: samples before td are skipped */
+    double from, to;             /* the window; to = 0 leaves it open */
+    double at;                   /* FIND_AT: the time */
+    int32_t rise, fall, cross;   /* WHEN: the event's count, ESPL_MEAS_UNSET or ESPL_MEAS_LAST */
+    uint32_t reserved;
+} espl_meas;
+espl_status espl_set_meas(espl_lanes *h, uint32_t net, const espl_meas *passes, uint32_t n);
+espl_status espl_get_meas(espl_lanes *h, uint32_t net, double *value, double *at);
+
 /* Timing of the last solve/launch, milliseconds of device time per kernel
  * family (CUDA events on the launching stream), for roofline reporting. */
 typedef struct {

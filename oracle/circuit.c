@@ -533,6 +533,9 @@ typedef struct {
     espl_step_report *reports;
     uint32_t meas_row;
     double meas_level, meas_t_start;
+    const espl_meas *passes;
+    uint32_t n_passes;
+    double *meas_value, *meas_at;
     double *period;
 } job_t;
 
@@ -699,6 +702,11 @@ static void tran_one(job_t *j, uint32_t li) {
     seed_limits(k, x, 1);
     orc_newton_result r0 = newton(k, x, &op, 1, 0.0, NULL, NULL);
     if (!r0.converged) { rep->status = 4; ckt_free(k); return; }
+    orc_meas_state mst[ESPL_MEAS_MAX_PASSES];
+    for (uint32_t p = 0; p < j->n_passes; p++) {
+        orc_meas_init(&j->passes[p], &mst[p]);
+        orc_meas_feed(&j->passes[p], &mst[p], 0.0, x[j->passes[p].row]);
+    }
     uint32_t n1 = n + 1;
     uint32_t ns = k->n_sites;
     /* Row charge ring: logical 1 and 2 start at q(x_op); site ring 1..3 too. */
@@ -854,6 +862,7 @@ static void tran_one(job_t *j, uint32_t li) {
             for (uint32_t pi = 0; pi < j->n_probes; pi++) row[pi] = x[j->probes[pi]];
         }
         rows++;
+        for (uint32_t p = 0; p < j->n_passes; p++) orc_meas_feed(&j->passes[p], &mst[p], t_new, x[j->passes[p].row]);
         if (has_meas && t_new >= j->meas_t_start) {
             double v = x[j->meas_row];
             if (m_have && m_prev_v < j->meas_level && v >= j->meas_level) {
@@ -898,6 +907,9 @@ static void tran_one(job_t *j, uint32_t li) {
     rep->dt = dt;
     rep->steps = steps;
     if (has_meas && j->period) j->period[li] = m_cross >= 2 ? (m_last - m_first) / (double)(m_cross - 1) : NAN;
+    for (uint32_t p = 0; p < j->n_passes; p++)
+        orc_meas_result(&j->passes[p], &mst[p], &j->meas_value[(size_t)li * j->n_passes + p],
+                        &j->meas_at[(size_t)li * j->n_passes + p]);
     free(q1); free(q2); free(ip); free(s0); free(s1); free(s2); free(s3); free(sip);
     free(cur); free(prev); free(lim_save);
     ckt_free(k);
@@ -935,6 +947,33 @@ int orc_tran_lanes(const espl_netlist *net, uint32_t lane0, uint32_t count, cons
     j.meas_level = meas_level;
     j.meas_t_start = meas_t_start;
     j.period = period;
+    j.q = q;
+    atomic_init(&j.next, 0);
+    run_pool(&j, threads, tran_worker);
+    free(q);
+    return 0;
+}
+
+int orc_tran_meas(const espl_netlist *net, uint32_t lane0, uint32_t count, const espl_tran_opts *opts,
+                  const espl_meas *passes, uint32_t n_passes, double *value, double *at, double *x_final,
+                  espl_step_report *reports, uint32_t threads) {
+    if (n_passes > ESPL_MEAS_MAX_PASSES) return -1;
+    for (uint32_t li = 0; li < count * n_passes; li++) value[li] = at[li] = NAN;
+    uint32_t *q = (uint32_t *)malloc(sizeof(uint32_t) * (net->n ? net->n : 1));
+    if (orc_order(net->n, net->col_ptr, net->row_idx, q) != 0) { free(q); return -1; }
+    job_t j;
+    memset(&j, 0, sizeof(j));
+    j.net = net;
+    j.lane0 = lane0;
+    j.count = count;
+    j.topts = opts;
+    j.x_out = x_final;
+    j.reports = reports;
+    j.meas_row = UINT32_MAX;
+    j.passes = passes;
+    j.n_passes = n_passes;
+    j.meas_value = value;
+    j.meas_at = at;
     j.q = q;
     atomic_init(&j.next, 0);
     run_pool(&j, threads, tran_worker);

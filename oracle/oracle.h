@@ -85,6 +85,28 @@ int orc_tran_lanes(const espl_netlist *net, uint32_t lane0, uint32_t count, cons
                    double *x_final, espl_step_report *reports, uint32_t meas_row, double meas_level,
                    double meas_t_start, double *period, uint32_t threads);
 
+/* Streaming .meas passes (measure.c, after src/output/scan.zig): one pass's
+ * state, fed a sample at a time. */
+typedef struct {
+    int done, first, above, pending, found, inside, cut, np;
+    int32_t rise, fall, cross, want_rise, want_fall, want_cross;
+    double prev, prev_x, last, hit;
+    uint64_t rows, count;
+    double px, pv, py, value, xv, m, m_at, span;
+    double p[4][2], first_x, cut_x, sum[3];
+} orc_meas_state;
+void orc_meas_init(const espl_meas *c, orc_meas_state *s);
+void orc_meas_feed(const espl_meas *c, orc_meas_state *s, double x, double v);
+void orc_meas_result(const espl_meas *c, orc_meas_state *s, double *value, double *at);
+/* One pass over a whole series (x[k], v[k]). */
+int orc_meas_series(const espl_meas *c, const double *x, const double *v, uint32_t n, double *value, double *at);
+/* orc_tran_lanes with .meas passes instead of probes and the period: each
+ * pass reads its row at t = 0 and at every accepted step; value and at are
+ * [count][n_passes]. */
+int orc_tran_meas(const espl_netlist *net, uint32_t lane0, uint32_t count, const espl_tran_opts *opts,
+                  const espl_meas *passes, uint32_t n_passes, double *value, double *at, double *x_final,
+                  espl_step_report *reports, uint32_t threads);
+
 /* Device-model probes for the finite-difference tests: evaluates instance
  * `inst` of batch `b` in lane `lane` at node voltages v (terminals order)
  * with no limiting; writes the residual rows f[terms] and the Jacobian

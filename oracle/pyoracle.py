@@ -12,7 +12,8 @@ from typing import Optional, Sequence, Tuple
 
 import numpy as np
 
-from egspice_b200.abi import (CNet, NetlistC, NewtonOpts, OrcNewtonResult, StepReport, TranOpts, f64p, u32p)
+from egspice_b200.abi import (CNet, MeasPass, NetlistC, NewtonOpts, OrcNewtonResult, StepReport, TranOpts, f64p,
+                              u32p)
 from egspice_b200.decks import Netlist
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -31,6 +32,11 @@ def lib():
         if not os.path.exists(LIB):
             build()
         L = C.CDLL(LIB)
+        L.orc_tran_meas.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.POINTER(MeasPass), C.c_uint32,
+                                    f64p, f64p, f64p, C.c_void_p, C.c_uint32]
+        L.orc_tran_meas.restype = C.c_int
+        L.orc_meas_series.argtypes = [C.POINTER(MeasPass), f64p, f64p, C.c_uint32, f64p, f64p]
+        L.orc_meas_series.restype = C.c_int
         L.orc_order.argtypes = [C.c_uint32, u32p, u32p, u32p]
         L.orc_order.restype = C.c_int
         L.orc_order_ws.argtypes = [C.c_uint32, u32p, u32p, u32p, u32p, C.c_size_t]
@@ -234,6 +240,33 @@ def tran_lanes(net: Netlist, opts: TranOpts, lane0: int = 0, count: Optional[int
                              x.ctypes.data_as(f64p), reps, mrow, mlev, mt0, perp, threads)
     assert r == 0
     return x, list(reps), rows, per
+
+
+def tran_meas(net: Netlist, opts: TranOpts, passes: Sequence[MeasPass], threads: int = 1):
+    """Transients of every lane with streaming .meas passes. Returns
+    (value [lanes, passes], at [lanes, passes], x_final, reports)."""
+    count = net.lanes
+    cn = CNet(net)
+    n = len(passes)
+    arr = (MeasPass * max(n, 1))(*passes)
+    val = np.full((count, max(n, 1)), np.nan)
+    at = np.full((count, max(n, 1)), np.nan)
+    x = np.zeros((count, net.n))
+    reps = (StepReport * count)()
+    r = lib().orc_tran_meas(C.byref(cn.c), 0, count, C.byref(opts), arr, n, val.ctypes.data_as(f64p),
+                            at.ctypes.data_as(f64p), x.ctypes.data_as(f64p), reps, threads)
+    assert r == 0
+    return val[:, :n], at[:, :n], x, list(reps)
+
+
+def meas_series(p: MeasPass, xs, vs) -> Tuple[float, float]:
+    """One pass over the samples (xs[k], vs[k])."""
+    xs = np.ascontiguousarray(xs, dtype=np.float64)
+    vs = np.ascontiguousarray(vs, dtype=np.float64)
+    v, a = C.c_double(), C.c_double()
+    lib().orc_meas_series(C.byref(p), xs.ctypes.data_as(f64p), vs.ctypes.data_as(f64p), len(xs), C.byref(v),
+                          C.byref(a))
+    return v.value, a.value
 
 
 def device_probe(net: Netlist, batch: int, inst: int, lane: int, v):

@@ -229,3 +229,33 @@ vin s0 0 dc {vin}
     assert worst(x[both], xo[both]) <= 1.0
     out = x[:, net.node("s4")]
     assert out[0] < 0.1 and out[-1] > 1.7  # four inversions: the output follows the input to its rail
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_streaming_meas_passes(oracle, precision):
+    """The device .meas passes (include/espice_lanes.h espl_set_meas) on the
+    ring oscillator against the oracle's (oracle/measure.c) over the same
+    transient: WHEN with a count and a delay, MAX, MIN, AVG and RMS over a
+    window, INTEG, FIND ... AT."""
+    net = decks.ring_oscillator(16, stages=15)
+    s1, s3, s5 = net.node("s1"), net.node("s3"), net.node("s5")
+    M = abi.meas_pass
+    passes = [M(abi.MEAS_WHEN, s3, val=0.9, td=0.5e-9, rise=2), M(abi.MEAS_WHEN, s1, val=0.9, cross=abi.MEAS_LAST),
+              M(abi.MEAS_MAX, s3), M(abi.MEAS_MIN, s3, from_=1e-9), M(abi.MEAS_AVG, s3, from_=1e-9, to=2.5e-9),
+              M(abi.MEAS_INTEG, s1), M(abi.MEAS_RMS, s1, from_=1e-9), M(abi.MEAS_FIND_AT, s5, at=2.2e-9)]
+    opts = abi.tran_opts(t_stop=3e-9, dt=1e-12, dt_max=5e-12, method=1, max_iter=20)
+    vo, ao, _, ro = oracle.tran_meas(net, opts, passes, threads=8)
+    with Lanes([net], precision=precision) as L:
+        L.set_meas(0, passes)
+        reps = L.run_tran(opts, steps_per_launch=2048)
+        v, a = L.get_meas(0)
+    assert all(r.status == 1 for r in reps)
+    assert np.isfinite(vo).all() and np.isfinite(v).all()
+    # the 1e-6 bar; voltages with the bar's 1e-9 V floor, times and the
+    # integral (V s) relative only
+    for k in range(len(passes)):
+        atol = 1e-9 if k in (2, 3, 4, 6, 7) else 0.0
+        np.testing.assert_allclose(v[:, k], vo[:, k], rtol=1e-6, atol=atol, err_msg=f"pass {k}")
+    # where an extremum was taken is not pinned: the rails are flat, and the
+    # last of several samples within an ulp of the extremum is the one kept
+    assert ((a[:, 2:4] >= 0) & (a[:, 2:4] <= opts.t_stop)).all()
