@@ -345,6 +345,97 @@ Plan build_plan(const Group& g) {
     return pl;
 }
 
+// ngspice's diagonal-gmin placement (gminStamps, src/analysis/dc/op.zig:
+// 712-792, after Sparse's spMNA_Preorder and LoadGmin): a column position
+// with no diagonal element (a branch row nothing stamps a diagonal into)
+// swaps with a "twin" whose transposed entry is +-1 too, so a grounded
+// source's gmin lands on its two incidence entries. Lone twins first, then
+// the first column with several. A slot's value is known here only when its
+// G contributions are the constant +-1 cells of the source incidences (the
+// entries the twin rule reads); every other slot is treated as not +-1.
+// Returns (slot, row, column) triples for rows 1 .. n-1.
+std::vector<uint32_t> gmin_stamps(const Group& g, const Plan& pl) {
+    const uint32_t n = g.n;
+    const uint32_t none = 0xFFFFFFFFu;
+    const uint32_t kP = pl.c_const, kM = pl.c_const + 1;
+    // the value of slot p when it is a sum of constant cells (NaN otherwise)
+    auto gval = [&](uint32_t p) {
+        double v = 0.0;
+        for (uint32_t e : pl.g[p]) {
+            const uint32_t cell = e & ~kNeg;
+            if (cell != kP && cell != kM) return (double)NAN;
+            const double c = cell == kP ? 1.0 : -1.0;
+            v += (e & kNeg) ? -c : c;
+        }
+        return v;
+    };
+    auto unit = [&](uint32_t p) { return std::fabs(gval(p)) == 1.0; };
+    std::vector<uint32_t> perm(n), dcol(n);
+    for (uint32_t i = 0; i < n; i++) {
+        const uint32_t slot = g.diag[i];
+        const bool empty = pl.g[slot].empty() || gval(slot) == 0.0;
+        perm[i] = i;
+        dcol[i] = (g.cur_row[i] && empty && pl.c[slot].empty()) ? none : i;
+    }
+    struct Twin {
+        uint32_t count, row;
+    };
+    auto twins = [&](uint32_t j) {
+        Twin t{0, 0};
+        const uint32_t col = perm[j];
+        for (uint32_t p = g.col_ptr[col]; p < g.col_ptr[col + 1]; p++) {
+            const uint32_t r = g.row_idx[p];
+            if (!unit(p)) continue;
+            const uint32_t q = find_slot(g, j, perm[r]);
+            if (q >= g.nnz || !unit(q)) continue;
+            t.count++;
+            if (t.count == 1) t.row = r;
+            else break;
+        }
+        return t;
+    };
+    auto swap = [&](uint32_t j, uint32_t r) {
+        dcol[j] = perm[r];
+        dcol[r] = perm[j];
+        std::swap(perm[j], perm[r]);
+    };
+    uint32_t start = 1;
+    for (;;) {
+        bool swapped = false, again = false;
+        for (uint32_t j = start; j < n; j++) {
+            if (dcol[j] != none) continue;
+            const Twin t = twins(j);
+            if (t.count == 1) {
+                swap(j, t.row);
+                swapped = true;
+            } else if (t.count > 1 && !again) {
+                again = true;
+                start = j;
+            }
+        }
+        if (!again) break;
+        for (uint32_t j = start; !swapped && j < n; j++) {
+            if (dcol[j] != none) continue;
+            const Twin t = twins(j);
+            if (t.count > 0) {
+                swap(j, t.row);
+                swapped = true;
+            }
+        }
+        if (!swapped) break;
+    }
+    std::vector<uint32_t> out;
+    for (uint32_t i = 1; i < n; i++) {
+        if (dcol[i] == none) continue;
+        const uint32_t slot = find_slot(g, i, dcol[i]);
+        if (slot >= g.nnz) continue;
+        out.push_back(slot);
+        out.push_back(i);
+        out.push_back(dcol[i]);
+    }
+    return out;
+}
+
 // Allocates the lane-major state of a group; the LU buffers come later.
 espl_status alloc_group(espl_lanes* h, Group& g) {
     GroupDev& d = g.dev;
@@ -439,6 +530,11 @@ espl_status alloc_group(espl_lanes* h, Group& g) {
             split(16, d.gsplit16);
             if ((s = dupload(h, own, &d.gi_ptr, ip)) || (s = dupload(h, own, &d.gi_ent, ie))) return s;
         }
+        {
+            std::vector<uint32_t> gs = gmin_stamps(g, pl);
+            d.n_gstamp = (uint32_t)(gs.size() / 3);
+            if ((s = dupload(h, own, &d.gstamp, gs))) return s;
+        }
         if ((s = dupload(h, own, &d.site_cell, pl.sites))) return s;
         if ((s = dupload(h, own, &d.slot_diag, pl.slot_diag))) return s;
         // two cells buffers: an iteration's instance phase and the next one's
@@ -524,6 +620,7 @@ espl_status alloc_group(espl_lanes* h, Group& g) {
     AL(lim_dio, (size_t)d.n_dio * P);
     AL(q1, n1 * P);
     AL(q2, n1 * P);
+    AL(x_good, n1 * P);
     AL(ip, n1 * P);
     AL(cur, n1 * P);
     AL(prev, n1 * P);
@@ -1134,6 +1231,263 @@ espl_status espl_solve_static(espl_lanes* h, const espl_newton_opts* opts, espl_
                 out[k].refactor_fallbacks = st.fallbacks;
                 out[k].reserved = 0;
                 iters += st.iterations;
+                k++;
+            }
+        h->stats.lane_iterations = iters;
+    }
+    return ESPL_OK;
+}
+
+// The operating point with the continuation ladder (op.zig solveLadder and
+// afterPlain, rungs 1 to 3, and the final clean solve): every lane first
+// takes the plain rung from the cold start; a lane that fails it walks its
+// own dynamic gmin descent, then source stepping (with the sources-off gmin
+// start), then the final full-source solve. All lanes still on the ladder
+// solve together, each at its own gmin, source scale and start, one device
+// launch per ladder solve; the host keeps every lane's step logic.
+espl_status espl_solve_op(espl_lanes* h, const espl_newton_opts* opts, espl_lane_newton* out) {
+    if (!h || !opts) return ESPL_INVALID_ARGUMENT;
+    if (opts->max_iter == 0 || opts->max_iter > 100000) return fail(h, ESPL_INVALID_ARGUMENT, "max_iter out of range");
+    const uint32_t N = h->total_lanes;
+    const double gtarget = 1e-12, gmin_start = 1e-2;  // numerics.zig Tolerances gmin, gmin_start
+    const uint16_t budget = 100;                       // optionsFromTolerances(tol, itl2 = 50): at least 100
+    const uint32_t max_solves = 1000, stall_solves = 20;
+    const double stall_factor = std::pow(10.0, 1.0 / stall_solves);
+    espl_status s;
+    LadderLane* d_par = nullptr;
+    uint8_t* d_act = nullptr;
+    CK(cudaMalloc(&d_par, sizeof(LadderLane) * N));
+    if (cudaMalloc(&d_act, N) != cudaSuccess) {
+        cudaFree(d_par);
+        return fail(h, ESPL_OUT_OF_MEMORY, "ladder scratch");
+    }
+    auto release = [&]() {
+        cudaFree(d_par);
+        cudaFree(d_act);
+    };
+    auto actions = [&](std::vector<uint8_t>& a) -> espl_status {
+        CK(cudaMemcpyAsync(d_act, a.data(), N, cudaMemcpyHostToDevice, h->stream));
+        k_ladder_x<<<grid_of(h), kBlock, 0, h->stream>>>(launch_map(h), d_act);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(h->stream));
+        std::fill(a.begin(), a.end(), 0);
+        return ESPL_OK;
+    };
+    std::vector<uint8_t> pre(N, 1), post(N, 0);
+    // rung 1: plain Newton, no gmin, from the cold start (x = 0, MODEINITJCT seeds)
+    if ((s = actions(pre))) return release(), s;
+    if (seed(h, 1)) return release(), ESPL_DRIVER;
+    espl_newton_opts plain = *opts;
+    plain.gmin = 0.0;
+    plain.init_fix = 1;
+    if ((s = run_static(h, newton_params(plain, h->precision, h->refine_sweeps), 0))) return release(), s;
+    CK(cudaMemcpyAsync(h->h_state.data(), h->d_state, sizeof(LaneState) * N, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    enum Phase : uint8_t { kDone = 0, kGmin, kClean, kSrc, kSrcOff, kFinal };
+    struct Lad {
+        Phase phase = kDone;
+        bool converged = false, have_good = false;
+        double factor = 10.0, good_gmin = 1e-2, gmin_val = 1e-3;
+        std::vector<std::pair<double, bool>> steps;
+        double lambda = 0.0, lambda_good = -1.0, delta = 0.25, off_g = 0.0;
+        uint32_t solves = 0, off_i = 0, total = 0;
+    };
+    std::vector<Lad> lad(N);
+    std::vector<LadderLane> par(N);
+    bool any = false;
+    for (auto& g : h->groups)
+        for (uint32_t l = 0; l < g.lanes; l++) {
+            const LaneState& st = h->h_state[g.lane0 + l];
+            Lad& z = lad[g.lane0 + l];
+            z.total = st.iterations;
+            z.converged = (st.bits & kConverged) != 0;
+            if (!z.converged) {
+                // rung 2 starts from the cold start
+                z.phase = kGmin;
+                z.good_gmin = gmin_start;
+                z.gmin_val = z.good_gmin / z.factor;
+                pre[g.lane0 + l] = 1;
+                any = true;
+            }
+        }
+    auto stalled = [&](const Lad& z, double next) {
+        const size_t m = z.steps.size();
+        if (m < stall_solves) return false;
+        double good = gmin_start;
+        for (size_t i = 0; i < m; i++) {
+            if (z.steps[i].second) good = z.steps[i].first;
+            if (i < m - stall_solves) continue;
+            const double following = i + 1 < m ? z.steps[i + 1].first : next;
+            if (good / following >= stall_factor) return false;
+        }
+        return true;
+    };
+    auto gfactor = [&](double f, uint32_t it) {
+        if (it <= budget / 4) return std::min(f * std::sqrt(f), 10.0);
+        if (it > 3 * (budget / 4)) return std::max(std::sqrt(f), 1.00005);
+        return f;
+    };
+    for (uint32_t round = 0; any && round < 4 * max_solves; round++) {
+        any = false;
+        for (uint32_t k = 0; k < N; k++) {
+            const Lad& z = lad[k];
+            LadderLane& p = par[k];
+            p = LadderLane{0.0, 1.0, 0u, 0u};
+            switch (z.phase) {
+            case kGmin: p = LadderLane{z.gmin_val, 1.0, 1u, z.have_good ? 0u : 1u}; break;
+            case kClean: p = LadderLane{0.0, 1.0, 1u, 0u}; break;
+            case kSrc: p = LadderLane{0.0, z.lambda, 1u, z.lambda_good < 0.0 ? 1u : 0u}; break;
+            case kSrcOff: p = LadderLane{z.off_g, z.lambda, 1u, z.off_i == 0 ? 1u : 0u}; break;
+            case kFinal: p = LadderLane{0.0, 1.0, 1u, 0u}; break;
+            default: break;
+            }
+            any |= p.on != 0;
+        }
+        if (!any) break;
+        // a warm solve starts its limiter state at the lane's x
+        for (uint32_t k = 0; k < N; k++)
+            if (par[k].on && !par[k].init_fix && pre[k] == 0) pre[k] = 4;
+        if ((s = actions(pre))) return release(), s;
+        CK(cudaMemcpyAsync(d_par, par.data(), sizeof(LadderLane) * N, cudaMemcpyHostToDevice, h->stream));
+        espl_newton_opts o = *opts;
+        o.gmin = 0.0;
+        o.max_iter = budget;
+        NewtonParams np = newton_params(o, h->precision, h->refine_sweeps);
+        np.ladder = d_par;
+        if ((s = run_static(h, np, 0))) return release(), s;
+        CK(cudaMemcpyAsync(h->h_state.data(), h->d_state, sizeof(LaneState) * N, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        for (uint32_t k = 0; k < N; k++) {
+            Lad& z = lad[k];
+            if (!par[k].on) continue;
+            const LaneState& st = h->h_state[k];
+            const bool singular = (st.bits & kSingular) != 0;
+            const bool conv = !singular && (st.bits & kConverged) != 0;
+            const uint32_t it = singular ? 0u : st.iterations;
+            z.total = std::min<uint32_t>(z.total + it, 65535u);
+            switch (z.phase) {
+            case kGmin: {
+                const double tried = z.gmin_val;
+                bool to_src = false;
+                if (conv) {
+                    if (z.gmin_val <= gtarget) {
+                        z.phase = kClean;
+                        break;
+                    }
+                    post[k] = 3;
+                    z.have_good = true;
+                    z.good_gmin = z.gmin_val;
+                    z.factor = gfactor(z.factor, it);
+                    if (z.gmin_val < z.factor * gtarget) {
+                        z.factor = z.gmin_val / gtarget;
+                        z.gmin_val = gtarget;
+                    } else {
+                        z.gmin_val /= z.factor;
+                    }
+                } else {
+                    if (z.factor < 1.00005) {
+                        to_src = true;
+                    } else {
+                        z.factor = singular ? std::sqrt(z.factor) : std::sqrt(std::sqrt(z.factor));
+                        z.gmin_val = z.good_gmin / z.factor;
+                        pre[k] = z.have_good ? 2 : 1;
+                    }
+                }
+                if (!to_src) {
+                    z.steps.emplace_back(tried, conv);
+                    z.solves++;
+                    if (stalled(z, z.gmin_val) || z.solves >= max_solves) to_src = true;
+                }
+                if (to_src) {
+                    z.phase = kSrc;
+                    z.lambda = 0.0;
+                    z.lambda_good = -1.0;
+                    z.delta = 0.25;
+                    z.solves = 0;
+                    pre[k] = 1;
+                }
+                break;
+            }
+            case kClean:
+                if (conv) {
+                    z.phase = kDone;
+                    z.converged = true;
+                } else {
+                    z.phase = kSrc;
+                    z.lambda = 0.0;
+                    z.lambda_good = -1.0;
+                    z.delta = 0.25;
+                    z.solves = 0;
+                    pre[k] = 1;
+                }
+                break;
+            case kSrc:
+            case kSrcOff: {
+                bool ok = conv, decided = true;
+                if (z.phase == kSrc && !conv && z.lambda_good < 0.0) {
+                    // sourcesOffGmin: eleven solves from 1e10 x gmin down, a decade each
+                    z.phase = kSrcOff;
+                    z.off_i = 0;
+                    z.off_g = gtarget * 1e10;
+                    pre[k] = 1;
+                    decided = false;
+                } else if (z.phase == kSrcOff) {
+                    if (conv && z.off_i < 10) {
+                        z.off_i++;
+                        z.off_g /= 10;
+                        decided = false;
+                    } else {
+                        ok = conv;  // all eleven converged, or one failed
+                        z.phase = kSrc;
+                    }
+                }
+                if (!decided) break;
+                if (ok) {
+                    if (z.lambda >= 1.0) {
+                        z.phase = kFinal;
+                        break;
+                    }
+                    z.lambda_good = z.lambda;
+                    post[k] = 3;
+                    z.delta *= 1.5;
+                    z.lambda = std::min(z.lambda + z.delta, 1.0);
+                } else {
+                    z.delta *= 0.5;
+                    if (z.delta < 1e-4 || z.lambda_good < 0.0) {
+                        z.phase = kFinal;
+                        break;
+                    }
+                    pre[k] = 2;
+                    z.lambda = std::min(z.lambda_good + z.delta, 1.0);
+                }
+                if (++z.solves >= max_solves) z.phase = kFinal;
+                break;
+            }
+            case kFinal:
+                z.phase = kDone;
+                z.converged = conv;
+                break;
+            default: break;
+            }
+        }
+        if ((s = actions(post))) return release(), s;
+        any = true;
+    }
+    release();
+    // the ladder's solves say nothing about the tape the plain rung replays
+    if ((s = clear_stale(h))) return s;
+    if (out) {
+        size_t k = 0;
+        uint64_t iters = 0;
+        for (auto& g : h->groups)
+            for (uint32_t l = 0; l < g.lanes; l++) {
+                const Lad& z = lad[g.lane0 + l];
+                const LaneState& st = h->h_state[g.lane0 + l];
+                out[k].bits = z.converged ? kConverged : (st.bits & (kSingular | kParked));
+                out[k].iterations = z.total;
+                out[k].refactor_fallbacks = st.fallbacks;
+                out[k].reserved = 0;
+                iters += z.total;
                 k++;
             }
         h->stats.lane_iterations = iters;

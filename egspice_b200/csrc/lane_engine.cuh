@@ -101,6 +101,12 @@ struct GroupDev {
     // iteration, at least half of a tile's active lanes failed the replay;
     // [1] the smallest such failing lane (the host retapes from its A).
     uint32_t* stale;
+    // ngspice's diagonal-gmin placement for the ladder's gmin steps (slot,
+    // row, column triples: gmin on A[slot], gmin * x[column] on row), and
+    // the lanes' last converged iterate of a ladder rung.
+    const uint32_t* gstamp;
+    uint32_t n_gstamp, gstamp_pad;
+    double* x_good;
     uint32_t stage_mode;  // what a tile stages in shared memory (lane_smem.cuh)
     uint32_t refine_rows; // the row view is staged (FP32 refinement sweeps on)
 };
@@ -116,12 +122,22 @@ struct LaneState {
     uint32_t s_rot, fp64, peels, pad1;
 };
 
+// One lane's solve in a rung of the operating-point continuation ladder
+// (espl_solve_op): its diagonal gmin at the template's gmin stamps (0:
+// none), the scale of its independent sources, whether it solves in this
+// launch and whether from a cold start.
+struct LadderLane {
+    double gmin, src;
+    uint32_t on, init_fix;
+};
+
 struct NewtonParams {
     double reltol, abstol, vntol, gmin, residual_tol;
     uint32_t max_iter, init_fix;
     uint32_t mixed, stall_ticks;   // mixed: FP32 LU; a lane past stall_ticks refactors in FP64
     uint32_t refine;               // mixed: FP64-residual refinement sweeps per solve
     uint32_t pad;
+    const LadderLane* ladder;      // per lane (all templates' lanes), or null: gmin, init_fix, all lanes
 };
 
 struct TranParams {

@@ -48,6 +48,7 @@ struct TileShared {
     unsigned long long acc0[32], acc1[32], acc2[32];
     double limit[32];
     double ag0[32], ag1[32], ag2[32], t[32], xfact[32], dt_next[32];
+    double lgmin[32], lsrc[32];  // the lane's ladder gmin and source scale
     uint32_t method[32], on[32], accept[32], rot[32];
 };
 
@@ -72,23 +73,31 @@ __device__ __forceinline__ void newton_tile(const TileCtx& c, LaneState* s, cons
     const bool sm = d.stage_mode == kStageLu;
     SmemTile st{};
     if (sm) st = smem_tile(dsm, smem_plan(d, kStageLu, MIXED));
+    // a ladder rung's lane: its own gmin (at the gmin stamps), source scale
+    // and cold or warm start
+    const LadderLane* lad = (o.ladder && c.valid) ? &o.ladder[d.lane0 + l] : nullptr;
+    const bool init_fix = lad ? lad->init_fix != 0 : o.init_fix != 0;
     if (warp == 0) {
         sh.active[lane] = (c.valid && on) ? 1u : 0u;
-        sh.bits[lane] = (o.init_fix ? kInitFix : 0u);
+        sh.bits[lane] = (init_fix ? kInitFix : 0u);
         sh.limit[lane] = kXPlausible;
         sh.acc0[lane] = dbits(1.0);
         sh.acc1[lane] = 0;
         sh.acc2[lane] = 0;
-        if (s) {
+        sh.lgmin[lane] = lad ? lad->gmin : 0.0;
+        sh.lsrc[lane] = lad ? lad->src : 1.0;
+        if (s && on) {
             s->iterations = o.max_iter;
             // Mixed tiles factor in FP32 once Newton contracts (warm starts,
             // transient steps); a cold start (INITFIX, MODEINITJCT seeds)
             // walks through ill-conditioned iterates and runs in FP64.
-            s->fp64 = (MIXED && o.init_fix) ? 1u : 0u;
+            s->fp64 = (MIXED && init_fix) ? 1u : 0u;
         }
     }
+    __syncthreads();
+    const double src = sh.lsrc[lane];
     if (eval0 && c.valid && on)
-        for (uint32_t t = warp; t < ninst; t += nw) inst_eval(d, l, t, tran, 0.0, cell_buf(d, 0));
+        for (uint32_t t = warp; t < ninst; t += nw) inst_eval(d, l, t, tran, 0.0, cell_buf(d, 0), src);
     __syncthreads();
     uint32_t cur = 0;
     for (uint32_t it = 0; it < o.max_iter; it++) {
@@ -117,9 +126,24 @@ __device__ __forceinline__ void newton_tile(const TileCtx& c, LaneState* s, cons
                 it0 = (uint32_t)((uint64_t)d.n_items * warp / nw);
                 it1 = (uint32_t)((uint64_t)d.n_items * (warp + 1) / nw);
             }
-            gather_items<T>(d, l, lane, it0, it1, cp, o.gmin, cells, sm ? static_cast<T*>(st.a) : nullptr);
+            gather_items<T>(d, l, lane, it0, it1, cp, o.ladder ? 0.0 : o.gmin, cells,
+                            sm ? static_cast<T*>(st.a) : nullptr);
         }
         __syncthreads();
+        if (o.ladder) {
+            // the rung's gmin at ngspice's diagonal-gmin places (loadGmin,
+            // converger.zig:700-717): A[slot] += gmin, rhs[row] += gmin x[col]
+            const double gl = sh.lgmin[lane];
+            if (warp == 0 && act && gl > 0.0)
+                for (uint32_t k = 0; k < d.n_gstamp; k++) {
+                    const uint32_t slot = d.gstamp[3 * k], row = d.gstamp[3 * k + 1], col = d.gstamp[3 * k + 2];
+                    const double a = LM(d.a, slot) + gl;
+                    LM(d.a, slot) = a;
+                    if (sm) static_cast<T*>(st.a)[slot * 32 + lane] = (T)a;
+                    LM(d.rhs, row) += gl * LM(d.x, col);
+                }
+            __syncthreads();
+        }
         if (it == 0) {
             // plausibleLimit (kernels/lane.zig:202-214).
             double g = 1.0;
@@ -263,7 +287,7 @@ __device__ __forceinline__ void newton_tile(const TileCtx& c, LaneState* s, cons
         if (act) {
             double* next = cell_buf(d, cur ^ 1u);
             for (uint32_t t = warp; t < ninst; t += nw)
-                if (inst_limit_eval(d, l, t, tran, tm, next)) flags |= kLimited;
+                if (inst_limit_eval(d, l, t, tran, tm, next, src)) flags |= kLimited;
             double lim = sh.limit[lane];
             for (uint32_t i = warp; i < d.n; i += nw) {
                 double xi = LM(d.x, i);
@@ -304,7 +328,7 @@ __device__ __forceinline__ void newton_tile(const TileCtx& c, LaneState* s, cons
         cur ^= 1u;
     }
     __syncthreads();
-    if (warp == 0 && s) s->bits = sh.bits[lane];
+    if (warp == 0 && s && on) s->bits = sh.bits[lane];
 }
 
 
@@ -315,7 +339,31 @@ __global__ void __launch_bounds__(WIDE ? kWideThreads : kTileThreads, WIDE ? 1 :
     TileCtx c = tile_ctx(m);
     c.d = stage_template(*c.d, sh.gd, g_dsm, MIXED);
     LaneState* s = (c.warp == 0 && c.valid) ? &st[c.d->lane0 + c.l] : nullptr;
-    newton_tile<MIXED>(c, s, o, tran, false, true, sh, g_dsm, true);
+    const bool on = !o.ladder || (c.valid && o.ladder[c.d->lane0 + c.l].on != 0);
+    newton_tile<MIXED>(c, s, o, tran, false, on, sh, g_dsm, true);
+}
+
+// The ladder's per-lane bookkeeping (action[lane0 + l]): 1 the cold start
+// (x = 0 with the MODEINITJCT limiter seeds, op.zig coldStart), 2 back to the
+// lane's last converged iterate of the rung (x = x_good, limiter state seeded
+// there), 3 keeps the lane's iterate (x_good = x), 4 seeds the limiter
+// state at the lane's x (a warm solve from where it is), 0 nothing. Warp 0
+// only, one thread per lane (no barrier).
+__global__ void __launch_bounds__(kTileThreads) k_ladder_x(TileMap m, const uint8_t* action) {
+    TileCtx c = tile_ctx(m);
+    if (!c.valid || c.warp != 0) return;
+    const GroupDev& d = *c.d;
+    const uint32_t P = d.P, l = c.l;
+    const uint32_t a = action[d.lane0 + l];
+    if (a == 0) return;
+    if (a == 3) {
+        for (uint32_t i = 0; i <= d.n; i++) LM(d.x_good, i) = LM(d.x, i);
+        return;
+    }
+    if (a != 4)
+        for (uint32_t i = 0; i <= d.n; i++) LM(d.x, i) = a == 1 ? 0.0 : LM(d.x_good, i);
+    const uint32_t ninst = n_instances(d);
+    for (uint32_t t = 0; t < ninst; t++) inst_seed(d, l, t, a == 1 ? 1 : 0, d.x);
 }
 
 // Bias-independent prep per (instance, lane) from the raw lane-major rows,

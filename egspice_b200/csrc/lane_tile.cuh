@@ -123,8 +123,9 @@ __device__ __forceinline__ void mos_cells(const GroupDev& d, uint32_t l, uint32_
     LM(cells, c + 14) = o.gbd + o.gbs;
 }
 
+// `src` scales the independent sources (source stepping; 1 otherwise).
 __device__ __forceinline__ void inst_eval(const GroupDev& d, uint32_t l, uint32_t t, int tran, double tm,
-                                          double* __restrict__ cells) {
+                                          double* __restrict__ cells, double src = 1.0) {
     const uint32_t P = d.P;
     const double* __restrict__ x = d.x;
     uint32_t i = t;
@@ -156,7 +157,7 @@ __device__ __forceinline__ void inst_eval(const GroupDev& d, uint32_t l, uint32_
                                   LM(pp, b9 + 5), LM(pp, b9 + 6), LM(pp, b9 + 7), LM(pp, b9 + 8), tran, tm);
         uint32_t c = d.c_vsrc + kVsrcCells * i;
         LM(cells, c) = LM(x, tb);
-        LM(cells, c + 1) = (LM(x, tp) - LM(x, tn)) - val;
+        LM(cells, c + 1) = (LM(x, tp) - LM(x, tn)) - val * src;
         return;
     }
     i -= d.n_vsrc;
@@ -165,7 +166,7 @@ __device__ __forceinline__ void inst_eval(const GroupDev& d, uint32_t l, uint32_
         uint32_t b9 = 9 * i;
         LM(cells, d.c_isrc + i) = source_value(LM(pp, b9 + 0), LM(pp, b9 + 1), LM(pp, b9 + 2), LM(pp, b9 + 3),
                                                LM(pp, b9 + 4), LM(pp, b9 + 5), LM(pp, b9 + 6), LM(pp, b9 + 7),
-                                               LM(pp, b9 + 8), tran, tm);
+                                               LM(pp, b9 + 8), tran, tm) * src;
         return;
     }
     i -= d.n_isrc;
@@ -226,13 +227,13 @@ __device__ __forceinline__ void inst_seed(const GroupDev& d, uint32_t l, uint32_
 // the next Newton iteration's instance phase would compute), on one load of
 // the instance's state: true when the limiter clamped.
 __device__ __forceinline__ bool inst_limit_eval(const GroupDev& d, uint32_t l, uint32_t t, int tran, double tm,
-                                                double* __restrict__ cells) {
+                                                double* __restrict__ cells, double src = 1.0) {
     const uint32_t P = d.P;
     const double* x = d.x;
     const double eps16 = 16 * 2.220446049250313e-16;
     uint32_t base = d.n_res + d.n_cap + d.n_vsrc + d.n_isrc;
     if (t < base) {
-        inst_eval(d, l, t, tran, tm, cells);
+        inst_eval(d, l, t, tran, tm, cells, src);
         return false;
     }
     uint32_t i = t - base;
@@ -248,7 +249,7 @@ __device__ __forceinline__ bool inst_limit_eval(const GroupDev& d, uint32_t l, u
     }
     i -= d.n_dio;
     if (i >= d.n_mos) {
-        inst_eval(d, l, t, tran, tm, cells);
+        inst_eval(d, l, t, tran, tm, cells, src);
         return false;
     }
     const uint32_t* tmv = d.mos_t + 4 * i;

@@ -60,6 +60,8 @@ def lib():
         L.espl_get_period_meas.restype = C.c_uint32
         L.espl_get_stats.argtypes = [C.c_void_p, C.POINTER(Stats)]
         L.espl_get_stats.restype = C.c_uint32
+        L.espl_solve_op.argtypes = [C.c_void_p, C.POINTER(NewtonOpts), C.POINTER(LaneNewton)]
+        L.espl_solve_op.restype = C.c_uint32
         L.espl_set_meas.argtypes = [C.c_void_p, C.c_uint32, C.POINTER(MeasPass), C.c_uint32]
         L.espl_set_meas.restype = C.c_uint32
         L.espl_get_meas.argtypes = [C.c_void_p, C.c_uint32, f64p, f64p]
@@ -130,6 +132,15 @@ class Lanes:
         """Newton per lane; returns [total, 3] of (bits, iterations, fp64 fallbacks)."""
         out = (LaneNewton * self.total)()
         self._check(lib().espl_solve_static(self.h, C.byref(opts), out), "espl_solve_static")
+        return np.array([[o.bits, o.iterations, o.refactor_fallbacks] for o in out], dtype=np.int64)
+
+    def solve_op(self, opts: NewtonOpts) -> np.ndarray:
+        """The operating point from the cold start with the continuation
+        ladder (plain rung, gmin stepping, source stepping, final solve);
+        returns [total, 3] of (bits, iterations over every rung, fp64
+        fallbacks)."""
+        out = (LaneNewton * self.total)()
+        self._check(lib().espl_solve_op(self.h, C.byref(opts), out), "espl_solve_op")
         return np.array([[o.bits, o.iterations, o.refactor_fallbacks] for o in out], dtype=np.int64)
 
     def init_steps(self, topts: TranOpts):

@@ -170,6 +170,21 @@ espl_status espl_get_x(espl_lanes *h, uint32_t net, double *x);
  * of every template, template-major. */
 espl_status espl_solve_static(espl_lanes *h, const espl_newton_opts *opts, espl_lane_newton *out);
 
+/* The operating point of every lane with the reference's continuation ladder
+ * (`op.solve` -> solveLadder / afterPlain, src/analysis/dc/op.zig:111-330):
+ * the plain rung from the cold start (x = 0, MODEINITJCT seeds), and for a
+ * lane that fails it the dynamic gmin descent (gmin from 1e-3 toward 1e-12 at
+ * ngspice's diagonal-gmin places, the step factor adapting to the Newton
+ * count, backing off on failures, a stall exit), a clean solve without gmin,
+ * then source stepping (an adaptive source scale from 0 to 1, with the
+ * sources-off gmin start) and a final full-source solve. The JFNK and OPtran
+ * rungs are not built: a lane that fails the final solve reports not
+ * converged. Each lane runs its own ladder; the lanes still on it solve
+ * together, one launch per ladder solve. iterations sums every rung's Newton
+ * iterations (saturating at 65535). Uses opts' tolerances; gmin and init_fix
+ * are the ladder's. */
+espl_status espl_solve_op(espl_lanes *h, const espl_newton_opts *opts, espl_lane_newton *out);
+
 /* Transient lanes with device step control (`initSteps` lanes.zig:1827,
  * `deviceLaunch` :1917; the step machine `stepBegin/stepEndA/stepEndB`,
  * src/solver/kernels/lane.zig:505-700). */

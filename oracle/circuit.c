@@ -52,6 +52,10 @@ typedef struct {
     int has_charge;
     orc_direct *slv;
     double *x_old, *dx;
+    double src;           /* independent sources' scale (source stepping) */
+    uint32_t *gst;        /* gmin stamps (slot, row, col) of the ladder's gmin steps */
+    uint32_t n_gst;
+    double gst_gmin;      /* the gmin they load (0: none) */
 } ockt;
 
 static uint32_t terms_of(uint32_t kind) {
@@ -95,6 +99,7 @@ static int stamps(uint32_t kind, uint32_t r, uint32_t c) {
 }
 
 static void ckt_free(ockt *k) {
+    if (k) free(k->gst);
     if (!k) return;
     for (uint32_t i = 0; i < k->nb; i++) {
         free(k->b[i].slot);
@@ -180,6 +185,7 @@ static ockt *ckt_new(const espl_netlist *net, uint32_t lane, const uint32_t *q_o
     k->dx = (double *)calloc(n1, sizeof(double));
     k->slv = orc_direct_new(k->n, k->col_ptr, k->row_idx, q_order);
     if (!k->slv) { ckt_free(k); return NULL; }
+    k->src = 1.0;
     return k;
 }
 
@@ -310,13 +316,13 @@ static void eval_planes(ockt *k, const double *x, int tran, double t) {
                 k->g[sl[0 * 3 + 2]] += 1.0;
                 add_rhs(k, tm[1], -ib);
                 k->g[sl[1 * 3 + 2]] += -1.0;
-                add_rhs(k, tm[2], (xat(x, tm[0]) - xat(x, tm[1])) - val);
+                add_rhs(k, tm[2], (xat(x, tm[0]) - xat(x, tm[1])) - val * k->src);
                 k->g[sl[2 * 3 + 0]] += 1.0;
                 k->g[sl[2 * 3 + 1]] += -1.0;
                 break;
             }
             case ESPL_ISRC: {
-                double val = dev_source_value(p, tran, t);
+                double val = dev_source_value(p, tran, t) * k->src;
                 add_rhs(k, tm[0], val);
                 add_rhs(k, tm[1], -val);
                 break;
@@ -482,6 +488,12 @@ static orc_newton_result newton(ockt *k, double *x, const espl_newton_opts *o, i
             for (uint32_t i = 0; i < k->n; i++) k->a[k->diag[i]] += o->gmin;
             for (uint32_t i = 0; i < k->n; i++) k->rhs[i] += o->gmin * x[i];
         }
+        if (k->n_gst && k->gst_gmin > 0) { /* converger.zig loadGmin at the stamps */
+            for (uint32_t s = 0; s < k->n_gst; s++) {
+                k->a[k->gst[3 * s]] += k->gst_gmin;
+                k->rhs[k->gst[3 * s + 1]] += k->gst_gmin * x[k->gst[3 * s + 2]];
+            }
+        }
         if (iter == 0) limit = plausible_limit(k, x, k->rhs, v);
         int path = -1;
         int frc = orc_direct_factor(k->slv, v, &path);
@@ -556,6 +568,222 @@ static void op_one(job_t *j, uint32_t li) {
     ckt_free(k);
 }
 
+/* ---------------- the operating-point ladder ---------------- */
+
+/* op.zig gminStamps :712-792: ngspice's diagonal-gmin places after Sparse's
+ * spMNA_Preorder, read off the last assembly's G values (k->g). */
+static void gmin_stamps(ockt *k) {
+    uint32_t n = k->n, none = UINT32_MAX;
+    uint32_t *perm = (uint32_t *)malloc(sizeof(uint32_t) * n), *dcol = (uint32_t *)malloc(sizeof(uint32_t) * n);
+    for (uint32_t i = 0; i < n; i++) {
+        uint32_t slot = k->diag[i];
+        perm[i] = i;
+        dcol[i] = (k->cur_row[i] && k->g[slot] == 0 && k->c[slot] == 0) ? none : i;
+    }
+    uint32_t start = 1;
+    for (;;) {
+        int swapped = 0, again = 0;
+        for (int pass = 0; pass < 2; pass++) {
+            for (uint32_t jj = start; jj < n; jj++) {
+                if (pass == 1 && swapped) break;
+                if (dcol[jj] != none) continue;
+                /* CountTwins: +-1 entries of column position jj whose transposes are +-1 */
+                uint32_t cnt = 0, trow = 0, col = perm[jj];
+                for (uint32_t p = k->col_ptr[col]; p < k->col_ptr[col + 1]; p++) {
+                    uint32_t r = k->row_idx[p];
+                    if (fabs(k->g[p]) != 1.0) continue;
+                    uint32_t q = find_slot(k, jj, perm[r]);
+                    if (q >= k->nnz || fabs(k->g[q]) != 1.0) continue;
+                    cnt++;
+                    if (cnt == 1) trow = r;
+                    else break;
+                }
+                int take = pass == 0 ? cnt == 1 : cnt > 0;
+                if (take) {
+                    dcol[jj] = perm[trow];
+                    dcol[trow] = perm[jj];
+                    uint32_t t = perm[jj]; perm[jj] = perm[trow]; perm[trow] = t;
+                    swapped = 1;
+                } else if (pass == 0 && cnt > 1 && !again) {
+                    again = 1;
+                    start = jj;
+                }
+            }
+            if (pass == 0 && !again) break;
+        }
+        if (!again || !swapped) break;
+    }
+    free(k->gst);
+    k->gst = (uint32_t *)malloc(sizeof(uint32_t) * 3 * (n ? n : 1));
+    k->n_gst = 0;
+    for (uint32_t i = 1; i < n; i++) {
+        if (dcol[i] == none) continue;
+        uint32_t slot = find_slot(k, i, dcol[i]);
+        if (slot >= k->nnz) continue;
+        k->gst[3 * k->n_gst] = slot;
+        k->gst[3 * k->n_gst + 1] = i;
+        k->gst[3 * k->n_gst + 2] = dcol[i];
+        k->n_gst++;
+    }
+    free(perm);
+    free(dcol);
+}
+
+static void cold_start(ockt *k, double *x) {
+    memset(x, 0, sizeof(double) * k->n);
+    seed_limits(k, x, 1);
+}
+
+static orc_newton_result run_rung(ockt *k, double *x, const espl_newton_opts *base, double gmin, double src,
+                                  int init_fix, uint32_t max_iter, uint32_t *total) {
+    espl_newton_opts o = *base;
+    o.gmin = 0.0;
+    o.init_fix = init_fix ? 1 : 0;
+    o.max_iter = max_iter;
+    k->gst_gmin = gmin;
+    k->src = src;
+    if (!init_fix) seed_limits(k, x, 0);
+    orc_newton_result r = newton(k, x, &o, 0, 0.0, NULL, NULL);
+    k->gst_gmin = 0.0;
+    k->src = 1.0;
+    uint32_t it = r.singular ? 0 : r.iterations;
+    *total = *total + it > 65535u ? 65535u : *total + it;
+    return r;
+}
+
+/* op.zig afterPlain rungs 2 and 3 and the final solve (:163-312), after the
+ * plain rung failed; gminFactor :384-388, gminStalled :363-376,
+ * sourcesOffGmin :397-421. */
+static int ladder_one(ockt *k, double *x, const espl_newton_opts *o, uint32_t *total) {
+    const double gtarget = 1e-12, gmin_start = 1e-2;
+    const uint32_t budget = 100, max_solves = 1000, stall = 20;
+    const double stall_factor = pow(10.0, 1.0 / stall);
+    uint32_t n = k->n;
+    double *x_good = (double *)malloc(sizeof(double) * n);
+    double *st_g = (double *)malloc(sizeof(double) * max_solves);
+    int *st_c = (int *)malloc(sizeof(int) * max_solves);
+    int converged = 0;
+    gmin_stamps(k);
+    cold_start(k, x);
+    {
+        double factor = 10.0, good = gmin_start, g = good / factor;
+        int have_good = 0;
+        for (uint32_t solves = 0; solves < max_solves; solves++) {
+            double tried = g;
+            orc_newton_result r = run_rung(k, x, o, g, 1.0, !have_good, budget, total);
+            int refused = r.singular;
+            int conv = !refused && r.converged;
+            if (conv) {
+                if (g <= gtarget) {
+                    orc_newton_result c = run_rung(k, x, o, 0.0, 1.0, 0, budget, total);
+                    if (c.converged && !c.singular) { converged = 1; goto done; }
+                    break;
+                }
+                memcpy(x_good, x, sizeof(double) * n);
+                have_good = 1;
+                good = g;
+                uint32_t it = r.iterations;
+                if (it <= budget / 4) factor = fmin(factor * sqrt(factor), 10.0);
+                else if (it > 3 * (budget / 4)) factor = fmax(sqrt(factor), 1.00005);
+                if (g < factor * gtarget) { factor = g / gtarget; g = gtarget; }
+                else g /= factor;
+            } else {
+                if (factor < 1.00005) break;
+                factor = refused ? sqrt(factor) : sqrt(sqrt(factor));
+                g = good / factor;
+                if (have_good) memcpy(x, x_good, sizeof(double) * n);
+                else cold_start(k, x);
+            }
+            st_g[solves] = tried;
+            st_c[solves] = conv;
+            uint32_t m = solves + 1;
+            if (m >= stall) {
+                double gd = gmin_start;
+                int stalled = 1;
+                for (uint32_t i = 0; i < m; i++) {
+                    if (st_c[i]) gd = st_g[i];
+                    if (i < m - stall) continue;
+                    double following = i + 1 < m ? st_g[i + 1] : g;
+                    if (gd / following >= stall_factor) { stalled = 0; break; }
+                }
+                if (stalled) break;
+            }
+        }
+    }
+    cold_start(k, x);
+    {
+        double lambda = 0.0, lambda_good = -1.0, delta = 0.25;
+        for (uint32_t solves = 0; solves < max_solves; solves++) {
+            orc_newton_result r = run_rung(k, x, o, 0.0, lambda, lambda_good < 0.0, budget, total);
+            int conv = !r.singular && r.converged;
+            if (!conv && lambda_good < 0.0) {
+                /* sourcesOffGmin: eleven solves from 1e10 x gmin down a decade each */
+                cold_start(k, x);
+                double g = gtarget * 1e10;
+                conv = 1;
+                for (int i = 0; i < 11; i++) {
+                    orc_newton_result s = run_rung(k, x, o, g, lambda, i == 0, budget, total);
+                    if (!(s.converged && !s.singular)) { conv = 0; break; }
+                    g /= 10;
+                }
+            }
+            if (conv) {
+                if (lambda >= 1.0) break;
+                lambda_good = lambda;
+                memcpy(x_good, x, sizeof(double) * n);
+                delta *= 1.5;
+                lambda = fmin(lambda + delta, 1.0);
+            } else {
+                delta *= 0.5;
+                if (delta < 1e-4) break;
+                if (lambda_good < 0.0) break;
+                memcpy(x, x_good, sizeof(double) * n);
+                lambda = fmin(lambda_good + delta, 1.0);
+            }
+        }
+    }
+    {
+        orc_newton_result f = run_rung(k, x, o, 0.0, 1.0, 0, budget, total);
+        converged = f.converged && !f.singular;
+    }
+done:
+    free(x_good);
+    free(st_g);
+    free(st_c);
+    return converged;
+}
+
+static void op_ladder_one(job_t *j, uint32_t li) {
+    uint32_t lane = j->lane0 + li;
+    uint32_t n = j->net->n;
+    ockt *k = ckt_new(j->net, lane, j->q);
+    double *x = j->x_out + (size_t)li * n;
+    orc_newton_result *res = &j->res[li];
+    memset(res, 0, sizeof(*res));
+    if (!k) { res->singular = 1; return; }
+    cold_start(k, x);
+    espl_newton_opts plain = *j->opts;
+    plain.gmin = 0.0;
+    plain.init_fix = 1;
+    orc_newton_result r = newton(k, x, &plain, 0, 0.0, NULL, NULL);
+    uint32_t total = r.singular ? 0 : r.iterations;
+    int conv = r.converged && !r.singular;
+    if (!conv) conv = ladder_one(k, x, j->opts, &total);
+    res->converged = conv;
+    res->iterations = total;
+    ckt_free(k);
+}
+
+static void *op_ladder_worker(void *arg) {
+    job_t *j = (job_t *)arg;
+    for (;;) {
+        uint32_t li = atomic_fetch_add(&j->next, 1);
+        if (li >= j->count) break;
+        op_ladder_one(j, li);
+    }
+    return NULL;
+}
+
 static void *op_worker(void *arg) {
     job_t *j = (job_t *)arg;
     for (;;) {
@@ -575,6 +803,25 @@ static int run_pool(job_t *j, uint32_t threads, void *(*fn)(void *)) {
     for (uint32_t i = 0; i < threads; i++) pthread_create(&th[i], NULL, fn, j);
     for (uint32_t i = 0; i < threads; i++) pthread_join(th[i], NULL);
     free(th);
+    return 0;
+}
+
+int orc_op_ladder(const espl_netlist *net, uint32_t lane0, uint32_t count, const espl_newton_opts *opts,
+                  double *x_out, orc_newton_result *res, uint32_t threads) {
+    uint32_t *q = (uint32_t *)malloc(sizeof(uint32_t) * (net->n ? net->n : 1));
+    if (orc_order(net->n, net->col_ptr, net->row_idx, q) != 0) { free(q); return -1; }
+    job_t j;
+    memset(&j, 0, sizeof(j));
+    j.net = net;
+    j.lane0 = lane0;
+    j.count = count;
+    j.opts = opts;
+    j.x_out = x_out;
+    j.res = res;
+    j.q = q;
+    atomic_init(&j.next, 0);
+    run_pool(&j, threads, op_ladder_worker);
+    free(q);
     return 0;
 }
 

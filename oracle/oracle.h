@@ -72,6 +72,10 @@ typedef struct {
 /* Operating point of lanes [lane0, lane0 + count) of `net`, each from its
  * own cold start (init_fix = 1) or from x_in (warm). x_out is point-major
  * [count][n]. Runs on `threads` host threads, one lane per task. */
+/* op.solve's ladder per lane (op.zig solveLadder / afterPlain rungs 1-3 and
+ * the final solve): res[i].converged and .iterations (all rungs). */
+int orc_op_ladder(const espl_netlist *net, uint32_t lane0, uint32_t count, const espl_newton_opts *opts,
+                  double *x_out, orc_newton_result *res, uint32_t threads);
 int orc_op_lanes(const espl_netlist *net, uint32_t lane0, uint32_t count, const espl_newton_opts *opts,
                  const double *x_in, double *x_out, orc_newton_result *res, uint32_t threads);
 

@@ -37,6 +37,8 @@ def lib():
         L.orc_tran_meas.restype = C.c_int
         L.orc_meas_series.argtypes = [C.POINTER(MeasPass), f64p, f64p, C.c_uint32, f64p, f64p]
         L.orc_meas_series.restype = C.c_int
+        L.orc_op_ladder.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, f64p, C.c_void_p, C.c_uint32]
+        L.orc_op_ladder.restype = C.c_int
         L.orc_order.argtypes = [C.c_uint32, u32p, u32p, u32p]
         L.orc_order.restype = C.c_int
         L.orc_order_ws.argtypes = [C.c_uint32, u32p, u32p, u32p, u32p, C.c_size_t]
@@ -207,6 +209,20 @@ def op_lanes(net: Netlist, opts: NewtonOpts, lane0: int = 0, count: Optional[int
     if x_in is not None:
         xi, xin = _f64(x_in)
     r = lib().orc_op_lanes(C.byref(cn.c), lane0, count, C.byref(opts), xin, x.ctypes.data_as(f64p), res, threads)
+    assert r == 0
+    out = np.array([[e.converged, e.singular, e.iterations] for e in res], dtype=np.int64)
+    return x, out
+
+
+def op_ladder(net: Netlist, opts: NewtonOpts, threads: int = 1) -> Tuple[np.ndarray, np.ndarray]:
+    """Operating points of every lane through the continuation ladder from
+    the cold start; returns x [lanes, n] and results [lanes, 3] (converged,
+    singular, iterations over every rung)."""
+    count = net.lanes
+    cn = CNet(net)
+    x = np.zeros((count, net.n))
+    res = (OrcNewtonResult * count)()
+    r = lib().orc_op_ladder(C.byref(cn.c), 0, count, C.byref(opts), x.ctypes.data_as(f64p), res, threads)
     assert r == 0
     out = np.array([[e.converged, e.singular, e.iterations] for e in res], dtype=np.int64)
     return x, out

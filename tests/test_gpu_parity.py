@@ -259,3 +259,27 @@ def test_streaming_meas_passes(oracle, precision):
     # where an extremum was taken is not pinned: the rails are flat, and the
     # last of several samples within an ulp of the extremum is the one kept
     assert ((a[:, 2:4] >= 0) & (a[:, 2:4] <= opts.t_stop)).all()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_operating_point_ladder(oracle, precision):
+    """espl_solve_op from the cold start: the op-amp lanes the plain rung
+    leaves unconverged walk the continuation ladder on the device and all
+    converge, onto the oracle ladder's fixed point within the Newton
+    tolerance (each lane's ladder may step differently once a Newton count
+    differs by one); lanes the plain rung converges keep the plain answer."""
+    net = decks.miller_opamp(256)
+    opts = abi.newton_opts()
+    xo, ro = oracle.op_ladder(net, opts, threads=8)
+    with Lanes([net], precision=precision) as L:
+        r = L.solve_op(opts)
+        x = L.get_x(0)
+    assert (ro[:, 0] == 1).all()
+    assert ((r[:, 0] & abi.CONVERGED) != 0).all(), int(((r[:, 0] & abi.CONVERGED) != 0).sum())
+    cur = np.asarray(net.current_rows, dtype=bool)
+    tol = opts.reltol * np.maximum(np.abs(x), np.abs(xo)) + np.where(cur, opts.abstol, opts.vntol)
+    assert float((np.abs(x - xo) / tol).max()) <= 2.0
+    same = float((r[:, 1] == ro[:, 2]).mean())
+    print(f"lanes with the oracle's ladder iteration count: {same:.2f}")
+    if precision == "fp64":
+        assert same >= 0.5
