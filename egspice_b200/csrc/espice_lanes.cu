@@ -14,6 +14,7 @@
 
 #include "../../include/espice_lanes.h"
 #include "lane_kernels.cuh"
+#include "lane_ac.cuh"
 #include "tape.h"
 
 using namespace espl;
@@ -1492,6 +1493,101 @@ espl_status espl_solve_op(espl_lanes* h, const espl_newton_opts* opts, espl_lane
             }
         h->stats.lane_iterations = iters;
     }
+    return ESPL_OK;
+}
+
+espl_status espl_ac(espl_lanes* h, uint32_t net, uint32_t vsrc, const double* omega, uint32_t n_freq,
+                    const uint32_t* rows, uint32_t n_rows, double* out_re, double* out_im) {
+    if (!h || net >= h->groups.size() || !omega || !n_freq || !rows || !n_rows || !out_re || !out_im)
+        return ESPL_INVALID_ARGUMENT;
+    Group& g = h->groups[net];
+    const KindHost& vk = g.kinds[ESPL_VSRC];
+    if (vsrc >= vk.count) return fail(h, ESPL_INVALID_ARGUMENT, "no such voltage source");
+    const uint32_t exc = vk.term[3 * vsrc + 2];
+    if (exc >= g.n) return fail(h, ESPL_INVALID_ARGUMENT, "the source has no branch row");
+    for (uint32_t k = 0; k < n_rows; k++)
+        if (rows[k] >= g.n) return fail(h, ESPL_INVALID_ARGUMENT, "AC row out of range");
+    for (uint32_t f = 0; f < n_freq; f++)
+        if (!(omega[f] >= 0.0) || !(omega[f] < INFINITY)) return fail(h, ESPL_INVALID_ARGUMENT, "bad frequency");
+    const size_t P = g.P, nnz = g.nnz, n = g.n;
+    std::vector<void*> own;
+    auto release = [&]() {
+        for (void* p : own) cudaFree(p);
+    };
+    espl_status s;
+    double *gpl, *cpl;
+    uint32_t* tiles;
+    if ((s = dalloc(h, own, &gpl, nnz * P)) || (s = dalloc(h, own, &cpl, nnz * P)) ||
+        (s = dalloc(h, own, &tiles, P / 32)))
+        return release(), s;
+    std::vector<uint32_t> tl(P / 32);
+    for (uint32_t t = 0; t < P / 32; t++) tl[t] = g.tile0 + t;
+    CK(cudaMemcpyAsync(tiles, tl.data(), tl.size() * 4, cudaMemcpyHostToDevice, h->stream));
+    const TileMap m{h->d_groups, h->d_warp_group, tiles, (uint32_t)tl.size()};
+    k_ac_planes<<<(uint32_t)tl.size(), kBlock, 0, h->stream>>>(m, gpl, cpl);
+    CK(cudaGetLastError());
+    // the tape: the lead lane's |G| + w_c |C| at the geometric centre
+    std::vector<double> g0(nnz), c0(nnz);
+    if (nnz) {
+        CK(cudaMemcpy2DAsync(g0.data(), 8, gpl, 8 * P, 8, nnz, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpy2DAsync(c0.data(), 8, cpl, 8 * P, 8, nnz, cudaMemcpyDeviceToHost, h->stream));
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    double lo = INFINITY, hi = 0.0;
+    for (uint32_t f = 0; f < n_freq; f++) {
+        if (omega[f] > 0.0) lo = std::min(lo, omega[f]);
+        hi = std::max(hi, omega[f]);
+    }
+    const double wc = hi > 0.0 ? std::sqrt(lo * hi) : 0.0;
+    std::vector<double> proxy(nnz);
+    for (size_t p = 0; p < nnz; p++) proxy[p] = std::fabs(g0[p]) + wc * std::fabs(c0[p]);
+    Tape t;
+    if (!factor_tape(g.n, g.col_ptr.data(), g.row_idx.data(), proxy.data(), g.q, t))
+        return release(), fail(h, ESPL_NO_TAPE, "the lead lane's AC proxy matrix is singular");
+    if (!t.void_slots.empty()) return release(), fail(h, ESPL_INCOMPATIBLE, "AC lanes do not replay void columns");
+    std::vector<uint32_t> qinv(n);
+    for (uint32_t j = 0; j < n; j++) qinv[t.q[j]] = j;
+    AcArgs A{};
+    const uint32_t *uq, *uqinv, *upinv, *uprow, *ulp, *uli, *uup, *uui, *urows;
+    if ((s = dupload(h, own, &uq, t.q)) || (s = dupload(h, own, &uqinv, qinv)) || (s = dupload(h, own, &upinv, t.pinv)) ||
+        (s = dupload(h, own, &uprow, t.prow)) || (s = dupload(h, own, &ulp, t.lp)) || (s = dupload(h, own, &uli, t.li)) ||
+        (s = dupload(h, own, &uup, t.up)) || (s = dupload(h, own, &uui, t.ui)) ||
+        (s = dupload(h, own, &urows, std::vector<uint32_t>(rows, rows + n_rows))))
+        return release(), s;
+    const double* uom;
+    if ((s = dupload(h, own, &uom, std::vector<double>(omega, omega + n_freq)))) return release(), s;
+    A.q = uq;
+    A.qinv = uqinv;
+    A.pinv = upinv;
+    A.prow = uprow;
+    A.lp = ulp;
+    A.li = uli;
+    A.up = uup;
+    A.ui = uui;
+    A.n = g.n;
+    A.nnz_l = (uint32_t)t.li.size();
+    A.nnz_u = (uint32_t)t.ui.size();
+    A.n_freq = n_freq;
+    A.n_rows = n_rows;
+    A.exc_row = exc;
+    A.omega = uom;
+    A.rows = urows;
+    A.g = gpl;
+    A.c = cpl;
+    const size_t nl = std::max<size_t>(A.nnz_l, 1), nu = std::max<size_t>(A.nnz_u, 1);
+    if ((s = dalloc(h, own, &A.ar, nnz * P)) || (s = dalloc(h, own, &A.ai, nnz * P)) ||
+        (s = dalloc(h, own, &A.wr, n * P)) || (s = dalloc(h, own, &A.wi, n * P)) || (s = dalloc(h, own, &A.lr, nl * P)) ||
+        (s = dalloc(h, own, &A.li_, nl * P)) || (s = dalloc(h, own, &A.ur, nu * P)) ||
+        (s = dalloc(h, own, &A.ui_, nu * P)) || (s = dalloc(h, own, &A.dr, n * P)) || (s = dalloc(h, own, &A.di, n * P)) ||
+        (s = dalloc(h, own, &A.out_re, P * n_freq * n_rows)) || (s = dalloc(h, own, &A.out_im, P * n_freq * n_rows)))
+        return release(), s;
+    k_ac<<<(uint32_t)tl.size(), kBlock, 0, h->stream>>>(m, A);
+    CK(cudaGetLastError());
+    const size_t per = (size_t)n_freq * n_rows;
+    CK(cudaMemcpyAsync(out_re, A.out_re, sizeof(double) * per * g.lanes, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(out_im, A.out_im, sizeof(double) * per * g.lanes, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    release();
     return ESPL_OK;
 }
 

@@ -94,8 +94,9 @@ __device__ __forceinline__ void newton_tile(const TileCtx& c, LaneState* s, cons
             s->fp64 = (MIXED && init_fix) ? 1u : 0u;
         }
     }
-    __syncthreads();
-    const double src = sh.lsrc[lane];
+    // the ladder's source scale (uniform branch: o.ladder is the launch's)
+    if (o.ladder) __syncthreads();
+    const double src = o.ladder ? sh.lsrc[lane] : 1.0;
     if (eval0 && c.valid && on)
         for (uint32_t t = warp; t < ninst; t += nw) inst_eval(d, l, t, tran, 0.0, cell_buf(d, 0), src);
     __syncthreads();

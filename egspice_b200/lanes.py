@@ -60,6 +60,8 @@ def lib():
         L.espl_get_period_meas.restype = C.c_uint32
         L.espl_get_stats.argtypes = [C.c_void_p, C.POINTER(Stats)]
         L.espl_get_stats.restype = C.c_uint32
+        L.espl_ac.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, f64p, C.c_uint32, u32p, C.c_uint32, f64p, f64p]
+        L.espl_ac.restype = C.c_uint32
         L.espl_solve_op.argtypes = [C.c_void_p, C.POINTER(NewtonOpts), C.POINTER(LaneNewton)]
         L.espl_solve_op.restype = C.c_uint32
         L.espl_set_meas.argtypes = [C.c_void_p, C.c_uint32, C.POINTER(MeasPass), C.c_uint32]
@@ -142,6 +144,19 @@ class Lanes:
         out = (LaneNewton * self.total)()
         self._check(lib().espl_solve_op(self.h, C.byref(opts), out), "espl_solve_op")
         return np.array([[o.bits, o.iterations, o.refactor_fallbacks] for o in out], dtype=np.int64)
+
+    def ac(self, net: int, vsrc: int, omega, rows) -> np.ndarray:
+        """Small-signal response to a unit AC voltage on voltage source
+        `vsrc` of template `net` at angular frequencies `omega`: complex
+        [lanes, len(omega), len(rows)]."""
+        om = np.ascontiguousarray(omega, dtype=np.float64)
+        rw = np.ascontiguousarray(rows, dtype=np.uint32)
+        lanes = self.nets[net].lanes
+        re = np.zeros((lanes, len(om), len(rw)))
+        im = np.zeros((lanes, len(om), len(rw)))
+        self._check(lib().espl_ac(self.h, net, vsrc, om.ctypes.data_as(f64p), len(om), rw.ctypes.data_as(u32p), len(rw),
+                                  re.ctypes.data_as(f64p), im.ctypes.data_as(f64p)), "espl_ac")
+        return re + 1j * im
 
     def init_steps(self, topts: TranOpts):
         self._check(lib().espl_init_steps(self.h, C.byref(topts)), "espl_init_steps")

@@ -185,6 +185,21 @@ espl_status espl_solve_static(espl_lanes *h, const espl_newton_opts *opts, espl_
  * are the ladder's. */
 espl_status espl_solve_op(espl_lanes *h, const espl_newton_opts *opts, espl_lane_newton *out);
 
+/* Small-signal AC lanes (the reference's frequency-domain lanes,
+ * src/solver/lane/clu.zig over src/analysis/gpu/freq.zig): every lane of
+ * template `net` linearized at its current x (an operating point: call after
+ * espl_solve_op or espl_solve_static), driven by a unit AC voltage on its
+ * voltage source number `vsrc` (in the order of the template's ESPL_VSRC
+ * batches), solved at the angular frequencies omega[n_freq]:
+ * (G + j omega C) x = e. The complex values replay a real pivot tape chosen
+ * on the host from the lead lane's |G| + omega_c |C| at the geometric centre
+ * frequency; a lane and frequency whose pivot fails the check (max(|re|,
+ * |im|) of the pivot against 1e-12 of its column) reports NaN. Out:
+ * out_re/out_im[lane][freq][k] = x(omega)[rows[k]]. Leaves the lanes' limiter
+ * state seeded at x. */
+espl_status espl_ac(espl_lanes *h, uint32_t net, uint32_t vsrc, const double *omega, uint32_t n_freq,
+                    const uint32_t *rows, uint32_t n_rows, double *out_re, double *out_im);
+
 /* Transient lanes with device step control (`initSteps` lanes.zig:1827,
  * `deviceLaunch` :1917; the step machine `stepBegin/stepEndA/stepEndB`,
  * src/solver/kernels/lane.zig:505-700). */

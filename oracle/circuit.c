@@ -806,6 +806,23 @@ static int run_pool(job_t *j, uint32_t threads, void *(*fn)(void *)) {
     return 0;
 }
 
+int orc_planes(const espl_netlist *net, uint32_t lane, const double *x, double *g, double *c) {
+    uint32_t *q = (uint32_t *)malloc(sizeof(uint32_t) * (net->n ? net->n : 1));
+    if (orc_order(net->n, net->col_ptr, net->row_idx, q) != 0) { free(q); return -1; }
+    ockt *k = ckt_new(net, lane, q);
+    free(q);
+    if (!k) return -1;
+    double *xx = (double *)malloc(sizeof(double) * (net->n ? net->n : 1));
+    memcpy(xx, x, sizeof(double) * net->n);
+    seed_limits(k, xx, 0);
+    eval_planes(k, xx, 0, 0.0);
+    memcpy(g, k->g, sizeof(double) * k->nnz);
+    memcpy(c, k->c, sizeof(double) * k->nnz);
+    free(xx);
+    ckt_free(k);
+    return 0;
+}
+
 int orc_op_ladder(const espl_netlist *net, uint32_t lane0, uint32_t count, const espl_newton_opts *opts,
                   double *x_out, orc_newton_result *res, uint32_t threads) {
     uint32_t *q = (uint32_t *)malloc(sizeof(uint32_t) * (net->n ? net->n : 1));

@@ -76,6 +76,8 @@ typedef struct {
  * the final solve): res[i].converged and .iterations (all rungs). */
 int orc_op_ladder(const espl_netlist *net, uint32_t lane0, uint32_t count, const espl_newton_opts *opts,
                   double *x_out, orc_newton_result *res, uint32_t threads);
+/* G and C of lane `lane` linearized at x (limiter state seeded there). */
+int orc_planes(const espl_netlist *net, uint32_t lane, const double *x, double *g, double *c);
 int orc_op_lanes(const espl_netlist *net, uint32_t lane0, uint32_t count, const espl_newton_opts *opts,
                  const double *x_in, double *x_out, orc_newton_result *res, uint32_t threads);
 

@@ -37,6 +37,8 @@ def lib():
         L.orc_tran_meas.restype = C.c_int
         L.orc_meas_series.argtypes = [C.POINTER(MeasPass), f64p, f64p, C.c_uint32, f64p, f64p]
         L.orc_meas_series.restype = C.c_int
+        L.orc_planes.argtypes = [C.c_void_p, C.c_uint32, f64p, f64p, f64p]
+        L.orc_planes.restype = C.c_int
         L.orc_op_ladder.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, f64p, C.c_void_p, C.c_uint32]
         L.orc_op_ladder.restype = C.c_int
         L.orc_order.argtypes = [C.c_uint32, u32p, u32p, u32p]
@@ -226,6 +228,36 @@ def op_ladder(net: Netlist, opts: NewtonOpts, threads: int = 1) -> Tuple[np.ndar
     assert r == 0
     out = np.array([[e.converged, e.singular, e.iterations] for e in res], dtype=np.int64)
     return x, out
+
+
+def ac_lanes(net: Netlist, x: np.ndarray, vsrc: int, omega, rows) -> np.ndarray:
+    """Small-signal AC response of every lane at its operating point x
+    [lanes, n] to a unit AC voltage on voltage source number `vsrc`:
+    (G + j omega C) x = e_branch, G and C from the oracle's device models,
+    solved densely (numpy). Complex [lanes, len(omega), len(rows)]."""
+    cn = CNet(net)
+    n, nnz = net.n, len(net.row_idx)
+    cp = np.asarray(net.col_ptr, dtype=np.int64)
+    ri = np.asarray(net.row_idx, dtype=np.int64)
+    cols = np.repeat(np.arange(n), np.diff(cp))
+    vb = [b for b in net.batches if b.kind == 3][0]
+    branch = int(np.asarray(vb.term).reshape(-1, 3)[vsrc, 2])
+    out = np.zeros((net.lanes, len(omega), len(rows)), dtype=complex)
+    g = np.zeros(nnz)
+    c = np.zeros(nnz)
+    for l in range(net.lanes):
+        xl = np.ascontiguousarray(x[l], dtype=np.float64)
+        assert lib().orc_planes(C.byref(cn.c), l, xl.ctypes.data_as(f64p), g.ctypes.data_as(f64p),
+                                c.ctypes.data_as(f64p)) == 0
+        G = np.zeros((n, n))
+        Cm = np.zeros((n, n))
+        np.add.at(G, (ri, cols), g)
+        np.add.at(Cm, (ri, cols), c)
+        e = np.zeros(n, dtype=complex)
+        e[branch] = 1.0
+        for f, w in enumerate(omega):
+            out[l, f] = np.linalg.solve(G + 1j * w * Cm, e)[list(rows)]
+    return out
 
 
 def tran_lanes(net: Netlist, opts: TranOpts, lane0: int = 0, count: Optional[int] = None,

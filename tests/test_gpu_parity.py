@@ -283,3 +283,29 @@ def test_operating_point_ladder(oracle, precision):
     print(f"lanes with the oracle's ladder iteration count: {same:.2f}")
     if precision == "fp64":
         assert same >= 0.5
+
+
+def test_ac_lanes(oracle):
+    """espl_ac: an RC low pass against its analytic response, and the op-amp
+    (64 Monte Carlo lanes at their warm operating points) from its input
+    source to its output over a frequency sweep, against the oracle's dense
+    complex solve at the same operating points."""
+    r, c = np.array([1e3, 2e3, 5e3]), np.array([1e-12, 1e-12, 2e-13])
+    rc = decks.rc_points(3, r, c)
+    om = np.logspace(5, 11, 13)
+    with Lanes([rc]) as L:
+        L.solve_static(abi.newton_opts())
+        h = L.ac(0, 0, om, [rc.node("out")])
+    np.testing.assert_allclose(h[:, :, 0], 1.0 / (1.0 + 1j * om[None, :] * (r * c)[:, None]), rtol=1e-12)
+    net = decks.miller_opamp(64)
+    om = np.logspace(2, 10, 17)
+    out = net.node("out")
+    with Lanes([net]) as L:
+        L.put_x(0, opamp_start(net), False)
+        res = L.solve_static(abi.newton_opts(init_fix=0))
+        x = L.get_x(0)
+        h = L.ac(0, 1, om, [out])
+    assert ((res[:, 0] & abi.CONVERGED) != 0).all()
+    ho = oracle.ac_lanes(net, x, 1, om, [out])
+    assert np.isfinite(h).all()
+    np.testing.assert_allclose(h, ho, rtol=1e-8, atol=1e-12 * np.abs(ho).max())
