@@ -320,10 +320,6 @@ struct TapeView {
     uint32_t n;
 };
 
-__device__ __forceinline__ TapeView tape_view(const GroupDev& d) {
-    return TapeView{d.q, d.col_ptr, d.prow, d.up, d.ui, d.lp, d.li, d.flags, d.pinv, d.n};
-}
-
 // The staged tape of a kStageLu tile, addressed from the shared-memory symbol.
 __device__ __forceinline__ TapeView tape_view_smem(const GroupDev& d, const SmemPlan& p) {
     const uint32_t* u = reinterpret_cast<const uint32_t*>(g_dsm);

@@ -282,8 +282,8 @@ __device__ __forceinline__ double gather_sum(const double* __restrict__ cells, u
     return s;
 }
 
-// Gather phase: A (G + ag0 C, with gmin on the diagonals), the residual
-// with the companion rows and gmin load, and the row charges.
+// One slot of A = G + ag0 C (gmin on a diagonal) from the per-slot lists
+// (the retape's assembly; Newton gathers through gather_items).
 __device__ __forceinline__ double slot_value(const GroupDev& d, uint32_t l, uint32_t p, const Companion& cp,
                                              double gmin, const double* __restrict__ cells) {
     const uint32_t P = d.P;
@@ -305,25 +305,11 @@ __device__ __forceinline__ double gather_slot(const GroupDev& d, uint32_t l, uin
     return a;
 }
 
-__device__ __forceinline__ double gather_row(const GroupDev& d, uint32_t l, uint32_t i, const Companion& cp,
-                                             double gmin, const double* __restrict__ cells) {
-    const uint32_t P = d.P;
-    double r = gather_sum(cells, P, l, d.r_ptr, d.r_cell, i);
-    if (cp.on) {
-        double q = gather_sum(cells, P, l, d.q_ptr, d.q_cell, i);
-        LM(d.qrow, i) = q;
-        double dq = cp.ag0 * (q - LM(d.q1, i));
-        double base = r + dq;
-        r = cp.method == 1 ? base - cp.ag1 * LM(d.ip, i) : base;
-    }
-    if (gmin > 0.0) r += gmin * LM(d.x, i);
-    LM(d.rhs, i) = r;
-    return r;
-}
-
 // The gather of Newton's items it0 .. it1 (slots, then rows) from the flat
-// list: gather_slot and gather_row's sums, term for term in the same order,
-// with the loads of kGiChunk entries in flight at a time instead of one sum's.
+// list: per slot A = G + ag0 C (+ gmin on a diagonal), per row the residual
+// with its companion and gmin terms and the row charge, term for term in the
+// order the host stamping adds them, with the loads of kGiChunk entries in
+// flight at a time instead of one sum's.
 // Slot values also go to `sa` (the shared LU chain's A) when it is given.
 template <typename T>
 __device__ __forceinline__ void gather_items(const GroupDev& d, uint32_t l, uint32_t lane, uint32_t it0, uint32_t it1,
