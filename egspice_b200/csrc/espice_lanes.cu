@@ -538,8 +538,8 @@ espl_status alloc_group(espl_lanes* h, Group& g) {
         }
         if ((s = dupload(h, own, &d.site_cell, pl.sites))) return s;
         if ((s = dupload(h, own, &d.slot_diag, pl.slot_diag))) return s;
-        // two cells buffers: an iteration's instance phase and the next one's
-        if ((s = dalloc(h, own, &d.cells, 2 * (size_t)pl.n_cells * P))) return s;
+        if ((s = dalloc(h, own, &d.cells, (size_t)pl.n_cells * P))) return s;
+        if ((s = dalloc(h, own, &d.site_prev, (size_t)d.n_sites * P))) return s;
     }
 #define UP(field, vec) if ((s = dupload(h, own, &d.field, vec))) return s
     UP(col_ptr, g.col_ptr);

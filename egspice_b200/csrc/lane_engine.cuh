@@ -86,6 +86,7 @@ struct GroupDev {
     const uint32_t *g_ptr, *g_cell, *c_ptr, *c_cell, *r_ptr, *r_cell, *q_ptr, *q_cell, *site_cell;
     const uint8_t* slot_diag;
     double* cells;
+    double* site_prev;  // an iteration's site charges, kept before its limiter pass overwrites the cells
     uint32_t n_gc, n_cc, n_rc, n_qc;  // lengths of g_cell, c_cell, r_cell, q_cell
     // The same sums as one flat list for the Newton gather (lane_tile.cuh
     // gather_items): items are the nnz slots, then the n rows; an item's

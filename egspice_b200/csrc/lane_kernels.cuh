@@ -44,7 +44,6 @@ struct TileShared {
     uint32_t bits[32];
     uint32_t restore[32];
     uint32_t accf[32];
-    uint32_t cbuf[32];  // the cells buffer of a converged lane's published iterate
     unsigned long long acc0[32], acc1[32], acc2[32];
     double limit[32];
     double ag0[32], ag1[32], ag2[32], t[32], xfact[32], dt_next[32];
@@ -60,8 +59,8 @@ constexpr uint32_t kLimited = 1, kImplausible = 2, kResidualMiss = 4;
 // limit, gates, finalize). `on` lanes take part; with `tran_companion` a
 // lane's companion scalars and time come from the shared arrays. The
 // instance phase of iteration k + 1 runs inside iteration k's limiter pass
-// (same loads, into the other cells buffer); `eval0` runs iteration 0's
-// instance phase first (else the caller left it in cells buffer 0).
+// (same loads; the gather has read the cells by then); `eval0` runs
+// iteration 0's instance phase first (else the caller left it in the cells).
 template <bool MIXED>
 __device__ __forceinline__ void newton_tile(const TileCtx& c, LaneState* s, const NewtonParams& o, int tran,
                                             bool tran_companion, bool on, TileShared& sh, unsigned char* dsm,
@@ -100,7 +99,6 @@ __device__ __forceinline__ void newton_tile(const TileCtx& c, LaneState* s, cons
     if (eval0 && c.valid && on)
         for (uint32_t t = warp; t < ninst; t += nw) inst_eval(d, l, t, tran, 0.0, cell_buf(d, 0), src);
     __syncthreads();
-    uint32_t cur = 0;
     for (uint32_t it = 0; it < o.max_iter; it++) {
         bool act = c.valid && sh.active[lane];
         if (!__syncthreads_or(act)) break;
@@ -114,7 +112,7 @@ __device__ __forceinline__ void newton_tile(const TileCtx& c, LaneState* s, cons
             cp.ag2 = sh.ag2[lane];
             tm = sh.t[lane];
         }
-        const double* cells = cell_buf(d, cur);
+        const double* cells = d.cells;
         if (act) {
             uint32_t it0, it1;
             if (nw == 4) {
@@ -279,6 +277,10 @@ __device__ __forceinline__ void newton_tile(const TileCtx& c, LaneState* s, cons
                 unsigned long long b = dbits(score);
                 worst = worst > b ? worst : b;
             }
+        // the iteration's site charges, before the limiter pass overwrites
+        // the cells (a lane that converges here publishes them)
+        if (act)
+            for (uint32_t j = warp; j < d.n_sites; j += nw) LM(d.site_prev, j) = LM(d.cells, d.site_cell[j]);
         if (act) atomicMax(&sh.acc0[lane], worst);
         __syncthreads();
         // The limiter pass over instances (each then evaluated at its new
@@ -286,7 +288,7 @@ __device__ __forceinline__ void newton_tile(const TileCtx& c, LaneState* s, cons
         // over rows.
         uint32_t flags = 0;
         if (act) {
-            double* next = cell_buf(d, cur ^ 1u);
+            double* next = d.cells;
             for (uint32_t t = warp; t < ninst; t += nw)
                 if (inst_limit_eval(d, l, t, tran, tm, next, src)) flags |= kLimited;
             double lim = sh.limit[lane];
@@ -314,7 +316,6 @@ __device__ __forceinline__ void newton_tile(const TileCtx& c, LaneState* s, cons
                     sh.bits[lane] |= kConverged;
                     sh.active[lane] = 0;
                     sh.restore[lane] = 1;
-                    sh.cbuf[lane] = cur;
                     s->iterations = it + 1;
                 }
                 if (MIXED && sh.active[lane] && !s->fp64 && it + 1 >= o.stall_ticks) {
@@ -326,7 +327,6 @@ __device__ __forceinline__ void newton_tile(const TileCtx& c, LaneState* s, cons
         __syncthreads();
         if (c.valid && sh.restore[lane])
             for (uint32_t i = warp; i < d.n; i += nw) LM(d.x, i) = LM(d.x_old, i);
-        cur ^= 1u;
     }
     __syncthreads();
     if (warp == 0 && s && on) s->bits = sh.bits[lane];
@@ -396,10 +396,8 @@ __global__ void __launch_bounds__(kTileThreads) k_prep(TileMap m, const double* 
         for (int k = 0; k < DiodePrep::count; k++) LM(dd, DiodePrep::count * i + k) = o[k];
     }
     if (c.warp == 0) {
-        for (uint32_t b = 0; b < 2; b++) {
-            LM(cell_buf(d, b), d.c_const) = 1.0;
-            LM(cell_buf(d, b), d.c_const + 1) = -1.0;
-        }
+        LM(d.cells, d.c_const) = 1.0;
+        LM(d.cells, d.c_const + 1) = -1.0;
     }
 }
 
@@ -653,7 +651,7 @@ __global__ void __launch_bounds__(WIDE ? kWideThreads : kTileThreads, WIDE ? 1 :
         __syncthreads();
         // The limiter state restarts from the accepted point, then limits the
         // predicted iterate and evaluates the instances there (the instance
-        // phase of Newton's iteration 0, into cells buffer 0).
+        // phase of Newton's iteration 0, into the cells).
         if (on)
             for (uint32_t t = warp; t < ninst; t += nw) {
                 inst_seed(d, l, t, 0, d.cur);
@@ -671,8 +669,7 @@ __global__ void __launch_bounds__(WIDE ? kWideThreads : kTileThreads, WIDE ? 1 :
         }
         if (conv) {
             double* r0 = ring_slot(d, sh.rot[lane], 0);
-            const double* cb = cell_buf(d, sh.cbuf[lane]);
-            for (uint32_t j = warp; j < ns; j += nw) LM(r0, j) = LM(cb, d.site_cell[j]);
+            for (uint32_t j = warp; j < ns; j += nw) LM(r0, j) = LM(d.site_prev, j);
         }
         __syncthreads();
         // The LTE bound of a converged LTE-controlled step, its sites split

@@ -383,11 +383,11 @@ __device__ __forceinline__ void gather_charge_row(const GroupDev& d, uint32_t l,
     LM(d.qrow, i) = gather_sum(cells, P, l, d.q_ptr, d.q_cell, i);
 }
 
-// Cells buffer b (0 or 1) of a template: the instance phase of one Newton
-// iteration writes one while the gather of the same iteration reads it, and
-// the limiter pass evaluates the next iteration into the other.
-__device__ __forceinline__ double* cell_buf(const GroupDev& d, uint32_t b) {
-    return d.cells + (b ? (size_t)d.n_cells * d.P : 0);
-}
+// The cells of a template: an iteration's instance phase writes them, its
+// gather reads them, and its limiter pass (after the gather) overwrites them
+// with the next iteration's instance phase. One buffer: the only values of
+// an iteration still needed after that pass, its site charges, are kept in
+// site_prev by the update phase before it.
+__device__ __forceinline__ double* cell_buf(const GroupDev& d, uint32_t) { return d.cells; }
 
 }  // namespace espl
