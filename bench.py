@@ -290,10 +290,17 @@ def run_learned_dc(points: int = 65536, train_points: int = 8192, epochs: int = 
             return r, L.get_x(0), L.stats().newton_ms
 
     r_plain, x_plain, dev_plain = solve(net, x0, "fp64")
+    # context: the same points from the cold start through the continuation
+    # ladder (what an operating point costs without a start point), wall time
+    import torch
+    with Lanes([net], precision="fp64") as L:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r_cold = L.solve_op(abi.newton_opts())
+        t_cold = time.perf_counter() - t0
     head = net.subset(list(range(train_points)))
     tail = net.subset(list(range(train_points, points)))
     r_head, x_head, dev_head = solve(head, x0[:train_points], "mixed")
-    import torch
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     with Mlp(net.sweep.shape[1], net.n, capacity=8192, seed=7) as m:
@@ -332,7 +339,11 @@ def run_learned_dc(points: int = 65536, train_points: int = 8192, epochs: int = 
                           "mean_newton_iters_predicted": float(r_tail[:, 1].mean()),
                           "mean_newton_iters_all": float(r_learned[:, 1].mean()), "converged": conv(r_learned),
                           "fallbacks_to_nominal": refallback},
+        "plain_cold_ladder_fp64": {"points_per_s": points / t_cold, "ms": t_cold * 1e3,
+                                   "mean_newton_iters": float(r_cold[:, 1].mean()),
+                                   "converged": conv(r_cold)},
         "learned_over_plain": t_plain / t_learned,
+        "learned_over_cold_ladder": t_cold / t_learned,
         "max_err_over_newton_tol": err_newton,
         "max_err_over_1e-6_bar": err_bar,
         "note": "learned and plain runs stop at the same Newton test, so they agree to the Newton tolerance "
