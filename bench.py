@@ -269,7 +269,7 @@ def opamp_nominal(net):
     return x0
 
 
-def run_learned_dc(points: int = 65536, train_points: int = 8192, epochs: int = 120, seed: int = 0):
+def run_learned_dc(points: int = 65536, train_points: int = 8192, epochs: int = 20, seed: int = 0):
     """Config 4: a Monte-Carlo op-amp operating-point sweep (16 varied
     parameters). Plain: every point's Newton (FP64 LU) starts from the
     nominal operating point. Learned + mixed: the first `train_points` points
