@@ -269,13 +269,17 @@ def opamp_nominal(net):
     return x0
 
 
-def run_learned_dc(points: int = 65536, train_points: int = 8192, epochs: int = 20, seed: int = 0):
+def run_learned_dc(points: int = 65536, train_points: int = 8192, epochs: int = 80, seed: int = 0, batch: int = 4096,
+                   lr: float = 1e-2):
     """Config 4: a Monte-Carlo op-amp operating-point sweep (16 varied
     parameters). Plain: every point's Newton (FP64 LU) starts from the
     nominal operating point. Learned + mixed: the first `train_points` points
     are solved that way (FP32 LU), the MLP is trained on them on the GPU, and
     the remaining points start from its predictions. Time = Newton device time
-    plus the MLP's training and inference (wall, synchronized)."""
+    plus the MLP's training and inference (wall, synchronized). Garbage from
+    earlier runs is collected before each wall-timed region, so no lane
+    handle is freed inside one."""
+    import gc
     from egspice_b200 import abi, decks
     from egspice_b200.lanes import Lanes
     from egspice_b200.learned import Mlp, train_opts
@@ -294,6 +298,7 @@ def run_learned_dc(points: int = 65536, train_points: int = 8192, epochs: int = 
     # ladder (what an operating point costs without a start point), wall time
     import torch
     with Lanes([net], precision="fp64") as L:
+        gc.collect()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         r_cold = L.solve_op(abi.newton_opts())
@@ -301,10 +306,11 @@ def run_learned_dc(points: int = 65536, train_points: int = 8192, epochs: int = 
     head = net.subset(list(range(train_points)))
     tail = net.subset(list(range(train_points, points)))
     r_head, x_head, dev_head = solve(head, x0[:train_points], "mixed")
+    gc.collect()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     with Mlp(net.sweep.shape[1], net.n, capacity=8192, seed=7) as m:
-        losses = m.train(net.sweep[:train_points], x_head, train_opts(epochs=epochs, batch=512, lr=3e-3,
+        losses = m.train(net.sweep[:train_points], x_head, train_opts(epochs=epochs, batch=batch, lr=lr,
                                                                       lr_final=1e-4))
         t_train = time.perf_counter() - t0
         guess = m.predict(net.sweep[train_points:])
@@ -335,7 +341,7 @@ def run_learned_dc(points: int = 65536, train_points: int = 8192, epochs: int = 
         "learned_mixed": {"points_per_s": points / t_learned, "ms": t_learned * 1e3,
                           "newton_ms": dev_head + dev_tail, "mlp_train_ms": t_train * 1e3,
                           "mlp_predict_ms": (t_mlp - t_train) * 1e3, "train_points": train_points,
-                          "epochs": epochs, "final_loss": float(losses[-1]),
+                          "epochs": epochs, "batch": batch, "lr": lr, "final_loss": float(losses[-1]),
                           "mean_newton_iters_predicted": float(r_tail[:, 1].mean()),
                           "mean_newton_iters_all": float(r_learned[:, 1].mean()), "converged": conv(r_learned),
                           "fallbacks_to_nominal": refallback},

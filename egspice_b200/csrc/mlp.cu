@@ -505,8 +505,10 @@ espl_status espl_mlp_train(espl_mlp* h, const double* x, const double* y, uint32
         return ESPL_INVALID_ARGUMENT;
     espl_status s = ESPL_OK;
     if (!h->scaled && (s = set_scaling(h, x, y, n))) return s;
-    // The data set stays on the device, standardized; each epoch uploads a
-    // permutation and every Adam step gathers its rows on the device.
+    const uint32_t chunk_ep = std::max(1u, std::min(o->epochs, (uint32_t)((64u << 20) / (sizeof(uint32_t) * n))));
+    // The data set stays on the device, standardized; the epochs'
+    // permutations go up in chunks of up to 64 MB and every Adam step
+    // gathers its rows on the device.
     double *xr = nullptr, *yr = nullptr, *lsum = nullptr;
     __nv_bfloat16* xs = nullptr;
     float* ts = nullptr;
@@ -523,7 +525,7 @@ espl_status espl_mlp_train(espl_mlp* h, const double* x, const double* y, uint32
     };
     if (dalloc((void**)&xr, sizeof(double) * n * h->D) || dalloc((void**)&yr, sizeof(double) * n * h->O) ||
         dalloc((void**)&xs, sizeof(__nv_bfloat16) * n * h->Dp) || dalloc((void**)&ts, sizeof(float) * n * h->Op) ||
-        dalloc((void**)&perm, sizeof(uint32_t) * n) || dalloc((void**)&lsum, sizeof(double) * o->epochs)) {
+        dalloc((void**)&perm, sizeof(uint32_t) * n * chunk_ep) || dalloc((void**)&lsum, sizeof(double) * o->epochs)) {
         cleanup();
         h->msg = "out of device memory for the training set";
         return ESPL_OUT_OF_MEMORY;
@@ -541,22 +543,31 @@ espl_status espl_mlp_train(espl_mlp* h, const double* x, const double* y, uint32
     const float b1 = o->beta1, b2 = o->beta2;
     const uint32_t per_epoch = n / o->batch;
     const int rows = (int)o->batch;
+    std::vector<uint32_t> perms((size_t)n * chunk_ep);
     for (uint32_t ep = 0; ep < o->epochs && !s; ep++) {
-        std::shuffle(order.begin(), order.end(), rng);
-        // the permutation buffer is rewritten each epoch: order the copy
-        // after the previous epoch's gathers
-        if (cudaStreamSynchronize(h->stream) != cudaSuccess ||
-            cudaMemcpyAsync(perm, order.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, h->stream) !=
-                cudaSuccess) {
-            s = ESPL_DRIVER;
-            break;
+        const uint32_t slot = ep % chunk_ep;
+        if (slot == 0) {
+            const uint32_t count = std::min(chunk_ep, o->epochs - ep);
+            for (uint32_t e = 0; e < count; e++) {
+                std::shuffle(order.begin(), order.end(), rng);
+                std::copy(order.begin(), order.end(), perms.begin() + (size_t)e * n);
+            }
+            // the permutation buffer is rewritten per chunk: order the copy
+            // after the previous chunk's gathers
+            if (cudaStreamSynchronize(h->stream) != cudaSuccess ||
+                cudaMemcpyAsync(perm, perms.data(), sizeof(uint32_t) * n * count, cudaMemcpyHostToDevice,
+                                h->stream) != cudaSuccess) {
+                s = ESPL_DRIVER;
+                break;
+            }
         }
+        const uint32_t* ep_perm = perm + (size_t)slot * n;
         float lr = o->lr;
         if (o->lr_final > 0.0f && o->epochs > 1)
             lr = o->lr * std::pow(o->lr_final / o->lr, (float)ep / (float)(o->epochs - 1));
         for (uint32_t b = 0; b < per_epoch && !s; b++) {
             long long nb = (long long)rows * std::max(h->Dp, h->Op);
-            k_gather_rows<<<blocks(nb), 256, 0, h->stream>>>(xs, ts, perm + (size_t)b * rows, rows, h->Dp, h->Op,
+            k_gather_rows<<<blocks(nb), 256, 0, h->stream>>>(xs, ts, ep_perm + (size_t)b * rows, rows, h->Dp, h->Op,
                                                              h->xb, h->t);
             if ((s = forward(h, rows))) break;
             if ((s = backward(h, rows, lsum + ep))) break;

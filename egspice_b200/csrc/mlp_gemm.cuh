@@ -119,9 +119,85 @@ __device__ __forceinline__ void tc_ld16(uint32_t taddr, float (&v)[16]) {
     for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
 
-// Stages rows [r0, r0 + rows) x K [k0, k0 + kBK) of a strided operand into
-// a K-major tile; out-of-range elements are zero. Consecutive threads walk
-// the contiguous dimension of the source.
+// How an operand is staged: kStageK when K is contiguous (s_k == 1) and rows
+// start on 16 bytes, kStageRows when rows are contiguous (s_row == 1) and K
+// steps are 16 bytes, kStageAny otherwise. The first two move 8 elements per
+// 16-byte load.
+enum StageMode : int { kStageK = 0, kStageRows = 1, kStageAny = 2 };
+
+__device__ __forceinline__ int stage_mode(const __nv_bfloat16* src, long long s_row, long long s_k) {
+    if (reinterpret_cast<uintptr_t>(src) & 15u) return kStageAny;
+    if (s_k == 1 && (s_row & 7) == 0) return kStageK;
+    if (s_row == 1 && (s_k & 7) == 0) return kStageRows;
+    return kStageAny;
+}
+
+// 8 contiguous elements from p; those at positions >= valid read as zero and
+// are not touched.
+__device__ __forceinline__ uint4 load8(const __nv_bfloat16* p, int valid) {
+    if (valid >= 8) return __ldg(reinterpret_cast<const uint4*>(p));
+    const unsigned short* q = reinterpret_cast<const unsigned short*>(p);
+    uint32_t w[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const uint32_t lo = 2 * j < valid ? q[2 * j] : 0u;
+        const uint32_t hi = 2 * j + 1 < valid ? q[2 * j + 1] : 0u;
+        w[j] = lo | hi << 16;
+    }
+    return make_uint4(w[0], w[1], w[2], w[3]);
+}
+
+// A ROWS x kBK operand tile in flight: ROWS * kBK / 8 chunks of 16 bytes,
+// ROWS / 16 per thread, chunk e = threadIdx.x + i * kGemmThreads.
+//   kStageK:    chunk e holds row (e >> 6) * 8 + (e & 7), K block (e >> 3) & 7,
+//               which is exactly tile bytes [16 e, 16 e + 16).
+//   kStageRows: chunk e holds rows (e >> 6) * 8 .. + 7 at K index e & 63.
+template <int ROWS>
+struct StageBuf {
+    uint4 v[ROWS / 16];
+};
+
+// Issues every global load of one tile (rows [r0, r0 + ROWS), K [k0, k0 +
+// kBK), out-of-range elements zero) before any of them is consumed.
+template <int ROWS>
+__device__ __forceinline__ void stage_load(StageBuf<ROWS>& b, int mode, const __nv_bfloat16* src, long long s_row,
+                                           long long s_k, int r0, int rows_total, int k0, int k_total) {
+#pragma unroll
+    for (int i = 0; i < ROWS / 16; i++) {
+        const int e = threadIdx.x + i * kGemmThreads;
+        if (mode == kStageK) {
+            const int gr = r0 + (e >> 6) * 8 + (e & 7), gk = k0 + ((e >> 3) & 7) * 8;
+            const int valid = gr < rows_total ? max(0, min(8, k_total - gk)) : 0;
+            b.v[i] = load8(src + (long long)gr * s_row + gk, valid);
+        } else if (mode == kStageRows) {
+            const int gr = r0 + (e >> 6) * 8, gk = k0 + (e & 63);
+            const int valid = gk < k_total ? max(0, min(8, rows_total - gr)) : 0;
+            b.v[i] = load8(src + gr + (long long)gk * s_k, valid);
+        }
+    }
+}
+
+template <int ROWS>
+__device__ __forceinline__ void stage_store(unsigned char* tile, const StageBuf<ROWS>& b, int mode) {
+#pragma unroll
+    for (int i = 0; i < ROWS / 16; i++) {
+        const int e = threadIdx.x + i * kGemmThreads;
+        if (mode == kStageK) {
+            *reinterpret_cast<uint4*>(tile + (uint32_t)e * 16u) = b.v[i];
+        } else if (mode == kStageRows) {
+            const uint32_t w[4] = {b.v[i].x, b.v[i].y, b.v[i].z, b.v[i].w};
+            const int rb = e >> 6, k = e & 63;
+#pragma unroll
+            for (int j = 0; j < 8; j++)
+                *reinterpret_cast<unsigned short*>(tile + tile_off((uint32_t)(rb * 8 + j), (uint32_t)k)) =
+                    (unsigned short)(w[j >> 1] >> ((j & 1) * 16));
+        }
+    }
+}
+
+// Stages rows [r0, r0 + rows) x K [k0, k0 + kBK) of an operand with any
+// strides into a K-major tile, one element at a time; out-of-range elements
+// are zero. Consecutive threads walk the contiguous dimension of the source.
 __device__ __forceinline__ void stage_operand(unsigned char* tile, const __nv_bfloat16* src, long long s_row,
                                               long long s_k, int r0, int rows_total, int rows, int k0, int k_total) {
     const int tid = threadIdx.x;
@@ -145,10 +221,52 @@ __device__ __forceinline__ void stage_operand(unsigned char* tile, const __nv_bf
     }
 }
 
+constexpr int kEpPitch = 20;  // floats between the epilogue's staged rows
+
+// Epilogue of C(m, n .. n + 3), the columns at or past N left alone; `vec`
+// when C (and Cb) rows allow 16-byte (8-byte) stores.
+template <int EPI>
+__device__ __forceinline__ void epilogue4(const GemmArgs& g, int m, int n, float4 x, bool vec) {
+    float v[4] = {x.x, x.y, x.z, x.w};
+    const long long o = (long long)m * g.ldc + n;
+    if constexpr (EPI == kEpiAtomic) {
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+            if (n + j < g.N) atomicAdd(g.c + o + j, v[j]);
+        return;
+    }
+    if constexpr (EPI == kEpiBias || EPI == kEpiBiasTanh) {
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const float b = n + j < g.N ? g.bias[n + j] : 0.0f;
+            v[j] = EPI == kEpiBiasTanh ? tanhf(v[j] + b) : v[j] + b;
+        }
+    }
+    if (vec && n + 4 <= g.N) {
+        *reinterpret_cast<float4*>(g.c + o) = make_float4(v[0], v[1], v[2], v[3]);
+        if (EPI == kEpiBiasTanh) {
+            __nv_bfloat162 lo = __floats2bfloat162_rn(v[0], v[1]), hi = __floats2bfloat162_rn(v[2], v[3]);
+            uint2 u;
+            u.x = *reinterpret_cast<uint32_t*>(&lo);
+            u.y = *reinterpret_cast<uint32_t*>(&hi);
+            *reinterpret_cast<uint2*>(g.cb + o) = u;
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+            if (n + j < g.N) {
+                g.c[o + j] = v[j];
+                if (EPI == kEpiBiasTanh) g.cb[o + j] = __float2bfloat16(v[j]);
+            }
+    }
+}
+
 // BN: columns of C per CTA (16..128, a multiple of 16).
 template <int BN, int EPI>
 __global__ void __launch_bounds__(kGemmThreads) k_gemm_tc(GemmArgs g) {
     constexpr uint32_t kTmemCols = BN <= 32 ? 32 : BN <= 64 ? 64 : 128;
+    static_assert(kBK == 64 && BN % 16 == 0, "the staging chunk maps assume 64-element K tiles");
+    static_assert(kGemmThreads * kEpPitch * 4 <= kBM * kBK * 2, "the epilogue rows fit in the A tile");
     __shared__ __align__(1024) unsigned char sa[kBM * kBK * 2];
     __shared__ __align__(1024) unsigned char sb[BN * kBK * 2];
     __shared__ __align__(8) uint64_t bar;
@@ -174,11 +292,20 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm_tc(GemmArgs g) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = tmem_base;
     const uint32_t idesc = instr_desc(BN);
+    const int ma = stage_mode(g.a, g.sam, g.sak), mb = stage_mode(g.b, g.sbn, g.sbk);
+    StageBuf<kBM> ba;
+    StageBuf<BN> bb;
     uint32_t phase = 0;
     bool issued = false;
+    if (kb < ke) {
+        stage_load<kBM>(ba, ma, g.a, g.sam, g.sak, m0, g.M, kb, ke);
+        stage_load<BN>(bb, mb, g.b, g.sbn, g.sbk, n0, g.N, kb, ke);
+    }
     for (int k0 = kb; k0 < ke; k0 += kBK) {
-        stage_operand(sa, g.a, g.sam, g.sak, m0, g.M, kBM, k0, ke);
-        stage_operand(sb, g.b, g.sbn, g.sbk, n0, g.N, BN, k0, ke);
+        if (ma == kStageAny) stage_operand(sa, g.a, g.sam, g.sak, m0, g.M, kBM, k0, ke);
+        else stage_store<kBM>(sa, ba, ma);
+        if (mb == kStageAny) stage_operand(sb, g.b, g.sbn, g.sbk, n0, g.N, BN, k0, ke);
+        else stage_store<BN>(sb, bb, mb);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -192,6 +319,11 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm_tc(GemmArgs g) {
             tc_commit(&bar);
         }
         issued = true;
+        // the next chunk's loads overlap the MMAs
+        if (k0 + kBK < ke) {
+            stage_load<kBM>(ba, ma, g.a, g.sam, g.sak, m0, g.M, k0 + kBK, ke);
+            stage_load<BN>(bb, mb, g.b, g.sbn, g.sbk, n0, g.N, k0 + kBK, ke);
+        }
         // the tile buffers are reused: wait until the MMAs have read them
         bool ok = mbar_wait_bounded(&bar, phase);
         if (!ok) failed = 1;
@@ -208,31 +340,30 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm_tc(GemmArgs g) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (failed) {
     } else if (issued) {
-        const int m = m0 + warp * 32 + lane;
-#pragma unroll
+        // Each warp reads its 32 accumulator rows 16 columns at a time and
+        // passes them through shared memory (the A tile, free once the last
+        // MMA completed; rows kEpPitch floats apart, so the 16-byte writes
+        // of 8 consecutive rows fall in distinct banks), then writes them out
+        // as 4-column runs, 4 lanes per row.
+        float* ep = reinterpret_cast<float*>(sa) + warp * 32 * kEpPitch;
+        const bool vec = (g.ldc & 3) == 0 && (reinterpret_cast<uintptr_t>(g.c) & 15u) == 0 &&
+                         (EPI != kEpiBiasTanh || (reinterpret_cast<uintptr_t>(g.cb) & 7u) == 0);
+#pragma unroll 1
         for (int c0 = 0; c0 < BN; c0 += 16) {
             float v[16];
             tc_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
-            if (m < g.M) {
+            float4* own = reinterpret_cast<float4*>(ep + lane * kEpPitch);
 #pragma unroll
-                for (int i = 0; i < 16; i++) {
-                    const int n = n0 + c0 + i;
-                    if (n >= g.N) continue;
-                    float x = v[i];
-                    float* cp = g.c + (long long)m * g.ldc + n;
-                    if (EPI == kEpiAtomic) {
-                        atomicAdd(cp, x);
-                    } else if (EPI == kEpiBiasTanh) {
-                        x = tanhf(x + g.bias[n]);
-                        *cp = x;
-                        g.cb[(long long)m * g.ldc + n] = __float2bfloat16(x);
-                    } else if (EPI == kEpiBias) {
-                        *cp = x + g.bias[n];
-                    } else {
-                        *cp = x;
-                    }
-                }
+            for (int q = 0; q < 4; q++) own[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+            __syncwarp();
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const int idx = lane + 32 * i, r = idx >> 2, q = idx & 3;
+                const int m = m0 + warp * 32 + r, n = n0 + c0 + q * 4;
+                const float4 x = *reinterpret_cast<const float4*>(ep + r * kEpPitch + q * 4);
+                if (m < g.M && n < g.N) epilogue4<EPI>(g, m, n, x, vec);
             }
+            __syncwarp();
         }
     } else if (EPI != kEpiAtomic) {
         // an empty K range: C = epilogue(0)
