@@ -62,16 +62,19 @@ class Stats(C.Structure):
 class MeasPass(C.Structure):
     _fields_ = [("kind", C.c_uint32), ("row", C.c_uint32), ("val", C.c_double), ("td", C.c_double),
                 ("from_", C.c_double), ("to", C.c_double), ("at", C.c_double), ("rise", C.c_int32),
-                ("fall", C.c_int32), ("cross", C.c_int32), ("reserved", C.c_uint32)]
+                ("fall", C.c_int32), ("cross", C.c_int32), ("level_row", C.c_uint32)]
 
 
 MEAS_WHEN, MEAS_FIND_AT, MEAS_MIN, MEAS_MAX, MEAS_AVG, MEAS_INTEG, MEAS_RMS = 1, 2, 3, 4, 5, 6, 7
+MEAS_DERIV_AT, MEAS_FIND_WHEN, MEAS_DERIV_WHEN, MEAS_TARG = 8, 9, 10, 11
 MEAS_UNSET, MEAS_LAST = -1, -2
 
 
 def meas_pass(kind, row, val=0.0, td=0.0, from_=0.0, to=0.0, at=0.0, rise=MEAS_UNSET, fall=MEAS_UNSET,
-              cross=MEAS_UNSET) -> MeasPass:
-    return MeasPass(kind, row, val, td, from_, to, at, rise, fall, cross, 0)
+              cross=MEAS_UNSET, level_row=None) -> MeasPass:
+    """One espl_meas pass; `level_row` names the unknown a WHEN or TARG
+    crossing is measured against (None: the constant `val`)."""
+    return MeasPass(kind, row, val, td, from_, to, at, rise, fall, cross, 0 if level_row is None else level_row + 1)
 
 
 class ClassInfo(C.Structure):

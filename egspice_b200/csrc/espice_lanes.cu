@@ -1721,9 +1721,15 @@ espl_status espl_set_meas(espl_lanes* h, uint32_t net, const espl_meas* passes, 
     if (n > ESPL_MEAS_MAX_PASSES) return fail(h, ESPL_TOO_LARGE, "more .meas passes than ESPL_MEAS_MAX_PASSES");
     Group& g = h->groups[net];
     for (uint32_t p = 0; p < n; p++) {
-        if (passes[p].kind < ESPL_MEAS_WHEN || passes[p].kind > ESPL_MEAS_RMS)
+        const espl_meas& c = passes[p];
+        if (c.kind < ESPL_MEAS_WHEN || c.kind > ESPL_MEAS_TARG)
             return fail(h, ESPL_INVALID_ARGUMENT, "unknown .meas kind");
-        if (passes[p].row >= g.n) return fail(h, ESPL_INVALID_ARGUMENT, ".meas row out of range");
+        if (c.row >= g.n) return fail(h, ESPL_INVALID_ARGUMENT, ".meas row out of range");
+        if (c.level_row > g.n) return fail(h, ESPL_INVALID_ARGUMENT, ".meas level row out of range");
+        if (c.level_row && c.kind != ESPL_MEAS_WHEN && c.kind != ESPL_MEAS_TARG)
+            return fail(h, ESPL_INVALID_ARGUMENT, "a .meas level vector belongs to WHEN or TARG");
+        if (meas_reads_previous(c.kind) && (p == 0 || passes[p - 1].kind != ESPL_MEAS_WHEN))
+            return fail(h, ESPL_INVALID_ARGUMENT, "FIND/DERIV WHEN and TARG follow their WHEN (TRIG) pass");
     }
     for (void* p : g.meas_owned) cudaFree(p);
     g.meas_owned.clear();

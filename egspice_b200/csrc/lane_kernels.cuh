@@ -520,6 +520,18 @@ __device__ void step_bound_part(const GroupDev& d, uint32_t l, uint32_t rot, uin
     }
 }
 
+// Feeds lane l's sample at time t to every .meas pass of its template, in
+// order (a pass that reads the one before it sees it after this sample).
+__device__ __forceinline__ void meas_feed_all(const GroupDev& d, uint32_t l, double t) {
+    const uint32_t P = d.P;
+    for (uint32_t p = 0; p < d.n_mpass; p++) {
+        const espl_meas& c = d.mpass[p];
+        double* ms = d.mstate + (size_t)p * kMeasWords * P + l;
+        const double* prev = p > 0 ? ms - (size_t)kMeasWords * P : nullptr;
+        meas_feed(c, ms, P, prev, t, LM(d.x, c.row), c.level_row ? LM(d.x, c.level_row - 1) : 0.0);
+    }
+}
+
 // Transient start from the operating point in x: histories, the site ring,
 // the first step (tran.zig:688-699 under LTE control), breakpoints.
 __global__ void __launch_bounds__(kTileThreads) k_tran_init(TileMap m, TranParams o, LaneState* st) {
@@ -582,8 +594,8 @@ __global__ void __launch_bounds__(kTileThreads) k_tran_init(TileMap m, TranParam
     for (uint32_t p = 0; p < d.n_mpass; p++) {
         double* ms = d.mstate + (size_t)p * kMeasWords * P + l;
         meas_init(d.mpass[p], ms, P);
-        meas_feed(d.mpass[p], ms, P, 0.0, LM(d.x, d.mpass[p].row));
     }
+    meas_feed_all(d, l, 0.0);
 }
 
 // Up to o.launch_steps attempts per lane, each: stepBegin, the linear
@@ -797,8 +809,7 @@ __global__ void __launch_bounds__(WIDE ? kWideThreads : kTileThreads, WIDE ? 1 :
                 s->m_prev_t = t_new;
                 s->m_have = 1;
             }
-            for (uint32_t p = 0; p < d.n_mpass; p++)
-                meas_feed(d.mpass[p], d.mstate + (size_t)p * kMeasWords * P + l, P, t_new, LM(d.x, d.mpass[p].row));
+            meas_feed_all(d, l, t_new);
             // stepEndB (kernels/lane.zig:667-700).
             s->t = t_new;
             if (!o.fixed_step) {

@@ -1,11 +1,15 @@
 // Streaming .meas passes over a lane's transient, one sample (t, v) at a
-// time: the event count of WHEN, the value at a point (FIND ... AT), the
-// extremum and average (MIN, MAX, AVG) and the integral (INTEG, RMS), with
-// ngspice's com_measure2.c semantics as the reference streams them on its
-// lanes (src/output/scan.zig Cross, At, Extremum, Integ; run per lane in
+// time: the event count of WHEN (against a constant or a second vector),
+// the value or slope at a point (FIND/DERIV ... AT), the value or slope at
+// the previous pass's WHEN event (FIND/DERIV ... WHEN), a TARG event counted
+// from the previous pass's TRIG event, the extremum and average (MIN, MAX,
+// AVG) and the integral (INTEG, RMS), with ngspice's com_measure2.c
+// semantics as the reference streams them on its lanes (src/output/scan.zig
+// Cross :60-169, At :171-192, Extremum, Integ, Find :340-390; run per lane in
 // src/solver/lane_device.zig). A pass's state is kMeasWords doubles, word k
 // of pass p of lane l at ((p * kMeasWords + k) * P + l); feeding stops once
-// a pass reports the end of its window.
+// a pass reports the end of its window. Passes are fed in order, so a pass
+// that reads the one before it sees that pass after the same sample.
 #pragma once
 
 #include <cmath>
@@ -16,7 +20,7 @@
 
 namespace espl {
 
-constexpr uint32_t kMeasWords = 24;
+constexpr uint32_t kMeasWords = 32;
 constexpr uint32_t kMeasDone = 0;  // the pass read its last sample
 
 #define MW(k) st[(size_t)(k) * stride]
@@ -41,13 +45,26 @@ __host__ __device__ inline double meas_line(double x0, double y0, double x1, dou
     return slope * x + icept;
 }
 
-// WHEN state words.
+// WHEN state words (also the TARG pass's event count).
 enum : uint32_t {
     kWFirst = 1, kWAbove, kWPending, kWRise, kWFall, kWCross, kWWantRise, kWWantFall, kWWantCross, kWPrev,
-    kWPrevX, kWFound, kWLast, kWHit
+    kWPrevX, kWFound, kWLast, kWHit, kWPrev2
 };
-// FIND ... AT.
+// FIND/DERIV ... AT, and the value pass of FIND/DERIV ... WHEN.
 enum : uint32_t { kARows = 1, kAPx, kAPv, kAValue };
+// FIND/DERIV ... WHEN: the event time once armed, the stage (kMeas*), rows
+// read, and the last rows (scale, value, level) oldest first.
+enum : uint32_t { kFAt = 5, kFStage, kFRows, kFRingLen, kFRing };
+// TARG: the TRIG event time, the stage, rows read and the ring after the
+// event count's words.
+enum : uint32_t { kTTrig = 16, kTStage, kTRows, kTRingLen, kTRing };
+enum : uint32_t { kMeasWaiting = 0, kMeasArmed = 1, kMeasNoEvent = 2 };
+constexpr uint32_t kMeasRing = 3;
+static_assert(kTRing + 3 * kMeasRing <= kMeasWords, "the TARG state fits a pass");
+
+__host__ __device__ constexpr bool meas_reads_previous(uint32_t kind) {
+    return kind == ESPL_MEAS_FIND_WHEN || kind == ESPL_MEAS_DERIV_WHEN || kind == ESPL_MEAS_TARG;
+}
 // MIN, MAX, AVG.
 enum : uint32_t { kXFirst = 1, kXM, kXAt, kXLast, kXPv, kXPx, kXSpan };
 // INTEG, RMS: up to four pending window points (scale, value) from word kIP.
@@ -58,13 +75,21 @@ __host__ __device__ inline void meas_init(const espl_meas& c, double* st, size_t
     for (uint32_t k = 0; k < kMeasWords; k++) MW(k) = 0.0;
     switch (c.kind) {
     case ESPL_MEAS_WHEN:
+    case ESPL_MEAS_TARG:
         MW(kWWantRise) = c.rise;
         MW(kWWantFall) = c.fall;
         MW(kWWantCross) = c.cross;
         MW(kWLast) = NAN;
         MW(kWHit) = NAN;
+        MW(kTTrig) = c.kind == ESPL_MEAS_TARG ? NAN : 0.0;
         break;
-    case ESPL_MEAS_FIND_AT: MW(kAValue) = NAN; break;
+    case ESPL_MEAS_FIND_AT:
+    case ESPL_MEAS_DERIV_AT: MW(kAValue) = NAN; break;
+    case ESPL_MEAS_FIND_WHEN:
+    case ESPL_MEAS_DERIV_WHEN:
+        MW(kAValue) = NAN;
+        MW(kFAt) = NAN;
+        break;
     case ESPL_MEAS_INTEG:
     case ESPL_MEAS_RMS:
         MW(kIFirstX) = NAN;
@@ -104,78 +129,178 @@ __host__ __device__ inline void meas_panel(double* st, size_t stride, uint32_t a
     MW(kINp) = keep;
 }
 
-// Feeds sample (x, v) to pass c unless it is done; marks it done where the
-// whole-waveform scan would stop.
-__host__ __device__ inline void meas_feed(const espl_meas& c, double* st, size_t stride, double x, double v) {
+__host__ __device__ inline bool meas_nan(double v) { return v != v; }
+
+// Cross.feed (scan.zig :88-160) on the event-count words 1..15 of `st`:
+// samples before `td` or `from` are skipped, the first past a nonzero `to`
+// ends the pass (true), as does the event the counts ask for. The level is
+// `val`, or the second vector's value `v2` when the pass names one.
+__host__ __device__ inline bool meas_cross(const espl_meas& c, double* st, size_t stride, double td, double x,
+                                           double v, double v2) {
+    if (x < td || x < c.from) return false;
+    if (c.to != 0 && x > c.to) return true;
+    const bool two = c.level_row != 0;
+    const double level = two ? v2 : c.val;
+    const double prev_level = two ? MW(kWPrev2) : c.val;
+    const double first = MW(kWFirst);
+    if (first == 1.0) {
+        MW(kWCross) = 0;
+        const bool above = !(v < level);
+        MW(kWAbove) = above;
+        if (!above && MW(kWPrev) >= prev_level) {
+            MW(kWFall) = 1;
+            MW(kWCross) = 1;
+        } else if (above && MW(kWPrev) < prev_level) {
+            MW(kWRise) = 1;
+            MW(kWCross) = 1;
+        }
+    }
+    if (first > 1.0) {
+        if (MW(kWAbove) == 0.0 && v >= level) {
+            MW(kWAbove) = 1;
+            MW(kWCross) += 1;
+            MW(kWRise) += 1;
+            if (c.fall != ESPL_MEAS_LAST) MW(kWPending) = 1;
+        } else if (MW(kWAbove) != 0.0 && v <= level) {
+            MW(kWAbove) = 0;
+            MW(kWCross) += 1;
+            MW(kWFall) += 1;
+            if (c.rise != ESPL_MEAS_LAST) MW(kWPending) = 1;
+        }
+        const double px = MW(kWPrevX), pv = MW(kWPrev);
+        const double hit = px + (prev_level - pv) * (x - px) / (v - pv - level + prev_level);
+        if (MW(kWCross) == MW(kWWantCross) || MW(kWRise) == MW(kWWantRise) || MW(kWFall) == MW(kWWantFall)) {
+            MW(kWHit) = hit;
+            MW(kWFound) = 1;
+            return true;
+        }
+        if (MW(kWPending) != 0.0) {
+            if (c.cross == ESPL_MEAS_UNSET && c.rise == ESPL_MEAS_UNSET && c.fall == ESPL_MEAS_UNSET) {
+                MW(kWHit) = hit;
+                MW(kWFound) = 1;
+                return true;
+            }
+            if (c.cross == ESPL_MEAS_LAST || c.rise == ESPL_MEAS_LAST || c.fall == ESPL_MEAS_LAST) MW(kWLast) = hit;
+            MW(kWPending) = 0;
+        }
+    }
+    MW(kWFirst) = first + 1;
+    MW(kWPrev) = v;
+    if (two) MW(kWPrev2) = v2;
+    MW(kWPrevX) = x;
+    return false;
+}
+
+// The event time of a WHEN pass's state (Cross.finish :163-169): the one its
+// count asked for, else the last one (LAST), else NaN.
+__host__ __device__ inline double meas_event(const double* st, size_t stride) {
+    return MW(kWFound) != 0.0 ? MW(kWHit) : MW(kWLast);
+}
+
+// At.feed (scan.zig :182-192) on words kARows..kAValue: true once the
+// segment from the previous sample holds `at`, with the value there (linear)
+// or the segment's slope.
+__host__ __device__ inline bool meas_at(double* st, size_t stride, double at, bool slope, double x, double v) {
+    const double px = MW(kAPx), pv = MW(kAPv);
+    if (MW(kARows) > 0 && px <= at && x >= at) {
+        MW(kAValue) = slope ? (v - pv) / (x - px) : pv + (at - px) * (v - pv) / (x - px);
+        return true;
+    }
+    MW(kARows) += 1;
+    MW(kAPx) = x;
+    MW(kAPv) = v;
+    return false;
+}
+
+// Find.push (scan.zig :357-361): appends (x, v, v2) to the ring of the last
+// kMeasRing samples at word `ring`, length at word `len_word`.
+__host__ __device__ inline void meas_push(double* st, size_t stride, uint32_t ring, uint32_t len_word, double x,
+                                          double v, double v2) {
+    uint32_t len = (uint32_t)MW(len_word);
+    if (len == kMeasRing)
+        for (uint32_t k = 0; k < 3 * (kMeasRing - 1); k++) MW(ring + k) = MW(ring + 3 + k);
+    len = len < kMeasRing ? len + 1 : kMeasRing;
+    MW(len_word) = len;
+    MW(ring + 3 * (len - 1)) = x;
+    MW(ring + 3 * (len - 1) + 1) = v;
+    MW(ring + 3 * (len - 1) + 2) = v2;
+}
+
+// Feeds sample (x, v) to pass c unless it is done, v2 being the value of
+// the pass's level vector (unused without one) and `prev` the state of the
+// pass before it (FIND/DERIV WHEN and TARG read it; nullptr for pass 0);
+// marks the pass done where the whole-waveform scan would stop.
+__host__ __device__ inline void meas_feed(const espl_meas& c, double* st, size_t stride, const double* prev,
+                                          double x, double v, double v2) {
     if (MW(kMeasDone) != 0.0) return;
     bool stop = false;
     switch (c.kind) {
-    case ESPL_MEAS_WHEN: {
-        if (x < c.td || x < c.from) break;
-        if (c.to != 0 && x > c.to) {
+    case ESPL_MEAS_WHEN: stop = meas_cross(c, st, stride, c.td, x, v, v2); break;
+    case ESPL_MEAS_FIND_AT:
+    case ESPL_MEAS_DERIV_AT:
+        // a transient's times rise: past `at`, no later segment holds it
+        stop = meas_at(st, stride, c.at, c.kind == ESPL_MEAS_DERIV_AT, x, v) || x > c.at;
+        break;
+    case ESPL_MEAS_FIND_WHEN:
+    case ESPL_MEAS_DERIV_WHEN: {
+        // Find.feed (scan.zig :365-388): the last rows are kept until the
+        // WHEN pass ends; at its event this becomes the At there, fed those
+        // rows first.
+        const bool slope = c.kind == ESPL_MEAS_DERIV_WHEN;
+        if (MW(kFStage) == kMeasArmed) {
+            stop = meas_at(st, stride, MW(kFAt), slope, x, v) || x > MW(kFAt);
+            break;
+        }
+        meas_push(st, stride, kFRing, kFRingLen, x, v, 0.0);
+        MW(kFRows) += 1;
+        if (!prev || prev[(size_t)kMeasDone * stride] == 0.0) break;
+        const double t = meas_event(prev, stride);
+        if (meas_nan(t)) {
+            MW(kFStage) = kMeasNoEvent;
             stop = true;
             break;
         }
-        const double level = c.val;
-        const double first = MW(kWFirst);
-        if (first == 1.0) {
-            MW(kWCross) = 0;
-            const bool above = !(v < level);
-            MW(kWAbove) = above;
-            if (!above && MW(kWPrev) >= level) {
-                MW(kWFall) = 1;
-                MW(kWCross) = 1;
-            } else if (above && MW(kWPrev) < level) {
-                MW(kWRise) = 1;
-                MW(kWCross) = 1;
-            }
+        MW(kFStage) = kMeasArmed;
+        MW(kFAt) = t;
+        const uint32_t len = (uint32_t)MW(kFRingLen);
+        if (MW(kFRows) > len && t <= MW(kFRing)) {
+            stop = true;
+            break;
         }
-        if (first > 1.0) {
-            if (MW(kWAbove) == 0.0 && v >= level) {
-                MW(kWAbove) = 1;
-                MW(kWCross) += 1;
-                MW(kWRise) += 1;
-                if (c.fall != ESPL_MEAS_LAST) MW(kWPending) = 1;
-            } else if (MW(kWAbove) != 0.0 && v <= level) {
-                MW(kWAbove) = 0;
-                MW(kWCross) += 1;
-                MW(kWFall) += 1;
-                if (c.rise != ESPL_MEAS_LAST) MW(kWPending) = 1;
-            }
-            const double px = MW(kWPrevX), pv = MW(kWPrev);
-            const double hit = px + (level - pv) * (x - px) / (v - pv - level + level);
-            if (MW(kWCross) == MW(kWWantCross) || MW(kWRise) == MW(kWWantRise) || MW(kWFall) == MW(kWWantFall)) {
-                MW(kWHit) = hit;
-                MW(kWFound) = 1;
-                stop = true;
-                break;
-            }
-            if (MW(kWPending) != 0.0) {
-                if (c.cross == ESPL_MEAS_UNSET && c.rise == ESPL_MEAS_UNSET && c.fall == ESPL_MEAS_UNSET) {
-                    MW(kWHit) = hit;
-                    MW(kWFound) = 1;
-                    stop = true;
-                    break;
-                }
-                if (c.cross == ESPL_MEAS_LAST || c.rise == ESPL_MEAS_LAST || c.fall == ESPL_MEAS_LAST) MW(kWLast) = hit;
-                MW(kWPending) = 0;
-            }
+        for (uint32_t j = 0; j < len && !stop; j++) {
+            const double rx = MW(kFRing + 3 * j), rv = MW(kFRing + 3 * j + 1);
+            stop = meas_at(st, stride, t, slope, rx, rv) || rx > t;
         }
-        MW(kWFirst) = first + 1;
-        MW(kWPrev) = v;
-        MW(kWPrevX) = x;
         break;
     }
-    case ESPL_MEAS_FIND_AT: {
-        const double px = MW(kAPx), pv = MW(kAPv);
-        if (MW(kARows) > 0 && px <= c.at && x >= c.at) {
-            MW(kAValue) = pv + (c.at - px) * (v - pv) / (x - px);
+    case ESPL_MEAS_TARG: {
+        // TARG's event count with TD = the TRIG pass's event (the reference
+        // replays its recording from there, measure.zig Stream.next): the
+        // last rows are kept until the TRIG pass ends, then fed first. A
+        // TRIG event before the oldest kept row, with rows before it, leaves
+        // TARG unresolved.
+        if (MW(kTStage) == kMeasArmed) {
+            stop = meas_cross(c, st, stride, MW(kTTrig), x, v, v2);
+            break;
+        }
+        meas_push(st, stride, kTRing, kTRingLen, x, v, v2);
+        MW(kTRows) += 1;
+        if (!prev || prev[(size_t)kMeasDone * stride] == 0.0) break;
+        const double t = meas_event(prev, stride);
+        if (meas_nan(t)) {
+            MW(kTStage) = kMeasNoEvent;
             stop = true;
             break;
         }
-        MW(kARows) += 1;
-        MW(kAPx) = x;
-        MW(kAPv) = v;
+        MW(kTStage) = kMeasArmed;
+        MW(kTTrig) = t;
+        const uint32_t len = (uint32_t)MW(kTRingLen);
+        if (MW(kTRows) > len && t < MW(kTRing)) {
+            stop = true;
+            break;
+        }
+        for (uint32_t j = 0; j < len && !stop; j++)
+            stop = meas_cross(c, st, stride, t, MW(kTRing + 3 * j), MW(kTRing + 3 * j + 1), MW(kTRing + 3 * j + 2));
         break;
     }
     case ESPL_MEAS_MIN:
@@ -253,8 +378,10 @@ __host__ __device__ inline void meas_feed(const espl_meas& c, double* st, size_t
 }
 
 // The result of pass c from its state: `value`, and `at` (the event time of
-// WHEN is its value; MIN/MAX: where; AVG: the last scale value read;
-// INTEG/RMS: the window's end). Folds pending INTEG/RMS points on a copy.
+// WHEN is its value; FIND/DERIV AT: `at`; FIND/DERIV WHEN: the event time;
+// TARG: the TARG event, its value the time from the TRIG event; MIN/MAX:
+// where; AVG: the last scale value read; INTEG/RMS: the window's end). Folds
+// pending INTEG/RMS points on a copy.
 __host__ inline void meas_result(const espl_meas& c, const double* st_in, size_t stride, double& value, double& at) {
     double st_copy[kMeasWords];
     for (uint32_t k = 0; k < kMeasWords; k++) st_copy[k] = st_in[(size_t)k * stride];
@@ -265,12 +392,22 @@ __host__ inline void meas_result(const espl_meas& c, const double* st_in, size_t
     at = nan;
     switch (c.kind) {
     case ESPL_MEAS_WHEN:
-        value = MW(kWFound) != 0.0 ? MW(kWHit) : MW(kWLast);
+        value = meas_event(st, 1);
         at = value;
         break;
+    case ESPL_MEAS_TARG:
+        at = meas_event(st, 1);
+        value = at - MW(kTTrig);
+        break;
     case ESPL_MEAS_FIND_AT:
+    case ESPL_MEAS_DERIV_AT:
         value = MW(kAValue);
         at = c.at;
+        break;
+    case ESPL_MEAS_FIND_WHEN:
+    case ESPL_MEAS_DERIV_WHEN:
+        value = MW(kAValue);
+        at = MW(kFAt);
         break;
     case ESPL_MEAS_MIN:
     case ESPL_MEAS_MAX:

@@ -246,23 +246,38 @@ espl_status espl_get_period_meas(espl_lanes *h, uint32_t net, double *period, ui
 /* Streaming .meas passes over each lane's transient, on the device: every
  * pass reads unknown `row` at t = 0 (the operating point) and at every
  * accepted step, with ngspice's measure semantics as the reference streams
- * them on its lanes (src/output/scan.zig Cross, At, Extremum, Integ; run per
- * lane from src/solver/lane_device.zig). Kinds:
+ * them on its lanes (src/output/scan.zig Cross, At, Extremum, Integ, Find;
+ * run per lane from src/solver/lane_device.zig). Kinds:
  *   WHEN     the time `row` crosses `val` (after `td`, inside [from, to]):
  *            the `rise`-th rising, `fall`-th falling or `cross`-th crossing
- *            (ESPL_MEAS_LAST: the last one; all ESPL_MEAS_UNSET: the first)
- *   FIND_AT  the value at time `at` (linear between steps)
+ *            (ESPL_MEAS_LAST: the last one; all ESPL_MEAS_UNSET: the first);
+ *            with `level_row` = 1 + u, the time `row` crosses unknown u
+ *            (WHEN v(a)=v(b))
+ *   FIND_AT  the value at time `at` (linear between steps); DERIV_AT the
+ *            slope of the step holding `at`
+ *   FIND_WHEN, DERIV_WHEN
+ *            the value or slope of `row` at the event of the pass before
+ *            it, which must be a WHEN pass (FIND v(x) WHEN v(y)=..., the
+ *            pass's own `at` is ignored); `at` reads the event time. If
+ *            that WHEN resolves only at the end of the run (LAST with no
+ *            `to`), the value is NaN
+ *   TARG     the TARG of a TRIG/TARG pair: the previous pass is the TRIG
+ *            (a WHEN pass); this pass counts its own crossing (val or
+ *            level_row, rise/fall/cross, from/to; its `td` is replaced by
+ *            the TRIG event time) from the TRIG event on; value = TARG
+ *            time - TRIG time, `at` = the TARG time
  *   MIN/MAX  the extremum over [from, to] (to = 0: to the end), `at` where
  *   AVG      the trapezoidal average over [from, to]
  *   INTEG    the integral over [from, to] (Simpson 3/8, Simpson, trapezoid
  *            panels as ngspice chooses them); RMS its root-mean-square
- * TRIG/TARG is the difference of two WHEN passes, PP that of MAX and MIN.
+ * PP is the difference of MAX and MIN.
  * Set before espl_init_steps (at most ESPL_MEAS_MAX_PASSES per template);
  * read after the run: value and at are [lanes][n], NaN where a pass saw no
  * result. */
 enum {
     ESPL_MEAS_WHEN = 1, ESPL_MEAS_FIND_AT = 2, ESPL_MEAS_MIN = 3, ESPL_MEAS_MAX = 4, ESPL_MEAS_AVG = 5,
-    ESPL_MEAS_INTEG = 6, ESPL_MEAS_RMS = 7
+    ESPL_MEAS_INTEG = 6, ESPL_MEAS_RMS = 7, ESPL_MEAS_DERIV_AT = 8, ESPL_MEAS_FIND_WHEN = 9,
+    ESPL_MEAS_DERIV_WHEN = 10, ESPL_MEAS_TARG = 11
 };
 #define ESPL_MEAS_UNSET (-1)
 #define ESPL_MEAS_LAST (-2)
@@ -275,7 +290,7 @@ typedef struct {
     double from, to;             /* the window; to = 0 leaves it open */
     double at;                   /* FIND_AT: the time */
     int32_t rise, fall, cross;   /* WHEN: the event's count, ESPL_MEAS_UNSET or ESPL_MEAS_LAST */
-    uint32_t reserved;
+    uint32_t level_row;          /* WHEN, TARG: 0 = the level is `val`; 1 + u = unknown u */
 } espl_meas;
 espl_status espl_set_meas(espl_lanes *h, uint32_t net, const espl_meas *passes, uint32_t n);
 espl_status espl_get_meas(espl_lanes *h, uint32_t net, double *value, double *at);

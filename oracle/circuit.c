@@ -951,6 +951,16 @@ static double next_bp(const ockt *k, double t) {
     return best;
 }
 
+/* Feeds the sample of every .meas pass at time t, in order (a pass that
+ * reads the pass before it sees that pass after this sample). */
+static void feed_passes(const espl_meas *passes, uint32_t n, orc_meas_state *mst, double t, const double *x) {
+    for (uint32_t p = 0; p < n; p++) {
+        const espl_meas *c = &passes[p];
+        orc_meas_feed(c, &mst[p], p ? &passes[p - 1] : NULL, p ? &mst[p - 1] : NULL, t, x[c->row],
+                      c->level_row ? x[c->level_row - 1] : 0.0);
+    }
+}
+
 static void tran_one(job_t *j, uint32_t li) {
     const espl_tran_opts *o = j->topts;
     uint32_t lane = j->lane0 + li;
@@ -967,10 +977,8 @@ static void tran_one(job_t *j, uint32_t li) {
     orc_newton_result r0 = newton(k, x, &op, 1, 0.0, NULL, NULL);
     if (!r0.converged) { rep->status = 4; ckt_free(k); return; }
     orc_meas_state mst[ESPL_MEAS_MAX_PASSES];
-    for (uint32_t p = 0; p < j->n_passes; p++) {
-        orc_meas_init(&j->passes[p], &mst[p]);
-        orc_meas_feed(&j->passes[p], &mst[p], 0.0, x[j->passes[p].row]);
-    }
+    for (uint32_t p = 0; p < j->n_passes; p++) orc_meas_init(&j->passes[p], &mst[p]);
+    feed_passes(j->passes, j->n_passes, mst, 0.0, x);
     uint32_t n1 = n + 1;
     uint32_t ns = k->n_sites;
     /* Row charge ring: logical 1 and 2 start at q(x_op); site ring 1..3 too. */
@@ -1126,7 +1134,7 @@ static void tran_one(job_t *j, uint32_t li) {
             for (uint32_t pi = 0; pi < j->n_probes; pi++) row[pi] = x[j->probes[pi]];
         }
         rows++;
-        for (uint32_t p = 0; p < j->n_passes; p++) orc_meas_feed(&j->passes[p], &mst[p], t_new, x[j->passes[p].row]);
+        feed_passes(j->passes, j->n_passes, mst, t_new, x);
         if (has_meas && t_new >= j->meas_t_start) {
             double v = x[j->meas_row];
             if (m_have && m_prev_v < j->meas_level && v >= j->meas_level) {

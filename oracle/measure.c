@@ -1,8 +1,10 @@
 /* Test infrastructure only (the oracle): the streaming .meas passes the
  * GPU lanes run, restated in plain C from the reference's sample-at-a-time
- * measures (src/output/scan.zig: Cross :61-169, At :171-192, Extremum
- * :195-254, Integ :257-341), which follow ngspice's com_measure2.c. The
- * product never links this file. */
+ * measures (src/output/scan.zig: Cross :61-169 with its level vector, At
+ * :171-192 with its slope, Extremum :195-254, Integ :257-341, Find
+ * :340-390), which follow ngspice's com_measure2.c, and the TARG stage of
+ * src/output/measure.zig Stream.next :708-733 (a Cross with TD at the TRIG
+ * event). The product never links this file. */
 #include <math.h>
 #include <stdint.h>
 #include <string.h>
@@ -38,6 +40,74 @@ void orc_meas_init(const espl_meas *c, orc_meas_state *s) {
     s->value = NAN;
     s->first_x = NAN;
     s->cut_x = NAN;
+    s->t0 = NAN;
+}
+
+/* Cross.feed (scan.zig :88-160, tran mode, one event): returns 1 where the
+ * pass stops. The level is c->val, or v2 with a level vector. */
+static int cross_feed(const espl_meas *c, orc_meas_state *s, double td, double x, double v, double v2) {
+    if (x < td) return 0;
+    if (x < c->from) return 0;
+    if (c->to != 0 && x > c->to) return 1;
+    int two = c->level_row != 0;
+    double level = two ? v2 : c->val;
+    double prev_level = two ? s->prev2 : c->val;
+    if (s->first == 1) {
+        s->cross = 0;
+        s->above = !(v < level);
+        if (!s->above && s->prev >= prev_level) { s->fall = 1; s->cross = 1; }
+        else if (s->above && s->prev < prev_level) { s->rise = 1; s->cross = 1; }
+    }
+    if (s->first > 1) {
+        if (!s->above && v >= level) {
+            s->above = 1; s->cross++; s->rise++;
+            if (c->fall != ESPL_MEAS_LAST) s->pending = 1;
+        } else if (s->above && v <= level) {
+            s->above = 0; s->cross++; s->fall++;
+            if (c->rise != ESPL_MEAS_LAST) s->pending = 1;
+        }
+        double hit = s->prev_x + (prev_level - s->prev) * (x - s->prev_x) / (v - s->prev - level + prev_level);
+        if (s->cross == s->want_cross || s->rise == s->want_rise || s->fall == s->want_fall) {
+            s->hit = hit; s->found = 1; return 1;
+        }
+        if (s->pending) {
+            if (c->cross == ESPL_MEAS_UNSET && c->rise == ESPL_MEAS_UNSET && c->fall == ESPL_MEAS_UNSET) {
+                s->hit = hit; s->found = 1; return 1;
+            }
+            if (c->cross == ESPL_MEAS_LAST || c->rise == ESPL_MEAS_LAST || c->fall == ESPL_MEAS_LAST) s->last = hit;
+            s->pending = 0;
+        }
+    }
+    s->first++;
+    s->prev = v;
+    if (two) s->prev2 = v2;
+    s->prev_x = x;
+    return 0;
+}
+
+/* Cross.finish (scan.zig :163-169) for one event: the count's, else LAST's. */
+static double cross_event(const orc_meas_state *s) { return s->found ? s->hit : s->last; }
+
+/* At.feed (scan.zig :182-192): 1 once the segment from the previous sample
+ * holds `at`, with the value (or slope) there in s->value. */
+static int at_feed(orc_meas_state *s, double at, int slope, double x, double v) {
+    if (s->rows > 0 && s->px <= at && x >= at) {
+        s->value = slope ? (v - s->pv) / (x - s->px) : s->pv + (at - s->px) * (v - s->pv) / (x - s->px);
+        return 1;
+    }
+    s->rows++;
+    s->px = x;
+    s->pv = v;
+    return 0;
+}
+
+/* Find.push (scan.zig :357-361) with the level value kept beside. */
+static void ring_push(orc_meas_state *s, double x, double v, double v2) {
+    if (s->ring_len == 3) memmove(s->ring[0], s->ring[1], sizeof(s->ring[0]) * 2);
+    if (s->ring_len < 3) s->ring_len++;
+    s->ring[s->ring_len - 1][0] = x;
+    s->ring[s->ring_len - 1][1] = v;
+    s->ring[s->ring_len - 1][2] = v2;
 }
 
 /* Integ.panel :307-328: Simpson 3/8 over three equal spacings, Simpson over
@@ -71,55 +141,54 @@ static void panel(orc_meas_state *s, int avail) {
     s->np = keep;
 }
 
-void orc_meas_feed(const espl_meas *c, orc_meas_state *s, double x, double v) {
+void orc_meas_feed(const espl_meas *c, orc_meas_state *s, const espl_meas *prev_c, const orc_meas_state *prev,
+                   double x, double v, double v2) {
+    (void)prev_c;
     if (s->done) return;
     switch (c->kind) {
-    case ESPL_MEAS_WHEN: { /* Cross.feed, tran mode, one event */
-        if (x < c->td) return;
-        if (x < c->from) return;
-        if (c->to != 0 && x > c->to) { s->done = 1; return; }
-        double level = c->val;
-        if (s->first == 1) {
-            s->cross = 0;
-            s->above = !(v < level);
-            if (!s->above && s->prev >= level) { s->fall = 1; s->cross = 1; }
-            else if (s->above && s->prev < level) { s->rise = 1; s->cross = 1; }
-        }
-        if (s->first > 1) {
-            if (!s->above && v >= level) {
-                s->above = 1; s->cross++; s->rise++;
-                if (c->fall != ESPL_MEAS_LAST) s->pending = 1;
-            } else if (s->above && v <= level) {
-                s->above = 0; s->cross++; s->fall++;
-                if (c->rise != ESPL_MEAS_LAST) s->pending = 1;
-            }
-            double hit = s->prev_x + (level - s->prev) * (x - s->prev_x) / (v - s->prev - level + level);
-            if (s->cross == s->want_cross || s->rise == s->want_rise || s->fall == s->want_fall) {
-                s->hit = hit; s->found = 1; s->done = 1; return;
-            }
-            if (s->pending) {
-                if (c->cross == ESPL_MEAS_UNSET && c->rise == ESPL_MEAS_UNSET && c->fall == ESPL_MEAS_UNSET) {
-                    s->hit = hit; s->found = 1; s->done = 1; return;
-                }
-                if (c->cross == ESPL_MEAS_LAST || c->rise == ESPL_MEAS_LAST || c->fall == ESPL_MEAS_LAST) s->last = hit;
-                s->pending = 0;
-            }
-        }
-        s->first++;
-        s->prev = v;
-        s->prev_x = x;
+    case ESPL_MEAS_WHEN:
+        s->done = cross_feed(c, s, c->td, x, v, v2);
         return;
-    }
-    case ESPL_MEAS_FIND_AT: /* At.feed */
-        if (s->rows > 0 && s->px <= c->at && x >= c->at) {
-            s->value = s->pv + (c->at - s->px) * (v - s->pv) / (x - s->px);
-            s->done = 1;
+    case ESPL_MEAS_FIND_AT:
+    case ESPL_MEAS_DERIV_AT: /* Dev.feed's .at: past `at` no later segment holds it */
+        s->done = at_feed(s, c->at, c->kind == ESPL_MEAS_DERIV_AT, x, v) || x > c->at;
+        return;
+    case ESPL_MEAS_FIND_WHEN:
+    case ESPL_MEAS_DERIV_WHEN: { /* Find.feed */
+        int slope = c->kind == ESPL_MEAS_DERIV_WHEN;
+        if (s->stage == 1) {
+            s->done = at_feed(s, s->t0, slope, x, v) || x > s->t0;
             return;
         }
-        s->rows++;
-        s->px = x;
-        s->pv = v;
+        ring_push(s, x, v, 0.0);
+        s->kept_rows++;
+        if (!prev || !prev->done) return;
+        double t = cross_event(prev);
+        if (isnan(t)) { s->stage = 2; s->done = 1; return; }
+        s->stage = 1;
+        s->t0 = t;
+        if (s->kept_rows > (uint64_t)s->ring_len && t <= s->ring[0][0]) { s->done = 1; return; }
+        for (int k = 0; k < s->ring_len; k++)
+            if (at_feed(s, t, slope, s->ring[k][0], s->ring[k][1]) || s->ring[k][0] > t) { s->done = 1; return; }
         return;
+    }
+    case ESPL_MEAS_TARG: { /* Stream.next's TARG: a Cross from the TRIG event on */
+        if (s->stage == 1) {
+            s->done = cross_feed(c, s, s->t0, x, v, v2);
+            return;
+        }
+        ring_push(s, x, v, v2);
+        s->kept_rows++;
+        if (!prev || !prev->done) return;
+        double t = cross_event(prev);
+        if (isnan(t)) { s->stage = 2; s->done = 1; return; }
+        s->stage = 1;
+        s->t0 = t;
+        if (s->kept_rows > (uint64_t)s->ring_len && t < s->ring[0][0]) { s->done = 1; return; }
+        for (int k = 0; k < s->ring_len; k++)
+            if (cross_feed(c, s, t, s->ring[k][0], s->ring[k][1], s->ring[k][2])) { s->done = 1; return; }
+        return;
+    }
     case ESPL_MEAS_MIN:
     case ESPL_MEAS_MAX:
     case ESPL_MEAS_AVG: /* Extremum.feed */
@@ -185,12 +254,22 @@ void orc_meas_result(const espl_meas *c, orc_meas_state *s, double *value, doubl
     *at = NAN;
     switch (c->kind) {
     case ESPL_MEAS_WHEN: /* Cross.finish */
-        *value = s->found ? s->hit : s->last;
+        *value = cross_event(s);
         *at = *value;
         return;
+    case ESPL_MEAS_TARG:
+        *at = cross_event(s);
+        *value = *at - s->t0;
+        return;
     case ESPL_MEAS_FIND_AT:
+    case ESPL_MEAS_DERIV_AT:
         *value = s->value;
         *at = c->at;
+        return;
+    case ESPL_MEAS_FIND_WHEN:
+    case ESPL_MEAS_DERIV_WHEN:
+        *value = s->value;
+        *at = s->t0;
         return;
     case ESPL_MEAS_MIN:
     case ESPL_MEAS_MAX: /* Extremum.stat */
@@ -217,9 +296,27 @@ void orc_meas_result(const espl_meas *c, orc_meas_state *s, double *value, doubl
 }
 
 int orc_meas_series(const espl_meas *c, const double *x, const double *v, uint32_t n, double *value, double *at) {
-    orc_meas_state s;
-    orc_meas_init(c, &s);
-    for (uint32_t k = 0; k < n; k++) orc_meas_feed(c, &s, x[k], v[k]);
-    orc_meas_result(c, &s, value, at);
+    espl_meas one = *c;
+    one.row = 0;
+    one.level_row = 0;
+    return orc_meas_table(&one, 1, x, v, 1, n, value, at);
+}
+
+int orc_meas_table(const espl_meas *passes, uint32_t n_passes, const double *x, const double *cols, uint32_t n_cols,
+                   uint32_t n, double *value, double *at) {
+    if (n_passes > ESPL_MEAS_MAX_PASSES) return 1;
+    orc_meas_state s[ESPL_MEAS_MAX_PASSES];
+    for (uint32_t p = 0; p < n_passes; p++) {
+        if (passes[p].row >= n_cols || passes[p].level_row > n_cols) return 1;
+        orc_meas_init(&passes[p], &s[p]);
+    }
+    for (uint32_t k = 0; k < n; k++)
+        for (uint32_t p = 0; p < n_passes; p++) {
+            const espl_meas *c = &passes[p];
+            const double *row = cols + (size_t)k * n_cols;
+            orc_meas_feed(c, &s[p], p ? &passes[p - 1] : NULL, p ? &s[p - 1] : NULL, x[k], row[c->row],
+                          c->level_row ? row[c->level_row - 1] : 0.0);
+        }
+    for (uint32_t p = 0; p < n_passes; p++) orc_meas_result(&passes[p], &s[p], &value[p], &at[p]);
     return 0;
 }

@@ -96,16 +96,29 @@ int orc_tran_lanes(const espl_netlist *net, uint32_t lane0, uint32_t count, cons
 typedef struct {
     int done, first, above, pending, found, inside, cut, np;
     int32_t rise, fall, cross, want_rise, want_fall, want_cross;
-    double prev, prev_x, last, hit;
+    double prev, prev2, prev_x, last, hit;
     uint64_t rows, count;
     double px, pv, py, value, xv, m, m_at, span;
     double p[4][2], first_x, cut_x, sum[3];
+    /* FIND/DERIV WHEN and TARG: stage (0 waiting, 1 armed, 2 no event),
+     * the event time they start at, rows kept (x, v, level) and read */
+    int stage, ring_len;
+    double t0, ring[3][3];
+    uint64_t kept_rows;
 } orc_meas_state;
 void orc_meas_init(const espl_meas *c, orc_meas_state *s);
-void orc_meas_feed(const espl_meas *c, orc_meas_state *s, double x, double v);
+/* Feeds (x, v) to pass c; v2 is its level vector's value (WHEN/TARG with
+ * level_row), prev_c/prev the pass before it (NULL for the first). */
+void orc_meas_feed(const espl_meas *c, orc_meas_state *s, const espl_meas *prev_c, const orc_meas_state *prev,
+                   double x, double v, double v2);
 void orc_meas_result(const espl_meas *c, orc_meas_state *s, double *value, double *at);
-/* One pass over a whole series (x[k], v[k]). */
+/* One pass over a whole series (x[k], v[k]); the pass's row is ignored. */
 int orc_meas_series(const espl_meas *c, const double *x, const double *v, uint32_t n, double *value, double *at);
+/* n_passes passes over a series of n samples, column u of sample k at
+ * cols[k * n_cols + u] (a pass reads column `row`, its level column
+ * level_row - 1); value and at are [n_passes]. */
+int orc_meas_table(const espl_meas *passes, uint32_t n_passes, const double *x, const double *cols, uint32_t n_cols,
+                   uint32_t n, double *value, double *at);
 /* orc_tran_lanes with .meas passes instead of probes and the period: each
  * pass reads its row at t = 0 and at every accepted step; value and at are
  * [count][n_passes]. */

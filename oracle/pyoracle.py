@@ -37,6 +37,8 @@ def lib():
         L.orc_tran_meas.restype = C.c_int
         L.orc_meas_series.argtypes = [C.POINTER(MeasPass), f64p, f64p, C.c_uint32, f64p, f64p]
         L.orc_meas_series.restype = C.c_int
+        L.orc_meas_table.argtypes = [C.POINTER(MeasPass), C.c_uint32, f64p, f64p, C.c_uint32, C.c_uint32, f64p, f64p]
+        L.orc_meas_table.restype = C.c_int
         L.orc_planes.argtypes = [C.c_void_p, C.c_uint32, f64p, f64p, f64p]
         L.orc_planes.restype = C.c_int
         L.orc_op_ladder.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, f64p, C.c_void_p, C.c_uint32]
@@ -315,6 +317,23 @@ def meas_series(p: MeasPass, xs, vs) -> Tuple[float, float]:
     lib().orc_meas_series(C.byref(p), xs.ctypes.data_as(f64p), vs.ctypes.data_as(f64p), len(xs), C.byref(v),
                           C.byref(a))
     return v.value, a.value
+
+
+def meas_table(passes: Sequence[MeasPass], xs, cols):
+    """Passes over a table of samples: cols[k, u] is column u at xs[k]; a
+    pass reads column `row` (and its level column). Returns (value, at),
+    one entry per pass."""
+    xs = np.ascontiguousarray(xs, dtype=np.float64)
+    cols = np.ascontiguousarray(cols, dtype=np.float64)
+    assert cols.ndim == 2 and len(cols) == len(xs)
+    n = len(passes)
+    arr = (MeasPass * max(n, 1))(*passes)
+    val = np.full(max(n, 1), np.nan)
+    at = np.full(max(n, 1), np.nan)
+    r = lib().orc_meas_table(arr, n, xs.ctypes.data_as(f64p), cols.ctypes.data_as(f64p), cols.shape[1], len(xs),
+                             val.ctypes.data_as(f64p), at.ctypes.data_as(f64p))
+    assert r == 0
+    return val[:n], at[:n]
 
 
 def device_probe(net: Netlist, batch: int, inst: int, lane: int, v):

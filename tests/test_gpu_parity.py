@@ -262,6 +262,45 @@ def test_streaming_meas_passes(oracle, precision):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_chained_meas_passes(oracle, precision):
+    """The passes that read another vector or the pass before them, on the
+    ring oscillator against the oracle: FIND and DERIV at a WHEN event,
+    DERIV at a time, WHEN one node crosses another, and a TRIG/TARG pair
+    whose TARG counts from the TRIG event."""
+    net = decks.ring_oscillator(16, stages=15)
+    s1, s3, s4 = net.node("s1"), net.node("s3"), net.node("s4")
+    M = abi.meas_pass
+    passes = [M(abi.MEAS_WHEN, s3, val=0.9, td=0.5e-9, rise=2),   # 0: the event
+              M(abi.MEAS_FIND_WHEN, s4),                           # 1: s4 (falling) there
+              M(abi.MEAS_WHEN, s3, val=0.9, td=0.5e-9, rise=2),
+              M(abi.MEAS_DERIV_WHEN, s4),                          # 3: its slope there
+              M(abi.MEAS_DERIV_AT, s3, at=2.2e-9),                 # 4
+              M(abi.MEAS_WHEN, s1, level_row=s3, cross=2),         # 5: s1 = s3
+              M(abi.MEAS_WHEN, s1, val=0.9, rise=1),               # 6: TRIG
+              M(abi.MEAS_TARG, s3, val=0.9, fall=1)]               # 7: TARG
+    opts = abi.tran_opts(t_stop=3e-9, dt=1e-12, dt_max=5e-12, method=1, max_iter=20)
+    vo, ao, _, ro = oracle.tran_meas(net, opts, passes, threads=8)
+    with Lanes([net], precision=precision) as L:
+        L.set_meas(0, passes)
+        reps = L.run_tran(opts, steps_per_launch=2048)
+        v, a = L.get_meas(0)
+    assert all(r.status == 1 for r in reps)
+    assert np.isfinite(vo).all() and np.isfinite(v).all()
+    for k in (0, 5, 6):  # event times
+        np.testing.assert_allclose(v[:, k], vo[:, k], rtol=1e-6, err_msg=f"pass {k}")
+    np.testing.assert_allclose(a[:, 7], ao[:, 7], rtol=1e-6)  # the TARG time
+    np.testing.assert_allclose(v[:, 7], vo[:, 7], rtol=0, atol=2e-6 * opts.t_stop)
+    np.testing.assert_array_equal(a[:, 1], v[:, 0])  # FIND reads at the WHEN's event
+    # a value at an event moves with the event: slope x time difference
+    slope_tol = np.abs(vo[:, 3]) * 2 * np.abs(v[:, 0] - vo[:, 0])
+    assert (np.abs(v[:, 1] - vo[:, 1]) <= 1e-6 * np.abs(vo[:, 1]) + 1e-9 + slope_tol).all()
+    # slopes of one step: a sample's error over the step (V/s)
+    for k in (3, 4):
+        np.testing.assert_allclose(v[:, k], vo[:, k], rtol=1e-3, atol=1e6, err_msg=f"pass {k}")
+    assert (np.abs(vo[:, 3]) > 1e9).all() and (np.abs(vo[:, 4]) > 1e8).any()  # the slopes are not flat
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_operating_point_ladder(oracle, precision):
     """espl_solve_op from the cold start: the op-amp lanes the plain rung
     leaves unconverged walk the continuation ladder on the device and all
