@@ -68,6 +68,7 @@ class MeasPass(C.Structure):
 MEAS_WHEN, MEAS_FIND_AT, MEAS_MIN, MEAS_MAX, MEAS_AVG, MEAS_INTEG, MEAS_RMS = 1, 2, 3, 4, 5, 6, 7
 MEAS_DERIV_AT, MEAS_FIND_WHEN, MEAS_DERIV_WHEN, MEAS_TARG = 8, 9, 10, 11
 MEAS_UNSET, MEAS_LAST = -1, -2
+MEAS_MAX_PASSES = 16  # per template
 
 
 def meas_pass(kind, row, val=0.0, td=0.0, from_=0.0, to=0.0, at=0.0, rise=MEAS_UNSET, fall=MEAS_UNSET,

@@ -111,6 +111,8 @@ class Netlist:
     current_rows: np.ndarray  # uint8 [n]
     # Sweep parameters per lane (the MLP's inputs), [lanes, k]; may be empty.
     sweep: Optional[np.ndarray] = None
+    # The branch-current unknown of each named voltage source.
+    branch_names: Dict[str, int] = dataclasses.field(default_factory=dict)
 
     @property
     def nnz(self) -> int:
@@ -135,6 +137,7 @@ class Builder:
         self.nodes: Dict[str, int] = {}
         self.devs: Dict[int, List[Tuple[List[str], np.ndarray]]] = {k: [] for k in TERMS}
         self.vsrc_names: List[str] = []
+        self.vsrc_labels: Dict[str, str] = {}
 
     def _lane(self, v) -> np.ndarray:
         a = np.asarray(v, dtype=np.float64)
@@ -166,10 +169,13 @@ class Builder:
     def m(self, d, g, s, b, typ, vto, kp, w, l, gamma=0.0, phi=0.6, lam=0.0, is_=1e-14):
         self.add(MOS1, [d, g, s, b], [typ, vto, kp, gamma, phi, lam, is_, w, l])
 
-    def v(self, p, n, dc=0.0, pulse=None):
-        """pulse = (v1, v2, td, tr, tf, pw, per)."""
+    def v(self, p, n, dc=0.0, pulse=None, label=None):
+        """pulse = (v1, v2, td, tr, tf, pw, per); `label` names the source
+        (its branch current is then Netlist.branch_names[label])."""
         name = f"#br{len(self.vsrc_names)}"
         self.vsrc_names.append(name)
+        if label is not None:
+            self.vsrc_labels[label] = name
         self.add(VSRC, [p, n, name], _src_params(dc, pulse))
 
     def i(self, p, n, dc=0.0, pulse=None):
@@ -208,8 +214,9 @@ class Builder:
             rows.extend(rr)
             col_ptr[c + 1] = len(rows)
         node_names = {k: v for k, v in idx.items() if k != "0"}
+        branches = {label: idx[br] for label, br in self.vsrc_labels.items()}
         return Netlist(self.name, n, col_ptr, np.array(rows, dtype=np.uint32), batches, self.lanes,
-                       node_names, cur, sweep)
+                       node_names, cur, sweep, branches)
 
 
 def _src_params(dc, pulse):

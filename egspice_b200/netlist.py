@@ -19,8 +19,10 @@ the lanes carry:
   over numbers, parameters, + - * / ** and parentheses
 * ``+`` continuation lines, ``*`` comment lines, ``;`` and ``$ `` inline
   comments; the first line is the title; ``.end`` ends the deck; analysis
-  cards (.op .tran .dc .option .options .temp .meas .print .save .probe) are
-  accepted and ignored (the caller runs the analysis through the API).
+  cards (.op .tran .dc .option .options .temp .print .save .probe) are
+  accepted and ignored (the caller runs the analysis through the API);
+  ``.meas tran`` cards are read by `read_measures` into the lanes' streaming
+  measure passes.
 
 Per-lane values: `params` maps parameter names to a scalar or to an array of
 one value per lane (a Monte Carlo draw or a sweep); they override `.param`
@@ -34,6 +36,7 @@ outside the subset raises `DeckError` naming the line.
 from __future__ import annotations
 
 import ast
+import dataclasses
 import math
 import operator
 import re
@@ -41,6 +44,7 @@ from typing import Dict, List, Mapping, Optional, Sequence, Union
 
 import numpy as np
 
+from . import abi
 from .decks import Builder, Netlist
 
 Value = Union[float, np.ndarray]
@@ -237,6 +241,17 @@ def _kv(tokens: Sequence[str], where: str) -> Dict[str, str]:
     return out
 
 
+def _read_params(cards: Sequence[tuple], env: _Env) -> None:
+    """The .param cards into `env`, values given by the caller kept."""
+    for ln, card in cards:
+        toks = _split(card)
+        if toks[0] == ".param":
+            where = f"line {ln}"
+            for k, v in _kv(toks[1:], where).items():
+                if k not in env.given:
+                    env.vals[k] = env.value(v, where)
+
+
 def read_deck(text: str, lanes: int = 1, params: Optional[Mapping[str, Value]] = None,
               name: Optional[str] = None) -> Netlist:
     """The deck `text` as a Netlist of `lanes` lanes; `params` gives
@@ -247,16 +262,13 @@ def read_deck(text: str, lanes: int = 1, params: Optional[Mapping[str, Value]] =
     env = _Env(lanes, params)
     cards = _logical_lines(text)
     title = text.splitlines()[0].strip() if text.strip() else "deck"
-    # .param and .model first (SPICE cards are order-free)
+    _read_params(cards, env)
+    # .model next (SPICE cards are order-free)
     models: Dict[str, tuple] = {}
     for ln, card in cards:
         toks = _split(card)
         where = f"line {ln}"
-        if toks[0] == ".param":
-            for k, v in _kv(toks[1:], where).items():
-                if k not in env.given:
-                    env.vals[k] = env.value(v, where)
-        elif toks[0] == ".model":
+        if toks[0] == ".model":
             if len(toks) < 3:
                 raise DeckError(f"{where}: .model needs a name and a type")
             mtype = toks[2].split("(")[0]
@@ -328,7 +340,10 @@ def read_deck(text: str, lanes: int = 1, params: Optional[Mapping[str, Value]] =
             if len(toks) < 3:
                 raise DeckError(f"{where}: a source needs two nodes")
             dc, pulse = source(toks[3:], where)
-            (b.v if kind == "v" else b.i)(node(toks[1]), node(toks[2]), dc=dc, pulse=pulse)
+            if kind == "v":
+                b.v(node(toks[1]), node(toks[2]), dc=dc, pulse=pulse, label=head)
+            else:
+                b.i(node(toks[1]), node(toks[2]), dc=dc, pulse=pulse)
         elif kind == "d":
             if len(toks) != 4:
                 raise DeckError(f"{where}: D needs two nodes and a model")
@@ -359,3 +374,188 @@ def read_deck(text: str, lanes: int = 1, params: Optional[Mapping[str, Value]] =
     arrays = [np.asarray(v, dtype=np.float64) for k, v in params.items() if np.ndim(v) == 1]
     sweep = np.stack(arrays, axis=1) if arrays else None
     return b.freeze(sweep)
+
+
+# ---------------------------------------------------------------------------
+# .meas tran cards -> the lanes' streaming measure passes (espl_meas)
+
+
+@dataclasses.dataclass
+class Measure:
+    """One `.meas tran` card: its name, the consecutive passes that compute
+    it, and how its value comes out of them: the last pass's value, or (PP)
+    the first pass's (MAX) minus the second's (MIN)."""
+    name: str
+    passes: List[abi.MeasPass]
+    pp: bool = False
+
+
+_COUNTS = ("rise", "fall", "cross")
+
+
+def _vector(tok: str, net: Netlist, where: str) -> int:
+    """The unknown a waveform token reads: v(node) or i(vsource)."""
+    m = re.fullmatch(r"([vi])\(([^(),]+)\)", tok)
+    if not m:
+        raise DeckError(f"{where}: the measure reads {tok!r}; only v(node) and i(vsource) ride the lanes")
+    kind, name = m.group(1), m.group(2).strip()
+    if kind == "v":
+        if name in ("0", "gnd"):
+            raise DeckError(f"{where}: v(0) is the ground")
+        if name not in net.node_names:
+            raise DeckError(f"{where}: no node {name!r}")
+        return net.node_names[name]
+    if name not in net.branch_names:
+        raise DeckError(f"{where}: no voltage source {name!r} for i({name})")
+    return net.branch_names[name]
+
+
+def _scalar(env: _Env, text: str, where: str) -> float:
+    v = env.value(text, where)
+    if np.ndim(v) != 0:
+        raise DeckError(f"{where}: a measure's {text!r} must be the same on every lane")
+    return float(v)
+
+
+def _clause(toks: List[str], net: Netlist, env: _Env, where: str, opts_ok: Sequence[str]) -> Dict[str, object]:
+    """Options name=value of one clause (rise/fall/cross as counts or LAST,
+    the others as scalars); a bare `last` is RISE/FALL/CROSS=LAST's shorthand
+    for CROSS."""
+    out: Dict[str, object] = {}
+    for t in toks:
+        if t == "last":
+            out["cross"] = abi.MEAS_LAST
+            continue
+        if "=" not in t:
+            raise DeckError(f"{where}: unexpected {t!r} in a .meas card")
+        k, v = t.split("=", 1)
+        if k not in opts_ok:
+            raise DeckError(f"{where}: the .meas option {k.upper()} is outside what the lanes carry")
+        if k in _COUNTS:
+            if v == "last":
+                out[k] = abi.MEAS_LAST
+            else:
+                c = _scalar(env, v, where)
+                if c != int(c) or c < 1:
+                    raise DeckError(f"{where}: {k.upper()}={v} must be a count from 1 or LAST")
+                out[k] = int(c)
+        else:
+            out["from_" if k == "from" else k] = _scalar(env, v, where)
+    if sum(k in out for k in _COUNTS) > 1:
+        raise DeckError(f"{where}: give one of RISE, FALL, CROSS")
+    return out
+
+
+def _when(test: str, net: Netlist, env: _Env, where: str) -> Dict[str, object]:
+    """`vec=value` or `vec=vec2` of a WHEN: the pass's row and its level."""
+    if "=" not in test:
+        raise DeckError(f"{where}: WHEN needs vector=value")
+    lhs, rhs = test.split("=", 1)
+    row = _vector(lhs, net, where)
+    if re.fullmatch(r"[vi]\([^()]*\)", rhs):
+        return {"row": row, "level_row": _vector(rhs, net, where)}
+    return {"row": row, "val": _scalar(env, rhs, where)}
+
+
+def _measure(name: str, func: str, rest: List[str], net: Netlist, env: _Env, where: str) -> Measure:
+    M = abi.meas_pass
+    window = ("from", "to")
+    counts_td = _COUNTS + ("td",)
+    if func == "when":
+        if not rest:
+            raise DeckError(f"{where}: WHEN needs vector=value")
+        w = _when(rest[0], net, env, where)
+        o = _clause(rest[1:], net, env, where, counts_td + window)
+        return Measure(name, [M(abi.MEAS_WHEN, w.pop("row"), **w, **o)])
+    if func in ("find", "deriv"):
+        if len(rest) < 2:
+            raise DeckError(f"{where}: {func.upper()} needs a vector and AT= or WHEN")
+        row = _vector(rest[0], net, where)
+        if rest[1].startswith("at="):
+            if len(rest) > 2:
+                raise DeckError(f"{where}: {func.upper()} ... AT takes no other option")
+            kind = abi.MEAS_FIND_AT if func == "find" else abi.MEAS_DERIV_AT
+            return Measure(name, [M(kind, row, at=_scalar(env, rest[1][3:], where))])
+        if rest[1] != "when" or len(rest) < 3:
+            raise DeckError(f"{where}: {func.upper()} needs AT= or WHEN vector=value")
+        w = _when(rest[2], net, env, where)
+        o = _clause(rest[3:], net, env, where, counts_td + window)
+        kind = abi.MEAS_FIND_WHEN if func == "find" else abi.MEAS_DERIV_WHEN
+        return Measure(name, [M(abi.MEAS_WHEN, w.pop("row"), **w, **o), M(kind, row)])
+    if func == "trig":
+        if "targ" not in rest:
+            raise DeckError(f"{where}: TRIG needs its TARG")
+        k = rest.index("targ")
+        trig, targ = rest[:k], rest[k + 1:]
+        passes = []
+        for part, kind in ((trig, abi.MEAS_WHEN), (targ, abi.MEAS_TARG)):
+            if not part or part[0].startswith("at="):
+                raise DeckError(f"{where}: TRIG/TARG AT= is outside what the lanes carry; give a vector and VAL=")
+            row = _vector(part[0], net, where)
+            o = _clause(part[1:], net, env, where, ("val",) + counts_td + window)
+            if kind == abi.MEAS_TARG:
+                o.pop("td", None)  # the TARG counts from the TRIG event
+            passes.append(M(kind, row, **o))
+        return Measure(name, passes)
+    stats = {"max": abi.MEAS_MAX, "min": abi.MEAS_MIN, "avg": abi.MEAS_AVG, "rms": abi.MEAS_RMS,
+             "integ": abi.MEAS_INTEG, "integral": abi.MEAS_INTEG}
+    if func in stats or func == "pp":
+        if not rest:
+            raise DeckError(f"{where}: {func.upper()} needs a vector")
+        row = _vector(rest[0], net, where)
+        o = _clause(rest[1:], net, env, where, window)
+        if func == "pp":
+            return Measure(name, [M(abi.MEAS_MAX, row, **o), M(abi.MEAS_MIN, row, **o)], pp=True)
+        return Measure(name, [M(stats[func], row, **o)])
+    raise DeckError(f"{where}: the measure {func.upper()} is outside what the lanes carry")
+
+
+def read_measures(text: str, net: Netlist, params: Optional[Mapping[str, Value]] = None) -> List[Measure]:
+    """The deck's `.meas tran` cards as measures on `net` (the deck read by
+    `read_deck`, with the same `params`): WHEN (against a value or a second
+    vector; RISE/FALL/CROSS counts or LAST, TD, FROM, TO), FIND and DERIV at
+    a time or at a WHEN, TRIG ... TARG (VAL and counts per clause; the TARG
+    counts from the TRIG event, as the reference's measure stream does),
+    MAX, MIN, AVG, RMS, INTEG, PP over a window. Vectors are v(node) and
+    i(vsource); values are numbers or parameters the same on every lane.
+    Anything else raises DeckError naming the line."""
+    env = _Env(net.lanes, dict(params or {}))
+    cards = _logical_lines(text)
+    _read_params(cards, env)
+    out: List[Measure] = []
+    for ln, card in cards:
+        toks = _split(card)
+        if toks[0] not in (".meas", ".measure"):
+            continue
+        where = f"line {ln}"
+        if len(toks) < 4:
+            raise DeckError(f"{where}: .meas needs an analysis, a name and a measure")
+        if toks[1] != "tran":
+            raise DeckError(f"{where}: only .meas tran rides the lanes")
+        name = toks[2]
+        if any(m.name == name for m in out):
+            raise DeckError(f"{where}: a second measure named {name!r}")
+        out.append(_measure(name, toks[3], toks[4:], net, env, where))
+    return out
+
+
+def measure_passes(measures: Sequence[Measure]) -> List[abi.MeasPass]:
+    """Every measure's passes, in order, for Lanes.set_meas."""
+    passes = [p for m in measures for p in m.passes]
+    if len(passes) > abi.MEAS_MAX_PASSES:
+        raise DeckError(f"the measures need {len(passes)} passes; a template takes {abi.MEAS_MAX_PASSES}")
+    return passes
+
+
+def measure_values(measures: Sequence[Measure], value: np.ndarray) -> Dict[str, np.ndarray]:
+    """Each measure's value per lane from Lanes.get_meas's `value` [lanes,
+    passes] (NaN where it has none)."""
+    out: Dict[str, np.ndarray] = {}
+    k = 0
+    for m in measures:
+        if m.pp:
+            out[m.name] = value[:, k] - value[:, k + 1]
+        else:
+            out[m.name] = value[:, k + len(m.passes) - 1]
+        k += len(m.passes)
+    return out

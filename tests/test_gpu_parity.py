@@ -232,6 +232,49 @@ vin s0 0 dc {vin}
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_deck_measures(oracle, precision):
+    """`.meas tran` cards of a deck (egspice_b200/netlist.py read_measures)
+    on the lanes against the oracle: 64 RC lanes with per-lane R, every kind
+    of card the lanes take, a source current among the vectors."""
+    from egspice_b200.netlist import measure_passes, measure_values, read_deck, read_measures
+    text = """RC step response with measures
+vin in 0 dc 0 pulse(0 1 0 0.2n 0.2n 1 2)
+r1 in out rval
+c1 out 0 1p
+.meas tran t50 when v(out)=0.5
+.meas tran rise trig v(out) val=0.1 rise=1 targ v(out) val=0.9 rise=1
+.meas tran v2n find v(out) at=2n
+.meas tran slope2n deriv v(out) at=2n
+.meas tran iin find i(vin) at=2n
+.meas tran early find v(out) when v(in)=0.5
+.meas tran swing pp v(out)
+.meas tran avg avg v(out) from=1n to=5n
+.meas tran rms rms v(out) from=1n
+.meas tran area integ v(in) to=5n
+.end
+"""
+    params = {"rval": np.random.default_rng(5).uniform(0.5e3, 1.5e3, 64)}
+    net = read_deck(text, lanes=64, params=params)
+    ms = read_measures(text, net, params=params)
+    opts = abi.tran_opts(t_stop=6e-9, dt=1e-12, dt_max=5e-12, method=1, max_iter=20)
+    vo, _, _, ro = oracle.tran_meas(net, opts, measure_passes(ms), threads=8)
+    with Lanes([net], precision=precision) as L:
+        L.set_meas(0, measure_passes(ms))
+        reps = L.run_tran(opts, steps_per_launch=2048)
+        v, _ = L.get_meas(0)
+    assert all(r.status == 1 for r in reps)
+    got, want = measure_values(ms, v), measure_values(ms, vo)
+    # the 1e-6 bar; voltages with its 1e-9 V floor, amperes 1e-12 A, times
+    # and the integral relative only; a slope over one step: its samples'
+    # floor over the step (V/s)
+    atol = {"v2n": 1e-9, "early": 1e-9, "swing": 1e-9, "avg": 1e-9, "rms": 1e-9, "iin": 1e-12, "slope2n": 1e3}
+    for name in want:
+        assert np.isfinite(want[name]).all(), name
+        np.testing.assert_allclose(got[name], want[name], rtol=1e-5 if name == "slope2n" else 1e-6,
+                                   atol=atol.get(name, 0.0), err_msg=name)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_streaming_meas_passes(oracle, precision):
     """The device .meas passes (include/espice_lanes.h espl_set_meas) on the
     ring oscillator against the oracle's (oracle/measure.c) over the same
