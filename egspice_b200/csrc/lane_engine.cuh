@@ -21,6 +21,7 @@
 
 #include <cstdint>
 
+#include "lane_gates.cuh"
 #include "lane_meas.cuh"
 #include "lane_models.cuh"
 

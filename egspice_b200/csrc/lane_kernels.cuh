@@ -295,9 +295,7 @@ __device__ __forceinline__ void newton_tile(const TileCtx& c, LaneState* s, cons
             for (uint32_t i = warp; i < d.n; i += nw) {
                 double xi = LM(d.x, i);
                 if (!(fabs(xi) <= lim)) flags |= kImplausible;
-                double scale = fabs(LM(d.a, d.diag[i]));
-                double sc = scale == 0.0 ? 1.0 : scale;
-                double tol = fmax(o.residual_tol, 10.0 * sc * (o.reltol * fabs(xi) + o.vntol));
+                const double tol = residual_gate(o.residual_tol, o.reltol, o.vntol, LM(d.a, d.diag[i]), xi);
                 if (!(fabs(LM(d.rhs, i)) <= tol)) flags |= kResidualMiss;
             }
         }

@@ -441,12 +441,17 @@ static double update_and_norm(const ockt *k, double *x, const double *dx, double
     return bits2d(worst);
 }
 
+/* converger.zig residualGate :340-350 (@max returns the other operand of a
+ * NaN, as fmax does). */
+double orc_residual_gate(double residual_tol, double reltol, double vntol, double diag, double xi) {
+    double scale = fabs(diag);
+    double s = scale == 0 ? 1.0 : scale;
+    return fmax(residual_tol, 10.0 * s * (reltol * fabs(xi) + vntol));
+}
+
 static int residual_ok(const ockt *k, const espl_newton_opts *o, const double *res, const double *x, const double *vals) {
     for (uint32_t i = 0; i < k->n; i++) {
-        double scale = fabs(vals[k->diag[i]]);
-        double s = scale == 0 ? 1.0 : scale;
-        double a = 10.0 * s * (o->reltol * fabs(x[i]) + o->vntol);
-        double tol = o->residual_tol > a ? o->residual_tol : a;
+        double tol = orc_residual_gate(o->residual_tol, o->reltol, o->vntol, vals[k->diag[i]], x[i]);
         if (!(fabs(res[i]) <= tol)) return 0;
     }
     return 1;

@@ -91,6 +91,9 @@ int orc_tran_lanes(const espl_netlist *net, uint32_t lane0, uint32_t count, cons
                    double *x_final, espl_step_report *reports, uint32_t meas_row, double meas_level,
                    double meas_t_start, double *period, uint32_t threads);
 
+/* Newton's residual gate of one row: |F_i| passes when <= this. */
+double orc_residual_gate(double residual_tol, double reltol, double vntol, double diag, double xi);
+
 /* Streaming .meas passes (measure.c, after src/output/scan.zig): one pass's
  * state, fed a sample at a time. */
 typedef struct {
