@@ -559,3 +559,53 @@ def measure_values(measures: Sequence[Measure], value: np.ndarray) -> Dict[str, 
             out[m.name] = value[:, k + len(m.passes) - 1]
         k += len(m.passes)
     return out
+
+
+# The reasons a point has no value, or not all of them (include/espice.h
+# espice_reason :260-284).
+REASON_OK = 0
+REASON_NO_CONVERGENCE = 1
+REASON_TIMESTEP_TOO_SMALL = 2
+REASON_SINGULAR_MATRIX = 3
+REASON_MEASURE_UNRESOLVED = 5
+REASON_OTHER = 255
+
+
+def point_measures(measures: Sequence[Measure], value: np.ndarray, names: Optional[Sequence[str]] = None,
+                   reports: Optional[Sequence] = None, op: Optional[np.ndarray] = None):
+    """Each lane's measures and reason as the reference's points API copies
+    them (include/espice.h espice_copy_point_measures :324-338): values
+    [lanes][len(names)] (names case-insensitive, default every measure in
+    card order) and reasons [lanes]. A failed lane reads NaN throughout: its
+    operating point (`op`, the espl_lane_newton rows [lanes, 4]) did not
+    converge (SINGULAR_MATRIX when it was singular, else NO_CONVERGENCE), or
+    its transient (`reports`, espl_step_report per lane) ended otherwise than
+    done (TIMESTEP_TOO_SMALL on a step underflow, else OTHER). Otherwise NaN
+    marks a measure with no value and the reason is MEASURE_UNRESOLVED."""
+    allv = measure_values(measures, value)
+    keys = {k.lower(): k for k in allv}
+    if names is None:
+        names = list(allv)
+    cols = []
+    for nm in names:
+        if nm.lower() not in keys:
+            raise DeckError(f"UnknownMeasure: no .meas card named {nm!r}")
+        cols.append(allv[keys[nm.lower()]])
+    lanes = value.shape[0]
+    out = np.stack(cols, axis=1) if cols else np.zeros((lanes, 0))
+    reasons = np.zeros(lanes, dtype=np.uint32)
+    failed = np.zeros(lanes, dtype=bool)
+    if op is not None:
+        bits = np.asarray(op)[:, 0]
+        bad = (bits & abi.CONVERGED) == 0
+        reasons[bad] = np.where((bits[bad] & abi.SINGULAR) != 0, REASON_SINGULAR_MATRIX, REASON_NO_CONVERGENCE)
+        failed |= bad
+    if reports is not None:
+        status = np.array([r.status for r in reports], dtype=np.uint32)
+        bad = (status != 1) & ~failed
+        reasons[bad] = np.where(status[bad] == 2, REASON_TIMESTEP_TOO_SMALL, REASON_OTHER)
+        failed |= bad
+    out[failed] = np.nan
+    unresolved = ~failed & np.isnan(out).any(axis=1)
+    reasons[unresolved] = REASON_MEASURE_UNRESOLVED
+    return out, reasons

@@ -102,3 +102,31 @@ def test_too_many_passes_are_refused():
     ms = read_measures(text, net, params={"rval": r})
     with pytest.raises(DeckError, match="a template takes 16"):
         measure_passes(ms)
+
+
+def test_point_measures_and_reasons():
+    """espice_copy_point_measures' rules (include/espice.h :324-338): a
+    failed point reads NaN throughout with the first failure's reason; a
+    point with a measure that never resolved reads NaN there and names it."""
+    from types import SimpleNamespace as R
+
+    from egspice_b200 import netlist as nl
+    net, r = _rc()
+    ms = read_measures(RC_DECK, net, params={"rval": r})
+    lanes, n_pass = 5, len(measure_passes(ms))
+    value = np.arange(lanes * n_pass, dtype=np.float64).reshape(lanes, n_pass) + 1.0
+    value[3, 0] = np.nan                              # t50 never happened on lane 3
+    reports = [R(status=1), R(status=2), R(status=1), R(status=1), R(status=4)]
+    op = np.zeros((lanes, 4), dtype=np.uint32)
+    op[:, 0] = abi.CONVERGED
+    op[2, 0] = abi.SINGULAR                           # lane 2's operating point failed
+    out, reasons = nl.point_measures(ms, value, ["T50", "swing"], reports=reports, op=op)
+    assert out.shape == (lanes, 2)
+    assert list(reasons) == [nl.REASON_OK, nl.REASON_TIMESTEP_TOO_SMALL, nl.REASON_SINGULAR_MATRIX,
+                             nl.REASON_MEASURE_UNRESOLVED, nl.REASON_OTHER]
+    swing = measure_passes(ms).index(ms[6].passes[0])
+    assert out[0, 0] == value[0, 0] and out[0, 1] == value[0, swing] - value[0, swing + 1]
+    assert np.isnan(out[1:3]).all() and np.isnan(out[4]).all()
+    assert np.isnan(out[3, 0]) and not np.isnan(out[3, 1])
+    with pytest.raises(DeckError, match="UnknownMeasure"):
+        nl.point_measures(ms, value, ["nope"])
