@@ -1,0 +1,166 @@
+"""The reference's points API (include/espice.h :244-362:
+espice_append_points, espice_copy_point_measures, espice_release_points,
+espice_lane_width) over the GPU lanes: one SPICE deck as a template, run at
+many rows of its live parameters, each row a point whose `.meas tran`
+measures and reason are copied back by query id.
+
+Points run as lanes of one template per batch (at most `lane_width()` lanes,
+the reference's GPU lane cap), in the order they were appended; a point's
+measures depend only on the deck and its values up to the lanes' numerics,
+not on which batch carried it. The deck's `.tran tstep tstop [tstart [tmax]]`
+card sets the transient (tstart must be 0: the lanes record from t = 0);
+every point has one query, its transient, so point k of an append has id
+first_id + k. Errors raise PointsError carrying the reference's status code
+and diagnostic name."""
+from __future__ import annotations
+
+from typing import Dict, List, Mapping, Optional, Sequence
+
+import numpy as np
+
+from . import abi
+from .netlist import (DeckError, _logical_lines, _split, measure_passes, parse_number, point_measures,
+                      read_deck, read_measures)
+
+# espice_status (include/espice.h :33-37)
+OK, INVALID_ARGUMENT, INVALID_QUERY, RESULT_UNAVAILABLE, FAILED = 0, 1, 4, 5, 6
+# espice_reason (include/espice.h :260-284) for a point refused as appended
+REASON_INVALID_PARAMETER = 9
+LANE_WIDTH = 16384  # espice_lane_width under GPU lanes
+
+
+class PointsError(RuntimeError):
+    def __init__(self, status: int, name: str):
+        super().__init__(f"{name} (status {status})")
+        self.status, self.name = status, name
+
+
+def _tran_card(text: str):
+    """(tstep, tstop, tmax) of the deck's one .tran card."""
+    found = None
+    for ln, card in _logical_lines(text):
+        toks = _split(card)
+        if toks[0] in (".step", ".data", ".alter"):
+            raise PointsError(INVALID_ARGUMENT, "SweptTemplate")
+        if toks[0] != ".tran":
+            continue
+        if found is not None:
+            raise DeckError(f"line {ln}: a second .tran card")
+        nums = [t for t in toks[1:] if t != "uic"]
+        if "uic" in toks[1:]:
+            raise DeckError(f"line {ln}: UIC is refused on the lanes (as the reference's GPU lanes do)")
+        vals = [parse_number(t) for t in nums]
+        if len(vals) < 2 or any(v is None for v in vals):
+            raise DeckError(f"line {ln}: .tran needs tstep and tstop as numbers")
+        if len(vals) > 2 and vals[2] != 0:
+            raise DeckError(f"line {ln}: a nonzero tstart is outside what the lanes carry")
+        tmax = vals[3] if len(vals) > 3 else None
+        found = (vals[0], vals[1], tmax)
+    if found is None:
+        raise DeckError("the deck has no .tran card; the points run transients")
+    return found
+
+
+class Points:
+    """A deck `text` as a points template over `live_params` (names of the
+    deck's parameters each point gives values for; the others keep their
+    .param values). `precision` as Lanes takes it; `tran` overrides fields
+    of the transient options (abi.tran_opts keywords). TMAX defaults to
+    ngspice's min(TSTEP, TSTOP / 50). A measure may read parameters, but no
+    live one: a template's measure passes are the same on every lane."""
+
+    def __init__(self, text: str, live_params: Sequence[str], precision: str = "fp64",
+                 tran: Optional[Mapping[str, float]] = None):
+        self.text = text
+        self.live = [p.lower() for p in live_params]
+        self.precision = precision
+        tstep, tstop, tmax = _tran_card(text)
+        kw = dict(t_stop=tstop, dt=tstep, dt_max=tmax if tmax else min(tstep, tstop / 50))
+        kw.update(tran or {})
+        self.topts = abi.tran_opts(**kw)
+        # the measures are read once on a two-lane instance of the template
+        # whose live values differ, so a card that names no vector, or reads
+        # a live parameter, fails here
+        probe_params = {p: np.array([0.0, 1.0]) for p in self.live}
+        probe = read_deck(text, lanes=2, params=probe_params)
+        self.measures = read_measures(text, probe, params=probe_params)
+        measure_passes(self.measures)
+        self.rows: List[np.ndarray] = []     # each point's values
+        self.state: List[int] = []           # 0 pending, 1 complete, 2 released
+        self.values: Dict[int, np.ndarray] = {}
+        self.reasons: Dict[int, int] = {}
+
+    @staticmethod
+    def lane_width() -> int:
+        return LANE_WIDTH
+
+    def append_points(self, values) -> int:
+        """Appends count points (values [count][len(live_params)]); returns
+        point 0's query id. A point with a non-finite value is appended
+        already failed (INVALID_PARAMETER)."""
+        if not self.live:
+            raise PointsError(INVALID_ARGUMENT, "NoLiveParameters")
+        v = np.asarray(values, dtype=np.float64)
+        if v.ndim != 2 or v.shape[0] == 0 or v.shape[1] != len(self.live):
+            raise PointsError(INVALID_ARGUMENT, "InvalidArgument")
+        first = len(self.rows)
+        for row in v:
+            self.rows.append(row.copy())
+            if np.isfinite(row).all():
+                self.state.append(0)
+            else:
+                k = len(self.rows) - 1
+                self.state.append(1)
+                self.values[k] = np.full(len(self.measures), np.nan)
+                self.reasons[k] = REASON_INVALID_PARAMETER
+        return first
+
+    def run(self) -> None:
+        """Runs every pending point on the GPU lanes, lane_width() at a time."""
+        from .lanes import Lanes
+        pending = [k for k, s in enumerate(self.state) if s == 0]
+        names = [m.name for m in self.measures]
+        for b0 in range(0, len(pending), LANE_WIDTH):
+            ids = pending[b0:b0 + LANE_WIDTH]
+            block = np.stack([self.rows[k] for k in ids])
+            params = {p: block[:, j] for j, p in enumerate(self.live)}
+            net = read_deck(self.text, lanes=len(ids), params=params)
+            ms = read_measures(self.text, net, params=params)
+            with Lanes([net], precision=self.precision) as L:
+                L.set_meas(0, measure_passes(ms))
+                reps = L.run_tran(self.topts, steps_per_launch=2048)
+                value, _ = L.get_meas(0)
+            out, reasons = point_measures(ms, value, names, reports=reps)
+            for i, k in enumerate(ids):
+                self.values[k] = out[i]
+                self.reasons[k] = int(reasons[i])
+                self.state[k] = 1
+
+    def copy_point_measures(self, first_id: int, count: int, names: Sequence[str]):
+        """(values [count][len(names)], reasons [count]) of the points from
+        first_id; names case-insensitive."""
+        if count < 1 or first_id < 0 or first_id + count > len(self.rows):
+            raise PointsError(INVALID_QUERY, "InvalidQuery")
+        keys = {m.name.lower(): j for j, m in enumerate(self.measures)}
+        cols = []
+        for nm in names:
+            if nm.lower() not in keys:
+                raise PointsError(INVALID_ARGUMENT, "UnknownMeasure")
+            cols.append(keys[nm.lower()])
+        ids = range(first_id, first_id + count)
+        if any(self.state[k] != 1 for k in ids):
+            raise PointsError(RESULT_UNAVAILABLE, "ResultUnavailable")
+        out = np.stack([self.values[k][cols] for k in ids])
+        reasons = np.array([self.reasons[k] for k in ids], dtype=np.uint32)
+        return out, reasons
+
+    def release_points(self, first_id: int, count: int) -> None:
+        """Frees the results of count points from first_id; copying them
+        afterwards is RESULT_UNAVAILABLE."""
+        if count < 1 or first_id < 0 or first_id + count > len(self.rows):
+            raise PointsError(INVALID_QUERY, "InvalidQuery")
+        for k in range(first_id, first_id + count):
+            if self.state[k] == 1:
+                self.state[k] = 2
+                self.values.pop(k, None)
+                self.reasons.pop(k, None)

@@ -391,3 +391,51 @@ def test_ac_lanes(oracle):
     ho = oracle.ac_lanes(net, x, 1, om, [out])
     assert np.isfinite(h).all()
     np.testing.assert_allclose(h, ho, rtol=1e-8, atol=1e-12 * np.abs(ho).max())
+
+
+def test_points_api(oracle):
+    """The points mirror (egspice_b200/points.py, include/espice.h :244-362)
+    on the lanes: 100 RC points appended in two calls and run as one batch,
+    copied by id against the oracle's transient of the same values; the same
+    rows appended in the reverse order give the same measures (a point's
+    measures depend on its values, not its batch); a non-finite row comes
+    back failed."""
+    from egspice_b200 import points as pt
+    from egspice_b200.netlist import measure_passes, measure_values, read_deck, read_measures
+    deck = """RC points
+vin in 0 dc 0 pulse(0 1 0 0.2n 0.2n 1 2)
+r1 in out {rval}
+c1 out 0 {cval}
+.param rval=1k cval=1p
+.tran 1p 6n
+.meas tran t50 when v(out)=0.5
+.meas tran v2n find v(out) at=2n
+.meas tran rise trig v(out) val=0.1 rise=1 targ v(out) val=0.9 rise=1
+.end
+"""
+    rng = np.random.default_rng(11)
+    rows = np.stack([rng.uniform(0.5e3, 1.5e3, 100), rng.uniform(0.5e-12, 1.5e-12, 100)], axis=1)
+    p = pt.Points(deck, ["rval", "cval"])
+    a0 = p.append_points(rows[:60])
+    a1 = p.append_points(rows[60:])
+    bad = p.append_points([[1e3, np.inf]])
+    assert (a0, a1, bad) == (0, 60, 100)
+    p.run()
+    names = ["t50", "v2n", "rise"]
+    v, r = p.copy_point_measures(0, 100, names)
+    assert (r == 0).all()
+    vb, rb = p.copy_point_measures(bad, 1, names)
+    assert np.isnan(vb).all() and rb[0] == pt.REASON_INVALID_PARAMETER
+    params = {"rval": rows[:, 0], "cval": rows[:, 1]}
+    net = read_deck(deck, lanes=100, params=params)
+    ms = read_measures(deck, net, params=params)
+    vo, _, _, ro = oracle.tran_meas(net, p.topts, measure_passes(ms), threads=8)
+    want = measure_values(ms, vo)
+    for j, name in enumerate(names):
+        np.testing.assert_allclose(v[:, j], want[name], rtol=1e-6, atol=1e-9 if name == "v2n" else 0.0,
+                                   err_msg=name)
+    q = pt.Points(deck, ["rval", "cval"])
+    q.append_points(rows[::-1])
+    q.run()
+    vr, _ = q.copy_point_measures(0, 100, names)
+    np.testing.assert_allclose(vr[::-1], v, rtol=1e-9, atol=1e-15)
