@@ -241,6 +241,77 @@ def _kv(tokens: Sequence[str], where: str) -> Dict[str, str]:
     return out
 
 
+_NODE_TOKENS = {"r": 2, "c": 2, "d": 2, "v": 2, "i": 2, "m": 4}
+
+
+def _expand_subckts(cards: List[tuple]) -> List[tuple]:
+    """Flattens `.subckt name ports ... .ends` definitions and their `x`
+    instances (nested to any depth): an instance's cards get its ports for
+    the definition's port names, `inst.node` for the definition's own nodes
+    (ngspice's naming, so v(x1.y) reads an internal node) and `head.inst`
+    for element names; the ground stays global. Subcircuit parameters are
+    outside what the lanes carry."""
+    defs: Dict[str, tuple] = {}
+    top: List[tuple] = []
+    stack: List[list] = []
+    for ln, card in cards:
+        toks = _split(card)
+        if toks[0] == ".subckt":
+            if len(toks) < 2:
+                raise DeckError(f"line {ln}: .subckt needs a name")
+            if any("=" in t or t == "params:" for t in toks[2:]):
+                raise DeckError(f"line {ln}: subcircuit parameters are outside what the lanes carry")
+            stack.append([toks[1], toks[2:], [], ln])
+        elif toks[0] == ".ends":
+            if not stack:
+                raise DeckError(f"line {ln}: .ends without .subckt")
+            name, ports, body, _ = stack.pop()
+            defs[name] = (ports, body)
+        elif stack:
+            stack[-1][2].append((ln, card))
+        else:
+            top.append((ln, card))
+    if stack:
+        raise DeckError(f"line {stack[-1][3]}: .subckt {stack[-1][0]} has no .ends")
+
+    def expand(body: List[tuple], inst: str, nodes: Dict[str, str], depth: int) -> List[tuple]:
+        if depth > 32:
+            raise DeckError("subcircuits nest deeper than 32 (a recursive definition?)")
+        out: List[tuple] = []
+        for ln, card in body:
+            toks = _split(card)
+            head = toks[0]
+            rename = (lambda t: t if t in ("0", "gnd") else nodes.get(t, f"{inst}.{t}")) if inst else (lambda t: t)
+            if head.startswith("."):
+                if inst:
+                    raise DeckError(f"line {ln}: the card {head} inside a subcircuit is outside what the lanes carry")
+                out.append((ln, card))
+                continue
+            if head[0] == "x":
+                args = [t for t in toks[1:] if "=" not in t]
+                if len(args) < 1 or len(args) < len(toks) - 1:
+                    raise DeckError(f"line {ln}: instance parameters of a subcircuit are outside what the lanes carry")
+                sub = args[-1]
+                if sub not in defs:
+                    raise DeckError(f"line {ln}: unknown subcircuit {sub!r}")
+                ports, sbody = defs[sub]
+                conn = [rename(t) for t in args[:-1]]
+                if len(conn) != len(ports):
+                    raise DeckError(f"line {ln}: {sub} takes {len(ports)} nodes, given {len(conn)}")
+                path = f"{inst}.{head}" if inst else head  # x1.x2: x2 inside x1
+                out += expand(sbody, path, dict(zip(ports, conn)), depth + 1)
+                continue
+            k = _NODE_TOKENS.get(head[0])
+            if k is None or not inst:
+                out.append((ln, card))
+                continue
+            toks = [f"{head}.{inst}"] + [rename(t) for t in toks[1:1 + k]] + toks[1 + k:]
+            out.append((ln, " ".join(toks)))
+        return out
+
+    return expand(top, "", {}, 0) if defs or any(_split(c)[0][0] == "x" for _, c in top) else top
+
+
 def _read_params(cards: Sequence[tuple], env: _Env) -> None:
     """The .param cards into `env`, values given by the caller kept."""
     for ln, card in cards:
@@ -260,7 +331,7 @@ def read_deck(text: str, lanes: int = 1, params: Optional[Mapping[str, Value]] =
         raise DeckError("a deck needs at least one lane")
     params = dict(params or {})
     env = _Env(lanes, params)
-    cards = _logical_lines(text)
+    cards = _expand_subckts(_logical_lines(text))
     title = text.splitlines()[0].strip() if text.strip() else "deck"
     _read_params(cards, env)
     # .model next (SPICE cards are order-free)
@@ -520,7 +591,7 @@ def read_measures(text: str, net: Netlist, params: Optional[Mapping[str, Value]]
     i(vsource); values are numbers or parameters the same on every lane.
     Anything else raises DeckError naming the line."""
     env = _Env(net.lanes, dict(params or {}))
-    cards = _logical_lines(text)
+    cards = _expand_subckts(_logical_lines(text))
     _read_params(cards, env)
     out: List[Measure] = []
     for ln, card in cards:

@@ -92,3 +92,51 @@ def test_monte_carlo_inverter_chain_matches_the_generator():
 def test_cards_outside_the_subset_are_refused(card, msg):
     with pytest.raises(DeckError, match=msg):
         read_deck("title\nv0 a 0 1\n" + card + "\n.end\n")
+
+
+def test_subcircuits_flatten_to_the_flat_deck():
+    """`.subckt` definitions (nested) and `x` instances expand to the same
+    netlist as the deck written out flat, internal nodes named inst.node as
+    ngspice names them."""
+    models = ".model nx nmos level=1 vto=0.4 kp=150u\n.model px pmos level=1 vto=-0.4 kp=60u\n"
+    sub = """subckt chain
+vdd vdd 0 1.8
+vin a0 0 dc 0.3
+.subckt inv in out sup
+mn out in 0 0 nx w=1u l=0.2u
+mp out in sup sup px w=2u l=0.2u
+.ends
+.subckt buf in out sup
+x1 in mid sup inv
+x2 mid out sup inv
+cl mid 0 2f
+.ends
+xa a0 a1 vdd buf
+xb a1 a2 vdd buf
+r1 a2 0 10k
+""" + models + ".end\n"
+    flat = """flat chain
+vdd vdd 0 1.8
+vin a0 0 dc 0.3
+""" + "".join(f"mn.{x} {o} {i} 0 0 nx w=1u l=0.2u\nmp.{x} {o} {i} vdd vdd px w=2u l=0.2u\n"
+              for x, i, o in (("xa.x1", "a0", "xa.mid"), ("xa.x2", "xa.mid", "a1"),
+                              ("xb.x1", "a1", "xb.mid"), ("xb.x2", "xb.mid", "a2"))) + """cl.xa xa.mid 0 2f
+cl.xb xb.mid 0 2f
+r1 a2 0 10k
+""" + models + ".end\n"
+    a, b = read_deck(sub, lanes=3), read_deck(flat, lanes=3)
+    _same(a, b)
+    assert a.node_names == b.node_names and "xa.mid" in a.node_names
+
+
+@pytest.mark.parametrize("card,msg", [
+    (".subckt s a b\nr1 a b 1k\n", "no .ends"),
+    (".subckt s a b\nr1 a b 1k\n.ends\nx1 a s", "takes 2 nodes"),
+    (".subckt s a b\nr1 a b 1k\n.ends\nx1 a 0 s w=1", "instance parameters"),
+    (".subckt s a b params: w=1\nr1 a b 1k\n.ends", "subcircuit parameters"),
+    ("x1 a 0 nosuch", "unknown subcircuit"),
+    (".subckt s a b\nx1 a b s\n.ends\nx1 a 0 s", "deeper than 32"),
+])
+def test_subcircuit_errors(card, msg):
+    with pytest.raises(DeckError, match=msg):
+        read_deck("title\nv0 a 0 1\n" + card + "\n.end\n")
