@@ -19,12 +19,14 @@ from typing import Dict, List, Mapping, Optional, Sequence
 import numpy as np
 
 from . import abi
+from .decks import RES
 from .netlist import (DeckError, _logical_lines, _split, measure_passes, parse_number, point_measures,
                       read_deck, read_measures)
 
 # espice_status (include/espice.h :33-37)
 OK, INVALID_ARGUMENT, INVALID_QUERY, RESULT_UNAVAILABLE, FAILED = 0, 1, 4, 5, 6
 # espice_reason (include/espice.h :260-284) for a point refused as appended
+REASON_TOPOLOGY_CHANGED = 8
 REASON_INVALID_PARAMETER = 9
 LANE_WIDTH = 16384  # espice_lane_width under GPU lanes
 
@@ -97,22 +99,33 @@ class Points:
     def append_points(self, values) -> int:
         """Appends count points (values [count][len(live_params)]); returns
         point 0's query id. A point with a non-finite value is appended
-        already failed (INVALID_PARAMETER)."""
+        already failed (INVALID_PARAMETER), as is one whose values short a
+        resistor (TOPOLOGY_CHANGED: a zero resistance collapses two nodes,
+        which the template's pattern cannot)."""
         if not self.live:
             raise PointsError(INVALID_ARGUMENT, "NoLiveParameters")
         v = np.asarray(values, dtype=np.float64)
         if v.ndim != 2 or v.shape[0] == 0 or v.shape[1] != len(self.live):
             raise PointsError(INVALID_ARGUMENT, "InvalidArgument")
         first = len(self.rows)
-        for row in v:
+        finite = np.isfinite(v).all(axis=1)
+        shorted = np.zeros(len(v), dtype=bool)
+        if finite.any():
+            net = read_deck(self.text, lanes=len(v), params={p: np.where(finite, v[:, j], 1.0)
+                                                             for j, p in enumerate(self.live)})
+            for b in net.batches:
+                if b.kind == RES:
+                    shorted |= (b.param[:, 0, :] == 0).any(axis=0)
+        for i, row in enumerate(v):
             self.rows.append(row.copy())
-            if np.isfinite(row).all():
+            reason = REASON_INVALID_PARAMETER if not finite[i] else REASON_TOPOLOGY_CHANGED if shorted[i] else None
+            if reason is None:
                 self.state.append(0)
             else:
                 k = len(self.rows) - 1
                 self.state.append(1)
                 self.values[k] = np.full(len(self.measures), np.nan)
-                self.reasons[k] = REASON_INVALID_PARAMETER
+                self.reasons[k] = reason
         return first
 
     def run(self) -> None:

@@ -439,3 +439,51 @@ c1 out 0 {cval}
     q.run()
     vr, _ = q.copy_point_measures(0, 100, names)
     np.testing.assert_allclose(vr[::-1], v, rtol=1e-9, atol=1e-15)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_chain_fixture_points_in_three_orders(oracle, precision):
+    """The reference's lane lockstep fixture (tests/golden/chain_deck.json,
+    from src/tests/espice.zig:3072-3122) as points on the lanes, appended in
+    the identity, reversed and a shuffled order: each row's TRIG/TARG
+    measures and reason are the same in every order and match the oracle's
+    transient of the row; the extreme wire is unresolved, the shorted wire
+    refused as a topology change."""
+    import json
+    import os
+
+    from egspice_b200 import points as pt
+    from egspice_b200.netlist import measure_passes, measure_values, read_deck, read_measures
+    fx = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "chain_deck.json")))
+    rows, live, deck = np.array(fx["rows"]), fx["live"], fx["deck"]
+    names = ["tpd", "trise", "tfall"]
+    k = len(rows)
+    orders = [np.arange(k), np.arange(k)[::-1], np.random.default_rng(207).permutation(k)]
+    runs = []
+    for order in orders:
+        p = pt.Points(deck, live, precision=precision)
+        p.append_points(rows[order])
+        p.run()
+        v, r = p.copy_point_measures(0, k, names)
+        back = np.empty_like(v)
+        back[order] = v
+        rb = np.empty_like(r)
+        rb[order] = r
+        runs.append((back, rb))
+    # FP64 lanes: roundoff apart (each batch's tape comes from its lead
+    # lane); mixed lanes: within the FP32 factors' reach of the 1e-6 bar
+    for v, r in runs[1:]:
+        np.testing.assert_array_equal(r, runs[0][1])
+        np.testing.assert_allclose(v, runs[0][0], rtol=1e-9 if precision == "fp64" else 2e-6, atol=0)
+    v, r = runs[0]
+    assert list(r[:17]) == [0] * 17
+    assert r[17] == 5 and r[18] == pt.REASON_TOPOLOGY_CHANGED  # MEASURE_UNRESOLVED, refused
+    ok = rows[:18]
+    params = {name: ok[:, j] for j, name in enumerate(live)}
+    net = read_deck(deck, lanes=len(ok), params=params)
+    ms = read_measures(deck, net, params=params)
+    vo, _, _, _ = oracle.tran_meas(net, pt.Points(deck, live).topts, measure_passes(ms), threads=8)
+    want = measure_values(ms, vo)
+    for j, name in enumerate(names):
+        np.testing.assert_allclose(v[:17, j], want[name][:17], rtol=1e-6, err_msg=name)
+        assert np.isnan(v[17, j]) and np.isnan(want[name][17])
