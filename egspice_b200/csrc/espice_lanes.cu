@@ -1505,6 +1505,19 @@ espl_status espl_ac(espl_lanes* h, uint32_t net, uint32_t vsrc, const double* om
     if (vsrc >= vk.count) return fail(h, ESPL_INVALID_ARGUMENT, "no such voltage source");
     const uint32_t exc = vk.term[3 * vsrc + 2];
     if (exc >= g.n) return fail(h, ESPL_INVALID_ARGUMENT, "the source has no branch row");
+    // a unit AC voltage on the source: b = e_branch
+    std::vector<double> br(g.n, 0.0), bi(g.n, 0.0);
+    br[exc] = 1.0;
+    return espl_ac_solve(h, net, omega, n_freq, br.data(), bi.data(), 1, 0, rows, n_rows, out_re, out_im);
+}
+
+espl_status espl_ac_solve(espl_lanes* h, uint32_t net, const double* omega, uint32_t n_freq, const double* rhs_re,
+                          const double* rhs_im, uint32_t n_rhs, uint32_t adjoint, const uint32_t* rows,
+                          uint32_t n_rows, double* out_re, double* out_im) {
+    if (!h || net >= h->groups.size() || !omega || !n_freq || !rhs_re || !rhs_im || !n_rhs || adjoint > 1 || !rows ||
+        !n_rows || !out_re || !out_im)
+        return ESPL_INVALID_ARGUMENT;
+    Group& g = h->groups[net];
     for (uint32_t k = 0; k < n_rows; k++)
         if (rows[k] >= g.n) return fail(h, ESPL_INVALID_ARGUMENT, "AC row out of range");
     for (uint32_t f = 0; f < n_freq; f++)
@@ -1554,8 +1567,13 @@ espl_status espl_ac(espl_lanes* h, uint32_t net, uint32_t vsrc, const double* om
         (s = dupload(h, own, &uup, t.up)) || (s = dupload(h, own, &uui, t.ui)) ||
         (s = dupload(h, own, &urows, std::vector<uint32_t>(rows, rows + n_rows))))
         return release(), s;
-    const double* uom;
-    if ((s = dupload(h, own, &uom, std::vector<double>(omega, omega + n_freq)))) return release(), s;
+    const double *uom, *ubr, *ubi;
+    if ((s = dupload(h, own, &uom, std::vector<double>(omega, omega + n_freq))) ||
+        (s = dupload(h, own, &ubr, std::vector<double>(rhs_re, rhs_re + (size_t)n_rhs * n))) ||
+        (s = dupload(h, own, &ubi, std::vector<double>(rhs_im, rhs_im + (size_t)n_rhs * n))))
+        return release(), s;
+    A.b_re = ubr;
+    A.b_im = ubi;
     A.q = uq;
     A.qinv = uqinv;
     A.pinv = upinv;
@@ -1569,7 +1587,8 @@ espl_status espl_ac(espl_lanes* h, uint32_t net, uint32_t vsrc, const double* om
     A.nnz_u = (uint32_t)t.ui.size();
     A.n_freq = n_freq;
     A.n_rows = n_rows;
-    A.exc_row = exc;
+    A.n_rhs = n_rhs;
+    A.adjoint = adjoint;
     A.omega = uom;
     A.rows = urows;
     A.g = gpl;
@@ -1579,11 +1598,12 @@ espl_status espl_ac(espl_lanes* h, uint32_t net, uint32_t vsrc, const double* om
         (s = dalloc(h, own, &A.wr, n * P)) || (s = dalloc(h, own, &A.wi, n * P)) || (s = dalloc(h, own, &A.lr, nl * P)) ||
         (s = dalloc(h, own, &A.li_, nl * P)) || (s = dalloc(h, own, &A.ur, nu * P)) ||
         (s = dalloc(h, own, &A.ui_, nu * P)) || (s = dalloc(h, own, &A.dr, n * P)) || (s = dalloc(h, own, &A.di, n * P)) ||
-        (s = dalloc(h, own, &A.out_re, P * n_freq * n_rows)) || (s = dalloc(h, own, &A.out_im, P * n_freq * n_rows)))
+        (s = dalloc(h, own, &A.out_re, P * n_freq * n_rhs * n_rows)) ||
+        (s = dalloc(h, own, &A.out_im, P * n_freq * n_rhs * n_rows)))
         return release(), s;
     k_ac<<<(uint32_t)tl.size(), kBlock, 0, h->stream>>>(m, A);
     CK(cudaGetLastError());
-    const size_t per = (size_t)n_freq * n_rows;
+    const size_t per = (size_t)n_freq * n_rhs * n_rows;
     CK(cudaMemcpyAsync(out_re, A.out_re, sizeof(double) * per * g.lanes, cudaMemcpyDeviceToHost, h->stream));
     CK(cudaMemcpyAsync(out_im, A.out_im, sizeof(double) * per * g.lanes, cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));

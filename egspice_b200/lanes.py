@@ -62,6 +62,9 @@ def lib():
         L.espl_get_stats.restype = C.c_uint32
         L.espl_ac.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, f64p, C.c_uint32, u32p, C.c_uint32, f64p, f64p]
         L.espl_ac.restype = C.c_uint32
+        L.espl_ac_solve.argtypes = [C.c_void_p, C.c_uint32, f64p, C.c_uint32, f64p, f64p, C.c_uint32, C.c_uint32,
+                                    u32p, C.c_uint32, f64p, f64p]
+        L.espl_ac_solve.restype = C.c_uint32
         L.espl_solve_op.argtypes = [C.c_void_p, C.POINTER(NewtonOpts), C.POINTER(LaneNewton)]
         L.espl_solve_op.restype = C.c_uint32
         L.espl_set_meas.argtypes = [C.c_void_p, C.c_uint32, C.POINTER(MeasPass), C.c_uint32]
@@ -156,6 +159,23 @@ class Lanes:
         im = np.zeros((lanes, len(om), len(rw)))
         self._check(lib().espl_ac(self.h, net, vsrc, om.ctypes.data_as(f64p), len(om), rw.ctypes.data_as(u32p), len(rw),
                                   re.ctypes.data_as(f64p), im.ctypes.data_as(f64p)), "espl_ac")
+        return re + 1j * im
+
+    def ac_solve(self, net: int, omega, rhs, rows, adjoint: bool = False) -> np.ndarray:
+        """(G + j omega C) x = b for each row b of `rhs` (complex [n_rhs, n],
+        the same on every lane), or the transpose system when `adjoint`:
+        complex [lanes, len(omega), n_rhs, len(rows)]."""
+        om = np.ascontiguousarray(omega, dtype=np.float64)
+        rw = np.ascontiguousarray(rows, dtype=np.uint32)
+        b = np.atleast_2d(np.asarray(rhs, dtype=complex))
+        br = np.ascontiguousarray(b.real)
+        bi = np.ascontiguousarray(b.imag)
+        lanes = self.nets[net].lanes
+        re = np.zeros((lanes, len(om), len(b), len(rw)))
+        im = np.zeros((lanes, len(om), len(b), len(rw)))
+        self._check(lib().espl_ac_solve(self.h, net, om.ctypes.data_as(f64p), len(om), br.ctypes.data_as(f64p),
+                                        bi.ctypes.data_as(f64p), len(b), int(adjoint), rw.ctypes.data_as(u32p),
+                                        len(rw), re.ctypes.data_as(f64p), im.ctypes.data_as(f64p)), "espl_ac_solve")
         return re + 1j * im
 
     def init_steps(self, topts: TranOpts):

@@ -199,6 +199,16 @@ espl_status espl_solve_op(espl_lanes *h, const espl_newton_opts *opts, espl_lane
  * state seeded at x. */
 espl_status espl_ac(espl_lanes *h, uint32_t net, uint32_t vsrc, const double *omega, uint32_t n_freq,
                     const uint32_t *rows, uint32_t n_rows, double *out_re, double *out_im);
+/* The same lanes and tape for any right-hand sides: rhs_re/rhs_im[e][n]
+ * (n_rhs of them, the same on every lane), solved as (G + j omega C) x = b,
+ * or with adjoint = 1 as the transpose (G + j omega C)^T z = b (the adjoint
+ * solves of noise analysis: z[u] is the transfer from a current injected at
+ * unknown u to the output b selects). Out: out_re/out_im[lane][freq][e][k]
+ * = the solution's unknown rows[k]. espl_ac is this with b = the source's
+ * branch row. */
+espl_status espl_ac_solve(espl_lanes *h, uint32_t net, const double *omega, uint32_t n_freq, const double *rhs_re,
+                          const double *rhs_im, uint32_t n_rhs, uint32_t adjoint, const uint32_t *rows,
+                          uint32_t n_rows, double *out_re, double *out_im);
 
 /* Transient lanes with device step control (`initSteps` lanes.zig:1827,
  * `deviceLaunch` :1917; the step machine `stepBegin/stepEndA/stepEndB`,

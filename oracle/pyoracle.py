@@ -262,6 +262,34 @@ def ac_lanes(net: Netlist, x: np.ndarray, vsrc: int, omega, rows) -> np.ndarray:
     return out
 
 
+def ac_solve_lanes(net: Netlist, x: np.ndarray, omega, rhs, rows, adjoint: bool = False) -> np.ndarray:
+    """(G + j omega C) z = b, or its transpose when `adjoint`, for each row b
+    of `rhs` (complex [n_rhs, n]) on every lane at its operating point x,
+    G and C from the oracle's device models, solved densely (numpy).
+    Complex [lanes, len(omega), n_rhs, len(rows)]."""
+    cn = CNet(net)
+    n, nnz = net.n, len(net.row_idx)
+    cp = np.asarray(net.col_ptr, dtype=np.int64)
+    ri = np.asarray(net.row_idx, dtype=np.int64)
+    cols = np.repeat(np.arange(n), np.diff(cp))
+    b = np.atleast_2d(np.asarray(rhs, dtype=complex))
+    out = np.zeros((net.lanes, len(omega), len(b), len(rows)), dtype=complex)
+    g = np.zeros(nnz)
+    c = np.zeros(nnz)
+    for l in range(net.lanes):
+        xl = np.ascontiguousarray(x[l], dtype=np.float64)
+        assert lib().orc_planes(C.byref(cn.c), l, xl.ctypes.data_as(f64p), g.ctypes.data_as(f64p),
+                                c.ctypes.data_as(f64p)) == 0
+        G = np.zeros((n, n))
+        Cm = np.zeros((n, n))
+        np.add.at(G, (ri, cols), g)
+        np.add.at(Cm, (ri, cols), c)
+        for f, w in enumerate(omega):
+            Y = G + 1j * w * Cm
+            out[l, f] = np.linalg.solve(Y.T if adjoint else Y, b.T).T[:, list(rows)]
+    return out
+
+
 def tran_lanes(net: Netlist, opts: TranOpts, lane0: int = 0, count: Optional[int] = None,
                probes: Sequence[int] = (), max_rows: int = 0, meas: Optional[Tuple[int, float, float]] = None,
                threads: int = 1):

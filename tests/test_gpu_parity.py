@@ -393,6 +393,39 @@ def test_ac_lanes(oracle):
     np.testing.assert_allclose(h, ho, rtol=1e-8, atol=1e-12 * np.abs(ho).max())
 
 
+def test_ac_solve_lists_and_adjoints(oracle):
+    """espl_ac_solve on the op-amp's 64 lanes at their warm operating
+    points: two right-hand sides (the output node, the input source's branch
+    row), forward and adjoint (transpose) solves against the oracle's dense
+    solves; espl_ac is the forward solve of the branch row, and the two
+    modes agree by reciprocity (z[branch] of the adjoint of e_out is x[out]
+    of the forward of e_branch)."""
+    net = decks.miller_opamp(64)
+    om = np.logspace(2, 10, 9)
+    out = net.node("out")
+    branch = int([b for b in net.batches if b.kind == decks.VSRC][0].term[1, 2])
+    n = net.n
+    rhs = np.zeros((2, n), dtype=complex)
+    rhs[0, out] = 1.0
+    rhs[1, branch] = 1.0
+    rows = np.arange(n)
+    with Lanes([net]) as L:
+        L.put_x(0, opamp_start(net), False)
+        res = L.solve_static(abi.newton_opts(init_fix=0))
+        x = L.get_x(0)
+        fwd = L.ac_solve(0, om, rhs, rows)
+        adj = L.ac_solve(0, om, rhs, rows, adjoint=True)
+        h = L.ac(0, 1, om, rows)
+    assert ((res[:, 0] & abi.CONVERGED) != 0).all()
+    assert np.isfinite(fwd).all() and np.isfinite(adj).all()
+    np.testing.assert_array_equal(h, fwd[:, :, 1])
+    for got, adjoint in ((fwd, False), (adj, True)):
+        want = oracle.ac_solve_lanes(net, x, om, rhs, rows, adjoint=adjoint)
+        scale = np.abs(want).max(axis=3, keepdims=True)
+        assert (np.abs(got - want) <= 1e-8 * np.abs(want) + 1e-12 * scale).all(), adjoint
+    np.testing.assert_allclose(adj[:, :, 0, branch], fwd[:, :, 1, out], rtol=1e-9)
+
+
 def test_points_api(oracle):
     """The points mirror (egspice_b200/points.py, include/espice.h :244-362)
     on the lanes: 100 RC points appended in two calls and run as one batch,
