@@ -1511,6 +1511,36 @@ espl_status espl_ac(espl_lanes* h, uint32_t net, uint32_t vsrc, const double* om
     return espl_ac_solve(h, net, omega, n_freq, br.data(), bi.data(), 1, 0, rows, n_rows, out_re, out_im);
 }
 
+espl_status espl_noise_sources(espl_lanes* h, uint32_t net, double* psd, uint32_t* n_src) {
+    if (!h || net >= h->groups.size() || !n_src) return ESPL_INVALID_ARGUMENT;
+    Group& g = h->groups[net];
+    const uint32_t ns = g.kinds[ESPL_RES].count + g.kinds[ESPL_DIODE].count + g.kinds[ESPL_MOS1].count;
+    *n_src = ns;
+    if (!psd || ns == 0) return ESPL_OK;
+    const size_t P = g.P;
+    std::vector<void*> own;
+    auto release = [&]() {
+        for (void* p : own) cudaFree(p);
+    };
+    espl_status s;
+    double* dpsd;
+    uint32_t* tiles;
+    if ((s = dalloc(h, own, &dpsd, ns * P)) || (s = dalloc(h, own, &tiles, P / 32))) return release(), s;
+    std::vector<uint32_t> tl(P / 32);
+    for (uint32_t t = 0; t < P / 32; t++) tl[t] = g.tile0 + t;
+    CK(cudaMemcpyAsync(tiles, tl.data(), tl.size() * 4, cudaMemcpyHostToDevice, h->stream));
+    const TileMap m{h->d_groups, h->d_warp_group, tiles, (uint32_t)tl.size()};
+    k_noise<<<(uint32_t)tl.size(), kBlock, 0, h->stream>>>(m, dpsd);
+    CK(cudaGetLastError());
+    std::vector<double> host(ns * P);
+    CK(cudaMemcpyAsync(host.data(), dpsd, sizeof(double) * host.size(), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    release();
+    for (uint32_t l = 0; l < g.lanes; l++)
+        for (uint32_t k = 0; k < ns; k++) psd[(size_t)l * ns + k] = host[(size_t)k * P + l];
+    return ESPL_OK;
+}
+
 espl_status espl_ac_solve(espl_lanes* h, uint32_t net, const double* omega, uint32_t n_freq, const double* rhs_re,
                           const double* rhs_im, uint32_t n_rhs, uint32_t adjoint, const uint32_t* rows,
                           uint32_t n_rows, double* out_re, double* out_im) {

@@ -54,6 +54,47 @@ __global__ void __launch_bounds__(kTileThreads) k_ac_planes(TileMap m, double* _
     }
 }
 
+// White noise current densities (A^2/Hz) of every lane's noise sources at
+// its x, as the reference's models declare them at 27 C (tk = 300.15 K):
+// resistors 4kT/R across their terminals (models/resistor.va, resnoise.c),
+// diodes 2q|Id| of the junction current without the gmin shunt
+// (models/diode.va:326, dionoise.c), level-1 MOS channel thermal noise
+// 4kT (2/3)|gm| between drain and source (models/mos1.va:480-489, NLEV
+// below 3; gm as mos1load.c computes it); flicker noise is zero (KF = 0)
+// and RD/RS are absent. Source s (resistors, then diodes, then MOS in
+// their batch order) of lane l goes to psd[s * P + l].
+__global__ void __launch_bounds__(kTileThreads) k_noise(TileMap m, double* __restrict__ psd) {
+    TileCtx c = tile_ctx(m);
+    const GroupDev& d = *c.d;
+    const uint32_t P = d.P, l = c.l, nw = c.nw;
+    const uint32_t ninst = n_instances(d);
+    double* cells = cell_buf(d, 0);
+    if (c.valid)
+        for (uint32_t t = c.warp; t < ninst; t += nw) {
+            inst_seed(d, l, t, 0, d.x);
+            inst_eval(d, l, t, 0, 0.0, cells);
+        }
+    __syncthreads();
+    if (!c.valid) return;
+    const double kt4 = 4.0 * 1.38064852e-23 * 300.15, q2 = 2.0 * 1.6021766208e-19;
+    const uint32_t n_src = d.n_res + d.n_dio + d.n_mos;
+    for (uint32_t s = c.warp; s < n_src; s += nw) {
+        double v;
+        if (s < d.n_res) {
+            v = kt4 * fabs(ACM(cells, d.c_res + kResCells * s));
+        } else if (s < d.n_res + d.n_dio) {
+            const uint32_t i = s - d.n_res;
+            const double vd = ACM(d.x, d.dio_t[2 * i]) - ACM(d.x, d.dio_t[2 * i + 1]);
+            const double gmin = ACM(d.dio_d, DiodePrep::count * i + DiodePrep::gmin);
+            v = q2 * fabs(ACM(cells, d.c_dio + kDioCells * i + 1) - gmin * vd);
+        } else {
+            const uint32_t i = s - d.n_res - d.n_dio;
+            v = kt4 * (2.0 / 3.0) * fabs(ACM(cells, d.c_mos + kMosCells * i + 4));
+        }
+        ACM(psd, s) = v;
+    }
+}
+
 __global__ void __launch_bounds__(kTileThreads) k_ac(TileMap m, AcArgs A) {
     TileCtx c = tile_ctx(m);
     if (!c.valid || c.warp != 0) return;

@@ -65,6 +65,8 @@ def lib():
         L.espl_ac_solve.argtypes = [C.c_void_p, C.c_uint32, f64p, C.c_uint32, f64p, f64p, C.c_uint32, C.c_uint32,
                                     u32p, C.c_uint32, f64p, f64p]
         L.espl_ac_solve.restype = C.c_uint32
+        L.espl_noise_sources.argtypes = [C.c_void_p, C.c_uint32, f64p, u32p]
+        L.espl_noise_sources.restype = C.c_uint32
         L.espl_solve_op.argtypes = [C.c_void_p, C.POINTER(NewtonOpts), C.POINTER(LaneNewton)]
         L.espl_solve_op.restype = C.c_uint32
         L.espl_set_meas.argtypes = [C.c_void_p, C.c_uint32, C.POINTER(MeasPass), C.c_uint32]
@@ -80,6 +82,33 @@ def lib():
 
 
 PRECISION = {"fp64": abi.ESPL_FP64, "mixed": abi.ESPL_MIXED}
+
+
+def noise_terminals(net: Netlist) -> np.ndarray:
+    """The (from, to) unknowns of each noise source of `net`, in the order
+    espl_noise_sources reports them: resistors (p, n), diodes (anode,
+    cathode), MOS (drain, source); a grounded terminal reads net.n."""
+    from .decks import DIODE, GROUND, MOS1, RES
+    out = []
+    for kind, cols in ((RES, (0, 1)), (DIODE, (0, 1)), (MOS1, (0, 2))):
+        for b in net.batches:
+            if b.kind == kind:
+                t = np.asarray(b.term, dtype=np.int64).reshape(len(b.term), -1)
+                t = np.where(t == GROUND, net.n, t)
+                out += [(int(r[cols[0]]), int(r[cols[1]])) for r in t]
+    return np.array(out, dtype=np.int64).reshape(-1, 2)
+
+
+def noise_sum(psd: np.ndarray, z: np.ndarray, terms: np.ndarray) -> np.ndarray:
+    """sum_s psd[l, s] |z[l, f, a_s] - z[l, f, b_s]|^2: the output density
+    from source densities psd [lanes, n_src] and the adjoint solutions
+    z [lanes, F, n] (z[u]: transfer from a unit current into unknown u to
+    the output; index n, the ground, reads zero)."""
+    if len(terms) == 0:
+        return np.zeros(z.shape[:2])
+    z = np.concatenate([z, np.zeros(z.shape[:2] + (1,), dtype=z.dtype)], axis=2)
+    h = z[:, :, terms[:, 0]] - z[:, :, terms[:, 1]]
+    return np.einsum("ls,lfs->lf", psd, np.abs(h) ** 2)
 
 
 class Lanes:
@@ -177,6 +206,30 @@ class Lanes:
                                         bi.ctypes.data_as(f64p), len(b), int(adjoint), rw.ctypes.data_as(u32p),
                                         len(rw), re.ctypes.data_as(f64p), im.ctypes.data_as(f64p)), "espl_ac_solve")
         return re + 1j * im
+
+    def noise_sources(self, net: int):
+        """(psd [lanes, n_src] in A^2/Hz, terminals [n_src, 2]) of template
+        `net`'s noise sources at the lanes' x: resistors, diodes, MOS."""
+        n = C.c_uint32()
+        self._check(lib().espl_noise_sources(self.h, net, None, C.byref(n)), "espl_noise_sources")
+        psd = np.zeros((self.nets[net].lanes, max(n.value, 1)))
+        self._check(lib().espl_noise_sources(self.h, net, psd.ctypes.data_as(f64p), C.byref(n)),
+                    "espl_noise_sources")
+        return psd[:, :n.value], noise_terminals(self.nets[net])
+
+    def noise(self, net: int, omega, out: int, ref: Optional[int] = None) -> np.ndarray:
+        """Output noise density (V^2/Hz, or A^2/Hz for a branch row) of
+        unknown `out` (minus `ref`) at angular frequencies `omega`, every
+        lane at its operating point: one adjoint solve per frequency and
+        each source's density times its squared transfer. [lanes, len(omega)]."""
+        nl = self.nets[net]
+        b = np.zeros(nl.n, dtype=complex)
+        b[out] = 1.0
+        if ref is not None:
+            b[ref] = -1.0
+        psd, terms = self.noise_sources(net)
+        z = self.ac_solve(net, omega, b[None, :], np.arange(nl.n), adjoint=True)[:, :, 0, :]
+        return noise_sum(psd, z, terms)
 
     def init_steps(self, topts: TranOpts):
         self._check(lib().espl_init_steps(self.h, C.byref(topts)), "espl_init_steps")

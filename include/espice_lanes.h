@@ -210,6 +210,18 @@ espl_status espl_ac_solve(espl_lanes *h, uint32_t net, const double *omega, uint
                           const double *rhs_im, uint32_t n_rhs, uint32_t adjoint, const uint32_t *rows,
                           uint32_t n_rows, double *out_re, double *out_im);
 
+/* The white noise current densities (A^2/Hz) of every lane's noise
+ * sources at its current x (an operating point), as the reference's device
+ * models declare them at 27 C: resistors 4kT/R between their terminals,
+ * diodes 2q|Id| (junction current, gmin shunt excluded) from anode to
+ * cathode, level-1 MOS channel thermal noise 4kT (2/3)|gm| from drain to
+ * source (flicker noise zero: KF = 0). Sources are the template's
+ * resistors, then its diodes, then its MOS, in batch order; *n_src receives
+ * their count, and psd (when not NULL) [lanes][n_src] the densities. With
+ * espl_ac_solve's adjoint solve of the output row, the output noise is
+ * sum_s psd[s] |z[a_s] - z[b_s]|^2. Leaves the limiter state seeded at x. */
+espl_status espl_noise_sources(espl_lanes *h, uint32_t net, double *psd, uint32_t *n_src);
+
 /* Transient lanes with device step control (`initSteps` lanes.zig:1827,
  * `deviceLaunch` :1917; the step machine `stepBegin/stepEndA/stepEndB`,
  * src/solver/kernels/lane.zig:505-700). */

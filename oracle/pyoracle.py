@@ -290,6 +290,50 @@ def ac_solve_lanes(net: Netlist, x: np.ndarray, omega, rhs, rows, adjoint: bool 
     return out
 
 
+KT4 = 4.0 * 1.38064852e-23 * 300.15  # 4kT at 27 C, the models' default temperature
+Q2 = 2.0 * 1.6021766208e-19
+
+
+def noise_densities(net: Netlist, x: np.ndarray) -> np.ndarray:
+    """White noise current densities [lanes, n_src] of the reference's
+    models (resistor.va 4kT/R, diode.va:326 2q|Id| without the gmin shunt,
+    mos1.va:480-489 4kT (2/3)|gm|) from the oracle's device probes at each
+    lane's x; sources ordered resistors, diodes, MOS (batch order)."""
+    out = []
+    for kind in (1, 5, 6):
+        for bi, b in enumerate(net.batches):
+            if b.kind != kind:
+                continue
+            t = np.asarray(b.term, dtype=np.int64).reshape(len(b.term), -1)
+            t = np.where(t == 0xFFFFFFFF, net.n, t)  # the ground reads 0 V
+            for i in range(len(t)):
+                col = np.zeros(net.lanes)
+                for l in range(net.lanes):
+                    v = np.append(x[l], 0.0)[t[i]]
+                    f, j, _, _ = device_probe(net, bi, i, l, v)
+                    if kind == 1:
+                        col[l] = KT4 * abs(j[0, 0])
+                    elif kind == 5:
+                        col[l] = Q2 * abs(f[0] - 1e-12 * (v[0] - v[1]))
+                    else:
+                        col[l] = KT4 * (2.0 / 3.0) * abs(j[0, 1])
+                out.append(col)
+    return np.stack(out, axis=1) if out else np.zeros((net.lanes, 0))
+
+
+def noise_lanes(net: Netlist, x: np.ndarray, omega, out: int, terms: np.ndarray) -> np.ndarray:
+    """Output noise density of unknown `out` [lanes, len(omega)]: the dense
+    adjoint solve per lane and frequency, each source's density times
+    |z[a] - z[b]|^2 (terms [n_src, 2], in noise_densities' order)."""
+    e = np.zeros((1, net.n), dtype=complex)
+    e[0, out] = 1.0
+    z = ac_solve_lanes(net, x, omega, e, np.arange(net.n), adjoint=True)[:, :, 0, :]
+    z = np.concatenate([z, np.zeros(z.shape[:2] + (1,), dtype=complex)], axis=2)  # the ground
+    psd = noise_densities(net, x)
+    h = z[:, :, terms[:, 0]] - z[:, :, terms[:, 1]]
+    return np.einsum("ls,lfs->lf", psd, np.abs(h) ** 2)
+
+
 def tran_lanes(net: Netlist, opts: TranOpts, lane0: int = 0, count: Optional[int] = None,
                probes: Sequence[int] = (), max_rows: int = 0, meas: Optional[Tuple[int, float, float]] = None,
                threads: int = 1):

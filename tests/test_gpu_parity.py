@@ -426,6 +426,34 @@ def test_ac_solve_lists_and_adjoints(oracle):
     np.testing.assert_allclose(adj[:, :, 0, branch], fwd[:, :, 1, out], rtol=1e-9)
 
 
+def test_noise_lanes(oracle):
+    """espl_noise_sources and the adjoint solves: an RC low pass against its
+    analytic output noise 4kTR / (1 + (wRC)^2), and the op-amp's 64 lanes at
+    their warm operating points (MOS channel noise) against the oracle's
+    densities and dense adjoint solves."""
+    r, c = np.array([1e3, 2e3, 5e3]), np.array([1e-12, 1e-12, 2e-13])
+    rc = decks.rc_points(3, r, c)
+    om = np.logspace(5, 12, 15)
+    with Lanes([rc]) as L:
+        L.solve_static(abi.newton_opts())
+        s = L.noise(0, om, rc.node("out"))
+    want = oracle.KT4 * r[:, None] / (1.0 + (om[None, :] * (r * c)[:, None]) ** 2)
+    np.testing.assert_allclose(s, want, rtol=1e-9)
+    net = decks.miller_opamp(64)
+    om = np.logspace(2, 10, 9)
+    out = net.node("out")
+    with Lanes([net]) as L:
+        L.put_x(0, opamp_start(net), False)
+        res = L.solve_static(abi.newton_opts(init_fix=0))
+        x = L.get_x(0)
+        psd, terms = L.noise_sources(0)
+        s = L.noise(0, om, out)
+    assert ((res[:, 0] & abi.CONVERGED) != 0).all()
+    np.testing.assert_allclose(psd, oracle.noise_densities(net, x), rtol=1e-9, atol=1e-40)
+    assert (psd > 0).any()
+    np.testing.assert_allclose(s, oracle.noise_lanes(net, x, om, out, terms), rtol=1e-8)
+
+
 def test_points_api(oracle):
     """The points mirror (egspice_b200/points.py, include/espice.h :244-362)
     on the lanes: 100 RC points appended in two calls and run as one batch,
