@@ -453,12 +453,15 @@ def read_deck(text: str, lanes: int = 1, params: Optional[Mapping[str, Value]] =
 
 @dataclasses.dataclass
 class Measure:
-    """One `.meas tran` card: its name, the consecutive passes that compute
-    it, and how its value comes out of them: the last pass's value, or (PP)
-    the first pass's (MAX) minus the second's (MIN)."""
+    """One `.meas` card: its name, the consecutive passes that compute it
+    (`.meas tran`), and how its value comes out of them: the last pass's
+    value, or (PP) the first pass's (MAX) minus the second's (MIN). A
+    `.meas op ... find vec` card has no passes and reads unknown `op_row`
+    of the operating point."""
     name: str
     passes: List[abi.MeasPass]
     pp: bool = False
+    op_row: Optional[int] = None
 
 
 _COUNTS = ("rise", "fall", "cross")
@@ -601,11 +604,16 @@ def read_measures(text: str, net: Netlist, params: Optional[Mapping[str, Value]]
         where = f"line {ln}"
         if len(toks) < 4:
             raise DeckError(f"{where}: .meas needs an analysis, a name and a measure")
-        if toks[1] != "tran":
-            raise DeckError(f"{where}: only .meas tran rides the lanes")
         name = toks[2]
         if any(m.name == name for m in out):
             raise DeckError(f"{where}: a second measure named {name!r}")
+        if toks[1] == "op":
+            if toks[3] != "find" or len(toks) != 5:
+                raise DeckError(f"{where}: .meas op takes FIND vector")
+            out.append(Measure(name, [], op_row=_vector(toks[4], net, where)))
+            continue
+        if toks[1] != "tran":
+            raise DeckError(f"{where}: only .meas tran and .meas op ride the lanes")
         out.append(_measure(name, toks[3], toks[4:], net, env, where))
     return out
 
@@ -618,12 +626,17 @@ def measure_passes(measures: Sequence[Measure]) -> List[abi.MeasPass]:
     return passes
 
 
-def measure_values(measures: Sequence[Measure], value: np.ndarray) -> Dict[str, np.ndarray]:
+def measure_values(measures: Sequence[Measure], value: np.ndarray,
+                   x_op: Optional[np.ndarray] = None) -> Dict[str, np.ndarray]:
     """Each measure's value per lane from Lanes.get_meas's `value` [lanes,
-    passes] (NaN where it has none)."""
+    passes] (NaN where it has none); `.meas op` cards read the operating
+    points x_op [lanes, n] (NaN without them)."""
     out: Dict[str, np.ndarray] = {}
     k = 0
     for m in measures:
+        if m.op_row is not None:
+            out[m.name] = x_op[:, m.op_row].copy() if x_op is not None else np.full(value.shape[0], np.nan)
+            continue
         if m.pp:
             out[m.name] = value[:, k] - value[:, k + 1]
         else:
@@ -643,7 +656,8 @@ REASON_OTHER = 255
 
 
 def point_measures(measures: Sequence[Measure], value: np.ndarray, names: Optional[Sequence[str]] = None,
-                   reports: Optional[Sequence] = None, op: Optional[np.ndarray] = None):
+                   reports: Optional[Sequence] = None, op: Optional[np.ndarray] = None,
+                   x_op: Optional[np.ndarray] = None):
     """Each lane's measures and reason as the reference's points API copies
     them (include/espice.h espice_copy_point_measures :324-338): values
     [lanes][len(names)] (names case-insensitive, default every measure in
@@ -652,8 +666,9 @@ def point_measures(measures: Sequence[Measure], value: np.ndarray, names: Option
     converge (SINGULAR_MATRIX when it was singular, else NO_CONVERGENCE), or
     its transient (`reports`, espl_step_report per lane) ended otherwise than
     done (TIMESTEP_TOO_SMALL on a step underflow, else OTHER). Otherwise NaN
-    marks a measure with no value and the reason is MEASURE_UNRESOLVED."""
-    allv = measure_values(measures, value)
+    marks a measure with no value and the reason is MEASURE_UNRESOLVED.
+    `.meas op` cards read x_op, the operating points [lanes, n]."""
+    allv = measure_values(measures, value, x_op)
     keys = {k.lower(): k for k in allv}
     if names is None:
         names = list(allv)

@@ -38,12 +38,15 @@ class PointsError(RuntimeError):
 
 
 def _tran_card(text: str):
-    """(tstep, tstop, tmax) of the deck's one .tran card."""
+    """(tstep, tstop, tmax) of the deck's one .tran card, or None for a deck
+    whose one analysis is .op."""
     found = None
+    has_op = False
     for ln, card in _logical_lines(text):
         toks = _split(card)
         if toks[0] in (".step", ".data", ".alter"):
             raise PointsError(INVALID_ARGUMENT, "SweptTemplate")
+        has_op |= toks[0] == ".op"
         if toks[0] != ".tran":
             continue
         if found is not None:
@@ -58,8 +61,8 @@ def _tran_card(text: str):
             raise DeckError(f"line {ln}: a nonzero tstart is outside what the lanes carry")
         tmax = vals[3] if len(vals) > 3 else None
         found = (vals[0], vals[1], tmax)
-    if found is None:
-        raise DeckError("the deck has no .tran card; the points run transients")
+    if found is None and not has_op:
+        raise DeckError("the deck has neither a .tran nor an .op card")
     return found
 
 
@@ -69,24 +72,32 @@ class Points:
     .param values). `precision` as Lanes takes it; `tran` overrides fields
     of the transient options (abi.tran_opts keywords). TMAX defaults to
     ngspice's min(TSTEP, TSTOP / 50). A measure may read parameters, but no
-    live one: a template's measure passes are the same on every lane."""
+    live one: a template's measure passes are the same on every lane. A
+    deck with .op and no .tran runs operating points (the continuation
+    ladder), which `.meas op ... find` cards read; in a .tran deck they read
+    the operating point solved the same way before the transient."""
 
     def __init__(self, text: str, live_params: Sequence[str], precision: str = "fp64",
                  tran: Optional[Mapping[str, float]] = None):
         self.text = text
         self.live = [p.lower() for p in live_params]
         self.precision = precision
-        tstep, tstop, tmax = _tran_card(text)
-        kw = dict(t_stop=tstop, dt=tstep, dt_max=tmax if tmax else min(tstep, tstop / 50))
-        kw.update(tran or {})
-        self.topts = abi.tran_opts(**kw)
+        card = _tran_card(text)
+        self.topts = None
+        if card is not None:
+            tstep, tstop, tmax = card
+            kw = dict(t_stop=tstop, dt=tstep, dt_max=tmax if tmax else min(tstep, tstop / 50))
+            kw.update(tran or {})
+            self.topts = abi.tran_opts(**kw)
         # the measures are read once on a two-lane instance of the template
         # whose live values differ, so a card that names no vector, or reads
         # a live parameter, fails here
         probe_params = {p: np.array([0.0, 1.0]) for p in self.live}
         probe = read_deck(text, lanes=2, params=probe_params)
         self.measures = read_measures(text, probe, params=probe_params)
-        measure_passes(self.measures)
+        if self.topts is None and measure_passes(self.measures):
+            raise DeckError("a .meas tran card needs the deck's .tran card")
+        self.need_op = self.topts is None or any(m.op_row is not None for m in self.measures)
         self.rows: List[np.ndarray] = []     # each point's values
         self.state: List[int] = []           # 0 pending, 1 complete, 2 released
         self.values: Dict[int, np.ndarray] = {}
@@ -139,11 +150,17 @@ class Points:
             params = {p: block[:, j] for j, p in enumerate(self.live)}
             net = read_deck(self.text, lanes=len(ids), params=params)
             ms = read_measures(self.text, net, params=params)
+            op = x_op = reps = None
+            value = np.zeros((len(ids), 0))
             with Lanes([net], precision=self.precision) as L:
-                L.set_meas(0, measure_passes(ms))
-                reps = L.run_tran(self.topts, steps_per_launch=2048)
-                value, _ = L.get_meas(0)
-            out, reasons = point_measures(ms, value, names, reports=reps)
+                if self.need_op:
+                    op = L.solve_op(abi.newton_opts())
+                    x_op = L.get_x(0)
+                if self.topts is not None:
+                    L.set_meas(0, measure_passes(ms))
+                    reps = L.run_tran(self.topts, steps_per_launch=2048)
+                    value, _ = L.get_meas(0)
+            out, reasons = point_measures(ms, value, names, reports=reps, op=op, x_op=x_op)
             for i, k in enumerate(ids):
                 self.values[k] = out[i]
                 self.reasons[k] = int(reasons[i])

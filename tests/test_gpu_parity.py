@@ -548,3 +548,29 @@ def test_chain_fixture_points_in_three_orders(oracle, precision):
     for j, name in enumerate(names):
         np.testing.assert_allclose(v[:17, j], want[name][:17], rtol=1e-6, err_msg=name)
         assert np.isnan(v[17, j]) and np.isnan(want[name][17])
+
+
+def test_points_operating_points():
+    """An .op deck as points (egspice_b200/points.py): `.meas op ... find`
+    reads each point's operating point; a resistive divider against its
+    analytic node voltage and supply current (the source's branch current,
+    from its + node through it: minus the current it delivers)."""
+    from egspice_b200 import points as pt
+    deck = """divider
+vdd vdd 0 1.8
+r1 vdd mid {rtop}
+r2 mid 0 10k
+.param rtop=10k
+.op
+.meas op vmid find v(mid)
+.meas op idd find i(vdd)
+.end
+"""
+    rtop = np.linspace(1e3, 1e5, 50)
+    p = pt.Points(deck, ["rtop"])
+    p.append_points(rtop[:, None])
+    p.run()
+    v, r = p.copy_point_measures(0, 50, ["vmid", "idd"])
+    assert (r == 0).all()
+    np.testing.assert_allclose(v[:, 0], 1.8 * 1e4 / (rtop + 1e4), rtol=1e-9)
+    np.testing.assert_allclose(v[:, 1], -1.8 / (rtop + 1e4), rtol=1e-9)

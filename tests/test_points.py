@@ -26,7 +26,7 @@ def test_template_checks():
     # numbers as ngspice reads them; TMAX = min(TSTEP, TSTOP / 50)
     assert p.topts.t_stop == parse_number("6n") and p.topts.dt_max == parse_number("1p")
     assert pt.Points.lane_width() == 16384
-    with pytest.raises(DeckError, match="no .tran"):
+    with pytest.raises(DeckError, match="neither a .tran nor an .op"):
         pt.Points(DECK.replace(".tran 1p 6n\n", ""), ["rval"])
     with pytest.raises(DeckError, match="UIC"):
         pt.Points(DECK.replace(".tran 1p 6n", ".tran 1p 6n uic"), ["rval"])
@@ -60,3 +60,27 @@ def test_append_copy_release():
     assert e.value.status == pt.RESULT_UNAVAILABLE
     with pytest.raises(pt.PointsError, match="NoLiveParameters"):
         pt.Points(DECK, []).append_points([[1.0]])
+
+
+def test_op_decks_and_op_measures():
+    op_deck = """leakage of a divider
+vdd vdd 0 1.8
+r1 vdd mid {rtop}
+r2 mid 0 10k
+.param rtop=10k
+.op
+.meas op vmid find v(mid)
+.meas op idd find i(vdd)
+.end
+"""
+    p = pt.Points(op_deck, ["rtop"])
+    assert p.topts is None and p.need_op
+    assert [m.op_row is not None for m in p.measures] == [True, True]
+    with pytest.raises(DeckError, match="needs the deck's .tran"):
+        pt.Points(op_deck.replace(".end", ".meas tran t1 max v(mid)\n.end"), ["rtop"])
+    with pytest.raises(DeckError, match="neither a .tran nor an .op"):
+        pt.Points(op_deck.replace(".op\n", ""), ["rtop"])
+    with pytest.raises(DeckError, match="FIND vector"):
+        pt.Points(op_deck.replace("find v(mid)", "max v(mid)"), ["rtop"])
+    q = pt.Points(DECK.replace(".end", ".meas op v0 find v(out)\n.end"), ["rval", "cval"])
+    assert q.topts is not None and q.need_op
