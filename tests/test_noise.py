@@ -6,7 +6,6 @@ analytic output noise 4kTR / (1 + (wRC)^2), whose integral over frequency
 is kT/C. The GPU densities (espl_noise_sources) and adjoint solves are
 checked in tests/test_gpu_parity.py."""
 import numpy as np
-import pytest
 
 from egspice_b200 import abi, decks
 from egspice_b200.lanes import noise_sum, noise_terminals
