@@ -195,16 +195,18 @@ def _logical_lines(text: str) -> List[tuple]:
 
 
 def _split(card: str) -> List[str]:
-    """Tokens of a card: spaces separate, `=` binds, braces and parentheses
-    keep their contents together."""
+    """Tokens of a card: spaces separate, `=` binds, braces, parentheses
+    and single quotes keep their contents together."""
     card = re.sub(r"\s*=\s*", "=", card)
-    toks, cur, depth = [], "", 0
+    toks, cur, depth, quoted = [], "", 0, False
     for ch in card:
-        if ch in "{(":
+        if ch == "'":
+            quoted = not quoted
+        elif ch in "{(":
             depth += 1
         elif ch in "})":
             depth -= 1
-        if (ch.isspace() or ch == ",") and depth == 0:
+        if (ch.isspace() or ch == ",") and depth == 0 and not quoted:
             if cur:
                 toks.append(cur)
             cur = ""
@@ -457,11 +459,15 @@ class Measure:
     (`.meas tran`), and how its value comes out of them: the last pass's
     value, or (PP) the first pass's (MAX) minus the second's (MIN). A
     `.meas op ... find vec` card has no passes and reads unknown `op_row`
-    of the operating point."""
+    of the operating point; a `.meas tran name param='expr'` card has none
+    either and evaluates `expr` over the parameters (`params`, as read with
+    the deck) and the measures before it."""
     name: str
     passes: List[abi.MeasPass]
     pp: bool = False
     op_row: Optional[int] = None
+    expr: Optional[str] = None
+    params: Optional[Dict[str, Value]] = None
 
 
 _COUNTS = ("rise", "fall", "cross")
@@ -590,8 +596,10 @@ def read_measures(text: str, net: Netlist, params: Optional[Mapping[str, Value]]
     vector; RISE/FALL/CROSS counts or LAST, TD, FROM, TO), FIND and DERIV at
     a time or at a WHEN, TRIG ... TARG (VAL and counts per clause; the TARG
     counts from the TRIG event, as the reference's measure stream does),
-    MAX, MIN, AVG, RMS, INTEG, PP over a window. Vectors are v(node) and
-    i(vsource); values are numbers or parameters the same on every lane.
+    MAX, MIN, AVG, RMS, INTEG, PP over a window, and PARAM='expr' over the
+    parameters and the measures before it; `.meas op ... find vec` reads the
+    operating point. Vectors are v(node) and i(vsource); values are numbers
+    or parameters the same on every lane.
     Anything else raises DeckError naming the line."""
     env = _Env(net.lanes, dict(params or {}))
     cards = _expand_subckts(_logical_lines(text))
@@ -614,6 +622,16 @@ def read_measures(text: str, net: Netlist, params: Optional[Mapping[str, Value]]
             continue
         if toks[1] != "tran":
             raise DeckError(f"{where}: only .meas tran and .meas op ride the lanes")
+        if toks[3].startswith("param="):
+            if len(toks) != 4:
+                raise DeckError(f"{where}: PARAM takes one expression")
+            text = toks[3][len("param="):].strip("'{}")
+            trial = _Env(net.lanes, {})
+            trial.vals = dict(env.vals)
+            trial.vals.update({m.name: np.zeros(net.lanes) for m in out})
+            trial.expr(text, where)  # names only parameters and earlier measures
+            out.append(Measure(name, [], expr=text, params=dict(env.vals)))
+            continue
         out.append(_measure(name, toks[3], toks[4:], net, env, where))
     return out
 
@@ -633,7 +651,16 @@ def measure_values(measures: Sequence[Measure], value: np.ndarray,
     points x_op [lanes, n] (NaN without them)."""
     out: Dict[str, np.ndarray] = {}
     k = 0
+    lanes = value.shape[0]
     for m in measures:
+        if m.expr is not None:
+            ev = _Env(lanes, {})
+            ev.vals = dict(m.params or {})
+            ev.vals.update(out)
+            with np.errstate(all="ignore"):
+                out[m.name] = np.broadcast_to(np.asarray(ev.expr(m.expr, m.name), dtype=np.float64),
+                                              (lanes,)).copy()
+            continue
         if m.op_row is not None:
             out[m.name] = x_op[:, m.op_row].copy() if x_op is not None else np.full(value.shape[0], np.nan)
             continue

@@ -130,3 +130,25 @@ def test_point_measures_and_reasons():
     assert np.isnan(out[3, 0]) and not np.isnan(out[3, 1])
     with pytest.raises(DeckError, match="UnknownMeasure"):
         nl.point_measures(ms, value, ["nope"])
+
+
+def test_param_measures():
+    """`.meas tran name param='expr'` over the measures before it and the
+    deck's parameters, per lane; unknown names refused at read time."""
+    net, r = _rc()
+    text = RC_DECK.replace(".end", ".meas tran mid param='(t50 + rise) / 2 + 0 * half'\n"
+                                   ".meas tran scaled param='swing * 1k'\n.end")
+    ms = read_measures(text, net, params={"rval": r})
+    assert [m.name for m in ms][-2:] == ["mid", "scaled"] and ms[-1].passes == []
+    n_pass = len(measure_passes(ms))
+    value = np.random.default_rng(1).uniform(1, 2, size=(2, n_pass))
+    got = measure_values(ms, value)
+    np.testing.assert_allclose(got["mid"], (got["t50"] + got["rise"]) / 2)
+    np.testing.assert_allclose(got["scaled"], got["swing"] * 1e3)
+    bad = RC_DECK.replace(".end", ".meas tran oops param='t50 + nosuch'\n.end")
+    with pytest.raises(DeckError, match="unknown parameter 'nosuch'"):
+        read_measures(bad, net, params={"rval": r})
+    later = RC_DECK.replace(".meas tran t50 when v(out)=half", ".meas tran early2 param='t50 * 2'\n"
+                                                               ".meas tran t50 when v(out)=half")
+    with pytest.raises(DeckError, match="unknown parameter 't50'"):
+        read_measures(later, net, params={"rval": r})
