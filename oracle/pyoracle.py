@@ -294,11 +294,25 @@ KT4 = 4.0 * 1.38064852e-23 * 300.15  # 4kT at 27 C, the models' default temperat
 Q2 = 2.0 * 1.6021766208e-19
 
 
+def _mos_alone(b, i: int, lanes: int) -> Netlist:
+    """MOS instance i of batch b alone, its four terminals on four distinct
+    nodes, so a probe's drain-row Jacobian reads gm even where the deck ties
+    the gate to the drain (a probe on the deck's own nodes sums the tied
+    terminals' columns)."""
+    from egspice_b200.decks import Builder
+    p = np.asarray(b.param)[i]  # [9, lanes]: type, vto, kp, gamma, phi, lambda, is, w, l
+    bl = Builder("mos", lanes)
+    bl.m("d", "g", "s", "b", p[0], p[1], p[2], p[7], p[8], gamma=p[3], phi=p[4], lam=p[5], is_=p[6])
+    return bl.freeze()
+
+
 def noise_densities(net: Netlist, x: np.ndarray) -> np.ndarray:
     """White noise current densities [lanes, n_src] of the reference's
-    models (resistor.va 4kT/R, diode.va:326 2q|Id| without the gmin shunt,
-    mos1.va:480-489 4kT (2/3)|gm|) from the oracle's device probes at each
-    lane's x; sources ordered resistors, diodes, MOS (batch order)."""
+    models at each lane's x: resistors 4kT/R (resistor.va, R from the
+    batch), diodes 2q|Id| without the gmin shunt (diode.va:326, Id from the
+    oracle's device probe), MOS 4kT (2/3)|gm| (mos1.va:480-489, gm the
+    probe's drain-row gate entry with the terminals apart); sources ordered
+    resistors, diodes, MOS (batch order)."""
     out = []
     for kind in (1, 5, 6):
         for bi, b in enumerate(net.batches):
@@ -307,15 +321,18 @@ def noise_densities(net: Netlist, x: np.ndarray) -> np.ndarray:
             t = np.asarray(b.term, dtype=np.int64).reshape(len(b.term), -1)
             t = np.where(t == 0xFFFFFFFF, net.n, t)  # the ground reads 0 V
             for i in range(len(t)):
+                if kind == 1:
+                    out.append(KT4 / np.abs(np.asarray(b.param)[i, 0]))
+                    continue
+                alone = _mos_alone(b, i, net.lanes) if kind == 6 else None
                 col = np.zeros(net.lanes)
                 for l in range(net.lanes):
                     v = np.append(x[l], 0.0)[t[i]]
-                    f, j, _, _ = device_probe(net, bi, i, l, v)
-                    if kind == 1:
-                        col[l] = KT4 * abs(j[0, 0])
-                    elif kind == 5:
+                    if kind == 5:
+                        f, _, _, _ = device_probe(net, bi, i, l, v)
                         col[l] = Q2 * abs(f[0] - 1e-12 * (v[0] - v[1]))
                     else:
+                        _, j, _, _ = device_probe(alone, 0, 0, l, v)
                         col[l] = KT4 * (2.0 / 3.0) * abs(j[0, 1])
                 out.append(col)
     return np.stack(out, axis=1) if out else np.zeros((net.lanes, 0))
