@@ -1814,6 +1814,34 @@ espl_status espl_get_meas(espl_lanes* h, uint32_t net, double* value, double* at
     return ESPL_OK;
 }
 
+espl_status espl_meas_done(espl_lanes* h, uint32_t net, uint8_t* done) {
+    if (!h || net >= h->groups.size() || !done) return ESPL_INVALID_ARGUMENT;
+    Group& g = h->groups[net];
+    const uint32_t n = (uint32_t)g.passes.size();
+    if (!n) return ESPL_OK;
+    std::vector<double> st((size_t)n * kMeasWords * g.P);
+    CK(cudaMemcpyAsync(st.data(), g.dev.mstate, st.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    for (uint32_t l = 0; l < g.lanes; l++)
+        for (uint32_t p = 0; p < n; p++)
+            done[(size_t)l * n + p] = st[((size_t)p * kMeasWords + kMeasDone) * g.P + l] != 0.0;
+    return ESPL_OK;
+}
+
+espl_status espl_request_stop(espl_lanes* h, uint32_t net, const uint8_t* stop) {
+    if (!h || net >= h->groups.size() || !stop) return ESPL_INVALID_ARGUMENT;
+    Group& g = h->groups[net];
+    LaneState* dev = h->d_state + g.lane0;
+    LaneState* host = h->h_state.data() + g.lane0;
+    CK(cudaMemcpyAsync(host, dev, sizeof(LaneState) * g.lanes, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    for (uint32_t l = 0; l < g.lanes; l++)
+        if (stop[l] && host[l].status == 0) host[l].status = 4;
+    CK(cudaMemcpyAsync(dev, host, sizeof(LaneState) * g.lanes, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return ESPL_OK;
+}
+
 espl_status espl_get_stats(espl_lanes* h, espl_stats* out) {
     if (!h || !out) return ESPL_INVALID_ARGUMENT;
     CK(cudaMemcpyAsync(h->h_state.data(), h->d_state, sizeof(LaneState) * h->total_lanes, cudaMemcpyDeviceToHost,

@@ -67,6 +67,10 @@ def lib():
         L.espl_ac_solve.restype = C.c_uint32
         L.espl_noise_sources.argtypes = [C.c_void_p, C.c_uint32, f64p, u32p]
         L.espl_noise_sources.restype = C.c_uint32
+        L.espl_meas_done.argtypes = [C.c_void_p, C.c_uint32, C.POINTER(C.c_uint8)]
+        L.espl_meas_done.restype = C.c_uint32
+        L.espl_request_stop.argtypes = [C.c_void_p, C.c_uint32, C.POINTER(C.c_uint8)]
+        L.espl_request_stop.restype = C.c_uint32
         L.espl_solve_op.argtypes = [C.c_void_p, C.POINTER(NewtonOpts), C.POINTER(LaneNewton)]
         L.espl_solve_op.restype = C.c_uint32
         L.espl_set_meas.argtypes = [C.c_void_p, C.c_uint32, C.POINTER(MeasPass), C.c_uint32]
@@ -287,6 +291,23 @@ class Lanes:
         a = np.full((lanes, max(n, 1)), np.nan)
         self._check(lib().espl_get_meas(self.h, net, v.ctypes.data_as(f64p), a.ctypes.data_as(f64p)), "espl_get_meas")
         return v[:, :n], a[:, :n]
+
+    def meas_done(self, net: int) -> np.ndarray:
+        """[lanes, passes] bool: passes that have read their last sample."""
+        n = getattr(self, "_n_meas", {}).get(net, 0)
+        out = np.zeros((self.nets[net].lanes, max(n, 1)), dtype=np.uint8)
+        if n:
+            self._check(lib().espl_meas_done(self.h, net, out.ctypes.data_as(C.POINTER(C.c_uint8))),
+                        "espl_meas_done")
+        return out[:, :n].astype(bool)
+
+    def request_stop(self, net: int, stop) -> None:
+        """Stops the still-stepping lanes of template `net` where `stop`
+        [lanes] is true, before the next device launch."""
+        m = np.ascontiguousarray(np.asarray(stop, dtype=bool), dtype=np.uint8)
+        assert m.shape == (self.nets[net].lanes,)
+        self._check(lib().espl_request_stop(self.h, net, m.ctypes.data_as(C.POINTER(C.c_uint8))),
+                    "espl_request_stop")
 
     def classes(self) -> List[dict]:
         """The launch classes in launch order, each with its kernel's device

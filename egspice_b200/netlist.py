@@ -684,7 +684,7 @@ REASON_OTHER = 255
 
 def point_measures(measures: Sequence[Measure], value: np.ndarray, names: Optional[Sequence[str]] = None,
                    reports: Optional[Sequence] = None, op: Optional[np.ndarray] = None,
-                   x_op: Optional[np.ndarray] = None):
+                   x_op: Optional[np.ndarray] = None, stopped_ok: bool = False):
     """Each lane's measures and reason as the reference's points API copies
     them (include/espice.h espice_copy_point_measures :324-338): values
     [lanes][len(names)] (names case-insensitive, default every measure in
@@ -694,7 +694,9 @@ def point_measures(measures: Sequence[Measure], value: np.ndarray, names: Option
     its transient (`reports`, espl_step_report per lane) ended otherwise than
     done (TIMESTEP_TOO_SMALL on a step underflow, else OTHER). Otherwise NaN
     marks a measure with no value and the reason is MEASURE_UNRESOLVED.
-    `.meas op` cards read x_op, the operating points [lanes, n]."""
+    `.meas op` cards read x_op, the operating points [lanes, n]. With
+    `stopped_ok` a transient stopped on request (status 4, an early stop
+    once its measures resolved) counts as done."""
     allv = measure_values(measures, value, x_op)
     keys = {k.lower(): k for k in allv}
     if names is None:
@@ -715,7 +717,7 @@ def point_measures(measures: Sequence[Measure], value: np.ndarray, names: Option
         failed |= bad
     if reports is not None:
         status = np.array([r.status for r in reports], dtype=np.uint32)
-        bad = (status != 1) & ~failed
+        bad = (status != 1) & ~(stopped_ok & (status == 4)) & ~failed
         reasons[bad] = np.where(status[bad] == 2, REASON_TIMESTEP_TOO_SMALL, REASON_OTHER)
         failed |= bad
     out[failed] = np.nan

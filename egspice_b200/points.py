@@ -72,14 +72,17 @@ class Points:
     .param values). `precision` as Lanes takes it; `tran` overrides fields
     of the transient options (abi.tran_opts keywords). TMAX defaults to
     ngspice's min(TSTEP, TSTOP / 50). A measure may read parameters, but no
-    live one: a template's measure passes are the same on every lane. A
+    live one: a template's measure passes are the same on every lane.
+    `early_stop` (espice_points_options.early_stop) ends each point's
+    transient once all its measure passes have resolved. A
     deck with .op and no .tran runs operating points (the continuation
     ladder), which `.meas op ... find` cards read; in a .tran deck they read
     the operating point solved the same way before the transient."""
 
     def __init__(self, text: str, live_params: Sequence[str], precision: str = "fp64",
-                 tran: Optional[Mapping[str, float]] = None):
+                 tran: Optional[Mapping[str, float]] = None, early_stop: bool = False):
         self.text = text
+        self.early_stop = early_stop
         self.live = [p.lower() for p in live_params]
         self.precision = precision
         card = _tran_card(text)
@@ -157,14 +160,33 @@ class Points:
                     op = L.solve_op(abi.newton_opts())
                     x_op = L.get_x(0)
                 if self.topts is not None:
-                    L.set_meas(0, measure_passes(ms))
-                    reps = L.run_tran(self.topts, steps_per_launch=2048)
+                    passes = measure_passes(ms)
+                    L.set_meas(0, passes)
+                    if self.early_stop and passes:
+                        reps = self._run_early_stop(L)
+                    else:
+                        reps = L.run_tran(self.topts, steps_per_launch=2048)
                     value, _ = L.get_meas(0)
-            out, reasons = point_measures(ms, value, names, reports=reps, op=op, x_op=x_op)
+            out, reasons = point_measures(ms, value, names, reports=reps, op=op, x_op=x_op,
+                                          stopped_ok=self.early_stop)
             for i, k in enumerate(ids):
                 self.values[k] = out[i]
                 self.reasons[k] = int(reasons[i])
                 self.state[k] = 1
+
+    def _run_early_stop(self, L, steps_per_launch: int = 512, max_launches: int = 100000):
+        """The transient in launches of `steps_per_launch` steps; between
+        launches every lane whose passes have all resolved is stopped."""
+        L.init_steps(self.topts)
+        reps = None
+        for _ in range(max_launches):
+            reps = L.device_launch(steps_per_launch)
+            if all(r.status != 0 for r in reps):
+                break
+            done = L.meas_done(0).all(axis=1)
+            if done.any():
+                L.request_stop(0, done)
+        return reps
 
     def copy_point_measures(self, first_id: int, count: int, names: Sequence[str]):
         """(values [count][len(names)], reasons [count]) of the points from

@@ -316,6 +316,15 @@ typedef struct {
 } espl_meas;
 espl_status espl_set_meas(espl_lanes *h, uint32_t net, const espl_meas *passes, uint32_t n);
 espl_status espl_get_meas(espl_lanes *h, uint32_t net, double *value, double *at);
+/* done[lane][pass] = 1 where a pass has read its last sample (its result
+ * can no longer change), between launches. */
+espl_status espl_meas_done(espl_lanes *h, uint32_t net, uint8_t *done);
+/* Stops every lane l of template `net` with stop[l] != 0 that is still
+ * stepping before the next espl_device_launch (its report then says 4,
+ * stopped); lanes already done keep their status (the reference's
+ * GpuLanes.requestStop, src/analysis/gpu/lanes.zig:2059-2064). With
+ * espl_meas_done this ends a lane's transient once its measures resolve. */
+espl_status espl_request_stop(espl_lanes *h, uint32_t net, const uint8_t *stop);
 
 /* Timing of the last solve/launch, milliseconds of device time per kernel
  * family (CUDA events on the launching stream), for roofline reporting. */

@@ -152,3 +152,17 @@ def test_param_measures():
                                                                ".meas tran t50 when v(out)=half")
     with pytest.raises(DeckError, match="unknown parameter 't50'"):
         read_measures(later, net, params={"rval": r})
+
+
+def test_stopped_lanes_count_as_done_only_when_asked():
+    from types import SimpleNamespace as R
+
+    from egspice_b200 import netlist as nl
+    net, r = _rc()
+    ms = read_measures(RC_DECK, net, params={"rval": r})
+    value = np.ones((2, len(measure_passes(ms))))
+    reports = [R(status=4), R(status=1)]
+    _, reasons = nl.point_measures(ms, value, ["t50"], reports=reports)
+    assert list(reasons) == [nl.REASON_OTHER, nl.REASON_OK]
+    _, reasons = nl.point_measures(ms, value, ["t50"], reports=reports, stopped_ok=True)
+    assert list(reasons) == [nl.REASON_OK, nl.REASON_OK]

@@ -574,3 +574,56 @@ r2 mid 0 10k
     assert (r == 0).all()
     np.testing.assert_allclose(v[:, 0], 1.8 * 1e4 / (rtop + 1e4), rtol=1e-9)
     np.testing.assert_allclose(v[:, 1], -1.8 / (rtop + 1e4), rtol=1e-9)
+
+
+def test_early_stop():
+    """espl_meas_done / espl_request_stop: RC lanes whose measures all
+    resolve early stop there (report status 4 before t_stop) with the same
+    measures as the full run; the points layer's early_stop gives the same
+    values and reasons as without it."""
+    from egspice_b200 import points as pt
+    from egspice_b200.netlist import measure_passes, read_deck, read_measures
+    deck = """RC points
+vin in 0 dc 0 pulse(0 1 0 0.2n 0.2n 1 2)
+r1 in out {rval}
+c1 out 0 1p
+.param rval=1k
+.tran 1p 20n
+.meas tran t50 when v(out)=0.5
+.meas tran rise trig v(out) val=0.1 rise=1 targ v(out) val=0.9 rise=1
+.end
+"""
+    rval = np.linspace(0.5e3, 1.5e3, 40)
+    params = {"rval": rval}
+    net = read_deck(deck, lanes=40, params=params)
+    passes = measure_passes(read_measures(deck, net, params=params))
+    opts = pt.Points(deck, ["rval"]).topts
+    with Lanes([net]) as L:
+        L.set_meas(0, passes)
+        full = L.run_tran(opts, steps_per_launch=2048)
+        v_full, _ = L.get_meas(0)
+    with Lanes([net]) as L:
+        L.set_meas(0, passes)
+        L.init_steps(opts)
+        reps = None
+        for _ in range(1000):
+            reps = L.device_launch(256)
+            if all(r.status != 0 for r in reps):
+                break
+            done = L.meas_done(0).all(axis=1)
+            if done.any():
+                L.request_stop(0, done)
+        v_stop, _ = L.get_meas(0)
+    assert all(r.status == 1 for r in full)
+    assert all(r.status == 4 for r in reps) and max(r.t for r in reps) < opts.t_stop
+    # launches of 256 steps resume the same step sequence as launches of 2048
+    np.testing.assert_allclose(v_stop, v_full, rtol=1e-9)
+    a = pt.Points(deck, ["rval"])
+    b = pt.Points(deck, ["rval"], early_stop=True)
+    for p in (a, b):
+        p.append_points(rval[:, None])
+        p.run()
+    va, ra = a.copy_point_measures(0, 40, ["t50", "rise"])
+    vb, rb = b.copy_point_measures(0, 40, ["t50", "rise"])
+    np.testing.assert_allclose(va, vb, rtol=1e-9)
+    assert (ra == 0).all() and (rb == 0).all()
