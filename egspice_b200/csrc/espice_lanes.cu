@@ -1814,6 +1814,31 @@ espl_status espl_get_meas(espl_lanes* h, uint32_t net, double* value, double* at
     return ESPL_OK;
 }
 
+espl_status espl_meas_table(const espl_meas* passes, uint32_t n_passes, const double* x, const double* cols,
+                            uint32_t n_cols, uint32_t n, double* value, double* at) {
+    if ((n_passes && (!passes || !value || !at)) || (n && (!x || !cols)) || n_passes > ESPL_MEAS_MAX_PASSES)
+        return ESPL_INVALID_ARGUMENT;
+    for (uint32_t p = 0; p < n_passes; p++) {
+        const espl_meas& c = passes[p];
+        if (c.kind < ESPL_MEAS_WHEN || c.kind > ESPL_MEAS_TARG || c.row >= n_cols || c.level_row > n_cols)
+            return ESPL_INVALID_ARGUMENT;
+        if (meas_reads_previous(c.kind) && (p == 0 || passes[p - 1].kind != ESPL_MEAS_WHEN))
+            return ESPL_INVALID_ARGUMENT;
+    }
+    // the kernels' own measure code (lane_meas.cuh), one lane, stride 1
+    std::vector<double> st((size_t)n_passes * kMeasWords);
+    for (uint32_t p = 0; p < n_passes; p++) meas_init(passes[p], st.data() + (size_t)p * kMeasWords, 1);
+    for (uint32_t k = 0; k < n; k++)
+        for (uint32_t p = 0; p < n_passes; p++) {
+            const espl_meas& c = passes[p];
+            const double* row = cols + (size_t)k * n_cols;
+            meas_feed(c, st.data() + (size_t)p * kMeasWords, 1, p ? st.data() + (size_t)(p - 1) * kMeasWords : nullptr,
+                      x[k], row[c.row], c.level_row ? row[c.level_row - 1] : 0.0);
+        }
+    for (uint32_t p = 0; p < n_passes; p++) meas_result(passes[p], st.data() + (size_t)p * kMeasWords, 1, value[p], at[p]);
+    return ESPL_OK;
+}
+
 espl_status espl_meas_done(espl_lanes* h, uint32_t net, uint8_t* done) {
     if (!h || net >= h->groups.size() || !done) return ESPL_INVALID_ARGUMENT;
     Group& g = h->groups[net];

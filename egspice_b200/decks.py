@@ -113,6 +113,9 @@ class Netlist:
     sweep: Optional[np.ndarray] = None
     # The branch-current unknown of each named voltage source.
     branch_names: Dict[str, int] = dataclasses.field(default_factory=dict)
+    # Small-signal sources: ("v", branch row, mag, phase in degrees) or
+    # ("i", from row, to row, mag, phase), rows GROUND where grounded.
+    ac_sources: List[tuple] = dataclasses.field(default_factory=list)
 
     @property
     def nnz(self) -> int:
@@ -138,6 +141,7 @@ class Builder:
         self.devs: Dict[int, List[Tuple[List[str], np.ndarray]]] = {k: [] for k in TERMS}
         self.vsrc_names: List[str] = []
         self.vsrc_labels: Dict[str, str] = {}
+        self.ac: List[tuple] = []  # ("v", branch name, mag, ph) or ("i", p, n, mag, ph)
 
     def _lane(self, v) -> np.ndarray:
         a = np.asarray(v, dtype=np.float64)
@@ -169,16 +173,21 @@ class Builder:
     def m(self, d, g, s, b, typ, vto, kp, w, l, gamma=0.0, phi=0.6, lam=0.0, is_=1e-14):
         self.add(MOS1, [d, g, s, b], [typ, vto, kp, gamma, phi, lam, is_, w, l])
 
-    def v(self, p, n, dc=0.0, pulse=None, label=None):
+    def v(self, p, n, dc=0.0, pulse=None, label=None, ac=None):
         """pulse = (v1, v2, td, tr, tf, pw, per); `label` names the source
-        (its branch current is then Netlist.branch_names[label])."""
+        (its branch current is then Netlist.branch_names[label]); `ac` =
+        (magnitude, phase in degrees) of its small-signal value."""
         name = f"#br{len(self.vsrc_names)}"
         self.vsrc_names.append(name)
+        if ac is not None:
+            self.ac.append(("v", name, float(ac[0]), float(ac[1])))
         if label is not None:
             self.vsrc_labels[label] = name
         self.add(VSRC, [p, n, name], _src_params(dc, pulse))
 
-    def i(self, p, n, dc=0.0, pulse=None):
+    def i(self, p, n, dc=0.0, pulse=None, ac=None):
+        if ac is not None:
+            self.ac.append(("i", p, n, float(ac[0]), float(ac[1])))
         self.add(ISRC, [p, n], _src_params(dc, pulse))
 
     def freeze(self, sweep: Optional[np.ndarray] = None) -> Netlist:
@@ -215,8 +224,10 @@ class Builder:
             col_ptr[c + 1] = len(rows)
         node_names = {k: v for k, v in idx.items() if k != "0"}
         branches = {label: idx[br] for label, br in self.vsrc_labels.items()}
+        acs = [("v", idx[a[1]], a[2], a[3]) if a[0] == "v" else ("i", idx[a[1]], idx[a[2]], a[3], a[4])
+               for a in self.ac]
         return Netlist(self.name, n, col_ptr, np.array(rows, dtype=np.uint32), batches, self.lanes,
-                       node_names, cur, sweep, branches)
+                       node_names, cur, sweep, branches, acs)
 
 
 def _src_params(dc, pulse):

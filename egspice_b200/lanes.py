@@ -67,6 +67,9 @@ def lib():
         L.espl_ac_solve.restype = C.c_uint32
         L.espl_noise_sources.argtypes = [C.c_void_p, C.c_uint32, f64p, u32p]
         L.espl_noise_sources.restype = C.c_uint32
+        L.espl_meas_table.argtypes = [C.POINTER(MeasPass), C.c_uint32, f64p, f64p, C.c_uint32, C.c_uint32, f64p,
+                                      f64p]
+        L.espl_meas_table.restype = C.c_uint32
         L.espl_meas_done.argtypes = [C.c_void_p, C.c_uint32, C.POINTER(C.c_uint8)]
         L.espl_meas_done.restype = C.c_uint32
         L.espl_request_stop.argtypes = [C.c_void_p, C.c_uint32, C.POINTER(C.c_uint8)]
@@ -86,6 +89,22 @@ def lib():
 
 
 PRECISION = {"fp64": abi.ESPL_FP64, "mixed": abi.ESPL_MIXED}
+
+
+def meas_table(passes: Sequence[MeasPass], xs, cols):
+    """The measure passes over a host table (espl_meas_table): cols[k, u]
+    is column u at scale xs[k]. Returns (value, at), one per pass."""
+    xs = np.ascontiguousarray(xs, dtype=np.float64)
+    cols = np.ascontiguousarray(np.atleast_2d(cols), dtype=np.float64)
+    n = len(passes)
+    arr = (MeasPass * max(n, 1))(*passes)
+    val = np.full(max(n, 1), np.nan)
+    at = np.full(max(n, 1), np.nan)
+    st = lib().espl_meas_table(arr, n, xs.ctypes.data_as(f64p), cols.ctypes.data_as(f64p), cols.shape[1], len(xs),
+                               val.ctypes.data_as(f64p), at.ctypes.data_as(f64p))
+    if st != 0:
+        raise LaneError(f"espl_meas_table failed with status {st}")
+    return val[:n], at[:n]
 
 
 def noise_terminals(net: Netlist) -> np.ndarray:

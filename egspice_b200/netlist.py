@@ -7,7 +7,7 @@ src/frontend/netlist.zig `parse` and `Circuit.freeze`), as an
 the lanes carry:
 
 * R, C            ``Rname n1 n2 value``
-* V, I            ``Vname n+ n- [DC] value [PULSE(v1 v2 td tr tf pw per)]``
+* V, I            ``Vname n+ n- [DC] value [PULSE(v1 v2 td tr tf pw per)] [AC mag [phase]]``
 * D               ``Dname anode cathode model``
 * M (level 1)     ``Mname d g s b model [W=value] [L=value]``
 * ``.model name nmos|pmos|d (params)`` — MOS: LEVEL=1, VTO, KP, GAMMA, PHI,
@@ -19,10 +19,10 @@ the lanes carry:
   over numbers, parameters, + - * / ** and parentheses
 * ``+`` continuation lines, ``*`` comment lines, ``;`` and ``$ `` inline
   comments; the first line is the title; ``.end`` ends the deck; analysis
-  cards (.op .tran .dc .option .options .temp .print .save .probe) are
-  accepted and ignored (the caller runs the analysis through the API);
-  ``.meas tran`` cards are read by `read_measures` into the lanes' streaming
-  measure passes.
+  cards (.op .tran .ac .dc .option .options .temp .print .save .probe) are
+  accepted and ignored (the caller runs the analysis through the API;
+  egspice_b200.points reads .op, .tran and .ac); ``.meas tran``, ``.meas
+  ac`` and ``.meas op`` cards are read by `read_measures`.
 
 Per-lane values: `params` maps parameter names to a scalar or to an array of
 one value per lane (a Monte Carlo draw or a sweep); they override `.param`
@@ -217,7 +217,7 @@ def _split(card: str) -> List[str]:
     return toks
 
 
-_IGNORED = {".op", ".tran", ".dc", ".option", ".options", ".temp", ".meas", ".measure", ".print", ".save",
+_IGNORED = {".op", ".tran", ".ac", ".dc", ".option", ".options", ".temp", ".meas", ".measure", ".print", ".save",
             ".probe", ".plot", ".control", ".endc", ".title"}
 _MOS_DEFAULTS = dict(level=1.0, vto=0.0, kp=2e-5, gamma=0.0, phi=0.6, lambda_=0.0, is_=1e-14, tox=0.0, rd=0.0,
                      rs=0.0)
@@ -365,13 +365,22 @@ def read_deck(text: str, lanes: int = 1, params: Optional[Mapping[str, Value]] =
         return mtype, vals
 
     def source(toks: List[str], where: str) -> tuple:
-        dc, pulse = 0.0, None
+        dc, pulse, ac = 0.0, None, None
         i = 0
         while i < len(toks):
             t = toks[i]
             if t == "dc":
                 dc = env.value(toks[i + 1], where)
                 i += 2
+            elif t == "ac":
+                # AC magnitude [phase in degrees], the same on every lane
+                vals = []
+                for u in toks[i + 1:i + 3]:
+                    if parse_number(u) is None and u not in env.vals and not u.startswith(("{", "'")):
+                        break
+                    vals.append(_scalar(env, u, where))
+                ac = (vals[0] if vals else 1.0, vals[1] if len(vals) > 1 else 0.0)
+                i += 1 + len(vals)
             elif t.startswith("pulse"):
                 body = t[len("pulse"):].strip()
                 if not body.startswith("("):
@@ -383,12 +392,12 @@ def read_deck(text: str, lanes: int = 1, params: Optional[Mapping[str, Value]] =
                 if len(vals) != 7:
                     raise DeckError(f"{where}: PULSE needs all seven values (v1 v2 td tr tf pw per)")
                 pulse = tuple(vals)
-            elif t.startswith(("sin", "exp", "pwl", "sffm", "am", "ac")):
-                raise DeckError(f"{where}: only DC and PULSE sources ride the lanes")
+            elif t.startswith(("sin", "exp", "pwl", "sffm", "am")):
+                raise DeckError(f"{where}: only DC and PULSE sources (and an AC value) ride the lanes")
             else:
                 dc = env.value(t, where)
                 i += 1
-        return dc, pulse
+        return dc, pulse, ac
 
     for ln, card in cards:
         toks = _split(card)
@@ -412,11 +421,11 @@ def read_deck(text: str, lanes: int = 1, params: Optional[Mapping[str, Value]] =
         elif kind in "vi":
             if len(toks) < 3:
                 raise DeckError(f"{where}: a source needs two nodes")
-            dc, pulse = source(toks[3:], where)
+            dc, pulse, ac = source(toks[3:], where)
             if kind == "v":
-                b.v(node(toks[1]), node(toks[2]), dc=dc, pulse=pulse, label=head)
+                b.v(node(toks[1]), node(toks[2]), dc=dc, pulse=pulse, label=head, ac=ac)
             else:
-                b.i(node(toks[1]), node(toks[2]), dc=dc, pulse=pulse)
+                b.i(node(toks[1]), node(toks[2]), dc=dc, pulse=pulse, ac=ac)
         elif kind == "d":
             if len(toks) != 4:
                 raise DeckError(f"{where}: D needs two nodes and a model")
@@ -468,6 +477,11 @@ class Measure:
     op_row: Optional[int] = None
     expr: Optional[str] = None
     params: Optional[Dict[str, Value]] = None
+    # `.meas ac`: its passes read `columns`, each (form, unknown) with form
+    # m (magnitude), db (20 log10 |.|), p (phase, radians), r or i (real or
+    # imaginary part) of the AC solution over frequency.
+    analysis: str = "tran"
+    columns: Optional[List[tuple]] = None
 
 
 _COUNTS = ("rise", "fall", "cross")
@@ -526,31 +540,34 @@ def _clause(toks: List[str], net: Netlist, env: _Env, where: str, opts_ok: Seque
     return out
 
 
-def _when(test: str, net: Netlist, env: _Env, where: str) -> Dict[str, object]:
-    """`vec=value` or `vec=vec2` of a WHEN: the pass's row and its level."""
+def _when(test: str, net: Netlist, env: _Env, where: str, vec=None) -> Dict[str, object]:
+    """`vec=value` or `vec=vec2` of a WHEN: the pass's row and its level;
+    `vec` resolves a vector token (default: an unknown of `net`)."""
+    vec = vec or (lambda t: _vector(t, net, where))
     if "=" not in test:
         raise DeckError(f"{where}: WHEN needs vector=value")
     lhs, rhs = test.split("=", 1)
-    row = _vector(lhs, net, where)
-    if re.fullmatch(r"[vi]\([^()]*\)", rhs):
-        return {"row": row, "level_row": _vector(rhs, net, where)}
+    row = vec(lhs)
+    if re.fullmatch(r"[a-z]+\([^()]*\)", rhs):
+        return {"row": row, "level_row": vec(rhs)}
     return {"row": row, "val": _scalar(env, rhs, where)}
 
 
-def _measure(name: str, func: str, rest: List[str], net: Netlist, env: _Env, where: str) -> Measure:
+def _measure(name: str, func: str, rest: List[str], net: Netlist, env: _Env, where: str, vec=None) -> Measure:
+    vec = vec or (lambda t: _vector(t, net, where))
     M = abi.meas_pass
     window = ("from", "to")
     counts_td = _COUNTS + ("td",)
     if func == "when":
         if not rest:
             raise DeckError(f"{where}: WHEN needs vector=value")
-        w = _when(rest[0], net, env, where)
+        w = _when(rest[0], net, env, where, vec)
         o = _clause(rest[1:], net, env, where, counts_td + window)
         return Measure(name, [M(abi.MEAS_WHEN, w.pop("row"), **w, **o)])
     if func in ("find", "deriv"):
         if len(rest) < 2:
             raise DeckError(f"{where}: {func.upper()} needs a vector and AT= or WHEN")
-        row = _vector(rest[0], net, where)
+        row = vec(rest[0])
         if rest[1].startswith("at="):
             if len(rest) > 2:
                 raise DeckError(f"{where}: {func.upper()} ... AT takes no other option")
@@ -558,7 +575,7 @@ def _measure(name: str, func: str, rest: List[str], net: Netlist, env: _Env, whe
             return Measure(name, [M(kind, row, at=_scalar(env, rest[1][3:], where))])
         if rest[1] != "when" or len(rest) < 3:
             raise DeckError(f"{where}: {func.upper()} needs AT= or WHEN vector=value")
-        w = _when(rest[2], net, env, where)
+        w = _when(rest[2], net, env, where, vec)
         o = _clause(rest[3:], net, env, where, counts_td + window)
         kind = abi.MEAS_FIND_WHEN if func == "find" else abi.MEAS_DERIV_WHEN
         return Measure(name, [M(abi.MEAS_WHEN, w.pop("row"), **w, **o), M(kind, row)])
@@ -571,7 +588,7 @@ def _measure(name: str, func: str, rest: List[str], net: Netlist, env: _Env, whe
         for part, kind in ((trig, abi.MEAS_WHEN), (targ, abi.MEAS_TARG)):
             if not part or part[0].startswith("at="):
                 raise DeckError(f"{where}: TRIG/TARG AT= is outside what the lanes carry; give a vector and VAL=")
-            row = _vector(part[0], net, where)
+            row = vec(part[0])
             o = _clause(part[1:], net, env, where, ("val",) + counts_td + window)
             if kind == abi.MEAS_TARG:
                 o.pop("td", None)  # the TARG counts from the TRIG event
@@ -582,7 +599,7 @@ def _measure(name: str, func: str, rest: List[str], net: Netlist, env: _Env, whe
     if func in stats or func == "pp":
         if not rest:
             raise DeckError(f"{where}: {func.upper()} needs a vector")
-        row = _vector(rest[0], net, where)
+        row = vec(rest[0])
         o = _clause(rest[1:], net, env, where, window)
         if func == "pp":
             return Measure(name, [M(abi.MEAS_MAX, row, **o), M(abi.MEAS_MIN, row, **o)], pp=True)
@@ -620,8 +637,27 @@ def read_measures(text: str, net: Netlist, params: Optional[Mapping[str, Value]]
                 raise DeckError(f"{where}: .meas op takes FIND vector")
             out.append(Measure(name, [], op_row=_vector(toks[4], net, where)))
             continue
+        if toks[1] == "ac":
+            columns: List[tuple] = []
+
+            def acvec(tok, where=where, columns=columns):
+                m = re.fullmatch(r"(v|vm|vdb|vp|vr|vi|i|im|idb|ip|ir|ii)\(([^(),]+)\)", tok)
+                if not m:
+                    raise DeckError(f"{where}: the AC measure reads {tok!r}; only v/vm/vdb/vp/vr/vi(node) and "
+                                    "i/im/idb/ip/ir/ii(vsource) ride the lanes")
+                f, nm = m.group(1), m.group(2).strip()
+                row = _vector(f[0] + "(" + nm + ")", net, where)
+                key = ("m" if len(f) == 1 else f[1:], row)
+                if key not in columns:
+                    columns.append(key)
+                return columns.index(key)
+
+            mm = _measure(name, toks[3], toks[4:], net, env, where, vec=acvec)
+            mm.analysis, mm.columns = "ac", columns
+            out.append(mm)
+            continue
         if toks[1] != "tran":
-            raise DeckError(f"{where}: only .meas tran and .meas op ride the lanes")
+            raise DeckError(f"{where}: only .meas tran, ac and op ride the lanes")
         if toks[3].startswith("param="):
             if len(toks) != 4:
                 raise DeckError(f"{where}: PARAM takes one expression")
@@ -638,17 +674,18 @@ def read_measures(text: str, net: Netlist, params: Optional[Mapping[str, Value]]
 
 def measure_passes(measures: Sequence[Measure]) -> List[abi.MeasPass]:
     """Every measure's passes, in order, for Lanes.set_meas."""
-    passes = [p for m in measures for p in m.passes]
+    passes = [p for m in measures if m.analysis == "tran" for p in m.passes]
     if len(passes) > abi.MEAS_MAX_PASSES:
         raise DeckError(f"the measures need {len(passes)} passes; a template takes {abi.MEAS_MAX_PASSES}")
     return passes
 
 
-def measure_values(measures: Sequence[Measure], value: np.ndarray,
-                   x_op: Optional[np.ndarray] = None) -> Dict[str, np.ndarray]:
+def measure_values(measures: Sequence[Measure], value: np.ndarray, x_op: Optional[np.ndarray] = None,
+                   ac: Optional[Mapping[str, np.ndarray]] = None) -> Dict[str, np.ndarray]:
     """Each measure's value per lane from Lanes.get_meas's `value` [lanes,
     passes] (NaN where it has none); `.meas op` cards read the operating
-    points x_op [lanes, n] (NaN without them)."""
+    points x_op [lanes, n], `.meas ac` cards their values in `ac` (NaN
+    without them)."""
     out: Dict[str, np.ndarray] = {}
     k = 0
     lanes = value.shape[0]
@@ -663,6 +700,9 @@ def measure_values(measures: Sequence[Measure], value: np.ndarray,
             continue
         if m.op_row is not None:
             out[m.name] = x_op[:, m.op_row].copy() if x_op is not None else np.full(value.shape[0], np.nan)
+            continue
+        if m.analysis == "ac":
+            out[m.name] = np.asarray(ac[m.name]) if ac and m.name in ac else np.full(lanes, np.nan)
             continue
         if m.pp:
             out[m.name] = value[:, k] - value[:, k + 1]
@@ -684,7 +724,8 @@ REASON_OTHER = 255
 
 def point_measures(measures: Sequence[Measure], value: np.ndarray, names: Optional[Sequence[str]] = None,
                    reports: Optional[Sequence] = None, op: Optional[np.ndarray] = None,
-                   x_op: Optional[np.ndarray] = None, stopped_ok: bool = False):
+                   x_op: Optional[np.ndarray] = None, stopped_ok: bool = False,
+                   ac: Optional[Mapping[str, np.ndarray]] = None):
     """Each lane's measures and reason as the reference's points API copies
     them (include/espice.h espice_copy_point_measures :324-338): values
     [lanes][len(names)] (names case-insensitive, default every measure in
@@ -697,7 +738,7 @@ def point_measures(measures: Sequence[Measure], value: np.ndarray, names: Option
     `.meas op` cards read x_op, the operating points [lanes, n]. With
     `stopped_ok` a transient stopped on request (status 4, an early stop
     once its measures resolved) counts as done."""
-    allv = measure_values(measures, value, x_op)
+    allv = measure_values(measures, value, x_op, ac)
     keys = {k.lower(): k for k in allv}
     if names is None:
         names = list(allv)

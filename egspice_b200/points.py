@@ -37,9 +37,9 @@ class PointsError(RuntimeError):
         self.status, self.name = status, name
 
 
-def _tran_card(text: str):
+def _tran_card(text: str, allow_none: bool = False):
     """(tstep, tstop, tmax) of the deck's one .tran card, or None for a deck
-    whose one analysis is .op."""
+    whose analyses are .op (or, with allow_none, .ac)."""
     found = None
     has_op = False
     for ln, card in _logical_lines(text):
@@ -61,9 +61,77 @@ def _tran_card(text: str):
             raise DeckError(f"line {ln}: a nonzero tstart is outside what the lanes carry")
         tmax = vals[3] if len(vals) > 3 else None
         found = (vals[0], vals[1], tmax)
-    if found is None and not has_op:
+    if found is None and not has_op and not allow_none:
         raise DeckError("the deck has neither a .tran nor an .op card")
     return found
+
+
+def ac_frequencies(text: str) -> Optional[np.ndarray]:
+    """The frequencies (Hz) of the deck's `.ac dec|oct|lin n fstart fstop`
+    card as ngspice steps them (dec/oct: fstart times 10^(1/n) or 2^(1/n)
+    repeatedly while at most fstop; lin: n points from fstart to fstop), or
+    None without one."""
+    found = None
+    for ln, card in _logical_lines(text):
+        toks = _split(card)
+        if toks[0] != ".ac":
+            continue
+        if found is not None:
+            raise DeckError(f"line {ln}: a second .ac card")
+        vals = [parse_number(t) for t in toks[2:5]]
+        if len(toks) != 5 or toks[1] not in ("dec", "oct", "lin") or any(v is None for v in vals):
+            raise DeckError(f"line {ln}: .ac needs dec|oct|lin, a count, fstart and fstop")
+        n, f0, f1 = int(vals[0]), vals[1], vals[2]
+        if n < 1 or not (0 < f0 <= f1):
+            raise DeckError(f"line {ln}: .ac needs a count from 1 and 0 < fstart <= fstop")
+        if toks[1] == "lin":
+            found = np.linspace(f0, f1, n)
+        else:
+            step = (10.0 if toks[1] == "dec" else 2.0) ** (1.0 / n)
+            fs = [f0]
+            while fs[-1] * step <= f1 * (1 + 1e-12):
+                fs.append(fs[-1] * step)
+            found = np.array(fs)
+    return found
+
+
+def ac_rhs(net) -> np.ndarray:
+    """The small-signal excitation b of the deck's AC sources: a voltage
+    source's branch row gets mag e^{j ph}; a current source from p to n adds
+    -mag e^{j ph} at p and +mag e^{j ph} at n (it leaves p)."""
+    from .decks import GROUND
+    b = np.zeros(net.n, dtype=complex)
+    for a in net.ac_sources:
+        if a[0] == "v":
+            b[a[1]] += a[2] * np.exp(1j * np.deg2rad(a[3]))
+        else:
+            v = a[3] * np.exp(1j * np.deg2rad(a[4]))
+            if a[1] != GROUND:
+                b[a[1]] -= v
+            if a[2] != GROUND:
+                b[a[2]] += v
+    return b
+
+
+def ac_measure_values(measures: Sequence, freqs: np.ndarray, z: np.ndarray) -> Dict[str, np.ndarray]:
+    """Each `.meas ac` card's value per lane from the AC solution z
+    [lanes, F, n] at `freqs`: its columns (magnitude, dB, phase, real or
+    imaginary part of an unknown) over frequency through the lanes' measure
+    passes on the host (espl_meas_table)."""
+    from .lanes import meas_table
+    out: Dict[str, np.ndarray] = {}
+    forms = {"m": np.abs, "db": lambda v: 20.0 * np.log10(np.abs(v)), "p": np.angle, "r": np.real, "i": np.imag}
+    for m in measures:
+        if m.analysis != "ac":
+            continue
+        vals = np.full(z.shape[0], np.nan)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            table = np.stack([forms[f](z[:, :, row]) for f, row in m.columns], axis=2)  # [lanes, F, cols]
+        for l in range(z.shape[0]):
+            v, _ = meas_table(m.passes, freqs, table[l])
+            vals[l] = v[0] - v[1] if m.pp else v[-1]
+        out[m.name] = vals
+    return out
 
 
 class Points:
@@ -85,7 +153,8 @@ class Points:
         self.early_stop = early_stop
         self.live = [p.lower() for p in live_params]
         self.precision = precision
-        card = _tran_card(text)
+        self.freqs = ac_frequencies(text)
+        card = _tran_card(text, allow_none=self.freqs is not None)
         self.topts = None
         if card is not None:
             tstep, tstop, tmax = card
@@ -100,7 +169,12 @@ class Points:
         self.measures = read_measures(text, probe, params=probe_params)
         if self.topts is None and measure_passes(self.measures):
             raise DeckError("a .meas tran card needs the deck's .tran card")
-        self.need_op = self.topts is None or any(m.op_row is not None for m in self.measures)
+        if any(m.analysis == "ac" for m in self.measures) and self.freqs is None:
+            raise DeckError("a .meas ac card needs the deck's .ac card")
+        if self.freqs is not None and not probe.ac_sources:
+            raise DeckError("the .ac analysis needs a source with an AC value")
+        self.need_op = (self.topts is None or self.freqs is not None
+                        or any(m.op_row is not None for m in self.measures))
         self.rows: List[np.ndarray] = []     # each point's values
         self.state: List[int] = []           # 0 pending, 1 complete, 2 released
         self.values: Dict[int, np.ndarray] = {}
@@ -153,7 +227,7 @@ class Points:
             params = {p: block[:, j] for j, p in enumerate(self.live)}
             net = read_deck(self.text, lanes=len(ids), params=params)
             ms = read_measures(self.text, net, params=params)
-            op = x_op = reps = None
+            op = x_op = reps = ac = None
             value = np.zeros((len(ids), 0))
             with Lanes([net], precision=self.precision) as L:
                 if self.need_op:
@@ -167,8 +241,13 @@ class Points:
                     else:
                         reps = L.run_tran(self.topts, steps_per_launch=2048)
                     value, _ = L.get_meas(0)
+                if self.freqs is not None:
+                    # the AC sweep at the operating point solve_op left in x
+                    L.put_x(0, x_op, False)
+                    z = L.ac_solve(0, 2 * np.pi * self.freqs, ac_rhs(net)[None, :], np.arange(net.n))[:, :, 0, :]
+                    ac = ac_measure_values(ms, self.freqs, z)
             out, reasons = point_measures(ms, value, names, reports=reps, op=op, x_op=x_op,
-                                          stopped_ok=self.early_stop)
+                                          stopped_ok=self.early_stop, ac=ac)
             for i, k in enumerate(ids):
                 self.values[k] = out[i]
                 self.reasons[k] = int(reasons[i])

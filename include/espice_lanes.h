@@ -316,6 +316,12 @@ typedef struct {
 } espl_meas;
 espl_status espl_set_meas(espl_lanes *h, uint32_t net, const espl_meas *passes, uint32_t n);
 espl_status espl_get_meas(espl_lanes *h, uint32_t net, double *value, double *at);
+/* The same passes over a table on the host, for measures of results the
+ * host already holds (an AC sweep's magnitudes, a DC sweep): sample k has
+ * scale x[k] and columns cols[k * n_cols + u]; a pass reads column `row`
+ * (and level column level_row - 1). value/at are [n_passes]. */
+espl_status espl_meas_table(const espl_meas *passes, uint32_t n_passes, const double *x, const double *cols,
+                            uint32_t n_cols, uint32_t n, double *value, double *at);
 /* done[lane][pass] = 1 where a pass has read its last sample (its result
  * can no longer change), between launches. */
 espl_status espl_meas_done(espl_lanes *h, uint32_t net, uint8_t *done);

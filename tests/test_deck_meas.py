@@ -78,7 +78,7 @@ def test_rc_measures_against_the_analytic_response(oracle):
 
 
 @pytest.mark.parametrize("card,msg", [
-    (".meas ac g1 max v(out)", "only .meas tran"),
+    (".meas dc g1 max v(out)", "only .meas tran"),
     (".meas tran d1 find v(out,in) at=1n", "only v\\(node\\)"),
     (".meas tran d2 trig at=1n targ v(out) val=0.5 rise=1", "AT= is outside"),
     (".meas tran d3 when v(out)=0.5 rise=1 fall=1", "one of RISE"),

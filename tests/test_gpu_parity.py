@@ -627,3 +627,43 @@ c1 out 0 1p
     vb, rb = b.copy_point_measures(0, 40, ["t50", "rise"])
     np.testing.assert_allclose(va, vb, rtol=1e-9)
     assert (ra == 0).all() and (rb == 0).all()
+
+
+def test_points_ac_measures(oracle):
+    """An .ac deck as points: the operating point, the lanes' AC solve of
+    the AC sources' excitation, and `.meas ac` cards (a -3 dB bandwidth, a
+    gain at a frequency, a phase at an event, a peak) against the same
+    measures of the oracle's dense AC solves, and the bandwidth against the
+    RC's analytic 3 dB point."""
+    import math
+
+    from egspice_b200 import points as pt
+    from egspice_b200.netlist import read_deck, read_measures
+    deck = """RC AC
+vin in 0 dc 0 ac 1
+r1 in out {rval}
+c1 out 0 1p
+.param rval=1k
+.ac dec 50 1meg 10g
+.meas ac bw when vdb(out)=-3 fall=1
+.meas ac g1m find vdb(out) at=1meg
+.meas ac ph find vp(out) when vdb(out)=-3
+.meas ac peak max vm(out)
+.end
+"""
+    r = np.linspace(0.5e3, 2e3, 20)
+    p = pt.Points(deck, ["rval"])
+    p.append_points(r[:, None])
+    p.run()
+    names = ["bw", "g1m", "ph", "peak"]
+    v, reasons = p.copy_point_measures(0, 20, names)
+    assert (reasons == 0).all()
+    net = read_deck(deck, lanes=20, params={"rval": r})
+    ms = read_measures(deck, net, params={"rval": r})
+    x = np.zeros((20, net.n))
+    z = oracle.ac_solve_lanes(net, x, 2 * np.pi * p.freqs, pt.ac_rhs(net)[None, :], np.arange(net.n))[:, :, 0, :]
+    want = pt.ac_measure_values(ms, p.freqs, z)
+    for j, name in enumerate(names):
+        np.testing.assert_allclose(v[:, j], want[name], rtol=1e-8, atol=1e-12, err_msg=name)
+    f3 = math.sqrt(10 ** 0.3 - 1) / (2 * np.pi * r * 1e-12)
+    np.testing.assert_allclose(v[:, 0], f3, rtol=2e-3)

@@ -170,3 +170,25 @@ def test_device_passes_match_the_oracle_bitwise(oracle, device_meas):
             resolved[p.kind] += not math.isnan(v)
     # every kind produced values, not only NaNs that trivially agree
     assert min(resolved.values()) >= 20, resolved
+
+
+def test_library_host_table_matches_the_oracle(oracle):
+    """espl_meas_table, the product's host entry running the kernels' measure
+    code over a table (AC sweeps use it), bit for bit against the oracle."""
+    from egspice_b200.lanes import meas_table
+    rng = np.random.default_rng(7)
+    chained = (abi.MEAS_FIND_WHEN, abi.MEAS_DERIV_WHEN, abi.MEAS_TARG)
+    plain = (abi.MEAS_WHEN, abi.MEAS_FIND_AT, abi.MEAS_DERIV_AT, abi.MEAS_MIN, abi.MEAS_MAX, abi.MEAS_AVG,
+             abi.MEAS_INTEG, abi.MEAS_RMS)
+    for _ in range(100):
+        t, cols = _random_table(rng)
+        passes = []
+        while len(passes) < 8:
+            kind = int(rng.choice(plain))
+            passes.append(_random_pass(rng, kind, t, cols))
+            if kind == abi.MEAS_WHEN:
+                passes.append(_random_pass(rng, int(rng.choice(chained)), t, cols))
+        ov, oa = po.meas_table(passes, t, cols)
+        lv, la = meas_table(passes, t, cols)
+        np.testing.assert_array_equal(lv, ov)
+        np.testing.assert_array_equal(la, oa)
