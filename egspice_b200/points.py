@@ -14,6 +14,7 @@ first_id + k. Errors raise PointsError carrying the reference's status code
 and diagnostic name."""
 from __future__ import annotations
 
+import os
 from typing import Dict, List, Mapping, Optional, Sequence
 
 import numpy as np
@@ -148,8 +149,10 @@ class Points:
     the operating point solved the same way before the transient."""
 
     def __init__(self, text: str, live_params: Sequence[str], precision: str = "fp64",
-                 tran: Optional[Mapping[str, float]] = None, early_stop: bool = False):
+                 tran: Optional[Mapping[str, float]] = None, early_stop: bool = False, device: Optional[int] = None):
         self.text = text
+        # the GPU this process runs its points on (default: LOCAL_RANK under torchrun, else 0)
+        self.device = int(os.environ.get("LOCAL_RANK", "0")) if device is None else device
         self.early_stop = early_stop
         self.live = [p.lower() for p in live_params]
         self.precision = precision
@@ -216,20 +219,47 @@ class Points:
                 self.reasons[k] = reason
         return first
 
-    def run(self) -> None:
-        """Runs every pending point on the GPU lanes, lane_width() at a time."""
-        from .lanes import Lanes
+    def run(self, group=None) -> None:
+        """Runs every pending point on the GPU lanes, lane_width() at a time.
+        Under torch.distributed (one process per GPU), the pending points
+        split into contiguous slices, one per rank of `group`, each rank runs
+        its slice on its own GPU, and every rank receives every result (no
+        collective touches the lanes: the exchange is of finished results)."""
         pending = [k for k, s in enumerate(self.state) if s == 0]
+        rank, world, dist = 0, 1, None
+        try:
+            import torch.distributed as td
+            if td.is_available() and td.is_initialized():
+                dist, rank, world = td, td.get_rank(group), td.get_world_size(group)
+        except ImportError:
+            pass
+        per = -(-len(pending) // world) if pending else 0
+        results = self._run_ids(pending[rank * per:(rank + 1) * per])
+        parts = [results]
+        if world > 1:
+            parts = [None] * world
+            dist.all_gather_object(parts, results, group=group)
+        for part in parts:
+            for k, (values, reason) in part.items():
+                self.values[k] = np.asarray(values, dtype=np.float64)
+                self.reasons[k] = int(reason)
+                self.state[k] = 1
+
+    def _run_ids(self, ids: Sequence[int]) -> Dict[int, tuple]:
+        """{id: (measure values in card order, reason)} of the points `ids`,
+        run as lane batches of at most lane_width() on this process's GPU."""
+        from .lanes import Lanes
         names = [m.name for m in self.measures]
-        for b0 in range(0, len(pending), LANE_WIDTH):
-            ids = pending[b0:b0 + LANE_WIDTH]
-            block = np.stack([self.rows[k] for k in ids])
+        done: Dict[int, tuple] = {}
+        for b0 in range(0, len(ids), LANE_WIDTH):
+            batch = list(ids[b0:b0 + LANE_WIDTH])
+            block = np.stack([self.rows[k] for k in batch])
             params = {p: block[:, j] for j, p in enumerate(self.live)}
-            net = read_deck(self.text, lanes=len(ids), params=params)
+            net = read_deck(self.text, lanes=len(batch), params=params)
             ms = read_measures(self.text, net, params=params)
             op = x_op = reps = ac = None
-            value = np.zeros((len(ids), 0))
-            with Lanes([net], precision=self.precision) as L:
+            value = np.zeros((len(batch), 0))
+            with Lanes([net], precision=self.precision, device=self.device) as L:
                 if self.need_op:
                     op = L.solve_op(abi.newton_opts())
                     x_op = L.get_x(0)
@@ -248,10 +278,9 @@ class Points:
                     ac = ac_measure_values(ms, self.freqs, z)
             out, reasons = point_measures(ms, value, names, reports=reps, op=op, x_op=x_op,
                                           stopped_ok=self.early_stop, ac=ac)
-            for i, k in enumerate(ids):
-                self.values[k] = out[i]
-                self.reasons[k] = int(reasons[i])
-                self.state[k] = 1
+            for i, k in enumerate(batch):
+                done[k] = (out[i], int(reasons[i]))
+        return done
 
     def _run_early_stop(self, L, steps_per_launch: int = 512, max_launches: int = 100000):
         """The transient in launches of `steps_per_launch` steps; between

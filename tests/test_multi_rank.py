@@ -1,7 +1,9 @@
 """Multi-GPU sharding logic on CPU: two gloo ranks, each taking its slice of
 the lanes (devices.zig capacity split) with the same lead-lane tape, solved by
 the CPU oracle; the gathered result equals a single-process run lane for
-lane, so results do not depend on the rank count (multi.zig:1-5)."""
+lane, so results do not depend on the rank count (multi.zig:1-5); and the
+points layer's split of pending points across ranks with every rank
+receiving every result."""
 import os
 import socket
 import sys
@@ -71,3 +73,62 @@ def test_two_ranks_match_one(tmp_path):
     x1, _ = po.op_lanes(net, abi.newton_opts())
     assert allx.shape == x1.shape
     assert np.array_equal(allx, x1)
+
+
+def _points_worker(rank, world, port, out):
+    sys.path.insert(0, ROOT)
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    import datetime
+
+    import torch.distributed as dist
+
+    from egspice_b200 import points as pt
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    p = pt.Points(POINTS_DECK, ["rval"])
+    seen = []
+
+    def fake_run_ids(ids):  # stands in for the GPU run: a result that names its point
+        seen.extend(ids)
+        return {k: (np.array([p.rows[k][0], -float(k)]), k % 3) for k in ids}
+
+    p._run_ids = fake_run_ids
+    p.append_points(np.arange(1, 12, dtype=np.float64)[:, None] * 1e3)
+    p.append_points([[np.nan]])  # refused as appended: no rank runs it
+    p.run()
+    v, r = p.copy_point_measures(0, 12, ["t50", "v2n"])
+    ran = np.array(sorted(seen) + [-1] * (12 - len(seen)), dtype=np.float64)
+    np.save(out + f".{rank}.npy", np.concatenate([v, r[:, None], ran[:, None]], axis=1))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+POINTS_DECK = """RC points
+vin in 0 dc 0 pulse(0 1 0 0.2n 0.2n 1 2)
+r1 in out {rval}
+c1 out 0 1p
+.param rval=1k
+.tran 1p 6n
+.meas tran t50 when v(out)=0.5
+.meas tran v2n find v(out) at=2n
+.end
+"""
+
+
+def test_points_split_across_two_ranks(tmp_path):
+    """Points.run under torch.distributed (gloo, two ranks, the GPU run
+    replaced by a result naming its point): the 11 pending points split into
+    contiguous slices, one per rank, and both ranks end with every point's
+    result, equal to a one-process run."""
+    out = str(tmp_path / "p")
+    mp.spawn(_points_worker, args=(2, _free_port(), out), nprocs=2, join=True)
+    a, b = np.load(out + ".0.npy"), np.load(out + ".1.npy")
+    np.testing.assert_array_equal(a[:, :3], b[:, :3])
+    rows = np.arange(1, 12) * 1e3
+    np.testing.assert_array_equal(a[:11, 0], rows)
+    np.testing.assert_array_equal(a[:11, 1], -np.arange(11))
+    np.testing.assert_array_equal(a[:11, 2], np.arange(11) % 3)
+    assert np.isnan(a[11, :2]).all() and a[11, 2] == 9  # INVALID_PARAMETER
+    # rank 0 ran points 0..5, rank 1 points 6..10
+    np.testing.assert_array_equal(a[:6, 3], np.arange(6))
+    np.testing.assert_array_equal(b[:5, 3], np.arange(6, 11))
