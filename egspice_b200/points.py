@@ -15,6 +15,7 @@ and diagnostic name."""
 from __future__ import annotations
 
 import os
+import sys
 from typing import Dict, List, Mapping, Optional, Sequence
 
 import numpy as np
@@ -227,12 +228,9 @@ class Points:
         collective touches the lanes: the exchange is of finished results)."""
         pending = [k for k, s in enumerate(self.state) if s == 0]
         rank, world, dist = 0, 1, None
-        try:
-            import torch.distributed as td
-            if td.is_available() and td.is_initialized():
-                dist, rank, world = td, td.get_rank(group), td.get_world_size(group)
-        except ImportError:
-            pass
+        td = sys.modules.get("torch.distributed")  # a process group needs torch imported already
+        if td is not None and td.is_available() and td.is_initialized():
+            dist, rank, world = td, td.get_rank(group), td.get_world_size(group)
         per = -(-len(pending) // world) if pending else 0
         results = self._run_ids(pending[rank * per:(rank + 1) * per])
         parts = [results]
