@@ -192,3 +192,17 @@ def test_library_host_table_matches_the_oracle(oracle):
         lv, la = meas_table(passes, t, cols)
         np.testing.assert_array_equal(lv, ov)
         np.testing.assert_array_equal(la, oa)
+
+
+def test_library_host_table_refuses_bad_passes():
+    from egspice_b200.lanes import LaneError, meas_table
+    t, cols = _sines(1.0, 11)
+    for passes in ([M(abi.MEAS_FIND_WHEN, 0)],                              # no WHEN before it
+                   [M(abi.MEAS_MAX, 0), M(abi.MEAS_TARG, 0, val=0.1)],      # TARG after a non-WHEN
+                   [M(abi.MEAS_MAX, 2)],                                    # column out of range
+                   [M(abi.MEAS_WHEN, 0, level_row=2)],                      # level column out of range
+                   [M(99, 0)]):                                             # unknown kind
+        with pytest.raises(LaneError, match="status 1"):
+            meas_table(passes, t, cols)
+    v, a = meas_table([], t, cols)
+    assert v.size == 0 and a.size == 0
