@@ -37,7 +37,7 @@ ABI_VERSION = 2
 
 class CreateOpts(C.Structure):
     _fields_ = [("abi_version", C.c_uint32), ("precision", C.c_uint32), ("device", C.c_uint32),
-                ("lanes_per_cta", C.c_uint32), ("refine_sweeps", C.c_uint32), ("reserved", C.c_uint32)]
+                ("lanes_per_cta", C.c_uint32), ("refine_sweeps", C.c_uint32), ("polish", C.c_uint32)]
 
 
 class TranOpts(C.Structure):

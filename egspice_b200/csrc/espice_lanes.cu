@@ -22,6 +22,8 @@ using namespace espl;
 namespace {
 
 constexpr uint32_t kBlock = kTileThreads;
+// Polish iterations a lane may take after Newton's test passes.
+constexpr uint32_t kPolishMax = 4;
 // The banded streaming replay: widest band, largest L ring, chunk capacity.
 constexpr uint32_t kBandMax = 15, kBandLRing = 64, kBandWords = 1024, kBandEntries = 64;
 
@@ -110,6 +112,7 @@ struct espl_lanes {
     int device = 0;
     uint32_t precision = ESPL_FP64;
     uint32_t refine_sweeps = 0;
+    uint32_t polish = 0;  // espl_create_opts.polish: the tightened test's 10^-polish
     std::vector<Group> groups;
     uint32_t n_warps = 0, total_lanes = 0;
     GroupDev* d_groups = nullptr;
@@ -1004,7 +1007,8 @@ espl_status retape_stale(espl_lanes* h) {
     return clear_stale(h);
 }
 
-NewtonParams newton_params(const espl_newton_opts& o, uint32_t precision, uint32_t refine) {
+NewtonParams newton_params(const espl_newton_opts& o, const espl_lanes* h) {
+    const uint32_t precision = h->precision, refine = h->refine_sweeps;
     NewtonParams p{};
     p.reltol = o.reltol;
     p.abstol = o.abstol;
@@ -1016,6 +1020,8 @@ NewtonParams newton_params(const espl_newton_opts& o, uint32_t precision, uint32
     p.mixed = precision == ESPL_MIXED;
     p.stall_ticks = 12;
     p.refine = p.mixed ? refine : 0;
+    p.polish = h->polish ? std::pow(10.0, -(double)h->polish) : 0.0;
+    p.polish_max = kPolishMax;
     return p;
 }
 
@@ -1067,8 +1073,9 @@ espl_status espl_create(const espl_netlist* nets, uint32_t n_nets, const espl_cr
     h->device = opts ? (int)opts->device : 0;
     h->precision = opts ? opts->precision : ESPL_FP64;
     h->refine_sweeps = opts ? opts->refine_sweeps : 0;
+    h->polish = opts ? opts->polish : 0;
     if (opts && (opts->refine_sweeps > 4 || (opts->lanes_per_cta != 0 && opts->lanes_per_cta != 32) ||
-                 opts->precision > ESPL_MIXED)) {
+                 opts->precision > ESPL_MIXED || opts->polish > ESPL_POLISH_MAX_DIGITS)) {
         delete h;
         return ESPL_INVALID_ARGUMENT;
     }
@@ -1214,7 +1221,7 @@ espl_status espl_get_x(espl_lanes* h, uint32_t net, double* x) {
 espl_status espl_solve_static(espl_lanes* h, const espl_newton_opts* opts, espl_lane_newton* out) {
     if (!h || !opts) return ESPL_INVALID_ARGUMENT;
     if (opts->max_iter == 0 || opts->max_iter > 100000) return fail(h, ESPL_INVALID_ARGUMENT, "max_iter out of range");
-    NewtonParams np = newton_params(*opts, h->precision, h->refine_sweeps);
+    NewtonParams np = newton_params(*opts, h);
     espl_status s = run_static(h, np, 0);
     if (s) return s;
     if ((s = retape_stale(h))) return s;
@@ -1281,7 +1288,7 @@ espl_status espl_solve_op(espl_lanes* h, const espl_newton_opts* opts, espl_lane
     espl_newton_opts plain = *opts;
     plain.gmin = 0.0;
     plain.init_fix = 1;
-    if ((s = run_static(h, newton_params(plain, h->precision, h->refine_sweeps), 0))) return release(), s;
+    if ((s = run_static(h, newton_params(plain, h), 0))) return release(), s;
     CK(cudaMemcpyAsync(h->h_state.data(), h->d_state, sizeof(LaneState) * N, cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     enum Phase : uint8_t { kDone = 0, kGmin, kClean, kSrc, kSrcOff, kFinal };
@@ -1353,7 +1360,7 @@ espl_status espl_solve_op(espl_lanes* h, const espl_newton_opts* opts, espl_lane
         espl_newton_opts o = *opts;
         o.gmin = 0.0;
         o.max_iter = budget;
-        NewtonParams np = newton_params(o, h->precision, h->refine_sweeps);
+        NewtonParams np = newton_params(o, h);
         np.ladder = d_par;
         if ((s = run_static(h, np, 0))) return release(), s;
         CK(cudaMemcpyAsync(h->h_state.data(), h->d_state, sizeof(LaneState) * N, cudaMemcpyDeviceToHost, h->stream));
@@ -1673,7 +1680,7 @@ espl_status espl_init_steps(espl_lanes* h, const espl_tran_opts* o) {
     if (s) return s;
     if (seed(h, 1)) return ESPL_DRIVER;
     espl_newton_opts op{o->reltol, o->abstol, o->vntol, 0.0, o->residual_tol, 100, 1};
-    NewtonParams np = newton_params(op, h->precision, h->refine_sweeps);
+    NewtonParams np = newton_params(op, h);
     s = run_static(h, np, 1);
     if (s) return s;
     // The step tape: the lead lane's G + C / dt at the operating point.
@@ -1695,7 +1702,7 @@ espl_status espl_device_launch(espl_lanes* h, uint32_t max_steps, espl_step_repo
     TranParams t = h->tran;
     t.launch_steps = max_steps ? max_steps : 1;
     espl_newton_opts op{t.reltol, t.abstol, t.vntol, 0.0, t.residual_tol, t.max_iter, 0};
-    NewtonParams np = newton_params(op, h->precision, h->refine_sweeps);
+    NewtonParams np = newton_params(op, h);
     CK(cudaEventRecord(h->ev0, h->stream));
     espl_status s =
         launch_classes(h, [&](const TileMap& m, uint32_t grid, uint32_t smem, cudaStream_t st, bool wide) {
@@ -2009,8 +2016,17 @@ extern "C" espl_status espl_tape_replay_noalloc(const espl_tape* t, const uint32
     }
     const Tape& tp = t->t;
     const uint64_t n = tp.q.size(), nnz = tp.prow.size(), nl = tp.li.size(), nu = tp.ui.size();
-    if ((nl && !lx) || (nu && !ux) || col_ptr[n] != nnz) {
-        put_err(err, err_cap, "factor arrays missing or col_ptr does not match the tape");
+    if ((nl && !lx) || (nu && !ux)) {
+        put_err(err, err_cap, "factor arrays missing");
+        return ESPL_INVALID_ARGUMENT;
+    }
+    // The replay reads vals[p * lanes + l] for p in col_ptr[k] .. col_ptr[k + 1]:
+    // a pattern that is not the tape's would read past vals.
+    bool cp_ok = col_ptr[0] == 0 && col_ptr[n] == nnz;
+    for (uint64_t k = 0; cp_ok && k < n; k++) cp_ok = col_ptr[k] <= col_ptr[k + 1] && col_ptr[k + 1] <= nnz;
+    if (!cp_ok) {
+        put_err(err, err_cap, "col_ptr is not the tape's pattern (col_ptr[0] = 0, non-decreasing, col_ptr[n] = " +
+                                  std::to_string(nnz) + ")");
         return ESPL_INVALID_ARGUMENT;
     }
     // Layout: the tape words (q, col_ptr, prow, up, ui, lp, li, flags,
@@ -2032,9 +2048,14 @@ extern "C" espl_status espl_tape_replay_noalloc(const espl_tape* t, const uint32
     }
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess || dev < 0 || dev >= kReplayMaxDevices) {
+    if (e != cudaSuccess) {
         put_err(err, err_cap, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
-        return e == cudaSuccess ? ESPL_INVALID_ARGUMENT : ESPL_NO_IMAGE;
+        return ESPL_NO_IMAGE;
+    }
+    if (dev < 0 || dev >= kReplayMaxDevices) {
+        put_err(err, err_cap, "device " + std::to_string(dev) + " is past the " + std::to_string(kReplayMaxDevices) +
+                                  " devices this entry point serves");
+        return ESPL_INVALID_ARGUMENT;
     }
     unsigned char* base = nullptr;
     {

@@ -135,10 +135,14 @@ struct LadderLane {
 
 struct NewtonParams {
     double reltol, abstol, vntol, gmin, residual_tol;
+    // polish > 0: once a lane's step passes Newton's test, it keeps iterating
+    // until the step also passes the test with every tolerance scaled by
+    // `polish`, for at most polish_max further iterations
+    double polish;
     uint32_t max_iter, init_fix;
     uint32_t mixed, stall_ticks;   // mixed: FP32 LU; a lane past stall_ticks refactors in FP64
     uint32_t refine;               // mixed: FP64-residual refinement sweeps per solve
-    uint32_t pad;
+    uint32_t polish_max;
     const LadderLane* ladder;      // per lane (all templates' lanes), or null: gmin, init_fix, all lanes
 };
 

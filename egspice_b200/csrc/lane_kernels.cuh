@@ -49,6 +49,7 @@ struct TileShared {
     double ag0[32], ag1[32], ag2[32], t[32], xfact[32], dt_next[32];
     double lgmin[32], lsrc[32];  // the lane's ladder gmin and source scale
     uint32_t method[32], on[32], accept[32], rot[32];
+    uint32_t pit[32];  // the lane's polish iterations so far
 };
 
 // Gate flags reduced over warps.
@@ -85,6 +86,7 @@ __device__ __forceinline__ void newton_tile(const TileCtx& c, LaneState* s, cons
         sh.acc2[lane] = 0;
         sh.lgmin[lane] = lad ? lad->gmin : 0.0;
         sh.lsrc[lane] = lad ? lad->src : 1.0;
+        sh.pit[lane] = 0;
         if (s && on) {
             s->iterations = o.max_iter;
             // Mixed tiles factor in FP32 once Newton contracts (warm starts,
@@ -310,6 +312,10 @@ __device__ __forceinline__ void newton_tile(const TileCtx& c, LaneState* s, cons
                 bool ok = !(f & kLimited) && it != 0 && !(scaled >= 1.0) && !(f & (kImplausible | kResidualMiss));
                 if (ok && (sh.bits[lane] & kInitFix)) {
                     sh.bits[lane] &= ~kInitFix;
+                } else if (ok && o.polish > 0.0 && !(scaled < o.polish) && sh.pit[lane] < o.polish_max) {
+                    // the polish: Newton's test passed but not the tightened
+                    // one; the lane goes on from x + dx
+                    sh.pit[lane]++;
                 } else if (ok) {
                     sh.bits[lane] |= kConverged;
                     sh.active[lane] = 0;

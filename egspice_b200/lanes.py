@@ -138,11 +138,14 @@ class Lanes:
     """Lanes of one or more templates on one GPU."""
 
     def __init__(self, nets: Sequence[Netlist], precision: str = "fp64", dt0: float = 0.0, device: int = 0,
-                 refine_sweeps: int = 0):
+                 refine_sweeps: int = 0, polish: int = 0):
+        """`polish` k > 0: every Newton solve keeps iterating after the
+        reference's convergence test passes until its step also passes the
+        test with the tolerances scaled by 10^-k (espl_create_opts.polish)."""
         self.nets = list(nets)
         self._keep, arr = abi.cnets(self.nets)
         self._arr = arr
-        opts = CreateOpts(abi.ABI_VERSION, PRECISION[precision], device, 0, refine_sweeps, 0)
+        opts = CreateOpts(abi.ABI_VERSION, PRECISION[precision], device, 0, refine_sweeps, polish)
         h = C.c_void_p()
         st = lib().espl_create(arr, len(self.nets), C.byref(opts), dt0, C.byref(h))
         if st != 0:

@@ -325,6 +325,20 @@ def _read_params(cards: Sequence[tuple], env: _Env) -> None:
                     env.vals[k] = env.value(v, where)
 
 
+def param_defaults(text: str, names: Sequence[str]) -> Optional[Dict[str, float]]:
+    """The deck's own `.param` values of `names` (lower-cased keys), or
+    None when the deck does not give every one of them a single value."""
+    env = _Env(1, {})
+    _read_params(_expand_subckts(_logical_lines(text)), env)
+    out = {}
+    for k in names:
+        v = env.vals.get(k.lower())
+        if v is None or np.ndim(v) != 0 or not np.isfinite(v):
+            return None
+        out[k.lower()] = float(v)
+    return out
+
+
 def read_deck(text: str, lanes: int = 1, params: Optional[Mapping[str, Value]] = None,
               name: Optional[str] = None) -> Netlist:
     """The deck `text` as a Netlist of `lanes` lanes; `params` gives

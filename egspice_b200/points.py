@@ -22,8 +22,8 @@ import numpy as np
 
 from . import abi
 from .decks import RES
-from .netlist import (DeckError, _logical_lines, _split, measure_passes, parse_number, point_measures,
-                      read_deck, read_measures)
+from .netlist import (DeckError, _logical_lines, _split, measure_passes, param_defaults, parse_number,
+                      point_measures, read_deck, read_measures)
 
 # espice_status (include/espice.h :33-37)
 OK, INVALID_ARGUMENT, INVALID_QUERY, RESULT_UNAVAILABLE, FAILED = 0, 1, 4, 5, 6
@@ -179,6 +179,15 @@ class Points:
             raise DeckError("the .ac analysis needs a source with an AC value")
         self.need_op = (self.topts is None or self.freqs is not None
                         or any(m.op_row is not None for m in self.measures))
+        # The lead lane of every batch, whose matrix gives the batch's pivot
+        # tape: the deck's own .param values of the live parameters when it
+        # gives them all. Each batch then replays the same tape, and a lane's
+        # arithmetic reads only its own values, so a point's results are
+        # bitwise the same in any order, batch or rank split (the points
+        # API's promise, include/espice.h:246-250). Without them the first
+        # point of each batch leads, and results agree to roundoff only.
+        d = param_defaults(text, self.live)
+        self.lead = None if d is None else np.array([d[p] for p in self.live])
         self.rows: List[np.ndarray] = []     # each point's values
         self.state: List[int] = []           # 0 pending, 1 complete, 2 released
         self.values: Dict[int, np.ndarray] = {}
@@ -220,21 +229,44 @@ class Points:
                 self.reasons[k] = reason
         return first
 
+    def batches(self, ids: Sequence[int]) -> List[List[int]]:
+        """The lane batches of the points `ids` as one process runs them:
+        consecutive runs of lane_width() lanes, one of them the lead lane
+        when the deck gives the live parameters' values."""
+        per = LANE_WIDTH - (1 if self.lead is not None else 0)
+        return [list(ids[b0:b0 + per]) for b0 in range(0, len(ids), per)]
+
+    def rank_batches(self, pending: Sequence[int], rank: int, world: int) -> List[List[int]]:
+        """Rank `rank`'s share of the one-process batches: contiguous whole
+        batches, so every batch keeps its members (and lead) at any world
+        size."""
+        bs = self.batches(pending)
+        per = -(-len(bs) // world) if bs else 0
+        return bs[rank * per:(rank + 1) * per]
+
     def run(self, group=None) -> None:
         """Runs every pending point on the GPU lanes, lane_width() at a time.
-        Under torch.distributed (one process per GPU), the pending points
-        split into contiguous slices, one per rank of `group`, each rank runs
-        its slice on its own GPU, and every rank receives every result (no
-        collective touches the lanes: the exchange is of finished results)."""
+        Under torch.distributed (one process per GPU), the one-process lane
+        batches split into contiguous runs of whole batches, one per rank of
+        `group`, each rank runs its batches on its own GPU, and every rank
+        receives every result (no collective touches the lanes: the exchange
+        is of finished results)."""
         pending = [k for k, s in enumerate(self.state) if s == 0]
         rank, world, dist = 0, 1, None
         td = sys.modules.get("torch.distributed")  # a process group needs torch imported already
         if td is not None and td.is_available() and td.is_initialized():
             dist, rank, world = td, td.get_rank(group), td.get_world_size(group)
-        per = -(-len(pending) // world) if pending else 0
-        results = self._run_ids(pending[rank * per:(rank + 1) * per])
+            if rank < 0:
+                raise PointsError(INVALID_ARGUMENT, "NotInProcessGroup")
+        results = {}
+        for batch in self.rank_batches(pending, rank, world):
+            results.update(self._run_ids(batch))
         parts = [results]
         if world > 1:
+            if td.get_backend(group) == "nccl":
+                # all_gather_object stages its tensors on the current device
+                import torch
+                torch.cuda.set_device(self.device)
             parts = [None] * world
             dist.all_gather_object(parts, results, group=group)
         for part in parts:
@@ -249,11 +281,11 @@ class Points:
         from .lanes import Lanes
         names = [m.name for m in self.measures]
         done: Dict[int, tuple] = {}
-        for b0 in range(0, len(ids), LANE_WIDTH):
-            batch = list(ids[b0:b0 + LANE_WIDTH])
-            block = np.stack([self.rows[k] for k in batch])
+        lead = 1 if self.lead is not None else 0
+        for batch in self.batches(ids):
+            block = np.stack(([self.lead] if lead else []) + [self.rows[k] for k in batch])
             params = {p: block[:, j] for j, p in enumerate(self.live)}
-            net = read_deck(self.text, lanes=len(batch), params=params)
+            net = read_deck(self.text, lanes=len(block), params=params)
             ms = read_measures(self.text, net, params=params)
             op = x_op = reps = ac = None
             value = np.zeros((len(batch), 0))
@@ -277,7 +309,7 @@ class Points:
             out, reasons = point_measures(ms, value, names, reports=reps, op=op, x_op=x_op,
                                           stopped_ok=self.early_stop, ac=ac)
             for i, k in enumerate(batch):
-                done[k] = (out[i], int(reasons[i]))
+                done[k] = (out[lead + i], int(reasons[lead + i]))
         return done
 
     def _run_early_stop(self, L, steps_per_launch: int = 512, max_launches: int = 100000):

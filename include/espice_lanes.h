@@ -102,7 +102,10 @@ typedef struct {
     double gmin;         /* diagonal gmin; 0 in the plain operating-point rung */
     double residual_tol; /* 1e-9 */
     uint32_t max_iter;   /* 100 */
-    uint32_t init_fix;   /* 1: cold operating point (MODEINITJCT/INITFIX) */
+    uint32_t init_fix;   /* 1: cold operating point (MODEINITJCT/INITFIX). This
+                          * word is the reference NewtonOpts' trailing `_pad`
+                          * (48 bytes either way): a host that binds the
+                          * reference layout passes 0 there, a warm start. */
 } espl_newton_opts;
 
 /* Per-lane outcome: `LaneNewton` of lanes.zig. bits: 4 converged,
@@ -131,8 +134,22 @@ typedef struct {
                               * each FP32 solve inside Newton (0: none; each Newton
                               * iteration then refines the step against the FP64
                               * KCL residual). At most 4. */
-    uint32_t reserved;       /* 0 */
+    uint32_t polish;         /* 0: Newton publishes the iterate whose step passes
+                              * the reference's test (converger.zig: |dx| <
+                              * reltol |x| + vntol or abstol), as the reference does.
+                              * k in 1..ESPL_POLISH_MAX_DIGITS: after that test
+                              * passes, the lane keeps iterating (at most 4 more
+                              * Newton iterations) until its step also passes the
+                              * test with every tolerance scaled by 10^-k, and
+                              * publishes that iterate. The converged point then
+                              * no longer depends on where Newton started (a
+                              * predicted start, a learned one, FP32 factors) to
+                              * well below the Newton tolerance. Every Newton
+                              * solve of the handle (operating points, the ladder,
+                              * transient steps) polishes; iteration counts
+                              * include the polish. */
 } espl_create_opts;
+#define ESPL_POLISH_MAX_DIGITS 12u
 
 typedef struct espl_lanes espl_lanes;
 
@@ -419,7 +436,12 @@ espl_status espl_error_message(espl_lanes *h, char *buf, size_t cap);
  * entry point is aborted. Calls on one device share the array: overlapping
  * calls (other streams, other host threads) race; serialize them. The first
  * call on a device resolves the array's address (cudaGetSymbolAddress, with
- * that device current); make it before any stream capture begins. */
+ * that device current) and keeps it for the life of the process; make it
+ * before any stream capture begins. A device reset (cudaDeviceReset) or the
+ * primary context's teardown invalidates that address: do not call this
+ * entry point on the device afterwards in the same process. col_ptr must be
+ * the pattern the tape was built from (col_ptr[0] = 0, non-decreasing,
+ * col_ptr[n] = nnz), else ESPL_INVALID_ARGUMENT. */
 #define ESPL_REPLAY_SCRATCH_BYTES (8u << 20)
 espl_status espl_tape_replay_noalloc(const espl_tape *t, const uint32_t *col_ptr, const double *vals,
                                      uint32_t lanes, double *lx, double *ux, double *udiag, uint32_t *lane_status,

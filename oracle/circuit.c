@@ -467,10 +467,21 @@ typedef struct {
     const double *i_prev; /* row companion currents there */
 } companion;
 
-/* newtonLanes at W = 1 (converger.zig:200-319). */
+/* The polish (espl_create_opts.polish of the product): 0 off, else the
+ * tightened test's tolerances are scaled by 10^-digits. Set before a run;
+ * read by every Newton solve. */
+static double g_polish = 0.0;
+#define ORC_POLISH_MAX 4u
+void orc_set_polish(uint32_t digits) { g_polish = digits ? pow(10.0, -(double)digits) : 0.0; }
+
+/* newtonLanes at W = 1 (converger.zig:200-319). With the polish on, a lane
+ * whose step passes the reference's test keeps iterating from x + dx until
+ * the step also passes the test with the tolerances scaled by g_polish (at
+ * most ORC_POLISH_MAX more iterations), and publishes that iterate. */
 static orc_newton_result newton(ockt *k, double *x, const espl_newton_opts *o, int tran, double t, const companion *cp, uint32_t *fail_factor) {
     orc_newton_result r = {0, 0, 0, 0};
     int init_fix = o->init_fix != 0;
+    uint32_t polished = 0;
     double limit = X_PLAUSIBLE;
     for (uint32_t iter = 0; iter < o->max_iter; iter++) {
         eval_planes(k, x, tran, t);
@@ -520,6 +531,8 @@ static orc_newton_result newton(ockt *k, double *x, const espl_newton_opts *o, i
         if (ok) ok = residual_ok(k, o, k->rhs, x, v);
         if (ok && init_fix) {
             init_fix = 0;
+        } else if (ok && g_polish > 0.0 && !(scaled < g_polish) && polished < ORC_POLISH_MAX) {
+            polished++;
         } else if (ok) {
             memcpy(x, k->x_old, sizeof(double) * k->n);
             r.converged = 1;

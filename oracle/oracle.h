@@ -91,6 +91,12 @@ int orc_tran_lanes(const espl_netlist *net, uint32_t lane0, uint32_t count, cons
                    double *x_final, espl_step_report *reports, uint32_t meas_row, double meas_level,
                    double meas_t_start, double *period, uint32_t threads);
 
+/* The polish of every later Newton solve (the product's
+ * espl_create_opts.polish): 0 the reference's test alone; k: after it passes,
+ * iterate until the step passes it with the tolerances scaled by 10^-k (at
+ * most 4 more iterations). Process-wide; set it before a run. */
+void orc_set_polish(uint32_t digits);
+
 /* Newton's residual gate of one row: |F_i| passes when <= this. */
 double orc_residual_gate(double residual_tol, double reltol, double vntol, double diag, double xi);
 

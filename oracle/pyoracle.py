@@ -5,6 +5,7 @@ the product package never imports it.
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes as C
 import os
 import subprocess
@@ -74,6 +75,8 @@ def lib():
         L.orc_device_probe.argtypes = [C.POINTER(NetlistC), C.c_uint32, C.c_uint32, C.c_uint32, f64p, f64p, f64p,
                                        f64p, f64p]
         L.orc_device_probe.restype = C.c_int
+        L.orc_set_polish.argtypes = [C.c_uint32]
+        L.orc_set_polish.restype = None
         L.orc_pnjlim.argtypes = [C.c_double, C.c_double, C.c_double, C.c_double, C.POINTER(C.c_int)]
         L.orc_pnjlim.restype = C.c_double
         L.orc_fetlim.argtypes = [C.c_double, C.c_double, C.c_double]
@@ -88,6 +91,19 @@ def lib():
         L.orc_step_bound.restype = C.c_double
         _lib = L
     return _lib
+
+
+@contextlib.contextmanager
+def polish(digits: int):
+    """Every oracle Newton solve inside the block polishes: after the
+    reference's test passes it iterates until the step passes the test with
+    the tolerances scaled by 10^-digits (orc_set_polish; the product's
+    espl_create_opts.polish). Process-wide."""
+    lib().orc_set_polish(int(digits))
+    try:
+        yield
+    finally:
+        lib().orc_set_polish(0)
 
 
 def _u32(a):

@@ -5,20 +5,20 @@ and its 19 rows of (wn, wp, rw, cw, td) from src/tests/espice.zig
 table and sweep removed so the rows come in as points. The reference test
 runs each row alone and in three orders and asserts the same measures; the
 tests run the rows as lanes on the GPU and through the oracle. Run from the
-repository root while the reference tree is present:
+repository root with the path of the reference's source tree:
 
-    python tests/golden/extract_chain_deck.py
+    python tests/golden/extract_chain_deck.py <reference tree>
 """
 import json
 import os
 import re
+import sys
 
-SRC = "/root/reference/src/tests/espice.zig"
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "chain_deck.json")
 
 
-def main():
-    text = open(SRC).read().splitlines()
+def main(tree: str):
+    text = open(os.path.join(tree, "src", "tests", "espice.zig")).read().splitlines()
     start = next(i for i, l in enumerate(text) if l.startswith("const chain_deck ="))
     deck = []
     for line in text[start + 1:]:
@@ -44,4 +44,6 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    if len(sys.argv) != 2:
+        sys.exit("usage: extract_chain_deck.py <reference source tree>")
+    main(sys.argv[1])

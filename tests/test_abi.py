@@ -49,3 +49,36 @@ def test_symbolic_seam_on_cpu():
     assert list(symbolic.order(cp, ri)) in ([0, 1], [1, 0])
     t = symbolic.tape(cp, ri, [2.0, 1.0, 1.0, 3.0], [0, 1])
     assert list(t["pinv"]) == [0, 1] and len(t["li"]) == 1 and len(t["ui"]) == 1
+
+
+def test_noalloc_replay_refuses_a_pattern_that_is_not_the_tapes():
+    """espl_tape_replay_noalloc checks the caller's col_ptr on the host
+    before any device work: a decreasing entry, an entry past nnz or a wrong
+    first entry is ESPL_INVALID_ARGUMENT with the reason, so the replay
+    never reads past the lanes' values. (The device pointers here are
+    stand-ins that the refused call never reads.)"""
+    import ctypes as C
+
+    from egspice_b200.lanes import lib
+    from egspice_b200 import symbolic
+    L = symbolic._setup(lib())
+    u32p = C.POINTER(C.c_uint32)
+    L.espl_tape_replay_noalloc.argtypes = [C.c_void_p, u32p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p,
+                                           C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p, C.c_size_t]
+    L.espl_tape_replay_noalloc.restype = C.c_uint32
+    cp = np.array([0, 2, 4, 6], np.uint32)
+    ri = np.array([0, 1, 0, 1, 1, 2], np.uint32)
+    vals = np.array([4.0, 1.0, 1.0, 4.0, 1.0, 4.0])
+    q = np.ascontiguousarray(symbolic.order(cp, ri), dtype=np.uint32)
+    h = C.c_void_p()
+    assert L.espl_tape_build(3, cp.ctypes.data_as(u32p), ri.ctypes.data_as(u32p),
+                             vals.ctypes.data_as(C.POINTER(C.c_double)), q.ctypes.data_as(u32p), C.byref(h)) == 0
+    fake = C.c_void_p(256)
+    try:
+        for bad in ([0, 4, 2, 6], [0, 2, 7, 6], [1, 2, 4, 6]):
+            b = np.array(bad, np.uint32)
+            err = C.create_string_buffer(256)
+            st = L.espl_tape_replay_noalloc(h, b.ctypes.data_as(u32p), fake, 4, fake, fake, fake, fake, None, err, 256)
+            assert st == 1 and b"col_ptr" in err.value, (bad, st, err.value)
+    finally:
+        L.espl_tape_free(h)

@@ -85,10 +85,13 @@ def _points_worker(rank, world, port, out):
 
     from egspice_b200 import points as pt
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    pt.LANE_WIDTH = 4  # batches of the lead lane and 3 points, so 11 points make 4 batches
     p = pt.Points(POINTS_DECK, ["rval"])
     seen = []
+    calls = []
 
     def fake_run_ids(ids):  # stands in for the GPU run: a result that names its point
+        calls.append(list(ids))
         seen.extend(ids)
         return {k: (np.array([p.rows[k][0], -float(k)]), k % 3) for k in ids}
 
@@ -99,6 +102,11 @@ def _points_worker(rank, world, port, out):
     v, r = p.copy_point_measures(0, 12, ["t50", "v2n"])
     ran = np.array(sorted(seen) + [-1] * (12 - len(seen)), dtype=np.float64)
     np.save(out + f".{rank}.npy", np.concatenate([v, r[:, None], ran[:, None]], axis=1))
+    # every batch a rank ran is a whole batch of the one-process batching,
+    # led by the deck's own value of the live parameter
+    one = [b for b in p.batches(list(range(11)))]
+    assert all(c in one for c in calls), (calls, one)
+    assert p.lead is not None and p.lead.tolist() == [1000.0]
     dist.barrier()
     dist.destroy_process_group()
 
@@ -117,9 +125,10 @@ c1 out 0 1p
 
 def test_points_split_across_two_ranks(tmp_path):
     """Points.run under torch.distributed (gloo, two ranks, the GPU run
-    replaced by a result naming its point): the 11 pending points split into
-    contiguous slices, one per rank, and both ranks end with every point's
-    result, equal to a one-process run."""
+    replaced by a result naming its point): the one-process batches of the
+    11 pending points (the lead lane and 3 points each) split into
+    contiguous runs of whole batches, one per rank, and both ranks end with
+    every point's result, equal to a one-process run."""
     out = str(tmp_path / "p")
     mp.spawn(_points_worker, args=(2, _free_port(), out), nprocs=2, join=True)
     a, b = np.load(out + ".0.npy"), np.load(out + ".1.npy")
