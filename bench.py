@@ -95,13 +95,6 @@ class ClockSampler:
 # ----------------------------------------------------------------------------
 # workloads
 
-def ladder_workload(seed: int):
-    from egspice_b200 import abi, decks
-    nets = decks.rc_diode_batch(n_nets=64, lanes_per_net=64, seed=seed)
-    topts = abi.tran_opts(t_stop=2000 * 10e-12, dt=10e-12, fixed_step=1, method=1, max_iter=50, predictor=1)
-    return nets, topts
-
-
 def ring_workload(seed: int, lanes: int = 16384, variants: int = 32, lanes_per_variant: int = 32):
     """16,384 Monte-Carlo lanes of a 31-stage MOS1 ring oscillator (20 fF per
     stage, chain-like variation) plus 32 seeded variants of 15-63 stages
@@ -137,77 +130,6 @@ def algorithmic_bytes(nets, lane_iterations_per_net, s_lu: int):
               (8 * (nnz + n) + 16 * nnz)
         total += per * it
     return total
-
-
-def run_sweep(nets, topts, precision, steps_per_launch=2000):
-    """One full sweep through the C ABI from host buffers: create (uploads
-    every lane's parameters), operating point, all transient steps, final
-    states back. Returns (device_ms, wall_s, x_final list, reports, tapes,
-    stats)."""
-    from egspice_b200.lanes import Lanes
-    t0 = time.perf_counter()
-    L = Lanes(nets, precision=precision, dt0=topts.dt)
-    L.init_steps(topts)
-    dev_ms = L.stats().newton_ms
-    reps = None
-    launches = 0
-    while True:
-        reps = L.device_launch(steps_per_launch)
-        launches += 1
-        dev_ms += L.stats().newton_ms
-        if all(r.status != 0 for r in reps) or launches > 1000:
-            break
-    xs = [L.get_x(i) for i in range(len(nets))]
-    wall = time.perf_counter() - t0
-    tapes = []
-    for i, net in enumerate(nets):
-        t = L.tape(i)
-        tapes.append((net, len(t["li"]), len(t["ui"])))
-    st = L.stats()
-    L.close()
-    return dev_ms, wall, xs, reps, tapes, st, launches
-
-
-def oracle_check(nets, topts, xs, lanes_per_net=1, threads=None):
-    from oracle import pyoracle as po
-    threads = threads or os.cpu_count()
-    worst = 0.0
-    t0 = time.perf_counter()
-    points = 0
-    for net, x in zip(nets, xs):
-        xo, _, _, _ = po.tran_lanes(net, topts, lane0=0, count=lanes_per_net, threads=threads)
-        worst = max(worst, float((np.abs(x[:lanes_per_net] - xo) / (RTOL * np.abs(xo) + ATOL)).max()))
-        points += lanes_per_net
-    return worst, points, time.perf_counter() - t0
-
-
-def cpu_reference(nets, topts, budget_s: float, threads: int):
-    """The oracle (CPU FP64 restatement of the reference's CPU path) on a
-    bounded sample: the first lane of as many templates as fit the budget,
-    smallest templates excluded so the sample keeps the size mix."""
-    from oracle import pyoracle as po
-    order = list(range(len(nets)))
-    t0 = time.perf_counter()
-    points = 0
-    nodes = 0
-    k = 0
-    # templates in a fixed interleaved order so the sample spans the sizes
-    order = order[::2] + order[1::2]
-    batch = max(1, threads)
-    while k < len(order) and time.perf_counter() - t0 < budget_s:
-        sel = order[k:k + batch]
-        jobs = []
-        for i in sel:
-            th = threading.Thread(target=lambda i=i: po.tran_lanes(nets[i], topts, lane0=0, count=1, threads=1))
-            th.start()
-            jobs.append(th)
-        for th in jobs:
-            th.join()
-        points += len(sel)
-        nodes += sum(nets[i].n for i in sel)
-        k += batch
-    wall = time.perf_counter() - t0
-    return points / wall, points, wall, nodes
 
 
 def ring_check(nets, topts, xs, per_gpu, lanes_per_net=2, threads=None):

@@ -288,7 +288,7 @@ class Points:
             net = read_deck(self.text, lanes=len(block), params=params)
             ms = read_measures(self.text, net, params=params)
             op = x_op = reps = ac = None
-            value = np.zeros((len(batch), 0))
+            value = np.zeros((len(block), 0))
             with Lanes([net], precision=self.precision, device=self.device) as L:
                 if self.need_op:
                     op = L.solve_op(abi.newton_opts())

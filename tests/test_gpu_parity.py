@@ -34,8 +34,18 @@ def test_tape_bit_exact_with_oracle(oracle):
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_inverter_chain_cold_operating_points(oracle, precision):
     """Config 1 at its size: 1,024 Monte-Carlo points of the 16-stage chain
-    from the cold start. Every lane the oracle converges converges on the
-    GPU too, and every one of them meets the bar."""
+    from the cold start.
+
+    The plain rung alone (solve_static from x = 0 with INITFIX): where both
+    sides converge, every lane meets the bar. From a cold start the limiting
+    walk amplifies last-bit differences (a fused multiply-add, the last bit
+    of exp), so a lane near the 100-iteration limit can converge on one side
+    and not the other; at most 1 % of lanes may differ that way.
+
+    The whole operating point (solve_op: the plain rung, then the
+    continuation ladder for the lanes it leaves) with the polish, against
+    the oracle's ladder with the same polish: every lane converges on both
+    sides and every lane meets the bar."""
     net = decks.inverter_chain(1024)
     opts = abi.newton_opts()
     xo, ro = oracle.op_lanes(net, opts, threads=8)
@@ -45,9 +55,17 @@ def test_inverter_chain_cold_operating_points(oracle, precision):
     ok = (r[:, 0] & abi.CONVERGED) != 0
     oracle_ok = ro[:, 0] == 1
     assert oracle_ok.mean() >= 0.99
-    missed = np.nonzero(oracle_ok & ~ok)[0]
-    assert len(missed) == 0, f"lanes the oracle converges and the GPU does not: {missed.tolist()}"
-    assert worst(x[oracle_ok], xo[oracle_ok]) <= 1.0
+    both = ok & oracle_ok
+    assert (ok != oracle_ok).mean() <= 0.01, np.nonzero(ok != oracle_ok)[0].tolist()
+    assert worst(x[both], xo[both]) <= 1.0
+    with oracle.polish(6):
+        xl, rl = oracle.op_ladder(net, opts, threads=8)
+    with Lanes([net], precision=precision, polish=6) as L:
+        r = L.solve_op(opts)
+        x = L.get_x(0)
+    assert (rl[:, 0] == 1).all()
+    assert ((r[:, 0] & abi.CONVERGED) != 0).all()
+    assert worst(x, xl) <= 1.0
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
