@@ -50,7 +50,8 @@ class TranOpts(C.Structure):
 
 class StepReport(C.Structure):
     _fields_ = [("t", C.c_double), ("dt", C.c_double), ("attempts", C.c_uint64), ("nr_iters", C.c_uint64),
-                ("steps", C.c_uint32), ("rejects", C.c_uint32), ("status", C.c_uint32), ("reserved", C.c_uint32)]
+                ("steps", C.c_uint32), ("rejects", C.c_uint32), ("status", C.c_uint32),
+                ("learned_retries", C.c_uint32)]
 
 
 class Stats(C.Structure):

@@ -13,8 +13,10 @@
 #include <vector>
 
 #include "../../include/espice_lanes.h"
+#include "../../include/espice_learned.h"
 #include "lane_kernels.cuh"
 #include "lane_ac.cuh"
+#include "lane_learned.cuh"
 #include "tape.h"
 
 using namespace espl;
@@ -35,6 +37,7 @@ struct LaunchClass {
     uint32_t per_sm = 0;      // resident tiles per SM at that size
     bool wide = false;        // kWideWarps per tile (banded templates; the largest others while the rest fit)
     std::vector<uint32_t> tiles;
+    std::vector<uint32_t> groups;   // the templates whose tiles the class holds
     uint32_t* d_tiles = nullptr;
     cudaStream_t stream = nullptr;  // null: the handle's stream (a single class)
     cudaEvent_t t0 = nullptr, t1 = nullptr;  // around the class's last launch
@@ -104,6 +107,9 @@ struct Group {
     uint32_t tile0 = 0;
     uint32_t n_rec = 0;   // words of the uploaded replay records (0: none)
     uint32_t n_srec = 0;  // words of the uploaded solve records (0: none)
+    espl_mlp* pred = nullptr;            // the learned step predictor (borrowed), or none
+    std::vector<void*> learn_owned;      // prev2, xpred
+    std::vector<void*> rec_owned;        // the step recorder's buffers
 };
 
 }  // namespace
@@ -130,6 +136,14 @@ struct espl_lanes {
     std::vector<LaneState> h_state;
     std::vector<LaunchClass> classes;
     cudaEvent_t fork = nullptr;
+    // the learned predictor's attempt-at-a-time launches: their stream, the
+    // stepping-lane counter (device and pinned host word), whether the
+    // predictor kernel's shared-memory limit is raised
+    cudaStream_t step_stream = nullptr;
+    cudaEvent_t step_fork = nullptr, step_done = nullptr;
+    uint32_t* d_count = nullptr;
+    uint32_t* h_count = nullptr;
+    size_t predict_smem = 0;
 };
 
 namespace {
@@ -823,6 +837,7 @@ espl_status plan_classes(espl_lanes* h) {
         for (size_t i = 0; i < h->groups.size(); i++) {
             if ((per[i] | (wide[i] ? 0x10000u : 0u)) != key) continue;
             c.smem = std::max(c.smem, bytes[i]);
+            c.groups.push_back((uint32_t)i);
             for (uint32_t t = 0; t < h->groups[i].P / 32; t++) c.tiles.push_back(h->groups[i].tile0 + t);
         }
         h->classes.push_back(std::move(c));
@@ -1055,6 +1070,173 @@ espl_status seed(espl_lanes* h, int cold) {
     return ESPL_OK;
 }
 
+void launch_tran(const TileMap& m, uint32_t grid, uint32_t smem, cudaStream_t st, bool wide, const TranParams& t,
+                 const NewtonParams& np, LaneState* state) {
+    if (np.mixed && wide)
+        k_tran<true, true><<<grid, kWideThreads, smem, st>>>(m, t, np, state);
+    else if (np.mixed)
+        k_tran<true, false><<<grid, kBlock, smem, st>>>(m, t, np, state);
+    else if (wide)
+        k_tran<false, true><<<grid, kWideThreads, smem, st>>>(m, t, np, state);
+    else
+        k_tran<false, false><<<grid, kBlock, smem, st>>>(m, t, np, state);
+}
+
+// The history of the learned predictor (prev2) and, with `pred`, the
+// buffer of its starts (xpred), allocated once per template. prev2 starts
+// as prev when a transient is under way (exact from the next accepted step
+// on; k_tran_init sets it at a transient's start).
+espl_status ensure_learn_buffers(espl_lanes* h, Group& g, bool pred) {
+    const size_t words = (size_t)(g.n + 1) * g.P;
+    if (!g.dev.prev2) {
+        double* p = nullptr;
+        CK(cudaMalloc(&p, sizeof(double) * words));
+        g.learn_owned.push_back(p);
+        if (h->tran_ready)
+            CK(cudaMemcpyAsync(p, g.dev.prev, sizeof(double) * words, cudaMemcpyDeviceToDevice, h->stream));
+        else
+            CK(cudaMemsetAsync(p, 0, sizeof(double) * words, h->stream));
+        g.dev.prev2 = p;
+    }
+    if (pred && !g.dev.xpred) {
+        double* p = nullptr;
+        CK(cudaMalloc(&p, sizeof(double) * words));
+        g.learn_owned.push_back(p);
+        CK(cudaMemsetAsync(p, 0, sizeof(double) * words, h->stream));
+        g.dev.xpred = p;
+    }
+    return ESPL_OK;
+}
+
+// The predictor kernel for template gi on `st` (its network's view taken
+// beforehand: view() may pack the weights, which a stream capture cannot).
+void launch_predict(espl_lanes* h, uint32_t gi, const mlp::MlpView& v, cudaStream_t st) {
+    const Group& g = h->groups[gi];
+    StepPredictArgs a{h->d_groups + gi, h->d_state, v, h->tran.dt_max};
+    k_step_predict<<<(g.lanes + 127) / 128, 128, h->predict_smem, st>>>(a);
+}
+
+espl_status predictor_views(espl_lanes* h, std::vector<mlp::MlpView>& views, cudaStream_t st) {
+    views.assign(h->groups.size(), mlp::MlpView{});
+    size_t smem = 0;
+    for (size_t gi = 0; gi < h->groups.size(); gi++) {
+        Group& g = h->groups[gi];
+        if (!g.pred) continue;
+        espl_status s = espl_mlp_view(g.pred, &views[gi], st);
+        if (s) return fail(h, s, "the step predictor's network could not be read");
+        smem = std::max(smem, mlp::infer_smem_bytes(views[gi].dp, views[gi].op));
+    }
+    if (smem > h->predict_smem) {
+        CK(cudaFuncSetAttribute(k_step_predict, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        h->predict_smem = smem;
+    }
+    return ESPL_OK;
+}
+
+espl_status step_stream(espl_lanes* h) {
+    if (h->step_stream) return ESPL_OK;
+    CK(cudaStreamCreateWithFlags(&h->step_stream, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&h->step_fork, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&h->step_done, cudaEventDisableTiming));
+    CK(cudaMalloc(&h->d_count, sizeof(uint32_t)));
+    CK(cudaMallocHost(&h->h_count, sizeof(uint32_t)));
+    return ESPL_OK;
+}
+
+// One espl_device_launch with learned predictors: the classes without a
+// template that has one run their attempts in one persistent launch each,
+// as without; the classes with one run attempt by attempt, a CUDA graph of
+// the predictor kernels (every such template's lanes) and one k_tran attempt
+// per class replayed up to t.launch_steps times, until none of their lanes
+// is still stepping (checked every 64 replays).
+espl_status launch_learned(espl_lanes* h, const TranParams& t, const NewtonParams& np, uint64_t& launches) {
+    espl_status s;
+    if ((s = step_stream(h))) return s;
+    std::vector<mlp::MlpView> views;
+    if ((s = predictor_views(h, views, h->stream))) return s;
+    std::vector<size_t> stepped, persistent;
+    for (size_t k = 0; k < h->classes.size(); k++) {
+        bool any = false;
+        for (uint32_t gi : h->classes[k].groups) any |= h->groups[gi].pred != nullptr;
+        (any ? stepped : persistent).push_back(k);
+    }
+    CK(cudaEventRecord(h->fork, h->stream));
+    for (size_t k : persistent) {
+        LaunchClass& c = h->classes[k];
+        cudaStream_t st = c.stream ? c.stream : h->stream;
+        if (c.stream) CK(cudaStreamWaitEvent(st, h->fork, 0));
+        TileMap m{h->d_groups, h->d_warp_group, c.d_tiles, (uint32_t)c.tiles.size()};
+        CK(cudaEventRecord(c.t0, st));
+        launch_tran(m, (uint32_t)c.tiles.size(), c.smem, st, c.wide, t, np, h->d_state);
+        CK(cudaGetLastError());
+        CK(cudaEventRecord(c.t1, st));
+        if (c.stream) CK(cudaEventRecord(c.done, st));
+    }
+    cudaStream_t ss = h->step_stream;
+    CK(cudaStreamWaitEvent(ss, h->fork, 0));
+    for (size_t k : stepped) CK(cudaEventRecord(h->classes[k].t0, ss));
+    // the graph of one attempt
+    TranParams t1 = t;
+    t1.launch_steps = 1;
+    cudaGraph_t graph = nullptr;
+    CK(cudaStreamBeginCapture(ss, cudaStreamCaptureModeThreadLocal));
+    for (size_t gi = 0; gi < h->groups.size(); gi++)
+        if (h->groups[gi].pred) launch_predict(h, (uint32_t)gi, views[gi], ss);
+    cudaError_t ce = cudaSuccess;
+    if (stepped.size() > 1) ce = cudaEventRecord(h->step_fork, ss);
+    for (size_t k : stepped) {
+        if (ce != cudaSuccess) break;
+        LaunchClass& c = h->classes[k];
+        cudaStream_t st = (stepped.size() > 1 && c.stream) ? c.stream : ss;
+        if (st != ss) ce = cudaStreamWaitEvent(st, h->step_fork, 0);
+        TileMap m{h->d_groups, h->d_warp_group, c.d_tiles, (uint32_t)c.tiles.size()};
+        if (ce == cudaSuccess) launch_tran(m, (uint32_t)c.tiles.size(), c.smem, st, c.wide, t1, np, h->d_state);
+        if (ce == cudaSuccess) ce = cudaGetLastError();
+        if (ce == cudaSuccess && st != ss) ce = cudaEventRecord(c.done, st);
+        if (ce == cudaSuccess && st != ss) ce = cudaStreamWaitEvent(ss, c.done, 0);
+    }
+    cudaError_t ee = cudaStreamEndCapture(ss, &graph);
+    if (ce != cudaSuccess || ee != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        return fail(h, ESPL_DRIVER, std::string("capturing a transient attempt: ") +
+                                        cudaGetErrorString(ce != cudaSuccess ? ce : ee));
+    }
+    uint64_t per_attempt = stepped.size();
+    for (auto& g : h->groups) per_attempt += g.pred ? 1 : 0;
+    launches = persistent.size();
+    cudaGraphExec_t exec = nullptr;
+    ce = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ce != cudaSuccess) return fail(h, ESPL_DRIVER, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(ce));
+    s = ESPL_OK;
+    for (uint32_t a = 0; a < t.launch_steps && !s;) {
+        const uint32_t burst = std::min<uint32_t>(64u, t.launch_steps - a);
+        for (uint32_t b = 0; b < burst && ce == cudaSuccess; b++) ce = cudaGraphLaunch(exec, ss);
+        a += burst;
+        launches += burst * per_attempt + stepped.size();
+        if (ce == cudaSuccess) ce = cudaMemsetAsync(h->d_count, 0, sizeof(uint32_t), ss);
+        for (size_t k : stepped) {
+            if (ce != cudaSuccess) break;
+            LaunchClass& c = h->classes[k];
+            TileMap m{h->d_groups, h->d_warp_group, c.d_tiles, (uint32_t)c.tiles.size()};
+            k_count_stepping<<<(uint32_t)c.tiles.size(), kBlock, 0, ss>>>(m, h->d_state, h->d_count);
+            ce = cudaGetLastError();
+        }
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(h->h_count, h->d_count, sizeof(uint32_t), cudaMemcpyDeviceToHost, ss);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(ss);
+        if (ce != cudaSuccess) s = fail(h, ESPL_DRIVER, std::string("a learned transient attempt: ") + cudaGetErrorString(ce));
+        else if (*h->h_count == 0) break;
+    }
+    cudaGraphExecDestroy(exec);
+    if (s) return s;
+    for (size_t k : stepped) CK(cudaEventRecord(h->classes[k].t1, ss));
+    CK(cudaEventRecord(h->step_done, ss));
+    CK(cudaStreamWaitEvent(h->stream, h->step_done, 0));
+    for (size_t k : persistent)
+        if (h->classes[k].stream) CK(cudaStreamWaitEvent(h->stream, h->classes[k].done, 0));
+    return ESPL_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1150,7 +1332,14 @@ espl_status espl_destroy(espl_lanes* h) {
         for (void* p : g.owned) cudaFree(p);
         for (void* p : g.lu_owned) cudaFree(p);
         for (void* p : g.meas_owned) cudaFree(p);
+        for (void* p : g.learn_owned) cudaFree(p);
+        for (void* p : g.rec_owned) cudaFree(p);
     }
+    cudaFree(h->d_count);
+    if (h->h_count) cudaFreeHost(h->h_count);
+    if (h->step_fork) cudaEventDestroy(h->step_fork);
+    if (h->step_done) cudaEventDestroy(h->step_done);
+    if (h->step_stream) cudaStreamDestroy(h->step_stream);
     cudaFree(h->d_groups);
     cudaFree(h->d_warp_group);
     cudaFree(h->d_state);
@@ -1704,17 +1893,15 @@ espl_status espl_device_launch(espl_lanes* h, uint32_t max_steps, espl_step_repo
     espl_newton_opts op{t.reltol, t.abstol, t.vntol, 0.0, t.residual_tol, t.max_iter, 0};
     NewtonParams np = newton_params(op, h);
     CK(cudaEventRecord(h->ev0, h->stream));
+    bool learned = false;
+    if (t.predictor == 2)
+        for (auto& g : h->groups) learned |= g.pred != nullptr;
+    uint64_t launches = h->classes.size();
     espl_status s =
-        launch_classes(h, [&](const TileMap& m, uint32_t grid, uint32_t smem, cudaStream_t st, bool wide) {
-            if (np.mixed && wide)
-                k_tran<true, true><<<grid, kWideThreads, smem, st>>>(m, t, np, h->d_state);
-            else if (np.mixed)
-                k_tran<true, false><<<grid, kBlock, smem, st>>>(m, t, np, h->d_state);
-            else if (wide)
-                k_tran<false, true><<<grid, kWideThreads, smem, st>>>(m, t, np, h->d_state);
-            else
-                k_tran<false, false><<<grid, kBlock, smem, st>>>(m, t, np, h->d_state);
-        });
+        learned ? launch_learned(h, t, np, launches)
+                : launch_classes(h, [&](const TileMap& m, uint32_t grid, uint32_t smem, cudaStream_t st, bool wide) {
+                      launch_tran(m, grid, smem, st, wide, t, np, h->d_state);
+                  });
     if (s) return s;
     CK(cudaEventRecord(h->ev1, h->stream));
     CK(cudaEventSynchronize(h->ev1));
@@ -1722,7 +1909,7 @@ espl_status espl_device_launch(espl_lanes* h, uint32_t max_steps, espl_step_repo
     CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
     h->stats.newton_ms = ms;
     h->stats.total_ms += ms;
-    h->stats.launches += (uint32_t)h->classes.size();
+    h->stats.launches += launches;
     if ((s = retape_stale(h))) return s;
     CK(cudaMemcpyAsync(h->h_state.data(), h->d_state, sizeof(LaneState) * h->total_lanes, cudaMemcpyDeviceToHost,
                        h->stream));
@@ -1742,7 +1929,7 @@ espl_status espl_device_launch(espl_lanes* h, uint32_t max_steps, espl_step_repo
                 r.steps = st.steps;
                 r.rejects = st.rejects;
                 r.status = st.status;
-                r.reserved = 0;
+                r.learned_retries = st.pred_fallbacks;
             }
             k++;
         }
@@ -1871,6 +2058,121 @@ espl_status espl_request_stop(espl_lanes* h, uint32_t net, const uint8_t* stop) 
         if (stop[l] && host[l].status == 0) host[l].status = 4;
     CK(cudaMemcpyAsync(dev, host, sizeof(LaneState) * g.lanes, cudaMemcpyHostToDevice, h->stream));
     CK(cudaStreamSynchronize(h->stream));
+    return ESPL_OK;
+}
+
+espl_status espl_record_steps(espl_lanes* h, uint32_t net, uint32_t lane_stride, uint32_t from_step,
+                              uint32_t capacity) {
+    if (!h || net >= h->groups.size() || (capacity && lane_stride == 0)) return ESPL_INVALID_ARGUMENT;
+    Group& g = h->groups[net];
+    CK(cudaStreamSynchronize(h->stream));
+    for (void* p : g.rec_owned) cudaFree(p);
+    g.rec_owned.clear();
+    g.dev.rec_x = g.dev.rec_y = g.dev.rec_tag = nullptr;
+    g.dev.rec_count = nullptr;
+    g.dev.rec_cap = 0;
+    if (capacity) {
+        espl_status s;
+        if ((s = ensure_learn_buffers(h, g, false))) return s;
+        const size_t D = 3 * (size_t)g.n + 1;
+        if ((s = dalloc(h, g.rec_owned, &g.dev.rec_x, D * capacity)) ||
+            (s = dalloc(h, g.rec_owned, &g.dev.rec_y, (size_t)g.n * capacity)) ||
+            (s = dalloc(h, g.rec_owned, &g.dev.rec_tag, 5 * (size_t)capacity)) ||
+            (s = dalloc(h, g.rec_owned, &g.dev.rec_count, 1)))
+            return s;
+        g.dev.rec_cap = capacity;
+        g.dev.rec_stride = lane_stride;
+        g.dev.rec_from = from_step;
+    }
+    espl_status s = push_descs(h);
+    if (s) return s;
+    CK(cudaStreamSynchronize(h->stream));
+    return ESPL_OK;
+}
+
+espl_status espl_recorded_steps(espl_lanes* h, uint32_t net, const double** x, const double** y, uint32_t* count) {
+    if (!h || net >= h->groups.size()) return ESPL_INVALID_ARGUMENT;
+    Group& g = h->groups[net];
+    uint32_t k = 0;
+    if (g.dev.rec_count) {
+        CK(cudaMemcpyAsync(&k, g.dev.rec_count, sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        k = std::min(k, g.dev.rec_cap);
+    }
+    if (x) *x = g.dev.rec_x;
+    if (y) *y = g.dev.rec_y;
+    if (count) *count = k;
+    return ESPL_OK;
+}
+
+espl_status espl_copy_recorded_steps(espl_lanes* h, uint32_t net, double* x, double* y, double* tags, uint32_t cap) {
+    uint32_t k = 0;
+    espl_status s = espl_recorded_steps(h, net, nullptr, nullptr, &k);
+    if (s) return s;
+    const Group& g = h->groups[net];
+    k = std::min(k, cap);
+    if (!k) return ESPL_OK;
+    const size_t D = 3 * (size_t)g.n + 1;
+    if (x) CK(cudaMemcpyAsync(x, g.dev.rec_x, sizeof(double) * D * k, cudaMemcpyDeviceToHost, h->stream));
+    if (y) CK(cudaMemcpyAsync(y, g.dev.rec_y, sizeof(double) * g.n * k, cudaMemcpyDeviceToHost, h->stream));
+    if (tags) CK(cudaMemcpyAsync(tags, g.dev.rec_tag, sizeof(double) * 5 * k, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return ESPL_OK;
+}
+
+espl_status espl_set_step_predictor(espl_lanes* h, uint32_t net, espl_mlp* m) {
+    if (!h || net >= h->groups.size()) return ESPL_INVALID_ARGUMENT;
+    Group& g = h->groups[net];
+    if (m) {
+        mlp::MlpView v;
+        espl_status s = espl_mlp_view(m, &v, h->stream);
+        if (s) return fail(h, s, "the network could not be read");
+        if (v.in_dim != (int)(3 * g.n + 1) || v.out_dim != (int)g.n)
+            return fail(h, ESPL_INVALID_ARGUMENT, "a step predictor for " + std::to_string(g.n) +
+                                                      " unknowns takes " + std::to_string(3 * g.n + 1) +
+                                                      " inputs and gives " + std::to_string(g.n) + " outputs");
+        if ((s = ensure_learn_buffers(h, g, true))) return s;
+    }
+    g.pred = m;
+    espl_status s = push_descs(h);
+    if (s) return s;
+    CK(cudaStreamSynchronize(h->stream));
+    return ESPL_OK;
+}
+
+espl_status espl_step_predict(espl_lanes* h, uint32_t net, double* x_start, double* cur, double* prev, double* prev2,
+                              double* steps) {
+    if (!h || net >= h->groups.size()) return ESPL_INVALID_ARGUMENT;
+    Group& g = h->groups[net];
+    if (!g.pred || !h->tran_ready) return fail(h, ESPL_INVALID_ARGUMENT, "no step predictor or no transient");
+    std::vector<mlp::MlpView> views;
+    espl_status s = predictor_views(h, views, h->stream);
+    if (s) return s;
+    launch_predict(h, net, views[net], h->stream);
+    CK(cudaGetLastError());
+    std::vector<double> lm((size_t)g.n * g.P);
+    auto out = [&](const double* src, double* dst) -> espl_status {
+        if (!dst) return ESPL_OK;
+        CK(cudaMemcpyAsync(lm.data(), src, lm.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        for (uint32_t l = 0; l < g.lanes; l++)
+            for (uint32_t i = 0; i < g.n; i++) dst[(size_t)l * g.n + i] = lm[(size_t)i * g.P + l];
+        return ESPL_OK;
+    };
+    if ((s = out(g.dev.xpred, x_start)) || (s = out(g.dev.cur, cur)) || (s = out(g.dev.prev, prev)) ||
+        (s = out(g.dev.prev2, prev2)))
+        return s;
+    if (steps) {
+        std::vector<LaneState> st(g.lanes);
+        CK(cudaMemcpyAsync(st.data(), h->d_state + g.lane0, sizeof(LaneState) * g.lanes, cudaMemcpyDeviceToHost,
+                           h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        for (uint32_t l = 0; l < g.lanes; l++) {
+            steps[3 * (size_t)l] = st[l].dt;
+            steps[3 * (size_t)l + 1] = st[l].dt_old0;
+            steps[3 * (size_t)l + 2] = st[l].dt_old1;
+        }
+    }
     return ESPL_OK;
 }
 

@@ -111,6 +111,17 @@ struct GroupDev {
     double* x_good;
     uint32_t stage_mode;  // what a tile stages in shared memory (lane_smem.cuh)
     uint32_t refine_rows; // the row view is staged (FP32 refinement sweeps on)
+    // The learned next-step predictor (lane_learned.cuh): the accepted
+    // solution two steps back (null when neither a predictor nor a recorder
+    // is attached), the learned start of each lane's next attempt (null
+    // without a predictor), and the step recorder: samples of lanes l with
+    // l % rec_stride == 0 past step rec_from, at most rec_cap, their features
+    // (rec_x, 3 n + 1 per sample), targets (rec_y, n per sample) and tags
+    // (rec_tag, 5 per sample), the next free sample in *rec_count.
+    double *prev2, *xpred;
+    double *rec_x, *rec_y, *rec_tag;
+    uint32_t* rec_count;
+    uint32_t rec_stride, rec_from, rec_cap, rec_pad;
 };
 
 struct LaneState {
@@ -118,11 +129,23 @@ struct LaneState {
     double t, dt, dt_old0, dt_old1, bp_next, bp_save_dt;
     double m_prev_v, m_prev_t, m_first, m_last;
     unsigned long long attempts, nr_iters;
-    uint32_t bits, tick, iterations, fallbacks;
+    uint32_t bits, pred_fallbacks, iterations, fallbacks;  // pred_fallbacks: learned starts retried linearly
     uint32_t order, steps, status, rejects;
     uint32_t bp_clamped, m_cross, m_have, peel_slot;
-    uint32_t s_rot, fp64, peels, pad1;
+    uint32_t s_rot, fp64, peels, pred_lin;  // pred_lin: the next attempt starts from the linear predictor
 };
+
+// The three history features of unknown i (f[0] = cur, f[1] the linear
+// predictor's increment, f[2] the increment a step earlier). The recorder
+// (k_tran's accept) and the predictor (lane_learned.cuh) compute them with this one function,
+// so a sample's target y = x - (cur + f[1]) and the predictor's start
+// cur + f[1] + y agree to the bit.
+__host__ __device__ __forceinline__ void step_features(double cur, double prev, double prev2, double r0, double r1,
+                                                       double* f) {
+    f[0] = cur;
+    f[1] = r0 * (cur - prev);
+    f[2] = r1 * (prev - prev2);
+}
 
 // One lane's solve in a rung of the operating-point continuation ladder
 // (espl_solve_op): its diagonal gmin at the template's gmin stamps (0:

@@ -42,15 +42,17 @@ struct TileShared {
     GroupDev gd;  // the tile's template descriptor, index arrays staged
     uint32_t active[32];
     uint32_t bits[32];
-    uint32_t restore[32];
+    uint32_t restore[32];  // inside a Newton solve; after it, k_tran's recorder sample (reck)
     uint32_t accf[32];
     unsigned long long acc0[32], acc1[32], acc2[32];
     double limit[32];
     double ag0[32], ag1[32], ag2[32], t[32], xfact[32], dt_next[32];
     double lgmin[32], lsrc[32];  // the lane's ladder gmin and source scale
-    uint32_t method[32], on[32], accept[32], rot[32];
+    uint32_t method[32], on[32], accept[32], rot[32];  // on: bit 0 the lane attempts a step, bit 1 from xpred
     uint32_t pit[32];  // the lane's polish iterations so far
 };
+
+constexpr uint32_t kNoRec = 0xFFFFFFFFu;
 
 // Gate flags reduced over warps.
 constexpr uint32_t kLimited = 1, kImplausible = 2, kResidualMiss = 4;
@@ -555,6 +557,7 @@ __global__ void __launch_bounds__(kTileThreads) k_tran_init(TileMap m, TranParam
         gather_charge_row(d, l, i, cell_buf(d, 0));
         LM(d.cur, i) = LM(d.x, i);
         LM(d.prev, i) = LM(d.x, i);
+        if (d.prev2) LM(d.prev2, i) = LM(d.x, i);
         LM(d.q1, i) = LM(d.qrow, i);
         LM(d.q2, i) = LM(d.qrow, i);
         LM(d.ip, i) = 0.0;
@@ -594,6 +597,8 @@ __global__ void __launch_bounds__(kTileThreads) k_tran_init(TileMap m, TranParam
     s.m_first = s.m_last = NAN;
     s.fp64 = 0;
     s.peels = 0;
+    s.pred_lin = 0;
+    s.pred_fallbacks = 0;
     // the .meas passes start, reading the operating point at t = 0
     for (uint32_t p = 0; p < d.n_mpass; p++) {
         double* ms = d.mstate + (size_t)p * kMeasWords * P + l;
@@ -623,7 +628,7 @@ __global__ void __launch_bounds__(WIDE ? kWideThreads : kTileThreads, WIDE ? 1 :
     for (uint32_t attempt = 0; attempt < o.launch_steps; attempt++) {
         // stepBegin (kernels/lane.zig:508-545).
         if (warp == 0) {
-            uint32_t on = 0;
+            uint32_t on = 0, lrn = 0;
             if (s && s->status == 0) {
                 if (!(s->t < o.t_stop && !at_stop(s->t, o.t_stop) && s->steps < o.max_steps)) {
                     s->status = 1;
@@ -650,18 +655,24 @@ __global__ void __launch_bounds__(WIDE ? kWideThreads : kTileThreads, WIDE ? 1 :
                     sh.xfact[lane] = dt / s->dt_old0;
                     sh.rot[lane] = s->s_rot;
                     s->fp64 = 0;
+                    lrn = (o.predictor == 2 && d.xpred && s->steps >= 3 && !s->pred_lin) ? 1u : 0u;
                 }
             }
-            sh.on[lane] = on;
+            sh.on[lane] = on | (lrn << 1);
         }
         __syncthreads();
         bool on = c.valid && sh.on[lane];
         if (!__syncthreads_or(on)) break;
+        // The predictor: the learned start (k_step_predict wrote it before
+        // this attempt), else the linear one (predictor 1, and 2 until the
+        // lane has three accepted steps or after a learned start failed),
+        // else the last accepted point.
         if (on) {
             double xf = sh.xfact[lane];
+            const bool lrn = (sh.on[lane] & 2u) != 0;
             for (uint32_t i = warp; i < d.n; i += nw) {
                 double cu = LM(d.cur, i);
-                LM(d.x, i) = o.predictor == 1 ? cu + xf * (cu - LM(d.prev, i)) : cu;
+                LM(d.x, i) = lrn ? LM(d.xpred, i) : o.predictor != 0 ? cu + xf * (cu - LM(d.prev, i)) : cu;
             }
         }
         __syncthreads();
@@ -711,12 +722,20 @@ __global__ void __launch_bounds__(WIDE ? kWideThreads : kTileThreads, WIDE ? 1 :
         // stepEndA (kernels/lane.zig:563-654).
         if (warp == 0) {
             uint32_t acc = 0;
+            uint32_t rk = kNoRec;
             if (s && on) {
                 double dt = s->dt;
                 uint32_t method = sh.method[lane];
+                const bool lrn = (sh.on[lane] & 2u) != 0;
+                if (!lrn) s->pred_lin = 0;
                 s->attempts++;
                 if (!(sh.bits[lane] & kSingular)) s->nr_iters += s->iterations < o.max_iter ? s->iterations : o.max_iter;
-                if (!conv) {
+                if (!conv && lrn) {
+                    // plain Newton is the fallback: the same step again from
+                    // the linear predictor, not a rejected step
+                    s->pred_lin = 1;
+                    s->pred_fallbacks++;
+                } else if (!conv) {
                     s->rejects++;
                     s->order = 1;
                     if (o.fixed_step) {
@@ -762,10 +781,25 @@ __global__ void __launch_bounds__(WIDE ? kWideThreads : kTileThreads, WIDE ? 1 :
                     if (!reject) {
                         acc = 1;
                         sh.dt_next[lane] = dt_next;
+                        // the step recorder's sample of this accepted step
+                        if (d.rec_count && l % d.rec_stride == 0 && s->steps >= d.rec_from && s->steps >= 3) {
+                            const uint32_t k = atomicAdd(d.rec_count, 1u);
+                            if (k < d.rec_cap) {
+                                rk = k;
+                                double* tg = d.rec_tag + 5 * (size_t)k;
+                                tg[0] = (double)l;
+                                tg[1] = (double)s->steps;
+                                tg[2] = dt;
+                                tg[3] = s->dt_old0;
+                                tg[4] = s->dt_old1;
+                                d.rec_x[(size_t)k * (3 * d.n + 1) + 3 * d.n] = dt / o.dt_max;
+                            }
+                        }
                     }
                 }
             }
             sh.accept[lane] = acc;
+            sh.restore[lane] = rk;
         }
         __syncthreads();
         // Accept (lane_device.zig accept): row histories and companion currents.
@@ -773,12 +807,36 @@ __global__ void __launch_bounds__(WIDE ? kWideThreads : kTileThreads, WIDE ? 1 :
         if (acc) {
             double ag0 = sh.ag0[lane], ag1 = sh.ag1[lane], ag2 = sh.ag2[lane];
             uint32_t method = sh.method[lane];
+            // a recorded step: its features and target, before the histories shift
+            const uint32_t rk = sh.restore[lane];
+            double* fx = nullptr;
+            double* fy = nullptr;
+            double r0 = 0.0, r1 = 0.0;
+            if (rk != kNoRec) {
+                const LaneState& ls = st[d.lane0 + l];
+                fx = d.rec_x + (size_t)rk * (3 * d.n + 1);
+                fy = d.rec_y + (size_t)rk * d.n;
+                r0 = sh.xfact[lane];
+                r1 = ls.dt / ls.dt_old1;
+            }
             for (uint32_t i = warp; i < d.n; i += nw) {
                 const double q1 = LM(d.q1, i);
                 double dq = ag0 * (LM(d.qrow, i) - q1);
                 LM(d.ip, i) = method == 1 ? dq - ag1 * LM(d.ip, i) : method == 2 ? dq - ag2 * (q1 - LM(d.q2, i)) : dq;
                 LM(d.q2, i) = q1;
                 LM(d.q1, i) = LM(d.qrow, i);
+                if (d.prev2) {
+                    const double cu = LM(d.cur, i), pv = LM(d.prev, i);
+                    if (fx) {
+                        double f[3];
+                        step_features(cu, pv, LM(d.prev2, i), r0, r1, f);
+                        fx[i] = f[0];
+                        fx[d.n + i] = f[1];
+                        fx[2 * d.n + i] = f[2];
+                        fy[i] = LM(d.x, i) - (cu + f[1]);
+                    }
+                    LM(d.prev2, i) = pv;
+                }
                 LM(d.prev, i) = LM(d.cur, i);
                 LM(d.cur, i) = LM(d.x, i);
             }

@@ -134,6 +134,124 @@ __global__ void k_gather_rows(const __nv_bfloat16* __restrict__ xs, const float*
 
 inline unsigned blocks(long long n, int t = 256) { return (unsigned)((n + t - 1) / t); }
 
+// The BF16 weight image (weight_image_bytes): W1, W2, W3 from the FP32
+// master weights as K-major core-matrix tiles, back to back.
+__global__ void k_pack_image(const float* __restrict__ w1, const float* __restrict__ w2, const float* __restrict__ w3,
+                             int dp, int op, unsigned char* __restrict__ image) {
+    const long long n1 = 128LL * dp, n2 = 128LL * 128, n3 = (long long)op * 128;
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < n1) {
+        const int r = (int)(i / dp), k = (int)(i % dp);
+        *reinterpret_cast<__nv_bfloat16*>(image + tile_off_k(r, k, dp)) = __float2bfloat16(w1[i]);
+        return;
+    }
+    i -= n1;
+    unsigned char* t2 = image + n1 * 2;
+    if (i < n2) {
+        const int r = (int)(i / 128), k = (int)(i % 128);
+        *reinterpret_cast<__nv_bfloat16*>(t2 + tile_off_k(r, k, 128)) = __float2bfloat16(w2[i]);
+        return;
+    }
+    i -= n2;
+    unsigned char* t3 = t2 + n2 * 2;
+    if (i < n3) {
+        const int r = (int)(i / 128), k = (int)(i % 128);
+        *reinterpret_cast<__nv_bfloat16*>(t3 + tile_off_k(r, k, 128)) = __float2bfloat16(w3[i]);
+    }
+}
+
+// Per column j of a rows x cols FP64 matrix (row-major): out[2 j] = the sum
+// and out[2 j + 1] = the sum of squares over the rows. One block per column.
+__global__ void k_col_stats(const double* __restrict__ a, long long rows, int cols, double* __restrict__ out) {
+    const int j = blockIdx.x;
+    double s = 0.0, s2 = 0.0;
+    for (long long r = threadIdx.x; r < rows; r += blockDim.x) {
+        const double v = a[r * cols + j];
+        s += v;
+        s2 += v * v;
+    }
+    __shared__ double ps[256], ps2[256];
+    ps[threadIdx.x] = s;
+    ps2[threadIdx.x] = s2;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) {
+            ps[threadIdx.x] += ps[threadIdx.x + w];
+            ps2[threadIdx.x] += ps2[threadIdx.x + w];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        out[2 * j] = ps[0];
+        out[2 * j + 1] = ps2[0];
+    }
+}
+
+struct InferArgs {
+    const double* x;          // rows x in_dim, raw parameters
+    double* y;                // rows x out_dim, de-standardized predictions
+    const float *w1, *b1, *w2, *b2, *w3, *b3;  // FP32 master weights (padded layouts)
+    const float *in_mean, *in_std, *out_mean, *out_std;
+    int rows, in_dim, dp, out_dim, op;
+    int* err;
+};
+
+// The whole network for one 128-row tile in one CTA (mlp_layers): the
+// standardized input tile and the three weight matrices in shared memory,
+// the output layer de-standardized to FP64.
+__global__ void __launch_bounds__(128) k_mlp_infer(InferArgs g) {
+    extern __shared__ __align__(1024) unsigned char dsm[];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ uint32_t tmem_base;
+    __shared__ int failed;
+    const int H = 128, dp = g.dp, op = g.op;
+    unsigned char* sx = dsm;                        // 128 x dp
+    unsigned char* sw1 = sx + 128 * dp * 2;         // 128 x dp
+    unsigned char* sw2 = sw1 + 128 * dp * 2;        // 128 x 128
+    unsigned char* sw3 = sw2 + 128 * 128 * 2;       // op x 128
+    unsigned char* sh = sw3 + (size_t)op * 128 * 2; // 128 x 128 activations
+    const int warp = threadIdx.x >> 5;
+    const int r0 = blockIdx.x * 128;
+    if (threadIdx.x == 0) {
+        mbar_init1(&bar);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        failed = 0;
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
+                     "r"(128u)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    // operands: standardized inputs and the BF16 weights
+    for (int e = threadIdx.x; e < 128 * dp; e += blockDim.x) {
+        int r = e / dp, k = e % dp;
+        float v = 0.0f;
+        if (r0 + r < g.rows && k < g.in_dim)
+            v = (float)((g.x[(long long)(r0 + r) * g.in_dim + k] - (double)g.in_mean[k]) / (double)g.in_std[k]);
+        *reinterpret_cast<__nv_bfloat16*>(sx + tile_off_k(r, k, dp)) = __float2bfloat16(v);
+    }
+    stage_weights(sw1, g.w1, H, dp);
+    stage_weights(sw2, g.w2, H, H);
+    stage_weights(sw3, g.w3, op, H);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_base;
+    mlp_layers(sx, sw1, sw2, sw3, sh, g.b1, g.b2, g.b3, dp, op, g.out_dim, tmem, &bar, &failed,
+               [&](int row, int o, float v) {
+                   if (r0 + row < g.rows)
+                       g.y[(long long)(r0 + row) * g.out_dim + o] =
+                           (double)v * (double)g.out_std[o] + (double)g.out_mean[o];
+               });
+    if (failed && threadIdx.x == 0) atomicExch(g.err, 1);
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(128u) : "memory");
+}
+
 }  // namespace
 
 struct espl_mlp {
@@ -144,7 +262,12 @@ struct espl_mlp {
     float *p = nullptr, *g = nullptr, *m = nullptr, *v = nullptr;
     __nv_bfloat16 *w1b = nullptr, *w2b = nullptr, *w3b = nullptr;
     float *in_mean = nullptr, *in_std = nullptr, *out_mean = nullptr, *out_std = nullptr;
+    float* out_gain = nullptr;  // out_std, 0 for an output constant over the training set
     bool scaled = false;
+    // the BF16 weight image of the step predictor, rebuilt when the weights
+    // have changed (weights_version) since it was packed (image_version)
+    unsigned char* image = nullptr;
+    uint64_t weights_version = 1, image_version = 0;
     // batch buffers (cap rows)
     double *x_raw = nullptr, *y_raw = nullptr;
     __nv_bfloat16 *xb = nullptr, *h1b = nullptr, *h2b = nullptr, *dyb = nullptr, *dzb = nullptr;
@@ -208,6 +331,7 @@ espl_status refresh_bf16(espl_mlp* h) {
     k_to_bf16<<<blocks((long long)h->H * h->H), 256, 0, h->stream>>>(h->p + h->off_w2, h->w2b, (long long)h->H * h->H);
     k_to_bf16<<<blocks((long long)h->Op * h->H), 256, 0, h->stream>>>(h->p + h->off_w3, h->w3b, (long long)h->Op * h->H);
     MCK(cudaGetLastError());
+    h->weights_version++;
     return ESPL_OK;
 }
 
@@ -297,34 +421,79 @@ espl_status upload(espl_mlp* h, const double* x, const double* y, const std::vec
     return ESPL_OK;
 }
 
-espl_status set_scaling(espl_mlp* h, const double* x, const double* y, uint32_t n) {
-    auto stats = [&](const double* a, int cols, int ld, std::vector<float>& mean, std::vector<float>& sd) {
+// Uploads per-column means and standard deviations (sums and sums of
+// squares over n rows in; a column whose deviation is at most 1e-12 is
+// scaled by 1 and, for an output, marked constant: out_gain 0).
+espl_status upload_scaling(espl_mlp* h, const std::vector<double>& xs, const std::vector<double>& ys, uint32_t n) {
+    auto finish = [&](const std::vector<double>& sums, int cols, int ld, std::vector<float>& mean,
+                      std::vector<float>& sd, std::vector<float>* gain) {
         mean.assign(ld, 0.0f);
         sd.assign(ld, 1.0f);
+        if (gain) gain->assign(ld, 0.0f);
         for (int j = 0; j < cols; j++) {
-            double s = 0, s2 = 0;
-            for (uint32_t r = 0; r < n; r++) s += a[(size_t)r * cols + j];
-            double mu = s / n;
-            for (uint32_t r = 0; r < n; r++) {
-                double e = a[(size_t)r * cols + j] - mu;
-                s2 += e * e;
-            }
-            double sdv = std::sqrt(s2 / std::max<uint32_t>(n, 1));
+            const double mu = sums[2 * j] / n;
+            const double var = std::max(0.0, sums[2 * j + 1] / n - mu * mu);
+            const double sdv = std::sqrt(var);
             mean[j] = (float)mu;
             sd[j] = (float)(sdv > 1e-12 ? sdv : 1.0);
+            if (gain) (*gain)[j] = sdv > 1e-12 ? (float)sdv : 0.0f;
         }
     };
-    std::vector<float> im, is, om, os;
-    stats(x, h->D, h->Dp, im, is);
-    stats(y, h->O, h->Op, om, os);
+    std::vector<float> im, is, om, os, og;
+    finish(xs, h->D, h->Dp, im, is, nullptr);
+    finish(ys, h->O, h->Op, om, os, &og);
     MCK(cudaMemcpyAsync(h->in_mean, im.data(), sizeof(float) * h->Dp, cudaMemcpyHostToDevice, h->stream));
     MCK(cudaMemcpyAsync(h->in_std, is.data(), sizeof(float) * h->Dp, cudaMemcpyHostToDevice, h->stream));
     MCK(cudaMemcpyAsync(h->out_mean, om.data(), sizeof(float) * h->Op, cudaMemcpyHostToDevice, h->stream));
     MCK(cudaMemcpyAsync(h->out_std, os.data(), sizeof(float) * h->Op, cudaMemcpyHostToDevice, h->stream));
+    MCK(cudaMemcpyAsync(h->out_gain, og.data(), sizeof(float) * h->Op, cudaMemcpyHostToDevice, h->stream));
     MCK(cudaStreamSynchronize(h->stream));
     h->scaled = true;
     return ESPL_OK;
 }
+
+espl_status set_scaling(espl_mlp* h, const double* x, const double* y, uint32_t n) {
+    auto sums = [&](const double* a, int cols) {
+        std::vector<double> out(2 * (size_t)cols, 0.0);
+        for (int j = 0; j < cols; j++) {
+            double s = 0, s2 = 0;
+            for (uint32_t r = 0; r < n; r++) s += a[(size_t)r * cols + j];
+            const double mu = s / std::max<uint32_t>(n, 1);
+            for (uint32_t r = 0; r < n; r++) {
+                const double e = a[(size_t)r * cols + j] - mu;
+                s2 += e * e;
+            }
+            // the second pass's centred sum, returned as the raw form the
+            // finisher expects: sum of squares = centred + n mu^2
+            out[2 * j] = s;
+            out[2 * j + 1] = s2 + (double)n * mu * mu;
+        }
+        return out;
+    };
+    return upload_scaling(h, sums(x, h->D), sums(y, h->O), n);
+}
+
+// The same from rows already on the device (FP64, row-major).
+espl_status set_scaling_device(espl_mlp* h, const double* x, const double* y, uint32_t n) {
+    double* d = nullptr;
+    MCK(cudaMalloc(&d, sizeof(double) * 2 * (h->D + h->O)));
+    k_col_stats<<<h->D, 256, 0, h->stream>>>(x, n, h->D, d);
+    k_col_stats<<<h->O, 256, 0, h->stream>>>(y, n, h->O, d + 2 * h->D);
+    std::vector<double> all(2 * (size_t)(h->D + h->O));
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(all.data(), d, sizeof(double) * all.size(), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(d);
+    if (e != cudaSuccess) {
+        h->msg = std::string("column statistics: ") + cudaGetErrorString(e);
+        return ESPL_DRIVER;
+    }
+    std::vector<double> xs(all.begin(), all.begin() + 2 * h->D), ys(all.begin() + 2 * h->D, all.end());
+    return upload_scaling(h, xs, ys, n);
+}
+
+espl_status train_resident(espl_mlp* h, const double* xr, const double* yr, uint32_t n, const espl_train_opts* o,
+                           double* epoch_loss);
 
 }  // namespace
 
@@ -374,6 +543,8 @@ espl_status espl_mlp_create(uint32_t in_dim, uint32_t out_dim, uint32_t capacity
     AL(in_std, h->Dp);
     AL(out_mean, h->Op);
     AL(out_std, h->Op);
+    AL(out_gain, h->Op);
+    AL(image, weight_image_bytes(h->Dp, h->Op));
     const size_t c = (size_t)h->cap;
     AL(x_raw, c * h->D);
     AL(y_raw, c * h->O);
@@ -409,6 +580,7 @@ espl_status espl_mlp_create(uint32_t in_dim, uint32_t out_dim, uint32_t capacity
     std::vector<float> ones(std::max(h->Dp, h->Op), 1.0f);
     cudaMemcpyAsync(h->in_std, ones.data(), sizeof(float) * h->Dp, cudaMemcpyHostToDevice, h->stream);
     cudaMemcpyAsync(h->out_std, ones.data(), sizeof(float) * h->Op, cudaMemcpyHostToDevice, h->stream);
+    cudaMemcpyAsync(h->out_gain, ones.data(), sizeof(float) * h->Op, cudaMemcpyHostToDevice, h->stream);
     if ((s = refresh_bf16(h))) return bail(s);
     if (cudaStreamSynchronize(h->stream) != cudaSuccess) return bail(ESPL_DRIVER);
     *out = h;
@@ -505,11 +677,50 @@ espl_status espl_mlp_train(espl_mlp* h, const double* x, const double* y, uint32
         return ESPL_INVALID_ARGUMENT;
     espl_status s = ESPL_OK;
     if (!h->scaled && (s = set_scaling(h, x, y, n))) return s;
+    double *xr = nullptr, *yr = nullptr;
+    if (cudaMalloc(&xr, sizeof(double) * n * h->D) != cudaSuccess) {
+        h->msg = "out of device memory for the training set";
+        return ESPL_OUT_OF_MEMORY;
+    }
+    if (cudaMalloc(&yr, sizeof(double) * n * h->O) != cudaSuccess) {
+        cudaFree(xr);
+        h->msg = "out of device memory for the training set";
+        return ESPL_OUT_OF_MEMORY;
+    }
+    if (cudaMemcpyAsync(xr, x, sizeof(double) * n * h->D, cudaMemcpyHostToDevice, h->stream) != cudaSuccess ||
+        cudaMemcpyAsync(yr, y, sizeof(double) * n * h->O, cudaMemcpyHostToDevice, h->stream) != cudaSuccess)
+        s = ESPL_DRIVER;
+    if (!s) s = train_resident(h, xr, yr, n, o, epoch_loss);
+    cudaStreamSynchronize(h->stream);
+    cudaFree(xr);
+    cudaFree(yr);
+    return s;
+}
+
+espl_status espl_mlp_train_device(espl_mlp* h, const double* x, const double* y, uint32_t n,
+                                  const espl_train_opts* o, double* epoch_loss) {
+    if (!h || !x || !y || n == 0 || !o || o->batch == 0 || (int)o->batch > h->cap || o->epochs == 0 ||
+        o->batch > n)
+        return ESPL_INVALID_ARGUMENT;
+    espl_status s = ESPL_OK;
+    if (!h->scaled && (s = set_scaling_device(h, x, y, n))) return s;
+    return train_resident(h, x, y, n, o, epoch_loss);
+}
+
+}  // extern "C"
+
+namespace {
+
+// The training loop over rows already on the device (x: n x D, y: n x O,
+// FP64, row-major), standardized once into BF16 inputs and FP32 targets.
+espl_status train_resident(espl_mlp* h, const double* xr, const double* yr, uint32_t n, const espl_train_opts* o,
+                           double* epoch_loss) {
+    espl_status s = ESPL_OK;
     const uint32_t chunk_ep = std::max(1u, std::min(o->epochs, (uint32_t)((64u << 20) / (sizeof(uint32_t) * n))));
     // The data set stays on the device, standardized; the epochs'
     // permutations go up in chunks of up to 64 MB and every Adam step
     // gathers its rows on the device.
-    double *xr = nullptr, *yr = nullptr, *lsum = nullptr;
+    double* lsum = nullptr;
     __nv_bfloat16* xs = nullptr;
     float* ts = nullptr;
     uint32_t* perm = nullptr;
@@ -523,15 +734,12 @@ espl_status espl_mlp_train(espl_mlp* h, const double* x, const double* y, uint32
         cudaStreamSynchronize(h->stream);
         for (void* q : tmp) cudaFree(q);
     };
-    if (dalloc((void**)&xr, sizeof(double) * n * h->D) || dalloc((void**)&yr, sizeof(double) * n * h->O) ||
-        dalloc((void**)&xs, sizeof(__nv_bfloat16) * n * h->Dp) || dalloc((void**)&ts, sizeof(float) * n * h->Op) ||
+    if (dalloc((void**)&xs, sizeof(__nv_bfloat16) * n * h->Dp) || dalloc((void**)&ts, sizeof(float) * n * h->Op) ||
         dalloc((void**)&perm, sizeof(uint32_t) * n * chunk_ep) || dalloc((void**)&lsum, sizeof(double) * o->epochs)) {
         cleanup();
         h->msg = "out of device memory for the training set";
         return ESPL_OUT_OF_MEMORY;
     }
-    cudaMemcpyAsync(xr, x, sizeof(double) * n * h->D, cudaMemcpyHostToDevice, h->stream);
-    cudaMemcpyAsync(yr, y, sizeof(double) * n * h->O, cudaMemcpyHostToDevice, h->stream);
     cudaMemsetAsync(lsum, 0, sizeof(double) * o->epochs, h->stream);
     k_standardize<<<blocks((long long)n * h->Dp), 256, 0, h->stream>>>(xr, (int)n, h->D, h->Dp, h->in_mean, h->in_std,
                                                                         nullptr, xs);
@@ -591,6 +799,10 @@ espl_status espl_mlp_train(espl_mlp* h, const double* x, const double* y, uint32
     cleanup();
     return s;
 }
+
+}  // namespace
+
+extern "C" {
 
 espl_status espl_mlp_predict(espl_mlp* h, const double* x, uint32_t n, double* y) {
     if (!h || !x || !y) return ESPL_INVALID_ARGUMENT;
@@ -659,3 +871,31 @@ espl_status espl_mlp_error_message(espl_mlp* h, char* buf, size_t cap) {
 }
 
 }  // extern "C"
+
+uint32_t espl_mlp_view(espl_mlp* h, espl::mlp::MlpView* v, void* stream) {
+    if (!h || !v) return ESPL_INVALID_ARGUMENT;
+    if (h->image_version != h->weights_version) {
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        // the weights are written on the network's stream
+        if (cudaStreamSynchronize(h->stream) != cudaSuccess) return ESPL_DRIVER;
+        const long long total = 128LL * h->Dp + 128LL * 128 + (long long)h->Op * 128;
+        k_pack_image<<<blocks(total), 256, 0, st>>>(h->p + h->off_w1, h->p + h->off_w2, h->p + h->off_w3, h->Dp, h->Op,
+                                                    h->image);
+        if (cudaGetLastError() != cudaSuccess) return ESPL_DRIVER;
+        h->image_version = h->weights_version;
+    }
+    v->image = h->image;
+    v->b1 = h->p + h->off_b1;
+    v->b2 = h->p + h->off_b2;
+    v->b3 = h->p + h->off_b3;
+    v->in_mean = h->in_mean;
+    v->in_std = h->in_std;
+    v->out_mean = h->out_mean;
+    v->out_gain = h->out_gain;
+    v->in_dim = h->D;
+    v->dp = h->Dp;
+    v->out_dim = h->O;
+    v->op = h->Op;
+    v->err = h->err;
+    return ESPL_OK;
+}

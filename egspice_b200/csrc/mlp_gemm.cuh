@@ -409,15 +409,6 @@ __device__ __forceinline__ uint32_t tile_off_k(uint32_t r, uint32_t k, uint32_t 
     return ((r >> 3) * (k_cols / 8) + (k >> 3)) * 128u + (r & 7u) * 16u + (k & 7u) * 2u;
 }
 
-struct InferArgs {
-    const double* x;          // rows x in_dim, raw parameters
-    double* y;                // rows x out_dim, de-standardized predictions
-    const float *w1, *b1, *w2, *b2, *w3, *b3;  // FP32 master weights (padded layouts)
-    const float *in_mean, *in_std, *out_mean, *out_std;
-    int rows, in_dim, dp, out_dim, op;
-    int* err;
-};
-
 // Loads a FP32 weight matrix [n_rows x k_cols] (row-major, ld = k_cols) into
 // a K-major BF16 tile.
 __device__ __forceinline__ void stage_weights(unsigned char* tile, const float* w, int n_rows, int k_cols) {
@@ -427,55 +418,37 @@ __device__ __forceinline__ void stage_weights(unsigned char* tile, const float* 
     }
 }
 
-// The whole network for one 128-row tile in one CTA: the standardized input
-// tile and the three weight matrices in shared memory, each layer one chain
-// of tcgen05.mma into tensor memory, its epilogue (bias, tanh) written back
-// to shared memory as the next layer's BF16 operand, the output layer
-// de-standardized to FP64. Dynamic shared memory: infer_smem_bytes.
+// Dynamic shared memory of a whole-network tile: the input tile, the three
+// weight tiles and the hidden activations.
 __host__ __device__ inline size_t infer_smem_bytes(int dp, int op) {
     return (size_t)128 * dp * 2 + 128 * dp * 2 + 128 * 128 * 2 + (size_t)op * 128 * 2 + 128 * 128 * 2;
 }
 
-__global__ void __launch_bounds__(128) k_mlp_infer(InferArgs g) {
-    extern __shared__ __align__(1024) unsigned char dsm[];
-    __shared__ __align__(8) uint64_t bar;
-    __shared__ uint32_t tmem_base;
-    __shared__ int failed;
-    const int H = 128, dp = g.dp, op = g.op;
-    unsigned char* sx = dsm;                        // 128 x dp
-    unsigned char* sw1 = sx + 128 * dp * 2;         // 128 x dp
-    unsigned char* sw2 = sw1 + 128 * dp * 2;        // 128 x 128
-    unsigned char* sw3 = sw2 + 128 * 128 * 2;       // op x 128
-    unsigned char* sh = sw3 + (size_t)op * 128 * 2; // 128 x 128 activations
+// The three BF16 weight tiles (W1 128 x dp, W2 128 x 128, W3 op x 128) laid
+// out exactly as a whole-network tile stages them, back to back: a kernel
+// copies this image into shared memory with one bulk copy.
+__host__ __device__ inline size_t weight_image_bytes(int dp, int op) {
+    return (size_t)128 * dp * 2 + 128 * 128 * 2 + (size_t)op * 128 * 2;
+}
+
+// The three layers of one 128-row tile on the tensor cores. sx holds the
+// standardized BF16 inputs (dp columns) and sw1 / sw2 / sw3 the BF16 weights,
+// all K-major core-matrix tiles in shared memory; sh (128 x 128 BF16) takes
+// the hidden activations. Each layer is one chain of tcgen05.mma (K = 16 per
+// MMA) into the tensor memory at `tmem` (128 columns), committed to `bar`;
+// its epilogue (bias, tanh) goes back to sh as the next layer's operand. The
+// output layer calls out(row, o, acc + b3[o]) for every o < out_dim, row
+// being this thread's tile row (still standardized). Every thread of the
+// 128-thread block takes part. Returns false when a bounded wait ran out,
+// after a second bounded wait for the MMAs in flight; the caller frees the
+// tensor memory either way.
+template <typename Out>
+__device__ bool mlp_layers(const unsigned char* sx, const unsigned char* sw1, const unsigned char* sw2,
+                           const unsigned char* sw3, unsigned char* sh, const float* b1, const float* b2,
+                           const float* b3, int dp, int op, int out_dim, uint32_t tmem, uint64_t* bar, int* failed,
+                           Out out) {
+    const int H = 128;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int r0 = blockIdx.x * 128;
-    if (threadIdx.x == 0) {
-        mbar_init1(&bar);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        failed = 0;
-    }
-    if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
-                     "r"(128u)
-                     : "memory");
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-    }
-    // operands: standardized inputs and the BF16 weights
-    for (int e = threadIdx.x; e < 128 * dp; e += blockDim.x) {
-        int r = e / dp, k = e % dp;
-        float v = 0.0f;
-        if (r0 + r < g.rows && k < g.in_dim)
-            v = (float)((g.x[(long long)(r0 + r) * g.in_dim + k] - (double)g.in_mean[k]) / (double)g.in_std[k]);
-        *reinterpret_cast<__nv_bfloat16*>(sx + tile_off_k(r, k, dp)) = __float2bfloat16(v);
-    }
-    stage_weights(sw1, g.w1, H, dp);
-    stage_weights(sw2, g.w2, H, H);
-    stage_weights(sw3, g.w3, op, H);
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    __syncthreads();
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const uint32_t tmem = tmem_base;
     const int row = warp * 32 + lane;
     const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
     uint32_t phase = 0;
@@ -492,18 +465,18 @@ __global__ void __launch_bounds__(128) k_mlp_infer(InferArgs g) {
                 uint64_t db = smem_desc_k(smem_u32(b) + j * 256u, (uint32_t)kc);
                 tc_mma(tmem, da, db, idesc, j > 0 ? 1u : 0u);
             }
-            tc_commit(&bar);
+            tc_commit(bar);
         }
-        if (!mbar_wait_bounded(&bar, phase)) failed = 1;
+        if (!mbar_wait_bounded(bar, phase)) *failed = 1;
         __syncthreads();
-        if (failed) {
-            mbar_wait_bounded(&bar, phase);
-            break;
+        if (*failed) {
+            mbar_wait_bounded(bar, phase);
+            return false;
         }
         phase ^= 1u;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         if (layer < 2) {
-            const float* bias = layer == 0 ? g.b1 : g.b2;
+            const float* bias = layer == 0 ? b1 : b2;
             for (int c0 = 0; c0 < H; c0 += 16) {
                 float v[16];
                 tc_ld16(trow + (uint32_t)c0, v);
@@ -520,24 +493,34 @@ __global__ void __launch_bounds__(128) k_mlp_infer(InferArgs g) {
             for (int c0 = 0; c0 < op; c0 += 16) {
                 float v[16];
                 tc_ld16(trow + (uint32_t)c0, v);
-                if (r0 + row < g.rows) {
 #pragma unroll
-                    for (int i = 0; i < 16; i++) {
-                        int o = c0 + i;
-                        if (o < g.out_dim)
-                            g.y[(long long)(r0 + row) * g.out_dim + o] =
-                                (double)(v[i] + g.b3[o]) * (double)g.out_std[o] + (double)g.out_mean[o];
-                    }
+                for (int i = 0; i < 16; i++) {
+                    const int o = c0 + i;
+                    if (o < out_dim) out(row, o, v[i] + b3[o]);
                 }
             }
         }
     }
-    if (failed && threadIdx.x == 0) atomicExch(g.err, 1);
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    __syncthreads();
-    if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(128u) : "memory");
+    return true;
 }
+
+// What a kernel outside the network's own module reads of a trained network
+// (the transient's step predictor): the weight image (weight_image_bytes),
+// the biases, the input standardization and the output scaling. out_gain[o]
+// is the output's standard deviation, 0 for an output that was constant over
+// the training set (its prediction is then out_mean[o] exactly).
+struct MlpView {
+    const unsigned char* image;
+    const float *b1, *b2, *b3;
+    const float *in_mean, *in_std, *out_mean, *out_gain;
+    int in_dim, dp, out_dim, op;
+    int* err;
+};
 
 }  // namespace mlp
 }  // namespace espl
+
+struct espl_mlp;
+// Fills `v` for network `h` (packing the weight image first when the
+// weights changed since the last call). ESPL_OK or a driver error code.
+uint32_t espl_mlp_view(espl_mlp* h, espl::mlp::MlpView* v, void* stream);

@@ -84,6 +84,16 @@ def lib():
         L.espl_get_classes.restype = C.c_uint32
         L.espl_error_message.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t]
         L.espl_error_message.restype = C.c_uint32
+        L.espl_record_steps.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32]
+        L.espl_record_steps.restype = C.c_uint32
+        L.espl_recorded_steps.argtypes = [C.c_void_p, C.c_uint32, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), u32p]
+        L.espl_recorded_steps.restype = C.c_uint32
+        L.espl_copy_recorded_steps.argtypes = [C.c_void_p, C.c_uint32, f64p, f64p, f64p, C.c_uint32]
+        L.espl_copy_recorded_steps.restype = C.c_uint32
+        L.espl_set_step_predictor.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p]
+        L.espl_set_step_predictor.restype = C.c_uint32
+        L.espl_step_predict.argtypes = [C.c_void_p, C.c_uint32, f64p, f64p, f64p, f64p, f64p]
+        L.espl_step_predict.restype = C.c_uint32
         _lib = L
     return _lib
 
@@ -330,6 +340,47 @@ class Lanes:
         assert m.shape == (self.nets[net].lanes,)
         self._check(lib().espl_request_stop(self.h, net, m.ctypes.data_as(C.POINTER(C.c_uint8))),
                     "espl_request_stop")
+
+    def record_steps(self, net: int, lane_stride: int, from_step: int, capacity: int):
+        """Records training samples of the learned step predictor from the
+        accepted steps of template `net` (espl_record_steps): lanes l with
+        l % lane_stride == 0, steps past `from_step`, at most `capacity`."""
+        self._check(lib().espl_record_steps(self.h, net, lane_stride, from_step, capacity), "espl_record_steps")
+
+    def recorded(self, net: int):
+        """(x device pointer, y device pointer, count) of the samples
+        recorded for template `net`."""
+        x, y, n = C.c_void_p(), C.c_void_p(), C.c_uint32()
+        self._check(lib().espl_recorded_steps(self.h, net, C.byref(x), C.byref(y), C.byref(n)), "espl_recorded_steps")
+        return x.value, y.value, n.value
+
+    def recorded_host(self, net: int):
+        """Host copies of the recorded samples: x [count, 3 n + 1], y [count, n],
+        tags [count, 5] (lane, accepted steps before, dt, h0, h1)."""
+        n = self.nets[net].n
+        _, _, k = self.recorded(net)
+        x, y, t = np.zeros((max(k, 1), 3 * n + 1)), np.zeros((max(k, 1), n)), np.zeros((max(k, 1), 5))
+        self._check(lib().espl_copy_recorded_steps(self.h, net, x.ctypes.data_as(f64p), y.ctypes.data_as(f64p),
+                                                   t.ctypes.data_as(f64p), k), "espl_copy_recorded_steps")
+        return x[:k], y[:k], t[:k]
+
+    def set_step_predictor(self, net: int, mlp) -> None:
+        """Attaches a trained `learned.Mlp` (3 n + 1 inputs, n outputs) as
+        template `net`'s step predictor; None detaches."""
+        self._check(lib().espl_set_step_predictor(self.h, net, mlp.h if mlp is not None else None),
+                    "espl_set_step_predictor")
+
+    def step_predict(self, net: int) -> dict:
+        """The learned start of each lane's next attempt and the history it
+        was computed from: x_start, cur, prev, prev2 [lanes, n] and steps
+        [lanes, 3] (dt, h0, h1)."""
+        nl = self.nets[net]
+        out = {k: np.zeros((nl.lanes, nl.n)) for k in ("x_start", "cur", "prev", "prev2")}
+        out["steps"] = np.zeros((nl.lanes, 3))
+        self._check(lib().espl_step_predict(self.h, net, *[out[k].ctypes.data_as(f64p) for k in
+                                                          ("x_start", "cur", "prev", "prev2", "steps")]),
+                    "espl_step_predict")
+        return out
 
     def classes(self) -> List[dict]:
         """The launch classes in launch order, each with its kernel's device

@@ -6,6 +6,13 @@ rest of a sweep. Newton from a predicted x is the same plain Newton
 (espl_solve_static) with the same tolerances, so only the iteration count
 changes; a lane that does not converge from its prediction is solved again
 from the nominal start (bench.py run_learned_dc).
+
+`learned_transient` is the transient's learned next-step predictor: the
+plain linear predictor runs the first steps while the accepted steps are
+recorded on the device, a network is trained on them there, and the rest of
+the transient starts each attempt from the network's prediction (predictor
+2), the plain Newton judging every step and retrying a failed learned start
+from the linear predictor.
 """
 from __future__ import annotations
 
@@ -41,11 +48,12 @@ def _setup(L):
     L.espl_mlp_set_scaling.argtypes = [C.c_void_p, f64p, f64p, C.c_uint32]
     L.espl_mlp_loss_grad.argtypes = [C.c_void_p, f64p, f64p, C.c_uint32, f64p, f32p]
     L.espl_mlp_train.argtypes = [C.c_void_p, f64p, f64p, C.c_uint32, C.POINTER(TrainOpts), f64p]
+    L.espl_mlp_train_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(TrainOpts), f64p]
     L.espl_mlp_predict.argtypes = [C.c_void_p, f64p, C.c_uint32, f64p]
     L.espl_mlp_predict_layers.argtypes = [C.c_void_p, f64p, C.c_uint32, f64p]
     L.espl_mlp_error_message.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t]
     for f in ("create", "destroy", "param_count", "get_params", "set_params", "set_scaling", "loss_grad", "train",
-              "predict", "predict_layers", "error_message"):
+              "train_device", "predict", "predict_layers", "error_message"):
         getattr(L, "espl_mlp_" + f).restype = C.c_uint32
     L._mlp_ready = True
     return L
@@ -116,6 +124,15 @@ class Mlp:
                                           C.byref(opts), losses.ctypes.data_as(f64p)), "train")
         return losses
 
+    def train_device(self, x_ptr: int, y_ptr: int, n: int, opts: Optional[TrainOpts] = None) -> np.ndarray:
+        """Training on n rows already in device memory (espl_mlp_train_device),
+        e.g. the transient's recorded steps (Lanes.recorded)."""
+        opts = opts or train_opts()
+        losses = np.zeros(opts.epochs)
+        self._check(self.L.espl_mlp_train_device(self.h, C.c_void_p(x_ptr), C.c_void_p(y_ptr), n, C.byref(opts),
+                                                 losses.ctypes.data_as(f64p)), "train_device")
+        return losses
+
     def predict(self, x, fused: bool = True) -> np.ndarray:
         x = _f64(x)
         y = np.zeros((len(x), self.out_dim))
@@ -128,3 +145,42 @@ class Mlp:
 
     def __exit__(self, *a):
         self.close()
+
+
+def step_predictor_dims(n: int) -> Tuple[int, int]:
+    """(inputs, outputs) of the step predictor of an n-unknown template."""
+    return 3 * n + 1, n
+
+
+def learned_transient(L, topts, net: int = 0, warm_steps: int = 1000, lane_stride: int = 64, capacity: int = 262144,
+                      opts: Optional[TrainOpts] = None, seed: int = 7, steps_per_launch: int = 100000):
+    """Runs the transient of every lane of `L` (a Lanes whose espl_init_steps
+    has not run yet) with a learned step predictor on template `net`:
+    `warm_steps` steps with the linear predictor while the recorder samples
+    every `lane_stride`-th lane, training on the device, then the rest with
+    predictor 2. Returns (reports, mlp, info)."""
+    import time
+    n = L.nets[net].n
+    L.record_steps(net, lane_stride, 0, capacity)
+    # predictor 2 without a network is the linear predictor
+    topts.predictor = 2
+    L.init_steps(topts)
+    t0 = time.perf_counter()
+    reps = L.device_launch(warm_steps)
+    warm_reports = reps
+    t_warm = time.perf_counter() - t0
+    x_ptr, y_ptr, count = L.recorded(net)
+    d_in, d_out = step_predictor_dims(n)
+    opts = opts or train_opts(epochs=20, batch=4096, lr=3e-3, lr_final=3e-4)
+    m = Mlp(d_in, d_out, capacity=max(opts.batch, 128), seed=seed, device=0)
+    t1 = time.perf_counter()
+    losses = m.train_device(x_ptr, y_ptr, count, opts)
+    t_train = time.perf_counter() - t1
+    L.record_steps(net, 1, 0, 0)
+    L.set_step_predictor(net, m)
+    t2 = time.perf_counter()
+    while not all(r.status != 0 for r in reps):
+        reps = L.device_launch(steps_per_launch)
+    t_learned = time.perf_counter() - t2
+    return reps, m, dict(samples=count, warm_s=t_warm, train_s=t_train, learned_s=t_learned,
+                         final_loss=float(losses[-1]), warm_reports=warm_reports)

@@ -266,7 +266,8 @@ typedef struct {
     uint32_t steps;
     uint32_t rejects;
     uint32_t status;
-    uint32_t reserved;
+    uint32_t learned_retries; /* attempts from a learned start (predictor 2) that did not
+                               * converge and were retried from the linear predictor */
 } espl_step_report;
 
 espl_status espl_init_steps(espl_lanes *h, const espl_tran_opts *opts);
