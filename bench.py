@@ -4,11 +4,14 @@ Workload: 16,384 Monte-Carlo lanes of a 31-stage MOS1 ring oscillator plus
 32 seeded variants of 15-63 stages (32 lanes each, different patterns in the
 same launches), trapezoidal transient with LTE step control, 5,000 accepted
 steps per lane, and the oscillation period measured on the device. A "step"
-of the benchmark is one complete sweep of all 17,408 points. The metric is
-points/s of the mixed-precision lanes (FP32 LU and solves; FP64 device
-evaluation, residual, refinement and step control) next to the plain FP64
-lanes of the same build; a sample of lanes is checked against the FP64
-oracle (period and final state).
+of the benchmark is one complete sweep of all 17,408 points. Three arms, all
+with the Newton polish: plain FP64 lanes (linear predictor), mixed-precision
+lanes (FP32 LU and solves; FP64 device evaluation, residual, refinement and
+step control) and learned + mixed lanes (the bulk template's attempts start
+from a step-predictor MLP trained on the device on the run's own first
+steps). The metric is points/s of the learned + mixed arm; every lane of
+every arm is checked against the polished FP64 oracle (period and final
+state).
 
 Launch: `python bench.py --gpus N --steps K --warmup W`; for N > 1 one rank
 per GPU under torch.distributed.run (each rank runs its own seeded sweep:
@@ -132,37 +135,43 @@ def algorithmic_bytes(nets, lane_iterations_per_net, s_lu: int):
     return total
 
 
-def ring_check(nets, topts, xs, per_gpu, lanes_per_net=2, threads=None):
-    """Worst error of the GPU lanes against the FP64 oracle on a sample:
-    the oscillation period (.meas) and the final state."""
-    from oracle import pyoracle as po
-    threads = threads or os.cpu_count()
-    worst_p, worst_x = 0.0, 0.0
-    for k, (net, x) in enumerate(zip(nets, xs)):
-        row = net.node("s1")
-        xo, _, _, po_per = po.tran_lanes(net, topts, lane0=0, count=lanes_per_net, meas=(row, 0.9, 1e-9),
-                                         threads=threads)
-        pg = per_gpu[k][:lanes_per_net]
-        ok = np.isfinite(po_per) & np.isfinite(pg)
-        if ok.any():
-            worst_p = max(worst_p, float((np.abs(pg[ok] - po_per[ok]) / (RTOL * np.abs(po_per[ok]))).max()))
-        worst_x = max(worst_x, float((np.abs(x[:lanes_per_net] - xo) / (RTOL * np.abs(xo) + ATOL)).max()))
-    return worst_p, worst_x
+# Every arm and the oracle polish their Newton solves (espl_create_opts.polish,
+# orc_set_polish): once the reference's test passes, Newton goes on until its
+# step passes the test with the tolerances scaled by 10^-POLISH. The
+# converged points then do not depend on where Newton started (the linear or
+# the learned predictor, FP32 or FP64 factors) to far below the 1e-6 bar.
+POLISH = 6
 
 
-def run_ring_sweep(nets, topts, precision, steps_per_launch=5000):
+def run_ring_sweep(nets, topts, precision, learned=None):
+    """One full sweep through the C ABI from host buffers: create (uploads
+    every lane's parameters), operating point, every transient step, final
+    states and periods back. With `learned` (a dict: warm, stride, cap,
+    epochs, batch, lr, lr_final), the bulk template (net 0) runs `warm`
+    attempts with the linear predictor while the recorder samples every
+    stride-th lane, a step predictor is trained on the device, and the rest
+    of its transient starts each attempt from the network. Time: the CUDA-
+    event time of the Newton launches plus the training (wall, synchronized)."""
+    import copy
     from egspice_b200.lanes import Lanes
+    from egspice_b200.learned import Mlp, step_predictor_dims, train_opts
     t0 = time.perf_counter()
-    L = Lanes(nets, precision=precision, dt0=topts.dt)
+    L = Lanes(nets, precision=precision, dt0=topts.dt, polish=POLISH)
     for i, net in enumerate(nets):
         L.set_period_meas(i, net.node("s1"), 0.9, 1e-9)
-    L.init_steps(topts)
+    o = copy.copy(topts)
+    o.predictor = 2 if learned else 1
+    if learned:
+        L.record_steps(0, learned["stride"], 0, learned["cap"])
+    L.init_steps(o)
     dev_ms = L.stats().newton_ms
-    calls = 0
     classes = None
-    while True:
-        reps = L.device_launch(steps_per_launch)
-        calls += 1
+    m = None
+    info = {}
+
+    def launch(steps):
+        nonlocal dev_ms, classes
+        reps = L.device_launch(steps)
         dev_ms += L.stats().newton_ms
         cl = L.classes()
         if classes is None:
@@ -170,9 +179,30 @@ def run_ring_sweep(nets, topts, precision, steps_per_launch=5000):
         else:
             for a, b in zip(classes, cl):
                 a["ms"] += b["ms"]
+        return reps
+
+    if learned:
+        warm = launch(learned["warm"])
+        x_ptr, y_ptr, count = L.recorded(0)
+        tt = time.perf_counter()
+        d_in, d_out = step_predictor_dims(nets[0].n)
+        m = Mlp(d_in, d_out, capacity=learned["batch"], seed=7)
+        losses = m.train_device(x_ptr, y_ptr, count, train_opts(epochs=learned["epochs"], batch=learned["batch"],
+                                                                 lr=learned["lr"], lr_final=learned["lr_final"]))
+        t_train = time.perf_counter() - tt
+        L.record_steps(0, 1, 0, 0)
+        L.set_step_predictor(0, m)
+        info = dict(samples=count, train_ms=t_train * 1e3, final_loss=float(losses[-1]),
+                    warm_iters=sum(r.nr_iters for r in warm[:nets[0].lanes]),
+                    warm_attempts=sum(r.attempts for r in warm[:nets[0].lanes]))
+        dev_ms += t_train * 1e3
+    calls = 0
+    while True:
+        reps = launch(100000)
+        calls += 1
         if all(r.status != 0 for r in reps) or calls > 1000:
             break
-    launches = L.stats().launches  # Newton kernels: one per launch class per call
+    launches = L.stats().launches
     periods = [L.period_meas(i)[0] for i in range(len(nets))]
     xs = [L.get_x(i) for i in range(len(nets))]
     wall = time.perf_counter() - t0
@@ -181,7 +211,44 @@ def run_ring_sweep(nets, topts, precision, steps_per_launch=5000):
         t = L.tape(i)
         tapes.append((net, len(t["li"]), len(t["ui"])))
     L.close()
-    return dev_ms, wall, xs, reps, tapes, launches, periods, classes
+    if m is not None:
+        m.close()
+    return dict(dev_s=dev_ms / 1e3, wall_s=wall, xs=xs, reps=reps, tapes=tapes, launches=launches, periods=periods,
+                classes=classes, learned=info)
+
+
+def oracle_ring(nets, topts, lanes=None, threads=None):
+    """The polished FP64 oracle (linear predictor) on the first `lanes` lanes
+    of every template (all when None): (final x, period) per template."""
+    import copy
+    from oracle import pyoracle as po
+    threads = threads or os.cpu_count()
+    o = copy.copy(topts)
+    o.predictor = 1
+    out = []
+    with po.polish(POLISH):
+        for net in nets:
+            cnt = net.lanes if lanes is None else min(lanes, net.lanes)
+            xo, _, _, per = po.tran_lanes(net, o, lane0=0, count=cnt, meas=(net.node("s1"), 0.9, 1e-9),
+                                          threads=threads)
+            out.append((xo, per))
+    return out
+
+
+def ring_errors(res, ref):
+    """Worst period and final-state error over the 1e-6 bar against the
+    oracle, and how many lanes miss the bar (either)."""
+    wp, wx, bad, checked = 0.0, 0.0, 0, 0
+    for x, per, (xo, po_per) in zip(res["xs"], res["periods"], ref):
+        k = len(xo)
+        ep = np.abs(per[:k] - po_per) / (RTOL * np.abs(po_per))
+        ep = np.where(np.isfinite(po_per) & np.isfinite(per[:k]), ep, np.where(np.isnan(po_per) & np.isnan(per[:k]),
+                                                                               0.0, np.inf))
+        ex = (np.abs(x[:k] - xo) / (RTOL * np.abs(xo) + ATOL)).max(axis=1)
+        wp, wx = max(wp, float(ep.max())), max(wx, float(ex.max()))
+        bad += int(((ep > 1.0) | (ex > 1.0)).sum())
+        checked += k
+    return dict(period_err_over_tol=wp, final_x_err_over_tol=wx, lanes_over_bar=bad, lanes_checked=checked)
 
 
 def opamp_nominal(net):
@@ -192,15 +259,18 @@ def opamp_nominal(net):
 
 
 def run_learned_dc(points: int = 65536, train_points: int = 8192, epochs: int = 80, seed: int = 0, batch: int = 4096,
-                   lr: float = 1e-2):
+                   lr: float = 1e-2, check: bool = True):
     """Config 4: a Monte-Carlo op-amp operating-point sweep (16 varied
-    parameters). Plain: every point's Newton (FP64 LU) starts from the
-    nominal operating point. Learned + mixed: the first `train_points` points
-    are solved that way (FP32 LU), the MLP is trained on them on the GPU, and
-    the remaining points start from its predictions. Time = Newton device time
-    plus the MLP's training and inference (wall, synchronized). Garbage from
-    earlier runs is collected before each wall-timed region, so no lane
-    handle is freed inside one."""
+    parameters), every solve polished. Plain: every point's Newton (FP64 LU)
+    starts from the nominal operating point. Learned + mixed: the first
+    `train_points` points are solved that way (FP32 LU), the MLP is trained on
+    them on the GPU, and the remaining points start from its predictions; a
+    lane that does not converge from its prediction is solved again from the
+    nominal start. Time = Newton device time plus the MLP's training and
+    inference (wall, synchronized). Every lane of both arms is checked against
+    the polished FP64 oracle from the nominal start. Garbage from earlier runs
+    is collected before each wall-timed region, so no lane handle is freed
+    inside one."""
     import gc
     from egspice_b200 import abi, decks
     from egspice_b200.lanes import Lanes
@@ -209,17 +279,19 @@ def run_learned_dc(points: int = 65536, train_points: int = 8192, epochs: int = 
     x0 = opamp_nominal(net)
     opts = abi.newton_opts(init_fix=0)
 
-    def solve(sub, start, precision):
-        with Lanes([sub], precision=precision) as L:
+    def solve(sub, start, precision, max_iter=None):
+        o = opts if max_iter is None else abi.newton_opts(init_fix=0, max_iter=max_iter)
+        with Lanes([sub], precision=precision, polish=POLISH) as L:
             L.put_x(0, start, False)
-            r = L.solve_static(opts)
+            r = L.solve_static(o)
             return r, L.get_x(0), L.stats().newton_ms
 
     r_plain, x_plain, dev_plain = solve(net, x0, "fp64")
+    r_mixed, x_mixed, dev_mixed = solve(net, x0, "mixed")
     # context: the same points from the cold start through the continuation
     # ladder (what an operating point costs without a start point), wall time
     import torch
-    with Lanes([net], precision="fp64") as L:
+    with Lanes([net], precision="fp64", polish=POLISH) as L:
         gc.collect()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -237,9 +309,11 @@ def run_learned_dc(points: int = 65536, train_points: int = 8192, epochs: int = 
         t_train = time.perf_counter() - t0
         guess = m.predict(net.sweep[train_points:])
     t_mlp = time.perf_counter() - t0
-    r_tail, x_tail, dev_tail = solve(tail, guess, "mixed")
-    # plain Newton stays the fallback: a lane that does not converge from its
-    # predicted start is solved again from the nominal one
+    # from a learned start Newton gets three times the plain mean iteration
+    # count; a lane that has not converged by then restarts from the nominal
+    # point (one slow lane would otherwise hold its whole tile for 100)
+    cap = int(max(10, 3 * np.ceil(r_plain[:, 1].mean())))
+    r_tail, x_tail, dev_tail = solve(tail, guess, "mixed", max_iter=cap)
     bad = np.nonzero((r_tail[:, 0] & abi.CONVERGED) == 0)[0]
     refallback = len(bad)
     if refallback:
@@ -250,49 +324,75 @@ def run_learned_dc(points: int = 65536, train_points: int = 8192, epochs: int = 
     x_learned = np.concatenate([x_head, x_tail])
     r_learned = np.concatenate([r_head, r_tail])
     conv = lambda r: int(((r[:, 0] & abi.CONVERGED) != 0).sum())  # noqa: E731
-    cur = np.asarray(net.current_rows, dtype=bool)
-    newton_tol = opts.reltol * np.maximum(np.abs(x_plain), np.abs(x_learned)) + np.where(cur, opts.abstol, opts.vntol)
-    err_newton = float((np.abs(x_learned - x_plain) / newton_tol).max())
-    err_bar = float((np.abs(x_learned - x_plain) / (RTOL * np.abs(x_plain) + ATOL)).max())
+    bar = lambda x, xr: float((np.abs(x - xr) / (RTOL * np.abs(xr) + ATOL)).max())  # noqa: E731
     t_plain = dev_plain / 1e3
     t_learned = (dev_head + dev_tail) / 1e3 + t_mlp
-    return {
+    out = {
         "workload": f"miller_opamp_mc_dc ({points:,} points, 16 varied parameters)",
+        "polish": POLISH,
         "plain_fp64": {"points_per_s": points / t_plain, "ms": t_plain * 1e3,
                        "mean_newton_iters": float(r_plain[:, 1].mean()), "converged": conv(r_plain)},
+        "plain_mixed": {"points_per_s": points / (dev_mixed / 1e3), "ms": dev_mixed,
+                        "mean_newton_iters": float(r_mixed[:, 1].mean()), "converged": conv(r_mixed),
+                        "fp64_refactor_fallbacks": int(r_mixed[:, 2].sum())},
         "learned_mixed": {"points_per_s": points / t_learned, "ms": t_learned * 1e3,
                           "newton_ms": dev_head + dev_tail, "mlp_train_ms": t_train * 1e3,
                           "mlp_predict_ms": (t_mlp - t_train) * 1e3, "train_points": train_points,
                           "epochs": epochs, "batch": batch, "lr": lr, "final_loss": float(losses[-1]),
                           "mean_newton_iters_predicted": float(r_tail[:, 1].mean()),
                           "mean_newton_iters_all": float(r_learned[:, 1].mean()), "converged": conv(r_learned),
-                          "fallbacks_to_nominal": refallback},
+                          "fp64_refactor_fallbacks": int(r_learned[:, 2].sum()),
+                          "learned_start_max_iter": cap, "fallbacks_to_nominal": refallback},
         "plain_cold_ladder_fp64": {"points_per_s": points / t_cold, "ms": t_cold * 1e3,
                                    "mean_newton_iters": float(r_cold[:, 1].mean()),
                                    "converged": conv(r_cold)},
         "learned_over_plain": t_plain / t_learned,
         "learned_over_cold_ladder": t_cold / t_learned,
-        "max_err_over_newton_tol": err_newton,
-        "max_err_over_1e-6_bar": err_bar,
-        "note": "learned and plain runs stop at the same Newton test, so they agree to the Newton tolerance "
-                "(reltol|x| + vntol), not bit for bit",
+        "learned_vs_plain_err_over_1e-6_bar": bar(x_learned, x_plain),
     }
+    if check:
+        from oracle import pyoracle as po
+        with po.polish(POLISH):
+            xo, ro = po.op_lanes(net, opts, x_in=x0, threads=os.cpu_count())
+        out["oracle_check"] = {"lanes": points, "oracle_converged": int((ro[:, 0] == 1).sum()),
+                               "plain_fp64_err_over_1e-6_bar": bar(x_plain, xo),
+                               "learned_mixed_err_over_1e-6_bar": bar(x_learned, xo)}
+    return out
 
 
-def cpu_ring_reference(nets, topts, budget_s: float, threads: int):
-    """The oracle on a bounded sample of the ring workload: lanes of the
-    31-stage template (the workload's bulk), `threads` at a time, until the
-    budget is spent."""
+def reference_mix(nets, seed: int = 0):
+    """The points of the sweep in one fixed shuffled order (the 31-stage bulk
+    and the variants in the proportions of the sweep), for the CPU legs."""
+    pts = [(i, l) for i, net in enumerate(nets) for l in range(net.lanes)]
+    order = np.random.default_rng(seed).permutation(len(pts))
+    return [pts[k] for k in order]
+
+
+def cpu_ring_reference(nets, topts, budget_s: float, threads: int, mix=None, start: int = 0):
+    """The oracle (the reference's CPU path restated: linear predictor, no
+    polish) on a bounded sample of the sweep: points of `mix` from `start`
+    on, `threads` at a time (one point per thread), until `budget_s` is
+    spent. Returns (points/s, points, wall s, next start)."""
+    import copy
     from oracle import pyoracle as po
+    mix = mix or reference_mix(nets)
+    o = copy.copy(topts)
+    o.predictor = 1
     t0 = time.perf_counter()
     points = 0
-    lane = 0
-    while time.perf_counter() - t0 < budget_s and lane < nets[0].lanes:
-        po.tran_lanes(nets[0], topts, lane0=lane, count=threads, threads=threads)
-        lane += threads
+    k = start
+    while time.perf_counter() - t0 < budget_s:
+        sel = [mix[(k + j) % len(mix)] for j in range(threads)]
+        jobs = [threading.Thread(target=po.tran_lanes, args=(nets[i], o), kwargs=dict(lane0=l, count=1, threads=1))
+                for i, l in sel]
+        for th in jobs:
+            th.start()
+        for th in jobs:
+            th.join()
+        k += threads
         points += threads
     wall = time.perf_counter() - t0
-    return points / wall, points, wall
+    return points / wall, points, wall, k
 
 
 def main():
@@ -307,25 +407,25 @@ def main():
     ap.add_argument("--lanes", type=int, default=16384, help="lanes of the 31-stage template")
     ap.add_argument("--variants", type=int, default=32, help="seeded 15-63-stage variants, 32 lanes each")
     ap.add_argument("--max-steps", type=int, default=5000, help="accepted steps per lane")
-    ap.add_argument("--modes", default="fp64,mixed", help="precisions to run, comma-separated")
-    ap.add_argument("--no-check", action="store_true", help="skip the oracle check of sampled lanes")
+    ap.add_argument("--modes", default="fp64,mixed,learned",
+                    help="arms to run, comma-separated: fp64, mixed, learned (learned + mixed)")
+    ap.add_argument("--check", default="all", choices=["all", "sample", "none"],
+                    help="lanes checked against the polished oracle")
     ap.add_argument("--no-learned-dc", action="store_true", help="skip the learned warm-start DC measurement")
+    # the learned arm's step predictor
+    ap.add_argument("--learn-warm", type=int, default=1000, help="attempts with the linear predictor and recorder")
+    ap.add_argument("--learn-stride", type=int, default=64, help="the recorder samples every stride-th bulk lane")
+    ap.add_argument("--learn-epochs", type=int, default=10)
+    ap.add_argument("--learn-batch", type=int, default=4096)
+    ap.add_argument("--learn-lr", type=float, default=3e-3)
     args = ap.parse_args()
     modes = [m for m in args.modes.split(",") if m]
-    if not modes or any(m not in ("fp64", "mixed") for m in modes):
-        ap.error("--modes takes fp64 and/or mixed")
+    if not modes or any(m not in ("fp64", "mixed", "learned") for m in modes):
+        ap.error("--modes takes fp64, mixed and/or learned")
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    dist = None
-    if world > 1:
-        import datetime
-        import torch
-        import torch.distributed as dist_mod
-        dist = dist_mod
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
     nets, topts = ring_workload(seed=rank, lanes=args.lanes, variants=args.variants)
     topts.max_steps = args.max_steps
@@ -335,7 +435,9 @@ def main():
               "lanes": n_points,
               "stages": f"31 ({args.lanes:,} lanes) + {args.variants} variants of 15-63 (32 lanes each)",
               "steps_per_lane": args.max_steps,
-              "method": "trap, LTE step control", "predictor": "linear (SPICE xfact)",
+              "method": "trap, LTE step control",
+              "predictor": "learned (MLP on the last 3 solutions and the step) vs linear (SPICE xfact)",
+              "newton_polish": f"10^-{POLISH} of the Newton tolerances, every arm and the oracle",
               "meas": "oscillation period of stage 1 (rising 0.9 V)",
               "l2": "inputs larger than L2 (per-sweep working set > 126 MB)", "parallelism": f"lanes x{world} GPUs"}
 
@@ -343,24 +445,39 @@ def main():
         if rank != 0:
             return
         threads = os.cpu_count() or 1
-        vals = []
-        pts_total = 0
+        mix = reference_mix(nets)
+        budget = max(1.0, args.cpu_budget / max(1, args.steps))
+        k = 0
+        for _ in range(args.warmup and 1):
+            _, _, _, k = cpu_ring_reference(nets, topts, min(budget, 2.0), threads, mix, k)
+        pts_total, wall_total, walls = 0, 0.0, []
         for _ in range(max(1, args.steps)):
-            v, pts, wall = cpu_ring_reference(nets, topts, args.cpu_budget / max(1, args.steps), threads)
-            vals.append(v)
+            _, pts, wall, k = cpu_ring_reference(nets, topts, budget, threads, mix, k)
             pts_total += pts
-        v = statistics.median(vals)
+            wall_total += wall
+            walls.append(wall)
+        v = pts_total / wall_total
+        sample = (f"{pts_total} points of the sweep's template mix (31-stage bulk and 15-63-stage variants in "
+                  f"proportion, 5,000 steps each), {threads} threads, one point per thread; a step is one bounded "
+                  f"sample of ~{budget:.1f} s; scalar C restatement (-O3, x86-64-v3, no FP contraction), not the "
+                  f"reference's @Vector(W) lanes")
         line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "points/s", "n_gpus": args.gpus,
-                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * n_points / v,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * statistics.mean(walls),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic (seeded MC ring oscillators)", "config": config,
-                "cpu_baseline": {"value": v, "unit": "points/s", "cores": threads, "kind": "port",
-                                 "sample": f"{pts_total} lanes of the 31-stage template, 5,000 steps each, "
-                                           f"{threads} threads"},
+                "cpu_baseline": {"value": v, "unit": "points/s", "cores": threads, "kind": "port", "sample": sample},
                 "e2e": {"value": v, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return
 
+    dist = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist_mod
+        dist = dist_mod
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     import torch
     dev = local if world > 1 else 0
     torch.cuda.set_device(dev)
@@ -370,87 +487,126 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
+    learn = dict(warm=args.learn_warm, stride=args.learn_stride,
+                 cap=(args.lanes // args.learn_stride + 1) * args.learn_warm, epochs=args.learn_epochs,
+                 batch=args.learn_batch, lr=args.learn_lr, lr_final=args.learn_lr / 10)
     results = {}
-    for prec in modes:
+    for mode in modes:
+        prec = "fp64" if mode == "fp64" else "mixed"
+        lk = learn if mode == "learned" else None
         for _ in range(args.warmup):
-            run_ring_sweep(nets, topts, prec)
-        dev_ms, walls = [], []
+            run_ring_sweep(nets, topts, prec, lk)
+        runs = []
         barrier()
         with ClockSampler(dev) as clk:
             for _ in range(args.steps):
                 barrier()
-                d, w, xs, reps, tapes, launches, periods, classes = run_ring_sweep(nets, topts, prec)
+                runs.append(run_ring_sweep(nets, topts, prec, lk))
                 barrier()
-                dev_ms.append(d)
-                walls.append(w)
-        dmax = max(dev_ms) / 1000.0
-        wmax = max(walls)
+        r = runs[-1]
+        dmax = max(x["dev_s"] for x in runs)
+        wmax = max(x["wall_s"] for x in runs)
         if dist:
             t = torch.tensor([dmax, wmax], device="cuda", dtype=torch.float64)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             dmax, wmax = float(t[0]), float(t[1])
-        results[prec] = dict(dev_s=dmax, wall_s=wmax, xs=xs, reps=reps, tapes=tapes, clocks=clk.summary(),
-                             iters=sum(r.nr_iters for r in reps), rejects=sum(r.rejects for r in reps),
-                             launches=launches, periods=periods, classes=classes)
+        r.update(dev_s=dmax, wall_s=wmax, clocks=clk.summary())
+        results[mode] = r
 
-    best = results.get("mixed") or results["fp64"]
+    head = "learned" if "learned" in results else "mixed" if "mixed" in results else "fp64"
+    best = results[head]
     plain = results.get("fp64")
     points_all = n_points * world
     value = points_all / best["dev_s"]
     e2e = points_all / best["wall_s"]
-    err = {}
-    if rank == 0 and not args.no_check:
-        sample = [0] + list(range(1, len(nets), 8))
-        for prec in modes:
-            r = results[prec]
-            err[prec] = ring_check([nets[i] for i in sample], topts, [r["xs"][i] for i in sample],
-                                   [r["periods"][i] for i in sample])
+    errs = {}
+    check_s = None
+    if rank == 0 and args.check != "none":
+        tc = time.perf_counter()
+        ref = oracle_ring(nets, topts, lanes=None if args.check == "all" else 2)
+        check_s = time.perf_counter() - tc
+        errs = {m: ring_errors(results[m], ref) for m in results}
+    mix_run = results.get("mixed") or best
     per_net_iters = []
     off = 0
     for net in nets:
-        per_net_iters.append(sum(r.nr_iters for r in best["reps"][off:off + net.lanes]))
+        per_net_iters.append(sum(r.nr_iters for r in mix_run["reps"][off:off + net.lanes]))
         off += net.lanes
-    bytes_alg = algorithmic_bytes(best["tapes"], per_net_iters, 4)
+    s_lu = 8 if mix_run is plain else 4
+    bytes_alg = algorithmic_bytes(mix_run["tapes"], per_net_iters, s_lu)
     hbm, kind = peaks()
-    achieved = bytes_alg / best["dev_s"] / 1e9
+    achieved = bytes_alg / mix_run["dev_s"] / 1e9
     h2d = sum(sum(b.param.nbytes + b.term.nbytes for b in n.batches) + n.col_ptr.nbytes + n.row_idx.nbytes
               for n in nets)
     d2h = sum(n.lanes * n.n * 8 + n.lanes * 8 for n in nets)
+
+    def arm(m):
+        r = results[m]
+        it = sum(x.nr_iters for x in r["reps"])
+        at = sum(x.attempts for x in r["reps"])
+        d = {"points_per_s": points_all / r["dev_s"], "ms_per_sweep": r["dev_s"] * 1e3,
+             "newton_iters": it, "attempts": at, "iters_per_attempt": it / max(at, 1),
+             "rejects": sum(x.rejects for x in r["reps"]), "gpu_launches": int(r["launches"]),
+             "launch_classes": [[c["tiles"], int(c["wide"]), c["per_sm"], c["smem_bytes"], round(c["ms"], 1)]
+                                for c in (r["classes"] or [])],
+             "launch_classes_fields": "tiles, wide, resident tiles per SM, dynamic shared bytes per tile, ms",
+             "clocks": r["clocks"]}
+        d.update(errs.get(m, {}))
+        if m == "learned":
+            bulk = r["reps"][:nets[0].lanes]
+            info = r["learned"]
+            it_b = sum(x.nr_iters for x in bulk) - info["warm_iters"]
+            at_b = sum(x.attempts for x in bulk) - info["warm_attempts"]
+            d["step_predictor"] = dict(info, template="31-stage ring (bulk)", warm_attempts_per_lane=args.learn_warm,
+                                       recorder_stride=args.learn_stride, epochs=args.learn_epochs,
+                                       batch=args.learn_batch, lr=args.learn_lr,
+                                       bulk_iters_per_attempt_after_warm=it_b / max(at_b, 1),
+                                       learned_retries=sum(x.learned_retries for x in bulk))
+        return d
+
+    modes_out = {m: arm(m) for m in results}
+    if plain and "mixed" in results:
+        p = results["mixed"]
+        bulk_p = p["reps"][:nets[0].lanes]
+        modes_out["mixed"]["bulk_iters_per_attempt"] = (sum(x.nr_iters for x in bulk_p) /
+                                                        max(1, sum(x.attempts for x in bulk_p)))
     line = {
         "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": best["dev_s"] * 1000.0, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64 (eval, residual, step control); f32 LU in mixed",
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 (eval, residual, step control); f32 LU in mixed; bf16 MLP (f32 accumulation)",
         "data": "synthetic (seeded Monte-Carlo MOS1 ring oscillators)", "config": config,
-        "modes": dict(
-            {m: {"points_per_s": points_all / results[m]["dev_s"], "ms_per_sweep": results[m]["dev_s"] * 1e3,
-                 "newton_iters": results[m]["iters"], "rejects": results[m]["rejects"],
-                 "period_err_over_tol": err.get(m, (None,))[0],
-                 "final_x_err_over_tol": err.get(m, (None, None))[1],
-                 "launch_classes": [[c["tiles"], int(c["wide"]), c["per_sm"], round(c["ms"], 1)]
-                                    for c in results[m]["classes"]]} for m in modes},
-            mixed_over_fp64=(plain["dev_s"] / best["dev_s"]) if (plain and "mixed" in results) else None,
-            learned=False),
+        "headline_arm": head,
+        "modes": dict(modes_out,
+                      learned_mixed_over_fp64=(plain["dev_s"] / results["learned"]["dev_s"])
+                      if (plain and "learned" in results) else None,
+                      mixed_over_fp64=(plain["dev_s"] / results["mixed"]["dev_s"])
+                      if (plain and "mixed" in results) else None,
+                      learned_predictor=head == "learned",
+                      oracle_check={"lanes": "all" if args.check == "all" else "2 per template",
+                                    "polish": POLISH, "seconds": check_s} if errs else None),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "peak_kind": kind,
-                     "traffic": (DRAM_BYTES_PER_LANE_STEP * sum(r.steps for r in best["reps"]) / 1e9
-                                 if "mixed" in results else None),
+                     "traffic": (DRAM_BYTES_PER_LANE_STEP * sum(r.steps for r in mix_run["reps"]) / 1e9
+                                 if mix_run is not plain else None),
                      "traffic_unit": "GB per sweep (ncu capture scaled by lane-steps)",
-                     "traffic_per_lane_step": DRAM_BYTES_PER_LANE_STEP if "mixed" in results else None,
+                     "traffic_per_lane_step": DRAM_BYTES_PER_LANE_STEP if mix_run is not plain else None,
                      "algorithmic_per_sweep_gb": bytes_alg / 1e9,
-                     "kernel": ("k_tran<true>" if "mixed" in results else "k_tran<false>") +
-                               ": per-tile eval + gather + shared-memory LU + gates, fused"},
+                     "kernel": ("k_tran<true>" if mix_run is not plain else "k_tran<false>") +
+                               ": per-tile eval + gather + shared-memory LU + gates, fused (the mixed arm)"},
         "e2e": {"value": e2e, "unit": "points/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(best["launches"]),
         "clocks": best["clocks"],
     }
     if not args.no_learned_dc:
-        line["modes"]["learned_dc"] = run_learned_dc(seed=rank)
+        line["modes"]["learned_dc"] = run_learned_dc(seed=rank, check=rank == 0 and args.check != "none")
     if rank == 0 and not args.no_cpu_baseline and world == 1:
         threads = os.cpu_count() or 1
-        v, pts, wall = cpu_ring_reference(nets, topts, args.cpu_budget, threads)
+        v, pts, wall, _ = cpu_ring_reference(nets, topts, args.cpu_budget, threads)
         line["cpu_baseline"] = {"value": v, "unit": "points/s", "cores": threads, "kind": "port",
-                                "sample": f"{pts} lanes of the 31-stage template (5,000 steps each) in "
-                                          f"{wall:.1f} s on {threads} threads"}
+                                "sample": f"{pts} points of the sweep's template mix (5,000 steps each, the "
+                                          f"reference's linear predictor, no polish) in {wall:.1f} s on {threads} "
+                                          f"threads"}
     if rank == 0:
         print(json.dumps(line))
     if dist:

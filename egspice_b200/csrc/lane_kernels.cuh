@@ -46,8 +46,16 @@ struct TileShared {
     uint32_t accf[32];
     unsigned long long acc0[32], acc1[32], acc2[32];
     double limit[32];
-    double ag0[32], ag1[32], ag2[32], t[32], xfact[32], dt_next[32];
-    double lgmin[32], lsrc[32];  // the lane's ladder gmin and source scale
+    double ag0[32], ag1[32], ag2[32], t[32], xfact[32];
+    // The ladder's gmin and source scale of a lane live inside a Newton
+    // solve (an operating-point rung); a transient's next step size lives
+    // from stepEndA to the history advance, after its solve: they share.
+    union {
+        struct {
+            double lgmin[32], lsrc[32];
+        };
+        double dt_next[32];
+    };
     uint32_t method[32], on[32], accept[32], rot[32];  // on: bit 0 the lane attempts a step, bit 1 from xpred
     uint32_t pit[32];  // the lane's polish iterations so far
 };

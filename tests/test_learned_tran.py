@@ -16,7 +16,7 @@ from egspice_b200.lanes import Lanes
 pytestmark = pytest.mark.gpu
 
 RTOL, ATOL = 1e-6, 1e-9
-POLISH = 5
+POLISH = 6
 
 
 def ring_opts(steps):
@@ -74,6 +74,7 @@ def test_predictor_kernel_matches_the_network():
         L.device_launch(300 - 40)
         xp, yp, count = L.recorded(0)
         assert count > 10000
+        _, ys, _ = L.recorded_host(0)
         d_in, d_out = step_predictor_dims(n)
         with Mlp(d_in, d_out, capacity=4096, seed=3) as m:
             losses = m.train_device(xp, yp, count, train_opts(epochs=6, batch=2048, lr=3e-3, lr_final=1e-3))
@@ -86,17 +87,23 @@ def test_predictor_kernel_matches_the_network():
             y = m.predict(f)
     cur, prev, st = out["cur"][live], out["prev"][live], out["steps"][live]
     xlin = cur + (st[:, 0:1] / st[:, 1:2]) * (cur - prev)
-    want = xlin + y
     got = out["x_start"][live]
-    # row 0 is the ground: its target is constant, so its start is x_lin exactly
-    assert np.array_equal(got[:, 0], xlin[:, 0])
-    err = np.abs(got[:, 1:] - want[:, 1:]) / (1.0 + np.abs(want[:, 1:]))
+    # unknowns whose target never varied (the ground, the supply node) start
+    # at x_lin plus that constant, exactly; the network's output for them is
+    # not used (espl_mlp_predict, which de-standardizes every output, would
+    # add it)
+    const = ys.std(axis=0) == 0.0
+    assert const[0] and const.sum() < n // 2
+    assert np.array_equal(got[:, const], xlin[:, const] + ys[0, const])
+    want = xlin + y
+    err = np.abs(got[:, ~const] - want[:, ~const]) / (1.0 + np.abs(want[:, ~const]))
     assert float(err.max()) <= 1e-9, float(err.max())
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_learned_transient_meets_the_bar_in_fewer_iterations(oracle, precision):
-    """256 ring lanes, 1,500 LTE steps, polished: 400 steps with the linear
+    """256 ring lanes, 1,500 LTE steps, polished to 10^-6 of the Newton
+    tolerances: 400 steps with the linear
     predictor and the recorder, the network trained on the device, the rest
     from learned starts (an attempt at a time, a CUDA graph per attempt).
     Every lane's period and final state meet the bar against the polished
