@@ -11,7 +11,7 @@ OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libespice_lanes.so")
 SOURCES = ["espice_lanes.cu", "tape.cpp", "mlp.cu"]
 HEADERS = ["lane_engine.cuh", "lane_kernels.cuh", "lane_models.cuh", "lane_smem.cuh", "lane_tile.cuh", "lane_band.cuh", "lane_meas.cuh", "lane_ac.cuh", "lane_ac_core.cuh", "tape.h",
-           "mlp_gemm.cuh", "lane_gates.cuh", "lane_learned.cuh", "../../include/espice_learned.h",
+           "mlp_gemm.cuh", "lane_gates.cuh", "lane_learned.cuh", "lane_levels.cuh", "../../include/espice_learned.h",
            "../../include/espice_lanes.h"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",

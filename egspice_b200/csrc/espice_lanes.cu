@@ -648,6 +648,8 @@ espl_status alloc_group(espl_lanes* h, Group& g) {
     AL(corr, n1 * P);
     AL(udiag, n1 * P);
     AL(udiag32, n1 * P);
+    AL(fact_key, 4 * (size_t)P);
+    d.linear = (d.n_dio == 0 && d.n_mos == 0) ? 1u : 0u;
     // the dense peel's scratch, where the template's lanes need at most 4 GB
     // of it (past that a failed lane reports singular)
     if (g.n <= kDensePeelMax && (double)peel_doubles(g.n) * 8.0 * (double)P <= 4.0e9) {
@@ -756,7 +758,11 @@ espl_status plan_classes(espl_lanes* h) {
             bytes[i] = 0;
         }
         if (g.dev.stage_mode == kStageLu) g.dev.band_ok = 0;
-        wide[i] = g.dev.band_ok != 0;
+        // neither the shared chain nor the banded replay: past the dense
+        // peel's size, the whole CTA runs the LU by levels (lane_levels.cuh)
+        g.dev.big = (g.dev.stage_mode != kStageLu && !g.dev.band_ok && g.dev.n_fl > 0) ? 1u : 0u;
+        if (g.dev.big) bytes[i] = ((bytes[i] + 15u) & ~15u) + kBigScratch;
+        wide[i] = g.dev.band_ok != 0 || g.dev.big != 0;
         int t = 0;
         espl_status s;
         if ((s = tiles_per_sm(wide[i], bytes[i], t))) return s;
@@ -967,8 +973,28 @@ espl_status upload_tape(espl_lanes* h, Group& g) {
                 UP(band_rowof, bp.rowof);
             }
         }
+        // the level schedule of the CTA-wide LU, for templates past the
+        // dense peel's size (plan_classes decides which run it)
+        d.n_fl = d.n_bl = 0;
+        d.fl_ptr = d.fl_rows = d.bl_ptr = d.bl_rows = d.rl_ptr = d.rl_ent = d.ru_ptr = d.ru_ent = nullptr;
+        if (g.n > kDensePeelMax) {
+            LevelPlan lp;
+            level_plan(g.tape, lp);
+            d.n_fl = (uint32_t)lp.fl_ptr.size() - 1;
+            d.n_bl = (uint32_t)lp.bl_ptr.size() - 1;
+            UP(fl_ptr, lp.fl_ptr);
+            UP(fl_rows, lp.fl_rows);
+            UP(bl_ptr, lp.bl_ptr);
+            UP(bl_rows, lp.bl_rows);
+            UP(rl_ptr, lp.rl_ptr);
+            UP(rl_ent, lp.rl_ent);
+            UP(ru_ptr, lp.ru_ptr);
+            UP(ru_ent, lp.ru_ent);
+        }
 #undef UP
         size_t P = g.P;
+        // a new tape invalidates every lane's factor
+        if (d.fact_key) CK(cudaMemsetAsync(d.fact_key, 0, sizeof(double) * 4 * P, h->stream));
         if ((s = dalloc(h, own, &d.lx, (size_t)d.nnz_l * P))) return s;
         if ((s = dalloc(h, own, &d.ux, (size_t)d.nnz_u * P))) return s;
         if (h->precision == ESPL_MIXED) {

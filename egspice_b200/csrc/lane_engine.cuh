@@ -122,6 +122,16 @@ struct GroupDev {
     double *rec_x, *rec_y, *rec_tag;
     uint32_t* rec_count;
     uint32_t rec_stride, rec_from, rec_cap, rec_pad;
+    // Large templates (lane_levels.cuh, big = 1): the whole CTA refactors by
+    // columns and solves by levels (tape.h LevelPlan). linear: no nonlinear
+    // device, so a lane's A depends only on its companion coefficient and
+    // gmin; fact_key (2 per lane: the ag0 of the factored A, or -1 without a
+    // companion, and its gmin) names the A of the lane's last factor, and an
+    // unchanged key skips the refactor (the reference skips refactoring
+    // identical values, src/solver/direct.zig:313).
+    const uint32_t *fl_ptr, *fl_rows, *bl_ptr, *bl_rows, *rl_ptr, *rl_ent, *ru_ptr, *ru_ent;
+    uint32_t n_fl, n_bl, big, linear;
+    double* fact_key;
 };
 
 struct LaneState {

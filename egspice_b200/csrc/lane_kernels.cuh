@@ -10,6 +10,7 @@
 #include <type_traits>
 
 #include "lane_band.cuh"
+#include "lane_levels.cuh"
 
 namespace espl {
 
@@ -64,6 +65,97 @@ constexpr uint32_t kNoRec = 0xFFFFFFFFu;
 
 // Gate flags reduced over warps.
 constexpr uint32_t kLimited = 1, kImplausible = 2, kResidualMiss = 4;
+
+// The CTA-wide LU of a large template (lane_levels.cuh) needs, past the
+// tile's staged arrays in dynamic shared memory, the refactor's per-lane
+// reductions and the solves' partial sums (kWideWarps x 32 doubles).
+constexpr uint32_t kBigScratch = 2048 + kWideWarps * 32 * 8;
+
+template <bool MIXED>
+__device__ __forceinline__ unsigned char* big_scratch(const GroupDev& d, unsigned char* dsm) {
+    const uint32_t off = (smem_plan(d, d.stage_mode, MIXED).bytes + 15u) & ~15u;
+    return dsm + off;
+}
+
+struct BigLaneFlags {
+    uint32_t use32[32], need[32], ok[32];
+};
+
+// One Newton iteration's LU of a large template: each lane refactors when
+// its A changed (a linear template's key: the companion coefficient and
+// gmin; any other template every iteration) -- in FP32 on a mixed tile
+// until the lane falls back to FP64 -- then solves for dx (plus the FP64
+// refinement sweeps of a mixed solve). A lane whose replay fails is singular
+// (no dense peel past kDensePeelMax unknowns). All threads of the CTA call it.
+template <bool MIXED>
+__device__ void big_lu(const GroupDev& d, const TileCtx& c, bool act, LaneState* s, TileShared& sh,
+                       const NewtonParams& o, double key0, double key1, uint32_t it, unsigned char* scratch,
+                       bool& failed) {
+    const uint32_t lane = c.lane, warp = c.warp, nw = c.nw, l = c.l, P = d.P;
+    LevelShared& ls = *reinterpret_cast<LevelShared*>(scratch);
+    BigLaneFlags& bf = *reinterpret_cast<BigLaneFlags*>(scratch + sizeof(LevelShared));
+    void* red = scratch + 2048;
+    static_assert(sizeof(LevelShared) + sizeof(BigLaneFlags) <= 2048, "the scratch header fits 2 KB");
+    auto key_ok = [&](uint32_t kb) {
+        return d.linear && LM(d.fact_key, kb) == key0 && LM(d.fact_key, kb + 1) == key1;
+    };
+    if (warp == 0) {
+        const bool u32 = MIXED && act && !s->fp64;
+        bf.use32[lane] = u32 ? 1u : 0u;
+        bf.need[lane] = (act && !key_ok(u32 ? 2u : 0u)) ? 1u : 0u;
+        bf.ok[lane] = 1u;
+    }
+    __syncthreads();
+    if (MIXED) {
+        const bool go = bf.need[lane] && bf.use32[lane];
+        if (__syncthreads_or(go)) {
+            const int rc = lvl_refactor<float>(d, l, lane, warp, nw, go, d.w32, d.lx32, d.ux32, d.udiag32, ls);
+            if (warp == 0 && go) {
+                if (rc != 0) {
+                    // the FP32 factor fails: this lane refactors in FP64 from here on
+                    s->fp64 = 1;
+                    s->fallbacks++;
+                    LM(d.fact_key, 2) = NAN;
+                    bf.use32[lane] = 0;
+                    bf.need[lane] = key_ok(0) ? 0u : 1u;
+                } else {
+                    LM(d.fact_key, 2) = key0;
+                    LM(d.fact_key, 3) = key1;
+                }
+            }
+            __syncthreads();
+        }
+    }
+    {
+        const bool go = bf.need[lane] && !bf.use32[lane];
+        if (__syncthreads_or(go)) {
+            const int rc = lvl_refactor<double>(d, l, lane, warp, nw, go, d.w, d.lx, d.ux, d.udiag, ls);
+            if (warp == 0 && go) {
+                const bool ok = rc == 0 || (rc == 2 && replay_holds64(d, l));
+                bf.ok[lane] = ok ? 1u : 0u;
+                LM(d.fact_key, 0) = ok ? key0 : NAN;
+                LM(d.fact_key, 1) = key1;
+            }
+            __syncthreads();
+        }
+    }
+    if (warp == 0 && act && !bf.ok[lane]) {
+        sh.bits[lane] |= kSingular;
+        sh.active[lane] = 0;
+        s->iterations = it;
+    }
+    failed = act && !bf.ok[lane];
+    const bool solve = act && bf.ok[lane];
+    const bool u32 = bf.use32[lane] != 0;
+    if (MIXED && __syncthreads_or(solve && u32)) {
+        lvl_solve<float>(d, l, lane, warp, nw, solve && u32, d.rhs, d.dx, d.y32, d.lx32, d.ux32, d.udiag32,
+                         static_cast<float*>(red));
+        for (uint32_t r = 0; r < o.refine; r++) lvl_refine(d, l, lane, warp, nw, solve && u32, static_cast<float*>(red));
+    }
+    if (__syncthreads_or(solve && !u32))
+        lvl_solve<double>(d, l, lane, warp, nw, solve && !u32, d.rhs, d.dx, d.y, d.lx, d.ux, d.udiag,
+                          static_cast<double*>(red));
+}
 
 // One Newton solve per lane of the tile (converger.newtonLanes at W = 1 as
 // the lane kernels split it: assemble, gmin, refactor, solve, update,
@@ -187,77 +279,83 @@ __device__ __forceinline__ void newton_tile(const TileCtx& c, LaneState* s, cons
             sh.acc0[lane] = 0;
             sh.accf[lane] = 0;
         }
-        // The banded streaming replay (lane_band.cuh) of a template the
-        // shared chain cannot hold: every warp takes part; it replays the
-        // lanes in the tile's precision (FP32 lanes of a mixed tile, or FP64).
-        int band_rc = -1;
-        bool band_solved = false;
         bool failed = false;  // the lane's replay failed this iteration (it peels)
-        if (!sm && d.band_ok) {
-            const bool comp = warp == 0 && act && (!MIXED || !s->fp64);
-            band_rc = band_refactor<T>(d, warp, lane, l, comp);
-            if (!comp) band_rc = -1;
-            // lanes whose replay held solve through the streamed blocks too
-            band_solved = band_rc == 0;
-            band_solve<T>(d, warp, lane, l, band_solved);
-        }
-        if (warp == 0 && act) {
-            bool use32 = MIXED && !s->fp64;
-            bool done = band_solved;
-            if (band_solved && MIXED)
-                for (uint32_t r = 0; r < o.refine; r++) refine_mixed(d, l);
-            if (sm && (use32 || !MIXED)) {
-                int rc = d.n_rec ? refactor_rec<T>(d, st, lane, l) : refactor_smem<T>(d, st, lane, l);
-                if (MIXED && rc != 0) {
-                    s->fp64 = 1;
-                    s->fallbacks++;
-                    use32 = false;
-                } else {
-                    if (!MIXED && rc == 2) {
-                        spill_factor<T>(d, st, lane, l);
-                        rc = replay_holds64(d, l) ? 0 : 1;
-                    }
-                    if (rc == 0) {
-                        if (d.n_srec)
-                            solve_rec<T>(d, st, lane, l);
-                        else
-                            solve_smem<T>(d, st, lane, l);
-                        if (MIXED)
-                            for (uint32_t r = 0; r < o.refine; r++) refine_smem(d, st, lane, l);
+        if (d.big) {
+            // the whole CTA refactors (when the lane's A changed) and solves
+            const double key1 = o.ladder ? sh.lgmin[lane] : o.gmin;
+            big_lu<MIXED>(d, c, act, s, sh, o, cp.on ? cp.ag0 : -1.0, key1, it, big_scratch<MIXED>(d, dsm), failed);
+        } else {
+            // The banded streaming replay (lane_band.cuh) of a template the
+            // shared chain cannot hold: every warp takes part; it replays the
+            // lanes in the tile's precision (FP32 lanes of a mixed tile, or FP64).
+            int band_rc = -1;
+            bool band_solved = false;
+                if (!sm && d.band_ok) {
+                const bool comp = warp == 0 && act && (!MIXED || !s->fp64);
+                band_rc = band_refactor<T>(d, warp, lane, l, comp);
+                if (!comp) band_rc = -1;
+                // lanes whose replay held solve through the streamed blocks too
+                band_solved = band_rc == 0;
+                band_solve<T>(d, warp, lane, l, band_solved);
+            }
+            if (warp == 0 && act) {
+                bool use32 = MIXED && !s->fp64;
+                bool done = band_solved;
+                if (band_solved && MIXED)
+                    for (uint32_t r = 0; r < o.refine; r++) refine_mixed(d, l);
+                if (sm && (use32 || !MIXED)) {
+                    int rc = d.n_rec ? refactor_rec<T>(d, st, lane, l) : refactor_smem<T>(d, st, lane, l);
+                    if (MIXED && rc != 0) {
+                        s->fp64 = 1;
+                        s->fallbacks++;
+                        use32 = false;
                     } else {
+                        if (!MIXED && rc == 2) {
+                            spill_factor<T>(d, st, lane, l);
+                            rc = replay_holds64(d, l) ? 0 : 1;
+                        }
+                        if (rc == 0) {
+                            if (d.n_srec)
+                                solve_rec<T>(d, st, lane, l);
+                            else
+                                solve_smem<T>(d, st, lane, l);
+                            if (MIXED)
+                                for (uint32_t r = 0; r < o.refine; r++) refine_smem(d, st, lane, l);
+                        } else {
+                            failed = true;
+                            if (!peel_dense(d, l, *s)) {
+                                sh.bits[lane] |= kSingular;
+                                sh.active[lane] = 0;
+                                s->iterations = it;
+                            }
+                        }
+                        done = true;
+                    }
+                }
+                if (!done) {
+                    if (use32 && (band_rc >= 0 ? band_rc != 0 : refactor32(d, l))) {
+                        s->fp64 = 1;
+                        s->fallbacks++;
+                        use32 = false;
+                    }
+                    bool fail = false;
+                    if (!use32) {
+                        int rc = (!MIXED && band_rc >= 0) ? band_rc : refactor64(d, l);
+                        fail = rc == 1 || (rc == 2 && !replay_holds64(d, l));
+                    }
+                    if (fail) {
                         failed = true;
                         if (!peel_dense(d, l, *s)) {
                             sh.bits[lane] |= kSingular;
                             sh.active[lane] = 0;
                             s->iterations = it;
                         }
+                    } else if (use32) {
+                        solve32(d, l, d.rhs, d.dx);
+                        for (uint32_t r = 0; r < o.refine; r++) refine_mixed(d, l);
+                    } else {
+                        solve64(d, l, d.rhs, d.dx);
                     }
-                    done = true;
-                }
-            }
-            if (!done) {
-                if (use32 && (band_rc >= 0 ? band_rc != 0 : refactor32(d, l))) {
-                    s->fp64 = 1;
-                    s->fallbacks++;
-                    use32 = false;
-                }
-                bool fail = false;
-                if (!use32) {
-                    int rc = (!MIXED && band_rc >= 0) ? band_rc : refactor64(d, l);
-                    fail = rc == 1 || (rc == 2 && !replay_holds64(d, l));
-                }
-                if (fail) {
-                    failed = true;
-                    if (!peel_dense(d, l, *s)) {
-                        sh.bits[lane] |= kSingular;
-                        sh.active[lane] = 0;
-                        s->iterations = it;
-                    }
-                } else if (use32) {
-                    solve32(d, l, d.rhs, d.dx);
-                    for (uint32_t r = 0; r < o.refine; r++) refine_mixed(d, l);
-                } else {
-                    solve64(d, l, d.rhs, d.dx);
                 }
             }
         }

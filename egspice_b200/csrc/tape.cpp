@@ -1036,4 +1036,48 @@ bool band_plan(const Tape& t, const std::vector<uint32_t>& prog, uint32_t max_ba
     return true;
 }
 
+void level_plan(const Tape& t, LevelPlan& out) {
+    const uint32_t n = t.n;
+    // rows of L: column k's entries (row li[p] > k, slot p) go to row li[p]
+    auto by_rows = [n](const std::vector<uint32_t>& cptr, const std::vector<uint32_t>& rows,
+                       std::vector<uint32_t>& rptr, std::vector<uint32_t>& ent) {
+        rptr.assign(n + 1, 0);
+        for (uint32_t r : rows) rptr[r + 1]++;
+        for (uint32_t i = 0; i < n; i++) rptr[i + 1] += rptr[i];
+        ent.assign(2 * (size_t)rows.size(), 0);
+        std::vector<uint32_t> fill(rptr.begin(), rptr.end() - 1);
+        for (uint32_t k = 0; k < n; k++)
+            for (uint32_t p = cptr[k]; p < cptr[k + 1]; p++) {
+                const uint32_t e = fill[rows[p]]++;
+                ent[2 * (size_t)e] = k;
+                ent[2 * (size_t)e + 1] = p;
+            }
+    };
+    by_rows(t.lp, t.li, out.rl_ptr, out.rl_ent);
+    by_rows(t.up, t.ui, out.ru_ptr, out.ru_ent);
+    auto bucket = [n](const std::vector<uint32_t>& lev, std::vector<uint32_t>& ptr, std::vector<uint32_t>& rows) {
+        uint32_t top = 0;
+        for (uint32_t v : lev) top = std::max(top, v + 1);
+        ptr.assign(top + 1, 0);
+        for (uint32_t v : lev) ptr[v + 1]++;
+        for (uint32_t v = 0; v < top; v++) ptr[v + 1] += ptr[v];
+        rows.assign(n, 0);
+        std::vector<uint32_t> fill(ptr.begin(), ptr.end() - 1);
+        for (uint32_t i = 0; i < n; i++) rows[fill[lev[i]]++] = i;
+    };
+    std::vector<uint32_t> lev(n, 0);
+    for (uint32_t i = 0; i < n; i++) {
+        uint32_t v = 0;
+        for (uint32_t e = out.rl_ptr[i]; e < out.rl_ptr[i + 1]; e++) v = std::max(v, lev[out.rl_ent[2 * (size_t)e]] + 1);
+        lev[i] = v;
+    }
+    bucket(lev, out.fl_ptr, out.fl_rows);
+    for (uint32_t j = n; j-- > 0;) {
+        uint32_t v = 0;
+        for (uint32_t e = out.ru_ptr[j]; e < out.ru_ptr[j + 1]; e++) v = std::max(v, lev[out.ru_ent[2 * (size_t)e]] + 1);
+        lev[j] = v;
+    }
+    bucket(lev, out.bl_ptr, out.bl_rows);
+}
+
 }  // namespace espl

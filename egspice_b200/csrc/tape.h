@@ -104,4 +104,19 @@ constexpr uint32_t kSolveCols = 32, kSolveEntries = 64;
 bool band_plan(const Tape& t, const std::vector<uint32_t>& prog, uint32_t max_band, uint32_t max_l_ring,
                uint32_t chunk_words, uint32_t chunk_entries, BandPlan& out);
 
+// The level schedule of the row-oriented ("pull") triangular solves of a
+// large template, run by a whole CTA per 32-lane tile (lane_levels.cuh).
+// Forward: y_i -= sum_j L_ij y_j over row i of L, rows grouped by level
+// (a row's level is one more than the highest level among the rows it reads);
+// backward: y_j = (y_j - sum_k U_jk y_k) / U_jj over row j of U, levels
+// counted from the last row. Rows of a level are independent. Row entries
+// are (column, factor slot) pairs in ascending column order.
+struct LevelPlan {
+    std::vector<uint32_t> fl_ptr, fl_rows;   // forward levels: rows fl_rows[fl_ptr[v] .. fl_ptr[v + 1])
+    std::vector<uint32_t> bl_ptr, bl_rows;   // backward levels
+    std::vector<uint32_t> rl_ptr, rl_ent;    // L by rows: 2 words per entry (j, slot)
+    std::vector<uint32_t> ru_ptr, ru_ent;    // U by rows: 2 words per entry (k, slot)
+};
+void level_plan(const Tape& t, LevelPlan& out);
+
 }  // namespace espl
