@@ -801,8 +801,10 @@ espl_status plan_classes(espl_lanes* h) {
         double narrow_sms = 0.0;
         uint32_t wide_tiles = 0;
         std::vector<size_t> order;
+        // CTAs of a template: its tiles, or their parts for a large one
+        auto ctas = [&](size_t i) { return h->groups[i].P / 32 * (h->groups[i].dev.big ? (1u << kBigShift) : 1u); };
         for (size_t i = 0; i < h->groups.size(); i++) {
-            const uint32_t tiles = h->groups[i].P / 32;
+            const uint32_t tiles = ctas(i);
             if (wide[i]) {
                 wide_tiles += tiles;
             } else {
@@ -816,7 +818,7 @@ espl_status plan_classes(espl_lanes* h) {
         };
         std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return work(a) > work(b); });
         for (size_t i : order) {
-            const uint32_t tiles = h->groups[i].P / 32;
+            const uint32_t tiles = ctas(i);
             const double rest = narrow_sms - (double)tiles / per[i];
             // one SM of slack: tiles of different sizes do not pack an SM
             // as tightly as the count of SMs by occupancy assumes
@@ -844,7 +846,12 @@ espl_status plan_classes(espl_lanes* h) {
             if ((per[i] | (wide[i] ? 0x10000u : 0u)) != key) continue;
             c.smem = std::max(c.smem, bytes[i]);
             c.groups.push_back((uint32_t)i);
-            for (uint32_t t = 0; t < h->groups[i].P / 32; t++) c.tiles.push_back(h->groups[i].tile0 + t);
+            // a large template's tiles run as parts of kBigLanes lanes, one CTA
+            // each, so that more SMs share its LU
+            const uint32_t shift = h->groups[i].dev.big ? kBigShift : 0u;
+            for (uint32_t t = 0; t < h->groups[i].P / 32; t++)
+                for (uint32_t part = 0; part < (1u << shift); part++)
+                    c.tiles.push_back(tile_entry(h->groups[i].tile0 + t, part, shift));
         }
         h->classes.push_back(std::move(c));
     }

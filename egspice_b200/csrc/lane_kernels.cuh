@@ -23,14 +23,29 @@ struct TileMap {
     uint32_t n_tiles;
 };
 
+// The Newton launches of a large template run each 32-lane tile as
+// 32 >> kBigShift parts of kBigLanes lanes.
+constexpr uint32_t kBigShift = 2, kBigLanes = 32u >> kBigShift;
+
+// A tile-list entry: the tile in bits 0-23; in bits 24-27 the part of it
+// this CTA runs and in bits 28-31 the shift s of the part's width 32 >> s
+// (0: the whole tile).
+constexpr uint32_t kTileBits = 0x00FFFFFFu;
+__host__ __device__ inline uint32_t tile_entry(uint32_t tile, uint32_t part, uint32_t shift) {
+    return tile | part << 24 | shift << 28;
+}
+
 __device__ __forceinline__ TileCtx tile_ctx(const TileMap& m) {
     TileCtx c;
-    c.tile = m.tiles ? m.tiles[blockIdx.x] : blockIdx.x;
+    const uint32_t e = m.tiles ? m.tiles[blockIdx.x] : blockIdx.x;
+    c.tile = e & kTileBits;
+    const uint32_t part = (e >> 24) & 15u, shift = e >> 28;
+    c.tw = 32u >> shift;
     c.d = &m.groups[m.tile_group[c.tile]];
-    c.lane = threadIdx.x & 31;
-    c.warp = threadIdx.x >> 5;
-    c.nw = blockDim.x >> 5;
-    c.l = (c.tile - c.d->tile0) * 32 + c.lane;
+    c.lane = threadIdx.x % c.tw;
+    c.warp = threadIdx.x / c.tw;
+    c.nw = blockDim.x / c.tw;
+    c.l = (c.tile - c.d->tile0) * 32 + part * c.tw + c.lane;
     c.valid = c.l < c.d->lanes;
     return c;
 }
@@ -68,8 +83,8 @@ constexpr uint32_t kLimited = 1, kImplausible = 2, kResidualMiss = 4;
 
 // The CTA-wide LU of a large template (lane_levels.cuh) needs, past the
 // tile's staged arrays in dynamic shared memory, the refactor's per-lane
-// reductions and the solves' partial sums (kWideWarps x 32 doubles).
-constexpr uint32_t kBigScratch = 2048 + kWideWarps * 32 * 8;
+// reductions and the solves' partial sums (one double per thread).
+constexpr uint32_t kBigScratch = 2048 + kWideThreads * 8;
 
 template <bool MIXED>
 __device__ __forceinline__ unsigned char* big_scratch(const GroupDev& d, unsigned char* dsm) {
@@ -364,10 +379,12 @@ __device__ __forceinline__ void newton_tile(const TileCtx& c, LaneState* s, cons
         // the host rebuilds the template's tape from a failing lane's matrix
         // after the launch.
         if (warp == 0 && d.stale) {
-            const unsigned am = __ballot_sync(0xffffffffu, act), fm = __ballot_sync(0xffffffffu, act && failed);
+            // the tw lanes of the CTA are threads 0 .. tw-1 of its first warp
+            const unsigned mask = c.tw == 32 ? 0xffffffffu : (1u << c.tw) - 1u;
+            const unsigned am = __ballot_sync(mask, act), fm = __ballot_sync(mask, act && failed);
             if (lane == 0 && fm && 2u * (unsigned)__popc(fm) >= (unsigned)__popc(am)) {
                 atomicOr(&d.stale[0], 1u);
-                atomicMin(&d.stale[1], (c.tile - d.tile0) * 32u + (uint32_t)(__ffs(fm) - 1));
+                atomicMin(&d.stale[1], c.l - lane + (uint32_t)(__ffs(fm) - 1));
             }
         }
         __syncthreads();

@@ -135,7 +135,7 @@ __global__ void __launch_bounds__(kTileThreads) k_count_stepping(TileMap m, cons
     TileCtx c = tile_ctx(m);
     if (c.warp != 0) return;
     const bool run = c.valid && st[c.d->lane0 + c.l].status == 0;
-    const unsigned b = __ballot_sync(0xffffffffu, run);
+    const unsigned b = __ballot_sync(c.tw == 32 ? 0xffffffffu : (1u << c.tw) - 1u, run);
     if (c.lane == 0 && b) atomicAdd(count, (uint32_t)__popc(b));
 }
 

@@ -44,6 +44,34 @@ __device__ __forceinline__ uint64_t mag_bits(T v) {
     return dbits((double)fabs(v));
 }
 
+// sum over entries e = e0, e0 + stride, ... < e1 of vals[slot_e] y[col_e]
+// for one lane (entries are (col, slot) pairs), in batches of eight: a
+// batch's index, value and y loads are all issued before any is used (past
+// the row's end they are skipped and read as zero), so eight gathers are in
+// flight instead of one; a batch's products are added in a fixed order.
+template <typename T>
+__device__ __forceinline__ T row_dot(const uint2* __restrict__ e2, uint32_t e0, uint32_t e1, uint32_t stride,
+                                     const T* __restrict__ vals, const T* __restrict__ y, uint32_t P, uint32_t l) {
+    T acc = (T)0;
+    for (uint32_t e = e0; e < e1; e += 8 * stride) {
+        uint2 ce[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) ce[k] = e + k * stride < e1 ? e2[e + k * stride] : make_uint2(0u, kNone);
+        T v[8], yv[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            const bool ok = ce[k].y != kNone;
+            v[k] = ok ? LM(vals, ce[k].y) : (T)0;
+            yv[k] = ok ? LM(y, ce[k].x) : (T)0;
+        }
+        T s = v[0] * yv[0];
+#pragma unroll
+        for (int k = 1; k < 8; k++) s += v[k] * yv[k];
+        acc += s;
+    }
+    return acc;
+}
+
 // One lane's refactor status (0 holds, 1 fails, 2 only a multiplier past
 // 1 / pivot_tol) for every thread of the lane. `act`: the lane refactors;
 // lanes that do not leave their factor as it is. All threads of the CTA call
@@ -157,7 +185,7 @@ __device__ int lvl_refactor(const GroupDev& d, uint32_t l, uint32_t lane, uint32
 
 // One sweep of a level-scheduled solve over y (lane-interleaved): forward
 // (BACK false) y_i -= sum L_ij y_j by the L rows; backward y_j = (y_j -
-// sum U_jk y_k) / U_jj by the U rows. `red` holds nw x 32 partial sums.
+// sum U_jk y_k) / U_jj by the U rows. `red` holds one partial sum per thread.
 template <typename T, bool BACK>
 __device__ void lvl_sweep(const GroupDev& d, uint32_t l, uint32_t lane, uint32_t warp, uint32_t nw, bool act,
                           const uint32_t* __restrict__ lptr, const uint32_t* __restrict__ rows, uint32_t nlev,
@@ -171,11 +199,7 @@ __device__ void lvl_sweep(const GroupDev& d, uint32_t l, uint32_t lane, uint32_t
             if (act)
                 for (uint32_t k = r0 + warp; k < r0 + m; k += nw) {
                     const uint32_t i = rows[k];
-                    T acc = LM(y, i);
-                    for (uint32_t e = rptr[i]; e < rptr[i + 1]; e++) {
-                        const uint2 ce = e2[e];
-                        acc -= LM(vals, ce.y) * LM(y, ce.x);
-                    }
+                    T acc = LM(y, i) - row_dot<T>(e2, rptr[i], rptr[i + 1], 1u, vals, y, P, l);
                     if (BACK) acc = acc / LM(ud, i);
                     LM(y, i) = acc;
                 }
@@ -186,18 +210,16 @@ __device__ void lvl_sweep(const GroupDev& d, uint32_t l, uint32_t lane, uint32_t
             uint32_t i = 0;
             if (row < m) {
                 i = rows[r0 + row];
-                if (act)
-                    for (uint32_t e = rptr[i] + sub; e < rptr[i + 1]; e += gs) {
-                        const uint2 ce = e2[e];
-                        part += LM(vals, ce.y) * LM(y, ce.x);
-                    }
+                if (act) part = row_dot<T>(e2, rptr[i] + sub, rptr[i + 1], gs, vals, y, P, l);
             }
-            red[warp * 32 + lane] = part;
+            // thread (warp, lane) = threadIdx.x = warp * tw + lane
+            const uint32_t tw = blockDim.x / nw;
+            red[warp * tw + lane] = part;
             __syncthreads();
             if (row < m && sub == 0 && act) {
                 T acc = LM(y, i);
                 T sum = (T)0;
-                for (uint32_t s = 0; s < gs; s++) sum += red[(row * gs + s) * 32 + lane];
+                for (uint32_t s = 0; s < gs; s++) sum += red[(row * gs + s) * tw + lane];
                 acc -= sum;
                 if (BACK) acc = acc / LM(ud, i);
                 LM(y, i) = acc;

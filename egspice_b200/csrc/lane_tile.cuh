@@ -39,13 +39,19 @@ constexpr uint32_t kIsrcCells = 1;  // value
 constexpr uint32_t kDioCells = 4;   // g, f, c, q
 constexpr uint32_t kMosCells = 15;  // fd, fs, fb, jd[4], js[4], jb[4]
 
+// A CTA runs the lanes of one 32-lane tile, or of one part of it: the
+// Newton launches of a large template split each tile into 32 / tw parts
+// of tw lanes (tile_ctx), so that more SMs share its LU. Thread t works on
+// lane t % tw of the part; t / tw ("warp") chooses its share of the
+// per-lane work, nw such shares per lane.
 struct TileCtx {
     const GroupDev* d;
     uint32_t tile;   // tile index over all templates
     uint32_t l;      // lane in the template
-    uint32_t lane;   // 0..31
+    uint32_t lane;   // 0..tw-1
     uint32_t warp;   // 0..nw-1
-    uint32_t nw;     // warps of the CTA (kWarps, or kWideWarps for large templates)
+    uint32_t nw;     // work shares per lane (blockDim / tw)
+    uint32_t tw;     // lanes of the CTA: 32, or a part of a tile
     bool valid;      // l < lanes
 };
 

@@ -197,6 +197,28 @@ def test_power_grid_transient(oracle, precision, refine):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_power_grid_full_size(oracle, precision):
+    """Config 3 at its size: 256 lanes of the 200 x 200 mesh (40,005
+    unknowns, 2.1 million factor entries per lane), trapezoidal fixed steps
+    (20 here) through the large-template LU (the whole tile refactors by
+    columns and solves by levels, lane_levels.cuh); four lanes against the
+    oracle."""
+    net = decks.power_grid(256, side=200, loads=400)
+    topts = abi.tran_opts(t_stop=20 * 10e-12, dt=10e-12, fixed_step=1, method=1, max_iter=20)
+    with Lanes([net], precision=precision, dt0=topts.dt) as L:
+        cl = L.classes()
+        reps = L.run_tran(topts, steps_per_launch=4096)
+        x = L.get_x(0)
+    assert all(r.status == 1 and r.steps == 20 for r in reps)
+    assert all(r.nr_iters == 40 for r in reps)  # a linear circuit: two Newton iterations per step
+    assert len(cl) == 1 and cl[0]["wide"] and cl[0]["tiles"] == 256 // 8
+    pick = [0, 85, 170, 255]
+    for l in pick:
+        xo, _, _, _ = oracle.tran_lanes(net, topts, lane0=l, count=1, threads=1)
+        assert worst(x[l:l + 1], xo) <= 1.0, l
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_inverter_pair_width_step(oracle, precision):
     """The reference's GPU-vs-CPU lane deck shape (src/tests/espice.zig:
     3353-3389): two inverters with a .step over the NMOS width, cold
