@@ -151,7 +151,8 @@ def run_ring_sweep(nets, topts, precision, learned=None):
     attempts with the linear predictor while the recorder samples every
     stride-th lane, a step predictor is trained on the device, and the rest
     of its transient starts each attempt from the network. Time: the CUDA-
-    event time of the Newton launches plus the training (wall, synchronized)."""
+    event time of the Newton launches plus that of the training (both device
+    time; allocations, as in every arm, outside it)."""
     import copy
     from egspice_b200.lanes import Lanes
     from egspice_b200.learned import Mlp, step_predictor_dims, train_opts
@@ -190,12 +191,13 @@ def run_ring_sweep(nets, topts, precision, learned=None):
         losses = m.train_device(x_ptr, y_ptr, count, train_opts(epochs=learned["epochs"], batch=learned["batch"],
                                                                  lr=learned["lr"], lr_final=learned["lr_final"]))
         t_train = time.perf_counter() - tt
+        train_dev = m.train_ms()
         L.record_steps(0, 1, 0, 0)
         L.set_step_predictor(0, m)
-        info = dict(samples=count, train_ms=t_train * 1e3, final_loss=float(losses[-1]),
+        info = dict(samples=count, train_ms=train_dev, train_wall_ms=t_train * 1e3, final_loss=float(losses[-1]),
                     warm_iters=sum(r.nr_iters for r in warm[:nets[0].lanes]),
                     warm_attempts=sum(r.attempts for r in warm[:nets[0].lanes]))
-        dev_ms += t_train * 1e3
+        dev_ms += train_dev
     calls = 0
     while True:
         reps = launch(100000)
@@ -229,26 +231,39 @@ def oracle_ring(nets, topts, lanes=None, threads=None):
     with po.polish(POLISH):
         for net in nets:
             cnt = net.lanes if lanes is None else min(lanes, net.lanes)
-            xo, _, _, per = po.tran_lanes(net, o, lane0=0, count=cnt, meas=(net.node("s1"), 0.9, 1e-9),
-                                          threads=threads)
-            out.append((xo, per))
+            xo, reps, _, per = po.tran_lanes(net, o, lane0=0, count=cnt, meas=(net.node("s1"), 0.9, 1e-9),
+                                             threads=threads)
+            out.append((xo, per, [(r.steps, r.rejects) for r in reps]))
     return out
 
 
-def ring_errors(res, ref):
+def ring_errors(res, ref, nets):
     """Worst period and final-state error over the 1e-6 bar against the
-    oracle, and how many lanes miss the bar (either)."""
+    oracle, how many lanes miss the bar (either), and for each such lane its
+    accepted and rejected steps beside the oracle's: a lane whose step
+    control took one decision differently (an LTE test on the edge of 0.9 dt)
+    runs on another time grid from there."""
     wp, wx, bad, checked = 0.0, 0.0, 0, 0
-    for x, per, (xo, po_per) in zip(res["xs"], res["periods"], ref):
+    missed = []
+    off = 0
+    for t, (x, per, (xo, po_per, oreps)) in enumerate(zip(res["xs"], res["periods"], ref)):
         k = len(xo)
         ep = np.abs(per[:k] - po_per) / (RTOL * np.abs(po_per))
         ep = np.where(np.isfinite(po_per) & np.isfinite(per[:k]), ep, np.where(np.isnan(po_per) & np.isnan(per[:k]),
                                                                                0.0, np.inf))
         ex = (np.abs(x[:k] - xo) / (RTOL * np.abs(xo) + ATOL)).max(axis=1)
         wp, wx = max(wp, float(ep.max())), max(wx, float(ex.max()))
-        bad += int(((ep > 1.0) | (ex > 1.0)).sum())
+        over = np.nonzero((ep > 1.0) | (ex > 1.0))[0]
+        bad += len(over)
+        for l in over[:8]:
+            r = res["reps"][off + l]
+            missed.append({"template": f"{nets[t].name}", "lane": int(l), "period_err_over_tol": float(ep[l]),
+                           "final_x_err_over_tol": float(ex[l]), "steps_rejects": [r.steps, r.rejects],
+                           "oracle_steps_rejects": list(oreps[l])})
         checked += k
-    return dict(period_err_over_tol=wp, final_x_err_over_tol=wx, lanes_over_bar=bad, lanes_checked=checked)
+        off += nets[t].lanes
+    return dict(period_err_over_tol=wp, final_x_err_over_tol=wx, lanes_over_bar=bad, lanes_checked=checked,
+                lanes_over_bar_detail=missed)
 
 
 def opamp_nominal(net):
@@ -360,6 +375,151 @@ def run_learned_dc(points: int = 65536, train_points: int = 8192, epochs: int = 
     return out
 
 
+def lu_bytes(net, nl, nu, s_lu, iterations, assembly=True):
+    """SURVEY 8(d) algorithmic bytes of `iterations` lane-iterations of one
+    template (refactor + solve + update/gates + assembly; index words are
+    shared by the lanes and excluded)."""
+    n, nnz = net.n, net.nnz
+    per = (8 * nnz + s_lu * (nl + nu + n)) + (s_lu * (nl + nu + n) + 16 * n) + 40 * n
+    if assembly:
+        per += 8 * (nnz + n) + 16 * nnz
+    return per * iterations
+
+
+def run_config1(check: bool):
+    """Config 1: 1,024 Monte-Carlo operating points of the 16-stage chain,
+    FP64, from the cold start through the reference's operating-point path
+    (espl_solve_op: the plain rung, then the continuation ladder for a lane
+    it leaves), polished; every lane against the oracle's ladder."""
+    import torch
+    from egspice_b200 import abi, decks
+    from egspice_b200.lanes import Lanes
+    net = decks.inverter_chain(1024)
+    opts = abi.newton_opts()
+    with Lanes([net], precision="fp64", polish=POLISH) as L:
+        L.solve_op(opts)  # warm-up
+    with Lanes([net], precision="fp64", polish=POLISH) as L:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = L.solve_op(opts)
+        t = time.perf_counter() - t0
+        x = L.get_x(0)
+    out = {"workload": "inverter_chain_mc_op (1,024 points, 16 stages, cold start)", "precision": "fp64",
+           "points_per_s": 1024 / t, "ms": t * 1e3, "mean_newton_iters": float(r[:, 1].mean()),
+           "converged": int(((r[:, 0] & abi.CONVERGED) != 0).sum()), "time": "wall, synchronized"}
+    if check:
+        from oracle import pyoracle as po
+        threads = os.cpu_count() or 1
+        with po.polish(POLISH):
+            t0 = time.perf_counter()
+            xo, ro = po.op_ladder(net, opts, threads=threads)
+            tc = time.perf_counter() - t0
+        err = np.abs(x - xo) / (RTOL * np.abs(xo) + ATOL)
+        out["oracle_check"] = {"lanes": 1024, "err_over_1e-6_bar": float(err.max()),
+                               "lanes_over_bar": int((err.max(axis=1) > 1.0).sum()),
+                               "oracle_converged": int((ro[:, 0] == 1).sum())}
+        out["cpu_oracle"] = {"points_per_s": 1024 / tc, "threads": threads, "polish": POLISH}
+    return out
+
+
+def run_config2(check: bool, steps: int = 2000):
+    """Config 2: 4,096 lanes from 64 seeded RC-diode ladders of 200-5,000
+    nodes (64 lanes each, uneven patterns in the same launches), 2,000 fixed
+    10 ps trapezoidal steps, FP64; lane 0 of eight ladders (the largest
+    among them) against the oracle."""
+    import torch
+    from egspice_b200 import abi, decks
+    from egspice_b200.lanes import Lanes
+    nets = decks.rc_diode_batch(n_nets=64, lanes_per_net=64)
+    topts = abi.tran_opts(t_stop=steps * 10e-12, dt=10e-12, fixed_step=1, method=1, max_iter=50)
+    with Lanes(nets, precision="fp64", dt0=topts.dt) as L:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        L.init_steps(topts)
+        dev = L.stats().newton_ms
+        reps = L.device_launch(100000)
+        dev += L.stats().newton_ms
+        t = time.perf_counter() - t0
+        xs = [L.get_x(i) for i in range(len(nets))]
+        tapes = [(len(L.tape(i)["li"]), len(L.tape(i)["ui"])) for i in range(len(nets))]
+        cl = L.classes()
+    pts = sum(n.lanes for n in nets)
+    by = 0.0
+    off = 0
+    for net, (nl, nu) in zip(nets, tapes):
+        by += lu_bytes(net, nl, nu, 8, sum(r.nr_iters for r in reps[off:off + net.lanes]))
+        off += net.lanes
+    hbm, kind = peaks()
+    out = {"workload": f"rc_diode_ladders (64 nets of {min(n.n for n in nets)}-{max(n.n for n in nets)} unknowns, "
+                       f"64 lanes each, {steps} fixed trap steps)", "precision": "fp64",
+           "points_per_s": pts / (dev / 1e3), "ms": dev, "wall_ms": t * 1e3,
+           "all_done": all(r.status == 1 and r.steps == steps for r in reps),
+           "newton_iters": sum(r.nr_iters for r in reps),
+           "roofline": {"bound": "hbm", "achieved_gbs": by / (dev / 1e3) / 1e9, "peak": hbm, "peak_kind": kind,
+                        "frac": by / (dev / 1e3) / 1e9 / hbm},
+           "launch_classes": [[c["tiles"], int(c["wide"]), c["per_sm"], c["smem_bytes"], round(c["ms"], 1)]
+                              for c in cl]}
+    if check:
+        from oracle import pyoracle as po
+        order = sorted(range(len(nets)), key=lambda i: nets[i].n)
+        pick = order[-4:] + order[:4]
+        worst = 0.0
+        for i in pick:
+            xo, _, _, _ = po.tran_lanes(nets[i], topts, lane0=0, count=1, threads=1)
+            worst = max(worst, float((np.abs(xs[i][:1] - xo) / (RTOL * np.abs(xo) + ATOL)).max()))
+        out["oracle_check"] = {"lanes": f"lane 0 of {len(pick)} ladders ({nets[pick[0]].n} unknowns the largest)",
+                               "err_over_1e-6_bar": worst}
+    return out
+
+
+def run_config3(check: bool, steps: int = 100):
+    """Config 3: 256 lanes of the 200 x 200 power-grid mesh (40,005
+    unknowns), trapezoidal fixed 10 ps steps, mixed (FP32 LU and solves,
+    FP64 residual) and FP64, through the large-template LU (the whole CTA
+    refactors by columns and solves by levels); two lanes against the
+    oracle. `steps` of the config's 1,000 (the per-step cost is flat)."""
+    import torch
+    from egspice_b200 import abi, decks
+    from egspice_b200.lanes import Lanes
+    net = decks.power_grid(256, side=200, loads=400)
+    topts = abi.tran_opts(t_stop=steps * 10e-12, dt=10e-12, fixed_step=1, method=1, max_iter=20)
+    out = {"workload": f"power_grid_mesh (256 lanes, 200 x 200, {net.n} unknowns, {steps} of 1,000 fixed trap "
+                       f"steps)"}
+    hbm, kind = peaks()
+    for prec in ("mixed", "fp64"):
+        with Lanes([net], precision=prec, dt0=topts.dt) as L:
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            L.init_steps(topts)
+            op_ms = L.stats().newton_ms
+            reps = L.device_launch(100000)
+            dev = L.stats().newton_ms
+            t = time.perf_counter() - t0
+            x = L.get_x(0)
+            tp = L.tape(0)
+        its = sum(r.nr_iters for r in reps)
+        s_lu = 4 if prec == "mixed" else 8
+        # per Newton iteration of a linear lane the factor is reused: the
+        # solve pair's bytes (refactors: three per run, counted apart)
+        nl, nu = len(tp["li"]), len(tp["ui"])
+        solve_bytes = (s_lu * (nl + nu + net.n) + 16 * net.n) * its
+        d = {"points_per_s": 256 / ((op_ms + dev) / 1e3), "ms": op_ms + dev, "transient_ms": dev,
+             "operating_point_ms": op_ms, "wall_ms": t * 1e3, "newton_iters_per_lane": its / 256,
+             "all_done": all(r.status == 1 and r.steps == steps for r in reps), "nnz_l": nl, "nnz_u": nu,
+             "solve_roofline": {"bound": "hbm", "achieved_gbs": solve_bytes / (dev / 1e3) / 1e9, "peak": hbm,
+                                "peak_kind": kind, "frac": solve_bytes / (dev / 1e3) / 1e9 / hbm,
+                                "note": "the transient's solve bytes over its whole time (refactors included)"}}
+        if check:
+            from oracle import pyoracle as po
+            worst = 0.0
+            for l in (0, 255):
+                xo, _, _, _ = po.tran_lanes(net, topts, lane0=l, count=1, threads=1)
+                worst = max(worst, float((np.abs(x[l:l + 1] - xo) / (RTOL * np.abs(xo) + ATOL)).max()))
+            d["oracle_check"] = {"lanes": "0 and 255", "err_over_1e-6_bar": worst}
+        out[prec] = d
+    return out
+
+
 def reference_mix(nets, seed: int = 0):
     """The points of the sweep in one fixed shuffled order (the 31-stage bulk
     and the variants in the proportions of the sweep), for the CPU legs."""
@@ -412,11 +572,13 @@ def main():
     ap.add_argument("--check", default="all", choices=["all", "sample", "none"],
                     help="lanes checked against the polished oracle")
     ap.add_argument("--no-learned-dc", action="store_true", help="skip the learned warm-start DC measurement")
+    ap.add_argument("--no-configs", action="store_true", help="skip the runs of configs 1-3")
+    ap.add_argument("--config3-steps", type=int, default=100, help="steps of the config-3 mesh run (of 1,000)")
     # the learned arm's step predictor
     ap.add_argument("--learn-warm", type=int, default=1000, help="attempts with the linear predictor and recorder")
     ap.add_argument("--learn-stride", type=int, default=64, help="the recorder samples every stride-th bulk lane")
-    ap.add_argument("--learn-epochs", type=int, default=10)
-    ap.add_argument("--learn-batch", type=int, default=4096)
+    ap.add_argument("--learn-epochs", type=int, default=5)
+    ap.add_argument("--learn-batch", type=int, default=8192)
     ap.add_argument("--learn-lr", type=float, default=3e-3)
     args = ap.parse_args()
     modes = [m for m in args.modes.split(",") if m]
@@ -491,10 +653,12 @@ def main():
                  cap=(args.lanes // args.learn_stride + 1) * args.learn_warm, epochs=args.learn_epochs,
                  batch=args.learn_batch, lr=args.learn_lr, lr_final=args.learn_lr / 10)
     results = {}
-    for mode in modes:
+    for k, mode in enumerate(modes):
         prec = "fp64" if mode == "fp64" else "mixed"
         lk = learn if mode == "learned" else None
-        for _ in range(args.warmup):
+        # W warm-up sweeps before the first arm; later arms (the same
+        # kernels, the device already warm) one each
+        for _ in range(args.warmup if k == 0 else min(args.warmup, 1)):
             run_ring_sweep(nets, topts, prec, lk)
         runs = []
         barrier()
@@ -525,7 +689,7 @@ def main():
         tc = time.perf_counter()
         ref = oracle_ring(nets, topts, lanes=None if args.check == "all" else 2)
         check_s = time.perf_counter() - tc
-        errs = {m: ring_errors(results[m], ref) for m in results}
+        errs = {m: ring_errors(results[m], ref, nets) for m in results}
     mix_run = results.get("mixed") or best
     per_net_iters = []
     off = 0
@@ -600,6 +764,11 @@ def main():
     }
     if not args.no_learned_dc:
         line["modes"]["learned_dc"] = run_learned_dc(seed=rank, check=rank == 0 and args.check != "none")
+    if not args.no_configs:
+        chk = rank == 0 and args.check != "none"
+        line["modes"]["configs"] = {"config1": run_config1(chk), "config2": run_config2(chk),
+                                    "config3": run_config3(chk, steps=args.config3_steps),
+                                    "note": "one run each, outside the headline's timed sweeps"}
     if rank == 0 and not args.no_cpu_baseline and world == 1:
         threads = os.cpu_count() or 1
         v, pts, wall, _ = cpu_ring_reference(nets, topts, args.cpu_budget, threads)

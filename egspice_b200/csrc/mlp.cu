@@ -275,6 +275,7 @@ struct espl_mlp {
     double* loss = nullptr;
     int* err = nullptr;
     long long adam_t = 0;
+    double last_train_ms = 0.0;  // device time of the last training (events on the stream)
     cudaStream_t stream = nullptr;
     std::vector<void*> owned;
     std::string msg;
@@ -740,6 +741,10 @@ espl_status train_resident(espl_mlp* h, const double* xr, const double* yr, uint
         h->msg = "out of device memory for the training set";
         return ESPL_OUT_OF_MEMORY;
     }
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEventCreate(&ev0);
+    cudaEventCreate(&ev1);
+    cudaEventRecord(ev0, h->stream);
     cudaMemsetAsync(lsum, 0, sizeof(double) * o->epochs, h->stream);
     k_standardize<<<blocks((long long)n * h->Dp), 256, 0, h->stream>>>(xr, (int)n, h->D, h->Dp, h->in_mean, h->in_std,
                                                                         nullptr, xs);
@@ -786,7 +791,15 @@ espl_status train_resident(espl_mlp* h, const double* xr, const double* yr, uint
             s = refresh_bf16(h);
         }
     }
+    cudaEventRecord(ev1, h->stream);
     if (!s) s = check_err(h);
+    {
+        float ms = 0.0f;
+        if (!s && cudaEventSynchronize(ev1) == cudaSuccess && cudaEventElapsedTime(&ms, ev0, ev1) == cudaSuccess)
+            h->last_train_ms = ms;
+        cudaEventDestroy(ev0);
+        cudaEventDestroy(ev1);
+    }
     if (!s && epoch_loss) {
         std::vector<double> l(o->epochs);
         if (cudaMemcpyAsync(l.data(), lsum, sizeof(double) * o->epochs, cudaMemcpyDeviceToHost, h->stream) !=
@@ -860,6 +873,12 @@ espl_status espl_mlp_predict_layers(espl_mlp* h, const double* x, uint32_t n, do
         MCK(cudaStreamSynchronize(h->stream));
     }
     return check_err(h);
+}
+
+espl_status espl_mlp_train_ms(const espl_mlp* h, double* device_ms) {
+    if (!h || !device_ms) return ESPL_INVALID_ARGUMENT;
+    *device_ms = h->last_train_ms;
+    return ESPL_OK;
 }
 
 espl_status espl_mlp_error_message(espl_mlp* h, char* buf, size_t cap) {

@@ -49,11 +49,12 @@ def _setup(L):
     L.espl_mlp_loss_grad.argtypes = [C.c_void_p, f64p, f64p, C.c_uint32, f64p, f32p]
     L.espl_mlp_train.argtypes = [C.c_void_p, f64p, f64p, C.c_uint32, C.POINTER(TrainOpts), f64p]
     L.espl_mlp_train_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(TrainOpts), f64p]
+    L.espl_mlp_train_ms.argtypes = [C.c_void_p, f64p]
     L.espl_mlp_predict.argtypes = [C.c_void_p, f64p, C.c_uint32, f64p]
     L.espl_mlp_predict_layers.argtypes = [C.c_void_p, f64p, C.c_uint32, f64p]
     L.espl_mlp_error_message.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t]
     for f in ("create", "destroy", "param_count", "get_params", "set_params", "set_scaling", "loss_grad", "train",
-              "train_device", "predict", "predict_layers", "error_message"):
+              "train_device", "train_ms", "predict", "predict_layers", "error_message"):
         getattr(L, "espl_mlp_" + f).restype = C.c_uint32
     L._mlp_ready = True
     return L
@@ -132,6 +133,12 @@ class Mlp:
         self._check(self.L.espl_mlp_train_device(self.h, C.c_void_p(x_ptr), C.c_void_p(y_ptr), n, C.byref(opts),
                                                  losses.ctypes.data_as(f64p)), "train_device")
         return losses
+
+    def train_ms(self) -> float:
+        """Device time of the last training (espl_mlp_train_ms)."""
+        ms = C.c_double()
+        self._check(self.L.espl_mlp_train_ms(self.h, C.byref(ms)), "train_ms")
+        return ms.value
 
     def predict(self, x, fused: bool = True) -> np.ndarray:
         x = _f64(x)

@@ -73,6 +73,11 @@ espl_status espl_mlp_train(espl_mlp *m, const double *x, const double *y, uint32
 espl_status espl_mlp_train_device(espl_mlp *m, const double *x, const double *y, uint32_t n,
                                   const espl_train_opts *opts, double *epoch_loss);
 
+/* Device time of the last training call (CUDA events on the network's
+ * stream around its standardization and Adam steps; allocations and host
+ * copies excluded), milliseconds. */
+espl_status espl_mlp_train_ms(const espl_mlp *m, double *device_ms);
+
 /* Predictions for n rows (any n): one fused inference launch, each CTA
  * running the whole network on 128 rows from shared memory and tensor
  * memory. */
