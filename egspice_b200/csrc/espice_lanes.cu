@@ -1157,7 +1157,7 @@ espl_status predictor_views(espl_lanes* h, std::vector<mlp::MlpView>& views, cud
         if (!g.pred) continue;
         espl_status s = espl_mlp_view(g.pred, &views[gi], st);
         if (s) return fail(h, s, "the step predictor's network could not be read");
-        smem = std::max(smem, mlp::infer_smem_bytes(views[gi].dp, views[gi].op));
+        smem = std::max(smem, step_predict_smem(views[gi].dp, views[gi].op, g.n));
     }
     if (smem > h->predict_smem) {
         CK(cudaFuncSetAttribute(k_step_predict, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

@@ -19,6 +19,12 @@
 
 namespace espl {
 
+// The predictor's dynamic shared memory: the network's tiles and each lane's
+// linear predictor x_lin (n FP64 values per lane, read by the epilogue).
+__host__ __device__ inline size_t step_predict_smem(int dp, int op, uint32_t n) {
+    return mlp::infer_smem_bytes(dp, op) + (size_t)n * 128 * 8;
+}
+
 struct StepPredictArgs {
     const GroupDev* d;    // the template's descriptor (device copy)
     const LaneState* st;  // every lane's state; the template's from d->lane0
@@ -27,7 +33,7 @@ struct StepPredictArgs {
 };
 
 // Lanes of one template, 128 per CTA, 128 threads (one per lane). Dynamic
-// shared memory: mlp::infer_smem_bytes(dp, op). A lane that is not stepping,
+// shared memory: step_predict_smem(dp, op, n). A lane that is not stepping,
 // or has fewer than three accepted steps, gets a NaN row (k_tran starts it
 // from the linear predictor).
 __global__ void __launch_bounds__(128) k_step_predict(StepPredictArgs a) {
@@ -44,6 +50,7 @@ __global__ void __launch_bounds__(128) k_step_predict(StepPredictArgs a) {
     unsigned char* sw2 = sw1 + 128 * dp * 2;            // W2 128 x 128,
     unsigned char* sw3 = sw2 + 128 * 128 * 2;           // W3 op x 128
     unsigned char* shid = sw3 + (size_t)op * 128 * 2;   // 128 x 128 activations
+    double* sxl = reinterpret_cast<double*>(shid + 128 * 128 * 2);  // n x 128: each lane's x_lin
     const int warp = threadIdx.x >> 5;
     const uint32_t row = threadIdx.x;
     const uint32_t l = blockIdx.x * 128u + row;
@@ -80,12 +87,15 @@ __global__ void __launch_bounds__(128) k_step_predict(StepPredictArgs a) {
         *reinterpret_cast<__nv_bfloat16*>(sx + tile_off_k(row, k, (uint32_t)dp)) = __float2bfloat16(v);
     };
     const float *im = a.w.in_mean, *is = a.w.in_std;
+    // unknowns in fours: the histories' loads of four rows are in flight at once
+#pragma unroll 4
     for (uint32_t i = 0; i < n; i++) {
         float v0 = 0.0f, v1 = 0.0f, v2 = 0.0f;
         if (live) {
             const size_t e = (size_t)i * P + l;
             double f[3];
             step_features(d.cur[e], d.prev[e], d.prev2[e], r0, r1, f);
+            sxl[i * 128 + row] = f[0] + f[1];
             v0 = (float)((f[0] - (double)im[i]) / (double)is[i]);
             v1 = (float)((f[1] - (double)im[n + i]) / (double)is[n + i]);
             v2 = (float)((f[2] - (double)im[2 * n + i]) / (double)is[2 * n + i]);
@@ -112,10 +122,8 @@ __global__ void __launch_bounds__(128) k_step_predict(StepPredictArgs a) {
                            d.xpred[e] = __longlong_as_double(0x7FF8000000000000LL);
                            return;
                        }
-                       const double c = d.cur[e];
-                       double f1 = r0 * (c - d.prev[e]);
                        const double y = og[o] != 0.0f ? (double)v * (double)og[o] + (double)om[o] : (double)om[o];
-                       d.xpred[e] = (c + f1) + y;
+                       d.xpred[e] = sxl[o * 128 + row] + y;
                    });
     } else {
         // the weights never arrived: give the bulk copy a second bounded wait
