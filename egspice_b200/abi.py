@@ -32,7 +32,7 @@ class LaneNewton(C.Structure):
                 ("reserved", C.c_uint32)]
 
 
-ABI_VERSION = 2
+ABI_VERSION = 3
 
 
 class CreateOpts(C.Structure):
@@ -51,7 +51,8 @@ class TranOpts(C.Structure):
 class StepReport(C.Structure):
     _fields_ = [("t", C.c_double), ("dt", C.c_double), ("attempts", C.c_uint64), ("nr_iters", C.c_uint64),
                 ("steps", C.c_uint32), ("rejects", C.c_uint32), ("status", C.c_uint32),
-                ("learned_retries", C.c_uint32)]
+                ("learned_retries", C.c_uint32), ("t_new", C.c_double), ("attempted_dt", C.c_double),
+                ("event", C.c_uint32), ("reserved", C.c_uint32)]
 
 
 class Stats(C.Structure):

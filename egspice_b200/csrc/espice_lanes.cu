@@ -1963,6 +1963,10 @@ espl_status espl_device_launch(espl_lanes* h, uint32_t max_steps, espl_step_repo
                 r.rejects = st.rejects;
                 r.status = st.status;
                 r.learned_retries = st.pred_fallbacks;
+                r.t_new = st.t_new;
+                r.attempted_dt = st.attempted_dt;
+                r.event = st.event;
+                r.reserved = 0;
             }
             k++;
         }
@@ -2089,6 +2093,20 @@ espl_status espl_request_stop(espl_lanes* h, uint32_t net, const uint8_t* stop) 
     CK(cudaStreamSynchronize(h->stream));
     for (uint32_t l = 0; l < g.lanes; l++)
         if (stop[l] && host[l].status == 0) host[l].status = 4;
+    CK(cudaMemcpyAsync(dev, host, sizeof(LaneState) * g.lanes, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return ESPL_OK;
+}
+
+espl_status espl_resume_lanes(espl_lanes* h, uint32_t net, const uint8_t* resume) {
+    if (!h || net >= h->groups.size() || !resume) return ESPL_INVALID_ARGUMENT;
+    Group& g = h->groups[net];
+    LaneState* dev = h->d_state + g.lane0;
+    LaneState* host = h->h_state.data() + g.lane0;
+    CK(cudaMemcpyAsync(host, dev, sizeof(LaneState) * g.lanes, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    for (uint32_t l = 0; l < g.lanes; l++)
+        if (resume[l] && host[l].status == kStepParked) host[l].status = kStepRun;
     CK(cudaMemcpyAsync(dev, host, sizeof(LaneState) * g.lanes, cudaMemcpyHostToDevice, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     return ESPL_OK;

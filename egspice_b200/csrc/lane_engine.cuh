@@ -141,9 +141,15 @@ struct LaneState {
     unsigned long long attempts, nr_iters;
     uint32_t bits, pred_fallbacks, iterations, fallbacks;  // pred_fallbacks: learned starts retried linearly
     uint32_t order, steps, status, rejects;
-    uint32_t bp_clamped, m_cross, m_have, peel_slot;
+    uint32_t bp_clamped, m_cross, m_have, event;  // event: kernels/lane.zig step_idle/attempt/accept/reject
     uint32_t s_rot, fp64, peels, pred_lin;  // pred_lin: the next attempt starts from the linear predictor
+    double t_new, attempted_dt;  // the last attempt's candidate time and step
 };
+
+// LaneStep.event (src/solver/kernels/lane.zig:461-465).
+constexpr uint32_t kEventIdle = 0, kEventAttempt = 1, kEventAccept = 2, kEventReject = 3;
+// LaneStep.status (kernels/lane.zig:455-460).
+constexpr uint32_t kStepRun = 0, kStepDone = 1, kStepUnderflow = 2, kStepParked = 3, kStepStopped = 4;
 
 // The three history features of unknown i (f[0] = cur, f[1] the linear
 // predictor's increment, f[2] the increment a step earlier). The recorder

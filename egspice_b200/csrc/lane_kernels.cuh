@@ -722,6 +722,9 @@ __global__ void __launch_bounds__(kTileThreads) k_tran_init(TileMap m, TranParam
     s.peels = 0;
     s.pred_lin = 0;
     s.pred_fallbacks = 0;
+    s.event = kEventIdle;
+    s.t_new = 0.0;
+    s.attempted_dt = 0.0;
     // the .meas passes start, reading the operating point at t = 0
     for (uint32_t p = 0; p < d.n_mpass; p++) {
         double* ms = d.mstate + (size_t)p * kMeasWords * P + l;
@@ -752,12 +755,16 @@ __global__ void __launch_bounds__(WIDE ? kWideThreads : kTileThreads, WIDE ? 1 :
         // stepBegin (kernels/lane.zig:508-545).
         if (warp == 0) {
             uint32_t on = 0, lrn = 0;
+            if (s) s->event = kEventIdle;
             if (s && s->status == 0) {
                 if (!(s->t < o.t_stop && !at_stop(s->t, o.t_stop) && s->steps < o.max_steps)) {
                     s->status = 1;
                 } else {
                     on = 1;
                     double dt = s->dt;
+                    s->attempted_dt = dt;
+                    s->t_new = s->t + dt;
+                    s->event = kEventAttempt;
                     uint32_t method = s->order == 1 ? 0 : o.method;
                     sh.method[lane] = method;
                     // integrator.zig coeffs (src/analysis/tran/integrator.zig:39-52)
@@ -853,7 +860,14 @@ __global__ void __launch_bounds__(WIDE ? kWideThreads : kTileThreads, WIDE ? 1 :
                 if (!lrn) s->pred_lin = 0;
                 s->attempts++;
                 if (!(sh.bits[lane] & kSingular)) s->nr_iters += s->iterations < o.max_iter ? s->iterations : o.max_iter;
-                if (!conv && lrn) {
+                if (sh.bits[lane] & kParked) {
+                    // a gate that hands the lane back to the host (the
+                    // reference's reject_at / $bound_step, kernels/lane.zig
+                    // :565-573): the lane stops, its state kept, until the
+                    // host resumes it
+                    s->status = kStepParked;
+                    s->event = kEventIdle;
+                } else if (!conv && lrn) {
                     // plain Newton is the fallback: the same step again from
                     // the linear predictor, not a rejected step
                     s->pred_lin = 1;
@@ -861,6 +875,7 @@ __global__ void __launch_bounds__(WIDE ? kWideThreads : kTileThreads, WIDE ? 1 :
                 } else if (!conv) {
                     s->rejects++;
                     s->order = 1;
+                    s->event = kEventReject;
                     if (o.fixed_step) {
                         s->status = 2;
                     } else {
@@ -883,6 +898,7 @@ __global__ void __launch_bounds__(WIDE ? kWideThreads : kTileThreads, WIDE ? 1 :
                         if (!(del >= 0.9 * dt)) {
                             reject = true;
                             s->rejects++;
+                            s->event = kEventReject;
                             double ndt;
                             if (isnan(del)) { s->order = 1; ndt = dt / 8.0; }
                             else ndt = del;
@@ -903,6 +919,7 @@ __global__ void __launch_bounds__(WIDE ? kWideThreads : kTileThreads, WIDE ? 1 :
                     }
                     if (!reject) {
                         acc = 1;
+                        s->event = kEventAccept;
                         sh.dt_next[lane] = dt_next;
                         // the step recorder's sample of this accepted step
                         if (d.rec_count && l % d.rec_stride == 0 && s->steps >= d.rec_from && s->steps >= 3) {

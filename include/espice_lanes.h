@@ -25,7 +25,7 @@
 extern "C" {
 #endif
 
-#define ESPL_ABI_VERSION 2u
+#define ESPL_ABI_VERSION 3u
 
 /* A device terminal on the datum node. Its residual row and Jacobian
  * entries are dropped, as the reference's GROUND gather does
@@ -256,11 +256,15 @@ typedef struct {
     uint32_t reserved;
 } espl_tran_opts;
 
-/* `StepReport` (src/solver/kernels/lane.zig:441) per lane. status: 0
- * stepping, 1 done, 2 dt underflow, 3 parked, 4 stopped. */
+/* `StepReport` (src/solver/kernels/lane.zig:441-451) per lane, with this
+ * build's counters. status: 0 stepping, 1 done, 2 dt underflow, 3 parked
+ * (a gate handed the lane back to the host: it keeps its state and steps no
+ * further until espl_resume_lanes), 4 stopped. event: the lane's last
+ * attempt in the launch, 0 idle (none), 1 attempt (under way), 2 accepted,
+ * 3 rejected. */
 typedef struct {
-    double t;
-    double dt;
+    double t;              /* the lane's time: the last accepted step's */
+    double dt;             /* the next step */
     uint64_t attempts;
     uint64_t nr_iters;
     uint32_t steps;
@@ -268,6 +272,10 @@ typedef struct {
     uint32_t status;
     uint32_t learned_retries; /* attempts from a learned start (predictor 2) that did not
                                * converge and were retried from the linear predictor */
+    double t_new;          /* the last attempt's candidate time t + attempted_dt */
+    double attempted_dt;   /* the last attempt's step */
+    uint32_t event;
+    uint32_t reserved;
 } espl_step_report;
 
 espl_status espl_init_steps(espl_lanes *h, const espl_tran_opts *opts);
@@ -349,6 +357,11 @@ espl_status espl_meas_done(espl_lanes *h, uint32_t net, uint8_t *done);
  * GpuLanes.requestStop, src/analysis/gpu/lanes.zig:2059-2064). With
  * espl_meas_done this ends a lane's transient once its measures resolve. */
 espl_status espl_request_stop(espl_lanes *h, uint32_t net, const uint8_t *stop);
+/* Resumes every parked lane l of template `net` with resume[l] != 0 (status
+ * 3 -> 0): its next launch attempts again the step it was handed back at
+ * (the reference's host takes the parked step itself and re-arms the lane;
+ * here the lane resumes on the device). Other lanes are left as they are. */
+espl_status espl_resume_lanes(espl_lanes *h, uint32_t net, const uint8_t *resume);
 
 /* Timing of the last solve/launch, milliseconds of device time per kernel
  * family (CUDA events on the launching stream), for roofline reporting. */

@@ -115,6 +115,40 @@ def test_rc_points_lte_control(oracle, method):
     assert worst(x, xo) <= 1.0
 
 
+def test_step_report_events():
+    """The step report's per-attempt fields (StepReport, kernels/lane.zig
+    :441-451): one attempt per launch, so each report shows that attempt --
+    event 2 (accepted: t is t_new) or 3 (rejected: t is unchanged, the next
+    dt smaller than the attempted one) -- and a finished lane reads idle
+    (0), its last attempt's t_new its final time."""
+    r = np.array([1e3, 2e3, 5e3, 1e4])
+    c = np.array([1e-12, 0.5e-12, 2e-13, 2e-13])
+    net = decks.rc_points(4, r, c, tr=0.2e-9)
+    opts = abi.tran_opts(t_stop=2e-9, dt=1e-12, dt_max=20e-12, method=1, max_iter=20, reltol=1e-4)
+    seen = set()
+    with Lanes([net]) as L:
+        L.init_steps(opts)
+        prev = [0.0] * 4
+        for _ in range(4000):
+            reps = L.device_launch(1)
+            for k, rp in enumerate(reps):
+                if rp.status != 0:
+                    continue
+                seen.add(rp.event)
+                assert rp.event in (2, 3)
+                assert rp.attempted_dt > 0 and rp.t_new == prev[k] + rp.attempted_dt
+                if rp.event == 2:
+                    assert rp.t == rp.t_new
+                else:
+                    assert rp.t == prev[k] and rp.dt < rp.attempted_dt
+                prev[k] = rp.t
+            if all(rp.status != 0 for rp in reps):
+                break
+    assert seen == {2, 3}
+    for rp in reps:
+        assert rp.status == 1 and rp.event == 0 and rp.t_new == rp.t
+
+
 @pytest.mark.parametrize("method", [1, 2])
 def test_ring_oscillator_period(oracle, method):
     net = decks.ring_oscillator(16, stages=15)
