@@ -114,6 +114,18 @@ def ring_workload(seed: int, lanes: int = 16384, variants: int = 32, lanes_per_v
     return nets, topts
 
 
+# FP64 operations per lane-iteration of k_tran<true> (the mixed arm): the
+# FP64 thread instructions of one launch (2 DFMA + DADD + DMUL, ncu
+# smsp__sass_thread_inst_executed_op_{dfma,dadd,dmul}_pred_on.sum: 148.5 G
+# over 6.34 M lane-iterations of 4,352 ring lanes x 300 polished steps)
+# divided by its lane-iterations: device evaluation twice per iteration (the
+# instance phase and the limiter pass), the gather, the update, gates and
+# LTE. The pipe's activity in the same capture: 4.7 % of peak.
+FP64_FLOPS_PER_LANE_ITERATION = 23420.0
+FP64_PIPE_ACTIVE_PCT = 4.74
+# B200 FP64 peak, nominal: 148 SMs x 64 FP64 FMA per clock x 2 x 1.965 GHz.
+FP64_PEAK_TFLOPS = 148 * 64 * 2 * 1.965e9 / 1e12
+
 # DRAM bytes per lane-step of the bulk k_tran class (31-stage ring lanes, mixed):
 # dram__bytes_read.sum + dram__bytes_write.sum from one ncu capture of the
 # benchmark's full lane count cut to 200 steps (425.9 GB for 16,704 lanes x 200
@@ -575,8 +587,8 @@ def main():
     ap.add_argument("--no-configs", action="store_true", help="skip the runs of configs 1-3")
     ap.add_argument("--config3-steps", type=int, default=100, help="steps of the config-3 mesh run (of 1,000)")
     # the learned arm's step predictor
-    ap.add_argument("--learn-warm", type=int, default=1000, help="attempts with the linear predictor and recorder")
-    ap.add_argument("--learn-stride", type=int, default=64, help="the recorder samples every stride-th bulk lane")
+    ap.add_argument("--learn-warm", type=int, default=500, help="attempts with the linear predictor and recorder")
+    ap.add_argument("--learn-stride", type=int, default=32, help="the recorder samples every stride-th bulk lane")
     ap.add_argument("--learn-epochs", type=int, default=5)
     ap.add_argument("--learn-batch", type=int, default=8192)
     ap.add_argument("--learn-lr", type=float, default=3e-3)
@@ -697,6 +709,7 @@ def main():
         per_net_iters.append(sum(r.nr_iters for r in mix_run["reps"][off:off + net.lanes]))
         off += net.lanes
     s_lu = 8 if mix_run is plain else 4
+    mix_run_iters = sum(r.nr_iters for r in mix_run["reps"])
     bytes_alg = algorithmic_bytes(mix_run["tapes"], per_net_iters, s_lu)
     hbm, kind = peaks()
     achieved = bytes_alg / mix_run["dev_s"] / 1e9
@@ -758,6 +771,16 @@ def main():
                      "algorithmic_per_sweep_gb": bytes_alg / 1e9,
                      "kernel": ("k_tran<true>" if mix_run is not plain else "k_tran<false>") +
                                ": per-tile eval + gather + shared-memory LU + gates, fused (the mixed arm)"},
+        "roofline_fp64": ({"bound": "fp64", "kernel": "k_tran<true> (the mixed arm): device evaluation and the rest "
+                                                    "of the step in FP64",
+                           "flops_per_lane_iteration": FP64_FLOPS_PER_LANE_ITERATION,
+                           "achieved": FP64_FLOPS_PER_LANE_ITERATION * mix_run_iters / mix_run["dev_s"] / 1e12,
+                           "peak": FP64_PEAK_TFLOPS, "unit": "TFLOP/s",
+                           "frac": FP64_FLOPS_PER_LANE_ITERATION * mix_run_iters / mix_run["dev_s"] / 1e12 /
+                                   FP64_PEAK_TFLOPS,
+                           "peak_kind": "nominal (148 SMs x 64 FP64 FMA per clock x 2 x 1.965 GHz)",
+                           "pipe_active_pct_ncu": FP64_PIPE_ACTIVE_PCT}
+                          if mix_run is not plain else None),
         "e2e": {"value": e2e, "unit": "points/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(best["launches"]),
         "clocks": best["clocks"],
