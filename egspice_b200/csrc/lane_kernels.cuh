@@ -25,7 +25,7 @@ struct TileMap {
 
 // The Newton launches of a large template run each 32-lane tile as
 // 32 >> kBigShift parts of kBigLanes lanes.
-constexpr uint32_t kBigShift = 2, kBigLanes = 32u >> kBigShift;
+constexpr uint32_t kBigShift = 4, kBigLanes = 32u >> kBigShift;
 
 // A tile-list entry: the tile in bits 0-23; in bits 24-27 the part of it
 // this CTA runs and in bits 28-31 the shift s of the part's width 32 >> s

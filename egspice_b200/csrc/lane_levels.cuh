@@ -1,12 +1,13 @@
-// The LU of large templates, run by the whole CTA of a 32-lane tile.
+// The LU of large templates, run by the whole CTA.
 //
 // A template whose factor fits neither the tile's shared memory nor the
 // banded streaming replay (a power-grid mesh of 40,000 unknowns: 2 million
 // factor entries per lane) would leave one thread per lane walking its whole
-// factor while the other warps wait. Here every thread of the CTA works on
-// the LU of the tile's 32 lanes: thread (warp, lane) handles lane `lane` of
-// a share of the work chosen by `warp`, so every factor entry is still one
-// coalesced load of 32 lanes.
+// factor while the other warps wait. Here the template's tiles run as parts
+// of a few lanes, one CTA each, and every thread of the CTA works on the
+// LU of its part: thread (share, lane) handles lane `lane` of the share of
+// the work chosen by `share` (TileCtx.warp), a factor entry being one
+// contiguous load of the part's lanes.
 //
 // Refactor (lvl_refactor): the frozen tape's columns in order (the replay of
 // src/solver/kernels/lane.zig:56-125): a column's scatter, its U entries in

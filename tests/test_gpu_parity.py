@@ -245,7 +245,7 @@ def test_power_grid_full_size(oracle, precision):
         x = L.get_x(0)
     assert all(r.status == 1 and r.steps == 20 for r in reps)
     assert all(r.nr_iters == 40 for r in reps)  # a linear circuit: two Newton iterations per step
-    assert len(cl) == 1 and cl[0]["wide"] and cl[0]["tiles"] == 256 // 8
+    assert len(cl) == 1 and cl[0]["wide"] and cl[0]["tiles"] == 256 // 2  # 2-lane parts, one CTA each
     pick = [0, 85, 170, 255]
     for l in pick:
         xo, _, _, _ = oracle.tran_lanes(net, topts, lane0=l, count=1, threads=1)
