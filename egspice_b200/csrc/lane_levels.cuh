@@ -205,23 +205,35 @@ __device__ void lvl_sweep(const GroupDev& d, uint32_t l, uint32_t lane, uint32_t
                     LM(y, i) = acc;
                 }
         } else {
-            // m < nw rows: gs warps per row, each summing a strided share
-            const uint32_t gs = nw / m, row = warp / gs, sub = warp % gs;
+            // m < nw rows: gs shares per row (a power of two, so a row's
+            // shares are an aligned run of threads), each summing a strided
+            // part of the row; the parts are added by a butterfly of warp
+            // shuffles inside each hardware warp, then (a row over several
+            // warps) the warps' sums in order through shared memory -- a
+            // fixed order either way
+            uint32_t gs = 1;
+            while (gs * 2 * m <= nw) gs *= 2;
+            const uint32_t row = warp / gs, sub = warp % gs;
+            const uint32_t tw = blockDim.x / nw, spw = 32u / tw;  // shares per hardware warp
             T part = (T)0;
             uint32_t i = 0;
             if (row < m) {
                 i = rows[r0 + row];
                 if (act) part = row_dot<T>(e2, rptr[i] + sub, rptr[i + 1], gs, vals, y, P, l);
             }
-            // thread (warp, lane) = threadIdx.x = warp * tw + lane
-            const uint32_t tw = blockDim.x / nw;
-            red[warp * tw + lane] = part;
-            __syncthreads();
+            for (uint32_t o = 1; o < gs && o < spw; o *= 2) part += __shfl_xor_sync(0xffffffffu, part, o * tw);
+            if (gs > spw) {
+                if ((threadIdx.x & 31u) < tw) red[(threadIdx.x >> 5) * tw + lane] = part;
+                __syncthreads();
+                if (row < m && sub == 0 && act) {
+                    const uint32_t w0 = (row * gs) / spw, nwarps = gs / spw;
+                    T sum = (T)0;
+                    for (uint32_t k = 0; k < nwarps; k++) sum += red[(w0 + k) * tw + lane];
+                    part = sum;
+                }
+            }
             if (row < m && sub == 0 && act) {
-                T acc = LM(y, i);
-                T sum = (T)0;
-                for (uint32_t s = 0; s < gs; s++) sum += red[(row * gs + s) * tw + lane];
-                acc -= sum;
+                T acc = LM(y, i) - part;
                 if (BACK) acc = acc / LM(ud, i);
                 LM(y, i) = acc;
             }
