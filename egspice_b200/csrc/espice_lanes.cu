@@ -107,6 +107,13 @@ struct Group {
     uint32_t tile0 = 0;
     uint32_t n_rec = 0;   // words of the uploaded replay records (0: none)
     uint32_t n_srec = 0;  // words of the uploaded solve records (0: none)
+    // The streaming plan of a large template's solves (index arrays in
+    // lu_owned; sd_ok when one exists) and, once a launch class gives it
+    // the ring's shared memory, the factor values in streaming order and
+    // the device copy of the descriptor (d_sd).
+    StreamDev sd{};
+    StreamDev* d_sd = nullptr;
+    bool sd_ok = false;
     espl_mlp* pred = nullptr;            // the learned step predictor (borrowed), or none
     std::vector<void*> learn_owned;      // prev2, xpred
     std::vector<void*> rec_owned;        // the step recorder's buffers
@@ -699,6 +706,30 @@ void free_classes(espl_lanes* h) {
 // Shared-memory plan of every template and the launch classes: templates
 // whose LU chain fits the per-block opt-in limit run it in shared memory;
 // templates are grouped by how many of their tiles fit an SM together.
+// The value arrays of g's streaming plan (FP64, and FP32 for a mixed
+// handle) and the descriptor's device copy, allocated the first time a
+// launch class streams g's solves. The lanes' factors are then stale in
+// streaming order: every lane refactors at its next solve.
+espl_status ensure_stream(espl_lanes* h, Group& g, bool mixed) {
+    if (g.d_sd) return ESPL_OK;
+    espl_status s;
+    auto& own = g.lu_owned;
+    const size_t P = g.P;
+    if ((s = dalloc(h, own, &g.sd.vf, P * g.sd.fw.entries))) return s;
+    if ((s = dalloc(h, own, &g.sd.vb, P * g.sd.bw.entries))) return s;
+    if (mixed) {
+        if ((s = dalloc(h, own, &g.sd.vf32, P * g.sd.fw.entries))) return s;
+        if ((s = dalloc(h, own, &g.sd.vb32, P * g.sd.bw.entries))) return s;
+    }
+    StreamDev* p = nullptr;
+    if ((s = dalloc(h, own, &p, 1))) return s;
+    CK(cudaMemcpyAsync(p, &g.sd, sizeof(StreamDev), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    g.d_sd = p;
+    if (g.dev.fact_key) CK(cudaMemsetAsync(g.dev.fact_key, 0, sizeof(double) * 4 * P, h->stream));
+    return ESPL_OK;
+}
+
 template <bool MIXED>
 espl_status plan_classes(espl_lanes* h) {
     int dev = h->device, optin = 0;
@@ -762,9 +793,17 @@ espl_status plan_classes(espl_lanes* h) {
         // peel's size, the whole CTA runs the LU by levels (lane_levels.cuh)
         g.dev.big = (g.dev.stage_mode != kStageLu && !g.dev.band_ok && g.dev.n_fl > 0) ? 1u : 0u;
         if (g.dev.big) bytes[i] = ((bytes[i] + 15u) & ~15u) + kBigScratch;
+        // the solves stream the factor through a ring of shared memory where
+        // it fits beside the rest
+        g.dev.stream = nullptr;
+        espl_status s;
+        if (g.dev.big && g.sd_ok && bytes[i] + kBigRingBytes <= (uint32_t)max_dyn) {
+            if ((s = ensure_stream(h, g, MIXED))) return s;
+            g.dev.stream = g.d_sd;
+            bytes[i] += kBigRingBytes;
+        }
         wide[i] = g.dev.band_ok != 0 || g.dev.big != 0;
         int t = 0;
-        espl_status s;
         if ((s = tiles_per_sm(wide[i], bytes[i], t))) return s;
         if (g.dev.stage_mode == kStageLu && (g.dev.n_rec || g.dev.n_srec)) {
             // Staged records cost their own words of shared memory; where
@@ -932,7 +971,11 @@ espl_status upload_tape(espl_lanes* h, Group& g) {
     {
         for (void* p : g.lu_owned) cudaFree(p);
         g.lu_owned.clear();
+        g.sd = StreamDev{};
+        g.d_sd = nullptr;
+        g.sd_ok = false;
         GroupDev& d = g.dev;
+        d.stream = nullptr;
         d.nnz_l = (uint32_t)g.tape.li.size();
         d.nnz_u = (uint32_t)g.tape.ui.size();
         d.n_void = (uint32_t)g.tape.void_slots.size();
@@ -997,6 +1040,28 @@ espl_status upload_tape(espl_lanes* h, Group& g) {
             UP(rl_ent, lp.rl_ent);
             UP(ru_ptr, lp.ru_ptr);
             UP(ru_ent, lp.ru_ent);
+            // the same sweeps in streaming order, chunks of a ring slot
+            StreamPlan fw, bw;
+            if (stream_plan(lp.fl_ptr, lp.fl_rows, lp.rl_ptr, lp.rl_ent, kRingChunk, kRingRows, kRingSlots, true, fw) &&
+                stream_plan(lp.bl_ptr, lp.bl_rows, lp.ru_ptr, lp.ru_ent, kRingChunk, kRingRows, kRingSlots, false,
+                            bw) &&
+                fw.max_meta <= kRingMetaWords && bw.max_meta <= kRingMetaWords) {
+                auto put = [&](const StreamPlan& sp, StreamSweep& sw) -> espl_status {
+                    espl_status e;
+                    if ((e = dupload(h, own, &sw.col, sp.col))) return e;
+                    if ((e = dupload(h, own, &sw.slot, sp.slot))) return e;
+                    if ((e = dupload(h, own, &sw.ch, sp.ch))) return e;
+                    if ((e = dupload(h, own, &sw.meta, sp.meta))) return e;
+                    if ((e = dupload(h, own, &sw.mo, sp.mo))) return e;
+                    sw.entries = sp.entries;
+                    sw.n_chunks = sp.n_chunks;
+                    sw.max_meta = sp.max_meta;
+                    return ESPL_OK;
+                };
+                if ((s = put(fw, g.sd.fw))) return s;
+                if ((s = put(bw, g.sd.bw))) return s;
+                g.sd_ok = true;
+            }
         }
 #undef UP
         size_t P = g.P;

@@ -132,6 +132,21 @@ struct GroupDev {
     const uint32_t *fl_ptr, *fl_rows, *bl_ptr, *bl_rows, *rl_ptr, *rl_ent, *ru_ptr, *ru_ent;
     uint32_t n_fl, n_bl, big, linear;
     double* fact_key;
+    const struct StreamDev* stream;  // the sweeps in streaming order (lane_levels.cuh), or null
+};
+
+// One sweep of a large template's solve in streaming order (tape.h
+// StreamPlan), and the factor's values copied into that order: for the
+// lanes of part p (tw lanes), entry e of the sweep at (p * entries + e) * tw
+// + lane, so that a chunk of entries is one contiguous block per part.
+struct StreamSweep {
+    const uint32_t *col, *slot, *ch, *meta, *mo;
+    uint32_t entries, n_chunks, max_meta, pad;
+};
+struct StreamDev {
+    StreamSweep fw, bw;
+    double *vf, *vb;    // FP64 L and U values in streaming order
+    float *vf32, *vb32; // FP32 (mixed)
 };
 
 struct LaneState {

@@ -83,8 +83,16 @@ constexpr uint32_t kLimited = 1, kImplausible = 2, kResidualMiss = 4;
 
 // The CTA-wide LU of a large template (lane_levels.cuh) needs, past the
 // tile's staged arrays in dynamic shared memory, the refactor's per-lane
-// reductions and the solves' partial sums (one double per thread).
+// reductions, the lanes' flags and the ring's barriers (a 2 KB header), the
+// solves' partial sums (one double per thread) and, with a streaming plan
+// (GroupDev stream), the ring's slots (kBigRingBytes).
 constexpr uint32_t kBigScratch = 2048 + kWideThreads * 8;
+constexpr uint32_t kBigRingOff = 1536;
+constexpr uint32_t kBigRingBytes = ring_bytes(kBigLanes);
+// (lvl_sweep_ring adds a row's hardware warps' sums inside one warp)
+static_assert(kWideThreads / 32 * kBigLanes <= 32, "a row's warp sums fit one warp");
+// (and gathers a chunk's rows' own values, one row per logical warp)
+static_assert(kWideThreads / kBigLanes >= kRingRows, "a chunk's rows fit the logical warps");
 
 template <bool MIXED>
 __device__ __forceinline__ unsigned char* big_scratch(const GroupDev& d, unsigned char* dsm) {
@@ -110,7 +118,11 @@ __device__ void big_lu(const GroupDev& d, const TileCtx& c, bool act, LaneState*
     LevelShared& ls = *reinterpret_cast<LevelShared*>(scratch);
     BigLaneFlags& bf = *reinterpret_cast<BigLaneFlags*>(scratch + sizeof(LevelShared));
     void* red = scratch + 2048;
-    static_assert(sizeof(LevelShared) + sizeof(BigLaneFlags) <= 2048, "the scratch header fits 2 KB");
+    static_assert(sizeof(LevelShared) + sizeof(BigLaneFlags) <= kBigRingOff &&
+                      kBigRingOff + sizeof(RingShared) <= 2048,
+                  "the scratch header fits 2 KB");
+    RingShared* ring = d.stream ? reinterpret_cast<RingShared*>(scratch + kBigRingOff) : nullptr;
+    unsigned char* slots = scratch + kBigScratch;
     auto key_ok = [&](uint32_t kb) {
         return d.linear && LM(d.fact_key, kb) == key0 && LM(d.fact_key, kb + 1) == key1;
     };
@@ -138,6 +150,8 @@ __device__ void big_lu(const GroupDev& d, const TileCtx& c, bool act, LaneState*
                     LM(d.fact_key, 3) = key1;
                 }
             }
+            if (d.stream)
+                lvl_stream_store<float>(d, l, lane, warp, nw, go, d.lx32, d.ux32, d.stream->vf32, d.stream->vb32);
             __syncthreads();
         }
     }
@@ -151,6 +165,7 @@ __device__ void big_lu(const GroupDev& d, const TileCtx& c, bool act, LaneState*
                 LM(d.fact_key, 0) = ok ? key0 : NAN;
                 LM(d.fact_key, 1) = key1;
             }
+            if (d.stream) lvl_stream_store<double>(d, l, lane, warp, nw, go, d.lx, d.ux, d.stream->vf, d.stream->vb);
             __syncthreads();
         }
     }
@@ -164,12 +179,31 @@ __device__ void big_lu(const GroupDev& d, const TileCtx& c, bool act, LaneState*
     const bool u32 = bf.use32[lane] != 0;
     if (MIXED && __syncthreads_or(solve && u32)) {
         lvl_solve<float>(d, l, lane, warp, nw, solve && u32, d.rhs, d.dx, d.y32, d.lx32, d.ux32, d.udiag32,
-                         static_cast<float*>(red));
-        for (uint32_t r = 0; r < o.refine; r++) lvl_refine(d, l, lane, warp, nw, solve && u32, static_cast<float*>(red));
+                         static_cast<float*>(red), ring, slots, d.stream ? d.stream->vf32 : nullptr,
+                         d.stream ? d.stream->vb32 : nullptr);
+        for (uint32_t r = 0; r < o.refine; r++)
+            lvl_refine(d, l, lane, warp, nw, solve && u32, static_cast<float*>(red), ring, slots);
     }
     if (__syncthreads_or(solve && !u32))
         lvl_solve<double>(d, l, lane, warp, nw, solve && !u32, d.rhs, d.dx, d.y, d.lx, d.ux, d.udiag,
-                          static_cast<double*>(red));
+                          static_cast<double*>(red), ring, slots, d.stream ? d.stream->vf : nullptr,
+                          d.stream ? d.stream->vb : nullptr);
+    if (ring && ring->fail && act) {
+        // a staged chunk never arrived: the lane's step is lost
+        if (warp == 0) {
+            sh.bits[lane] |= kSingular;
+            sh.active[lane] = 0;
+            s->iterations = it;
+        }
+        failed = true;
+    }
+}
+
+// The ring's barriers, once per CTA of a large template with a streaming
+// plan, before its first solve.
+template <bool MIXED>
+__device__ __forceinline__ void big_ring_init(const GroupDev& d) {
+    if (d.big && d.stream) ring_init(*reinterpret_cast<RingShared*>(big_scratch<MIXED>(d, g_dsm) + kBigRingOff));
 }
 
 // One Newton solve per lane of the tile (converger.newtonLanes at W = 1 as
@@ -468,6 +502,7 @@ __global__ void __launch_bounds__(WIDE ? kWideThreads : kTileThreads, WIDE ? 1 :
     __shared__ TileShared sh;
     TileCtx c = tile_ctx(m);
     c.d = stage_template(*c.d, sh.gd, g_dsm, MIXED);
+    big_ring_init<MIXED>(*c.d);
     LaneState* s = (c.warp == 0 && c.valid) ? &st[c.d->lane0 + c.l] : nullptr;
     const bool on = !o.ladder || (c.valid && o.ladder[c.d->lane0 + c.l].on != 0);
     newton_tile<MIXED>(c, s, o, tran, false, on, sh, g_dsm, true);
@@ -743,6 +778,7 @@ __global__ void __launch_bounds__(WIDE ? kWideThreads : kTileThreads, WIDE ? 1 :
     __shared__ TileShared sh;
     TileCtx c = tile_ctx(m);
     c.d = stage_template(*c.d, sh.gd, g_dsm, MIXED);
+    big_ring_init<MIXED>(*c.d);
     const GroupDev& d = *c.d;
     const uint32_t P = d.P, l = c.l, lane = c.lane, warp = c.warp, nw = c.nw;
     const uint32_t ns = d.n_sites, ninst = n_instances(d);

@@ -29,6 +29,7 @@
 #pragma once
 
 #include "lane_engine.cuh"
+#include "lane_smem.cuh"
 
 namespace espl {
 
@@ -39,6 +40,39 @@ struct LevelShared {
     unsigned long long cmax[32];   // the column's largest |L| numerator (by bits)
     unsigned long long worst[32];  // the largest |L| over non-scaled columns (by bits)
 };
+
+// The ring of a streaming sweep (StreamDev): kRingSlots chunks staged by
+// bulk copies (cp.async.bulk, the TMA's 1-D form), each completing on the
+// mbarrier of its slot, up to kRingSlots chunks ahead of the levels that
+// read them. `seq` counts the chunks the CTA has staged (the slot of the
+// q-th is q % kRingSlots, its phase parity (q / kRingSlots) & 1); `fail`
+// is set for good when a chunk's wait runs out.
+constexpr uint32_t kRingSlots = 3, kRingChunk = 2048, kRingRows = 256;
+// a chunk's plan (tape.h StreamPlan meta): 8 header words (the last four:
+// the copy of the chunk kRingSlots ahead, which reuses its slot), at most
+// kRingRows segments of 3 words, kRingRows rows and kRingRows + 1 offsets,
+// padded to four words
+constexpr uint32_t kRingMetaWords = (8 + 5 * kRingRows + 1 + 3) & ~3u;
+struct RingShared {
+    unsigned long long bar[kRingSlots];
+    uint32_t seq, fail;
+};
+// A slot: kRingChunk entries' values for tw lanes (room for FP64), their
+// columns, and the chunk's plan.
+__host__ __device__ constexpr uint32_t ring_cols_off(uint32_t tw) { return kRingChunk * tw * 8u; }
+__host__ __device__ constexpr uint32_t ring_meta_off(uint32_t tw) { return kRingChunk * (tw * 8u + 4u); }
+__host__ __device__ constexpr uint32_t ring_slot_bytes(uint32_t tw) {
+    return ring_meta_off(tw) + kRingMetaWords * 4u;
+}
+// After the slots, the y values of the chunk being solved (room for FP64):
+// the entries' y (kRingChunk), then its rows' results (kRingRows), the
+// rows' own y before the sweep and (backward) their U diagonals.
+__host__ __device__ constexpr uint32_t ring_stage_bytes(uint32_t tw) {
+    return (kRingChunk + 3u * kRingRows) * tw * 8u;
+}
+__host__ __device__ constexpr uint32_t ring_bytes(uint32_t tw) {
+    return kRingSlots * ring_slot_bytes(tw) + ring_stage_bytes(tw);
+}
 
 template <typename T>
 __device__ __forceinline__ uint64_t mag_bits(T v) {
@@ -242,19 +276,271 @@ __device__ void lvl_sweep(const GroupDev& d, uint32_t l, uint32_t lane, uint32_t
     }
 }
 
+// The factor's values of one precision into streaming order (StreamDev),
+// after a refactor; the bulk copies that read them run in the async proxy,
+// so each writer fences its stores for it before the barrier.
+template <typename T>
+__device__ void lvl_stream_store(const GroupDev& d, uint32_t l, uint32_t lane, uint32_t warp, uint32_t nw, bool act,
+                                 const T* __restrict__ lx, const T* __restrict__ ux, T* __restrict__ vf,
+                                 T* __restrict__ vb) {
+    const uint32_t P = d.P, tw = blockDim.x / nw, part = l / tw;
+    const StreamDev& sd = *d.stream;
+    if (act) {
+        for (uint32_t e = warp; e < sd.fw.entries; e += nw) {
+            const uint32_t sl = sd.fw.slot[e];
+            vf[((size_t)part * sd.fw.entries + e) * tw + lane] = sl == kNone ? (T)0 : LM(lx, sl);
+        }
+        for (uint32_t e = warp; e < sd.bw.entries; e += nw) {
+            const uint32_t sl = sd.bw.slot[e];
+            vb[((size_t)part * sd.bw.entries + e) * tw + lane] = sl == kNone ? (T)0 : LM(ux, sl);
+        }
+    }
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+    __syncthreads();
+}
+
+__device__ __forceinline__ void ring_init(RingShared& r) {
+    if (threadIdx.x == 0) {
+        for (uint32_t k = 0; k < kRingSlots; k++) mbar_init(reinterpret_cast<uint64_t*>(&r.bar[k]), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        r.seq = 0;
+        r.fail = 0;
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ bool ring_wait(RingShared& r, uint32_t q) {
+    uint64_t* bar = reinterpret_cast<uint64_t*>(&r.bar[q % kRingSlots]);
+    const uint32_t parity = (q / kRingSlots) & 1u;
+    for (uint32_t tries = 0; tries < (1u << 22); tries++) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (tries > 64) __nanosleep(64);
+    }
+    return false;
+}
+
+// One sweep over the streaming order. Each chunk brings the values and
+// columns of its entries and its plan (segments: runs of one level's rows;
+// the rows; their entry offsets) into a ring slot. When a chunk starts, its
+// rows of earlier chunks are final, so the CTA gathers, all at once, the y
+// of every entry whose column an earlier chunk (or no row of the sweep)
+// computes, and each row's own y and U diagonal; an entry whose column a
+// row of the same chunk computes (kStreamLocal) reads that row's result,
+// which the row leaves in shared memory besides y. The levels then touch
+// global memory only to store their rows.
+//
+// Rows are split over the threads as in lvl_sweep (a segment of at least
+// nw rows: a row per logical warp; else gs logical warps per row, whose
+// parts a butterfly of warp shuffles adds, and where a row spans hardware
+// warps the warps' sums go through `red` and a second butterfly inside one
+// hardware warp). A barrier ends each level; there thread 0 refills the
+// slots whose chunks are done, so a chunk needs a barrier of its own for
+// its copies only when it is not yet staged.
+//
+// Thread 0 issues the copies; every thread waits for a chunk before reading
+// it, and the CTA agrees on the outcome (a barrier) before any thread reads
+// the chunk's plan. A wait that runs out ends the sweep: no more copies are
+// issued, thread 0 waits once more, bounded, for the copies still in
+// flight, and ring.fail is set, so that the sweep and every later one of
+// the CTA return false (their results are not used).
+template <typename T, bool BACK>
+__device__ bool lvl_sweep_ring(const GroupDev& d, uint32_t l, uint32_t lane, uint32_t warp, uint32_t nw, bool act,
+                               const StreamSweep& sw, const T* __restrict__ vso, const T* __restrict__ ud,
+                               T* __restrict__ y, T* red, RingShared& ring, unsigned char* slots) {
+    const uint32_t P = d.P, tw = blockDim.x / nw, spw = 32u / tw, part = l / tw;
+    const uint32_t sb = ring_slot_bytes(tw), nc = sw.n_chunks, q0 = ring.seq;
+    const uint32_t hw = threadIdx.x >> 5, hl = threadIdx.x & 31u;
+    const bool t0 = threadIdx.x == 0;
+    // the chunk's y: entries' (kRingChunk), then its rows' results, the
+    // rows' own y and U diagonals (kRingRows each); tw values per item
+    T* ys = reinterpret_cast<T*>(slots + kRingSlots * sb);
+    T* yo = ys + (kRingChunk + kRingRows) * tw;
+    T* yd = yo + kRingRows * tw;
+    if (ring.fail) return false;
+    uint32_t sent = 0, confirmed = 0;  // thread 0: chunks issued, and waited for
+    auto stage = [&](uint32_t lim) {   // thread 0: copies of the chunks before lim
+        for (; sent < lim; sent++) {
+            const uint32_t q = q0 + sent, slot = q % kRingSlots;
+            unsigned char* base = slots + slot * sb;
+            // the first chunks' copies from the plan in global memory, the
+            // later ones from the header of the chunk whose slot they take
+            uint32_t e0, len, m0, mlen;
+            if (sent < kRingSlots) {
+                e0 = sw.ch[sent];
+                len = sw.ch[sent + 1] - e0;
+                m0 = sw.mo[sent];
+                mlen = sw.mo[sent + 1] - m0;
+            } else {
+                const uint4 h = *reinterpret_cast<const uint4*>(base + ring_meta_off(tw) + 16);
+                e0 = h.x;
+                len = h.y;
+                m0 = h.z;
+                mlen = h.w;
+            }
+            const uint32_t vbytes = len * tw * (uint32_t)sizeof(T);
+            uint64_t* bar = reinterpret_cast<uint64_t*>(&ring.bar[slot]);
+            mbar_arrive_expect_tx(bar, vbytes + len * 4u + mlen * 4u);
+            bulk_g2s_once(base, vso + ((size_t)part * sw.entries + e0) * tw, vbytes, bar);
+            bulk_g2s(base + ring_cols_off(tw), sw.col + e0, len * 4u, bar);
+            bulk_g2s(base + ring_meta_off(tw), sw.meta + m0, mlen * 4u, bar);
+        }
+    };
+    // the chunks staged so far by the schedule every thread follows (thread 0
+    // issues them)
+    uint32_t sched = nc < kRingSlots ? nc : kRingSlots;
+    if (t0) stage(sched);
+    bool failed = false;
+    for (uint32_t c = 0; c < nc; c++) {
+        if (c >= sched) {
+            __syncthreads();  // every thread is done with chunk c - kRingSlots
+            sched = min(nc, c + kRingSlots);
+            if (t0) stage(sched);
+        }
+        const uint32_t slot = (q0 + c) % kRingSlots;
+        unsigned char* base = slots + slot * sb;
+        // (the barrier also orders the rows of earlier chunks before the gather)
+        if (__syncthreads_or(!ring_wait(ring, q0 + c))) {
+            failed = true;
+            break;
+        }
+        confirmed = c + 1;
+        const T* sv = reinterpret_cast<const T*>(base);
+        const uint32_t* sc = reinterpret_cast<const uint32_t*>(base + ring_cols_off(tw));
+        const uint32_t* meta = reinterpret_cast<const uint32_t*>(base + ring_meta_off(tw));
+        const uint32_t ns = meta[0], nr = meta[1], len = meta[2];
+        const uint32_t* sg = meta + 8;
+        const uint32_t* ri = sg + 3 * ns;
+        const uint32_t* rp = ri + nr;
+        if (act) {
+            // eight entries and a row per thread and batch, every load of a
+            // batch in flight before its stores
+            for (uint32_t b = warp; b < len || b < nr; b += 8 * nw) {
+                T ve[8], vo = (T)0, vd = (T)1;
+#pragma unroll
+                for (int k = 0; k < 8; k++) {
+                    const uint32_t j = b + k * nw;
+                    const uint32_t code = j < len ? sc[j] : kStreamLocal;
+                    ve[k] = (code & kStreamLocal) ? (T)0 : LM(y, code);
+                }
+                if (b < nr) {
+                    const uint32_t i = ri[b];
+                    vo = LM(y, i);
+                    if (BACK) vd = LM(ud, i);
+                }
+#pragma unroll
+                for (int k = 0; k < 8; k++) {
+                    const uint32_t j = b + k * nw;
+                    if (j < len) ys[j * tw + lane] = ve[k];
+                }
+                if (b < nr) {
+                    yo[b * tw + lane] = vo;
+                    if (BACK) yd[b * tw + lane] = vd;
+                }
+            }
+        }
+        __syncthreads();
+        // a row's sum over entries e = e0, e0 + stride, ... < e1 of the chunk
+        auto dot = [&](uint32_t e0, uint32_t e1, uint32_t stride) {
+            T acc = (T)0;
+            for (uint32_t e = e0; e < e1; e += 8 * stride) {
+                T v[8], yv[8];
+#pragma unroll
+                for (int k = 0; k < 8; k++) {
+                    const uint32_t ek = e + k * stride;
+                    const bool ok = ek < e1;
+                    const uint32_t j = ok ? ek : 0u, code = sc[j];
+                    const uint32_t at = (code & kStreamLocal) ? kRingChunk + (code & ~kStreamLocal) : j;
+                    v[k] = ok ? sv[j * tw + lane] : (T)0;
+                    yv[k] = ok ? ys[at * tw + lane] : (T)0;
+                }
+                T s = v[0] * yv[0];
+#pragma unroll
+                for (int k = 1; k < 8; k++) s += v[k] * yv[k];
+                acc += s;
+            }
+            return acc;
+        };
+        // row r of the chunk's result: y and its shared copy
+        auto finish = [&](uint32_t r, T part_sum) {
+            T acc = yo[r * tw + lane] - part_sum;
+            if (BACK) acc = acc / yd[r * tw + lane];
+            ys[(kRingChunk + r) * tw + lane] = acc;
+            LM(y, ri[r]) = acc;
+        };
+        for (uint32_t g = 0; g < ns; g++) {
+            const uint32_t k0 = sg[3 * g], k1 = sg[3 * g + 1], last = sg[3 * g + 2], m = k1 - k0;
+            bool reused = false;  // red was read: a barrier before its next use
+            if (m >= nw) {
+                if (act)
+                    for (uint32_t k = k0 + warp; k < k1; k += nw) finish(k, dot(rp[k], rp[k + 1], 1u));
+            } else {
+                uint32_t gs = 1;
+                while (gs * 2 * m <= nw) gs *= 2;
+                const uint32_t row = warp / gs, sub = warp % gs;
+                const bool across = gs > spw;  // a row spans hardware warps
+                T ps = (T)0;
+                if (row < m && act) ps = dot(rp[k0 + row] + sub, rp[k0 + row + 1], gs);
+                for (uint32_t o = 1; o < gs && o < spw; o *= 2) ps += __shfl_xor_sync(0xffffffffu, ps, o * tw);
+                if (across) {
+                    // hardware warp w's sum of its row at red[w * tw + lane];
+                    // hardware warp r adds row r's nh warps' sums
+                    const uint32_t nh = gs / spw;
+                    if (hl < tw) red[hw * tw + lane] = ps;
+                    __syncthreads();
+                    ps = (hw < m && hl < nh * tw) ? red[hw * nh * tw + hl] : (T)0;
+                    for (uint32_t o = tw; o < nh * tw; o *= 2) ps += __shfl_xor_sync(0xffffffffu, ps, o);
+                    if (hw < m && hl < tw && act) finish(k0 + hw, ps);
+                    reused = true;
+                } else if (row < m && sub == 0 && act) {
+                    finish(k0 + row, ps);
+                }
+            }
+            if (last || reused) __syncthreads();
+            if (last) {
+                // the chunks before c are done, and c itself after its last segment
+                const uint32_t lim = min(nc, c + kRingSlots + (g + 1 == ns ? 1u : 0u));
+                if (lim > sched) {
+                    sched = lim;
+                    if (t0) stage(sched);
+                }
+            }
+        }
+    }
+    __syncthreads();
+    if (t0) {
+        if (failed) {
+            // the copies still in flight, once more
+            for (uint32_t c = confirmed; c < sent; c++) ring_wait(ring, q0 + c);
+            ring.fail = 1;
+        }
+        ring.seq = q0 + nc;
+    }
+    __syncthreads();
+    return !failed;
+}
+
 // out = -A^-1 rhs through the lane's factors (luSolve with neg, solve64's
 // contract), every thread of the CTA taking part.
 template <typename T>
 __device__ void lvl_solve(const GroupDev& d, uint32_t l, uint32_t lane, uint32_t warp, uint32_t nw, bool act,
                           const double* __restrict__ rhs, double* __restrict__ out, T* __restrict__ y,
-                          const T* __restrict__ lx, const T* __restrict__ ux, const T* __restrict__ ud, T* red) {
+                          const T* __restrict__ lx, const T* __restrict__ ux, const T* __restrict__ ud, T* red,
+                          RingShared* ring = nullptr, unsigned char* slots = nullptr, const T* vf = nullptr,
+                          const T* vb = nullptr) {
     const uint32_t P = d.P;
     if (act)
         for (uint32_t r = warp; r < d.n; r += nw) LM(y, d.pinv[r]) = (T)(-LM(rhs, r));
     __syncthreads();
-    lvl_sweep<T, false>(d, l, lane, warp, nw, act, d.fl_ptr, d.fl_rows, d.n_fl, d.rl_ptr, d.rl_ent, lx, nullptr, y,
-                        red);
-    lvl_sweep<T, true>(d, l, lane, warp, nw, act, d.bl_ptr, d.bl_rows, d.n_bl, d.ru_ptr, d.ru_ent, ux, ud, y, red);
+    if (ring && vf) {
+        // (a failed sweep leaves ring->fail set; the caller reads it)
+        if (lvl_sweep_ring<T, false>(d, l, lane, warp, nw, act, d.stream->fw, vf, nullptr, y, red, *ring, slots))
+            lvl_sweep_ring<T, true>(d, l, lane, warp, nw, act, d.stream->bw, vb, ud, y, red, *ring, slots);
+    } else {
+        lvl_sweep<T, false>(d, l, lane, warp, nw, act, d.fl_ptr, d.fl_rows, d.n_fl, d.rl_ptr, d.rl_ent, lx, nullptr,
+                            y, red);
+        lvl_sweep<T, true>(d, l, lane, warp, nw, act, d.bl_ptr, d.bl_rows, d.n_bl, d.ru_ptr, d.ru_ent, ux, ud, y,
+                           red);
+    }
     if (act)
         for (uint32_t j = warp; j < d.n; j += nw) LM(out, d.q[j]) = (double)LM(y, j);
     __syncthreads();
@@ -264,7 +550,7 @@ __device__ void lvl_solve(const GroupDev& d, uint32_t l, uint32_t lane, uint32_t
 // contract), rows split over the warps through the row view of A:
 // r = rhs + A dx, dx += -A^-1 r by the FP32 factors.
 __device__ void lvl_refine(const GroupDev& d, uint32_t l, uint32_t lane, uint32_t warp, uint32_t nw, bool act,
-                           float* red) {
+                           float* red, RingShared* ring = nullptr, unsigned char* slots = nullptr) {
     const uint32_t P = d.P;
     if (act)
         for (uint32_t i = warp; i < d.n; i += nw) {
@@ -273,7 +559,8 @@ __device__ void lvl_refine(const GroupDev& d, uint32_t l, uint32_t lane, uint32_
             LM(d.rr, i) = r;
         }
     __syncthreads();
-    lvl_solve<float>(d, l, lane, warp, nw, act, d.rr, d.corr, d.y32, d.lx32, d.ux32, d.udiag32, red);
+    lvl_solve<float>(d, l, lane, warp, nw, act, d.rr, d.corr, d.y32, d.lx32, d.ux32, d.udiag32, red, ring, slots,
+                     d.stream ? d.stream->vf32 : nullptr, d.stream ? d.stream->vb32 : nullptr);
     if (act)
         for (uint32_t i = warp; i < d.n; i += nw) LM(d.dx, i) += LM(d.corr, i);
     __syncthreads();

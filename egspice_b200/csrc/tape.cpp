@@ -1080,4 +1080,83 @@ void level_plan(const Tape& t, LevelPlan& out) {
     bucket(lev, out.bl_ptr, out.bl_rows);
 }
 
+bool stream_plan(const std::vector<uint32_t>& lev_ptr, const std::vector<uint32_t>& rows,
+                 const std::vector<uint32_t>& row_ptr, const std::vector<uint32_t>& ent, uint32_t chunk,
+                 uint32_t max_rows, uint32_t ahead, bool skip_empty, StreamPlan& out) {
+    out = StreamPlan{};
+    out.ch.push_back(0);
+    out.mo.push_back(0);
+    // the open chunk: its segments (3 words each), rows and entry offsets
+    std::vector<uint32_t> seg, ri, rp;
+    // the chunk and position that compute each row
+    const size_t n = row_ptr.empty() ? 0 : row_ptr.size() - 1;
+    std::vector<uint32_t> in_chunk(n, kNone), at(n, 0);
+    uint32_t e = 0, c0 = 0;  // next entry, first entry of the open chunk
+    auto close = [&]() {
+        if (ri.empty()) return;
+        while (e % 4u) {  // the next chunk starts on a multiple of four entries
+            out.col.push_back(0);
+            out.slot.push_back(kNone);
+            e++;
+        }
+        rp.push_back(e - c0);
+        const uint32_t ns = (uint32_t)seg.size() / 3, nr = (uint32_t)ri.size();
+        const size_t m0 = out.meta.size();
+        out.meta.insert(out.meta.end(), {ns, nr, e - c0, 0u, 0u, 0u, 0u, 0u});
+        out.meta.insert(out.meta.end(), seg.begin(), seg.end());
+        out.meta.insert(out.meta.end(), ri.begin(), ri.end());
+        out.meta.insert(out.meta.end(), rp.begin(), rp.end());
+        while (out.meta.size() % 4u) out.meta.push_back(0);
+        out.max_meta = std::max(out.max_meta, (uint32_t)(out.meta.size() - m0));
+        out.ch.push_back(e);
+        out.mo.push_back((uint32_t)out.meta.size());
+        seg.clear();
+        ri.clear();
+        rp.clear();
+        c0 = e;
+    };
+    for (size_t v = 0; v + 1 < lev_ptr.size(); v++) {
+        bool open = false;  // a segment of this level is open in the chunk
+        for (uint32_t k = lev_ptr[v]; k < lev_ptr[v + 1]; k++) {
+            const uint32_t i = rows[k];
+            const uint32_t len = row_ptr[i + 1] - row_ptr[i];
+            if (len > chunk) return false;
+            if (len == 0 && skip_empty) continue;
+            if (e - c0 + len > chunk || ri.size() + 1 > max_rows) {
+                close();
+                open = false;
+            }
+            if (!open) {
+                seg.insert(seg.end(), {(uint32_t)ri.size(), (uint32_t)ri.size(), 0u});
+                open = true;
+            }
+            const uint32_t cur = (uint32_t)out.ch.size() - 1;
+            in_chunk[i] = cur;
+            at[i] = (uint32_t)ri.size();
+            ri.push_back(i);
+            rp.push_back(e - c0);
+            for (uint32_t p = row_ptr[i]; p < row_ptr[i + 1]; p++) {
+                const uint32_t j = ent[2 * (size_t)p];
+                out.col.push_back(in_chunk[j] == cur ? (kStreamLocal | at[j]) : j);
+                out.slot.push_back(ent[2 * (size_t)p + 1]);
+                e++;
+            }
+            seg[seg.size() - 2] = (uint32_t)ri.size();
+        }
+        if (open) seg.back() = 1;  // the level's last segment
+    }
+    close();
+    out.entries = e;
+    out.n_chunks = (uint32_t)out.ch.size() - 1;
+    for (uint32_t c = 0; c + ahead < out.n_chunks; c++) {
+        const uint32_t a = c + ahead;
+        uint32_t* h = out.meta.data() + out.mo[c];
+        h[4] = out.ch[a];
+        h[5] = out.ch[a + 1] - out.ch[a];
+        h[6] = out.mo[a];
+        h[7] = out.mo[a + 1] - out.mo[a];
+    }
+    return true;
+}
+
 }  // namespace espl

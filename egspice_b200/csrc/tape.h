@@ -119,4 +119,34 @@ struct LevelPlan {
 };
 void level_plan(const Tape& t, LevelPlan& out);
 
+// A sweep of the level schedule in streaming order, for solves that stage
+// the factor through shared memory: the sweep's entries in the order the
+// levels read them (level by level, row by row, a row's entries by
+// column), cut into chunks of at most `chunk` entries and `max_rows` rows
+// that end on a row and start on a multiple of four entries (padding
+// entries, column 0 and slot kNone, fill the gaps). With skip_empty the
+// rows without entries are left out (a forward row without L entries keeps
+// its value). False when a row is longer than `chunk`.
+//   col[e], slot[e]  column and factor slot of entry e (kNone: padding);
+//                    a column that a row of the same chunk computes is
+//                    kStreamLocal | that row's position in the chunk
+//   ch[c]            first entry of chunk c (n_chunks + 1 values)
+//   meta[mo[c] ..]   chunk c's plan, a multiple of four words: ns, nr, its
+//                    entries (ch[c + 1] - ch[c]), 0; the copy of chunk
+//                    c + ahead (first entry, entries, first plan word,
+//                    plan words; zeros past the last chunk);
+//                    ns segments (runs of rows of one level inside the
+//                    chunk) of 3 words: first row, end row (of the chunk's
+//                    rows), 1 when the segment ends its level; the nr rows'
+//                    indices; nr + 1 entry offsets (from ch[c]) of the rows
+//   max_meta         the longest chunk plan, words
+constexpr uint32_t kStreamLocal = 0x80000000u;
+struct StreamPlan {
+    uint32_t entries = 0, n_chunks = 0, max_meta = 0;
+    std::vector<uint32_t> col, slot, ch, meta, mo;
+};
+bool stream_plan(const std::vector<uint32_t>& lev_ptr, const std::vector<uint32_t>& rows,
+                 const std::vector<uint32_t>& row_ptr, const std::vector<uint32_t>& ent, uint32_t chunk,
+                 uint32_t max_rows, uint32_t ahead, bool skip_empty, StreamPlan& out);
+
 }  // namespace espl
