@@ -553,7 +553,11 @@ espl_status alloc_group(espl_lanes* h, Group& g) {
             };
             split(4, d.gsplit4);
             split(16, d.gsplit16);
-            if ((s = dupload(h, own, &d.gi_ptr, ip)) || (s = dupload(h, own, &d.gi_ent, ie))) return s;
+            std::vector<uint32_t> big(kBigWarps + 1);
+            split(kBigWarps, big.data());
+            if ((s = dupload(h, own, &d.gi_ptr, ip)) || (s = dupload(h, own, &d.gi_ent, ie)) ||
+                (s = dupload(h, own, &d.gsplit_big, big)))
+                return s;
         }
         {
             std::vector<uint32_t> gs = gmin_stamps(g, pl);
@@ -655,7 +659,7 @@ espl_status alloc_group(espl_lanes* h, Group& g) {
     AL(corr, n1 * P);
     AL(udiag, n1 * P);
     AL(udiag32, n1 * P);
-    AL(fact_key, 4 * (size_t)P);
+    AL(fact_key, kFactKeys * (size_t)P);
     d.linear = (d.n_dio == 0 && d.n_mos == 0) ? 1u : 0u;
     // the dense peel's scratch, where the template's lanes need at most 4 GB
     // of it (past that a failed lane reports singular)
@@ -726,7 +730,7 @@ espl_status ensure_stream(espl_lanes* h, Group& g, bool mixed) {
     CK(cudaMemcpyAsync(p, &g.sd, sizeof(StreamDev), cudaMemcpyHostToDevice, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     g.d_sd = p;
-    if (g.dev.fact_key) CK(cudaMemsetAsync(g.dev.fact_key, 0, sizeof(double) * 4 * P, h->stream));
+    if (g.dev.fact_key) CK(cudaMemsetAsync(g.dev.fact_key, 0, sizeof(double) * kFactKeys * P, h->stream));
     return ESPL_OK;
 }
 
@@ -1066,7 +1070,7 @@ espl_status upload_tape(espl_lanes* h, Group& g) {
 #undef UP
         size_t P = g.P;
         // a new tape invalidates every lane's factor
-        if (d.fact_key) CK(cudaMemsetAsync(d.fact_key, 0, sizeof(double) * 4 * P, h->stream));
+        if (d.fact_key) CK(cudaMemsetAsync(d.fact_key, 0, sizeof(double) * kFactKeys * P, h->stream));
         if ((s = dalloc(h, own, &d.lx, (size_t)d.nnz_l * P))) return s;
         if ((s = dalloc(h, own, &d.ux, (size_t)d.nnz_u * P))) return s;
         if (h->precision == ESPL_MIXED) {

@@ -35,6 +35,7 @@ constexpr double kWide = 1.0 / 1e-3;   // LaneTab.wide = 1 / pivot_tol
 // hands larger failed lanes to the host factor; with no host path here the
 // dense peel covers up to 256, within a scratch budget (alloc_group).
 constexpr uint32_t kDensePeelMax = 256;
+constexpr uint32_t kFactKeys = 6;  // GroupDev fact_key words per lane
 
 // Gate bits (kernels/lane.zig:708-711).
 constexpr uint32_t kActive = 1, kInitFix = 2, kConverged = 4, kSingular = 8, kPassed = 16, kParked = 32;
@@ -99,6 +100,7 @@ struct GroupDev {
     uint32_t n_gi, n_items;
     uint32_t gsplit4[5], gsplit16[17];
     uint32_t gsplit_pad[2];
+    const uint32_t* gsplit_big;  // the same for the kBigWarps shares of a large template's part
     // Stale-tape words of the template: [0] set when, in some Newton
     // iteration, at least half of a tile's active lanes failed the replay;
     // [1] the smallest such failing lane (the host retapes from its A).
@@ -125,10 +127,12 @@ struct GroupDev {
     // Large templates (lane_levels.cuh, big = 1): the whole CTA refactors by
     // columns and solves by levels (tape.h LevelPlan). linear: no nonlinear
     // device, so a lane's A depends only on its companion coefficient and
-    // gmin; fact_key (2 per lane: the ag0 of the factored A, or -1 without a
-    // companion, and its gmin) names the A of the lane's last factor, and an
-    // unchanged key skips the refactor (the reference skips refactoring
-    // identical values, src/solver/direct.zig:313).
+    // gmin; fact_key (kFactKeys per lane) names, by such a key pair (the
+    // ag0, or -1 without a companion, and the gmin), the A of the lane's
+    // FP64 factor (words 0-1), of its FP32 factor (2-3) and the A assembled
+    // in `a` (4-5). An unchanged key skips the refactor (the reference skips
+    // refactoring identical values, src/solver/direct.zig:313), and the
+    // gather of A's entries (the right-hand sides are still gathered).
     const uint32_t *fl_ptr, *fl_rows, *bl_ptr, *bl_rows, *rl_ptr, *rl_ent, *ru_ptr, *ru_ent;
     uint32_t n_fl, n_bl, big, linear;
     double* fact_key;

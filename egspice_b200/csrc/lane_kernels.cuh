@@ -26,6 +26,7 @@ struct TileMap {
 // The Newton launches of a large template run each 32-lane tile as
 // 32 >> kBigShift parts of kBigLanes lanes.
 constexpr uint32_t kBigShift = 4, kBigLanes = 32u >> kBigShift;
+constexpr uint32_t kBigWarps = kWideThreads / kBigLanes;  // work shares per lane of a part
 
 // A tile-list entry: the tile in bits 0-23; in bits 24-27 the part of it
 // this CTA runs and in bits 28-31 the shift s of the part's width 32 >> s
@@ -266,20 +267,39 @@ __device__ __forceinline__ void newton_tile(const TileCtx& c, LaneState* s, cons
             tm = sh.t[lane];
         }
         const double* cells = d.cells;
+        // A linear large template whose lanes' A was assembled for this
+        // iteration's companion coefficient and gmin keeps it: the CTA
+        // gathers only the right-hand sides.
+        bool rhs_only = false;
+        if (d.big && d.linear && !o.ladder) {
+            const double k0 = cp.on ? cp.ag0 : -1.0;
+            rhs_only = __syncthreads_and(!act || (LM(d.fact_key, 4) == k0 && LM(d.fact_key, 5) == o.gmin)) != 0;
+        }
         if (act) {
             uint32_t it0, it1;
-            if (nw == 4) {
+            if (rhs_only) {
+                it0 = d.nnz + (uint32_t)((uint64_t)d.n * warp / nw);
+                it1 = d.nnz + (uint32_t)((uint64_t)d.n * (warp + 1) / nw);
+            } else if (nw == 4) {
                 it0 = d.gsplit4[warp];
                 it1 = d.gsplit4[warp + 1];
             } else if (nw == 16) {
                 it0 = d.gsplit16[warp];
                 it1 = d.gsplit16[warp + 1];
+            } else if (nw == kBigWarps) {
+                it0 = d.gsplit_big[warp];
+                it1 = d.gsplit_big[warp + 1];
             } else {
                 it0 = (uint32_t)((uint64_t)d.n_items * warp / nw);
                 it1 = (uint32_t)((uint64_t)d.n_items * (warp + 1) / nw);
             }
             gather_items<T>(d, l, lane, it0, it1, cp, o.ladder ? 0.0 : o.gmin, cells,
                             sm ? static_cast<T*>(st.a) : nullptr);
+            if (d.big && d.linear && !rhs_only && warp == 0) {
+                // (the ladder adds its gmin to A below: no key names that A)
+                LM(d.fact_key, 4) = o.ladder ? NAN : (cp.on ? cp.ag0 : -1.0);
+                LM(d.fact_key, 5) = o.gmin;
+            }
         }
         __syncthreads();
         if (o.ladder) {
