@@ -320,8 +320,8 @@ __device__ __forceinline__ bool ring_wait(RingShared& r, uint32_t q) {
 }
 
 // One sweep over the streaming order. Each chunk brings the values and
-// columns of its entries and its plan (segments: runs of one level's rows;
-// the rows; their entry offsets) into a ring slot. When a chunk starts, its
+// columns of its entries and its plan (segments: runs of one level's rows,
+// with their longest row; the rows; their entry offsets) into a ring slot. When a chunk starts, its
 // rows of earlier chunks are final, so the CTA gathers, all at once, the y
 // of every entry whose column an earlier chunk (or no row of the sweep)
 // computes, and each row's own y and U diagonal; an entry whose column a
@@ -330,10 +330,10 @@ __device__ __forceinline__ bool ring_wait(RingShared& r, uint32_t q) {
 // global memory only to store their rows.
 //
 // Rows are split over the threads as in lvl_sweep (a segment of at least
-// nw rows: a row per logical warp; else gs logical warps per row, whose
-// parts a butterfly of warp shuffles adds, and where a row spans hardware
-// warps the warps' sums go through `red` and a second butterfly inside one
-// hardware warp). A barrier ends each level; there thread 0 refills the
+// nw rows: a row per logical warp; else gs logical warps per row, no more
+// than its longest row needs, whose parts a butterfly of warp shuffles
+// adds, and where a row spans hardware warps the warps' sums go through
+// `red` and a second butterfly inside one hardware warp). A barrier ends each level; there thread 0 refills the
 // slots whose chunks are done, so a chunk needs a barrier of its own for
 // its copies only when it is not yet staged.
 //
@@ -468,14 +468,18 @@ __device__ bool lvl_sweep_ring(const GroupDev& d, uint32_t l, uint32_t lane, uin
             LM(y, ri[r]) = acc;
         };
         for (uint32_t g = 0; g < ns; g++) {
-            const uint32_t k0 = sg[3 * g], k1 = sg[3 * g + 1], last = sg[3 * g + 2], m = k1 - k0;
+            const uint32_t k0 = sg[3 * g], k1 = sg[3 * g + 1], last = sg[3 * g + 2] & 1u, m = k1 - k0;
+            const uint32_t longest = sg[3 * g + 2] >> 1;
             bool reused = false;  // red was read: a barrier before its next use
             if (m >= nw) {
                 if (act)
                     for (uint32_t k = k0 + warp; k < k1; k += nw) finish(k, dot(rp[k], rp[k + 1], 1u));
             } else {
+                // shares per row: enough for one pass of the dot's eight
+                // entries over the longest row, as far as the rows leave
+                // logical warps (the others wait at the level's barrier)
                 uint32_t gs = 1;
-                while (gs * 2 * m <= nw) gs *= 2;
+                while (gs * 2 * m <= nw && gs * 8 < longest) gs *= 2;
                 const uint32_t row = warp / gs, sub = warp % gs;
                 const bool across = gs > spw;  // a row spans hardware warps
                 T ps = (T)0;

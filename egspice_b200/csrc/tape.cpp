@@ -1135,6 +1135,7 @@ bool stream_plan(const std::vector<uint32_t>& lev_ptr, const std::vector<uint32_
             at[i] = (uint32_t)ri.size();
             ri.push_back(i);
             rp.push_back(e - c0);
+            seg.back() = std::max(seg.back(), len << 1);
             for (uint32_t p = row_ptr[i]; p < row_ptr[i + 1]; p++) {
                 const uint32_t j = ent[2 * (size_t)p];
                 out.col.push_back(in_chunk[j] == cur ? (kStreamLocal | at[j]) : j);
@@ -1143,7 +1144,7 @@ bool stream_plan(const std::vector<uint32_t>& lev_ptr, const std::vector<uint32_
             }
             seg[seg.size() - 2] = (uint32_t)ri.size();
         }
-        if (open) seg.back() = 1;  // the level's last segment
+        if (open) seg.back() |= 1u;  // the level's last segment
     }
     close();
     out.entries = e;

@@ -137,8 +137,9 @@ void level_plan(const Tape& t, LevelPlan& out);
 //                    plan words; zeros past the last chunk);
 //                    ns segments (runs of rows of one level inside the
 //                    chunk) of 3 words: first row, end row (of the chunk's
-//                    rows), 1 when the segment ends its level; the nr rows'
-//                    indices; nr + 1 entry offsets (from ch[c]) of the rows
+//                    rows), and its longest row's entries times two, plus 1
+//                    when the segment ends its level; the nr rows' indices;
+//                    nr + 1 entry offsets (from ch[c]) of the rows
 //   max_meta         the longest chunk plan, words
 constexpr uint32_t kStreamLocal = 0x80000000u;
 struct StreamPlan {
