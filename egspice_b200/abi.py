@@ -85,6 +85,19 @@ class ClassInfo(C.Structure):
                 ("last_ms", C.c_double)]
 
 
+class PlanChoice(C.Structure):
+    """espl_plan_choice: a template's launch-plan choice (0 fields: automatic)."""
+    _fields_ = [("tile", C.c_uint32), ("stage", C.c_uint32), ("per_sm", C.c_uint32), ("pad", C.c_uint32)]
+
+
+class TuneReport(C.Structure):
+    _fields_ = [("trials", C.c_uint32), ("cached", C.c_uint32), ("auto_ms", C.c_double), ("best_ms", C.c_double)]
+
+
+TILE_AUTO, TILE_NARROW, TILE_WIDE = 0, 1, 2
+STAGE_AUTO, STAGE_LU, STAGE_LU_GLOBAL_RECORDS, STAGE_INDEX, STAGE_NONE = 0, 1, 2, 3, 4
+
+
 class OrcNewtonResult(C.Structure):
     _fields_ = [("converged", C.c_uint32), ("singular", C.c_uint32), ("iterations", C.c_uint32),
                 ("reserved", C.c_uint32)]

@@ -114,6 +114,8 @@ struct Group {
     StreamDev sd{};
     StreamDev* d_sd = nullptr;
     bool sd_ok = false;
+    bool band_avail = false;             // a banded replay plan exists (upload_tape)
+    espl_plan_choice choice{};           // the launch-plan choices (espl_set_plan), zeros: automatic
     espl_mlp* pred = nullptr;            // the learned step predictor (borrowed), or none
     std::vector<void*> learn_owned;      // prev2, xpred
     std::vector<void*> rec_owned;        // the step recorder's buffers
@@ -769,9 +771,28 @@ espl_status plan_classes(espl_lanes* h) {
         g.dev.n_srec = g.n_srec;
         g.dev.srec_stage = g.n_srec ? 1u : 0u;
         g.dev.stage_mode = kStageNone;
+        g.dev.band_ok = g.band_avail ? 1u : 0u;
         bytes[i] = 0;
         bool placed = false;
+        const espl_plan_choice& ch = g.choice;
+        if (ch.stage >= ESPL_STAGE_LU && ch.stage <= ESPL_STAGE_NONE) {
+            // the chosen staging, where it fits (else the automatic order below)
+            const uint32_t mode = ch.stage <= ESPL_STAGE_LU_GLOBAL_RECORDS ? kStageLu
+                                  : ch.stage == ESPL_STAGE_INDEX          ? kStageIndex
+                                                                          : kStageNone;
+            GroupDev trial = g.dev;
+            if (ch.stage == ESPL_STAGE_LU_GLOBAL_RECORDS) trial.rec_stage = trial.srec_stage = 0;
+            const SmemPlan sp = smem_plan(trial, mode, MIXED);
+            if (sp.bytes <= (uint32_t)max_dyn) {
+                g.dev = trial;
+                g.dev.stage_mode = mode;
+                g.dev.band_off = sp.band_off;
+                bytes[i] = sp.bytes;
+                placed = true;
+            }
+        }
         for (uint32_t mode : {kStageLu, kStageIndex, kStageNone}) {
+            if (placed) break;
             SmemPlan sp = smem_plan(g.dev, mode, MIXED);
             if (mode == kStageLu && sp.bytes > (uint32_t)max_dyn) {
                 // the chain may still fit with its records left in global memory
@@ -806,10 +827,11 @@ espl_status plan_classes(espl_lanes* h) {
             g.dev.stream = g.d_sd;
             bytes[i] += kBigRingBytes;
         }
-        wide[i] = g.dev.band_ok != 0 || g.dev.big != 0;
+        // (the banded replay and the CTA-wide LU need wide tiles)
+        wide[i] = g.dev.band_ok != 0 || g.dev.big != 0 || ch.tile == ESPL_TILE_WIDE;
         int t = 0;
         if ((s = tiles_per_sm(wide[i], bytes[i], t))) return s;
-        if (g.dev.stage_mode == kStageLu && (g.dev.n_rec || g.dev.n_srec)) {
+        if (g.dev.stage_mode == kStageLu && (g.dev.n_rec || g.dev.n_srec) && ch.stage == ESPL_STAGE_AUTO) {
             // Staged records cost their own words of shared memory; where
             // that drops a resident tile per SM they stay in global memory
             // (read through L1, one record ahead). The solve records go
@@ -852,7 +874,8 @@ espl_status plan_classes(espl_lanes* h) {
                 wide_tiles += tiles;
             } else {
                 narrow_sms += (double)tiles / per[i];
-                order.push_back(i);
+                // (a template whose tiles were chosen narrow stays so)
+                if (h->groups[i].choice.tile != ESPL_TILE_NARROW) order.push_back(i);
             }
         }
         auto work = [&](size_t i) {
@@ -873,6 +896,25 @@ espl_status plan_classes(espl_lanes* h) {
             per[i] = (uint32_t)t;
             wide_tiles += tiles;
             narrow_sms = rest;
+        }
+    }
+    // A cap on resident tiles per SM (espl_plan_choice.per_sm): the tile's
+    // dynamic shared memory grows until no more than the cap fit an SM.
+    {
+        int sm_smem = 0;
+        CK(cudaDeviceGetAttribute(&sm_smem, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+        const int stat = (int)std::max(fs.sharedSizeBytes, ft.sharedSizeBytes);
+        for (size_t i = 0; i < h->groups.size(); i++) {
+            const uint32_t cap = h->groups[i].choice.per_sm;
+            if (!cap || per[i] <= cap) continue;
+            // (cap + 1) tiles no longer fit: each takes its shared memory
+            // plus the static part and the 1 KB the runtime reserves per block
+            const int need = sm_smem / (int)(cap + 1) - stat - 1024 + 16;
+            bytes[i] = std::max(bytes[i], (uint32_t)std::min(need, max_dyn));
+            int t = 0;
+            espl_status s;
+            if ((s = tiles_per_sm(wide[i], bytes[i], t))) return s;
+            per[i] = (uint32_t)t;
         }
     }
     // classes by (tile width, resident tiles per SM), the one with the most
@@ -1011,8 +1053,10 @@ espl_status upload_tape(espl_lanes* h, Group& g) {
             // cannot hold (plan_classes decides which run it)
             BandPlan bp;
             d.band_ok = 0;
+            g.band_avail = false;
             if (d.n_prog && band_plan(g.tape, prog, kBandMax, kBandLRing, kBandWords, kBandEntries, bp)) {
                 d.band_ok = 1;
+                g.band_avail = true;
                 d.band_w = bp.w_ring;
                 d.band_l = bp.l_ring;
                 d.band_chunks = (uint32_t)bp.chunk_pc.size() - 1;
@@ -2326,6 +2370,190 @@ espl_status espl_get_classes(espl_lanes* h, espl_class_info* out, uint32_t cap, 
         else
             (void)cudaGetLastError();  // not launched yet: no time
     }
+    return ESPL_OK;
+}
+
+espl_status espl_set_plan(espl_lanes* h, const espl_plan_choice* choices) {
+    if (!h) return ESPL_INVALID_ARGUMENT;
+    for (size_t i = 0; choices && i < h->groups.size(); i++)
+        if (choices[i].tile > ESPL_TILE_WIDE || choices[i].stage > ESPL_STAGE_NONE)
+            return fail(h, ESPL_INVALID_ARGUMENT, "plan choice out of range");
+    for (size_t i = 0; i < h->groups.size(); i++) h->groups[i].choice = choices ? choices[i] : espl_plan_choice{};
+    espl_status s = h->precision == ESPL_MIXED ? plan_classes<true>(h) : plan_classes<false>(h);
+    if (s) return s;
+    return push_descs(h);
+}
+
+espl_status espl_get_plan(espl_lanes* h, espl_plan_choice* resolved) {
+    if (!h || !resolved) return ESPL_INVALID_ARGUMENT;
+    for (const LaunchClass& c : h->classes)
+        for (uint32_t gi : c.groups) {
+            const GroupDev& d = h->groups[gi].dev;
+            espl_plan_choice& o = resolved[gi];
+            o.tile = c.wide ? ESPL_TILE_WIDE : ESPL_TILE_NARROW;
+            o.per_sm = c.per_sm;
+            o.stage = d.stage_mode == kStageLu
+                          ? (d.rec_stage || !d.n_rec ? ESPL_STAGE_LU : ESPL_STAGE_LU_GLOBAL_RECORDS)
+                      : d.stage_mode == kStageIndex ? ESPL_STAGE_INDEX
+                                                    : ESPL_STAGE_NONE;
+            o.pad = 0;
+        }
+    return ESPL_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+bool same_choice(const espl_plan_choice& a, const espl_plan_choice& b) {
+    return a.tile == b.tile && a.stage == b.stage && a.per_sm == b.per_sm;
+}
+
+uint64_t fnv1a(uint64_t h, const void* p, size_t n) {
+    const unsigned char* b = static_cast<const unsigned char*>(p);
+    for (size_t i = 0; i < n; i++) {
+        h ^= b[i];
+        h *= 1099511628211ull;
+    }
+    return h;
+}
+
+// The autotuner's results for the process, by the hash of their inputs.
+struct TuneResult {
+    std::vector<espl_plan_choice> choices;
+    espl_tune_report report;
+};
+std::mutex g_tune_mu;
+std::vector<std::pair<uint64_t, TuneResult>> g_tune_cache;
+
+}  // namespace
+
+extern "C" {
+
+espl_status espl_autotune(const espl_netlist* nets, uint32_t n_nets, const espl_create_opts* opts, double dt0,
+                          const espl_tran_opts* tran, uint32_t trial_steps, uint32_t max_trials,
+                          espl_plan_choice* choices, espl_tune_report* report) {
+    if (!nets || !n_nets || !opts || !tran || !choices || !trial_steps) return ESPL_INVALID_ARGUMENT;
+    // the inputs' key: patterns, lane counts and device kinds of the
+    // templates, the options, and the device
+    uint64_t key = 14695981039346656037ull;
+    cudaDeviceProp prop{};
+    if (cudaGetDeviceProperties(&prop, (int)opts->device) != cudaSuccess) return ESPL_DRIVER;
+    key = fnv1a(key, prop.name, std::strlen(prop.name));
+    key = fnv1a(key, opts, sizeof(*opts));
+    key = fnv1a(key, &dt0, sizeof(dt0));
+    key = fnv1a(key, tran, sizeof(*tran));
+    key = fnv1a(key, &trial_steps, sizeof(trial_steps));
+    key = fnv1a(key, &max_trials, sizeof(max_trials));
+    for (uint32_t k = 0; k < n_nets; k++) {
+        const espl_netlist& n = nets[k];
+        key = fnv1a(key, &n.n, sizeof(n.n));
+        key = fnv1a(key, &n.nnz, sizeof(n.nnz));
+        key = fnv1a(key, &n.lanes, sizeof(n.lanes));
+        if (n.col_ptr) key = fnv1a(key, n.col_ptr, sizeof(uint32_t) * (n.n + 1));
+        if (n.row_idx) key = fnv1a(key, n.row_idx, sizeof(uint32_t) * n.nnz);
+        for (uint32_t b = 0; b < n.n_batches && n.batches; b++) {
+            key = fnv1a(key, &n.batches[b].kind, sizeof(uint32_t));
+            key = fnv1a(key, &n.batches[b].count, sizeof(uint32_t));
+        }
+    }
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        for (const auto& e : g_tune_cache)
+            if (e.first == key) {
+                std::copy(e.second.choices.begin(), e.second.choices.end(), choices);
+                if (report) {
+                    *report = e.second.report;
+                    report->cached = 1;
+                }
+                return ESPL_OK;
+            }
+    }
+    espl_tran_opts to = *tran;
+    to.predictor = std::min(to.predictor, 1u);  // trials have no network
+    uint32_t trials = 0;
+    // one timed transient of a plan: a scratch handle, its operating point
+    // and `trial_steps` attempts; the device time of that launch, and the
+    // plan it resolved to
+    auto trial = [&](const std::vector<espl_plan_choice>& ch, double& ms,
+                     std::vector<espl_plan_choice>& resolved) -> espl_status {
+        espl_lanes* t = nullptr;
+        espl_status s = espl_create(nets, n_nets, opts, dt0, &t);
+        if (s) return s;
+        if (!(s = espl_set_plan(t, ch.data())) && !(s = espl_init_steps(t, &to)) &&
+            !(s = espl_device_launch(t, trial_steps, nullptr))) {
+            espl_stats st{};
+            if (!(s = espl_get_stats(t, &st))) ms = st.newton_ms;
+            resolved.assign(n_nets, espl_plan_choice{});
+            if (!s) s = espl_get_plan(t, resolved.data());
+        }
+        espl_destroy(t);
+        trials++;
+        return s;
+    };
+    std::vector<espl_plan_choice> best(n_nets, espl_plan_choice{}), res;
+    double auto_ms = 0.0, best_ms = 0.0;
+    espl_status s;
+    // the automatic plan twice: the first run warms the process up
+    if ((s = trial(best, auto_ms, res)) || (s = trial(best, auto_ms, res))) return s;
+    best_ms = auto_ms;
+    std::vector<espl_plan_choice> best_res = res;
+    // launch classes of a resolved plan: templates by (tile, per_sm)
+    auto classes_of = [&](const std::vector<espl_plan_choice>& r) {
+        std::vector<std::vector<uint32_t>> out;
+        std::vector<std::pair<uint32_t, uint32_t>> keys;
+        for (uint32_t i = 0; i < n_nets; i++) {
+            const auto k = std::make_pair(r[i].tile, r[i].per_sm);
+            const size_t c = std::find(keys.begin(), keys.end(), k) - keys.begin();
+            if (c == keys.size()) {
+                keys.push_back(k);
+                out.emplace_back();
+            }
+            out[c].push_back(i);
+        }
+        return out;
+    };
+    bool improved = true;
+    while (improved && trials < max_trials) {
+        improved = false;
+        for (const auto& cls : classes_of(best_res)) {
+            const espl_plan_choice cur = best_res[cls[0]];
+            // the moves of this class: its staging, its tile width, one
+            // resident tile per SM fewer
+            std::vector<std::pair<int, uint32_t>> moves;  // (field, value)
+            if (cur.stage == ESPL_STAGE_LU) moves.push_back({0, ESPL_STAGE_LU_GLOBAL_RECORDS});
+            if (cur.stage != ESPL_STAGE_LU) moves.push_back({0, ESPL_STAGE_LU});
+            moves.push_back({1, cur.tile == ESPL_TILE_WIDE ? (uint32_t)ESPL_TILE_NARROW : (uint32_t)ESPL_TILE_WIDE});
+            if (cur.per_sm > 1) moves.push_back({2, cur.per_sm - 1});
+            for (const auto& mv : moves) {
+                if (trials >= max_trials) break;
+                std::vector<espl_plan_choice> ch = best;
+                for (uint32_t i : cls) {
+                    if (mv.first == 0) ch[i].stage = mv.second;
+                    if (mv.first == 1) ch[i].tile = mv.second;
+                    if (mv.first == 2) ch[i].per_sm = mv.second;
+                }
+                double ms = 0.0;
+                std::vector<espl_plan_choice> r;
+                if ((s = trial(ch, ms, r))) return s;
+                if (std::equal(r.begin(), r.end(), best_res.begin(), same_choice))
+                    continue;  // the move changed nothing (it did not fit)
+                if (ms < 0.98 * best_ms) {
+                    best = ch;
+                    best_ms = ms;
+                    best_res = r;
+                    improved = true;
+                    break;  // the classes may have regrouped: start over
+                }
+            }
+            if (improved) break;
+        }
+    }
+    std::copy(best.begin(), best.end(), choices);
+    const espl_tune_report rep{trials, 0, auto_ms, best_ms};
+    if (report) *report = rep;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_cache.push_back({key, TuneResult{best, rep}});
     return ESPL_OK;
 }
 

@@ -15,7 +15,8 @@ from typing import List, Optional, Sequence
 import numpy as np
 
 from . import abi
-from .abi import (ClassInfo, CreateOpts, MeasPass, LaneNewton, NetlistC, NewtonOpts, StepReport, Stats, TranOpts, f64p, u32p)
+from .abi import (ClassInfo, CreateOpts, MeasPass, LaneNewton, NetlistC, NewtonOpts, PlanChoice, StepReport, Stats,
+                  TranOpts, TuneReport, f64p, u32p)
 from .decks import Netlist
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -94,11 +95,37 @@ def lib():
         L.espl_set_step_predictor.restype = C.c_uint32
         L.espl_step_predict.argtypes = [C.c_void_p, C.c_uint32, f64p, f64p, f64p, f64p, f64p]
         L.espl_step_predict.restype = C.c_uint32
+        L.espl_set_plan.argtypes = [C.c_void_p, C.POINTER(PlanChoice)]
+        L.espl_set_plan.restype = C.c_uint32
+        L.espl_get_plan.argtypes = [C.c_void_p, C.POINTER(PlanChoice)]
+        L.espl_get_plan.restype = C.c_uint32
+        L.espl_autotune.argtypes = [C.POINTER(NetlistC), C.c_uint32, C.POINTER(CreateOpts), C.c_double,
+                                    C.POINTER(TranOpts), C.c_uint32, C.c_uint32, C.POINTER(PlanChoice),
+                                    C.POINTER(TuneReport)]
+        L.espl_autotune.restype = C.c_uint32
         _lib = L
     return _lib
 
 
 PRECISION = {"fp64": abi.ESPL_FP64, "mixed": abi.ESPL_MIXED}
+
+
+def autotune(nets: Sequence[Netlist], topts, precision: str = "fp64", dt0: float = 0.0, polish: int = 0,
+             refine_sweeps: int = 0, device: int = 0, trial_steps: int = 100, max_trials: int = 12):
+    """espl_autotune: the launch plan of `nets` for the transient `topts`,
+    searched by timing `trial_steps` attempts per plan on scratch handles.
+    Returns (choices, report): choices a list of PlanChoice for
+    Lanes.set_plan, report a dict (trials, cached, auto_ms, best_ms)."""
+    keep, arr = abi.cnets(list(nets))
+    opts = CreateOpts(abi.ABI_VERSION, PRECISION[precision], device, 0, refine_sweeps, polish)
+    out = (PlanChoice * len(nets))()
+    rep = TuneReport()
+    st = lib().espl_autotune(arr, len(nets), C.byref(opts), dt0, C.byref(topts), trial_steps, max_trials, out,
+                             C.byref(rep))
+    del keep
+    if st != 0:
+        raise LaneError(f"espl_autotune failed with status {st}")
+    return list(out), dict(trials=rep.trials, cached=rep.cached, auto_ms=rep.auto_ms, best_ms=rep.best_ms)
 
 
 def meas_table(passes: Sequence[MeasPass], xs, cols):
@@ -391,6 +418,20 @@ class Lanes:
         self._check(lib().espl_get_classes(self.h, out, n.value, C.byref(n)), "espl_get_classes")
         return [dict(tiles=c.tiles, wide=bool(c.wide), per_sm=c.per_sm, smem_bytes=c.smem_bytes, ms=c.last_ms)
                 for c in out[:n.value]]
+
+    def set_plan(self, choices=None):
+        """Re-plans the launches (espl_set_plan): one PlanChoice per
+        template, or None for the automatic plan."""
+        arr = None
+        if choices is not None:
+            arr = (PlanChoice * len(self.nets))(*choices)
+        self._check(lib().espl_set_plan(self.h, arr), "espl_set_plan")
+
+    def plan(self) -> List[dict]:
+        """The plan in effect, per template (espl_get_plan)."""
+        out = (PlanChoice * len(self.nets))()
+        self._check(lib().espl_get_plan(self.h, out), "espl_get_plan")
+        return [dict(tile=c.tile, stage=c.stage, per_sm=c.per_sm) for c in out]
 
     def stats(self) -> Stats:
         s = Stats()

@@ -396,6 +396,64 @@ typedef struct {
 } espl_class_info;
 espl_status espl_get_classes(espl_lanes *h, espl_class_info *out, uint32_t cap, uint32_t *count);
 
+/* ---- The launch plan and its autotuner ----
+ *
+ * How a template's lanes run: in tiles of 4 warps (narrow) or 16 (wide),
+ * with what staged in the tile's shared memory, and how many tiles share an
+ * SM. espl_create picks these per template from the CUDA occupancy
+ * calculator and a makespan rule (the automatic plan; the counterpart of
+ * the reference driver's fixed lane-layout choice, src/analysis/gpu/
+ * lanes.zig:92-98); espl_set_plan overrides them, and espl_autotune searches
+ * them by timing short transients. No reference counterpart for the search. */
+enum { ESPL_TILE_AUTO = 0, ESPL_TILE_NARROW = 1, ESPL_TILE_WIDE = 2 };
+enum {
+    ESPL_STAGE_AUTO = 0,
+    ESPL_STAGE_LU = 1,                 /* index words, LU chain and its 16-byte records */
+    ESPL_STAGE_LU_GLOBAL_RECORDS = 2,  /* index words and LU chain; records read from global memory */
+    ESPL_STAGE_INDEX = 3,              /* the template's index words only */
+    ESPL_STAGE_NONE = 4                /* nothing staged */
+};
+typedef struct {
+    uint32_t tile;    /* ESPL_TILE_*; templates whose LU needs wide tiles (the
+                       * banded replay, the CTA-wide LU) stay wide */
+    uint32_t stage;   /* ESPL_STAGE_*; a choice that does not fit the shared
+                       * memory falls back to the automatic order */
+    uint32_t per_sm;  /* 0: as many resident tiles per SM as fit; k: at most k
+                       * (the tile's shared memory grows to keep it so) */
+    uint32_t pad;
+} espl_plan_choice;
+
+/* Re-plans the launches with one choice per template (n_nets entries; NULL:
+ * all automatic). Lanes' state is kept. */
+espl_status espl_set_plan(espl_lanes *h, const espl_plan_choice *choices);
+/* The plan in effect, one entry per template, every field resolved (no AUTO
+ * values; per_sm the resident tiles per SM of its launch class). */
+espl_status espl_get_plan(espl_lanes *h, espl_plan_choice *resolved);
+
+typedef struct {
+    uint32_t trials;  /* transients timed */
+    uint32_t cached;  /* 1: the plan came from the process's cache, no trial ran */
+    double auto_ms;   /* the automatic plan's trial time, milliseconds */
+    double best_ms;   /* the returned plan's */
+} espl_tune_report;
+
+/* Searches the launch plan of templates `nets` for the transient `tran`:
+ * from the automatic plan, moves that change one launch class's templates at
+ * a time (records staged or read from global memory, narrow or wide tiles,
+ * one resident tile per SM fewer) are each timed on a scratch handle
+ * created with `opts` and `dt0` (the operating point, then `trial_steps`
+ * transient attempts of every lane; the device time of that launch), and a
+ * move is kept when it is at least 2 % faster; at most `max_trials`
+ * transients (the automatic plan's two runs included: the first warms the
+ * process up). `choices` (n_nets entries) gets the best plan for
+ * espl_set_plan. The result is cached for the process by the templates'
+ * patterns, lane counts and device kinds, the device and the options: a
+ * second call with the same inputs runs nothing. A learned predictor
+ * (tran->predictor 2) is timed as the linear one. */
+espl_status espl_autotune(const espl_netlist *nets, uint32_t n_nets, const espl_create_opts *opts, double dt0,
+                          const espl_tran_opts *tran, uint32_t trial_steps, uint32_t max_trials,
+                          espl_plan_choice *choices, espl_tune_report *report);
+
 /* Host-only symbolic seam, no GPU needed. `espl_order` is order.zig's
  * `order` (src/solver/order.zig:78): q[k] = the column factored at step k,
  * BTF sink block first, AMD or natural per block. ESPL_NO_TAPE on
