@@ -155,7 +155,7 @@ def algorithmic_bytes(nets, lane_iterations_per_net, s_lu: int):
 POLISH = 6
 
 
-def run_ring_sweep(nets, topts, precision, learned=None):
+def run_ring_sweep(nets, topts, precision, learned=None, plan=None):
     """One full sweep through the C ABI from host buffers: create (uploads
     every lane's parameters), operating point, every transient step, final
     states and periods back. With `learned` (a dict: warm, stride, cap,
@@ -164,12 +164,15 @@ def run_ring_sweep(nets, topts, precision, learned=None):
     stride-th lane, a step predictor is trained on the device, and the rest
     of its transient starts each attempt from the network. Time: the CUDA-
     event time of the Newton launches plus that of the training (both device
-    time; allocations, as in every arm, outside it)."""
+    time; allocations, as in every arm, outside it). `plan`: the launch
+    plan (espl_set_plan choices) the sweep runs with."""
     import copy
     from egspice_b200.lanes import Lanes
     from egspice_b200.learned import Mlp, step_predictor_dims, train_opts
     t0 = time.perf_counter()
     L = Lanes(nets, precision=precision, dt0=topts.dt, polish=POLISH)
+    if plan is not None:
+        L.set_plan(plan)
     for i, net in enumerate(nets):
         L.set_period_meas(i, net.node("s1"), 0.9, 1e-9)
     o = copy.copy(topts)
@@ -587,6 +590,9 @@ def main():
     ap.add_argument("--no-configs", action="store_true", help="skip the runs of configs 1-3")
     ap.add_argument("--config3-steps", type=int, default=100, help="steps of the config-3 mesh run (of 1,000)")
     # the learned arm's step predictor
+    ap.add_argument("--no-autotune", action="store_true", help="run the automatic launch plan, no search")
+    ap.add_argument("--tune-steps", type=int, default=200, help="transient attempts per autotuner trial")
+    ap.add_argument("--tune-trials", type=int, default=10, help="autotuner trials per precision")
     ap.add_argument("--learn-warm", type=int, default=500, help="attempts with the linear predictor and recorder")
     ap.add_argument("--learn-stride", type=int, default=32, help="the recorder samples every stride-th bulk lane")
     ap.add_argument("--learn-epochs", type=int, default=5)
@@ -664,6 +670,23 @@ def main():
     learn = dict(warm=args.learn_warm, stride=args.learn_stride,
                  cap=(args.lanes // args.learn_stride + 1) * args.learn_warm, epochs=args.learn_epochs,
                  batch=args.learn_batch, lr=args.learn_lr, lr_final=args.learn_lr / 10)
+    # the launch plan of each precision, searched by timing short
+    # transients (espl_autotune), before any arm; once per process
+    plans, tuned = {}, {}
+    for prec in dict.fromkeys("fp64" if m == "fp64" else "mixed" for m in modes):
+        if args.no_autotune:
+            plans[prec] = None
+            continue
+        from egspice_b200.lanes import autotune
+        tt = time.perf_counter()
+        plans[prec], rep = autotune(nets, topts, precision=prec, dt0=topts.dt, polish=POLISH,
+                                    trial_steps=args.tune_steps, max_trials=args.tune_trials)
+        rep["wall_s"] = time.perf_counter() - tt
+        rep["trial_steps"] = args.tune_steps
+        rep["plan"] = [[c.tile, c.stage, c.per_sm] for c in plans[prec]]
+        rep["plan_fields"] = "per template: tile (0 auto, 1 narrow, 2 wide), stage (0 auto, 1 LU chain and records, " \
+                             "2 LU chain, records global, 3 index words, 4 none), resident tiles per SM cap (0 none)"
+        tuned[prec] = rep
     results = {}
     for k, mode in enumerate(modes):
         prec = "fp64" if mode == "fp64" else "mixed"
@@ -671,13 +694,13 @@ def main():
         # W warm-up sweeps before the first arm; later arms (the same
         # kernels, the device already warm) one each
         for _ in range(args.warmup if k == 0 else min(args.warmup, 1)):
-            run_ring_sweep(nets, topts, prec, lk)
+            run_ring_sweep(nets, topts, prec, lk, plans[prec])
         runs = []
         barrier()
         with ClockSampler(dev) as clk:
             for _ in range(args.steps):
                 barrier()
-                runs.append(run_ring_sweep(nets, topts, prec, lk))
+                runs.append(run_ring_sweep(nets, topts, prec, lk, plans[prec]))
                 barrier()
         r = runs[-1]
         dmax = max(x["dev_s"] for x in runs)
@@ -760,6 +783,7 @@ def main():
                       mixed_over_fp64=(plain["dev_s"] / results["mixed"]["dev_s"])
                       if (plain and "mixed" in results) else None,
                       learned_predictor=head == "learned",
+                      autotune=tuned or None,
                       oracle_check={"lanes": "all" if args.check == "all" else "2 per template",
                                     "polish": POLISH, "seconds": check_s} if errs else None),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
