@@ -338,6 +338,8 @@ def run_learned_dc(points: int = 65536, train_points: int = 8192, epochs: int = 
                                                                       lr_final=1e-4))
         t_train = time.perf_counter() - t0
         guess = m.predict(net.sweep[train_points:])
+        predict_dev = m.predict_ms()
+        train_dev = m.train_ms()
     t_mlp = time.perf_counter() - t0
     # from a learned start Newton gets three times the plain mean iteration
     # count; a lane that has not converged by then restarts from the nominal
@@ -367,7 +369,8 @@ def run_learned_dc(points: int = 65536, train_points: int = 8192, epochs: int = 
                         "fp64_refactor_fallbacks": int(r_mixed[:, 2].sum())},
         "learned_mixed": {"points_per_s": points / t_learned, "ms": t_learned * 1e3,
                           "newton_ms": dev_head + dev_tail, "mlp_train_ms": t_train * 1e3,
-                          "mlp_predict_ms": (t_mlp - t_train) * 1e3, "train_points": train_points,
+                          "mlp_predict_ms": (t_mlp - t_train) * 1e3,
+                          "mlp_predict_device_ms": predict_dev, "mlp_train_device_ms": train_dev, "train_points": train_points,
                           "epochs": epochs, "batch": batch, "lr": lr, "final_loss": float(losses[-1]),
                           "mean_newton_iters_predicted": float(r_tail[:, 1].mean()),
                           "mean_newton_iters_all": float(r_learned[:, 1].mean()), "converged": conv(r_learned),

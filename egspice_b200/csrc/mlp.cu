@@ -276,6 +276,10 @@ struct espl_mlp {
     int* err = nullptr;
     long long adam_t = 0;
     double last_train_ms = 0.0;  // device time of the last training (events on the stream)
+    double last_predict_ms = 0.0;  // device time of the last espl_mlp_predict (copies and kernel)
+    // espl_mlp_predict's device buffers, grown on demand and kept until destroy
+    double *pred_x = nullptr, *pred_y = nullptr;
+    size_t pred_rows = 0;
     cudaStream_t stream = nullptr;
     std::vector<void*> owned;
     std::string msg;
@@ -592,6 +596,8 @@ espl_status espl_mlp_destroy(espl_mlp* h) {
     if (!h) return ESPL_OK;
     if (h->stream) cudaStreamSynchronize(h->stream);
     for (void* q : h->owned) cudaFree(q);
+    cudaFree(h->pred_x);
+    cudaFree(h->pred_y);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return ESPL_OK;
@@ -821,19 +827,33 @@ espl_status espl_mlp_predict(espl_mlp* h, const double* x, uint32_t n, double* y
     if (!h || !x || !y) return ESPL_INVALID_ARGUMENT;
     if (n == 0) return ESPL_OK;
     // One fused launch (k_mlp_infer): each CTA runs the whole network on 128
-    // rows with the weights and activations in shared memory.
-    double *dx = nullptr, *dy = nullptr;
-    MCK(cudaMalloc(&dx, sizeof(double) * (size_t)n * h->D));
-    if (cudaMalloc(&dy, sizeof(double) * (size_t)n * h->O) != cudaSuccess) {
-        cudaFree(dx);
-        h->msg = "out of device memory for the predictions";
-        return ESPL_OUT_OF_MEMORY;
+    // rows with the weights and activations in shared memory. The rows'
+    // device buffers are the handle's, grown when a call needs more.
+    if (n > h->pred_rows) {
+        MCK(cudaStreamSynchronize(h->stream));
+        cudaFree(h->pred_x);
+        cudaFree(h->pred_y);
+        h->pred_x = h->pred_y = nullptr;
+        h->pred_rows = 0;
+        if (cudaMalloc(&h->pred_x, sizeof(double) * (size_t)n * h->D) != cudaSuccess ||
+            cudaMalloc(&h->pred_y, sizeof(double) * (size_t)n * h->O) != cudaSuccess) {
+            cudaFree(h->pred_x);
+            h->pred_x = nullptr;
+            h->msg = "out of device memory for the predictions";
+            return ESPL_OUT_OF_MEMORY;
+        }
+        h->pred_rows = n;
     }
+    double *dx = h->pred_x, *dy = h->pred_y;
     espl_status s = ESPL_OK;
     const size_t smem = infer_smem_bytes(h->Dp, h->Op);
     InferArgs g{dx, dy, h->p + h->off_w1, h->p + h->off_b1, h->p + h->off_w2, h->p + h->off_b2, h->p + h->off_w3,
                 h->p + h->off_b3, h->in_mean, h->in_std, h->out_mean, h->out_std, (int)n, h->D, h->Dp, h->O, h->Op,
                 h->err};
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEventCreate(&ev0);
+    cudaEventCreate(&ev1);
+    cudaEventRecord(ev0, h->stream);
     if (cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
         cudaMemcpyAsync(dx, x, sizeof(double) * (size_t)n * h->D, cudaMemcpyHostToDevice, h->stream) != cudaSuccess) {
         s = ESPL_DRIVER;
@@ -844,9 +864,12 @@ espl_status espl_mlp_predict(espl_mlp* h, const double* x, uint32_t n, double* y
                 cudaSuccess)
             s = ESPL_DRIVER;
     }
+    cudaEventRecord(ev1, h->stream);
     cudaStreamSynchronize(h->stream);
-    cudaFree(dx);
-    cudaFree(dy);
+    float ms = 0.0f;
+    if (!s && cudaEventElapsedTime(&ms, ev0, ev1) == cudaSuccess) h->last_predict_ms = ms;
+    cudaEventDestroy(ev0);
+    cudaEventDestroy(ev1);
     if (s) {
         h->msg = "predict launch failed";
         return s;
@@ -878,6 +901,12 @@ espl_status espl_mlp_predict_layers(espl_mlp* h, const double* x, uint32_t n, do
 espl_status espl_mlp_train_ms(const espl_mlp* h, double* device_ms) {
     if (!h || !device_ms) return ESPL_INVALID_ARGUMENT;
     *device_ms = h->last_train_ms;
+    return ESPL_OK;
+}
+
+espl_status espl_mlp_predict_ms(const espl_mlp* h, double* device_ms) {
+    if (!h || !device_ms) return ESPL_INVALID_ARGUMENT;
+    *device_ms = h->last_predict_ms;
     return ESPL_OK;
 }
 

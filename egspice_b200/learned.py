@@ -50,11 +50,12 @@ def _setup(L):
     L.espl_mlp_train.argtypes = [C.c_void_p, f64p, f64p, C.c_uint32, C.POINTER(TrainOpts), f64p]
     L.espl_mlp_train_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(TrainOpts), f64p]
     L.espl_mlp_train_ms.argtypes = [C.c_void_p, f64p]
+    L.espl_mlp_predict_ms.argtypes = [C.c_void_p, f64p]
     L.espl_mlp_predict.argtypes = [C.c_void_p, f64p, C.c_uint32, f64p]
     L.espl_mlp_predict_layers.argtypes = [C.c_void_p, f64p, C.c_uint32, f64p]
     L.espl_mlp_error_message.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t]
     for f in ("create", "destroy", "param_count", "get_params", "set_params", "set_scaling", "loss_grad", "train",
-              "train_device", "train_ms", "predict", "predict_layers", "error_message"):
+              "train_device", "train_ms", "predict_ms", "predict", "predict_layers", "error_message"):
         getattr(L, "espl_mlp_" + f).restype = C.c_uint32
     L._mlp_ready = True
     return L
@@ -138,6 +139,12 @@ class Mlp:
         """Device time of the last training (espl_mlp_train_ms)."""
         ms = C.c_double()
         self._check(self.L.espl_mlp_train_ms(self.h, C.byref(ms)), "train_ms")
+        return ms.value
+
+    def predict_ms(self) -> float:
+        """Device time of the last fused prediction (espl_mlp_predict_ms)."""
+        ms = C.c_double()
+        self._check(self.L.espl_mlp_predict_ms(self.h, C.byref(ms)), "predict_ms")
         return ms.value
 
     def predict(self, x, fused: bool = True) -> np.ndarray:

@@ -77,6 +77,9 @@ espl_status espl_mlp_train_device(espl_mlp *m, const double *x, const double *y,
  * stream around its standardization and Adam steps; allocations and host
  * copies excluded), milliseconds. */
 espl_status espl_mlp_train_ms(const espl_mlp *m, double *device_ms);
+/* Device time of the last espl_mlp_predict (CUDA events on the network's
+ * stream around its copies and its launch), milliseconds. */
+espl_status espl_mlp_predict_ms(const espl_mlp *m, double *device_ms);
 
 /* Predictions for n rows (any n): one fused inference launch, each CTA
  * running the whole network on 128 rows from shared memory and tensor
