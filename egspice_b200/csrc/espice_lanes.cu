@@ -818,6 +818,13 @@ espl_status plan_classes(espl_lanes* h) {
         // peel's size, the whole CTA runs the LU by levels (lane_levels.cuh)
         g.dev.big = (g.dev.stage_mode != kStageLu && !g.dev.band_ok && g.dev.n_fl > 0) ? 1u : 0u;
         if (g.dev.big) bytes[i] = ((bytes[i] + 15u) & ~15u) + kBigScratch;
+        if (g.dev.big && !g.dev.wk) {
+            // the refactor's column groups past the first: work vectors of their own
+            espl_status s2;
+            const size_t words = (size_t)(kRefGroups - 1) * (g.n + 1) * g.P;
+            if ((s2 = dalloc(h, g.lu_owned, &g.dev.wk, words))) return s2;
+            if (MIXED && (s2 = dalloc(h, g.lu_owned, &g.dev.wk32, words))) return s2;
+        }
         // the solves stream the factor through a ring of shared memory where
         // it fits beside the rest
         g.dev.stream = nullptr;
@@ -1022,6 +1029,10 @@ espl_status upload_tape(espl_lanes* h, Group& g) {
         g.sd_ok = false;
         GroupDev& d = g.dev;
         d.stream = nullptr;
+        d.wk = nullptr;
+        d.wk32 = nullptr;
+        d.cl_ptr = d.cl_gp = d.cl_cols = nullptr;
+        d.n_cl = 0;
         d.nnz_l = (uint32_t)g.tape.li.size();
         d.nnz_u = (uint32_t)g.tape.ui.size();
         d.n_void = (uint32_t)g.tape.void_slots.size();
@@ -1088,6 +1099,13 @@ espl_status upload_tape(espl_lanes* h, Group& g) {
             UP(rl_ent, lp.rl_ent);
             UP(ru_ptr, lp.ru_ptr);
             UP(ru_ent, lp.ru_ent);
+            // the refactor's column levels and groups
+            ColPlan cp;
+            col_plan(g.tape, kRefGroups, cp);
+            d.n_cl = (uint32_t)cp.lv_ptr.size() - 1;
+            UP(cl_ptr, cp.lv_ptr);
+            UP(cl_gp, cp.gp);
+            UP(cl_cols, cp.cols);
             // the same sweeps in streaming order, chunks of a ring slot
             StreamPlan fw, bw;
             if (stream_plan(lp.fl_ptr, lp.fl_rows, lp.rl_ptr, lp.rl_ent, kRingChunk, kRingRows, kRingSlots, true, fw) &&

@@ -36,6 +36,7 @@ constexpr double kWide = 1.0 / 1e-3;   // LaneTab.wide = 1 / pivot_tol
 // dense peel covers up to 256, within a scratch budget (alloc_group).
 constexpr uint32_t kDensePeelMax = 256;
 constexpr uint32_t kFactKeys = 6;  // GroupDev fact_key words per lane
+constexpr uint32_t kRefGroups = 8;  // column groups of a large template's refactor
 
 // Gate bits (kernels/lane.zig:708-711).
 constexpr uint32_t kActive = 1, kInitFix = 2, kConverged = 4, kSingular = 8, kPassed = 16, kParked = 32;
@@ -137,6 +138,13 @@ struct GroupDev {
     uint32_t n_fl, n_bl, big, linear;
     double* fact_key;
     const struct StreamDev* stream;  // the sweeps in streaming order (lane_levels.cuh), or null
+    // The refactor's column levels (tape.h ColPlan; n_cl levels) and the
+    // work vectors of the column groups past the first (kRefGroups - 1
+    // copies of w, (n + 1) x P each; FP32 copies for a mixed handle), or null
+    const uint32_t *cl_ptr, *cl_gp, *cl_cols;
+    uint32_t n_cl, cl_pad;
+    double* wk;
+    float* wk32;
 };
 
 // One sweep of a large template's solve in streaming order (tape.h

@@ -84,12 +84,15 @@ constexpr uint32_t kLimited = 1, kImplausible = 2, kResidualMiss = 4;
 
 // The CTA-wide LU of a large template (lane_levels.cuh) needs, past the
 // tile's staged arrays in dynamic shared memory, the refactor's per-lane
-// reductions, the lanes' flags and the ring's barriers (a 2 KB header), the
+// reductions, the lanes' flags and the ring's barriers (a 4 KB header), the
 // solves' partial sums (one double per thread) and, with a streaming plan
 // (GroupDev stream), the ring's slots (kBigRingBytes).
-constexpr uint32_t kBigScratch = 2048 + kWideThreads * 8;
-constexpr uint32_t kBigRingOff = 1536;
+constexpr uint32_t kBigScratch = 4096 + kWideThreads * 8;
+constexpr uint32_t kBigRingOff = 3584;
 constexpr uint32_t kBigRingBytes = ring_bytes(kBigLanes);
+// The refactor runs while no chunk is staged: its window of work-vector rows
+// (lvl_refactor) takes the ring's shared memory.
+constexpr uint32_t kRingSpan = kBigRingBytes;
 // (lvl_sweep_ring adds a row's hardware warps' sums inside one warp)
 static_assert(kWideThreads / 32 * kBigLanes <= 32, "a row's warp sums fit one warp");
 // (and gathers a chunk's rows' own values, one row per logical warp)
@@ -118,10 +121,10 @@ __device__ void big_lu(const GroupDev& d, const TileCtx& c, bool act, LaneState*
     const uint32_t lane = c.lane, warp = c.warp, nw = c.nw, l = c.l, P = d.P;
     LevelShared& ls = *reinterpret_cast<LevelShared*>(scratch);
     BigLaneFlags& bf = *reinterpret_cast<BigLaneFlags*>(scratch + sizeof(LevelShared));
-    void* red = scratch + 2048;
+    void* red = scratch + 4096;
     static_assert(sizeof(LevelShared) + sizeof(BigLaneFlags) <= kBigRingOff &&
-                      kBigRingOff + sizeof(RingShared) <= 2048,
-                  "the scratch header fits 2 KB");
+                      kBigRingOff + sizeof(RingShared) <= 4096,
+                  "the scratch header fits 4 KB");
     RingShared* ring = d.stream ? reinterpret_cast<RingShared*>(scratch + kBigRingOff) : nullptr;
     unsigned char* slots = scratch + kBigScratch;
     auto key_ok = [&](uint32_t kb) {
@@ -137,7 +140,9 @@ __device__ void big_lu(const GroupDev& d, const TileCtx& c, bool act, LaneState*
     if (MIXED) {
         const bool go = bf.need[lane] && bf.use32[lane];
         if (__syncthreads_or(go)) {
-            const int rc = lvl_refactor<float>(d, l, lane, warp, nw, go, d.w32, d.lx32, d.ux32, d.udiag32, ls);
+            const int rc = lvl_refactor<float>(d, l, lane, warp, nw, go, d.w32, d.wk32, d.lx32, d.ux32, d.udiag32, ls,
+                                               d.stream ? reinterpret_cast<float*>(slots) : nullptr,
+                                               kRingSpan / (kBigLanes * 4u));
             if (warp == 0 && go) {
                 if (rc != 0) {
                     // the FP32 factor fails: this lane refactors in FP64 from here on
@@ -159,7 +164,9 @@ __device__ void big_lu(const GroupDev& d, const TileCtx& c, bool act, LaneState*
     {
         const bool go = bf.need[lane] && !bf.use32[lane];
         if (__syncthreads_or(go)) {
-            const int rc = lvl_refactor<double>(d, l, lane, warp, nw, go, d.w, d.lx, d.ux, d.udiag, ls);
+            const int rc = lvl_refactor<double>(d, l, lane, warp, nw, go, d.w, d.wk, d.lx, d.ux, d.udiag, ls,
+                                                d.stream ? reinterpret_cast<double*>(slots) : nullptr,
+                                                kRingSpan / (kBigLanes * 8u));
             if (warp == 0 && go) {
                 const bool ok = rc == 0 || (rc == 2 && replay_holds64(d, l));
                 bf.ok[lane] = ok ? 1u : 0u;

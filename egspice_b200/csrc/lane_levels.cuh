@@ -37,9 +37,15 @@ namespace espl {
 struct LevelShared {
     uint32_t bad[32];              // a dead pivot, growth failure or filled void slot
     uint32_t nonfinite[32];        // OR of (u - u) bits: a NaN somewhere
-    unsigned long long cmax[32];   // the column's largest |L| numerator (by bits)
     unsigned long long worst[32];  // the largest |L| over non-scaled columns (by bits)
+    unsigned long long cmax[kRefGroups][32];  // each group's column's largest |L| numerator (by bits)
 };
+
+// A barrier of the threads of one column group (ids 1 .. kRefGroups; 0 is
+// __syncthreads's).
+__device__ __forceinline__ void group_sync(uint32_t id, uint32_t threads) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
+}
 
 // The ring of a streaming sweep (StreamDev): kRingSlots chunks staged by
 // bulk copies (cp.async.bulk, the TMA's 1-D form), each completing on the
@@ -111,13 +117,31 @@ __device__ __forceinline__ T row_dot(const uint2* __restrict__ e2, uint32_t e0, 
 // 1 / pivot_tol) for every thread of the lane. `act`: the lane refactors;
 // lanes that do not leave their factor as it is. All threads of the CTA call
 // it.
+//
+// The columns run by levels (GroupDev cl_*): a level's columns read only the
+// L of earlier levels, so its G groups of the CTA's threads (G up to
+// kRefGroups) each factor their own columns at once, group g in work vector
+// g (w, then wk), with barriers of the group between a column's steps and a
+// CTA barrier between levels. A column's steps are those of the one-thread
+// replay (src/solver/kernels/lane.zig:56-125): its scatter, its U entries in
+// the tape's topological order (each entry's axpy of an L column split over
+// the group, a barrier between entries), the pivot with its L entries
+// split over the group; each row's updates come in the same order, so the
+// factor is the same to the bit whatever the grouping.
 template <typename T>
 __device__ int lvl_refactor(const GroupDev& d, uint32_t l, uint32_t lane, uint32_t warp, uint32_t nw, bool act,
-                            T* __restrict__ w, T* __restrict__ lx, T* __restrict__ ux, T* __restrict__ ud,
-                            LevelShared& ls) {
-    const uint32_t P = d.P;
+                            T* __restrict__ w, T* __restrict__ wk, T* __restrict__ lx, T* __restrict__ ux,
+                            T* __restrict__ ud, LevelShared& ls, T* win = nullptr, uint32_t win_rows = 0) {
+    const uint32_t P = d.P, tw = blockDim.x / nw;
     const double* __restrict__ a = d.a;
     constexpr bool F32 = sizeof(T) == 4;
+    // Group 0's work vector keeps its last win_rows rows (the trailing
+    // pivots: the top separators' dense chain of columns, which reads and
+    // updates them step after step) in shared memory. Like w, the window is
+    // zero between columns; it starts zeroed here.
+    const uint32_t t0 = win && win_rows < d.n ? d.n - win_rows : (win ? 0u : d.n);
+    if (win)
+        for (uint32_t r = t0 + warp; r < d.n; r += nw) win[(r - t0) * tw + lane] = (T)0;
     if (warp == 0) {
         uint32_t bad = 0;
         if (act)
@@ -125,91 +149,135 @@ __device__ int lvl_refactor(const GroupDev& d, uint32_t l, uint32_t lane, uint32
                 if (LM(a, d.void_slots[v]) != 0.0) bad = 1;
         ls.bad[lane] = bad;
         ls.nonfinite[lane] = 0;
-        ls.cmax[lane] = 0;
         ls.worst[lane] = 0;
+        for (uint32_t g = 0; g < kRefGroups; g++) ls.cmax[g][lane] = 0;
     }
     __syncthreads();
-    for (uint32_t k = 0; k < d.n; k++) {
-        const uint32_t c = d.q[k];
-        if (act)
-            for (uint32_t p = d.col_ptr[c] + warp; p < d.col_ptr[c + 1]; p += nw) LM(w, d.prow[p]) = (T)LM(a, p);
-        __syncthreads();
-        const uint32_t u0 = d.up[k], u1 = d.up[k + 1];
-        for (uint32_t p = u0; p < u1; p++) {
-            const uint32_t i = d.ui[p];
-            const T u = act ? LM(w, i) : (T)0;
-            if (act) {
-                for (uint32_t pl = d.lp[i] + warp; pl < d.lp[i + 1]; pl += nw) LM(w, d.li[pl]) -= LM(lx, pl) * u;
-                if (warp == 0) {
-                    LM(ux, p) = u;
-                    ls.nonfinite[lane] |= (uint32_t)(mag_bits(u - u) != 0);
+    for (uint32_t lv = 0; lv < d.n_cl; lv++) {
+        const uint32_t b = d.cl_ptr[lv], G = d.cl_ptr[lv + 1] - b - 1;
+        const uint32_t gsize = nw / G, g = warp / gsize, gw = warp % gsize;
+        const uint32_t bid = 1 + g, bthreads = blockDim.x / G;
+        T* __restrict__ wg = g == 0 ? w : wk + (size_t)(g - 1) * (d.n + 1) * P;
+        const uint32_t tg = g == 0 ? t0 : d.n;
+        // row r of the group's work vector
+        auto W = [&](uint32_t r) -> T& { return r >= tg ? win[(r - tg) * tw + lane] : LM(wg, r); };
+        unsigned long long& cmax = ls.cmax[g][lane];
+        const uint32_t c0 = d.cl_gp[b + g], c1 = d.cl_gp[b + g + 1];
+        for (uint32_t cc = c0; cc < c1; cc++) {
+            const uint32_t k = d.cl_cols[cc];
+            const uint32_t c = d.q[k];
+            if (act)
+                for (uint32_t p = d.col_ptr[c] + gw; p < d.col_ptr[c + 1]; p += gsize) W(d.prow[p]) = (T)LM(a, p);
+            group_sync(bid, bthreads);
+            const uint32_t u0 = d.up[k], u1 = d.up[k + 1];
+            // The next U entry's row, L column bounds and the first kPre
+            // entries of this thread's share of its L column (values and
+            // rows) are loaded while the current entry's axpy runs: none of
+            // them depends on the work vector.
+            constexpr uint32_t kPre = 4;
+            T pv[kPre];
+            uint32_t pr[kPre], pi = 0, pe0 = 0, pe1 = 0;
+            auto preload = [&](uint32_t p) {
+                pi = d.ui[p];
+                pe0 = d.lp[pi] + gw;
+                pe1 = d.lp[pi + 1];
+#pragma unroll
+                for (uint32_t r = 0; r < kPre; r++) {
+                    const uint32_t pl = pe0 + r * gsize;
+                    const bool ok = act && pl < pe1;
+                    pv[r] = ok ? LM(lx, pl) : (T)0;
+                    pr[r] = ok ? d.li[pl] : 0u;
                 }
+            };
+            if (u0 < u1) preload(u0);
+            for (uint32_t p = u0; p < u1; p++) {
+                const uint32_t i = pi, e0 = pe0, e1 = pe1;
+                T cv[kPre];
+                uint32_t cr[kPre];
+#pragma unroll
+                for (uint32_t r = 0; r < kPre; r++) {
+                    cv[r] = pv[r];
+                    cr[r] = pr[r];
+                }
+                if (p + 1 < u1) preload(p + 1);
+                const T u = act ? W(i) : (T)0;
+                if (act) {
+#pragma unroll
+                    for (uint32_t r = 0; r < kPre; r++)
+                        if (e0 + r * gsize < e1) W(cr[r]) -= cv[r] * u;
+                    for (uint32_t pl = e0 + kPre * gsize; pl < e1; pl += gsize) W(d.li[pl]) -= LM(lx, pl) * u;
+                    if (gw == 0) {
+                        LM(ux, p) = u;
+                        if (mag_bits(u - u) != 0) atomicOr(&ls.nonfinite[lane], 1u);
+                    }
+                }
+                group_sync(bid, bthreads);
             }
-            __syncthreads();
-        }
-        // the taken rows of the work vector (each U entry's row) go back to zero
-        if (act)
-            for (uint32_t p = u0 + warp; p < u1; p += nw) LM(w, d.ui[p]) = (T)0;
-        const uint32_t fl = d.flags[k];
-        if (fl & 1u) {
-            // a void column: unit pivot, no L entries, and every row its
-            // takes filled is cleared
-            if (act) {
-                for (uint32_t p = d.lp[k] + warp; p < d.lp[k + 1]; p += nw) {
-                    LM(lx, p) = (T)0;
-                    LM(w, d.li[p]) = (T)0;
+            // the taken rows of the work vector (each U entry's row) go back to zero
+            if (act)
+                for (uint32_t p = u0 + gw; p < u1; p += gsize) W(d.ui[p]) = (T)0;
+            const uint32_t fl = d.flags[k];
+            if (fl & 1u) {
+                // a void column: unit pivot, no L entries, and every row its
+                // takes filled is cleared
+                if (act) {
+                    for (uint32_t p = d.lp[k] + gw; p < d.lp[k + 1]; p += gsize) {
+                        LM(lx, p) = (T)0;
+                        W(d.li[p]) = (T)0;
+                    }
+                    for (uint32_t p = u0; p < u1; p++) {
+                        const uint32_t i = d.ui[p];
+                        for (uint32_t pl = d.lp[i] + gw; pl < d.lp[i + 1]; pl += gsize) W(d.li[pl]) = (T)0;
+                    }
+                    if (gw == 0) {
+                        LM(ud, k) = (T)1;
+                        W(k) = (T)0;
+                    }
                 }
-                for (uint32_t p = u0; p < u1; p++) {
-                    const uint32_t i = d.ui[p];
-                    for (uint32_t pl = d.lp[i] + warp; pl < d.lp[i + 1]; pl += nw) LM(w, d.li[pl]) = (T)0;
-                }
-                if (warp == 0) {
-                    LM(ud, k) = (T)1;
-                    LM(w, k) = (T)0;
-                }
+                group_sync(bid, bthreads);
+                continue;
             }
-            __syncthreads();
-            continue;
-        }
-        __syncthreads();
-        T dk = act ? LM(w, k) : (T)1;
-        const bool dead = dk == (T)0 || !(fabs(dk) < (T)INFINITY);
-        if (dead) dk = (T)1;
-        uint64_t cb = mag_bits(dk);
-        uint32_t nf = 0;
-        if (act)
-            for (uint32_t p = d.lp[k] + warp; p < d.lp[k + 1]; p += nw) {
-                const uint32_t r = d.li[p];
-                const T v = LM(w, r);
-                LM(w, r) = (T)0;
-                const uint64_t vb = mag_bits(v);
-                cb = cb > vb ? cb : vb;
-                const T lv = v / dk;
-                if (F32 || (fl & 2u)) nf |= (uint32_t)(mag_bits(lv - lv) != 0);
-                LM(lx, p) = lv;
+            group_sync(bid, bthreads);
+            T dk = act ? W(k) : (T)1;
+            const bool dead = dk == (T)0 || !(fabs(dk) < (T)INFINITY);
+            if (dead) dk = (T)1;
+            uint64_t cb = mag_bits(dk);
+            uint32_t nf = 0;
+            if (act)
+                for (uint32_t p = d.lp[k] + gw; p < d.lp[k + 1]; p += gsize) {
+                    const uint32_t r = d.li[p];
+                    const T v = W(r);
+                    W(r) = (T)0;
+                    const uint64_t vb = mag_bits(v);
+                    cb = cb > vb ? cb : vb;
+                    const T lv2 = v / dk;
+                    if (F32 || (fl & 2u)) nf |= (uint32_t)(mag_bits(lv2 - lv2) != 0);
+                    LM(lx, p) = lv2;
+                    if (!(fl & 2u)) {
+                        const uint64_t lb = mag_bits(lv2);
+                        if (lb > ls.worst[lane]) atomicMax(&ls.worst[lane], lb);
+                    }
+                }
+            if (act) {
+                atomicMax(&cmax, cb);
+                if (nf) atomicOr(&ls.nonfinite[lane], 1u);
+            }
+            group_sync(bid, bthreads);
+            if (gw == 0 && act) {
+                LM(ud, k) = dk;
+                W(k) = (T)0;
+                uint32_t bad = dead ? 1u : 0u;
+                const double cm = bitsd(cmax);
                 if (!(fl & 2u)) {
-                    const uint64_t lb = mag_bits(lv);
-                    if (lb > ls.worst[lane]) atomicMax(&ls.worst[lane], lb);
+                    if (F32)
+                        bad |= (!(fabs((double)dk) >= 1e-12 * cm) || !(cm / fabs((double)dk) <= kWide)) ? 1u : 0u;
+                    else
+                        bad |= !(fabs((double)dk) >= 1e-12 * cm) ? 1u : 0u;
                 }
+                if (bad) atomicOr(&ls.bad[lane], 1u);
+                cmax = 0;
             }
-        if (act) {
-            atomicMax(&ls.cmax[lane], cb);
-            if (nf) atomicOr(&ls.nonfinite[lane], 1u);
-        }
-        __syncthreads();
-        if (warp == 0 && act) {
-            LM(ud, k) = dk;
-            LM(w, k) = (T)0;
-            uint32_t bad = dead ? 1u : 0u;
-            const double cmax = bitsd(ls.cmax[lane]);
-            if (!(fl & 2u)) {
-                if (F32)
-                    bad |= (!(fabs((double)dk) >= 1e-12 * cmax) || !(cmax / fabs((double)dk) <= kWide)) ? 1u : 0u;
-                else
-                    bad |= !(fabs((double)dk) >= 1e-12 * cmax) ? 1u : 0u;
-            }
-            ls.bad[lane] |= bad;
-            ls.cmax[lane] = 0;
+            group_sync(bid, bthreads);
         }
         __syncthreads();
     }

@@ -1080,6 +1080,51 @@ void level_plan(const Tape& t, LevelPlan& out) {
     bucket(lev, out.bl_ptr, out.bl_rows);
 }
 
+void col_plan(const Tape& t, uint32_t max_groups, ColPlan& out) {
+    out = ColPlan{};
+    const uint32_t n = t.n;
+    std::vector<uint32_t> lev(n, 0);
+    std::vector<uint64_t> work(n, 0);
+    uint32_t top = 0;
+    for (uint32_t k = 0; k < n; k++) {
+        uint32_t v = 0;
+        uint64_t wk = 1 + (t.lp[k + 1] - t.lp[k]);
+        for (uint32_t p = t.up[k]; p < t.up[k + 1]; p++) {
+            const uint32_t i = t.ui[p];
+            v = std::max(v, lev[i] + 1);
+            wk += 1 + (t.lp[i + 1] - t.lp[i]);
+        }
+        lev[k] = v;
+        work[k] = wk;
+        top = std::max(top, v + 1);
+    }
+    std::vector<std::vector<uint32_t>> by(top);
+    for (uint32_t k = 0; k < n; k++) by[lev[k]].push_back(k);
+    out.lv_ptr.push_back(0);
+    for (uint32_t v = 0; v < top; v++) {
+        const auto& cs = by[v];
+        uint32_t G = 1;
+        while (G * 2 <= std::min<uint32_t>(max_groups, (uint32_t)cs.size())) G *= 2;
+        // the heaviest columns first, each to the least loaded group
+        std::vector<uint32_t> order(cs.begin(), cs.end());
+        std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return work[a] > work[b]; });
+        std::vector<uint64_t> load(G, 0);
+        std::vector<std::vector<uint32_t>> grp(G);
+        for (uint32_t k : order) {
+            const uint32_t g = (uint32_t)(std::min_element(load.begin(), load.end()) - load.begin());
+            grp[g].push_back(k);
+            load[g] += work[k];
+        }
+        for (uint32_t g = 0; g < G; g++) {
+            std::sort(grp[g].begin(), grp[g].end());
+            out.gp.push_back((uint32_t)out.cols.size());
+            out.cols.insert(out.cols.end(), grp[g].begin(), grp[g].end());
+        }
+        out.gp.push_back((uint32_t)out.cols.size());
+        out.lv_ptr.push_back((uint32_t)out.gp.size());
+    }
+}
+
 bool stream_plan(const std::vector<uint32_t>& lev_ptr, const std::vector<uint32_t>& rows,
                  const std::vector<uint32_t>& row_ptr, const std::vector<uint32_t>& ent, uint32_t chunk,
                  uint32_t max_rows, uint32_t ahead, bool skip_empty, StreamPlan& out) {

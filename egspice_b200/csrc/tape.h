@@ -119,6 +119,20 @@ struct LevelPlan {
 };
 void level_plan(const Tape& t, LevelPlan& out);
 
+// The refactor's columns by levels, for a CTA that factors independent
+// columns at once: a column's level is one more than the highest level
+// among the columns whose L it reads (the rows of its U entries), so the
+// columns of a level read only finished columns and write only their own.
+// Each level's columns are dealt to G groups (G the largest power of two
+// not above the level's columns or max_groups), greedily by their work, the
+// heaviest first; a group takes its columns in tape order.
+//   lv_ptr[v] .. lv_ptr[v + 1]   level v's G + 1 group starts in gp
+//   gp[lv_ptr[v] + g]            first entry of group g's columns in cols
+struct ColPlan {
+    std::vector<uint32_t> lv_ptr, gp, cols;
+};
+void col_plan(const Tape& t, uint32_t max_groups, ColPlan& out);
+
 // A sweep of the level schedule in streaming order, for solves that stage
 // the factor through shared memory: the sweep's entries in the order the
 // levels read them (level by level, row by row, a row's entries by
