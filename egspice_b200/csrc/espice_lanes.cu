@@ -1032,6 +1032,7 @@ espl_status upload_tape(espl_lanes* h, Group& g) {
         d.wk = nullptr;
         d.wk32 = nullptr;
         d.cl_ptr = d.cl_gp = d.cl_cols = nullptr;
+        d.cl_ustream = nullptr;
         d.n_cl = 0;
         d.nnz_l = (uint32_t)g.tape.li.size();
         d.nnz_u = (uint32_t)g.tape.ui.size();
@@ -1106,6 +1107,11 @@ espl_status upload_tape(espl_lanes* h, Group& g) {
             UP(cl_ptr, cp.lv_ptr);
             UP(cl_gp, cp.gp);
             UP(cl_cols, cp.cols);
+            {
+                const uint32_t* us = nullptr;
+                if ((s = dupload(h, own, &us, cp.ustream))) return s;
+                d.cl_ustream = reinterpret_cast<const uint4*>(us);
+            }
             // the same sweeps in streaming order, chunks of a ring slot
             StreamPlan fw, bw;
             if (stream_plan(lp.fl_ptr, lp.fl_rows, lp.rl_ptr, lp.rl_ent, kRingChunk, kRingRows, kRingSlots, true, fw) &&

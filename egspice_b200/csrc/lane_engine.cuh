@@ -142,6 +142,7 @@ struct GroupDev {
     // work vectors of the column groups past the first (kRefGroups - 1
     // copies of w, (n + 1) x P each; FP32 copies for a mixed handle), or null
     const uint32_t *cl_ptr, *cl_gp, *cl_cols;
+    const uint4* cl_ustream;  // per U entry: its row, its L column's bounds
     uint32_t n_cl, cl_pad;
     double* wk;
     float* wk32;

@@ -170,28 +170,30 @@ __device__ int lvl_refactor(const GroupDev& d, uint32_t l, uint32_t lane, uint32
                 for (uint32_t p = d.col_ptr[c] + gw; p < d.col_ptr[c + 1]; p += gsize) W(d.prow[p]) = (T)LM(a, p);
             group_sync(bid, bthreads);
             const uint32_t u0 = d.up[k], u1 = d.up[k + 1];
-            // The next U entry's row, L column bounds and the first kPre
-            // entries of this thread's share of its L column (values and
-            // rows) are loaded while the current entry's axpy runs: none of
+            // The next U entry's first kPre entries of this thread's share of
+            // its L column (values and rows) are loaded while the current
+            // entry's axpy runs, and its row and L bounds (the U entry
+            // stream, read in sequence) one entry earlier still: none of
             // them depends on the work vector.
             constexpr uint32_t kPre = 4;
+            const uint4* __restrict__ us = d.cl_ustream;
             T pv[kPre];
-            uint32_t pr[kPre], pi = 0, pe0 = 0, pe1 = 0;
-            auto preload = [&](uint32_t p) {
-                pi = d.ui[p];
-                pe0 = d.lp[pi] + gw;
-                pe1 = d.lp[pi + 1];
+            uint32_t pr[kPre];
+            uint4 pt = make_uint4(0, 0, 0, 0), nt = make_uint4(0, 0, 0, 0);
+            auto preload = [&](const uint4& t) {
+                pt = t;
 #pragma unroll
                 for (uint32_t r = 0; r < kPre; r++) {
-                    const uint32_t pl = pe0 + r * gsize;
-                    const bool ok = act && pl < pe1;
+                    const uint32_t pl = t.y + gw + r * gsize;
+                    const bool ok = act && pl < t.z;
                     pv[r] = ok ? LM(lx, pl) : (T)0;
                     pr[r] = ok ? d.li[pl] : 0u;
                 }
             };
-            if (u0 < u1) preload(u0);
+            if (u0 < u1) preload(us[u0]);
+            if (u0 + 1 < u1) nt = us[u0 + 1];
             for (uint32_t p = u0; p < u1; p++) {
-                const uint32_t i = pi, e0 = pe0, e1 = pe1;
+                const uint32_t i = pt.x, e0 = pt.y + gw, e1 = pt.z;
                 T cv[kPre];
                 uint32_t cr[kPre];
 #pragma unroll
@@ -199,7 +201,10 @@ __device__ int lvl_refactor(const GroupDev& d, uint32_t l, uint32_t lane, uint32
                     cv[r] = pv[r];
                     cr[r] = pr[r];
                 }
-                if (p + 1 < u1) preload(p + 1);
+                if (p + 1 < u1) {
+                    preload(nt);
+                    if (p + 2 < u1) nt = us[p + 2];
+                }
                 const T u = act ? W(i) : (T)0;
                 if (act) {
 #pragma unroll

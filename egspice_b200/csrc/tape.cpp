@@ -1098,6 +1098,14 @@ void col_plan(const Tape& t, uint32_t max_groups, ColPlan& out) {
         work[k] = wk;
         top = std::max(top, v + 1);
     }
+    out.ustream.resize(4 * (size_t)t.ui.size());
+    for (size_t p = 0; p < t.ui.size(); p++) {
+        const uint32_t i = t.ui[p];
+        out.ustream[4 * p] = i;
+        out.ustream[4 * p + 1] = t.lp[i];
+        out.ustream[4 * p + 2] = t.lp[i + 1];
+        out.ustream[4 * p + 3] = 0;
+    }
     std::vector<std::vector<uint32_t>> by(top);
     for (uint32_t k = 0; k < n; k++) by[lev[k]].push_back(k);
     out.lv_ptr.push_back(0);

@@ -128,8 +128,12 @@ void level_plan(const Tape& t, LevelPlan& out);
 // heaviest first; a group takes its columns in tape order.
 //   lv_ptr[v] .. lv_ptr[v + 1]   level v's G + 1 group starts in gp
 //   gp[lv_ptr[v] + g]            first entry of group g's columns in cols
+//   ustream[4 p .. 4 p + 3]      U entry p's row i and its L column's
+//                                bounds lp[i], lp[i + 1] (and a zero): the
+//                                refactor reads them in sequence instead of
+//                                as a chain of dependent loads
 struct ColPlan {
-    std::vector<uint32_t> lv_ptr, gp, cols;
+    std::vector<uint32_t> lv_ptr, gp, cols, ustream;
 };
 void col_plan(const Tape& t, uint32_t max_groups, ColPlan& out);
 
