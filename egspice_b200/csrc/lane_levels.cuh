@@ -170,53 +170,57 @@ __device__ int lvl_refactor(const GroupDev& d, uint32_t l, uint32_t lane, uint32
                 for (uint32_t p = d.col_ptr[c] + gw; p < d.col_ptr[c + 1]; p += gsize) W(d.prow[p]) = (T)LM(a, p);
             group_sync(bid, bthreads);
             const uint32_t u0 = d.up[k], u1 = d.up[k + 1];
-            // The next U entry's first kPre entries of this thread's share of
-            // its L column (values and rows) are loaded while the current
-            // entry's axpy runs, and its row and L bounds (the U entry
-            // stream, read in sequence) one entry earlier still: none of
-            // them depends on the work vector.
-            constexpr uint32_t kPre = 4;
+            // Two U entries' loads in flight: an entry's first kPre L entries
+            // of this thread's share (values and rows) are loaded two
+            // entries ahead, into the register set of its parity, and its
+            // row and L bounds (the U entry stream, read in sequence) four
+            // ahead. None of them depends on the work vector.
+            constexpr uint32_t kPre = 2;
+            struct Pre {
+                T v[kPre];
+                uint32_t r[kPre];
+                uint4 t;
+            };
             const uint4* __restrict__ us = d.cl_ustream;
-            T pv[kPre];
-            uint32_t pr[kPre];
-            uint4 pt = make_uint4(0, 0, 0, 0), nt = make_uint4(0, 0, 0, 0);
-            auto preload = [&](const uint4& t) {
-                pt = t;
+            const uint4 zero4 = make_uint4(0, 0, 0, 0);
+            auto fill = [&](Pre& x, const uint4& t) {
+                x.t = t;
 #pragma unroll
                 for (uint32_t r = 0; r < kPre; r++) {
                     const uint32_t pl = t.y + gw + r * gsize;
                     const bool ok = act && pl < t.z;
-                    pv[r] = ok ? LM(lx, pl) : (T)0;
-                    pr[r] = ok ? d.li[pl] : 0u;
+                    x.v[r] = ok ? LM(lx, pl) : (T)0;
+                    x.r[r] = ok ? d.li[pl] : 0u;
                 }
             };
-            if (u0 < u1) preload(us[u0]);
-            if (u0 + 1 < u1) nt = us[u0 + 1];
-            for (uint32_t p = u0; p < u1; p++) {
-                const uint32_t i = pt.x, e0 = pt.y + gw, e1 = pt.z;
-                T cv[kPre];
-                uint32_t cr[kPre];
-#pragma unroll
-                for (uint32_t r = 0; r < kPre; r++) {
-                    cv[r] = pv[r];
-                    cr[r] = pr[r];
-                }
-                if (p + 1 < u1) {
-                    preload(nt);
-                    if (p + 2 < u1) nt = us[p + 2];
-                }
+            Pre A, B;
+            uint4 q2 = zero4, q3 = zero4;  // the stream's entries p + 2 and p + 3
+            if (u0 < u1) fill(A, us[u0]);
+            if (u0 + 1 < u1) fill(B, us[u0 + 1]);
+            if (u0 + 2 < u1) q2 = us[u0 + 2];
+            if (u0 + 3 < u1) q3 = us[u0 + 3];
+            auto step = [&](uint32_t p, Pre& x) {
+                const uint32_t i = x.t.x, e0 = x.t.y + gw, e1 = x.t.z;
                 const T u = act ? W(i) : (T)0;
                 if (act) {
 #pragma unroll
                     for (uint32_t r = 0; r < kPre; r++)
-                        if (e0 + r * gsize < e1) W(cr[r]) -= cv[r] * u;
+                        if (e0 + r * gsize < e1) W(x.r[r]) -= x.v[r] * u;
                     for (uint32_t pl = e0 + kPre * gsize; pl < e1; pl += gsize) W(d.li[pl]) -= LM(lx, pl) * u;
                     if (gw == 0) {
                         LM(ux, p) = u;
                         if (mag_bits(u - u) != 0) atomicOr(&ls.nonfinite[lane], 1u);
                     }
                 }
+                // this set now takes entry p + 2
+                if (p + 2 < u1) fill(x, q2);
+                q2 = q3;
+                q3 = p + 4 < u1 ? us[p + 4] : zero4;
                 group_sync(bid, bthreads);
+            };
+            for (uint32_t p = u0; p < u1; p += 2) {
+                step(p, A);
+                if (p + 1 < u1) step(p + 1, B);
             }
             // the taken rows of the work vector (each U entry's row) go back to zero
             if (act)
