@@ -2462,7 +2462,10 @@ espl_status espl_autotune(const espl_netlist* nets, uint32_t n_nets, const espl_
     // templates, the options, and the device
     uint64_t key = 14695981039346656037ull;
     cudaDeviceProp prop{};
-    if (cudaGetDeviceProperties(&prop, (int)opts->device) != cudaSuccess) return ESPL_DRIVER;
+    if (cudaGetDeviceProperties(&prop, (int)opts->device) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return ESPL_NO_IMAGE;  // no such device (as espl_create reports it)
+    }
     key = fnv1a(key, prop.name, std::strlen(prop.name));
     key = fnv1a(key, opts, sizeof(*opts));
     key = fnv1a(key, &dt0, sizeof(dt0));

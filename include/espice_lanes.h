@@ -448,7 +448,8 @@ typedef struct {
  * process up). `choices` (n_nets entries) gets the best plan for
  * espl_set_plan. The result is cached for the process by the templates'
  * patterns, lane counts and device kinds, the device and the options: a
- * second call with the same inputs runs nothing. A learned predictor
+ * second call with the same inputs runs nothing. ESPL_NO_IMAGE without
+ * such a device, as espl_create. A learned predictor
  * (tran->predictor 2) is timed as the linear one. */
 espl_status espl_autotune(const espl_netlist *nets, uint32_t n_nets, const espl_create_opts *opts, double dt0,
                           const espl_tran_opts *tran, uint32_t trial_steps, uint32_t max_trials,

@@ -82,3 +82,31 @@ def test_noalloc_replay_refuses_a_pattern_that_is_not_the_tapes():
             assert st == 1 and b"col_ptr" in err.value, (bad, st, err.value)
     finally:
         L.espl_tape_free(h)
+
+
+def test_plan_entry_points_refuse_bad_arguments_without_a_gpu():
+    """The launch-plan entry points check their arguments before any device
+    work: a NULL handle or output is ESPL_INVALID_ARGUMENT; on a CPU-only
+    host the autotuner reports the driver's refusal instead of searching."""
+    import ctypes as C
+    import torch
+    from egspice_b200 import abi, decks
+    from egspice_b200.abi import PlanChoice, TuneReport
+    from egspice_b200.lanes import lib
+    L = lib()
+    assert C.sizeof(PlanChoice) == 16 and C.sizeof(TuneReport) == 24
+    assert L.espl_set_plan(None, None) == 1
+    assert L.espl_get_plan(None, None) == 1
+    net = decks.inverter_chain(2)
+    keep, arr = abi.cnets([net])
+    opts = abi.CreateOpts(abi.ABI_VERSION, 0, 0, 0, 0, 0)
+    topts = abi.tran_opts(t_stop=1e-9, dt=1e-12)
+    out = (PlanChoice * 1)()
+    rep = TuneReport()
+    # no templates, no options, no output, or zero trial steps: refused
+    assert L.espl_autotune(arr, 0, C.byref(opts), 0.0, C.byref(topts), 10, 4, out, C.byref(rep)) == 1
+    assert L.espl_autotune(arr, 1, None, 0.0, C.byref(topts), 10, 4, out, C.byref(rep)) == 1
+    assert L.espl_autotune(arr, 1, C.byref(opts), 0.0, C.byref(topts), 0, 4, out, C.byref(rep)) == 1
+    if not torch.cuda.is_available():
+        st = L.espl_autotune(arr, 1, C.byref(opts), 0.0, C.byref(topts), 10, 4, out, C.byref(rep))
+        assert st == 2  # ESPL_NO_IMAGE, as espl_create
