@@ -594,6 +594,8 @@ def main():
     ap.add_argument("--config3-steps", type=int, default=100, help="steps of the config-3 mesh run (of 1,000)")
     # the learned arm's step predictor
     ap.add_argument("--no-autotune", action="store_true", help="run the automatic launch plan, no search")
+    ap.add_argument("--polish-chord", action="store_true",
+                    help="polish iterations reuse the previous factor (espl_tran_opts.polish_chord), every arm")
     ap.add_argument("--tune-steps", type=int, default=200, help="transient attempts per autotuner trial")
     ap.add_argument("--tune-trials", type=int, default=10, help="autotuner trials per precision")
     ap.add_argument("--learn-warm", type=int, default=500, help="attempts with the linear predictor and recorder")
@@ -611,6 +613,7 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
 
     nets, topts = ring_workload(seed=rank, lanes=args.lanes, variants=args.variants)
+    topts.polish_chord = 1 if args.polish_chord else 0
     topts.max_steps = args.max_steps
     n_points = sum(n.lanes for n in nets)
     full = (args.lanes, args.variants, args.max_steps) == (16384, 32, 5000)

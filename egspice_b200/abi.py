@@ -45,7 +45,7 @@ class TranOpts(C.Structure):
                 ("reltol", C.c_double), ("abstol", C.c_double), ("chgtol", C.c_double), ("trtol", C.c_double),
                 ("vntol", C.c_double), ("residual_tol", C.c_double), ("method", C.c_uint32),
                 ("fixed_step", C.c_uint32), ("max_iter", C.c_uint32), ("max_steps", C.c_uint32),
-                ("predictor", C.c_uint32), ("reserved", C.c_uint32)]
+                ("predictor", C.c_uint32), ("polish_chord", C.c_uint32)]
 
 
 class StepReport(C.Structure):

@@ -2029,6 +2029,7 @@ espl_status espl_init_steps(espl_lanes* h, const espl_tran_opts* o) {
     t.max_iter = o->max_iter;
     t.max_steps = o->max_steps ? o->max_steps : 0xFFFFFFFFu;
     t.predictor = o->predictor;
+    t.polish_chord = o->polish_chord ? 1u : 0u;
     // Operating point at t = 0 with the sources at their t = 0 value, from
     // a cold start (tran.zig Run.init), on the static tape.
     for (auto& g : h->groups) {

@@ -210,13 +210,14 @@ struct NewtonParams {
     uint32_t mixed, stall_ticks;   // mixed: FP32 LU; a lane past stall_ticks refactors in FP64
     uint32_t refine;               // mixed: FP64-residual refinement sweeps per solve
     uint32_t polish_max;
+    uint32_t chord;                // polish iterations reuse the previous factor (shared-memory chain)
     const LadderLane* ladder;      // per lane (all templates' lanes), or null: gmin, init_fix, all lanes
 };
 
 struct TranParams {
     double t_stop, dt, dt_min, dt_max, reltol, abstol, chgtol, trtol, vntol, residual_tol;
     double delmin, min_break;
-    uint32_t method, fixed_step, max_iter, max_steps, predictor, launch_steps;
+    uint32_t method, fixed_step, max_iter, max_steps, predictor, launch_steps, polish_chord;
 };
 
 struct Companion {

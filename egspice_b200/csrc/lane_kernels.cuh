@@ -74,8 +74,11 @@ struct TileShared {
         double dt_next[32];
     };
     uint32_t method[32], on[32], accept[32], rot[32];  // on: bit 0 the lane attempts a step, bit 1 from xpred
-    uint32_t pit[32];  // the lane's polish iterations so far
+    // the lane's polish iterations so far (kPitMask), and kFactorHeld: its
+    // shared-memory factor is its last iteration's and held
+    uint32_t pit[32];
 };
+constexpr uint32_t kPitMask = 0xFFFFu, kFactorHeld = 0x10000u;
 
 constexpr uint32_t kNoRec = 0xFFFFFFFFu;
 
@@ -380,7 +383,11 @@ __device__ __forceinline__ void newton_tile(const TileCtx& c, LaneState* s, cons
                 if (band_solved && MIXED)
                     for (uint32_t r = 0; r < o.refine; r++) refine_mixed(d, l);
                 if (sm && (use32 || !MIXED)) {
-                    int rc = d.n_rec ? refactor_rec<T>(d, st, lane, l) : refactor_smem<T>(d, st, lane, l);
+                    // a polish iteration of a chord lane keeps the factor of
+                    // its previous iteration (still in shared memory)
+                    const bool keep = o.chord && (sh.pit[lane] & kPitMask) > 0 && (sh.pit[lane] & kFactorHeld);
+                    int rc = keep ? 0 : d.n_rec ? refactor_rec<T>(d, st, lane, l) : refactor_smem<T>(d, st, lane, l);
+                    sh.pit[lane] = (sh.pit[lane] & kPitMask) | (rc == 0 ? kFactorHeld : 0u);
                     if (MIXED && rc != 0) {
                         s->fp64 = 1;
                         s->fallbacks++;
@@ -498,7 +505,7 @@ __device__ __forceinline__ void newton_tile(const TileCtx& c, LaneState* s, cons
                 bool ok = !(f & kLimited) && it != 0 && !(scaled >= 1.0) && !(f & (kImplausible | kResidualMiss));
                 if (ok && (sh.bits[lane] & kInitFix)) {
                     sh.bits[lane] &= ~kInitFix;
-                } else if (ok && o.polish > 0.0 && !(scaled < o.polish) && sh.pit[lane] < o.polish_max) {
+                } else if (ok && o.polish > 0.0 && !(scaled < o.polish) && (sh.pit[lane] & kPitMask) < o.polish_max) {
                     // the polish: Newton's test passed but not the tightened
                     // one; the lane goes on from x + dx
                     sh.pit[lane]++;
@@ -814,6 +821,7 @@ __global__ void __launch_bounds__(WIDE ? kWideThreads : kTileThreads, WIDE ? 1 :
     NewtonParams np = no;
     np.init_fix = 0;
     np.max_iter = o.max_iter;
+    np.chord = o.polish_chord;
     for (uint32_t attempt = 0; attempt < o.launch_steps; attempt++) {
         // stepBegin (kernels/lane.zig:508-545).
         if (warp == 0) {

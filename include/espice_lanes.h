@@ -253,7 +253,12 @@ typedef struct {
     uint32_t max_iter;   /* Newton iterations per step (ITL4-like) */
     uint32_t max_steps;
     uint32_t predictor;  /* 0 none (x_prev), 1 linear (SPICE xfact), 2 learned */
-    uint32_t reserved;
+    uint32_t polish_chord; /* with espl_create_opts.polish: 1 lets a lane's polish
+                            * iterations (those after its step passed the
+                            * reference's test) reuse the factor of its previous
+                            * iteration (a chord step: the residual is fresh, the
+                            * LU replay is skipped) where the tile keeps its factor
+                            * in shared memory; 0 refactors every iteration */
 } espl_tran_opts;
 
 /* `StepReport` (src/solver/kernels/lane.zig:441-451) per lane, with this
