@@ -448,7 +448,8 @@ typedef struct {
  * one resident tile per SM fewer) are each timed on a scratch handle
  * created with `opts` and `dt0` (the operating point, then `trial_steps`
  * transient attempts of every lane; the device time of that launch), and a
- * move is kept when it is at least 2 % faster; at most `max_trials`
+ * move is kept when two timings of it (the second taken when the first is
+ * at least 3 % faster) are both at least 2 % faster; at most `max_trials`
  * transients (the automatic plan's two runs included: the first warms the
  * process up). `choices` (n_nets entries) gets the best plan for
  * espl_set_plan. The result is cached for the process by the templates'
